@@ -1,0 +1,569 @@
+// C ABI of the library: the device API (lepic_dev_*) and the Fortran
+// drop-in routines with the reference's names and argument lists.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lepic_internal.cuh"
+
+using namespace lepic;
+
+// Fortran COMMON blocks (Src/particle_info.h:53-70, Src/constants.h).  Weak,
+// so that the Fortran program's own COMMON storage wins when both exist.
+extern "C" {
+__attribute__((weak)) lepic_part_info_int_t part_info_int_ = {};
+__attribute__((weak)) lepic_part_info_dp_1_t part_info_dp_1_ = {};
+__attribute__((weak)) lepic_part_info_dp_2_t part_info_dp_2_ = {};
+__attribute__((weak)) lepic_part_info_dp_3_t part_info_dp_3_ = {};
+__attribute__((weak)) lepic_constants_t constants_ = {};
+}
+
+namespace {
+
+thread_local int g_last = 0;
+
+inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
+
+void record(int rc) {
+  if (rc && !g_last) g_last = rc;
+}
+
+// lepic_phys_t from the COMMON blocks (what the Fortran routines read)
+lepic_phys_t phys_from_common(int ntype) {
+  lepic_phys_t P;
+  memset(&P, 0, sizeof(P));
+  P.ntype = ntype;
+  for (int p = 0; p < LEPIC_NPART; ++p) {
+    P.charge[p] = part_info_dp_1_.charge[p];
+    P.mass[p] = part_info_dp_1_.mass[p];
+    P.vt0[p] = part_info_dp_1_.vt0[p];
+    P.Nm[p] = part_info_dp_2_.Nm[p];
+    P.np_mx[p] = part_info_dp_3_.np_mx[p];
+    P.nu_uplim[p] = part_info_dp_3_.nu_uplim[p];
+  }
+  P.dt = part_info_dp_2_.dt;
+  P.xmax = part_info_dp_2_.xmax;
+  P.ymax = part_info_dp_2_.ymax;
+  P.zmax = part_info_dp_2_.zmax;
+  P.x_load = part_info_dp_2_.x_load;
+  P.qe = constants_.qe;
+  P.eps0 = constants_.eps0;
+  P.pi = constants_.pi;
+  P.flag_B = part_info_int_.flag_B;
+  P.flag_B_pos = part_info_int_.flag_B_pos;
+  P.flag_pbc = part_info_int_.flag_pbc;
+  P.flag_nmn = part_info_int_.flag_nmn;
+  P.ns_coll = part_info_int_.ns_coll;
+  P.n_cell = part_info_int_.n_cell;
+  P.np_cell = part_info_int_.np_cell;
+  return P;
+}
+
+// device staging buffer keyed by name, with a host->device upload
+template <class T>
+T *upload(const char *name, const T *h, size_t n, cudaStream_t s) {
+  T *d = (T *)scratch(name, sizeof(T) * (n ? n : 1));
+  if (d && n) cudaMemcpyAsync(d, h, sizeof(T) * n, cudaMemcpyHostToDevice, s);
+  return d;
+}
+
+__global__ void k_aos_to_soa(const double *aos, double *soa, long long n, long long cap) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= 6 * n) return;
+  long long i = t / 6;
+  int c = (int)(t % 6);
+  soa[c * cap + i] = aos[t];
+}
+
+__global__ void k_soa_to_aos(const double *soa, double *aos, long long n, long long cap) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= 6 * n) return;
+  long long i = t / 6;
+  int c = (int)(t % 6);
+  aos[t] = soa[c * cap + i];
+}
+
+// Device-resident copy of one host species slice vxp(6, 1:np, ptype, 1).
+struct StagedSpecies {
+  lepic_species_f64_t s;
+  double *aos = nullptr;
+  int n = 0;
+};
+
+int stage_species(StagedSpecies &st, const double *vxp_h, int np, int nmax, int slot,
+                  const signed char *flag_dead_h, cudaStream_t s) {
+  char nm[48];
+  long long cap = nmax;
+  snprintf(nm, sizeof nm, "dropin_p%d", slot);
+  st.s.p = (double *)scratch(nm, sizeof(double) * 6 * cap);
+  snprintf(nm, sizeof nm, "dropin_q%d", slot);
+  st.s.p_alt = (double *)scratch(nm, sizeof(double) * 6 * cap);
+  snprintf(nm, sizeof nm, "dropin_cnt%d", slot);
+  st.s.count = (int *)scratch(nm, sizeof(int));
+  snprintf(nm, sizeof nm, "dropin_key%d", slot);
+  st.s.key = (int *)scratch(nm, sizeof(int) * cap);
+  snprintf(nm, sizeof nm, "dropin_aos%d", slot);
+  st.aos = (double *)scratch(nm, sizeof(double) * 6 * cap);
+  snprintf(nm, sizeof nm, "dropin_fd%d", slot);
+  st.s.flag_dead = (signed char *)scratch(nm, cap);
+  st.s.cap = nmax;
+  st.n = np;
+  if (!st.s.p || !st.s.p_alt || !st.s.count || !st.s.key || !st.aos || !st.s.flag_dead)
+    return LEPIC_ERR_CUDA;
+  LEPIC_CUDA(cudaMemcpyAsync(st.s.count, &st.n, sizeof(int), cudaMemcpyHostToDevice, s));
+  if (np > 0) {
+    LEPIC_CUDA(cudaMemcpyAsync(st.aos, vxp_h, sizeof(double) * 6 * (size_t)np, cudaMemcpyHostToDevice, s));
+    k_aos_to_soa<<<grid_for(6LL * np, 256), 256, 0, s>>>(st.aos, st.s.p, np, cap);
+  }
+  if (flag_dead_h) {
+    LEPIC_CUDA(cudaMemcpyAsync(st.s.flag_dead, flag_dead_h, (size_t)nmax, cudaMemcpyHostToDevice, s));
+  } else {
+    LEPIC_CUDA(cudaMemsetAsync(st.s.flag_dead, 0, (size_t)nmax, s));
+  }
+  LEPIC_CUDA(cudaGetLastError());
+  return LEPIC_OK;
+}
+
+int unstage_species(StagedSpecies &st, double *vxp_h, int *np_out, signed char *flag_dead_h,
+                    int nmax, cudaStream_t s) {
+  int n = 0;
+  LEPIC_CUDA(cudaMemcpyAsync(&n, st.s.count, sizeof(int), cudaMemcpyDeviceToHost, s));
+  LEPIC_CUDA(cudaStreamSynchronize(s));
+  if (n > nmax) n = nmax;
+  if (n > 0) {
+    k_soa_to_aos<<<grid_for(6LL * n, 256), 256, 0, s>>>(st.s.p, st.aos, n, st.s.cap);
+    LEPIC_CUDA(cudaGetLastError());
+    LEPIC_CUDA(cudaMemcpyAsync(vxp_h, st.aos, sizeof(double) * 6 * (size_t)n, cudaMemcpyDeviceToHost, s));
+  }
+  if (flag_dead_h)
+    LEPIC_CUDA(cudaMemcpyAsync(flag_dead_h, st.s.flag_dead, (size_t)nmax, cudaMemcpyDeviceToHost, s));
+  LEPIC_CUDA(cudaStreamSynchronize(s));
+  if (np_out) *np_out = n;
+  return LEPIC_OK;
+}
+
+// Geometry staging for the drop-ins: bcnd, kq and the cell-wall mask.
+int stage_grid(lepic_grid_t &g, const int *n, const double *h, const int *bcnd_h, const double *kq_h,
+               cudaStream_t s) {
+  Dims d(n);
+  for (int a = 0; a < 3; ++a) {
+    g.n[a] = n[a];
+    g.h[a] = h ? h[a] : 0.0;
+  }
+  g.bcnd = upload("dropin_bcnd", bcnd_h, (size_t)d.cnt(), s);
+  if (!g.bcnd) return LEPIC_ERR_CUDA;
+  g.kq = kq_h ? upload("dropin_kq", kq_h, (size_t)d.cnt(), s) : nullptr;
+  unsigned char *cw = (unsigned char *)scratch("dropin_cw", (size_t)((d.N1 - 1) * (d.N2 - 1) * (d.N3 - 1)));
+  if (!cw) return LEPIC_ERR_CUDA;
+  int rc = launch_cell_wall(d, g.bcnd, cw, s);
+  g.cell_wall = cw;
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lepic_gpu_last_error(void) {
+  int r = g_last;
+  g_last = 0;
+  return r;
+}
+
+const char *lepic_gpu_strerror(int code) {
+  switch (code) {
+    case LEPIC_OK: return "ok";
+    case LEPIC_ERR_CAPACITY: return "particle array capacity (nmax) exceeded";
+    case LEPIC_ERR_DIVERGED: return "PDE solver is diverging";
+    case LEPIC_ERR_PMAX: return "collision probability greater than 1";
+    case LEPIC_ERR_EKR_TABLE: return "collision energy above the cross-section table";
+    case LEPIC_ERR_NEG_ENERGY: return "negative collision energy";
+    case LEPIC_ERR_UNSUPPORTED: return "option not supported by the GPU path";
+    case LEPIC_ERR_FEW_COLL: return "collision time step too small for electrons";
+    case LEPIC_ERR_CUDA: return "CUDA runtime error";
+    case LEPIC_ERR_ARG: return "invalid argument";
+    case LEPIC_ERR_CELL: return "particle outside the grid";
+    case LEPIC_ERR_NOT_CONVERGED: return "iteration cap reached";
+    default: return "unknown status";
+  }
+}
+
+const char *lepic_build_info(void) {
+  static char buf[128];
+  snprintf(buf, sizeof buf, "lepic_gpu sm_100a nvcc %d.%d fmad=off", __CUDACC_VER_MAJOR__,
+           __CUDACC_VER_MINOR__);
+  return buf;
+}
+
+int lepic_dev_info(int *sm_count, char *name, int name_len) {
+  Ctx &c = ctx();
+  if (sm_count) *sm_count = c.sms;
+  if (name && name_len > 0) {
+    strncpy(name, c.prop.name, (size_t)name_len - 1);
+    name[name_len - 1] = 0;
+  }
+  return c.sms > 0 ? LEPIC_OK : LEPIC_ERR_CUDA;
+}
+
+// ------------------------------------------------------------ device API
+int lepic_dev_calc_rho(const lepic_grid_t *g, double *np, double *rhs, int ntype,
+                       const lepic_phys_t *P, void *stream) {
+  if (!g || !P || ntype < 1 || ntype > LEPIC_NPART) return LEPIC_ERR_ARG;
+  return launch_calc_rho(Dims(g->n), np, rhs, g->bcnd, ntype, *P, S(stream));
+}
+
+int lepic_dev_calc_efield(const lepic_grid_t *g, const double *phi, double *Ei, void *stream) {
+  if (!g) return LEPIC_ERR_ARG;
+  return launch_efield(Dims(g->n), g->h, phi, Ei, g->bcnd, S(stream));
+}
+
+int lepic_dev_pdesolver(const lepic_grid_t *g, double *u, const double *b, int ncycl, double eps,
+                        double omega, int ng, const lepic_phys_t *P, int *k, double *ktot,
+                        double *res, void *stream) {
+  if (!g || !P) return LEPIC_ERR_ARG;
+  if (P->flag_pbc || P->flag_nmn) return LEPIC_ERR_UNSUPPORTED;
+  return launch_pdesolver(Dims(g->n), g->h, u, b, g->bcnd, ncycl, eps, omega, ng, P->eps0, k, ktot,
+                          res, S(stream));
+}
+
+int lepic_dev_part_mover(const lepic_grid_t *g, const double *Ei, lepic_species_f64_t *s, int ptype,
+                         int ntype, int ngrid, const lepic_phys_t *P, double *p_mac,
+                         double *P_loss, void *stream) {
+  if (!g || !s || !P || ptype < 1 || ptype > ntype) return LEPIC_ERR_ARG;
+  return launch_part_mover(*g, Ei, *s, ptype, ntype, ngrid, *P, p_mac, P_loss, S(stream));
+}
+
+int lepic_dev_charge_deposition(const lepic_grid_t *g, const lepic_species_f64_t *s, int ptype,
+                                const lepic_phys_t *P, double *np, void *stream) {
+  if (!g || !s || !P || ptype < 1) return LEPIC_ERR_ARG;
+  return launch_deposit(*g, *s, ptype, *P, np, S(stream));
+}
+
+int lepic_dev_part_sorting(const lepic_grid_t *g, lepic_species_f64_t *s, int *Plist, int pl_max,
+                           void *stream) {
+  if (!g || !s || pl_max < 1) return LEPIC_ERR_ARG;
+  return launch_sort(*g, *s, Plist, pl_max, S(stream));
+}
+
+int lepic_dev_collisions(const lepic_grid_t *g, lepic_species_f64_t *sp, int ntype,
+                         const lepic_tables_t *T, const lepic_phys_t *P, unsigned long long seed,
+                         unsigned long long call_index, double *nu_max, long long *counts,
+                         void *stream) {
+  if (!g || !sp || !T || !P || ntype < 1) return LEPIC_ERR_ARG;
+  return launch_collisions(*g, sp, ntype, *T, *P, seed, call_index, nu_max, counts, S(stream));
+}
+
+int lepic_dev_load_uniform(const lepic_grid_t *g, lepic_species_f64_t *sp, int ntype,
+                           long long n_per_species, const lepic_phys_t *P, unsigned long long seed,
+                           void *stream) {
+  if (!g || !sp || !P || ntype < 1 || ntype > LEPIC_NPART || n_per_species < 0) return LEPIC_ERR_ARG;
+  return launch_load_uniform(*g, sp, ntype, n_per_species, *P, seed, S(stream));
+}
+
+int lepic_dev_cell_wall(const int *n, const int *bcnd, unsigned char *cell_wall, void *stream) {
+  if (!n || !bcnd || !cell_wall) return LEPIC_ERR_ARG;
+  return launch_cell_wall(Dims(n), bcnd, cell_wall, S(stream));
+}
+
+int lepic_dev_dens_red(const lepic_grid_t *g, const double *np, double *np_red, int ntype,
+                       double *np_mx, void *stream) {
+  if (!g || ntype < 1 || ntype > LEPIC_NPART) return LEPIC_ERR_ARG;
+  return launch_dens_red(Dims(g->n), np, np_red, g->bcnd, ntype, np_mx, S(stream));
+}
+
+// ------------------------------------------------------------ drop-ins
+void calc_rho_(const int *n, double *np, double *rhs_dom, const int *bcnd, const int *ntype,
+               const int *nproc, const int *nproc_mpi, const int *mpi_rank) {
+  (void)mpi_rank;
+  if (*nproc != 1 || *nproc_mpi != 1) return record(LEPIC_ERR_UNSUPPORTED);
+  cudaStream_t s = 0;
+  Dims d(n);
+  lepic_phys_t P = phys_from_common(*ntype);
+  size_t nn = (size_t)d.cnt() * (size_t)*ntype;
+  double *np_d = upload("dropin_np", np, nn, s);
+  int *bc_d = upload("dropin_bcnd", bcnd, (size_t)d.cnt(), s);
+  double *rhs_d = (double *)scratch("dropin_rhs", sizeof(double) * (size_t)d.rcnt());
+  if (!np_d || !bc_d || !rhs_d) return record(LEPIC_ERR_CUDA);
+  int rc = launch_calc_rho(d, np_d, rhs_d, bc_d, *ntype, P, s);
+  if (rc) return record(rc);
+  cudaMemcpyAsync(rhs_dom, rhs_d, sizeof(double) * (size_t)d.rcnt(), cudaMemcpyDeviceToHost, s);
+  if (P.flag_pbc) cudaMemcpyAsync(np, np_d, sizeof(double) * nn, cudaMemcpyDeviceToHost, s);
+  record(check_err(s));
+}
+
+void dens_red_(const int *n, const double *np, double *np_red, const int *bcnd, const int *ntype,
+               const int *nproc, const int *nproc_mpi) {
+  if (*nproc != 1 || *nproc_mpi != 1) return record(LEPIC_ERR_UNSUPPORTED);
+  cudaStream_t s = 0;
+  Dims d(n);
+  size_t nn = (size_t)d.cnt() * (size_t)*ntype;
+  double *np_d = upload("dropin_np", np, nn, s);
+  int *bc_d = upload("dropin_bcnd", bcnd, (size_t)d.cnt(), s);
+  double *red_d = (double *)scratch("dropin_npred", sizeof(double) * nn);
+  if (!np_d || !bc_d || !red_d) return record(LEPIC_ERR_CUDA);
+  double mx[LEPIC_NPART] = {0};
+  int rc = launch_dens_red(d, np_d, red_d, bc_d, *ntype, mx, s);
+  if (rc) return record(rc);
+  cudaMemcpyAsync(np_red, red_d, sizeof(double) * nn, cudaMemcpyDeviceToHost, s);
+  for (int p = 0; p < *ntype; ++p) part_info_dp_3_.np_mx[p] = mx[p];
+  record(check_err(s));
+}
+
+void pdesolver_(double *u, const double *b, const int *bcnd, const double *h, const int *n,
+                const int *ncycl, const double *eps, const double *omega, int *k, double *ktot,
+                double *res, const int *ng, const int *rank, const int *nproc) {
+  (void)rank;
+  if (*nproc != 1) return record(LEPIC_ERR_UNSUPPORTED);
+  if (part_info_int_.flag_pbc || part_info_int_.flag_nmn) return record(LEPIC_ERR_UNSUPPORTED);
+  cudaStream_t s = 0;
+  Dims d(n);
+  // u(0:n1+2,0:n2+2,-1:n3+2): skip the z = -1 ghost plane (MPI halo only)
+  double *u0 = u + d.N1 * d.N2;
+  double *u_d = upload("dropin_u", u0, (size_t)d.cnt(), s);
+  double *b_d = upload("dropin_b", b, (size_t)d.rcnt(), s);
+  int *bc_d = upload("dropin_bcnd", bcnd, (size_t)d.cnt(), s);
+  if (!u_d || !b_d || !bc_d) return record(LEPIC_ERR_CUDA);
+  int rc = launch_pdesolver(d, h, u_d, b_d, bc_d, *ncycl, *eps, *omega, *ng, constants_.eps0, k, ktot,
+                            res, s);
+  cudaMemcpyAsync(u0, u_d, sizeof(double) * (size_t)d.cnt(), cudaMemcpyDeviceToHost, s);
+  record(rc);
+  record(check_err(s));
+}
+
+void calc_efield_(const int *n, const double *h, const double *phi, double *Ei, const int *bcnd) {
+  cudaStream_t s = 0;
+  Dims d(n);
+  double *phi_d = upload("dropin_u", phi, (size_t)d.cnt(), s);
+  double *E_d = upload("dropin_E", Ei, 3 * (size_t)d.cnt(), s);
+  int *bc_d = upload("dropin_bcnd", bcnd, (size_t)d.cnt(), s);
+  if (!phi_d || !E_d || !bc_d) return record(LEPIC_ERR_CUDA);
+  int rc = launch_efield(d, h, phi_d, E_d, bc_d, s);
+  if (rc) return record(rc);
+  cudaMemcpyAsync(Ei, E_d, sizeof(double) * 3 * (size_t)d.cnt(), cudaMemcpyDeviceToHost, s);
+  record(check_err(s));
+}
+
+void part_mover_(const int *n, const double *h, const double *Ei, const double *Bi, double *p_mac,
+                 double *P_loss, double *vxp, const int *bcnd, const int *nmax, const int *ntype,
+                 const int *ngrid, signed char *flag_dead, const int *nproc, int *np_tot,
+                 const int *iproc, const int *ptype, int *flag_cex, int *cnt_cex, double *cnt_dead,
+                 double *beam_div, double *sum_q_xz, double *sum_q_yz, const int *dtype,
+                 int *iseed, const int *n_B, const double *h_B) {
+  (void)flag_cex;
+  (void)cnt_cex;
+  (void)cnt_dead;
+  (void)beam_div;
+  (void)sum_q_xz;
+  (void)sum_q_yz;
+  (void)dtype;
+  (void)iseed;
+  (void)h_B;
+  if (*nproc != 1 || *iproc != 1) return record(LEPIC_ERR_UNSUPPORTED);
+  if (part_info_int_.flag_die || part_info_int_.tag_neg == *ptype || part_info_dp_1_.gam_sec > 0.0)
+    return record(LEPIC_ERR_UNSUPPORTED);
+  lepic_phys_t P = phys_from_common(*ntype);
+  if (P.flag_B == 1) {
+    if (n_B[0] != 1) return record(LEPIC_ERR_UNSUPPORTED);  // B-field maps
+    // Bi(1:3,1,1,1) of Bi(4,0:n_B(1)+2,0:n_B(2)+2,0:n_B(3)+2)
+    long long e1 = 4, e2 = 4LL * (n_B[0] + 3), e3 = 4LL * (n_B[0] + 3) * (n_B[1] + 3);
+    for (int c = 0; c < 3; ++c) P.Bconst[c] = Bi[c + e1 + e2 + e3];
+  }
+  cudaStream_t s = 0;
+  Dims d(n);
+  lepic_grid_t g;
+  int rc = stage_grid(g, n, h, bcnd, nullptr, s);
+  if (rc) return record(rc);
+  const int p = *ptype - 1;
+  const long long slice = 6LL * *nmax * p;
+  StagedSpecies st;
+  rc = stage_species(st, vxp + slice, np_tot[p], *nmax, 0, flag_dead + (long long)*nmax * p, s);
+  if (rc) return record(rc);
+  double *E_d = upload("dropin_E", Ei, 3 * (size_t)d.cnt(), s);
+  if (!E_d) return record(LEPIC_ERR_CUDA);
+  rc = launch_part_mover(g, E_d, st.s, *ptype, *ntype, *ngrid, P, p_mac, P_loss, s);
+  int rc2 = unstage_species(st, vxp + slice, &np_tot[p], flag_dead + (long long)*nmax * p, *nmax, s);
+  record(rc);
+  record(rc2);
+}
+
+void charge_deposition_(const int *n, const double *h, const double *vxp, const int *nmax,
+                        const int *ntype, const double *kq, double *np, const int *nproc,
+                        const int *np_tot, double *sum_dEk, int *Nh, const int *iproc,
+                        const int *ptype) {
+  (void)sum_dEk;
+  (void)Nh;
+  if (*nproc != 1 || *iproc != 1) return record(LEPIC_ERR_UNSUPPORTED);
+  if (part_info_dp_2_.Pabs > 0.0 && *ptype == 1) return record(LEPIC_ERR_UNSUPPORTED);
+  cudaStream_t s = 0;
+  Dims d(n);
+  lepic_phys_t P = phys_from_common(*ntype);
+  lepic_grid_t g;
+  for (int a = 0; a < 3; ++a) {
+    g.n[a] = n[a];
+    g.h[a] = h[a];
+  }
+  g.bcnd = nullptr;
+  g.cell_wall = nullptr;
+  g.kq = upload("dropin_kq", kq, (size_t)d.cnt(), s);
+  const int p = *ptype - 1;
+  double *np_slice = np + (long long)d.cnt() * p;
+  double *np_d = upload("dropin_npdep", np_slice, (size_t)d.cnt(), s);
+  if (!g.kq || !np_d) return record(LEPIC_ERR_CUDA);
+  StagedSpecies st;
+  int rc = stage_species(st, vxp + 6LL * *nmax * p, np_tot[p], *nmax, 0, nullptr, s);
+  if (rc) return record(rc);
+  rc = launch_deposit(g, st.s, *ptype, P, np_d, s);
+  if (rc) return record(rc);
+  cudaMemcpyAsync(np_slice, np_d, sizeof(double) * (size_t)d.cnt(), cudaMemcpyDeviceToHost, s);
+  record(check_err(s));
+}
+
+void part_sorting_(double *vxp, double *sorting, const int *nmax, const int *ntype, const int *n,
+                   const double *h, int *Plist_thd, const int *pl_max, const int *nproc,
+                   const int *np_tot, const int *ptype) {
+  (void)sorting;
+  if (*nproc != 1) return record(LEPIC_ERR_UNSUPPORTED);
+  cudaStream_t s = 0;
+  lepic_grid_t g;
+  for (int a = 0; a < 3; ++a) {
+    g.n[a] = n[a];
+    g.h[a] = h[a];
+  }
+  g.bcnd = nullptr;
+  g.kq = nullptr;
+  g.cell_wall = nullptr;
+  const int p = *ptype - 1;
+  StagedSpecies st;
+  int rc = stage_species(st, vxp + 6LL * *nmax * p, np_tot[p], *nmax, 0, nullptr, s);
+  if (rc) return record(rc);
+  int *pl_d = (int *)scratch("dropin_plist", sizeof(int) * (size_t)(*pl_max + 1));
+  if (!pl_d) return record(LEPIC_ERR_CUDA);
+  rc = launch_sort(g, st.s, pl_d, *pl_max, s);
+  if (rc) return record(rc);
+  int np_out = 0;
+  rc = unstage_species(st, vxp + 6LL * *nmax * p, &np_out, nullptr, *nmax, s);
+  if (rc) return record(rc);
+  (void)ntype;
+  cudaMemcpy(Plist_thd + (long long)(*pl_max + 1) * p, pl_d, sizeof(int) * (size_t)(*pl_max + 1),
+             cudaMemcpyDeviceToHost);
+  record(check_err(s));
+}
+
+void collisions_(const int *it, double *vxp, const int *n, const double *h, const int *ntype,
+                 const int *nmax, const double *sig, const double *sig_Er, const int *sig_list,
+                 const double *sig_Eex, const int *ncol_mx, const int *npt_mx, double *cnt_col,
+                 double *P_loss, int *sour_xy, int *sour_xz, const int *Plist, const int *pl_max,
+                 const double *sigv_mx, const int *col_info, const double *np_red,
+                 signed char *flag_dead, int *flag_cex, const int *nproc, int *np_tot, int *iseed,
+                 const int *nproc_mpi, const int *mpi_rank, double *ss2D_xy, double *ss2D_xz,
+                 double *ss2D_yz, const int *flag_diag) {
+  (void)P_loss;
+  (void)sour_xy;
+  (void)sour_xz;
+  (void)Plist;
+  (void)pl_max;
+  (void)flag_cex;
+  (void)mpi_rank;
+  (void)ss2D_xy;
+  (void)ss2D_xz;
+  (void)ss2D_yz;
+  if (*nproc != 1 || *nproc_mpi != 1 || *flag_diag != 0) return record(LEPIC_ERR_UNSUPPORTED);
+  const int nt = *ntype;
+  if (nt > 3) return record(LEPIC_ERR_UNSUPPORTED);
+  cudaStream_t s = 0;
+  Dims d(n);
+  lepic_phys_t P = phys_from_common(nt);
+  lepic_grid_t g;
+  for (int a = 0; a < 3; ++a) {
+    g.n[a] = n[a];
+    g.h[a] = h[a];
+  }
+  g.bcnd = nullptr;
+  g.kq = nullptr;
+  g.cell_wall = nullptr;
+  const int ncol = part_info_int_.ncol;
+  if (ncol <= 0) return;
+  // tables (ordering output, reference layouts)
+  lepic_tables_t T;
+  memset(&T, 0, sizeof(T));
+  T.ncol = ncol;
+  T.npt = part_info_int_.sig_npt_mx;
+  T.npt_mx = *npt_mx;
+  T.sig_Er = upload("dropin_sigEr", sig_Er, (size_t)*npt_mx, s);
+  T.sig = upload("dropin_sig", sig, (size_t)*npt_mx * *ncol_mx, s);
+  T.sig_Eth = upload("dropin_sigEth", sig_Eex, (size_t)*ncol_mx, s);  // sig_Eex(:,ind_Eth)
+  std::vector<int> ci((size_t)ncol * 10);
+  for (int c = 0; c < ncol; ++c)
+    for (int q = 0; q < 10; ++q) ci[c + (size_t)ncol * q] = col_info[c + (size_t)*ncol_mx * q];
+  T.col_info_h = ci.data();
+  std::vector<int> sl((size_t)LEPIC_NPART * ncol);
+  std::vector<double> sv((size_t)LEPIC_NPART * ncol);
+  for (int c = 0; c < ncol; ++c)
+    for (int q = 0; q < LEPIC_NPART; ++q) {
+      sl[q + LEPIC_NPART * (size_t)c] = sig_list[q + LEPIC_NPART * (size_t)c];
+      sv[q + LEPIC_NPART * (size_t)c] = sigv_mx[q + LEPIC_NPART * (size_t)c];
+    }
+  T.sig_list = sl.data();
+  T.sigv_mx = sv.data();
+  T.p_ncol = part_info_int_.p_ncol;
+  if (!T.sig_Er || !T.sig || !T.sig_Eth) return record(LEPIC_ERR_CUDA);
+  StagedSpecies st[3];
+  lepic_species_f64_t sp[3];
+  for (int p = 0; p < nt; ++p) {
+    int rc = stage_species(st[p], vxp + 6LL * *nmax * p, np_tot[p], *nmax, p,
+                           flag_dead + (long long)*nmax * p, s);
+    if (rc) return record(rc);
+    sp[p] = st[p].s;
+  }
+  // region counters (Src/collisions.f90:153-157, 1005-1013)
+  RegionCount rgc;
+  memset(&rgc, 0, sizeof(rgc));
+  rgc.n_rg = part_info_int_.n_rg;
+  rgc.ncol_mx = *ncol_mx;
+  for (int q = 0; q < LEPIC_NM_RG; ++q) {
+    rgc.ixl[q] = part_info_int_.ixl_rg[q];
+    rgc.ixr[q] = part_info_int_.ixr_rg[q];
+  }
+  rgc.iyl = part_info_int_.iyl_rg;
+  rgc.iyr = part_info_int_.iyr_rg;
+  rgc.izl = part_info_int_.izl_rg;
+  rgc.izr = part_info_int_.izr_rg;
+  for (int p = 0; p < nt; ++p) {
+    double kk = h[0] * h[1] * h[2] / part_info_dp_2_.Nm[p];
+    for (int q = 0; q < rgc.n_rg && q < LEPIC_NM_RG; ++q) {
+      double sum = 0.0;
+      for (int iz = rgc.izl; iz <= rgc.izr; ++iz)
+        for (int iy = rgc.iyl; iy <= rgc.iyr; ++iy)
+          for (int ix = rgc.ixl[q]; ix <= rgc.ixr[q]; ++ix) sum += np_red[d.g(ix, iy, iz) + d.cnt() * p];
+      int np_rg = (int)(kk * sum);
+      rgc.w[p][q] = np_rg != 0 ? 1.0 / np_rg : 0.0;
+    }
+  }
+  size_t ncc = (size_t)*ncol_mx * (size_t)(rgc.n_rg > 0 ? rgc.n_rg : 1);
+  std::vector<double> cc_h(ncc, 0.0);
+  for (int q = 0; q < rgc.n_rg; ++q)
+    for (int c = 0; c < *ncol_mx; ++c)
+      cc_h[c + (size_t)*ncol_mx * q] = cnt_col[c + (size_t)*ncol_mx * (size_t)(*nproc) * q];
+  rgc.cnt_col_dev = upload("dropin_cntcol", cc_h.data(), ncc, s);
+  double nu_max[LEPIC_NPART] = {0};
+  long long counts[64] = {0};
+  unsigned long long seed = (unsigned long long)(unsigned)iseed[0];
+  int rc = launch_collisions(g, sp, nt, T, P, seed, (unsigned long long)*it, nu_max, counts, s,
+                             rgc.n_rg > 0 ? &rgc : nullptr);
+  for (int p = 0; p < nt; ++p) {
+    st[p].s = sp[p];
+    int rc2 = unstage_species(st[p], vxp + 6LL * *nmax * p, &np_tot[p],
+                              flag_dead + (long long)*nmax * p, *nmax, s);
+    record(rc2);
+  }
+  if (rgc.n_rg > 0) {
+    cudaMemcpy(cc_h.data(), rgc.cnt_col_dev, sizeof(double) * ncc, cudaMemcpyDeviceToHost);
+    for (int q = 0; q < rgc.n_rg; ++q)
+      for (int c = 0; c < *ncol_mx; ++c)
+        cnt_col[c + (size_t)*ncol_mx * (size_t)(*nproc) * q] = cc_h[c + (size_t)*ncol_mx * q];
+  }
+  for (int p = 0; p < nt; ++p) part_info_dp_3_.nu_max[p] = nu_max[p];
+  record(rc);
+}
+
+}  // extern "C"

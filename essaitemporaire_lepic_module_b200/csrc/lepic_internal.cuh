@@ -1,0 +1,131 @@
+// Internal declarations of the sm_100a PIC-MCC library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/lepic_gpu.h"
+
+namespace lepic {
+
+// Node-grid indexing of the reference arrays g(0:n1+2,0:n2+2,0:n3+2)
+// (column-major) and rhs arrays b(0:n1+1,0:n2+1,0:n3+1).
+struct Dims {
+  int n1, n2, n3;
+  long long N1, N2, N3;
+  __host__ __device__ Dims() : n1(0), n2(0), n3(0), N1(3), N2(3), N3(3) {}
+  __host__ __device__ Dims(int a, int b, int c) : n1(a), n2(b), n3(c), N1(a + 3), N2(b + 3), N3(c + 3) {}
+  __host__ __device__ explicit Dims(const int *n) : Dims(n[0], n[1], n[2]) {}
+  __host__ __device__ long long g(int ix, int iy, int iz) const { return ix + N1 * (iy + N2 * (long long)iz); }
+  __host__ __device__ long long cnt() const { return N1 * N2 * N3; }
+  __host__ __device__ long long r(int ix, int iy, int iz) const {
+    return ix + (N1 - 1) * (iy + (N2 - 1) * (long long)iz);
+  }
+  __host__ __device__ long long rcnt() const { return (N1 - 1) * (N2 - 1) * (N3 - 1); }
+  // cells with ix in 0..n1+1 (the clamped range of the loss test)
+  __host__ __device__ long long c(int ix, int iy, int iz) const {
+    return ix + (N1 - 1) * (iy + (N2 - 1) * (long long)iz);
+  }
+};
+
+// Device error word: [0] = first status code, [1] = detail (index / value).
+__device__ __forceinline__ void raise_err(int *err, int code, int info) {
+  if (atomicCAS(err, 0, code) == 0) err[1] = info;
+}
+
+// Per-device library context: error word, SM count, cached scratch.
+struct Ctx {
+  int device = -1;
+  int sms = 0;
+  int *d_err = nullptr;       // device int[2]
+  int *h_err = nullptr;       // pinned host int[2]
+  cudaDeviceProp prop{};
+};
+Ctx &ctx();                                     // context of the current device
+void *scratch(const char *name, size_t bytes);  // cached device buffer (grows)
+int check_err(cudaStream_t s);                  // sync, read + clear device error word
+int timer_start(const char *name, cudaStream_t s);  // -1 when timing is off
+void timer_stop(int id, cudaStream_t s);
+int cuda_status(cudaError_t e, const char *what);
+
+inline int grid_for(long long n, int block) {
+  long long g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > 2147483647LL) g = 2147483647LL;
+  return (int)g;
+}
+
+// ---------------------------------------------------------------- Philox
+// Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC'11): ten rounds of the
+// 32x32->64 multiply-xor round function with the published multipliers and
+// Weyl key increments.
+struct U4 { uint32_t x, y, z, w; };
+__host__ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    uint64_t p0 = (uint64_t)M0 * c.x, p1 = (uint64_t)M1 * c.z;
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    U4 n;
+    n.x = hi1 ^ c.y ^ k0;
+    n.y = lo1;
+    n.z = hi0 ^ c.w ^ k1;
+    n.w = lo0;
+    c = n;
+    k0 += W0;
+    k1 += W1;
+  }
+  return c;
+}
+// uniform in (0,1) from 32 random bits
+__host__ __device__ __forceinline__ double u01(uint32_t v) { return ((double)v + 0.5) * 2.3283064365386963e-10; }
+
+// ------------------------------------------------------------ launchers
+// fields.cu
+int launch_calc_rho(const Dims &d, double *np, double *rhs, const int *bcnd, int ntype,
+                    const lepic_phys_t &P, cudaStream_t s);
+int launch_dens_red(const Dims &d, const double *np, double *np_red, const int *bcnd, int ntype,
+                    double *np_mx_host, cudaStream_t s);
+int launch_efield(const Dims &d, const double h[3], const double *phi, double *Ei, const int *bcnd,
+                  cudaStream_t s);
+int launch_cell_wall(const Dims &d, const int *bcnd, unsigned char *cw, cudaStream_t s);
+// mg.cu
+int launch_pdesolver(const Dims &d, const double h[3], double *u, const double *b, const int *bcnd,
+                     int ncycl, double eps, double omega, int ng, double eps0, int *k, double *ktot,
+                     double *res, cudaStream_t s);
+// particles.cu
+int launch_part_mover(const lepic_grid_t &g, const double *Ei, lepic_species_f64_t &sp, int ptype,
+                      int ntype, int ngrid, const lepic_phys_t &P, double *p_mac, double *P_loss,
+                      cudaStream_t s);
+int launch_deposit(const lepic_grid_t &g, const lepic_species_f64_t &sp, int ptype,
+                   const lepic_phys_t &P, double *np, cudaStream_t s);
+int launch_sort(const lepic_grid_t &g, lepic_species_f64_t &sp, int *Plist, int pl_max,
+                cudaStream_t s);
+int launch_load_uniform(const lepic_grid_t &g, lepic_species_f64_t *sp, int ntype, long long n,
+                        const lepic_phys_t &P, unsigned long long seed, cudaStream_t s);
+int exclusive_scan_i32(const int *in, int *out, long long n, cudaStream_t s);
+// mcc.cu
+// Region counters of the drop-in path (Src/collisions.f90:1005-1013):
+// cnt_col(c, 1, i_rg) += 1/np_tot_rg(ptype, i_rg) for the first region that
+// contains the incident particle's cell.
+struct RegionCount {
+  double *cnt_col_dev;          // device (ncol_mx, n_rg) slice for iproc = 1
+  int n_rg, ncol_mx;
+  int ixl[LEPIC_NM_RG], ixr[LEPIC_NM_RG], iyl, iyr, izl, izr;
+  double w[LEPIC_NPART][LEPIC_NM_RG];
+};
+int launch_collisions(const lepic_grid_t &g, lepic_species_f64_t *sp, int ntype,
+                      const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
+                      unsigned long long call_index, double *nu_max, long long *counts,
+                      cudaStream_t s, const RegionCount *rg = nullptr);
+
+}  // namespace lepic
+
+#define LEPIC_CUDA(call)                                                 \
+  do {                                                                   \
+    cudaError_t e__ = (call);                                            \
+    if (e__ != cudaSuccess) return ::lepic::cuda_status(e__, #call);     \
+  } while (0)

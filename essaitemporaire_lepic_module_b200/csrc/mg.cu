@@ -1,0 +1,428 @@
+// Poisson solve of Src/pdesolver.f90 + Src/mg.f90 + Src/sors.f90 as ONE
+// persistent cooperative kernel: every V-cycle, every level, every
+// red-black sweep, the residual-ratio exit test of sor_rb and the outer
+// res/alpha < eps loop run on the device; the host sees a single launch.
+//
+// Schedule (identical to the reference, one MPI rank, Dirichlet walls):
+//   for each V-cycle k: down leg sor_rb(level l, dig<0) + restriction,
+//   coarsest sor_rb(dig=0) (up to 1e6 sweeps in cycle 1 until res <= eps,
+//   4 afterwards) + prolongation, up leg sor_rb(dig>0) + prolongation.
+//   sor_rb stops after 4 sweeps or when res/res_prev <= 0.6.
+//
+// Bit-exactness: node updates of one colour are independent, and every
+// expression keeps the Fortran evaluation order (the file is compiled with
+// --fmad=false), so the iterates equal the CPU oracle's.  The L1 residual is
+// summed per block in a fixed tree and then over blocks in block order by
+// every block, so all blocks take the same exit decision and the result is
+// deterministic run to run.
+//
+// Levels with few nodes (<= SMALL_NODES) are smoothed by block 0 alone with
+// __syncthreads, avoiding grid-wide barriers on the tiny coarse grids.
+#include <cooperative_groups.h>
+
+#include "lepic_internal.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace lepic {
+
+namespace {
+
+constexpr int MG_MAX = 13;
+constexpr int MG_BLOCK = 512;
+constexpr long long SMALL_NODES = 20000;
+
+struct MGLev {
+  int n1, n2, n3;
+  long long N1, N2;   // node extents n+3 in x, y
+  long long R1, R2;   // rhs extents n+2
+  double aw, ae, an, as, at, ab, ac;
+  double *u;          // (n+3)^3
+  double *b;          // (n+2)^3
+  int *bc;            // (n+3)^3
+  double *rf;         // (n+3)^3 fine residual scratch (levels that restrict)
+  __device__ long long g(int i, int j, int k) const { return i + N1 * (j + N2 * (long long)k); }
+  __device__ long long r(int i, int j, int k) const { return i + R1 * (j + R2 * (long long)k); }
+  __device__ long long nodes() const { return (long long)(n1 + 1) * (n2 + 1) * (n3 + 1); }
+};
+
+struct MGArgs {
+  MGLev L[MG_MAX + 1];
+  int ng, ncycl;
+  double alpha, eps, omega;
+  double *partial;    // [gridDim.x]
+  double *shared_d;   // [4]: small-level results
+  int *out_i;         // [0] k, [1] status, [2..] iterations per level of last cycle
+  double *out_d;      // [0] ktot, [1] res
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// deterministic block sum (fixed tree); result valid in all threads
+__device__ double block_sum(double v, double *sh) {
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  int nw = blockDim.x >> 5;
+  double t = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+  if (w == 0) t = warp_sum(t);
+  if (threadIdx.x == 0) sh[32] = t;
+  __syncthreads();
+  double r = sh[32];
+  __syncthreads();
+  return r;
+}
+
+// one colour of a red-black sweep, items [t0, items) strided by `stride`
+// colour 0 = red ((i+j+k) odd), 1 = black (Src/sors.f90:87-106, 249-267)
+__device__ __forceinline__ void sweep_colour(const MGLev &L, double omega, int colour, long long t0,
+                                             long long stride) {
+  const long long half = (L.n1 + 2) / 2;  // ceil((n1+1)/2)
+  const long long rows = (long long)(L.n2 + 1) * (L.n3 + 1);
+  const long long items = rows * half;
+  const long long sy = L.N1, sz = L.N1 * L.N2;
+  for (long long t = t0; t < items; t += stride) {
+    long long row = t / half;
+    int ii = (int)(t - row * half);
+    int j = 1 + (int)(row % (L.n2 + 1));
+    int k = 1 + (int)(row / (L.n2 + 1));
+    int ks = (k % 2 == 0) ? 0 : 1;
+    int is;
+    if (colour == 0) is = (j % 2 == 0) ? 1 : 2;
+    else is = (j % 2 == 0) ? 2 : 1;
+    is = is + ks;
+    if (is > 2) is = 1;
+    int i = is + 2 * ii;
+    if (i > L.n1 + 1) continue;
+    long long q = L.g(i, j, k);
+    if (L.bc[q] > 0) continue;
+    double tt = L.b[L.r(i, j, k)] - L.aw * L.u[q - 1] - L.an * L.u[q + sy] - L.as * L.u[q - sy] -
+                L.ae * L.u[q + 1] - L.at * L.u[q + sz] - L.ab * L.u[q - sz];
+    L.u[q] = (1.0 - omega) * L.u[q] + omega * tt / L.ac;
+  }
+}
+
+// sum of |residual| over plasma nodes handled by this thread
+__device__ __forceinline__ double residual_part(const MGLev &L, long long t0, long long stride) {
+  const long long nx = L.n1 + 1, ny = L.n2 + 1;
+  const long long tot = L.nodes();
+  const long long sy = L.N1, sz = L.N1 * L.N2;
+  double acc = 0.0;
+  for (long long t = t0; t < tot; t += stride) {
+    int i = 1 + (int)(t % nx);
+    int j = 1 + (int)((t / nx) % ny);
+    int k = 1 + (int)(t / (nx * ny));
+    long long q = L.g(i, j, k);
+    if (L.bc[q] != -1) continue;
+    double rij = L.b[L.r(i, j, k)] - (L.aw * L.u[q - 1] + L.an * L.u[q + sy] + L.as * L.u[q - sy] +
+                                      L.ae * L.u[q + 1] + L.ac * L.u[q] + L.at * L.u[q + sz] +
+                                      L.ab * L.u[q - sz]);
+    acc += fabs(rij);
+  }
+  return acc;
+}
+
+// Src/sors.f90:1-535, whole grid.  Returns res, ksor (uniform in all threads).
+__device__ void sor_rb(const MGArgs &a, const MGLev &L, int kmg, int dig, double eps_abs,
+                       cg::grid_group &grid, double *sh, double &res_out, int &ksor_out) {
+  long long nr = 4;
+  if (kmg == 1 && dig == 0) nr = 1000000;
+  const double eta = 0.6;
+  if (L.nodes() <= SMALL_NODES) {
+    if (blockIdx.x == 0) {
+      double res_s = 0.0, res = 0.0;
+      int ksor = 0;
+      for (long long l = 1; l <= nr; ++l) {
+        sweep_colour(L, a.omega, 0, threadIdx.x, blockDim.x);
+        __syncthreads();
+        sweep_colour(L, a.omega, 1, threadIdx.x, blockDim.x);
+        __syncthreads();
+        res = block_sum(residual_part(L, threadIdx.x, blockDim.x), sh);
+        ksor++;
+        bool stop = (dig == 0) ? (res <= eps_abs) : (res_s > 0.0 && (res / res_s) <= eta);
+        if (stop) break;
+        res_s = res;
+      }
+      if (threadIdx.x == 0) {
+        a.shared_d[0] = res;
+        a.shared_d[1] = (double)ksor;
+      }
+      __threadfence();
+    }
+    grid.sync();
+    res_out = a.shared_d[0];
+    ksor_out = (int)a.shared_d[1];
+    grid.sync();  // everyone has read shared_d before it is reused
+    return;
+  }
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  double res_s = 0.0, res = 0.0;
+  int ksor = 0;
+  for (long long l = 1; l <= nr; ++l) {
+    sweep_colour(L, a.omega, 0, tid, stride);
+    grid.sync();
+    sweep_colour(L, a.omega, 1, tid, stride);
+    grid.sync();
+    double part = block_sum(residual_part(L, tid, stride), sh);
+    if (threadIdx.x == 0) a.partial[blockIdx.x] = part;
+    grid.sync();
+    // every block sums the partials in the same fixed order
+    double v = 0.0;
+    if (threadIdx.x < 32) {
+      for (int bI = threadIdx.x; bI < (int)gridDim.x; bI += 32) v += a.partial[bI];
+      v = warp_sum(v);
+      if (threadIdx.x == 0) sh[33] = v;
+    }
+    __syncthreads();
+    res = sh[33];
+    __syncthreads();
+    ksor++;
+    bool stop = (dig == 0) ? (res <= eps_abs) : (res_s > 0.0 && (res / res_s) <= eta);
+    if (stop) break;
+    res_s = res;
+  }
+  res_out = res;
+  ksor_out = ksor;
+}
+
+// Src/mg.f90:808-847 (getres), Dirichlet form
+__device__ __forceinline__ double getres(const MGLev &L, long long q, double urhs) {
+  const long long sy = L.N1, sz = L.N1 * L.N2;
+  double uij = L.u[q], un = L.u[q + sy], us = L.u[q - sy], ue = L.u[q + 1];
+  double ut = L.u[q + sz], ub = L.u[q - sz], uw = L.u[q - 1];
+  return urhs - (L.aw * uw + L.ae * ue + L.an * un + L.as * us + L.ac * uij + L.at * ut + L.ab * ub);
+}
+
+__device__ __forceinline__ int fmap(int ic, int ncell) {
+  return ic == ncell / 2 + 2 ? ncell + 2 : (ic == 0 ? 0 : 2 * ic - 1);
+}
+
+// Src/mg.f90:248-805 (restriction), fine F -> coarse C
+__device__ void restriction(const MGLev &F, const MGLev &C, cg::grid_group &grid) {
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  {
+    const long long nx = F.n1 + 1, ny = F.n2 + 1, tot = F.nodes();
+    for (long long t = tid; t < tot; t += stride) {
+      int i = 1 + (int)(t % nx), j = 1 + (int)((t / nx) % ny), k = 1 + (int)(t / (nx * ny));
+      long long q = F.g(i, j, k);
+      F.rf[q] = (F.bc[q] > 0) ? 0.0 : getres(F, q, F.b[F.r(i, j, k)]);
+    }
+  }
+  grid.sync();
+  {
+    const long long CX = C.n1 + 3, CY = C.n2 + 3, tot = CX * CY * (C.n3 + 3);
+    const long long sy = F.N1, sz = F.N1 * F.N2;
+    for (long long t = tid; t < tot; t += stride) {
+      int i = (int)(t % CX), j = (int)((t / CX) % CY), k = (int)(t / (CX * CY));
+      long long qc = C.g(i, j, k);
+      int bc2 = F.bc[F.g(fmap(i, F.n1), fmap(j, F.n2), fmap(k, F.n3))];
+      C.bc[qc] = bc2;
+      C.u[qc] = 0.0;
+      if (i <= C.n1 + 1 && j <= C.n2 + 1 && k <= C.n3 + 1) {
+        double re = 0.0;
+        if (i >= 1 && j >= 1 && k >= 1 && bc2 <= 0) {
+          long long q = F.g(2 * i - 1, 2 * j - 1, 2 * k - 1);
+          const double *R = F.rf;
+          double r000 = R[q];
+          double rpp0 = R[q + 1 + sy], rp00 = R[q + 1], rpm0 = R[q + 1 - sy];
+          double r0m0 = R[q - sy], rmm0 = R[q - 1 - sy], rm00 = R[q - 1];
+          double rmp0 = R[q - 1 + sy], r0p0 = R[q + sy];
+          double r00p = R[q + sz], rppp = R[q + 1 + sy + sz], rp0p = R[q + 1 + sz];
+          double rpmp = R[q + 1 - sy + sz], r0mp = R[q - sy + sz];
+          double rmmp = R[q - 1 - sy + sz], rm0p = R[q - 1 + sz];
+          double rmpp = R[q - 1 + sy + sz], r0pp = R[q + sy + sz];
+          double r00m = R[q - sz], rppm = R[q + 1 + sy - sz], rp0m = R[q + 1 - sz];
+          double rpmm = R[q + 1 - sy - sz], r0mm = R[q - sy - sz];
+          double rmmm = R[q - 1 - sy - sz], rm0m = R[q - 1 - sz];
+          double rmpm = R[q - 1 + sy - sz], r0pm = R[q + sy - sz];
+          re = (8.0 * r000 + 4.0 * (rp00 + rm00 + r0p0 + r0m0 + r00p + r00m) +
+                2.0 * (rpp0 + rmp0 + rpm0 + rmm0 + rp0p + rm0p + r0pp + r0mp + rp0m + rm0m +
+                       r0pm + r0mm) +
+                rppp + rmpp + rpmp + rmmp + rppm + rmpm + rpmm + rmmm) /
+               64.0;
+        }
+        C.b[C.r(i, j, k)] = re;
+      }
+    }
+  }
+  grid.sync();
+}
+
+// Src/mg.f90:849-939 (prolongation): coarse C added into fine F
+__device__ void prolongation(const MGLev &F, const MGLev &C, cg::grid_group &grid) {
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long nx = C.n1 + 1, ny = C.n2 + 1, tot = C.nodes();
+  const long long sy = F.N1, sz = F.N1 * F.N2;
+  const long long cy = C.N1, cz = C.N1 * C.N2;
+  for (long long t = tid; t < tot; t += stride) {
+    int i = 1 + (int)(t % nx), j = 1 + (int)((t / nx) % ny), k = 1 + (int)(t / (nx * ny));
+    long long c = C.g(i, j, k);
+    const double *E = C.u;
+    double r000 = E[c], r0m0 = E[c - cy], rmm0 = E[c - 1 - cy], rm00 = E[c - 1];
+    double r00m = E[c - cz], r0mm = E[c - cy - cz], rmmm = E[c - 1 - cy - cz], rm0m = E[c - 1 - cz];
+    long long q = F.g(2 * i - 1, 2 * j - 1, 2 * k - 1);
+    double *U = F.u;
+    const int *B = F.bc;
+    if (B[q] <= 0) U[q] = U[q] + r000;
+    if (B[q - sy] <= 0) U[q - sy] = U[q - sy] + (r000 + r0m0) / 2.0;
+    if (B[q - 1 - sy] <= 0) U[q - 1 - sy] = U[q - 1 - sy] + (r000 + r0m0 + rmm0 + rm00) / 4.0;
+    if (B[q - 1] <= 0) U[q - 1] = U[q - 1] + (r000 + rm00) / 2.0;
+    if (B[q - sz] <= 0) U[q - sz] = U[q - sz] + (r000 + r00m) / 2.0;
+    if (B[q - sy - sz] <= 0) U[q - sy - sz] = U[q - sy - sz] + (r000 + r00m + r0mm + r0m0) / 4.0;
+    if (B[q - 1 - sz] <= 0) U[q - 1 - sz] = U[q - 1 - sz] + (r000 + r00m + rm0m + rm00) / 4.0;
+    if (B[q - 1 - sy - sz] <= 0)
+      U[q - 1 - sy - sz] =
+          U[q - 1 - sy - sz] + (r000 + r00m + rm0m + rm00 + r0m0 + r0mm + rmmm + rmm0) / 8.0;
+  }
+  grid.sync();
+}
+
+__global__ void __launch_bounds__(MG_BLOCK) k_pdesolver(const MGArgs *__restrict__ ap) {
+  cg::grid_group grid = cg::this_grid();
+  const MGArgs &a = *ap;
+  __shared__ double sh[40];
+  const int ng = a.ng;
+  int k = 1;
+  double res_s = 0.0, ktot = 0.0, r = 0.0;
+  int status = 0;
+  bool converged = false;
+  while (!converged) {
+    int iter[MG_MAX + 1];
+    for (int i = 0; i <= MG_MAX; ++i) iter[i] = 0;
+    const double eps_abs = a.alpha * a.eps;
+    for (int ig = 1; ig <= 2 * ng - 1; ++ig) {
+      int ksor = 0;
+      if (ig < ng) {
+        int il = ig;
+        sor_rb(a, a.L[il], k, ig - ng, eps_abs, grid, sh, r, ksor);
+        iter[il] += ksor;
+        restriction(a.L[il], a.L[il + 1], grid);
+      } else if (ig == ng) {
+        sor_rb(a, a.L[ng], k, 0, eps_abs, grid, sh, r, ksor);
+        iter[ng] += ksor;
+        if (ng >= 2) prolongation(a.L[ng - 1], a.L[ng], grid);
+      } else {
+        int il = 2 * ng - ig;
+        sor_rb(a, a.L[il], k, ig - ng, eps_abs, grid, sh, r, ksor);
+        iter[il] += ksor;
+        if (il >= 2) prolongation(a.L[il - 1], a.L[il], grid);
+      }
+    }
+    for (int i = 1; i <= ng; ++i) ktot = ktot + (double)(float)iter[i] / exp2((double)(2 * (i - 1)));
+    r = r / a.alpha;
+    if (k == 1) {
+      res_s = r;
+    } else if (fabs(r / res_s) > 10.0) {
+      status = LEPIC_ERR_DIVERGED;
+      converged = true;
+    }
+    if (r < a.eps || k == a.ncycl) converged = true;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      for (int i = 1; i <= ng; ++i) a.out_i[2 + i] = iter[i];
+    }
+    k = k + 1;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.out_i[0] = k;
+    a.out_i[1] = status;
+    a.out_d[0] = ktot;
+    a.out_d[1] = r;
+  }
+}
+
+}  // namespace
+
+int launch_pdesolver(const Dims &d, const double h[3], double *u, const double *b, const int *bcnd,
+                     int ncycl, double eps, double omega, int ng, double eps0, int *k_out,
+                     double *ktot_out, double *res_out, cudaStream_t s) {
+  if (ng < 1 || ng > MG_MAX) return LEPIC_ERR_ARG;
+  int n[3] = {d.n1, d.n2, d.n3};
+  for (int a = 0; a < 3; ++a)
+    if (n[a] % (1 << (ng - 1))) return LEPIC_ERR_ARG;
+  Ctx &c = ctx();
+  MGArgs A;
+  memset(&A, 0, sizeof(A));
+  A.ng = ng;
+  A.ncycl = ncycl;
+  A.eps = eps;
+  A.omega = omega;
+  char nm[32];
+  for (int l = 1; l <= ng; ++l) {
+    MGLev &L = A.L[l];
+    L.n1 = n[0] >> (l - 1);
+    L.n2 = n[1] >> (l - 1);
+    L.n3 = n[2] >> (l - 1);
+    L.N1 = L.n1 + 3;
+    L.N2 = L.n2 + 3;
+    L.R1 = L.n1 + 2;
+    L.R2 = L.n2 + 2;
+    double hl[3];
+    for (int q = 0; q < 3; ++q) hl[q] = h[q] * (double)(1 << (l - 1));
+    L.aw = eps0 / (hl[0] * hl[0]);
+    L.ae = L.aw;
+    L.an = eps0 / (hl[1] * hl[1]);
+    L.as = L.an;
+    L.at = eps0 / (hl[2] * hl[2]);
+    L.ab = L.at;
+    L.ac = -(L.an + L.as + L.aw + L.ae + L.at + L.ab);
+    long long nn = (long long)(L.n1 + 3) * (L.n2 + 3) * (L.n3 + 3);
+    long long nr = (long long)(L.n1 + 2) * (L.n2 + 2) * (L.n3 + 2);
+    if (l == 1) {
+      L.u = u;
+      L.b = const_cast<double *>(b);
+      L.bc = const_cast<int *>(bcnd);
+    } else {
+      snprintf(nm, sizeof nm, "mg_e%d", l);
+      L.u = (double *)scratch(nm, sizeof(double) * nn);
+      snprintf(nm, sizeof nm, "mg_r%d", l);
+      L.b = (double *)scratch(nm, sizeof(double) * nr);
+      snprintf(nm, sizeof nm, "mg_bc%d", l);
+      L.bc = (int *)scratch(nm, sizeof(int) * nn);
+      if (!L.u || !L.b || !L.bc) return LEPIC_ERR_CUDA;
+    }
+    if (l < ng) {
+      snprintf(nm, sizeof nm, "mg_rf%d", l);
+      L.rf = (double *)scratch(nm, sizeof(double) * nn);
+      if (!L.rf) return LEPIC_ERR_CUDA;
+      LEPIC_CUDA(cudaMemsetAsync(L.rf, 0, sizeof(double) * nn, s));
+    }
+  }
+  double ac = A.L[1].ac;
+  A.alpha = fabs((double)((n[0] + 1) * (n[1] + 1) * (n[2] + 1)) * ac) * 1.0;
+  int occ = 0;
+  LEPIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pdesolver, MG_BLOCK, 0));
+  if (occ < 1) return LEPIC_ERR_CUDA;
+  int blocks = c.sms * (occ < 2 ? occ : 2);
+  A.partial = (double *)scratch("mg_partial", sizeof(double) * blocks);
+  A.shared_d = (double *)scratch("mg_shared", sizeof(double) * 4);
+  A.out_i = (int *)scratch("mg_out_i", sizeof(int) * (MG_MAX + 4));
+  A.out_d = (double *)scratch("mg_out_d", sizeof(double) * 2);
+  if (!A.partial || !A.shared_d || !A.out_i || !A.out_d) return LEPIC_ERR_CUDA;
+  MGArgs *dA = (MGArgs *)scratch("mg_args", sizeof(MGArgs));
+  if (!dA) return LEPIC_ERR_CUDA;
+  LEPIC_CUDA(cudaMemcpyAsync(dA, &A, sizeof(MGArgs), cudaMemcpyHostToDevice, s));
+  void *args[] = {&dA};
+  int tm = timer_start("pdesolver_f64", s);
+  LEPIC_CUDA(cudaLaunchCooperativeKernel((void *)k_pdesolver, dim3(blocks), dim3(MG_BLOCK), args, 0, s));
+  timer_stop(tm, s);
+  int hi[MG_MAX + 4];
+  double hd[2];
+  LEPIC_CUDA(cudaMemcpyAsync(hi, A.out_i, sizeof(hi), cudaMemcpyDeviceToHost, s));
+  LEPIC_CUDA(cudaMemcpyAsync(hd, A.out_d, sizeof(hd), cudaMemcpyDeviceToHost, s));
+  LEPIC_CUDA(cudaStreamSynchronize(s));
+  if (k_out) *k_out = hi[0];
+  if (ktot_out) *ktot_out = hd[0];
+  if (res_out) *res_out = hd[1];
+  return hi[1];
+}
+
+}  // namespace lepic

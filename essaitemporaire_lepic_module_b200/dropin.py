@@ -1,0 +1,245 @@
+"""Python mirror of the reference's hot-path routines, calling the GPU drop-ins.
+
+Each function has the name and argument meaning of the legacy Fortran
+routine it stands for and passes numpy arrays in the reference's layouts to
+the C ABI of liblepic_gpu.so (the same entry points a Fortran build links).
+Errors raise ``LepicError`` (the reference calls stop_calculation).
+
+Array layouts (C-order numpy views of the Fortran arrays):
+  node grid    (n3+3, n2+3, n1+3)            bcnd, kq, phi
+  rhs grid     (n3+2, n2+2, n1+2)
+  Ei           (n3+3, n2+3, n1+3, 3)
+  np           (ntype, n3+3, n2+3, n1+3)
+  vxp          (ntype, nmax, 6)
+  u (pdesolver) (n3+4, n2+3, n1+3): z from -1 like phi_dom
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, commons, lib
+from .constants import AMU, C_LIGHT, EPS0, PI, QE
+
+
+def _i(v):
+    return C.byref(C.c_int(int(v)))
+
+
+def _d(v):
+    return C.byref(C.c_double(float(v)))
+
+
+def _pi(a):
+    return a.ctypes.data_as(_lib.P_int)
+
+
+def _pd(a):
+    return a.ctypes.data_as(_lib.P_dbl)
+
+
+def set_commons(st, ncol=0, npt=0, p_ncol=None):
+    """Fill the library's COMMON blocks the way read_input/read_reactions/main
+    fill the Fortran ones (Src/main.f90:124-579)."""
+    cm = commons()
+    pi_, d1, d2, d3, cs = (cm["part_info_int"], cm["part_info_dp_1"], cm["part_info_dp_2"],
+                           cm["part_info_dp_3"], cm["constants"])
+    C.memset(C.addressof(pi_), 0, C.sizeof(pi_))
+    C.memset(C.addressof(d1), 0, C.sizeof(d1))
+    C.memset(C.addressof(d2), 0, C.sizeof(d2))
+    C.memset(C.addressof(d3), 0, C.sizeof(d3))
+    pi_.np_cell = st.np_cell
+    pi_.ncol = ncol
+    pi_.sig_npt_mx = npt
+    pi_.n_cell = st.n_cell
+    pi_.flag_B = st.flag_B
+    pi_.ns_coll = st.wl.ns_coll
+    pi_.flag_pbc = st.geom.flag_pbc
+    pi_.flag_nmn = st.geom.flag_nmn
+    pi_.flag_die = st.geom.flag_die
+    if p_ncol is not None:
+        for i in range(len(p_ncol)):
+            pi_.p_ncol[i] = int(p_ncol[i])
+    for i in range(_lib.NPART):
+        d1.charge[i] = st.charge[i]
+        d1.mass[i] = st.mass[i]
+        d1.Ti[i] = st.Ti[i]
+        d1.vt0[i] = st.vt0[i]
+        d2.Nm[i] = st.Nm[i]
+        d3.np_mx[i] = st.np_mx[i]
+        d3.nu_uplim[i] = st.nu_uplim[i]
+    d1.k_eps0 = 1.0
+    d1.gam_sec = -1.0
+    d2.Pabs = -1.0
+    d2.n0 = st.wl.n0
+    d2.ngas = st.ngas
+    d2.dt = st.dt
+    d2.xmax, d2.ymax, d2.zmax = (float(v) for v in st.geom.box)
+    d2.x_load = st.x_load
+    cs.qe, cs.eps0, cs.c, cs.pi, cs.amu = QE, EPS0, C_LIGHT, PI, AMU
+
+
+def calc_rho(st, np_grids):
+    """Src/calc_rho.f90:1 -- returns rhs = -rho on (n3+2, n2+2, n1+2)."""
+    n = _lib.np_i(st.n)
+    npg = np.ascontiguousarray(np_grids, dtype=np.float64)
+    rhs = np.zeros((st.n[2] + 2, st.n[1] + 2, st.n[0] + 2))
+    bc = _lib.np_i(st.geom.bcnd)
+    lib().calc_rho_(_pi(n), _pd(npg), _pd(rhs), _pi(bc), _i(st.ntype), _i(1), _i(1), _i(0))
+    check(lib().lepic_gpu_last_error(), "calc_rho")
+    np_grids[...] = npg
+    return rhs
+
+
+def dens_red(st, np_grids):
+    """Src/calc_rho.f90:116 -- returns (np_red, np_mx[ntype])."""
+    n = _lib.np_i(st.n)
+    npg = np.ascontiguousarray(np_grids, dtype=np.float64)
+    red = np.zeros_like(npg)
+    bc = _lib.np_i(st.geom.bcnd)
+    lib().dens_red_(_pi(n), _pd(npg), _pd(red), _pi(bc), _i(st.ntype), _i(1), _i(1))
+    check(lib().lepic_gpu_last_error(), "dens_red")
+    d3 = commons()["part_info_dp_3"]
+    return red, np.array([d3.np_mx[i] for i in range(st.ntype)])
+
+
+def pdesolver(st, phi, rhs, eps=None, omega=None, ng=None, ncycl=None):
+    """Src/pdesolver.f90:1 -- solves in place into phi (n3+3, n2+3, n1+3);
+    returns (k, ktot, res) like the reference."""
+    wl = st.wl
+    eps = wl.eps if eps is None else eps
+    omega = wl.omega if omega is None else omega
+    ng = st.ng if ng is None else ng
+    ncycl = wl.ncycl if ncycl is None else ncycl
+    n = _lib.np_i(st.n)
+    u = np.zeros((st.n[2] + 4, st.n[1] + 3, st.n[0] + 3))
+    u[1:] = phi
+    b = np.ascontiguousarray(rhs, dtype=np.float64)
+    bc = _lib.np_i(st.geom.bcnd)
+    h = np.ascontiguousarray(st.h, dtype=np.float64)
+    k = C.c_int(0)
+    ktot = C.c_double(0)
+    res = C.c_double(0)
+    lib().pdesolver_(_pd(u), _pd(b), _pi(bc), _pd(h), _pi(n), _i(ncycl), _d(eps), _d(omega),
+                     C.byref(k), C.byref(ktot), C.byref(res), _i(ng), _i(0), _i(1))
+    check(lib().lepic_gpu_last_error(), "pdesolver")
+    phi[...] = u[1:]
+    return k.value, ktot.value, res.value
+
+
+def calc_efield(st, phi, Ei=None):
+    """Src/Efield.f90:1 -- returns Ei (n3+3, n2+3, n1+3, 3); nodes the
+    routine does not write keep the values of the Ei passed in."""
+    n = _lib.np_i(st.n)
+    if Ei is None:
+        Ei = np.zeros(tuple(st.geom.bcnd.shape) + (3,))
+    E = np.ascontiguousarray(Ei, dtype=np.float64)
+    f = np.ascontiguousarray(phi, dtype=np.float64)
+    bc = _lib.np_i(st.geom.bcnd)
+    h = np.ascontiguousarray(st.h, dtype=np.float64)
+    lib().calc_efield_(_pi(n), _pd(h), _pd(f), _pd(E), _pi(bc))
+    check(lib().lepic_gpu_last_error(), "calc_efield")
+    return E
+
+
+def _bi_uniform(st):
+    Bi = np.zeros((4, 4, 4, 4))          # Bi(4, 0:3, 0:3, 0:3) with n_B = 1
+    Bi[1, 1, 1, 0:3] = st.Bconst
+    return Bi
+
+
+def part_mover(st, Ei, vxp, np_tot, flag_dead, p_mac, P_loss, ptype, ngrid=None):
+    """Src/part_expmover.f90:1 -- in place on vxp / np_tot / flag_dead /
+    p_mac (ntype, 2, 0:ngrid) C-order (ngrid+1, 2, ntype) / P_loss (ntype, 4)."""
+    ngrid = st.geom.ngrid if ngrid is None else ngrid
+    n = _lib.np_i(st.n)
+    h = np.ascontiguousarray(st.h, dtype=np.float64)
+    E = np.ascontiguousarray(Ei, dtype=np.float64)
+    Bi = _bi_uniform(st)
+    bc = _lib.np_i(st.geom.bcnd)
+    nmax = vxp.shape[1]
+    assert vxp.flags["C_CONTIGUOUS"] and np_tot.dtype == np.int32 and flag_dead.dtype == np.int8
+    dummy_i = np.zeros(16, dtype=np.int32)
+    dummy_d = np.zeros(16)
+    nB = np.array([1, 1, 1], dtype=np.int32)
+    lib().part_mover_(_pi(n), _pd(h), _pd(E), _pd(Bi), _pd(p_mac), _pd(P_loss), _pd(vxp), _pi(bc),
+                      _i(nmax), _i(st.ntype), _i(ngrid), flag_dead.ctypes.data_as(_lib.P_i8), _i(1),
+                      _pi(np_tot), _i(1), _i(ptype), _pi(dummy_i), _pi(dummy_i), _pd(dummy_d),
+                      _pd(dummy_d), _pd(dummy_d), _pd(dummy_d), _pi(dummy_i), _pi(dummy_i), _pi(nB),
+                      _pd(h))
+    check(lib().lepic_gpu_last_error(), "part_mover")
+
+
+def charge_deposition(st, vxp, np_tot, np_grids, ptype):
+    """Src/part_expmover.f90:570 -- accumulates into np_grids[ptype-1]."""
+    n = _lib.np_i(st.n)
+    h = np.ascontiguousarray(st.h, dtype=np.float64)
+    kq = np.ascontiguousarray(st.kq, dtype=np.float64)
+    assert np_grids.flags["C_CONTIGUOUS"]
+    s = np.zeros(1)
+    nh = np.zeros(1, dtype=np.int32)
+    lib().charge_deposition_(_pi(n), _pd(h), _pd(vxp), _i(vxp.shape[1]), _i(st.ntype), _pd(kq),
+                             _pd(np_grids), _i(1), _pi(np_tot), _pd(s), _pi(nh), _i(1), _i(ptype))
+    check(lib().lepic_gpu_last_error(), "charge_deposition")
+
+
+def pl_max_of(n):
+    """Src/main.f90:227."""
+    return n[0] + n[0] * (n[1] + n[1] * n[2]) + 1
+
+
+def part_sorting(st, vxp, np_tot, ptype):
+    """Src/sorting.f90:97 -- sorts species ptype in place, returns Plist
+    (0:pl_max) of that species."""
+    n = _lib.np_i(st.n)
+    h = np.ascontiguousarray(st.h, dtype=np.float64)
+    pl_max = pl_max_of(st.n)
+    Plist = np.zeros((st.ntype, pl_max + 1), dtype=np.int32)
+    dummy = np.zeros(1)
+    lib().part_sorting_(_pd(vxp), _pd(dummy), _i(vxp.shape[1]), _i(st.ntype), _pi(n), _pd(h),
+                        _pi(Plist), _i(pl_max), _i(1), _pi(np_tot), _i(ptype))
+    check(lib().lepic_gpu_last_error(), "part_sorting")
+    return Plist[ptype - 1].copy()
+
+
+def collisions(st, it, vxp, np_tot, flag_dead, iseed, np_red=None, ncol_mx=65, npt_mx=1300,
+               n_rg=0, cnt_col=None):
+    """Src/collisions.f90:1 -- in place on vxp / np_tot / flag_dead.  Returns
+    the per-species nu_max written to COMMON /part_info_dp_3/."""
+    T = st.tables
+    ncol = T.sig.shape[0]
+    npt = T.sig_Er.shape[0]
+    set_commons(st, ncol=ncol, npt=npt, p_ncol=T.p_ncol)
+    cm = commons()
+    cm["part_info_int"].n_rg = n_rg
+    n = _lib.np_i(st.n)
+    h = np.ascontiguousarray(st.h, dtype=np.float64)
+    sig = np.zeros((ncol_mx, npt_mx))
+    sig[:ncol, :npt] = T.sig
+    sig_Er = np.zeros(npt_mx)
+    sig_Er[:npt] = T.sig_Er
+    sig_list = np.zeros((ncol_mx, 10), dtype=np.int32)
+    sig_list[:ncol, :] = T.sig_list.T
+    sig_Eex = np.zeros((2, ncol_mx))
+    sig_Eex[0, :ncol] = T.Eth
+    sigv = np.zeros((ncol_mx, 10))
+    sigv[:ncol, :] = T.sigv_mx.T
+    col_info = np.zeros((10, ncol_mx), dtype=np.int32)
+    col_info[:, :ncol] = T.col_info.T
+    if cnt_col is None:
+        cnt_col = np.zeros((max(n_rg, 1), 1, ncol_mx))
+    if np_red is None:
+        np_red = np.zeros((st.ntype,) + tuple(st.geom.bcnd.shape))
+    zi = np.zeros(16, dtype=np.int32)
+    zd = np.zeros(16)
+    pl = np.zeros(1, dtype=np.int32)
+    lib().collisions_(_i(it), _pd(vxp), _pi(n), _pd(h), _i(st.ntype), _i(vxp.shape[1]), _pd(sig),
+                      _pd(sig_Er), _pi(sig_list), _pd(sig_Eex), _i(ncol_mx), _i(npt_mx), _pd(cnt_col),
+                      _pd(zd), _pi(zi), _pi(zi), _pi(pl), _i(0), _pd(sigv), _pi(col_info), _pd(np_red),
+                      flag_dead.ctypes.data_as(_lib.P_i8), _pi(zi), _i(1), _pi(np_tot), _pi(iseed),
+                      _i(1), _i(0), _pd(zd), _pd(zd), _pd(zd), _i(0))
+    check(lib().lepic_gpu_last_error(), "collisions")
+    d3 = cm["part_info_dp_3"]
+    return np.array([d3.nu_max[i] for i in range(st.ntype)])

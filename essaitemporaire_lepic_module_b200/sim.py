@@ -1,0 +1,239 @@
+"""Device-resident PIC-MCC time stepping on one B200 (FP64 form).
+
+``Simulation`` keeps every array of the hot path in HBM (torch tensors used
+as plain device buffers) and advances the legacy timestep of
+Src/main.f90:853-1277 through the C ABI of liblepic_gpu.so:
+
+    calc_rho -> pdesolver -> calc_Efield -> part_sorting (every nsort)
+    -> collisions (every ns_coll, it > 1) -> part_mover -> charge_deposition
+
+Layout in HBM (reference index bases, column-major like the Fortran arrays):
+    bcnd, kq, phi          (n3+3, n2+3, n1+3) int32 / float64
+    Ei                     (n3+3, n2+3, n1+3, 3) float64, component fastest
+    np                     (ntype, n3+3, n2+3, n1+3) float64
+    rhs                    (n3+2, n2+2, n1+2) float64
+    particles per species  SoA (6, cap) float64 = x, y, z, vx, vy, vz
+                           + second buffer (sort target), int32 keys,
+                           int8 dead flags, device int32 count
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import LepicGrid, LepicSpeciesF64, LepicTables, check, lib, phys_struct
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+class Species:
+    """One species' FP64 particle store on the device."""
+
+    def __init__(self, cap, device):
+        self.cap = int(cap)
+        self.p = torch.zeros((6, self.cap), dtype=torch.float64, device=device)
+        self.p_alt = torch.zeros((6, self.cap), dtype=torch.float64, device=device)
+        self.count = torch.zeros(1, dtype=torch.int32, device=device)
+        self.key = torch.zeros(self.cap, dtype=torch.int32, device=device)
+        self.flag_dead = torch.zeros(self.cap, dtype=torch.int8, device=device)
+        self.s = LepicSpeciesF64()
+        self._sync_struct()
+
+    def _sync_struct(self):
+        s = self.s
+        s.p, s.p_alt = self.p.data_ptr(), self.p_alt.data_ptr()
+        s.count, s.key = self.count.data_ptr(), self.key.data_ptr()
+        s.flag_dead, s.cap = self.flag_dead.data_ptr(), self.cap
+
+    def after_call(self):
+        """The sort swaps the two buffers inside the struct; follow it."""
+        if self.s.p != self.p.data_ptr():
+            self.p, self.p_alt = self.p_alt, self.p
+        self._sync_struct()
+
+    def n(self):
+        return int(self.count.item())
+
+    def to_vxp(self):
+        """Host copy in the reference layout vxp(6, 1:np) -> (np, 6)."""
+        n = self.n()
+        return self.p[:, :n].t().contiguous().cpu().numpy()
+
+
+class Simulation:
+    def __init__(self, st, cap=None, device="cuda", seed=123456, nsort=None, ns_coll=None):
+        self.st = st
+        self.dev = torch.device(device)
+        self.stream = torch.cuda.current_stream(self.dev)
+        self.nsort = st.wl.nsort if nsort is None else nsort
+        self.ns_coll = st.wl.ns_coll if ns_coll is None else ns_coll
+        self.seed = int(seed)
+        self.P = phys_struct(st)
+        g = st.geom
+        T = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=self.dev)
+        self.bcnd = T(g.bcnd, torch.int32)
+        self.kq = T(st.kq, torch.float64)
+        self.phi = T(g.phi, torch.float64)
+        n1, n2, n3 = st.n
+        self.cw = torch.zeros((n3 + 2) * (n2 + 2) * (n1 + 2), dtype=torch.uint8, device=self.dev)
+        self.Ei = torch.zeros(tuple(g.bcnd.shape) + (3,), dtype=torch.float64, device=self.dev)
+        self.np = torch.zeros((st.ntype,) + tuple(g.bcnd.shape), dtype=torch.float64, device=self.dev)
+        self.rhs = torch.zeros((n3 + 2, n2 + 2, n1 + 2), dtype=torch.float64, device=self.dev)
+        self.grid = LepicGrid()
+        for a in range(3):
+            self.grid.n[a] = st.n[a]
+            self.grid.h[a] = float(st.h[a])
+        self.grid.bcnd = self.bcnd.data_ptr()
+        self.grid.kq = self.kq.data_ptr()
+        self.grid.cell_wall = self.cw.data_ptr()
+        nn = (C.c_int * 3)(*st.n)
+        check(lib().lepic_dev_cell_wall(nn, C.c_void_p(self.bcnd.data_ptr()),
+                                        C.c_void_p(self.cw.data_ptr()), self._s()), "cell_wall")
+        if cap is None:
+            cap = int(st.n_particles() * 1.25) + 1024
+        self.sp = [Species(cap, self.dev) for _ in range(st.ntype)]
+        self.sp_arr = (LepicSpeciesF64 * max(st.ntype, 1))()
+        self.it = 0
+        self.p_mac = np.zeros((st.geom.ngrid + 1, 2, st.ntype))
+        self.P_loss = np.zeros((st.ntype, 4))
+        self.mg_last = None
+        self.counts = np.zeros(64, dtype=np.int64)
+        self.nu_max = np.zeros(10)
+        self._tables = None
+        if st.tables is not None:
+            self._setup_tables()
+
+    def _s(self):
+        return C.c_void_p(self.stream.cuda_stream)
+
+    def _setup_tables(self):
+        T = self.st.tables
+        ncol, npt = T.sig.shape
+        d = self.dev
+        self._tsig = torch.as_tensor(np.ascontiguousarray(T.sig), device=d)
+        self._tEr = torch.as_tensor(np.ascontiguousarray(T.sig_Er), device=d)
+        self._tEth = torch.as_tensor(np.ascontiguousarray(T.Eth), device=d)
+        self._ci_h = np.ascontiguousarray(T.col_info.T, dtype=np.int32)      # col_info(ncol,10)
+        self._tci = torch.as_tensor(self._ci_h, device=d)
+        self._sl_h = np.ascontiguousarray(T.sig_list.T, dtype=np.int32)      # sig_list(10,ncol)
+        self._pn_h = np.ascontiguousarray(T.p_ncol, dtype=np.int32)
+        self._sv_h = np.ascontiguousarray(T.sigv_mx.T, dtype=np.float64)     # sigv_mx(10,ncol)
+        t = LepicTables()
+        t.ncol, t.npt, t.npt_mx = ncol, npt, npt
+        t.sig_Er, t.sig, t.sig_Eth = self._tEr.data_ptr(), self._tsig.data_ptr(), self._tEth.data_ptr()
+        t.col_info = self._tci.data_ptr()
+        t.sig_list = self._sl_h.ctypes.data
+        t.p_ncol = self._pn_h.ctypes.data
+        t.sigv_mx = self._sv_h.ctypes.data
+        t.col_info_h = self._ci_h.ctypes.data
+        self._tables = t
+
+    # ----------------------------------------------------------- loading
+    def load_from_host(self, vxp, np_tot, np_grids=None):
+        """Initial state from host arrays in the reference layout
+        (vxp (ntype, nmax, 6), np_tot, np grids)."""
+        for p, s in enumerate(self.sp):
+            n = int(np_tot[p])
+            assert n <= s.cap
+            s.p[:, :n] = torch.as_tensor(np.ascontiguousarray(vxp[p, :n, :].T), device=self.dev)
+            s.count.fill_(n)
+        if np_grids is not None:
+            self.np.copy_(torch.as_tensor(np.ascontiguousarray(np_grids), device=self.dev))
+        else:
+            self.deposit()
+
+    def load_uniform(self, n_per_species=None, seed=None):
+        """GPU Philox loader + initial deposition."""
+        n = self.st.n_particles() if n_per_species is None else int(n_per_species)
+        arr = (LepicSpeciesF64 * len(self.sp))(*[s.s for s in self.sp])
+        check(lib().lepic_dev_load_uniform(C.byref(self.grid), arr, len(self.sp), C.c_longlong(n),
+                                           C.byref(self.P), C.c_ulonglong(seed or self.seed),
+                                           self._s()), "load_uniform")
+        self.deposit()
+
+    # ----------------------------------------------------------- kernels
+    def calc_rho(self):
+        check(lib().lepic_dev_calc_rho(C.byref(self.grid), _ptr(self.np), _ptr(self.rhs),
+                                       self.st.ntype, C.byref(self.P), self._s()), "calc_rho")
+
+    def pdesolver(self, eps=None, omega=None, ng=None, ncycl=None):
+        wl = self.st.wl
+        k = C.c_int(0)
+        ktot = C.c_double(0)
+        res = C.c_double(0)
+        check(lib().lepic_dev_pdesolver(C.byref(self.grid), _ptr(self.phi), _ptr(self.rhs),
+                                        wl.ncycl if ncycl is None else ncycl,
+                                        wl.eps if eps is None else eps,
+                                        wl.omega if omega is None else omega,
+                                        self.st.ng if ng is None else ng, C.byref(self.P),
+                                        C.byref(k), C.byref(ktot), C.byref(res), self._s()),
+              "pdesolver")
+        self.mg_last = (k.value, ktot.value, res.value)
+        return self.mg_last
+
+    def efield(self):
+        check(lib().lepic_dev_calc_efield(C.byref(self.grid), _ptr(self.phi), _ptr(self.Ei),
+                                          self._s()), "calc_efield")
+
+    def sort(self):
+        pl_max = self.st.n[0] + self.st.n[0] * (self.st.n[1] + self.st.n[1] * self.st.n[2]) + 1
+        if not hasattr(self, "_plist") or self._plist.numel() < pl_max + 1:
+            self._plist = torch.zeros(pl_max + 1, dtype=torch.int32, device=self.dev)
+        for s in self.sp:
+            check(lib().lepic_dev_part_sorting(C.byref(self.grid), C.byref(s.s), _ptr(self._plist),
+                                               pl_max, self._s()), "part_sorting")
+            s.after_call()
+
+    def collisions(self):
+        if self._tables is None:
+            return
+        arr = (LepicSpeciesF64 * len(self.sp))(*[s.s for s in self.sp])
+        nu = (C.c_double * 10)()
+        cnt = (C.c_longlong * 64)()
+        check(lib().lepic_dev_collisions(C.byref(self.grid), arr, len(self.sp), C.byref(self._tables),
+                                         C.byref(self.P), C.c_ulonglong(self.seed),
+                                         C.c_ulonglong(self.it), nu, cnt, self._s()), "collisions")
+        self.counts[:64] += np.array(cnt[:], dtype=np.int64)
+        self.nu_max[:] = nu[:]
+
+    def move(self):
+        pm = np.zeros((self.st.geom.ngrid + 1, 2, self.st.ntype))
+        pl = np.zeros((self.st.ntype, 4))
+        for p, s in enumerate(self.sp):
+            if self.st.charge[p] == 0.0:
+                continue
+            check(lib().lepic_dev_part_mover(C.byref(self.grid), _ptr(self.Ei), C.byref(s.s), p + 1,
+                                             self.st.ntype, self.st.geom.ngrid, C.byref(self.P),
+                                             pm.ctypes.data_as(_lib.P_dbl),
+                                             pl.ctypes.data_as(_lib.P_dbl), self._s()), "part_mover")
+        self.p_mac += pm
+        self.P_loss += pl
+
+    def deposit(self):
+        self.np.zero_()
+        for p, s in enumerate(self.sp):
+            check(lib().lepic_dev_charge_deposition(C.byref(self.grid), C.byref(s.s), p + 1,
+                                                    C.byref(self.P), C.c_void_p(self.np[p].data_ptr()),
+                                                    self._s()), "charge_deposition")
+
+    def step(self):
+        """One timestep in the reference's order (Src/main.f90:853-1277)."""
+        self.it += 1
+        it = self.it
+        self.calc_rho()
+        self.pdesolver()
+        self.efield()
+        if self.nsort and it % self.nsort == 1 % self.nsort:
+            self.sort()
+        if self._tables is not None and it > 1 and it % self.ns_coll == 1 % self.ns_coll:
+            self.collisions()
+        self.move()
+        self.deposit()
+
+    def counts_host(self):
+        return np.array([s.n() for s in self.sp])

@@ -1,0 +1,285 @@
+/*
+ * lepic_gpu.h -- C ABI of the B200 (sm_100a) PIC-MCC hot path.
+ *
+ * Two layers, both plain C (pointers and sizes only, no CUDA or torch types):
+ *
+ * 1. Drop-in replacements for the legacy Fortran routines of the reference.
+ *    The names carry the trailing underscore of gfortran/ifx external
+ *    symbols and every argument is a pointer, so a Fortran build that links
+ *    this library in place of the original objects calls them unchanged
+ *    (the routines are external subroutines with implicit interfaces).
+ *    Arrays are the Fortran host arrays (column-major, reference index
+ *    bases); each call copies its inputs to the GPU, runs the kernels and
+ *    copies its outputs back.  Physics constants are read from the Fortran
+ *    COMMON blocks declared below, exactly as the Fortran routines read them.
+ *    Contract: OMP_NUM_THREADS=1 (nproc = 1) and one MPI rank.
+ *
+ * 2. A device API (lepic_dev_*) on device pointers and a CUDA stream handle
+ *    (passed as void*), used by the host step loop and the PyTorch binding.
+ *
+ * Errors: every entry point returns / records an int status (0 = OK, codes
+ * below).  The drop-ins cannot return a value to Fortran, so they record it;
+ * lepic_gpu_last_error() reads and clears it.  GPU kernels never trap: they
+ * set a device error word that the host turns into these codes.
+ */
+#ifndef LEPIC_GPU_H
+#define LEPIC_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LEPIC_NPART 10
+#define LEPIC_NM_RG 5
+
+/* status codes (shared with the CPU oracle) */
+#define LEPIC_OK 0
+#define LEPIC_ERR_CAPACITY 1      /* particle array full (reference: nmax)        */
+#define LEPIC_ERR_DIVERGED 2      /* Poisson residual grew > 10x (pdesolver)      */
+#define LEPIC_ERR_PMAX 3          /* null-collision probability > 1               */
+#define LEPIC_ERR_EKR_TABLE 4     /* collision energy above the sigma table       */
+#define LEPIC_ERR_NEG_ENERGY 5    /* negative CM energy after threshold           */
+#define LEPIC_ERR_UNSUPPORTED 6   /* option outside the GPU path (B maps, ...)    */
+#define LEPIC_ERR_FEW_COLL 7      /* collision time step too small for electrons  */
+#define LEPIC_ERR_CUDA 20         /* CUDA runtime error                          */
+#define LEPIC_ERR_ARG 21          /* invalid argument / size                     */
+#define LEPIC_ERR_CELL 22         /* particle outside the grid (device check)    */
+#define LEPIC_ERR_NOT_CONVERGED 23 /* iteration cap reached                      */
+
+/* ------------------------------------------------------------------------ */
+/* Fortran COMMON blocks of Src/particle_info.h:53-70 and Src/constants.h,   */
+/* member for member.  The library defines them as weak symbols; when linked */
+/* into the Fortran program its COMMON storage takes precedence.             */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int np_cell, ncol, sig_npt_mx, flag_pdf, n_cell, nbak, flag_restart, ixl_pow, ixr_pow, flag_B,
+      ns_heat, ns_coll, p_ncol[LEPIC_NPART], nscol, p_nscol[LEPIC_NPART], n_rg, flag_pbc, n_holes,
+      flag_grd, ind_g, nB, cnt_seg, tag_neg, cnt_neg, tag_neu, flag_nmn, num_grd, ptype_pdf, ns_flx,
+      nhy, nhz, ixl_rg[LEPIC_NM_RG], ns_inj, ixr_rg[LEPIC_NM_RG], iyl_rg, iyr_rg, izl_rg, izr_rg,
+      flag_heat, flag_inj, opt_inj, flag_B_pos, ixg, ix_PE, omp_rank_max, mpi_rank_max, flag_die,
+      flag_thr, ix_pl, iz_pl, ix_thr, flag_convP, ig_die[5], flag_pbcz, tag_beam, every, cnt_plt,
+      flag_bak, igrid_sec, dir_sec, n_cath, flag_circxh, flag_ahp, flag_gridB, plt_src, flag_RFpot;
+} lepic_part_info_int_t;
+
+typedef struct {
+  double charge[LEPIC_NPART], mass[LEPIC_NPART], Ti[LEPIC_NPART], vt0[LEPIC_NPART], k_eps0,
+      B_scale[5], B0[5], dL[5], x0[5], y0[5], z0[5], jne, RNeta, THm, x_thr, y_thr, tseq,
+      tseq_init, tseq_final, gam_sec, zg_sec[2];
+} lepic_part_info_dp_1_t;
+
+typedef struct {
+  double Pabs, n0, ngas, Nm[LEPIC_NPART], dt, xmax, ymax, zmax, x_load, nu_h, Lgy, Lgz, Sg, Lhy,
+      Lhz, xg1, Bmax, nudt, R_ahp;
+} lepic_part_info_dp_2_t;
+
+typedef struct {
+  double np_mx[LEPIC_NPART], nu_max[LEPIC_NPART], nu_uplim[LEPIC_NPART];
+} lepic_part_info_dp_3_t;
+
+typedef struct {
+  double qe, eps0, c, pi, amu;
+} lepic_constants_t;
+
+extern lepic_part_info_int_t part_info_int_;
+extern lepic_part_info_dp_1_t part_info_dp_1_;
+extern lepic_part_info_dp_2_t part_info_dp_2_;
+extern lepic_part_info_dp_3_t part_info_dp_3_;
+extern lepic_constants_t constants_;
+
+/* ------------------------------------------------------------------------ */
+/* Drop-in routines (layer 1).  Each cites the reference routine it replaces. */
+/* ------------------------------------------------------------------------ */
+
+/* Src/calc_rho.f90:1 -- rhs_dom = -sum_species charge*np (+ periodic
+ * stitching of np).  np(0:n1+2,0:n2+2,0:n3+2,ntype,nproc),
+ * rhs_dom(0:n1+1,0:n2+1,0:n3+1), bcnd(0:n1+2,0:n2+2,0:n3+2). */
+void calc_rho_(const int *n, double *np, double *rhs_dom, const int *bcnd, const int *ntype,
+               const int *nproc, const int *nproc_mpi, const int *mpi_rank);
+
+/* Src/calc_rho.f90:116 -- np_red = sum over threads, np_mx = max over plasma
+ * nodes (written to COMMON /part_info_dp_3/ np_mx). */
+void dens_red_(const int *n, const double *np, double *np_red, const int *bcnd, const int *ntype,
+               const int *nproc, const int *nproc_mpi);
+
+/* Src/pdesolver.f90:1 -- multigrid V-cycles with red-black SOR smoothing
+ * until res/alpha < eps.  u(0:n1+2,0:n2+2,-1:n3+2) (warm start, Dirichlet
+ * values on walls), b(0:n1+1,0:n2+1,0:n3+1) = -rho. */
+void pdesolver_(double *u, const double *b, const int *bcnd, const double *h, const int *n,
+                const int *ncycl, const double *eps, const double *omega, int *k, double *ktot,
+                double *res, const int *ng, const int *rank, const int *nproc);
+
+/* Src/Efield.f90:1 -- E = -grad(phi) with wall extrapolation.
+ * phi(0:n1+2,0:n2+2,0:n3+2), Ei(3,0:n1+2,0:n2+2,0:n3+2). */
+void calc_efield_(const int *n, const double *h, const double *phi, double *Ei, const int *bcnd);
+
+/* Src/part_expmover.f90:1 as called at Src/main.f90:1250-1252 (26
+ * arguments) -- trilinear gather, Boris (uniform B, n_B(1) = 1) or leapfrog,
+ * position update, loss test and in-order compaction of species ptype. */
+void part_mover_(const int *n, const double *h, const double *Ei, const double *Bi, double *p_mac,
+                 double *P_loss, double *vxp, const int *bcnd, const int *nmax, const int *ntype,
+                 const int *ngrid, signed char *flag_dead, const int *nproc, int *np_tot,
+                 const int *iproc, const int *ptype, int *flag_cex, int *cnt_cex, double *cnt_dead,
+                 double *beam_div, double *sum_q_xz, double *sum_q_yz, const int *dtype,
+                 int *iseed, const int *n_B, const double *h_B);
+
+/* Src/part_expmover.f90:570 -- CIC deposition with kq into np(..,ptype,iproc). */
+void charge_deposition_(const int *n, const double *h, const double *vxp, const int *nmax,
+                        const int *ntype, const double *kq, double *np, const int *nproc,
+                        const int *np_tot, double *sum_dEk, int *Nh, const int *iproc,
+                        const int *ptype);
+
+/* Src/sorting.f90:97 -- counting sort of species ptype by cell.  Plist_thd
+ * (0:pl_max,ntype,nproc) receives the inclusive end offset of every cell.
+ * Within one cell the order is unspecified (the reference's OpenMP atomic
+ * capture scatter is not stable either). */
+void part_sorting_(double *vxp, double *sorting, const int *nmax, const int *ntype, const int *n,
+                   const double *h, int *Plist_thd, const int *pl_max, const int *nproc,
+                   const int *np_tot, const int *ptype);
+
+/* Src/collisions.f90:1 -- null-collision Monte Carlo against neutral
+ * targets.  Same 29 arguments.  The GPU draws from a Philox4x32-10 counter
+ * stream keyed by iseed(1) instead of the serial ran2 stream, so results
+ * agree with the reference statistically (collision counts per process,
+ * moments), not bit for bit.  cnt_col(ncol_mx,nproc,nm_rg) region counters
+ * are accumulated like the reference; the sour_xy, sour_xz and ss2D planes are left
+ * untouched (flag_diag = 1 is unsupported). */
+void collisions_(const int *it, double *vxp, const int *n, const double *h, const int *ntype,
+                 const int *nmax, const double *sig, const double *sig_Er, const int *sig_list,
+                 const double *sig_Eex, const int *ncol_mx, const int *npt_mx, double *cnt_col,
+                 double *P_loss, int *sour_xy, int *sour_xz, const int *Plist, const int *pl_max,
+                 const double *sigv_mx, const int *col_info, const double *np_red,
+                 signed char *flag_dead, int *flag_cex, const int *nproc, int *np_tot, int *iseed,
+                 const int *nproc_mpi, const int *mpi_rank, double *ss2D_xy, double *ss2D_xz,
+                 double *ss2D_yz, const int *flag_diag);
+
+/* Status of the last drop-in call on this thread, then cleared. */
+int lepic_gpu_last_error(void);
+/* Human-readable text for a status code. */
+const char *lepic_gpu_strerror(int code);
+
+/* ------------------------------------------------------------------------ */
+/* Device API (layer 2): device pointers, stream as void*.  No counterpart   */
+/* in the reference (which has no device boundary); each function names the  */
+/* reference routine whose semantics it implements.                          */
+/* ------------------------------------------------------------------------ */
+
+/* Physics constants for the device API: the subset of the COMMON blocks the
+ * hot path reads, one struct. */
+typedef struct {
+  int ntype, n_neu;
+  double charge[LEPIC_NPART], mass[LEPIC_NPART], vt0[LEPIC_NPART], Nm[LEPIC_NPART],
+      np_mx[LEPIC_NPART], nu_uplim[LEPIC_NPART];
+  double dt, xmax, ymax, zmax, x_load;
+  double qe, eps0, pi;
+  int flag_B, flag_B_pos, flag_pbc, flag_nmn;
+  int ns_coll, n_cell, np_cell;
+  double Bconst[3];
+} lepic_phys_t;
+
+/* Cross-section tables after Src/read_reactions.f90:ordering, device copies. */
+typedef struct {
+  int ncol, npt, npt_mx;
+  const double *sig_Er;   /* [npt] device                                    */
+  const double *sig;      /* sig(npt_mx, ncol) device, column-major          */
+  const double *sig_Eth;  /* [ncol] device                                   */
+  const int *col_info;    /* col_info(ncol, 10) device, column-major         */
+  const int *sig_list;    /* host: sig_list(10, ncol)                        */
+  const int *p_ncol;      /* host: [10]                                      */
+  const double *sigv_mx;  /* host: sigv_mx(10, ncol)                         */
+  const int *col_info_h;  /* host copy of col_info                           */
+} lepic_tables_t;
+
+/* Grid geometry on the device. */
+typedef struct {
+  int n[3];
+  double h[3];
+  const int *bcnd;        /* (n1+3)(n2+3)(n3+3) device                        */
+  const double *kq;       /* same shape, device                               */
+  const unsigned char *cell_wall; /* (n1+2)(n2+2)(n3+2): 1 if all 8 nodes of
+                                     cell (ix,iy,iz), ix in 0..n1+1, are walls */
+} lepic_grid_t;
+
+/* One species' FP64 particles on the device: SoA, component c of particle i
+ * at p[c*cap + i], c = x,y,z,vx,vy,vz.  count: device int. */
+typedef struct {
+  double *p;
+  double *p_alt;          /* second buffer of the same size (sort target)    */
+  int *count;             /* device int                                       */
+  int *key;               /* device int[cap] scratch                          */
+  signed char *flag_dead; /* device int8[cap] or NULL                         */
+  int cap;
+} lepic_species_f64_t;
+
+/* Src/calc_rho.f90:1 on device grids (nproc = 1). */
+int lepic_dev_calc_rho(const lepic_grid_t *g, double *np, double *rhs, int ntype,
+                       const lepic_phys_t *P, void *stream);
+
+/* Src/Efield.f90:1 on device grids. */
+int lepic_dev_calc_efield(const lepic_grid_t *g, const double *phi, double *Ei, void *stream);
+
+/* Src/pdesolver.f90:1 as one persistent cooperative kernel (all V-cycles,
+ * all levels, no host round trips).  u: (n+3)^3 device potential (z from 0),
+ * b: (n+2)^3.  Blocks until done; k/ktot/res returned like the reference. */
+int lepic_dev_pdesolver(const lepic_grid_t *g, double *u, const double *b, int ncycl, double eps,
+                        double omega, int ng, const lepic_phys_t *P, int *k, double *ktot,
+                        double *res, void *stream);
+
+/* Src/part_expmover.f90:1-482 for one species: push + loss + in-order
+ * compaction.  Ei device (3,(n+3)^3).  p_mac: host (ntype,2,0:ngrid),
+ * P_loss: host (4,ntype), accumulated. */
+int lepic_dev_part_mover(const lepic_grid_t *g, const double *Ei, lepic_species_f64_t *s,
+                         int ptype, int ntype, int ngrid, const lepic_phys_t *P, double *p_mac,
+                         double *P_loss, void *stream);
+
+/* Src/part_expmover.f90:570-686 for one species, accumulating into np
+ * (device grid of that species). */
+int lepic_dev_charge_deposition(const lepic_grid_t *g, const lepic_species_f64_t *s, int ptype,
+                                const lepic_phys_t *P, double *np, void *stream);
+
+/* Src/sorting.f90:97-258 for one species: counting sort by cell.  Plist:
+ * device int[pl_max+1] receiving inclusive end offsets. */
+int lepic_dev_part_sorting(const lepic_grid_t *g, lepic_species_f64_t *s, int *Plist, int pl_max,
+                           void *stream);
+
+/* Src/collisions.f90:1-212 + collision_OMP for neutral targets, Philox
+ * per-particle null collisions.  sp[ntype]; counts[ncol] host, accumulated
+ * (collisions per reaction); nu_max[ntype] host output. */
+int lepic_dev_collisions(const lepic_grid_t *g, lepic_species_f64_t *sp, int ntype,
+                         const lepic_tables_t *T, const lepic_phys_t *P, unsigned long long seed,
+                         unsigned long long call_index, double *nu_max, long long *counts,
+                         void *stream);
+
+/* GPU particle loader (counterpart of Src/load_part.f90:91-194 for the
+ * large workloads): n_per_species samples, positions uniform in
+ * [0,x_load) x [0,ymax) x [0,zmax) outside all-wall cells, shared by all
+ * species of a sample (co-located pairs), Maxwellian velocities with vt0.
+ * Draws come from a Philox4x32-10 stream keyed by seed (not ran2). */
+int lepic_dev_load_uniform(const lepic_grid_t *g, lepic_species_f64_t *sp, int ntype,
+                           long long n_per_species, const lepic_phys_t *P, unsigned long long seed,
+                           void *stream);
+
+/* Per-cell all-wall mask of the loss test (Src/part_expmover.f90:258-262):
+ * cell_wall((n1+2)(n2+2)(n3+2)) from bcnd, both device. */
+int lepic_dev_cell_wall(const int *n, const int *bcnd, unsigned char *cell_wall, void *stream);
+
+/* Src/calc_rho.f90:116 (dens_red) on device grids; np_mx host [ntype]. */
+int lepic_dev_dens_red(const lepic_grid_t *g, const double *np, double *np_red, int ntype,
+                       double *np_mx, void *stream);
+
+/* Per-kernel device timers (CUDA events around each named launch).  No
+ * counterpart in the reference (its MSTIMER buckets, Src/utils.f90:503-527,
+ * time host phases).  read: names '\n'-separated into buf, total ms and
+ * launch count per name; returns the number of names. */
+void lepic_timing_enable(int on);
+void lepic_timing_reset(void);
+int lepic_timing_read(char *buf, int buflen, double *ms, long long *launches, int max_names);
+
+/* Number of SMs, device name; 0 on success. */
+int lepic_dev_info(int *sm_count, char *name, int name_len);
+/* Library build identification (nvcc version, arch). */
+const char *lepic_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

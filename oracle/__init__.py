@@ -1,0 +1,298 @@
+"""ctypes wrapper of the CPU FP64 oracle -- TEST INFRASTRUCTURE ONLY.
+
+The oracle is the parity checker for the GPU path: a strict-IEEE C++
+restatement of the reference's legacy routines (see lepic_oracle.cpp).  Only
+tests/, the smoke check and bench.py's CPU-baseline leg use it; the product
+package never imports it.
+
+Parity pins: the geometry mask and the E-field stencil are pinned against
+the reference's committed output planes (tests/golden/).  The other routines
+are "parity unpinned" against the reference's own binary (no Fortran
+compiler here) and are pinned by analytic known-answer tests.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liblepic_oracle.so")
+
+P_int = C.POINTER(C.c_int)
+P_dbl = C.POINTER(C.c_double)
+P_i8 = C.POINTER(C.c_int8)
+P_ll = C.POINTER(C.c_longlong)
+
+
+class OTables(C.Structure):
+    _fields_ = [("ncol", C.c_int), ("npt", C.c_int), ("npt_mx", C.c_int),
+                ("sig_Er", P_dbl), ("sig", P_dbl), ("sig_Eth", P_dbl), ("col_info", P_int),
+                ("sig_list", P_int), ("p_ncol", P_int), ("sigv_mx", P_dbl)]
+
+
+def build():
+    """Compile the oracle with its Makefile (strict IEEE)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+_L = None
+
+
+def lib():
+    global _L
+    if _L is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        L.oracle_ran2.restype = C.c_double
+        L.oracle_ran2.argtypes = [P_int]
+        L.oracle_set_threads.restype = C.c_int
+        L.oracle_set_threads.argtypes = [C.c_int]
+        _L = L
+    return _L
+
+
+def _pd(a):
+    return a.ctypes.data_as(P_dbl)
+
+
+def _pi(a):
+    return a.ctypes.data_as(P_int)
+
+
+def ophys(st):
+    """OPhys has the layout of lepic_phys_t; reuse the package's struct."""
+    from essaitemporaire_lepic_module_b200._lib import phys_struct
+    return phys_struct(st)
+
+
+def set_threads(n):
+    return lib().oracle_set_threads(int(n))
+
+
+def ran2(seed):
+    s = C.c_int(seed)
+    r = lib().oracle_ran2(C.byref(s))
+    return r, s.value
+
+
+class State:
+    """Particle state in the reference layout: vxp (ntype, nmax, 6)."""
+
+    def __init__(self, st, nmax):
+        self.vxp = np.zeros((st.ntype, nmax, 6))
+        self.np_tot = np.zeros(st.ntype, dtype=np.int32)
+        self.flag_dead = np.zeros((st.ntype, nmax), dtype=np.int8)
+        self.np = np.zeros((st.ntype,) + tuple(st.geom.bcnd.shape))
+        self.iseed = np.array([123456], dtype=np.int32)
+
+    def copy(self):
+        o = object.__new__(State)
+        o.vxp = self.vxp.copy()
+        o.np_tot = self.np_tot.copy()
+        o.flag_dead = self.flag_dead.copy()
+        o.np = self.np.copy()
+        o.iseed = self.iseed.copy()
+        return o
+
+
+def load_part(st, nmax, seed=123456):
+    """Src/load_part.f90 with one thread (seed 123456*iproc, iproc = 1)."""
+    S = State(st, nmax)
+    S.iseed[0] = seed
+    n = np.array(st.n, dtype=np.int32)
+    h = np.ascontiguousarray(st.h)
+    bc = np.ascontiguousarray(st.geom.bcnd, dtype=np.int32)
+    kq = np.ascontiguousarray(st.kq)
+    ni0 = np.ascontiguousarray(st.ni0[:st.ntype])
+    P = ophys(st)
+    rc = lib().oracle_load_part(_pi(n), _pd(h), _pi(bc), _pd(S.np), _pd(S.vxp), C.c_int(st.ntype),
+                                C.c_int(nmax), _pd(kq), _pd(ni0), _pi(S.np_tot), _pi(S.iseed),
+                                C.byref(P))
+    if rc:
+        raise RuntimeError(f"oracle load_part status {rc}")
+    return S
+
+
+def calc_rho(st, np_grids):
+    n = np.array(st.n, dtype=np.int32)
+    rhs = np.zeros((st.n[2] + 2, st.n[1] + 2, st.n[0] + 2))
+    bc = np.ascontiguousarray(st.geom.bcnd, dtype=np.int32)
+    P = ophys(st)
+    lib().oracle_calc_rho(_pi(n), _pd(np_grids), _pd(rhs), _pi(bc), C.c_int(st.ntype), C.byref(P))
+    return rhs
+
+
+def dens_red(st, np_grids):
+    n = np.array(st.n, dtype=np.int32)
+    red = np.zeros_like(np_grids)
+    mx = np.zeros(10)
+    bc = np.ascontiguousarray(st.geom.bcnd, dtype=np.int32)
+    lib().oracle_dens_red(_pi(n), _pd(np_grids), _pd(red), _pi(bc), C.c_int(st.ntype), _pd(mx))
+    return red, mx[:st.ntype]
+
+
+def pdesolver(st, phi, rhs, eps=None, omega=None, ng=None, ncycl=None):
+    wl = st.wl
+    eps = wl.eps if eps is None else eps
+    omega = wl.omega if omega is None else omega
+    ng = st.ng if ng is None else ng
+    ncycl = wl.ncycl if ncycl is None else ncycl
+    n = np.array(st.n, dtype=np.int32)
+    h = np.ascontiguousarray(st.h)
+    bc = np.ascontiguousarray(st.geom.bcnd, dtype=np.int32)
+    k = C.c_int(0)
+    ktot = C.c_double(0)
+    res = C.c_double(0)
+    P = ophys(st)
+    assert phi.flags["C_CONTIGUOUS"]
+    rc = lib().oracle_pdesolver(_pd(phi), _pd(np.ascontiguousarray(rhs)), _pi(bc), _pd(h), _pi(n),
+                                C.c_int(ncycl), C.c_double(eps), C.c_double(omega), C.byref(k),
+                                C.byref(ktot), C.byref(res), C.c_int(ng), C.byref(P))
+    if rc:
+        raise RuntimeError(f"oracle pdesolver status {rc}")
+    return k.value, ktot.value, res.value
+
+
+def calc_efield(st, phi, Ei=None):
+    n = np.array(st.n, dtype=np.int32)
+    h = np.ascontiguousarray(st.h)
+    bc = np.ascontiguousarray(st.geom.bcnd, dtype=np.int32)
+    if Ei is None:
+        Ei = np.zeros(tuple(st.geom.bcnd.shape) + (3,))
+    E = np.ascontiguousarray(Ei).copy()
+    lib().oracle_calc_efield(_pi(n), _pd(h), _pd(np.ascontiguousarray(phi)), _pd(E), _pi(bc))
+    return E
+
+
+def part_mover(st, Ei, S, p_mac, P_loss, ptype, ngrid=None):
+    ngrid = st.geom.ngrid if ngrid is None else ngrid
+    n = np.array(st.n, dtype=np.int32)
+    h = np.ascontiguousarray(st.h)
+    bc = np.ascontiguousarray(st.geom.bcnd, dtype=np.int32)
+    P = ophys(st)
+    rc = lib().oracle_part_mover(_pi(n), _pd(h), _pd(np.ascontiguousarray(Ei)), _pd(p_mac),
+                                 _pd(P_loss), _pd(S.vxp), _pi(bc), C.c_int(S.vxp.shape[1]),
+                                 C.c_int(st.ntype), C.c_int(ngrid), S.flag_dead.ctypes.data_as(P_i8),
+                                 _pi(S.np_tot), C.c_int(ptype), C.byref(P))
+    if rc:
+        raise RuntimeError(f"oracle part_mover status {rc}")
+
+
+def charge_deposition(st, S, ptype):
+    n = np.array(st.n, dtype=np.int32)
+    h = np.ascontiguousarray(st.h)
+    kq = np.ascontiguousarray(st.kq)
+    P = ophys(st)
+    lib().oracle_charge_deposition(_pi(n), _pd(h), _pd(S.vxp), C.c_int(S.vxp.shape[1]),
+                                   C.c_int(st.ntype), _pd(kq), _pd(S.np), _pi(S.np_tot),
+                                   C.c_int(ptype), C.byref(P))
+
+
+def part_sorting(st, S, ptype):
+    n = np.array(st.n, dtype=np.int32)
+    h = np.ascontiguousarray(st.h)
+    pl_max = st.n[0] + st.n[0] * (st.n[1] + st.n[1] * st.n[2]) + 1
+    Plist = np.zeros(pl_max + 1, dtype=np.int32)
+    lib().oracle_part_sorting(_pd(S.vxp), C.c_int(S.vxp.shape[1]), C.c_int(st.ntype), _pi(n),
+                              _pd(h), _pi(Plist), C.c_int(pl_max), _pi(S.np_tot), C.c_int(ptype))
+    return Plist
+
+
+def tables_struct(T, keep):
+    """OTables over the package's reactions.Tables (arrays kept alive in
+    `keep`)."""
+    ncol, npt = T.sig.shape
+    sig = np.ascontiguousarray(T.sig)                      # (ncol, npt) == sig(npt, ncol)
+    Er = np.ascontiguousarray(T.sig_Er)
+    Eth = np.ascontiguousarray(T.Eth)
+    ci = np.ascontiguousarray(T.col_info.T, dtype=np.int32)  # col_info(ncol,10)
+    sl = np.ascontiguousarray(T.sig_list.T, dtype=np.int32)  # sig_list(10,ncol)
+    pn = np.ascontiguousarray(T.p_ncol, dtype=np.int32)
+    sv = np.ascontiguousarray(T.sigv_mx.T)                   # sigv_mx(10,ncol)
+    keep.extend([sig, Er, Eth, ci, sl, pn, sv])
+    return OTables(ncol, npt, npt, _pd(Er), _pd(sig), _pd(Eth), _pi(ci), _pi(sl), _pi(pn), _pd(sv))
+
+
+def collisions(st, S):
+    """Src/collisions.f90 with one thread; returns (nu_max, counts, Nc)."""
+    keep = []
+    T = tables_struct(st.tables, keep)
+    n = np.array(st.n, dtype=np.int32)
+    h = np.ascontiguousarray(st.h)
+    P = ophys(st)
+    nu = np.zeros(10)
+    cnt = np.zeros(64, dtype=np.int64)
+    Nc = np.zeros(10, dtype=np.int32)
+    rc = lib().oracle_collisions(_pd(S.vxp), _pi(n), _pd(h), C.c_int(st.ntype),
+                                 C.c_int(S.vxp.shape[1]), C.byref(T), S.flag_dead.ctypes.data_as(P_i8),
+                                 _pi(S.np_tot), _pi(S.iseed), C.byref(P), _pd(nu),
+                                 cnt.ctypes.data_as(P_ll), _pi(Nc))
+    if rc:
+        raise RuntimeError(f"oracle collisions status {rc}")
+    return nu[:st.ntype], cnt[:T.ncol], Nc[:st.ntype]
+
+
+def ordering(chem, npt_mx=4000):
+    """Src/read_reactions.f90:ordering in C for a reactions.Chemistry."""
+    ncol = len(chem.tables)
+    mx = max(len(t[0]) for t in chem.tables) + 1
+    E = np.zeros((ncol, mx))
+    Sg = np.zeros((ncol, mx))
+    npts = np.zeros(ncol, dtype=np.int32)
+    for c, (e, s) in enumerate(chem.tables):
+        E[c, :len(e)] = e
+        Sg[c, :len(s)] = s
+        npts[c] = len(e)
+    Eth = np.ascontiguousarray(chem.Eth)
+    ci = np.ascontiguousarray(chem.col_info.T, dtype=np.int32)
+    mass = np.zeros(10)
+    for i, s in enumerate(chem.species):
+        mass[i] = s.mass
+    from essaitemporaire_lepic_module_b200.constants import QE
+    sig_Er = np.zeros(npt_mx)
+    sig = np.zeros((ncol, npt_mx))
+    npt_out = C.c_int(0)
+    sl = np.zeros((ncol, 10), dtype=np.int32)
+    pn = np.zeros(10, dtype=np.int32)
+    sv = np.zeros((ncol, 10))
+    rc = lib().oracle_ordering(C.c_int(ncol), _pi(npts), _pd(E), _pd(Sg), C.c_int(mx), _pd(Eth),
+                               _pi(ci), _pd(mass), C.c_int(chem.ntype), C.c_double(QE), _pd(sig_Er),
+                               _pd(sig), C.c_int(npt_mx), C.byref(npt_out), _pi(sl), _pi(pn), _pd(sv))
+    if rc:
+        raise RuntimeError(f"oracle ordering status {rc}")
+    k = npt_out.value
+    return sig_Er[:k], sig[:, :k], sv.T, sl.T, pn
+
+
+def step(st, S, phi, Ei, it, p_mac=None, P_loss=None, nsort=10, ns_coll=10, mg=None):
+    """One legacy timestep in the order of Src/main.f90:853-1277:
+    calc_rho -> pdesolver -> calc_Efield -> (sort) -> (collisions) ->
+    part_mover -> charge_deposition.  Returns (Ei, mg result, MCC result)."""
+    rhs = calc_rho(st, S.np)
+    mg_out = pdesolver(st, phi, rhs, **(mg or {}))
+    Ei = calc_efield(st, phi, Ei)
+    if nsort and it % nsort == 1 % nsort:
+        for p in range(1, st.ntype + 1):
+            if S.np_tot[p - 1] > 0:
+                part_sorting(st, S, p)
+    mcc = None
+    if st.tables is not None and it > 1 and it % ns_coll == 1 % ns_coll:
+        mcc = collisions(st, S)
+    ng1 = st.geom.ngrid + 1
+    if p_mac is None:
+        p_mac = np.zeros((ng1, 2, st.ntype))
+    if P_loss is None:
+        P_loss = np.zeros((st.ntype, 4))
+    for p in range(1, st.ntype + 1):
+        if st.charge[p - 1] != 0.0:
+            part_mover(st, Ei, S, p_mac, P_loss, p)
+    for p in range(1, st.ntype + 1):
+        S.np[p - 1] = 0.0
+        if S.np_tot[p - 1] > 0:
+            charge_deposition(st, S, p)
+    return Ei, mg_out, mcc

@@ -1,0 +1,1165 @@
+// CPU FP64 oracle for the LePIC 3D PIC-MCC hot path -- TEST INFRASTRUCTURE.
+//
+// A restatement of the legacy Fortran routines of the reference (Src/*.f90),
+// in their loop order and with their expression order, built with
+// -O2 -fno-fast-math -ffp-contract=off so that every FP64 operation rounds
+// exactly as written.  Each routine cites the reference lines it follows.
+// The OpenMP pragmas only cover loops whose result does not depend on the
+// iteration order (one colour of a red-black sweep, per-particle pushes);
+// with one thread every routine reproduces the serial Fortran order.
+//
+// Parity pins: geometry masks and the E-field stencil are pinned against the
+// reference's committed output planes; the rest is pinned by analytic
+// known-answer tests ("parity unpinned" against the reference's own code,
+// which cannot be compiled here: no Fortran compiler, no MPI).
+#include "lepic_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+struct Dims {
+  int n1, n2, n3;     // cells
+  long N1, N2, N3;    // node extents (n+3)
+  Dims(const int n[3]) : n1(n[0]), n2(n[1]), n3(n[2]), N1(n[0] + 3), N2(n[1] + 3), N3(n[2] + 3) {}
+  long g(int ix, int iy, int iz) const { return ix + N1 * (iy + N2 * (long)iz); }
+  long cnt() const { return N1 * N2 * N3; }
+  // rhs arrays b(0:n1+1,0:n2+1,0:n3+1)
+  long r(int ix, int iy, int iz) const { return ix + (N1 - 1) * (iy + (N2 - 1) * (long)iz); }
+  long rcnt() const { return (N1 - 1) * (N2 - 1) * (N3 - 1); }
+};
+
+// Stencil coefficients of Src/mg.h:9-15 for spacing h.
+struct Coef {
+  double aw, ae, an, as, at, ab, ac;
+  Coef(const double h[3], double eps0) {
+    aw = eps0 / (h[0] * h[0]);
+    ae = aw;
+    an = eps0 / (h[1] * h[1]);
+    as = an;
+    at = eps0 / (h[2] * h[2]);
+    ab = at;
+    ac = -(an + as + aw + ae + at + ab);
+  }
+};
+
+// Numerical Recipes indexx (Src/indexx.f90:1-88), 1-based output indices.
+void indexx(int n, const double *arr, int *indx) {
+  const int M = 7, NSTACK = 50;
+  int istack[NSTACK + 1];
+  for (int j = 1; j <= n; ++j) indx[j - 1] = j;
+  auto A = [&](int i) { return arr[indx[i - 1] - 1]; };
+  int jstack = 0, l = 1, ir = n;
+  for (;;) {
+    if (ir - l < M) {
+      for (int j = l + 1; j <= ir; ++j) {
+        int indxt = indx[j - 1];
+        double a = arr[indxt - 1];
+        int i;
+        for (i = j - 1; i >= 1; --i) {
+          if (A(i) <= a) break;
+          indx[i] = indx[i - 1];
+        }
+        indx[i] = indxt;  // i == 0 when loop ran out
+      }
+      if (jstack == 0) return;
+      ir = istack[jstack];
+      l = istack[jstack - 1];
+      jstack -= 2;
+    } else {
+      int k = (l + ir) / 2;
+      std::swap(indx[k - 1], indx[l]);
+      if (A(l + 1) > A(ir)) std::swap(indx[l], indx[ir - 1]);
+      if (A(l) > A(ir)) std::swap(indx[l - 1], indx[ir - 1]);
+      if (A(l + 1) > A(l)) std::swap(indx[l], indx[l - 1]);
+      int i = l + 1, j = ir;
+      int indxt = indx[l - 1];
+      double a = arr[indxt - 1];
+      for (;;) {
+        do { ++i; } while (A(i) < a);
+        do { --j; } while (A(j) > a);
+        if (j < i) break;
+        std::swap(indx[i - 1], indx[j - 1]);
+      }
+      indx[l - 1] = indx[j - 1];
+      indx[j - 1] = indxt;
+      jstack += 2;
+      if (jstack > NSTACK) return;  // reference STOPs; never reached for n<=65
+      if (ir - i + 1 >= j - l) {
+        istack[jstack] = ir;
+        istack[jstack - 1] = i;
+        ir = j - 1;
+      } else {
+        istack[jstack] = j - 1;
+        istack[jstack - 1] = l;
+        l = i;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Src/ran2.f90:1-14 -- Park-Miller minimal standard with Schrage's trick.
+double oracle_ran2(int *irand) {
+  const int ia = 16807, im = 2147483647, iq = 127773, ir = 2836;
+  const double am = 1.0 / im;
+  int k = *irand / iq;
+  *irand = ia * (*irand - k * iq) - ir * k;
+  if (*irand < 0) *irand += im;
+  return am * (*irand);
+}
+
+// Src/load_part.f90:268-291 (load_gauss).
+void oracle_load_gauss(double *vx, double *vy, double vt, const double rnd[2], double pi) {
+  double vp = vt * std::sqrt(-std::log(1 - rnd[0]));
+  double theta = 2.0 * pi * rnd[1];
+  *vx = vp * std::cos(theta);
+  *vy = vp * std::sin(theta);
+}
+
+// Src/main.f90:336-347 -- kq = 2 on every node that is not plasma.
+void oracle_make_kq(const int n[3], const int *bcnd, double *kq) {
+  Dims d(n);
+  for (long i = 0; i < d.cnt(); ++i) kq[i] = (bcnd[i] != -1) ? 2.0 : 1.0;
+}
+
+// Src/load_part.f90:91-266 (load_part_OMP with one thread, one MPI rank).
+// np must hold ntype node grids; it is zeroed here like the reference.
+int oracle_load_part(const int n[3], const double h[3], const int *bcnd, double *np,
+                     double *vxp, int ntype, int nmax, const double *kq, const double *ni0,
+                     int *np_tot, int *iseed, const OPhys *P) {
+  Dims d(n);
+  std::vector<double> vz_sav(ntype, 0.0);
+  for (int p = 0; p < ntype; ++p) np_tot[p] = 0;
+  std::memset(np, 0, sizeof(double) * d.cnt() * ntype);
+  long jmax = std::lround((double)(float)((long)P->np_cell * P->n_cell));
+  for (long j = 1; j <= jmax; ++j) {
+    double x, y, z;
+    int ix, iy, iz;
+    for (;;) {
+      x = oracle_ran2(iseed) * P->x_load;
+      y = oracle_ran2(iseed) * P->ymax;
+      z = oracle_ran2(iseed) * P->zmax;
+      ix = (int)(x / h[0]) + 1;
+      iy = (int)(y / h[1]) + 1;
+      iz = (int)(z / h[2]) + 1;
+      bool wall = bcnd[d.g(ix, iy, iz)] >= 1 && bcnd[d.g(ix + 1, iy, iz)] >= 1 &&
+                  bcnd[d.g(ix + 1, iy + 1, iz)] >= 1 && bcnd[d.g(ix, iy + 1, iz)] >= 1 &&
+                  bcnd[d.g(ix, iy, iz + 1)] >= 1 && bcnd[d.g(ix + 1, iy, iz + 1)] >= 1 &&
+                  bcnd[d.g(ix + 1, iy + 1, iz + 1)] >= 1 && bcnd[d.g(ix, iy + 1, iz + 1)] >= 1;
+      if (!wall) break;
+    }
+    for (int p = 1; p <= ntype; ++p) {
+      double r = oracle_ran2(iseed);
+      if (r > ni0[p - 1]) continue;
+      int k = ++np_tot[p - 1];
+      if (k > nmax) return ORACLE_ERR_CAPACITY;
+      double vt = P->vt0[p - 1];
+      double *v = vxp + ((long)(p - 1) * nmax + (k - 1)) * 6;
+      v[0] = x;
+      v[1] = y;
+      v[2] = z;
+      double rnd[2], vx, vy;
+      rnd[0] = oracle_ran2(iseed);
+      rnd[1] = oracle_ran2(iseed);
+      oracle_load_gauss(&vx, &vy, vt, rnd, P->pi);
+      v[3] = vx;
+      v[4] = vy;
+      if (vz_sav[p - 1] == 0.0) {
+        rnd[0] = oracle_ran2(iseed);
+        rnd[1] = oracle_ran2(iseed);
+        oracle_load_gauss(&vx, &vy, vt, rnd, P->pi);
+        v[5] = vx;
+        vz_sav[p - 1] = vy;
+      } else {
+        v[5] = vz_sav[p - 1];
+        vz_sav[p - 1] = 0.0;
+      }
+      double px = (ix * h[0] - x) / h[0];
+      double py = (iy * h[1] - y) / h[1];
+      double pz = (iz * h[2] - z) / h[2];
+      double kp = P->Nm[p - 1] / (h[0] * h[1] * h[2]);
+      double ki[8];
+      ki[0] = kp * px * py * pz;
+      ki[1] = kp * (1.0 - px) * py * pz;
+      ki[2] = kp * (1.0 - px) * (1.0 - py) * pz;
+      ki[3] = kp * px * (1.0 - py) * pz;
+      ki[4] = kp * px * py * (1.0 - pz);
+      ki[5] = kp * (1.0 - px) * py * (1.0 - pz);
+      ki[6] = kp * (1.0 - px) * (1.0 - py) * (1.0 - pz);
+      ki[7] = kp * px * (1.0 - py) * (1.0 - pz);
+      double *g = np + (long)(p - 1) * d.cnt();
+      long nd[8] = {d.g(ix, iy, iz),         d.g(ix + 1, iy, iz),         d.g(ix + 1, iy + 1, iz),
+                    d.g(ix, iy + 1, iz),     d.g(ix, iy, iz + 1),         d.g(ix + 1, iy, iz + 1),
+                    d.g(ix + 1, iy + 1, iz + 1), d.g(ix, iy + 1, iz + 1)};
+      for (int c = 0; c < 8; ++c) g[nd[c]] = g[nd[c]] + kq[nd[c]] * ki[c];
+    }
+  }
+  return ORACLE_OK;
+}
+
+// Src/calc_rho.f90:1-114 with nproc = 1 and one MPI rank.  np is modified in
+// place by the periodic stitching exactly like the reference.
+void oracle_calc_rho(const int n[3], double *np, double *rhs, const int *bcnd, int ntype,
+                     const OPhys *P) {
+  Dims d(n);
+  for (long i = 0; i < d.rcnt(); ++i) rhs[i] = 0.0;
+  if (P->flag_pbc == 1) {
+    for (int p = 0; p < ntype; ++p) {
+      double *g = np + (long)p * d.cnt();
+      for (int iz = 1; iz <= d.n3 + 1; ++iz)
+        for (int ix = 1; ix <= d.n1 + 1; ++ix) {
+          if (bcnd[d.g(ix, 1, iz)] == 0) {
+            g[d.g(ix, 1, iz)] = 0.5 * (g[d.g(ix, 1, iz)] + g[d.g(ix, d.n2 + 1, iz)]);
+            g[d.g(ix, 0, iz)] = g[d.g(ix, d.n2, iz)];
+          }
+          if (bcnd[d.g(ix, d.n2 + 1, iz)] == 0) {
+            g[d.g(ix, d.n2 + 2, iz)] = g[d.g(ix, 2, iz)];
+            g[d.g(ix, d.n2 + 1, iz)] = g[d.g(ix, 1, iz)];
+          }
+        }
+      for (int iy = 1; iy <= d.n2 + 1; ++iy)
+        for (int ix = 1; ix <= d.n1 + 1; ++ix) {
+          if (bcnd[d.g(ix, iy, 1)] == 0) {
+            g[d.g(ix, iy, 1)] = 0.5 * (g[d.g(ix, iy, 1)] + g[d.g(ix, iy, d.n3 + 1)]);
+            g[d.g(ix, iy, 0)] = g[d.g(ix, iy, d.n3)];
+          }
+          if (bcnd[d.g(ix, iy, d.n3 + 1)] == 0) {
+            g[d.g(ix, iy, d.n3 + 2)] = g[d.g(ix, iy, 2)];
+            g[d.g(ix, iy, d.n3 + 1)] = g[d.g(ix, iy, 1)];
+          }
+        }
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (int iz = 1; iz <= d.n3 + 1; ++iz)
+    for (int iy = 1; iy <= d.n2 + 1; ++iy)
+      for (int ix = 1; ix <= d.n1 + 1; ++ix) {
+        double acc = rhs[d.r(ix, iy, iz)];
+        for (int p = 0; p < ntype; ++p)
+          acc = acc - P->charge[p] * np[(long)p * d.cnt() + d.g(ix, iy, iz)];
+        rhs[d.r(ix, iy, iz)] = acc;
+      }
+}
+
+// Src/calc_rho.f90:116-186 (dens_red), one thread: np_red = np, and the
+// maximum density over plasma nodes per species.
+void oracle_dens_red(const int n[3], const double *np, double *np_red, const int *bcnd, int ntype,
+                     double *np_mx_out) {
+  Dims d(n);
+  for (int p = 0; p < ntype; ++p) {
+    const double *g = np + (long)p * d.cnt();
+    double *o = np_red + (long)p * d.cnt();
+    for (long i = 0; i < d.cnt(); ++i) o[i] = 0.0;
+    double mx = 0.0;
+    for (int iz = 1; iz <= d.n3 + 1; ++iz)
+      for (int iy = 1; iy <= d.n2 + 1; ++iy)
+        for (int ix = 1; ix <= d.n1 + 1; ++ix) {
+          long i = d.g(ix, iy, iz);
+          o[i] = 0.0 + g[i];
+          if (bcnd[i] == -1) mx = std::max(mx, o[i]);
+        }
+    np_mx_out[p] = mx;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Multigrid: Src/pdesolver.f90, Src/mg.f90, Src/sors.f90 (Dirichlet walls;
+// periodic and Neumann planes are rejected).
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Level {
+  int n[3];
+  double h[3];
+  std::vector<double> e;   // (n+3)^3
+  std::vector<double> r;   // (n+2)^3
+  std::vector<int> bc;     // (n+3)^3
+};
+
+// Src/sors.f90:1-535 (sor_rb) for one rank.
+void sor_rb(double *u, const double *b, const double h[3], const int *bcnd, double *res_out,
+            const int n[3], double omega, double eps, int *ksor, int kmg, int dig, double eps0) {
+  Dims d(n);
+  Coef c(h, eps0);
+  double res_s = 0.0, res = 0.0;
+  *ksor = 0;
+  long nr = 4;
+  if (kmg == 1 && dig == 0) nr = 1000000;
+  const double eta = 0.6;
+  const int m = d.n3;
+  for (long l = 1; l <= nr; ++l) {
+    for (int color = 0; color < 2; ++color) {
+      // red: (i+j+k) odd; black: (i+j+k) even (Src/sors.f90:87-106, 249-267)
+#pragma omp parallel for schedule(static)
+      for (int k = 1; k <= m + 1; ++k)
+        for (int j = 1; j <= d.n2 + 1; ++j) {
+          int ks = (k % 2 == 0) ? 0 : 1;
+          int is;
+          if (color == 0) is = (j % 2 == 0) ? 1 : 2;
+          else is = (j % 2 == 0) ? 2 : 1;
+          is = is + ks;
+          if (is > 2) is = 1;
+          for (int i = is; i <= d.n1 + 1; i += 2) {
+            long q = d.g(i, j, k);
+            if (bcnd[q] > 0) continue;
+            double t = b[d.r(i, j, k)] - c.aw * u[q - 1] - c.an * u[q + d.N1] -
+                       c.as * u[q - d.N1] - c.ae * u[q + 1] - c.at * u[q + d.N1 * d.N2] -
+                       c.ab * u[q - d.N1 * d.N2];
+            u[q] = (1.0 - omega) * u[q] + omega * t / c.ac;
+          }
+        }
+    }
+    res = 0.0;
+    for (int k = 1; k <= m + 1; ++k)
+      for (int j = 1; j <= d.n2 + 1; ++j)
+        for (int i = 1; i <= d.n1 + 1; ++i) {
+          long q = d.g(i, j, k);
+          double rij = 0.0;
+          if (bcnd[q] == -1)
+            rij = b[d.r(i, j, k)] - (c.aw * u[q - 1] + c.an * u[q + d.N1] + c.as * u[q - d.N1] +
+                                     c.ae * u[q + 1] + c.ac * u[q] + c.at * u[q + d.N1 * d.N2] +
+                                     c.ab * u[q - d.N1 * d.N2]);
+          res = res + std::fabs(rij);
+        }
+    *ksor = *ksor + 1;
+    if (dig == 0) {
+      if (res <= eps) break;
+    } else {
+      if (res_s > 0.0 && (res / res_s) <= eta) break;
+    }
+    res_s = res;
+  }
+  *res_out = res;
+}
+
+// Src/mg.f90:808-847 (getres), Dirichlet form.
+inline double getres(const double *u, const double *b, const Coef &c, const Dims &d, int ir, int jr,
+                     int kr) {
+  long q = d.g(ir, jr, kr);
+  double uij = u[q], un = u[q + d.N1], us = u[q - d.N1], ue = u[q + 1];
+  double ut = u[q + d.N1 * d.N2], ub = u[q - d.N1 * d.N2], uw = u[q - 1];
+  double urhs = b[d.r(ir, jr, kr)];
+  return urhs - (c.aw * uw + c.ae * ue + c.an * un + c.as * us + c.ac * uij + c.at * ut + c.ab * ub);
+}
+
+// Src/mg.f90:248-805 (restriction) for one rank, no periodic planes.
+// fine level n (u, b, bcnd) -> coarse level n/2 (bcnd2h, r2h, e2h).
+void restriction(const double *u, const double *b, const double h[3], const int *bcnd, int *bcnd2h,
+                 double *r2h, double *e2h, const int n[3], double eps0) {
+  Dims d(n);
+  int nc[3] = {n[0] / 2, n[1] / 2, n[2] / 2};
+  Dims dc(nc);
+  Coef c(h, eps0);
+  // bcnd2h: injection of the fine mask; ghost planes from fine ghosts
+  // (Src/mg.f90:429-436; corner ghosts the reference leaves unset are
+  // defined the same way here and are never read for Dirichlet walls).
+  auto fmap = [](int ic, int ncell) { return ic == ncell / 2 + 2 ? ncell + 2 : (ic == 0 ? 0 : 2 * ic - 1); };
+  for (int k = 0; k <= nc[2] + 2; ++k)
+    for (int j = 0; j <= nc[1] + 2; ++j)
+      for (int i = 0; i <= nc[0] + 2; ++i)
+        bcnd2h[dc.g(i, j, k)] = bcnd[d.g(fmap(i, n[0]), fmap(j, n[1]), fmap(k, n[2]))];
+  for (long q = 0; q < dc.cnt(); ++q) e2h[q] = 0.0;
+  for (long q = 0; q < dc.rcnt(); ++q) r2h[q] = 0.0;
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= nc[2] + 1; ++k)
+    for (int j = 1; j <= nc[1] + 1; ++j)
+      for (int i = 1; i <= nc[0] + 1; ++i) {
+        int ir = 2 * i - 1, jr = 2 * j - 1, kr = 2 * k - 1;
+        if (bcnd2h[dc.g(i, j, k)] > 0) {
+          r2h[dc.r(i, j, k)] = 0.0;
+          continue;
+        }
+        auto R = [&](int a, int bb, int cc) -> double {
+          if (bcnd[d.g(a, bb, cc)] > 0) return 0.0;
+          return getres(u, b, c, d, a, bb, cc);
+        };
+        double r000 = R(ir, jr, kr);
+        double rpp0 = R(ir + 1, jr + 1, kr), rp00 = R(ir + 1, jr, kr), rpm0 = R(ir + 1, jr - 1, kr);
+        double r0m0 = R(ir, jr - 1, kr), rmm0 = R(ir - 1, jr - 1, kr), rm00 = R(ir - 1, jr, kr);
+        double rmp0 = R(ir - 1, jr + 1, kr), r0p0 = R(ir, jr + 1, kr);
+        double r00p = R(ir, jr, kr + 1), rppp = R(ir + 1, jr + 1, kr + 1), rp0p = R(ir + 1, jr, kr + 1);
+        double rpmp = R(ir + 1, jr - 1, kr + 1), r0mp = R(ir, jr - 1, kr + 1);
+        double rmmp = R(ir - 1, jr - 1, kr + 1), rm0p = R(ir - 1, jr, kr + 1);
+        double rmpp = R(ir - 1, jr + 1, kr + 1), r0pp = R(ir, jr + 1, kr + 1);
+        double r00m = R(ir, jr, kr - 1), rppm = R(ir + 1, jr + 1, kr - 1), rp0m = R(ir + 1, jr, kr - 1);
+        double rpmm = R(ir + 1, jr - 1, kr - 1), r0mm = R(ir, jr - 1, kr - 1);
+        double rmmm = R(ir - 1, jr - 1, kr - 1), rm0m = R(ir - 1, jr, kr - 1);
+        double rmpm = R(ir - 1, jr + 1, kr - 1), r0pm = R(ir, jr + 1, kr - 1);
+        double re = (8.0 * r000 + 4.0 * (rp00 + rm00 + r0p0 + r0m0 + r00p + r00m) +
+                     2.0 * (rpp0 + rmp0 + rpm0 + rmm0 + rp0p + rm0p + r0pp + r0mp + rp0m + rm0m +
+                            r0pm + r0mm) +
+                     rppp + rmpp + rpmp + rmmp + rppm + rmpm + rpmm + rmmm) /
+                    64.0;
+        r2h[dc.r(i, j, k)] = re;
+      }
+}
+
+// Src/mg.f90:849-939 (prolongation): trilinear add of e2h into u.
+void prolongation(double *u, const double *e2h, const int *bcnd, const int n[3]) {
+  Dims d(n);
+  int nc[3] = {n[0] / 2, n[1] / 2, n[2] / 2};
+  Dims dc(nc);
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= nc[2] + 1; ++k)
+    for (int j = 1; j <= nc[1] + 1; ++j)
+      for (int i = 1; i <= nc[0] + 1; ++i) {
+        double r000 = e2h[dc.g(i, j, k)], r0m0 = e2h[dc.g(i, j - 1, k)];
+        double rmm0 = e2h[dc.g(i - 1, j - 1, k)], rm00 = e2h[dc.g(i - 1, j, k)];
+        double r00m = e2h[dc.g(i, j, k - 1)], r0mm = e2h[dc.g(i, j - 1, k - 1)];
+        double rmmm = e2h[dc.g(i - 1, j - 1, k - 1)], rm0m = e2h[dc.g(i - 1, j, k - 1)];
+        int ir = 2 * i - 1, jr = 2 * j - 1, kr = 2 * k - 1;
+        long q;
+        q = d.g(ir, jr, kr);
+        if (bcnd[q] <= 0) u[q] = u[q] + r000;
+        q = d.g(ir, jr - 1, kr);
+        if (bcnd[q] <= 0) u[q] = u[q] + (r000 + r0m0) / 2.0;
+        q = d.g(ir - 1, jr - 1, kr);
+        if (bcnd[q] <= 0) u[q] = u[q] + (r000 + r0m0 + rmm0 + rm00) / 4.0;
+        q = d.g(ir - 1, jr, kr);
+        if (bcnd[q] <= 0) u[q] = u[q] + (r000 + rm00) / 2.0;
+        q = d.g(ir, jr, kr - 1);
+        if (bcnd[q] <= 0) u[q] = u[q] + (r000 + r00m) / 2.0;
+        q = d.g(ir, jr - 1, kr - 1);
+        if (bcnd[q] <= 0) u[q] = u[q] + (r000 + r00m + r0mm + r0m0) / 4.0;
+        q = d.g(ir - 1, jr, kr - 1);
+        if (bcnd[q] <= 0) u[q] = u[q] + (r000 + r00m + rm0m + rm00) / 4.0;
+        q = d.g(ir - 1, jr - 1, kr - 1);
+        if (bcnd[q] <= 0) u[q] = u[q] + (r000 + r00m + rm0m + rm00 + r0m0 + r0mm + rmmm + rmm0) / 8.0;
+      }
+}
+
+}  // namespace
+
+// Src/pdesolver.f90:1-134 driving Src/mg.f90:1-245 (one rank).
+// u: (n+3)^3 potential with Dirichlet values on wall nodes (updated in place,
+// warm start); b: (n+2)^3 right-hand side (-rho).  Returns 0, or
+// ORACLE_ERR_DIVERGED when the residual grows by more than 10x (the
+// reference's stop_calculation), or ORACLE_ERR_UNSUPPORTED for periodic /
+// Neumann planes.  *k = number of V-cycles + 1 (the reference's exit value).
+int oracle_pdesolver(double *u, const double *b, const int *bcnd, const double h[3], const int n[3],
+                     int ncycl, double eps, double omega, int *k, double *ktot, double *res, int ng,
+                     const OPhys *P) {
+  if (P->flag_pbc || P->flag_nmn) return ORACLE_ERR_UNSUPPORTED;
+  Coef c0(h, P->eps0);
+  const double u0 = 1.0;
+  double alpha = std::fabs((double)((n[0] + 1) * (n[1] + 1) * (n[2] + 1)) * c0.ac) * u0;
+  *ktot = 0.0;
+  double res_s = 0.0;
+  std::vector<Level> L(ng + 1);
+  for (int l = 1; l <= ng; ++l) {
+    for (int a = 0; a < 3; ++a) {
+      L[l].n[a] = n[a] >> (l - 1);
+      L[l].h[a] = h[a] * (double)(1 << (l - 1));
+    }
+    if (l >= 2) {
+      Dims dl(L[l].n);
+      L[l].e.assign(dl.cnt(), 0.0);
+      L[l].r.assign(dl.rcnt(), 0.0);
+      L[l].bc.assign(dl.cnt(), 0);
+    }
+  }
+  auto U = [&](int l) -> double * { return l == 1 ? u : L[l].e.data(); };
+  auto B = [&](int l) -> const double * { return l == 1 ? b : L[l].r.data(); };
+  auto BC = [&](int l) -> const int * { return l == 1 ? bcnd : L[l].bc.data(); };
+  *k = 1;
+  bool converged = false;
+  int rc = ORACLE_OK;
+  while (!converged) {
+    std::vector<int> iter(ng + 1, 0);
+    double r = 0.0;
+    int ksor = 0;
+    double eps_abs = alpha * eps;
+    for (int ig = 1; ig <= 2 * ng - 1; ++ig) {
+      if (ig < ng) {
+        int il = ig;
+        sor_rb(U(il), B(il), L[il].h, BC(il), &r, L[il].n, omega, eps_abs, &ksor, *k, ig - ng, P->eps0);
+        iter[il] += ksor;
+        restriction(U(il), B(il), L[il].h, BC(il), L[il + 1].bc.data(), L[il + 1].r.data(),
+                    L[il + 1].e.data(), L[il].n, P->eps0);
+      } else if (ig == ng) {
+        int il = ng;
+        sor_rb(U(il), B(il), L[il].h, BC(il), &r, L[il].n, omega, eps_abs, &ksor, *k, 0, P->eps0);
+        iter[il] += ksor;
+        if (ng >= 2) prolongation(U(il - 1), U(il), BC(il - 1), L[il - 1].n);
+      } else {
+        int il = 2 * ng - ig;
+        sor_rb(U(il), B(il), L[il].h, BC(il), &r, L[il].n, omega, eps_abs, &ksor, *k, ig - ng, P->eps0);
+        iter[il] += ksor;
+        if (il >= 2) prolongation(U(il - 1), U(il), BC(il - 1), L[il - 1].n);
+      }
+    }
+    for (int i = 1; i <= ng; ++i) *ktot = *ktot + (double)(float)iter[i] / std::pow(2.0, 2 * (i - 1));
+    r = r / alpha;
+    if (*k == 1) {
+      res_s = r;
+    } else if (std::fabs(r / res_s) > 10.0) {
+      rc = ORACLE_ERR_DIVERGED;
+      converged = true;
+    }
+    if (r < eps || *k == ncycl) converged = true;
+    *res = r;
+    *k = *k + 1;
+  }
+  return rc;
+}
+
+// Src/Efield.f90:1-191 -- E = -grad(phi) with wall extrapolation, periodic
+// planes and the left-hand Neumann plane.
+void oracle_calc_efield(const int n[3], const double h[3], const double *phi, double *Ei,
+                        const int *bcnd) {
+  Dims d(n);
+  auto E = [&](int c, int ix, int iy, int iz) -> double & { return Ei[3 * d.g(ix, iy, iz) + c]; };
+  auto F = [&](int ix, int iy, int iz) -> double { return phi[d.g(ix, iy, iz)]; };
+  auto B = [&](int ix, int iy, int iz) -> int { return bcnd[d.g(ix, iy, iz)]; };
+  const int n1 = d.n1, n2 = d.n2, n3 = d.n3;
+#pragma omp parallel for schedule(static)
+  for (int iz = 1; iz <= n3 + 1; ++iz)
+    for (int iy = 1; iy <= n2 + 1; ++iy)
+      for (int ix = 1; ix <= n1 + 1; ++ix)
+        if (B(ix, iy, iz) <= 0) {
+          E(0, ix, iy, iz) = -(F(ix + 1, iy, iz) - F(ix - 1, iy, iz)) / (2.0 * h[0]);
+          E(1, ix, iy, iz) = -(F(ix, iy + 1, iz) - F(ix, iy - 1, iz)) / (2.0 * h[1]);
+          E(2, ix, iy, iz) = -(F(ix, iy, iz + 1) - F(ix, iy, iz - 1)) / (2.0 * h[2]);
+        }
+  for (int iz = 1; iz <= n3 + 1; ++iz)
+    for (int iy = 1; iy <= n2 + 1; ++iy)
+      for (int ix = 1; ix <= n1 + 1; ++ix) {
+        int bc = B(ix, iy, iz);
+        if (bc == -1) continue;
+        if (bc == -2) {
+          E(0, 1, iy, iz) = 0.0;
+          if (iy > 1 && iy < n2 + 1 && iz > 1 && iz < n3 + 1) {
+            E(1, 1, iy, iz) = -(F(1, iy + 1, iz) - F(1, iy - 1, iz)) / (2.0 * h[1]);
+            E(2, 1, iy, iz) = -(F(1, iy, iz + 1) - F(1, iy, iz - 1)) / (2.0 * h[2]);
+            continue;
+          }
+        }
+        if (bc == 0 || bc == -2) {
+          if (iy == 1) {
+            E(1, ix, 1, iz) = -(F(ix, 2, iz) - F(ix, n2, iz)) / (2.0 * h[1]);
+            E(1, ix, 0, iz) = E(1, ix, n2, iz);
+            E(1, ix, n2 + 1, iz) = E(1, ix, 1, iz);
+            E(1, ix, n2 + 2, iz) = E(1, ix, 2, iz);
+            E(0, ix, 0, iz) = E(0, ix, n2, iz);
+            E(0, ix, n2 + 2, iz) = E(0, ix, 2, iz);
+            E(2, ix, 0, iz) = E(2, ix, n2, iz);
+            E(2, ix, n2 + 2, iz) = E(2, ix, 2, iz);
+          }
+          if (iz == 1) {
+            E(2, ix, iy, 1) = -(F(ix, iy, 2) - F(ix, iy, n3)) / (2.0 * h[2]);
+            E(2, ix, iy, 0) = E(2, ix, iy, n3);
+            E(2, ix, iy, n3 + 1) = E(2, ix, iy, 1);
+            E(2, ix, iy, n3 + 2) = E(2, ix, iy, 2);
+            E(0, ix, iy, 0) = E(0, ix, iy, n3);
+            E(0, ix, iy, n3 + 2) = E(0, ix, iy, 2);
+            E(1, ix, iy, 0) = E(1, ix, iy, n3);
+            E(1, ix, iy, n3 + 2) = E(1, ix, iy, 2);
+          }
+          continue;
+        }
+        // walls (bc >= 1)
+        if (B(ix + 1, iy, iz) <= 0) {
+          E(0, ix, iy, iz) = 2.0 * E(0, ix + 1, iy, iz) - E(0, ix + 2, iy, iz);
+          E(1, ix, iy, iz) = -(F(ix, iy + 1, iz) - F(ix, iy - 1, iz)) / (2.0 * h[1]);
+          E(2, ix, iy, iz) = -(F(ix, iy, iz + 1) - F(ix, iy, iz - 1)) / (2.0 * h[2]);
+        }
+        if (B(ix - 1, iy, iz) <= 0) {
+          E(0, ix, iy, iz) = 2.0 * E(0, ix - 1, iy, iz) - E(0, ix - 2, iy, iz);
+          E(1, ix, iy, iz) = -(F(ix, iy + 1, iz) - F(ix, iy - 1, iz)) / (2.0 * h[1]);
+          E(2, ix, iy, iz) = -(F(ix, iy, iz + 1) - F(ix, iy, iz - 1)) / (2.0 * h[2]);
+        }
+        if (B(ix, iy + 1, iz) <= 0) {
+          E(0, ix, iy, iz) = -(F(ix + 1, iy, iz) - F(ix - 1, iy, iz)) / (2.0 * h[0]);
+          E(1, ix, iy, iz) = 2.0 * E(1, ix, iy + 1, iz) - E(1, ix, iy + 2, iz);
+          E(2, ix, iy, iz) = -(F(ix, iy, iz + 1) - F(ix, iy, iz - 1)) / (2.0 * h[2]);
+        }
+        if (B(ix, iy - 1, iz) <= 0) {
+          E(0, ix, iy, iz) = -(F(ix + 1, iy, iz) - F(ix - 1, iy, iz)) / (2.0 * h[0]);
+          E(1, ix, iy, iz) = 2.0 * E(1, ix, iy - 1, iz) - E(1, ix, iy - 2, iz);
+          E(2, ix, iy, iz) = -(F(ix, iy, iz + 1) - F(ix, iy, iz - 1)) / (2.0 * h[2]);
+        }
+        if (B(ix, iy, iz + 1) <= 0) {
+          E(0, ix, iy, iz) = -(F(ix + 1, iy, iz) - F(ix - 1, iy, iz)) / (2.0 * h[0]);
+          E(1, ix, iy, iz) = -(F(ix, iy + 1, iz) - F(ix, iy - 1, iz)) / (2.0 * h[1]);
+          E(2, ix, iy, iz) = 2.0 * E(2, ix, iy, iz + 1) - E(2, ix, iy, iz + 2);
+        }
+        if (B(ix, iy, iz - 1) <= 0) {
+          E(0, ix, iy, iz) = -(F(ix + 1, iy, iz) - F(ix - 1, iy, iz)) / (2.0 * h[0]);
+          E(1, ix, iy, iz) = -(F(ix, iy + 1, iz) - F(ix, iy - 1, iz)) / (2.0 * h[1]);
+          E(2, ix, iy, iz) = 2.0 * E(2, ix, iy, iz - 1) - E(2, ix, iy, iz - 2);
+        }
+      }
+}
+
+// Src/part_expmover.f90:1-482 (part_mover) without the dbg_* counters, for
+// uniform B (n_B(1) = 1) and metal walls.  p_mac(ntype,2,0:ngrid) and
+// P_loss(4,ntype) are accumulated like the reference (column-major).
+// Dead particles (flag_dead = 1) are removed; lost particles are compacted
+// out in order.  Returns ORACLE_ERR_UNSUPPORTED for periodic/Neumann planes
+// combined with negative ions or dielectric walls (out of scope).
+int oracle_part_mover(const int n[3], const double h[3], const double *Ei, double *p_mac,
+                      double *P_loss, double *vxp, const int *bcnd, int nmax, int ntype, int ngrid,
+                      signed char *flag_dead, int *np_tot, int ptype, const OPhys *P) {
+  // Two passes: the push of every particle (independent, OpenMP over
+  // contiguous particle slices like the reference's thread slices), then the
+  // in-order compaction i_shift = i - np_lost (Src/part_expmover.f90:454-470).
+  // Loss sums are accumulated per slice and added in slice order; with one
+  // thread this is the serial order of the reference.
+  Dims d(n);
+  const int p = ptype - 1;
+  const double q = P->charge[p], mass = P->mass[p], Nm = P->Nm[p], dt = P->dt;
+  const double k1 = dt * q / (2.0 * mass);
+  const int N = np_tot[p];
+  double *V = vxp + (long)p * nmax * 6;
+  signed char *fd = flag_dead + (long)p * nmax;
+  std::vector<signed char> state(N);  // 0 kept, 1 dead, 2 lost
+  std::vector<int> lost_grid(N, 0);
+  std::vector<double> lost_E(N, 0.0);
+  int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+  for (int i = 0; i < N; ++i) {
+    double *v = V + (long)i * 6;
+    double xp = v[0], yp = v[1], zp = v[2], vx = v[3], vy = v[4], vz = v[5];
+    if (fd[i] == 1) {
+      fd[i] = 0;
+      state[i] = 1;
+      lost_E[i] = 0.5 * Nm * mass * (vx * vx + vy * vy + vz * vz);
+      continue;
+    }
+    int ix = (int)(xp / h[0]) + 1, iy = (int)(yp / h[1]) + 1, iz = (int)(zp / h[2]) + 1;
+    double px = (ix * h[0] - xp) / h[0];
+    double py = (iy * h[1] - yp) / h[1];
+    double pz = (iz * h[2] - zp) / h[2];
+    double ki[8];
+    ki[0] = px * py * pz;
+    ki[1] = (1.0 - px) * py * pz;
+    ki[2] = (1.0 - px) * (1.0 - py) * pz;
+    ki[3] = px * (1.0 - py) * pz;
+    ki[4] = px * py * (1.0 - pz);
+    ki[5] = (1.0 - px) * py * (1.0 - pz);
+    ki[6] = (1.0 - px) * (1.0 - py) * (1.0 - pz);
+    ki[7] = px * (1.0 - py) * (1.0 - pz);
+    long nd[8] = {d.g(ix, iy, iz),         d.g(ix + 1, iy, iz),         d.g(ix + 1, iy + 1, iz),
+                  d.g(ix, iy + 1, iz),     d.g(ix, iy, iz + 1),         d.g(ix + 1, iy, iz + 1),
+                  d.g(ix + 1, iy + 1, iz + 1), d.g(ix, iy + 1, iz + 1)};
+    double Ec[3];
+    for (int c = 0; c < 3; ++c) {
+      double s = ki[0] * Ei[3 * nd[0] + c];
+      for (int a = 1; a < 8; ++a) s = s + ki[a] * Ei[3 * nd[a] + c];
+      Ec[c] = s;
+    }
+    int flag_B_tmp = 0;
+    double Bx = 0, By = 0, Bz = 0;
+    if (P->flag_B == 1) {
+      Bx = P->Bconst[0];
+      By = P->Bconst[1];
+      Bz = P->Bconst[2];
+      flag_B_tmp = 1;
+    }
+    if (P->flag_B_pos == 1 && q > 0.0) flag_B_tmp = 0;
+    if (flag_B_tmp == 1) {
+      double B_tot = std::sqrt(Bx * Bx + By * By + Bz * Bz);
+      double k2 = k1 * (2.0 / (1.0 + (k1 * B_tot) * (k1 * B_tot)));
+      double v1x = vx + k1 * Ec[0], v1y = vy + k1 * Ec[1], v1z = vz + k1 * Ec[2];
+      double v3x = v1x + k1 * (v1y * Bz - v1z * By);
+      double v3y = v1y + k1 * (v1z * Bx - v1x * Bz);
+      double v3z = v1z + k1 * (v1x * By - v1y * Bx);
+      double v2x = v1x + k2 * (v3y * Bz - v3z * By);
+      double v2y = v1y + k2 * (v3z * Bx - v3x * Bz);
+      double v2z = v1z + k2 * (v3x * By - v3y * Bx);
+      vx = v2x + k1 * Ec[0];
+      vy = v2y + k1 * Ec[1];
+      vz = v2z + k1 * Ec[2];
+    } else {
+      vx = vx + 2.0 * k1 * Ec[0];
+      vy = vy + 2.0 * k1 * Ec[1];
+      vz = vz + 2.0 * k1 * Ec[2];
+    }
+    xp = xp + dt * vx;
+    yp = yp + dt * vy;
+    zp = zp + dt * vz;
+    ix = (int)std::floor(xp / h[0]) + 1;
+    iy = (int)std::floor(yp / h[1]) + 1;
+    iz = (int)std::floor(zp / h[2]) + 1;
+    if (ix < 0) ix = 0;
+    if (ix > d.n1 + 1) ix = d.n1 + 1;
+    if (iy < 0) iy = 0;
+    if (iy > d.n2 + 1) iy = d.n2 + 1;
+    if (iz < 0) iz = 0;
+    if (iz > d.n3 + 1) iz = d.n3 + 1;
+    int lost = bcnd[d.g(ix, iy, iz)] >= 1 && bcnd[d.g(ix + 1, iy, iz)] >= 1 &&
+               bcnd[d.g(ix + 1, iy + 1, iz)] >= 1 && bcnd[d.g(ix, iy + 1, iz)] >= 1 &&
+               bcnd[d.g(ix, iy, iz + 1)] >= 1 && bcnd[d.g(ix + 1, iy, iz + 1)] >= 1 &&
+               bcnd[d.g(ix + 1, iy + 1, iz + 1)] >= 1 && bcnd[d.g(ix, iy + 1, iz + 1)] >= 1;
+    if (lost) {
+      state[i] = 2;
+      lost_E[i] = 0.5 * Nm * mass * (vx * vx + vy * vy + vz * vz);
+      lost_grid[i] = bcnd[d.g(ix, iy, iz)];
+      if (lost_grid[i] > ngrid) bad = 1;
+      continue;
+    }
+    if (P->flag_nmn == 1 && xp <= 0.0) {
+      xp = -xp;
+      vx = -vx;
+    }
+    if (P->flag_pbc == 1) {
+      if (yp >= P->ymax) yp = yp - P->ymax;
+      if (yp <= 0.0) yp = P->ymax + yp;
+      if (zp >= P->zmax) zp = zp - P->zmax;
+      if (zp <= 0.0) zp = P->zmax + zp;
+    }
+    state[i] = 0;
+    v[0] = xp;
+    v[1] = yp;
+    v[2] = zp;
+    v[3] = vx;
+    v[4] = vy;
+    v[5] = vz;
+  }
+  if (bad) return ORACLE_ERR_UNSUPPORTED;
+  auto pm = [&](int which, int igrid) -> double & {
+    return p_mac[p + (long)ntype * (which + 2L * igrid)];
+  };
+  auto PL = [&](int which) -> double & { return P_loss[which + 4L * p]; };
+  int np_lost = 0;
+  for (int i = 0; i < N; ++i) {
+    if (state[i] == 1) {
+      np_lost++;
+      PL(2) = PL(2) - lost_E[i];
+    } else if (state[i] == 2) {
+      np_lost++;
+      PL(0) = PL(0) + lost_E[i];
+      pm(0, lost_grid[i]) = pm(0, lost_grid[i]) + 1.0;
+      pm(1, lost_grid[i]) = pm(1, lost_grid[i]) + lost_E[i];
+    } else if (np_lost) {
+      std::memcpy(V + (long)(i - np_lost) * 6, V + (long)i * 6, 6 * sizeof(double));
+    }
+  }
+  np_tot[p] = N - np_lost;
+  return ORACLE_OK;
+}
+
+// Src/part_expmover.f90:570-686 (charge_deposition): CIC with kq.  np of
+// species ptype is accumulated (the caller zeroes it, Src/main.f90:1268).
+void oracle_charge_deposition(const int n[3], const double h[3], const double *vxp, int nmax,
+                              int ntype, const double *kq, double *np, const int *np_tot, int ptype,
+                              const OPhys *P) {
+  (void)ntype;
+  Dims d(n);
+  const int p = ptype - 1;
+  const double *V = vxp + (long)p * nmax * 6;
+  double *g = np + (long)p * d.cnt();
+  const double k1 = P->Nm[p] / (h[0] * h[1] * h[2]);
+  const int N = np_tot[p];
+  int nth = 1;
+#ifdef _OPENMP
+  nth = omp_get_max_threads();
+#endif
+  // one private grid per thread slice (the reference's np(...,iproc)),
+  // summed in slice order afterwards; one thread deposits straight into g
+  std::vector<std::vector<double>> priv(nth > 1 ? nth : 0);
+#pragma omp parallel num_threads(nth)
+  {
+    int t = 0;
+#ifdef _OPENMP
+    t = omp_get_thread_num();
+#endif
+    double *G = g;
+    if (nth > 1) {
+      priv[t].assign(d.cnt(), 0.0);
+      G = priv[t].data();
+    }
+    long lo = (long)N * t / nth, hi = (long)N * (t + 1) / nth;
+    for (long i = lo; i < hi; ++i) {
+      const double *v = V + i * 6;
+      double xp = v[0], yp = v[1], zp = v[2];
+      int ix = (int)(xp / h[0]) + 1, iy = (int)(yp / h[1]) + 1, iz = (int)(zp / h[2]) + 1;
+      double px = (ix * h[0] - xp) / h[0];
+      double py = (iy * h[1] - yp) / h[1];
+      double pz = (iz * h[2] - zp) / h[2];
+      double ki[8];
+      ki[0] = k1 * px * py * pz;
+      ki[1] = k1 * (1.0 - px) * py * pz;
+      ki[2] = k1 * (1.0 - px) * (1.0 - py) * pz;
+      ki[3] = k1 * px * (1.0 - py) * pz;
+      ki[4] = k1 * px * py * (1.0 - pz);
+      ki[5] = k1 * (1.0 - px) * py * (1.0 - pz);
+      ki[6] = k1 * (1.0 - px) * (1.0 - py) * (1.0 - pz);
+      ki[7] = k1 * px * (1.0 - py) * (1.0 - pz);
+      long nd[8] = {d.g(ix, iy, iz),         d.g(ix + 1, iy, iz),         d.g(ix + 1, iy + 1, iz),
+                    d.g(ix, iy + 1, iz),     d.g(ix, iy, iz + 1),         d.g(ix + 1, iy, iz + 1),
+                    d.g(ix + 1, iy + 1, iz + 1), d.g(ix, iy + 1, iz + 1)};
+      for (int c = 0; c < 8; ++c) G[nd[c]] = G[nd[c]] + kq[nd[c]] * ki[c];
+    }
+  }
+  if (nth > 1) {
+#pragma omp parallel for schedule(static)
+    for (long q = 0; q < d.cnt(); ++q) {
+      double acc = g[q];
+      for (int t = 0; t < nth; ++t) acc = acc + priv[t][q];
+      g[q] = acc;
+    }
+  }
+}
+
+// Src/sorting.f90:97-258 (part_sorting) with one thread: a stable counting
+// sort on the cell index ic = (ix-1) + n1((iy-1) + n2(iz-1)) + 1.
+// Plist(0:pl_max) receives the inclusive end offset of each cell.
+void oracle_part_sorting(double *vxp, int nmax, int ntype, const int n[3], const double h[3],
+                         int *Plist, int pl_max, const int *np_tot, int ptype) {
+  (void)ntype;
+  const int p = ptype - 1;
+  double *V = vxp + (long)p * nmax * 6;
+  const int N = np_tot[p];
+  std::vector<int> cnt(pl_max + 1, 0), ic(N);
+  std::vector<double> tmp((size_t)N * 6);
+  for (int i = 0; i < N; ++i) {
+    const double *v = V + (long)i * 6;
+    int ix = (int)(v[0] / h[0]) + 1, iy = (int)(v[1] / h[1]) + 1, iz = (int)(v[2] / h[2]) + 1;
+    ic[i] = (ix - 1) + n[0] * ((iy - 1) + n[1] * (iz - 1)) + 1;
+    cnt[ic[i]] += 1;
+    std::memcpy(&tmp[(size_t)i * 6], v, 6 * sizeof(double));
+  }
+  int k = 0;
+  for (int i = 1; i <= pl_max; ++i) {
+    int j = cnt[i];
+    cnt[i] = k;
+    k += j;
+  }
+  for (int i = 0; i < N; ++i) {
+    int j = ++cnt[ic[i]];
+    std::memcpy(V + (long)(j - 1) * 6, &tmp[(size_t)i * 6], 6 * sizeof(double));
+  }
+  Plist[0] = 0;
+  for (int i = 1; i <= pl_max; ++i) Plist[i] = cnt[i] > 0 ? cnt[i] : 0;
+}
+
+// Src/read_reactions.f90:477-661 (ordering): merged sorted unique energy
+// grid, each table re-interpolated on it (below the first point the first
+// value is kept; above its last point the value of the previous grid point is
+// carried, as the reference's loop does), (sigma v)_max over E >= 1 eV and the
+// per-incident-species reaction lists.
+// Inputs: per reaction icol, sig_npt[icol] points at sig_tmp_E/s(ipt, icol)
+// with leading dimension npt_in_mx (column-major, the column must hold one
+// extra zero entry after the last point like the reference's array).
+int oracle_ordering(int ncol, const int *sig_npt, const double *sig_tmp_E, const double *sig_tmp_s,
+                    int npt_in_mx, const double *Eth, const int *col_info, const double *mass,
+                    int ntype, double qe, double *sig_Er, double *sig, int npt_mx, int *npt_out,
+                    int *sig_list, int *p_ncol, double *sigv_mx) {
+  (void)Eth;
+  int length = 0;
+  for (int c = 0; c < ncol; ++c) length += sig_npt[c];
+  std::vector<double> sortE(length);
+  std::vector<int> indx(length);
+  int q = 0;
+  for (int c = 0; c < ncol; ++c)
+    for (int ipt = 0; ipt < sig_npt[c]; ++ipt) sortE[q++] = sig_tmp_E[ipt + (long)npt_in_mx * c];
+  indexx(length, sortE.data(), indx.data());
+  int nnew = 0;
+  double sav = 1.0e10;
+  for (int ipt = 0; ipt < length; ++ipt) {
+    double e = sortE[indx[ipt] - 1];
+    if (e != sav) {
+      if (nnew >= npt_mx) return ORACLE_ERR_CAPACITY;
+      sig_Er[nnew++] = e;
+      sav = e;
+    }
+  }
+  *npt_out = nnew;
+  for (int c = 0; c < ncol; ++c) {
+    int npt = sig_npt[c];
+    const double *TE = sig_tmp_E + (long)npt_in_mx * c;
+    const double *TS = sig_tmp_s + (long)npt_in_mx * c;
+    double sig_p = 0.0;
+    for (int ipt = 0; ipt < nnew; ++ipt) {
+      double Ekp = sig_Er[ipt];
+      for (int j = 0; j < npt; ++j) {
+        double EL = TE[j], ER = TE[j + 1], sL = TS[j], sR = TS[j + 1];
+        if (Ekp < EL) {
+          sig_p = sL;
+          break;
+        }
+        if (Ekp >= EL && Ekp <= ER) {
+          sig_p = sL + (Ekp - EL) * (sR - sL) / (ER - EL);
+          break;
+        }
+      }
+      sig[ipt + (long)npt_mx * c] = sig_p;
+    }
+  }
+  for (int i = 0; i < ORACLE_NPART * ncol; ++i) {
+    sigv_mx[i] = 0.0;
+    sig_list[i] = 0;
+  }
+  int ind_col[ORACLE_NPART] = {0};
+  for (int c = 0; c < ncol; ++c) {
+    int r1 = col_info[c + (long)ncol * 2];  // col_info(icol, ind_nby+1)
+    int r2 = col_info[c + (long)ncol * 3];  // col_info(icol, ind_nby+2)
+    ind_col[r1 - 1] += 1;
+    sig_list[(r1 - 1) + ORACLE_NPART * (ind_col[r1 - 1] - 1)] = c + 1;
+    double m1 = std::fabs(mass[r1 - 1]), m2 = std::fabs(mass[r2 - 1]);
+    double mu = m1 * m2 / (m1 + m2);
+    for (int ipt = 0; ipt < nnew; ++ipt) {
+      double vr = std::sqrt(2.0 * sig_Er[ipt] * qe / mu);
+      if (sig_Er[ipt] >= 1.0) {
+        double &s = sigv_mx[(r1 - 1) + ORACLE_NPART * (long)c];
+        s = std::max(s, vr * sig[ipt + (long)npt_mx * c]);
+      }
+    }
+  }
+  for (int p = 0; p < ntype; ++p) p_ncol[p] = ind_col[p];
+  return ORACLE_OK;
+}
+
+// Src/collisions.f90:1022-1050 (scatter).
+void oracle_scatter(double *vx1, double *vy1, double *vz1, double vx, double vy, double vz,
+                    double costheta, double phi) {
+  double sintheta = std::sqrt(std::max(1.0 - costheta * costheta, 0.0));
+  double sinphi = std::sin(phi), cosphi = std::cos(phi);
+  double v = std::sqrt(vx * vx + vy * vy + vz * vz);
+  if (v == 0.0) return;
+  if (std::fabs(vy) > std::fabs(vz)) {
+    double vv = std::sqrt(vx * vx + vy * vy);
+    *vx1 = vx * costheta + (vy * v * sinphi + vx * vz * cosphi) / vv * sintheta;
+    *vy1 = vy * costheta + (-vx * v * sinphi + vy * vz * cosphi) / vv * sintheta;
+    *vz1 = vz * costheta - vv * cosphi * sintheta;
+  } else {
+    double vv = std::sqrt(vx * vx + vz * vz);
+    *vx1 = vx * costheta + (vz * v * sinphi - vy * vx * cosphi) / vv * sintheta;
+    *vy1 = vy * costheta + vv * cosphi * sintheta;
+    *vz1 = vz * costheta - (vx * v * sinphi + vy * vz * cosphi) / vv * sintheta;
+  }
+}
+
+// Src/collisions.f90:1-1020 (collisions + collision_OMP) with one thread,
+// one rank, neutral (Monte-Carlo) targets.  Charged (DSMC) targets are
+// rejected with ORACLE_ERR_UNSUPPORTED.  cnt_col[icol] counts the collisions
+// of each reaction; Nc_out[ptype] the number of picks.
+int oracle_collisions(double *vxp, const int n[3], const double h[3], int ntype, int nmax,
+                      const OTables *T, signed char *flag_dead, int *np_tot, int *iseed,
+                      const OPhys *P, double *nu_max, long long *cnt_col, int *Nc_out) {
+  (void)n;
+  (void)h;
+  const double qe = P->qe, pi = P->pi;
+  auto CI = [&](int icol, int info) { return T->col_info[(icol - 1) + (long)T->ncol * (info - 1)]; };
+  auto SL = [&](int p, int icol) { return T->sig_list[(p - 1) + ORACLE_NPART * (long)(icol - 1)]; };
+  auto SVM = [&](int p, int icol) { return T->sigv_mx[(p - 1) + ORACLE_NPART * (long)(icol - 1)]; };
+  auto SIG = [&](int ipt, int icol) { return T->sig[(ipt - 1) + (long)T->npt_mx * (icol - 1)]; };
+  auto absm = [&](int t) { return std::fabs(P->mass[t - 1]); };
+  std::vector<int> Nc(ntype + 1, 0), np_add(ntype + 1, 0);
+  std::vector<int> sav_ttype(T->ncol + 1, 0);
+  for (int p = 1; p <= ntype; ++p) {
+    nu_max[p - 1] = 0.0;
+    if (T->p_ncol[p - 1] == 0 || P->mass[p - 1] <= 0) continue;
+    for (int icol = 1; icol <= T->p_ncol[p - 1]; ++icol) {
+      int ind = SL(p, icol);
+      int n_re = CI(ind, 1);
+      int tt = CI(ind, 2 + n_re);
+      sav_ttype[ind] = tt;
+      nu_max[p - 1] = nu_max[p - 1] + P->np_mx[tt - 1] * SVM(p, ind);
+    }
+    nu_max[p - 1] = std::min(nu_max[p - 1], P->nu_uplim[p - 1]);
+    int sum_np = np_tot[p - 1];
+    double Pmax = nu_max[p - 1] * (double)(float)P->ns_coll * P->dt;
+    if (Pmax > 1.0) return ORACLE_ERR_PMAX;
+    double dNc = sum_np * Pmax / (double)(float)1;
+    int Nc_tmp = (int)dNc;
+    double rnd = oracle_ran2(&iseed[0]);
+    if (rnd <= (dNc - Nc_tmp)) Nc_tmp = Nc_tmp + 1;
+    Nc[p] = Nc_tmp;
+    if (P->n_cell > 0 && np_tot[0] / P->n_cell >= 1 && p == 1 && Nc_tmp <= 1) return ORACLE_ERR_FEW_COLL;
+  }
+  for (int p = 1; p <= ntype; ++p) {
+    Nc_out[p - 1] = Nc[p];
+    if (T->p_ncol[p - 1] == 0 || P->mass[p - 1] <= 0 || Nc[p] == 0 || np_tot[p - 1] == 0) continue;
+    double nu_max_omp =
+        (double)((float)Nc[p] / (float)np_tot[p - 1]) / ((double)(float)P->ns_coll * P->dt);
+    double vz_sav = 0.0;
+    const int pn = T->p_ncol[p - 1];
+    for (int ic = 1; ic <= Nc[p]; ++ic) {
+      double rnd[2];
+      rnd[0] = oracle_ran2(iseed);
+      int ip = (int)(np_tot[p - 1] * rnd[0]) + 1;
+      if (ip == np_tot[p - 1] + 1) return ORACLE_ERR_BAD_PICK;
+      double *vi = vxp + ((long)(p - 1) * nmax + (ip - 1)) * 6;
+      double vx[2] = {vi[3], 0}, vy[2] = {vi[4], 0}, vz[2] = {vi[5], 0};
+      int flag_ttype[ORACLE_NPART + 1] = {0};
+      double vr[ORACLE_NPART + 1] = {0}, Ekr[ORACLE_NPART + 1] = {0}, mu[ORACLE_NPART + 1] = {0};
+      double vxc[ORACLE_NPART + 1] = {0}, vyc[ORACLE_NPART + 1] = {0}, vzc[ORACLE_NPART + 1] = {0};
+      std::vector<double> nu(pn + 1, 0.0), sort_arr(pn, 0.0);
+      double sum_nu = 0.0;
+      for (int icol = 1; icol <= pn; ++icol) {
+        int ind = SL(p, icol);
+        int tt = sav_ttype[ind];
+        if (flag_ttype[tt] == 0) {
+          if (P->charge[tt - 1] != 0.0) return ORACLE_ERR_UNSUPPORTED;
+          rnd[0] = oracle_ran2(iseed);
+          rnd[1] = oracle_ran2(iseed);
+          oracle_load_gauss(&vx[1], &vy[1], P->vt0[tt - 1], rnd, pi);
+          if (vz_sav == 0.0) {
+            rnd[0] = oracle_ran2(iseed);
+            rnd[1] = oracle_ran2(iseed);
+            oracle_load_gauss(&vz[1], &vz_sav, P->vt0[tt - 1], rnd, pi);
+          } else {
+            vz[1] = vz_sav;
+            vz_sav = 0.0;
+          }
+          mu[tt] = absm(p) * absm(tt) / (absm(p) + absm(tt));
+          vr[tt] = std::sqrt((vx[0] - vx[1]) * (vx[0] - vx[1]) + (vy[0] - vy[1]) * (vy[0] - vy[1]) +
+                             (vz[0] - vz[1]) * (vz[0] - vz[1]));
+          Ekr[tt] = (0.5 * mu[tt] * (vr[tt] * vr[tt])) / qe;
+          double sm = absm(p) + absm(tt);
+          vxc[tt] = (absm(p) * vx[0] + absm(tt) * vx[1]) / sm;
+          vyc[tt] = (absm(p) * vy[0] + absm(tt) * vy[1]) / sm;
+          vzc[tt] = (absm(p) * vz[0] + absm(tt) * vz[1]) / sm;
+          if (Ekr[tt] > T->sig_Er[T->npt - 1]) return ORACLE_ERR_EKR_TABLE;
+          flag_ttype[tt] = 1;
+        }
+        int npt = T->npt, L = 1, R = npt;
+        for (int it = 1; it <= 5; ++it) {
+          int M = (int)((double)(float)(R - L) / 2.0) + L;
+          double EL = T->sig_Er[L - 1], ER = T->sig_Er[R - 1], EM = T->sig_Er[M - 1];
+          if (Ekr[tt] >= EL && Ekr[tt] <= EM) R = M;
+          if (Ekr[tt] > EM && Ekr[tt] <= ER) L = M;
+        }
+        for (int ipt = L + 1; ipt <= R; ++ipt) {
+          double EL = T->sig_Er[ipt - 2], ER = T->sig_Er[ipt - 1];
+          if (Ekr[tt] > EL && Ekr[tt] <= ER) {
+            double sL = SIG(ipt - 1, ind), sR = SIG(ipt, ind);
+            double sig_p = sL + (Ekr[tt] - EL) * (sR - sL) / (ER - EL);
+            double np_t = P->np_mx[tt - 1];
+            nu[icol] = np_t * sig_p * vr[tt] / nu_max_omp;
+            sum_nu = sum_nu + nu[icol];
+            sort_arr[icol - 1] = nu[icol];
+            break;
+          }
+        }
+      }
+      std::vector<int> ix(pn > 0 ? pn : 1);
+      indexx(pn, sort_arr.data(), ix.data());
+      rnd[0] = oracle_ran2(iseed);
+      int c_ind = 0;
+      if (rnd[0] <= sum_nu) {
+        double s = 0.0;
+        for (int icol = 1; icol <= pn; ++icol) {
+          s = s + nu[ix[icol - 1]];
+          if (rnd[0] <= s) {
+            c_ind = SL(p, ix[icol - 1]);
+            break;
+          }
+        }
+      }
+      if (c_ind == 0) continue;
+      cnt_col[c_ind - 1] += 1;
+      int n_re = CI(c_ind, 1), n_by = CI(c_ind, 2);
+      int rt = CI(c_ind, 2 + n_re + n_by + 1);
+      int tt = sav_ttype[c_ind];
+      if (rt != 4) {
+        double Eth = T->sig_Eth[c_ind - 1];
+        double Ee = 0.5 * mu[tt] * (vr[tt] * vr[tt]) - Eth * qe;
+        if (Ee < 0.0) return ORACLE_ERR_NEG_ENERGY;
+        double sum_mass = 0.0;
+        for (int a = 1; a <= n_by; ++a) sum_mass = sum_mass + 1.0 / absm(CI(c_ind, 2 + n_re + a));
+        rnd[0] = oracle_ran2(iseed);
+        rnd[1] = oracle_ran2(iseed);
+        double th_add = 2.0 * pi / (double)(float)n_by;
+        double cos_th = 1.0 - 2.0 * rnd[0];
+        double th = std::acos(cos_th);
+        double phi = 2.0 * pi * rnd[1];
+        double cos_ph = std::cos(phi), sin_ph = std::sin(phi);
+        rnd[0] = oracle_ran2(iseed);
+        rnd[1] = oracle_ran2(iseed);
+        double cos_th_s = 1.0 - 2.0 * rnd[0];
+        double phi_s = 2.0 * pi * rnd[1];
+        int flag_add[11] = {0};
+        flag_add[1] = flag_add[2] = -1;
+        for (int a = n_re + 1; a <= n_re + n_by; ++a) flag_add[a] = 0;
+        for (int i_by = 1; i_by <= n_by; ++i_by) {
+          double cth = std::cos(th), sth = std::sin(th);
+          th = th + th_add;
+          double ex = cth, ey = sth * sin_ph, ez = sth * cos_ph;
+          double ex1 = 0, ey1 = 0, ez1 = 0;
+          oracle_scatter(&ex1, &ey1, &ez1, ex, ey, ez, cos_th_s, phi_s);
+          int bt = CI(c_ind, 2 + n_re + i_by);
+          if (P->mass[bt - 1] <= 0) continue;
+          int opt_add = 1;
+          int ib = 0;
+          if (i_by == 1 && bt == p) {
+            ib = ip;
+            opt_add = 0;
+            flag_add[1] = 0;
+          }
+          if (rt == 1 || rt == 3) {
+            if (bt == p) ib = ip;
+            if (bt == tt) return ORACLE_ERR_UNSUPPORTED;  // charged target reuse
+            opt_add = 0;
+            flag_add[1] = flag_add[2] = 0;
+          }
+          if (opt_add == 1) {
+            np_add[bt] += 1;
+            ib = np_tot[bt - 1] + np_add[bt];
+            if (ib > nmax) return ORACLE_ERR_CAPACITY;
+            double *dst = vxp + ((long)(bt - 1) * nmax + (ib - 1)) * 6;
+            dst[0] = vi[0];
+            dst[1] = vi[1];
+            dst[2] = vi[2];
+            flag_add[n_re + i_by] = 1;
+          }
+          double vp = std::sqrt(2.0 * (Ee / sum_mass) / (absm(bt) * absm(bt)));
+          double *vb = vxp + ((long)(bt - 1) * nmax + (ib - 1)) * 6;
+          vb[3] = vxc[tt] + vp * ex1;
+          vb[4] = vyc[tt] + vp * ey1;
+          vb[5] = vzc[tt] + vp * ez1;
+        }
+        for (int i_re = 1; i_re <= n_re; ++i_re) {
+          int ct = CI(c_ind, 2 + i_re);
+          if (P->mass[ct - 1] <= 0) {
+            flag_add[i_re] = 0;
+            continue;
+          }
+          if (flag_add[i_re] == -1) {
+            if (ct == p) flag_dead[(long)(ct - 1) * nmax + (ip - 1)] = 1;
+            else return ORACLE_ERR_UNSUPPORTED;
+          }
+        }
+      } else {
+        for (int i_by = 1; i_by <= n_by; ++i_by) {
+          int bt = CI(c_ind, 2 + n_re + i_by);
+          if (P->mass[bt - 1] <= 0) continue;
+          if (bt != p) return ORACLE_ERR_UNSUPPORTED;
+          // ind_ce = 1 + 1 -> 2: the incident particle takes the target's
+          // velocity (Src/collisions.f90:956-971)
+          vi[3] = vx[1];
+          vi[4] = vy[1];
+          vi[5] = vz[1];
+        }
+      }
+    }
+  }
+  for (int p = 1; p <= ntype; ++p) np_tot[p - 1] += np_add[p];
+  return ORACLE_OK;
+}
+
+int oracle_set_threads(int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  return omp_get_max_threads();
+#else
+  (void)nthreads;
+  return 1;
+#endif
+}
+
+}  // extern "C"

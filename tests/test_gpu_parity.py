@@ -1,0 +1,274 @@
+"""GPU parity tests: the C-ABI drop-ins and device API against the CPU
+oracle on the same seeded inputs.
+
+Bars (from the benchmark definition, written in each test):
+  * calc_rho, calc_Efield, one push, Poisson solve (same inputs): bit-exact
+    where the operation order is fixed, else <= 1e-12 relative;
+  * deposition: <= 1e-12 relative (atomic summation order);
+  * sort: per-cell counts (Plist) bit-exact, same particles in every cell;
+  * collisionless trajectories after 100 steps: <= 1e-10 relative;
+  * MCC: collision counts per process within 3 sigma.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from essaitemporaire_lepic_module_b200 import config, dropin
+from tests.conftest import have_gpu
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not have_gpu(), reason="needs a CUDA GPU")]
+
+
+def rel(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    den = max(np.abs(b).max(), 1e-300)
+    return np.abs(a - b).max() / den
+
+
+@pytest.fixture(scope="module")
+def box16():
+    oracle.set_threads(1)
+    st = config.build("box16")
+    S = oracle.load_part(st, nmax=st.n_particles() + 4096)
+    dropin.set_commons(st)
+    return st, S
+
+
+@pytest.fixture(scope="module")
+def mcc32():
+    oracle.set_threads(1)
+    st = config.build("mcc32")
+    S = oracle.load_part(st, nmax=int(st.n_particles() * 1.3))
+    T = st.tables
+    dropin.set_commons(st, ncol=T.sig.shape[0], npt=T.sig_Er.shape[0], p_ncol=T.p_ncol)
+    return st, S
+
+
+def solved_fields(st, S):
+    rhs = oracle.calc_rho(st, S.np.copy())
+    phi = st.geom.phi.copy()
+    oracle.pdesolver(st, phi, rhs)
+    E = oracle.calc_efield(st, phi)
+    return rhs, phi, E
+
+
+def test_calc_rho_bit_exact(box16):
+    st, S = box16
+    dropin.set_commons(st)
+    r_o = oracle.calc_rho(st, S.np.copy())
+    r_g = dropin.calc_rho(st, S.np.copy())
+    np.testing.assert_array_equal(r_g, r_o)
+
+
+@pytest.mark.parametrize("name", ["box16", "box32", "poisson32", "penning_small"])
+def test_pdesolver_matches_oracle(name):
+    """Same schedule (V-cycles, sweeps per level) and phi to <= 1e-12."""
+    st = config.build(name)
+    dropin.set_commons(st)
+    if st.rhs_blobs is not None:
+        rhs = st.rhs_blobs
+    else:
+        # electrons alone: the co-located e/ion load makes the full rho zero
+        S = oracle.load_part(st, nmax=st.n_particles() + 4096)
+        npg = S.np.copy()
+        npg[1:] = 0.0
+        rhs = oracle.calc_rho(st, npg)
+    for warm in (False, True):
+        phi_o = st.geom.phi.copy()
+        if warm:
+            oracle.pdesolver(st, phi_o, rhs, eps=1e-6)
+        phi_g = phi_o.copy()
+        ko = oracle.pdesolver(st, phi_o, rhs)
+        kg = dropin.pdesolver(st, phi_g, rhs)
+        assert kg[0] == ko[0], (kg, ko)
+        assert abs(kg[1] - ko[1]) == 0.0, (kg, ko)
+        assert rel(phi_g, phi_o) <= 1e-12
+        assert kg[2] < st.wl.eps
+
+
+def test_efield_bit_exact(box16):
+    st, S = box16
+    dropin.set_commons(st)
+    _, phi, E_o = solved_fields(st, S)
+    E_g = dropin.calc_efield(st, phi)
+    np.testing.assert_array_equal(E_g, E_o)
+
+
+@pytest.mark.parametrize("cfg", ["box16", "mcc32"])
+def test_part_mover_one_step_bit_exact(cfg, box16, mcc32):
+    st, S = box16 if cfg == "box16" else mcc32
+    dropin.set_commons(st)
+    _, _, E = solved_fields(st, S)
+    # a strong field so that some particles reach the walls in one step
+    E = E * 1e3
+    So = S.copy()
+    Sg = S.copy()
+    ng1 = st.geom.ngrid + 1
+    pm_o, pl_o = np.zeros((ng1, 2, st.ntype)), np.zeros((st.ntype, 4))
+    pm_g, pl_g = np.zeros((ng1, 2, st.ntype)), np.zeros((st.ntype, 4))
+    for p in range(1, st.ntype + 1):
+        oracle.part_mover(st, E, So, pm_o, pl_o, p)
+        dropin.part_mover(st, E, Sg.vxp, Sg.np_tot, Sg.flag_dead, pm_g, pl_g, p)
+    np.testing.assert_array_equal(Sg.np_tot, So.np_tot)
+    for p in range(st.ntype):
+        n = So.np_tot[p]
+        np.testing.assert_array_equal(Sg.vxp[p, :n], So.vxp[p, :n])
+    assert (So.np_tot < S.np_tot).any(), "test meant to exercise losses"
+    np.testing.assert_allclose(pm_g, pm_o, rtol=1e-12, atol=0)
+    np.testing.assert_allclose(pl_g, pl_o, rtol=1e-12, atol=0)
+
+
+def test_charge_deposition(box16):
+    st, S = box16
+    dropin.set_commons(st)
+    So = S.copy()
+    So.np[:] = 0
+    g = np.zeros_like(S.np)
+    for p in range(1, st.ntype + 1):
+        oracle.charge_deposition(st, So, p)
+        dropin.charge_deposition(st, S.vxp, S.np_tot, g, p)
+    assert rel(g, So.np) <= 1e-12
+    # charge conservation: sum np/kq * h^3 = N Nm (exact up to rounding)
+    vol = st.h[0] * st.h[1] * st.h[2]
+    for p in range(st.ntype):
+        tot = (g[p] / st.kq).sum() * vol
+        assert abs(tot - S.np_tot[p] * st.Nm[p]) <= 1e-12 * S.np_tot[p] * st.Nm[p]
+
+
+def test_part_sorting_counts_and_cells(mcc32):
+    st, S = mcc32
+    dropin.set_commons(st)
+    So = S.copy()
+    Sg = S.copy()
+    for p in range(1, st.ntype + 1):
+        pl_o = oracle.part_sorting(st, So, p)
+        pl_g = dropin.part_sorting(st, Sg.vxp, Sg.np_tot, p)
+        np.testing.assert_array_equal(pl_g, pl_o)
+        n = So.np_tot[p - 1]
+        a, b = So.vxp[p - 1, :n], Sg.vxp[p - 1, :n]
+        # same particles in each cell segment (order inside a cell is free)
+        starts = np.concatenate([[0], pl_o[1:]])
+        cell_of = np.searchsorted(pl_o[1:], np.arange(n), side="right")
+        ka = np.lexsort((a[:, 5], a[:, 4], a[:, 3], a[:, 2], a[:, 1], a[:, 0], cell_of))
+        kb = np.lexsort((b[:, 5], b[:, 4], b[:, 3], b[:, 2], b[:, 1], b[:, 0], cell_of))
+        np.testing.assert_array_equal(a[ka], b[kb])
+        del starts
+
+
+def test_collisions_statistics(mcc32):
+    """Counts per process agree with the oracle's (ran2, with-replacement
+    picks) within 3 sigma of the difference of two counts."""
+    st, S = mcc32
+    T = st.tables
+    dropin.set_commons(st, ncol=T.sig.shape[0], npt=T.sig_Er.shape[0], p_ncol=T.p_ncol)
+    tot_o = np.zeros(T.sig.shape[0])
+    tot_g = np.zeros(T.sig.shape[0])
+    for call in range(4):
+        So = S.copy()
+        So.iseed[0] = 1234567 + 77 * call
+        _, cnt, _ = oracle.collisions(st, So)
+        tot_o += cnt
+        tot_g += _gpu_counts(st, S, 11 + 10 * call, 987654 + call)
+    assert tot_o.sum() > 1000
+    for r in range(len(tot_o)):
+        if tot_o[r] + tot_g[r] == 0:
+            continue
+        sig = np.sqrt(tot_o[r] + tot_g[r])
+        assert abs(tot_o[r] - tot_g[r]) <= 3 * sig + 1, (r, tot_o, tot_g)
+
+
+def test_collisions_dropin(mcc32):
+    """collisions_ through the Fortran-signature entry point: one region
+    covering the box; every ionization appends one e- and one Ar+; the region
+    counter sums 1/np_tot_rg per collision (Src/collisions.f90:1005-1013)."""
+    st, S = mcc32
+    Sg = S.copy()
+    n1, n2, n3 = st.n
+    from essaitemporaire_lepic_module_b200._lib import commons
+    T = st.tables
+    dropin.set_commons(st, ncol=T.sig.shape[0], npt=T.sig_Er.shape[0], p_ncol=T.p_ncol)
+    pi_ = commons()["part_info_int"]
+    pi_.ixl_rg[0], pi_.ixr_rg[0] = 1, n1 + 1
+    pi_.iyl_rg, pi_.iyr_rg, pi_.izl_rg, pi_.izr_rg = 1, n2 + 1, 1, n3 + 1
+    red, _ = oracle.dens_red(st, S.np.copy())
+    cnt_col = np.zeros((1, 1, 65))
+    before = Sg.np_tot.copy()
+    dropin.collisions(st, 11, Sg.vxp, Sg.np_tot, Sg.flag_dead, np.array([4242], dtype=np.int32),
+                      np_red=red, n_rg=1, cnt_col=cnt_col)
+    added = Sg.np_tot - before
+    assert added[0] == added[1] and added[0] > 0
+    # unchanged particles stay bit-identical (only collided ones change)
+    n = before[0]
+    changed = np.any(Sg.vxp[0, :n] != S.vxp[0, :n], axis=1)
+    assert 0 < changed.mean() < 0.2
+    assert cnt_col[0, 0, :4].sum() > 0
+
+
+def _gpu_counts(st, S, it, seed):
+    """Collision counts per reaction from the device API (same state)."""
+    import torch
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    sim = Simulation(st, cap=S.vxp.shape[1], seed=seed)
+    sim.load_from_host(S.vxp, S.np_tot, S.np)
+    sim.it = it
+    sim.collisions()
+    torch.cuda.synchronize()
+    return sim.counts[:st.tables.sig.shape[0]].astype(float)
+
+
+def test_step_loop_trajectories_100_steps():
+    """Collisionless box: 100 device-resident steps vs 100 oracle steps in
+    the reference order; positions/velocities within 1e-10 relative."""
+    import torch
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    oracle.set_threads(1)
+    st = config.build("box16")
+    nmax = st.n_particles() + 4096
+    S = oracle.load_part(st, nmax=nmax)
+    sim = Simulation(st, cap=nmax)
+    sim.load_from_host(S.vxp, S.np_tot, S.np)
+    phi = st.geom.phi.copy()
+    Ei = np.zeros(tuple(st.geom.bcnd.shape) + (3,))
+    steps = 100
+    for it in range(1, steps + 1):
+        Ei, _, _ = oracle.step(st, S, phi, Ei, it)
+        sim.step()
+    torch.cuda.synchronize()
+    for p in range(st.ntype):
+        g = sim.sp[p].to_vxp()
+        o = S.vxp[p, :S.np_tot[p]]
+        assert g.shape == o.shape
+        ko = np.lexsort((o[:, 2], o[:, 1], o[:, 0]))
+        kg = np.lexsort((g[:, 2], g[:, 1], g[:, 0]))
+        for c in range(6):
+            assert rel(g[kg, c], o[ko, c]) <= 1e-10, (p, c, rel(g[kg, c], o[ko, c]))
+    assert rel(sim.phi.cpu().numpy(), phi) <= 1e-10
+
+
+def test_load_uniform_moments():
+    """GPU Philox loader: uniform positions, Maxwellian velocities with
+    <v_i^2> = vt0^2 / 2 (load_gauss form), co-located species."""
+    import torch
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    st = config.build("mcc32")
+    sim = Simulation(st)
+    sim.load_uniform()
+    torch.cuda.synchronize()
+    n = st.n_particles()
+    for p, s in enumerate(sim.sp):
+        assert s.n() == n
+        v = s.p[3:6, :n].cpu().numpy()
+        var = (v ** 2).mean(axis=1)
+        want = st.vt0[p] ** 2 / 2
+        assert np.all(np.abs(var / want - 1) < 6 * np.sqrt(2.0 / n)), (var / want)
+    a = sim.sp[0].p[0:3, :n]
+    b = sim.sp[1].p[0:3, :n]
+    assert torch.equal(a, b)
+    # total deposited charge = N Nm per species
+    vol = st.h[0] * st.h[1] * st.h[2]
+    kq = torch.as_tensor(st.kq, device=sim.dev)
+    for p in range(st.ntype):
+        tot = float((sim.np[p] / kq).sum()) * vol
+        assert abs(tot - n * st.Nm[p]) <= 1e-12 * n * st.Nm[p]
