@@ -205,15 +205,22 @@ def part_sorting(st, vxp, np_tot, ptype):
 
 
 def collisions(st, it, vxp, np_tot, flag_dead, iseed, np_red=None, ncol_mx=65, npt_mx=1300,
-               n_rg=0, cnt_col=None):
-    """Src/collisions.f90:1 -- in place on vxp / np_tot / flag_dead.  Returns
-    the per-species nu_max written to COMMON /part_info_dp_3/."""
+               regions=(), cnt_col=None):
+    """Src/collisions.f90:1 -- in place on vxp / np_tot / flag_dead.
+    regions: [(ixl, ixr)] x-ranges of the counting regions (n_rg of them)
+    sharing the y/z range of the whole grid, like conditions.inp's regions.
+    Returns the per-species nu_max written to COMMON /part_info_dp_3/."""
     T = st.tables
     ncol = T.sig.shape[0]
     npt = T.sig_Er.shape[0]
     set_commons(st, ncol=ncol, npt=npt, p_ncol=T.p_ncol)
     cm = commons()
-    cm["part_info_int"].n_rg = n_rg
+    n_rg = len(regions)
+    pi_ = cm["part_info_int"]
+    pi_.n_rg = n_rg
+    for g, (lo, hi) in enumerate(regions):
+        pi_.ixl_rg[g], pi_.ixr_rg[g] = int(lo), int(hi)
+    pi_.iyl_rg, pi_.iyr_rg, pi_.izl_rg, pi_.izr_rg = 1, st.n[1] + 1, 1, st.n[2] + 1
     n = _lib.np_i(st.n)
     h = np.ascontiguousarray(st.h, dtype=np.float64)
     sig = np.zeros((ncol_mx, npt_mx))

@@ -185,18 +185,12 @@ def test_collisions_dropin(mcc32):
     counter sums 1/np_tot_rg per collision (Src/collisions.f90:1005-1013)."""
     st, S = mcc32
     Sg = S.copy()
-    n1, n2, n3 = st.n
-    from essaitemporaire_lepic_module_b200._lib import commons
-    T = st.tables
-    dropin.set_commons(st, ncol=T.sig.shape[0], npt=T.sig_Er.shape[0], p_ncol=T.p_ncol)
-    pi_ = commons()["part_info_int"]
-    pi_.ixl_rg[0], pi_.ixr_rg[0] = 1, n1 + 1
-    pi_.iyl_rg, pi_.iyr_rg, pi_.izl_rg, pi_.izr_rg = 1, n2 + 1, 1, n3 + 1
+    n1 = st.n[0]
     red, _ = oracle.dens_red(st, S.np.copy())
     cnt_col = np.zeros((1, 1, 65))
     before = Sg.np_tot.copy()
     dropin.collisions(st, 11, Sg.vxp, Sg.np_tot, Sg.flag_dead, np.array([4242], dtype=np.int32),
-                      np_red=red, n_rg=1, cnt_col=cnt_col)
+                      np_red=red, regions=[(1, n1 + 1)], cnt_col=cnt_col)
     added = Sg.np_tot - before
     assert added[0] == added[1] and added[0] > 0
     # unchanged particles stay bit-identical (only collided ones change)
