@@ -184,6 +184,7 @@ const char *lepic_gpu_strerror(int code) {
     case LEPIC_ERR_ARG: return "invalid argument";
     case LEPIC_ERR_CELL: return "particle outside the grid";
     case LEPIC_ERR_NOT_CONVERGED: return "iteration cap reached";
+    case LEPIC_ERR_SCRATCH_LIMIT: return "grid too large for the static scratch of the allocation-free solve";
     default: return "unknown status";
   }
 }

@@ -426,3 +426,145 @@ int launch_pdesolver(const Dims &d, const double h[3], double *u, const double *
 }
 
 }  // namespace lepic
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the Poisson solve.
+//
+// Some callers cannot call cudaMalloc once their time loop runs: a Fortran
+// driver (or a framework such as PyTorch) that owns the device memory through
+// its own pool hands every buffer in and forbids allocations inside the loop,
+// because cudaMalloc synchronises the whole device and fails once the pool has
+// claimed the memory.  lepic_dev_pdesolver_noalloc runs the same cooperative
+// kernel as lepic_dev_pdesolver, but carves all of its scratch (the level
+// arrays e, r, bcnd and the fine residuals of levels 2..ng, the block partial
+// sums, the argument block and the outputs) out of one file-scope device array
+// of MG_NOALLOC_BYTES bytes, which every GPU that loads the library holds until
+// the process exits.  The caller still passes u, b and bcnd.
+// ---------------------------------------------------------------------------
+namespace lepic {
+namespace {
+
+constexpr size_t MG_NOALLOC_BYTES = 8u << 20;  // 8 MiB: grids up to 64^3 cells
+static __device__ __align__(256) unsigned char g_mg_noalloc_scratch[MG_NOALLOC_BYTES];
+
+constexpr int MG_NOALLOC_MAX_DEVICES = 64;
+unsigned char *g_noalloc_ptr[MG_NOALLOC_MAX_DEVICES] = {nullptr};
+
+inline size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+}  // namespace
+
+}  // namespace lepic
+
+extern "C" int lepic_dev_pdesolver_noalloc(const lepic_grid_t *g, double *u, const double *b,
+                                           int ncycl, double eps, double omega, int ng,
+                                           const lepic_phys_t *P, int *k_out, double *ktot_out,
+                                           double *res_out, void *stream) {
+  using namespace lepic;
+  if (!g || !P) return LEPIC_ERR_ARG;
+  if (P->flag_pbc || P->flag_nmn) return LEPIC_ERR_UNSUPPORTED;
+  if (ng < 1 || ng > MG_MAX) return LEPIC_ERR_ARG;
+  const int n[3] = {g->n[0], g->n[1], g->n[2]};
+  for (int a = 0; a < 3; ++a)
+    if (n[a] < 1 || n[a] % (1 << (ng - 1))) return LEPIC_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  int dev = 0;
+  LEPIC_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= MG_NOALLOC_MAX_DEVICES) return LEPIC_ERR_ARG;
+  // Set-up, once per device with that device current: the host-side name of
+  // the __device__ array is not a device address, so look the address up.
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_mg_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_mg_noalloc_scratch)");
+    g_noalloc_ptr[dev] = (unsigned char *)p;
+  }
+  unsigned char *base = g_noalloc_ptr[dev];
+  int sms = 0, occ = 0;
+  LEPIC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  LEPIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pdesolver, MG_BLOCK, 0));
+  if (occ < 1 || sms < 1) return LEPIC_ERR_CUDA;
+  const int blocks = sms * (occ < 2 ? occ : 2);
+
+  MGArgs A;
+  memset(&A, 0, sizeof(A));
+  A.ng = ng;
+  A.ncycl = ncycl;
+  A.eps = eps;
+  A.omega = omega;
+  // carve the scratch array; rf regions are recorded to be zeroed
+  size_t off = 0;
+  auto carve = [&](size_t bytes) -> unsigned char * {
+    size_t at = off;
+    off = align256(off + bytes);
+    return off <= MG_NOALLOC_BYTES ? base + at : nullptr;
+  };
+  MGArgs *dA = (MGArgs *)carve(sizeof(MGArgs));
+  A.partial = (double *)carve(sizeof(double) * blocks);
+  A.shared_d = (double *)carve(sizeof(double) * 4);
+  A.out_i = (int *)carve(sizeof(int) * (MG_MAX + 4));
+  A.out_d = (double *)carve(sizeof(double) * 2);
+  double *rf_ptr[MG_MAX + 1] = {nullptr};
+  size_t rf_bytes[MG_MAX + 1] = {0};
+  bool fits = dA && A.partial && A.shared_d && A.out_i && A.out_d;
+  for (int l = 1; l <= ng && fits; ++l) {
+    MGLev &L = A.L[l];
+    L.n1 = n[0] >> (l - 1);
+    L.n2 = n[1] >> (l - 1);
+    L.n3 = n[2] >> (l - 1);
+    L.N1 = L.n1 + 3;
+    L.N2 = L.n2 + 3;
+    L.R1 = L.n1 + 2;
+    L.R2 = L.n2 + 2;
+    double hl[3];
+    for (int q = 0; q < 3; ++q) hl[q] = g->h[q] * (double)(1 << (l - 1));
+    L.aw = P->eps0 / (hl[0] * hl[0]);
+    L.ae = L.aw;
+    L.an = P->eps0 / (hl[1] * hl[1]);
+    L.as = L.an;
+    L.at = P->eps0 / (hl[2] * hl[2]);
+    L.ab = L.at;
+    L.ac = -(L.an + L.as + L.aw + L.ae + L.at + L.ab);
+    const size_t nn = (size_t)(L.n1 + 3) * (L.n2 + 3) * (L.n3 + 3);
+    const size_t nr = (size_t)(L.n1 + 2) * (L.n2 + 2) * (L.n3 + 2);
+    if (l == 1) {
+      L.u = u;
+      L.b = const_cast<double *>(b);
+      L.bc = const_cast<int *>(g->bcnd);
+    } else {
+      L.u = (double *)carve(sizeof(double) * nn);
+      L.b = (double *)carve(sizeof(double) * nr);
+      L.bc = (int *)carve(sizeof(int) * nn);
+      fits = fits && L.u && L.b && L.bc;
+    }
+    if (l < ng) {
+      L.rf = (double *)carve(sizeof(double) * nn);
+      rf_ptr[l] = L.rf;
+      rf_bytes[l] = sizeof(double) * nn;
+      fits = fits && L.rf;
+    }
+  }
+  if (!fits) {
+    fprintf(stderr,
+            "lepic_dev_pdesolver_noalloc: a %dx%dx%d grid with %d levels needs more than the %zu "
+            "bytes of static scratch (grids up to 64^3 cells fit); use lepic_dev_pdesolver\n",
+            n[0], n[1], n[2], ng, MG_NOALLOC_BYTES);
+    return LEPIC_ERR_SCRATCH_LIMIT;
+  }
+  A.alpha = fabs((double)((n[0] + 1) * (n[1] + 1) * (n[2] + 1)) * A.L[1].ac) * 1.0;
+  // the shared array keeps the previous call's contents: clear the fine
+  // residual arrays whose ghost entries the restriction may read
+  for (int l = 1; l < ng; ++l) LEPIC_CUDA(cudaMemsetAsync(rf_ptr[l], 0, rf_bytes[l], s));
+  LEPIC_CUDA(cudaMemcpyAsync(dA, &A, sizeof(MGArgs), cudaMemcpyHostToDevice, s));
+  void *args[] = {&dA};
+  LEPIC_CUDA(cudaLaunchCooperativeKernel((void *)k_pdesolver, dim3(blocks), dim3(MG_BLOCK), args, 0, s));
+  int hi[MG_MAX + 4];
+  double hd[2];
+  LEPIC_CUDA(cudaMemcpyAsync(hi, A.out_i, sizeof(hi), cudaMemcpyDeviceToHost, s));
+  LEPIC_CUDA(cudaMemcpyAsync(hd, A.out_d, sizeof(hd), cudaMemcpyDeviceToHost, s));
+  LEPIC_CUDA(cudaStreamSynchronize(s));
+  if (k_out) *k_out = hi[0];
+  if (ktot_out) *ktot_out = hd[0];
+  if (res_out) *res_out = hd[1];
+  return hi[1];
+}

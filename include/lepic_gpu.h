@@ -45,6 +45,8 @@ extern "C" {
 #define LEPIC_ERR_ARG 21          /* invalid argument / size                     */
 #define LEPIC_ERR_CELL 22         /* particle outside the grid (device check)    */
 #define LEPIC_ERR_NOT_CONVERGED 23 /* iteration cap reached                      */
+#define LEPIC_ERR_SCRATCH_LIMIT 24 /* grid too large for the static scratch of
+                                      lepic_dev_pdesolver_noalloc               */
 
 /* ------------------------------------------------------------------------ */
 /* Fortran COMMON blocks of Src/particle_info.h:53-70 and Src/constants.h,   */
@@ -223,6 +225,24 @@ int lepic_dev_calc_efield(const lepic_grid_t *g, const double *phi, double *Ei, 
 int lepic_dev_pdesolver(const lepic_grid_t *g, double *u, const double *b, int ncycl, double eps,
                         double omega, int ng, const lepic_phys_t *P, int *k, double *ktot,
                         double *res, void *stream);
+
+/* No counterpart in the reference.  The Poisson solve of lepic_dev_pdesolver
+ * for callers that cannot call cudaMalloc inside their time loop: drivers whose
+ * device memory is owned by their own pool (a Fortran host that hands every
+ * buffer in, or a framework allocator such as PyTorch's) and that forbid
+ * allocations there, since cudaMalloc synchronises the device and fails once
+ * the pool holds the memory.  This variant allocates nothing: its scratch is
+ * one static 8 MiB device array per GPU that loads the library, held until
+ * the process exits, which fits grids up to 64^3 cells; larger grids return
+ * LEPIC_ERR_SCRATCH_LIMIT.  The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress) and should be made before any
+ * stream capture.  All calls share the array and it keeps the last call's
+ * contents (what must start at zero is cleared per call); calls that overlap
+ * on the GPU, on any stream, race.  u, b and g->bcnd are the caller's device
+ * buffers exactly as for lepic_dev_pdesolver. */
+int lepic_dev_pdesolver_noalloc(const lepic_grid_t *g, double *u, const double *b, int ncycl,
+                                double eps, double omega, int ng, const lepic_phys_t *P, int *k,
+                                double *ktot, double *res, void *stream);
 
 /* Src/part_expmover.f90:1-482 for one species: push + loss + in-order
  * compaction.  Ei device (3,(n+3)^3).  p_mac: host (ntype,2,0:ngrid),
