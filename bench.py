@@ -152,7 +152,7 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     st = config.build(args.workload)
-    sim = Simulation(st, seed=20240601 + 7919 * rank)
+    sim = Simulation(st, seed=20240601 + 7919 * rank, nsort=args.nsort, fused=not args.unfused)
     sim.load_uniform()
     torch.cuda.synchronize()
     n_start = int(sim.counts_host().sum())
@@ -170,10 +170,12 @@ def run_ours(args):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     nps = 0
+    vcycles = []
     e0.record()
     for _ in range(args.steps):
         nps += int(sum(s.n() for s in sim.sp))
         sim.step()
+        vcycles.append(sim.mg_last[0] - 1)
     e1.record()
     torch.cuda.synchronize()
     clocks = clk.stop()
@@ -191,7 +193,8 @@ def run_ours(args):
 
     # --------------------------------------------------------- roofline
     peak, peak_kind = measured_peaks()
-    push = timers.get("push_f64", (0.0, 0))
+    kname = "push_deposit_f64" if "push_deposit_f64" in timers else "push_f64"
+    push = timers.get(kname, (0.0, 0))
     top = max(timers.items(), key=lambda kv: kv[1][0]) if timers else ("push_f64", push)
     per_launch_particles = nps / max(push[1], 1)
     bytes_per_launch = 96.0 * per_launch_particles
@@ -232,10 +235,11 @@ def run_ours(args):
                    "mcc": "Ar 1 Pa 300 K, every 10 steps", "sort_every": sim.nsort,
                    "l2": "inputs larger than L2 (12.9 GB particle state)",
                    "particles_at_start": n_start},
+        "mg_vcycles_per_solve": float(np.mean(vcycles)) if vcycles else None,
         "gpu_launches": int(sum(v[1] for v in timers.values())),
         "kernel_ms": {k: round(v[0], 3) for k, v in sorted(timers.items())},
         "kernel_launches": {k: v[1] for k, v in sorted(timers.items())},
-        "roofline": {"bound": "hbm", "kernel": "push_f64", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": None,
                      "algorithmic_bytes_per_launch": bytes_per_launch,
@@ -266,6 +270,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--cpu-ppc", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--nsort", type=int, default=None, help="sort cadence (default: the reference's 10)")
+    ap.add_argument("--unfused", action="store_true", help="separate push/compact/deposit kernels")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

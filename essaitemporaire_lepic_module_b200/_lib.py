@@ -120,6 +120,8 @@ def lib():
                                          C.POINTER(LepicPhys), P_int, P_dbl, P_dbl, vp], _I),
         "lepic_dev_part_mover": ([C.POINTER(LepicGrid), vp, C.POINTER(LepicSpeciesF64), _I, _I, _I,
                                   C.POINTER(LepicPhys), P_dbl, P_dbl, vp], _I),
+        "lepic_dev_push_deposit": ([C.POINTER(LepicGrid), vp, C.POINTER(LepicSpeciesF64), _I, _I,
+                                    C.POINTER(LepicPhys), vp, vp, _I, vp], _I),
         "lepic_dev_charge_deposition": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64), _I,
                                          C.POINTER(LepicPhys), vp, vp], _I),
         "lepic_dev_part_sorting": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64), vp, _I, vp], _I),
@@ -172,7 +174,7 @@ def exported_symbols():
     return ["lepic_gpu_last_error", "lepic_gpu_strerror", "lepic_build_info", "lepic_dev_info",
             "lepic_dev_calc_rho", "lepic_dev_calc_efield", "lepic_dev_pdesolver",
             "lepic_dev_pdesolver_noalloc",
-            "lepic_dev_part_mover", "lepic_dev_charge_deposition", "lepic_dev_part_sorting",
+            "lepic_dev_part_mover", "lepic_dev_push_deposit", "lepic_dev_charge_deposition", "lepic_dev_part_sorting",
             "lepic_dev_collisions", "lepic_dev_load_uniform", "lepic_dev_cell_wall",
             "lepic_dev_dens_red", "lepic_timing_enable", "lepic_timing_reset", "lepic_timing_read",
             "calc_rho_", "dens_red_", "pdesolver_", "calc_efield_",

@@ -193,29 +193,70 @@ __global__ void __launch_bounds__(PB) k_deposit_f64(Dims d, double h0, double h1
   atomicAdd(&np[q + sy + sz], kq[q + sy + sz] * (k1 * px * (1.0 - py) * (1.0 - pz)));
 }
 
-// cell key ic = (ix-1) + n1((iy-1) + n2(iz-1)) + 1 and its histogram
+__device__ __forceinline__ unsigned lane_le() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_le;" : "=r"(m));
+  return m;
+}
+
+// Runs of equal keys in consecutive lanes (particles are nearly sorted, so a
+// warp usually holds one or two cells): head lane, run start and length.
+struct Run {
+  bool head;
+  int start, len;
+};
+__device__ __forceinline__ Run lane_run(int key) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  int prev = __shfl_up_sync(full, key, 1);
+  Run r;
+  r.head = (lane == 0) || (prev != key);
+  unsigned heads = __ballot_sync(full, r.head);
+  r.start = 31 - __clz(heads & lane_le());
+  // next head above the run start (none: the run ends at lane 31)
+  unsigned above = (r.start == 31) ? 0u : (heads & ~((2u << r.start) - 1u));
+  r.len = (above ? __ffs(above) - 1 : 32) - r.start;
+  return r;
+}
+
+// cell key ic = (ix-1) + n1((iy-1) + n2(iz-1)) + 1 and its histogram, one
+// atomic per run of equal keys in a warp
 __global__ void k_sort_keys(Dims d, double h0, double h1, double h2, const double *__restrict__ p,
                             long long cap, const int *__restrict__ count, int *key, int *cnt,
                             int pl_max, int *err) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= *count) return;
-  int ix = (int)(p[i] / h0) + 1, iy = (int)(p[cap + i] / h1) + 1, iz = (int)(p[2 * cap + i] / h2) + 1;
-  int ic = (ix - 1) + d.n1 * ((iy - 1) + d.n2 * (iz - 1)) + 1;
-  if (ic < 1 || ic > pl_max) {
-    raise_err(err, LEPIC_ERR_CELL, (int)i);
-    ic = pl_max;
+  const int N = *count;
+  int ic = -1;
+  if (i < N) {
+    int ix = (int)(p[i] / h0) + 1, iy = (int)(p[cap + i] / h1) + 1, iz = (int)(p[2 * cap + i] / h2) + 1;
+    ic = (ix - 1) + d.n1 * ((iy - 1) + d.n2 * (iz - 1)) + 1;
+    if (ic < 1 || ic > pl_max) {
+      raise_err(err, LEPIC_ERR_CELL, (int)i);
+      ic = pl_max;
+    }
+    key[i] = ic;
   }
-  key[i] = ic;
-  atomicAdd(&cnt[ic], 1);
+  Run r = lane_run(ic);
+  if (r.head && ic >= 0) atomicAdd(&cnt[ic], r.len);
 }
 
+// scatter to cursor[key]: the run head reserves len slots, lanes take them in
+// lane order
 __global__ void k_sort_scatter(const double *__restrict__ p, double *__restrict__ q, long long cap,
                                const int *__restrict__ count, const int *__restrict__ key, int *cursor) {
+  const unsigned full = 0xffffffffu;
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= *count) return;
-  int j = atomicAdd(&cursor[key[i]], 1);
+  const int N = *count;
+  const int k = (i < N) ? key[i] : -1;
+  Run r = lane_run(k);
+  int base = 0;
+  if (r.head && k >= 0) base = atomicAdd(&cursor[k], r.len);
+  base = __shfl_sync(full, base, r.start);
+  if (i < N) {
+    const long long j = base + ((threadIdx.x & 31) - r.start);
 #pragma unroll
-  for (int c = 0; c < 6; ++c) q[c * cap + j] = p[c * cap + i];
+    for (int c = 0; c < 6; ++c) q[c * cap + j] = p[c * cap + i];
+  }
 }
 
 // ---------------------------------------------------------------- scan

@@ -66,8 +66,11 @@ class Species:
 
 
 class Simulation:
-    def __init__(self, st, cap=None, device="cuda", seed=123456, nsort=None, ns_coll=None):
+    def __init__(self, st, cap=None, device="cuda", seed=123456, nsort=None, ns_coll=None,
+                 fused=True):
         self.st = st
+        self.fused = fused
+        self._acc = None
         self.dev = torch.device(device)
         self.stream = torch.cuda.current_stream(self.dev)
         self.nsort = st.wl.nsort if nsort is None else nsort
@@ -221,6 +224,38 @@ class Simulation:
                                                     C.byref(self.P), C.c_void_p(self.np[p].data_ptr()),
                                                     self._s()), "charge_deposition")
 
+    def move_deposit(self):
+        """Fused in-place push + deposition of every species (the step path);
+        lost particles are removed by hole filling."""
+        st = self.st
+        if self._acc is None:
+            self._acc = torch.zeros((st.ntype, 2 + 2 * (st.geom.ngrid + 1)), dtype=torch.float64,
+                                    device=self.dev)
+        counts = torch.cat([s.count for s in self.sp]).cpu().numpy()
+        self.np.zero_()
+        for p, s in enumerate(self.sp):
+            if st.charge[p] == 0.0:
+                continue
+            check(lib().lepic_dev_push_deposit(C.byref(self.grid), _ptr(self.Ei), C.byref(s.s), p + 1,
+                                               st.geom.ngrid, C.byref(self.P),
+                                               C.c_void_p(self.np[p].data_ptr()),
+                                               C.c_void_p(self._acc[p].data_ptr()), int(counts[p]),
+                                               self._s()), "push_deposit")
+
+    def loss_stats(self):
+        """(p_mac (ngrid+1, 2, ntype), P_loss (ntype, 4)) accumulated so far."""
+        pm = self.p_mac.copy()
+        pl = self.P_loss.copy()
+        if self._acc is not None:
+            a = self._acc.cpu().numpy()
+            ng1 = self.st.geom.ngrid + 1
+            for p in range(self.st.ntype):
+                pl[p, 0] += a[p, 0]
+                pl[p, 2] += a[p, 1]
+                pm[:, 0, p] += a[p, 2:2 + 2 * ng1:2]
+                pm[:, 1, p] += a[p, 3:3 + 2 * ng1:2]
+        return pm, pl
+
     def step(self):
         """One timestep in the reference's order (Src/main.f90:853-1277)."""
         self.it += 1
@@ -232,8 +267,11 @@ class Simulation:
             self.sort()
         if self._tables is not None and it > 1 and it % self.ns_coll == 1 % self.ns_coll:
             self.collisions()
-        self.move()
-        self.deposit()
+        if self.fused:
+            self.move_deposit()
+        else:
+            self.move()
+            self.deposit()
 
     def counts_host(self):
         return np.array([s.n() for s in self.sp])

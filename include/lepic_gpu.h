@@ -251,6 +251,18 @@ int lepic_dev_part_mover(const lepic_grid_t *g, const double *Ei, lepic_species_
                          int ptype, int ntype, int ngrid, const lepic_phys_t *P, double *p_mac,
                          double *P_loss, void *stream);
 
+/* Src/part_expmover.f90:55-272 (gather, Boris, loss test of part_mover)
+ * fused with Src/part_expmover.f90:591-656 (CIC deposition of the new
+ * position) for one species, in place, for the device-resident step loop.
+ * Lost and killed particles are removed by moving tail particles into their
+ * slots (order not kept; the periodic sort restores cell order).  np: device
+ * grid of this species (accumulated); acc: device doubles [2 + 2(ngrid+1)]
+ * accumulating P_loss(1), P_loss(3) and p_mac(count, energy) per wall label.
+ * n_hint: an upper bound of the species' count (grid size), <= 0 = capacity. */
+int lepic_dev_push_deposit(const lepic_grid_t *g, const double *Ei, lepic_species_f64_t *s,
+                           int ptype, int ngrid, const lepic_phys_t *P, double *np, double *acc,
+                           int n_hint, void *stream);
+
 /* Src/part_expmover.f90:570-686 for one species, accumulating into np
  * (device grid of that species). */
 int lepic_dev_charge_deposition(const lepic_grid_t *g, const lepic_species_f64_t *s, int ptype,

@@ -212,16 +212,19 @@ def _gpu_counts(st, S, it, seed):
     return sim.counts[:st.tables.sig.shape[0]].astype(float)
 
 
-def test_step_loop_trajectories_100_steps():
+@pytest.mark.parametrize("fused", [True, False])
+def test_step_loop_trajectories_100_steps(fused):
     """Collisionless box: 100 device-resident steps vs 100 oracle steps in
-    the reference order; positions/velocities within 1e-10 relative."""
+    the reference order; positions/velocities within 1e-10 relative.
+    fused: in-place push + deposition with hole filling (the step path), else
+    the drop-in kernels (push, in-order compaction, deposition)."""
     import torch
     from essaitemporaire_lepic_module_b200.sim import Simulation
     oracle.set_threads(1)
     st = config.build("box16")
     nmax = st.n_particles() + 4096
     S = oracle.load_part(st, nmax=nmax)
-    sim = Simulation(st, cap=nmax)
+    sim = Simulation(st, cap=nmax, fused=fused)
     sim.load_from_host(S.vxp, S.np_tot, S.np)
     phi = st.geom.phi.copy()
     Ei = np.zeros(tuple(st.geom.bcnd.shape) + (3,))
@@ -239,6 +242,17 @@ def test_step_loop_trajectories_100_steps():
         for c in range(6):
             assert rel(g[kg, c], o[ko, c]) <= 1e-10, (p, c, rel(g[kg, c], o[ko, c]))
     assert rel(sim.phi.cpu().numpy(), phi) <= 1e-10
+    # charge conservation of the deposit: sum np/kq h^3 = N Nm per species
+    vol = st.h[0] * st.h[1] * st.h[2]
+    kq = torch.as_tensor(st.kq, device=sim.dev)
+    for p in range(st.ntype):
+        tot = float((sim.np[p] / kq).sum()) * vol
+        want = sim.sp[p].n() * st.Nm[p]
+        assert abs(tot - want) <= 1e-12 * want
+    # wall losses agree with the oracle's count of lost particles
+    pm, _ = sim.loss_stats()
+    assert np.allclose(pm[:, 0, :].sum(axis=0), S.np_tot * 0 + (np.array(
+        [st.n_particles()] * st.ntype) - S.np_tot))
 
 
 def test_load_uniform_moments():
