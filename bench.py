@@ -9,14 +9,19 @@ synthetic (seeded Philox loader on the device, analytic cross sections).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-value:  device-resident steps, CUDA events around exactly K steps, max
-        over ranks.  Particle arrays (2 x 6.4 GB FP64 SoA plus sort buffers)
-        are far larger than L2, so no flush is needed.
+value:  the mixed form (int32 cell + FP32 particles, FP32 V-cycles in FP64
+        refinement): device-resident steps, CUDA events around exactly K
+        steps, max over ranks.  The FP64 form is timed the same way first and
+        reported under "f64" with the ratio "mixed_over_f64"; phi_err_vs_f64
+        compares the last mixed solve with an FP64 solve of the same rhs.
+        Particle arrays (>= 7.5 GB) are far larger than L2, so no flush is
+        needed.
 e2e:    the same steps through the public host API: every step copies the
         host-owned wall potentials (pinned) in and the potential grid and
         particle counts out.
-roofline: the dominant kernel's algorithmic bytes (96 B per FP64
-        particle-step: read and write x,y,z,vx,vy,vz) over its average
+roofline: the dominant kernel's algorithmic bytes (mixed: 57 B per
+        particle-step = read and write cell + 6 FP32 planes, read the flag;
+        FP64: 96 B = read and write x,y,z,vx,vy,vz) over its average
         event-timed duration, against the measured HBM copy bandwidth.
 cpu_baseline: the FP64 CPU oracle (the reference restated in C++) on the
         host cores, on a bounded sample of the same workload.
@@ -37,7 +42,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "particle-steps/s (PIC-MCC timestep, FP64 form)"
+METRIC = "particle-steps/s (PIC-MCC timestep), mixed form vs FP64 form"
 UNIT = "particle-steps/s"
 
 
@@ -138,33 +143,8 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args):
-    import torch
-    import torch.distributed as dist
-    from essaitemporaire_lepic_module_b200 import _lib, config
-    from essaitemporaire_lepic_module_b200.sim import Simulation
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    st = config.build(args.workload)
-    sim = Simulation(st, seed=20240601 + 7919 * rank, nsort=args.nsort, fused=not args.unfused)
-    sim.load_uniform()
-    torch.cuda.synchronize()
-    n_start = int(sim.counts_host().sum())
-    for _ in range(args.warmup):
-        sim.step()
-    torch.cuda.synchronize()
-
-    # ------------------------------------------------------------ value
-    _lib.timing(enable=True)
-    _lib.timing(reset=True)
-    clk = ClockSampler(local)
-    clk.start()
+def _timed_steps(sim, steps, world, dist, torch):
+    """Exactly `steps` steps between CUDA events (device time, max over ranks)."""
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -172,13 +152,12 @@ def run_ours(args):
     nps = 0
     vcycles = []
     e0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         nps += int(sum(s.n() for s in sim.sp))
         sim.step()
-        vcycles.append(sim.mg_last[0] - 1)
+        vcycles.append(sim.mg_last[0])
     e1.record()
     torch.cuda.synchronize()
-    clocks = clk.stop()
     ms = e0.elapsed_time(e1)
     if world > 1:
         t = torch.tensor([ms], device="cuda")
@@ -187,21 +166,13 @@ def run_ours(args):
         c = torch.tensor([nps], device="cuda", dtype=torch.float64)
         dist.all_reduce(c)
         nps = float(c.item())
-    timers = _lib.timing()
-    _lib.timing(enable=False)
-    value = nps / (ms / 1e3)
+    return nps, ms, vcycles
 
-    # --------------------------------------------------------- roofline
-    peak, peak_kind = measured_peaks()
-    kname = "push_deposit_f64" if "push_deposit_f64" in timers else "push_f64"
-    push = timers.get(kname, (0.0, 0))
-    top = max(timers.items(), key=lambda kv: kv[1][0]) if timers else ("push_f64", push)
-    per_launch_particles = nps / max(push[1], 1)
-    bytes_per_launch = 96.0 * per_launch_particles
-    achieved = bytes_per_launch / (push[0] / max(push[1], 1) / 1e3) / 1e9 if push[1] else None
 
-    # ------------------------------------------------------------- e2e
-    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+def _e2e(sim, st, steps, world, dist, torch):
+    """Steps through the public API with host buffers: the host-owned wall
+    potentials (pinned) go in and the potential grid and the particle counts
+    come out every step, inside the timed region."""
     phi_host = torch.empty(tuple(st.geom.phi.shape), dtype=torch.float64).pin_memory()
     phi_host.copy_(torch.as_tensor(st.geom.phi))
     wall = torch.as_tensor(st.geom.bcnd >= 1, device=sim.dev)
@@ -211,44 +182,144 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+    nps = 0
+    for _ in range(steps):
         dphi = phi_host.to(sim.dev, non_blocking=True)
         sim.phi[wall] = dphi[wall]
         sim.step()
         out_phi.copy_(sim.phi, non_blocking=True)
         out_cnt.copy_(torch.cat([s.count for s in sim.sp]), non_blocking=True)
         torch.cuda.synchronize()
+        nps += int(out_cnt.sum())
     e2e_s = time.perf_counter() - t0
-    n_now = int(out_cnt.sum())
-    e2e_val = n_now * e2e_steps / e2e_s * (world if world > 1 else 1)
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+        c = torch.tensor([nps], device="cuda", dtype=torch.float64)
+        dist.all_reduce(c)
+        nps = float(c.item())
+    return {"value": nps / e2e_s, "unit": UNIT, "steps": steps,
+            "h2d_bytes_per_step": int(phi_host.numel() * 8),
+            "d2h_bytes_per_step": int(out_phi.numel() * 8 + out_cnt.numel() * 4)}
 
+
+def _roofline(timers, kname, bytes_per_particle, nps):
+    peak, peak_kind = measured_peaks()
+    push = timers.get(kname, (0.0, 0))
+    top = max(timers.items(), key=lambda kv: kv[1][0]) if timers else (kname, push)
+    per_launch_particles = nps / max(push[1], 1)
+    bytes_per_launch = bytes_per_particle * per_launch_particles
+    achieved = bytes_per_launch / (push[0] / max(push[1], 1) / 1e3) / 1e9 if push[1] else None
+    return {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+            "traffic": None, "algorithmic_bytes_per_launch": bytes_per_launch,
+            "algorithmic_bytes_per_particle": bytes_per_particle, "top_kernel": top[0]}
+
+
+def _run_form(args, st, precision, rank, world, dist, torch, e2e=True):
+    from essaitemporaire_lepic_module_b200 import _lib
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    sim = Simulation(st, seed=20240601 + 7919 * rank, nsort=args.nsort, fused=not args.unfused,
+                     precision=precision)
+    sim.load_uniform()
+    torch.cuda.synchronize()
+    n_start = int(sim.counts_host().sum())
+    for _ in range(args.warmup):
+        sim.step()
+    torch.cuda.synchronize()
+    _lib.timing(enable=True)
+    _lib.timing(reset=True)
+    clk = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clk.start()
+    nps, ms, iters = _timed_steps(sim, args.steps, world, dist, torch)
+    clocks = clk.stop()
+    timers = _lib.timing()
+    _lib.timing(enable=False)
+    out = {"sim": sim, "nps": nps, "ms": ms, "iters": iters, "timers": timers, "clocks": clocks,
+           "n_start": n_start, "value": nps / (ms / 1e3)}
+    if e2e:
+        out["e2e"] = _e2e(sim, st, max(1, min(args.steps, args.e2e_steps)), world, dist, torch)
+    return out
+
+
+def _phi_err(sim, st, torch):
+    """phi of the last mixed step (FP32 V-cycles in FP64 refinement, warm
+    start) against a cold-start FP64 multigrid solve of the same
+    right-hand side to the same tolerance: max |dphi| / max |phi|."""
+    import ctypes as C
+    from essaitemporaire_lepic_module_b200._lib import check, lib
+    phi64 = torch.as_tensor(st.geom.phi, device=sim.dev).clone()
+    k, kt, res = C.c_int(0), C.c_double(0), C.c_double(0)
+    wl = st.wl
+    check(lib().lepic_dev_pdesolver(C.byref(sim.grid), C.c_void_p(phi64.data_ptr()),
+                                    C.c_void_p(sim.rhs.data_ptr()), wl.ncycl, wl.eps, wl.omega, st.ng,
+                                    C.byref(sim.P), C.byref(k), C.byref(kt), C.byref(res), sim._s()),
+          "pdesolver")
+    torch.cuda.synchronize()
+    return float((sim.phi - phi64).abs().max() / phi64.abs().max())
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from essaitemporaire_lepic_module_b200 import config
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    st = config.build(args.workload)
+    forms = ["f64", "mixed"] if args.precision == "both" else [args.precision]
+    res = {}
+    for f in forms:
+        res[f] = _run_form(args, st, f, rank, world, dist, torch, e2e=(f == forms[-1]) or args.e2e_all)
+        if f != forms[-1]:
+            del res[f]["sim"]
+            torch.cuda.empty_cache()
+    head = forms[-1]
+    R = res[head]
+    phi_err = _phi_err(R["sim"], st, torch) if head == "mixed" else None
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
         return
+    kname = "push_deposit_mixed" if head == "mixed" else (
+        "push_deposit_f64" if "push_deposit_f64" in R["timers"] else "push_f64")
+    bpp = 57.0 if head == "mixed" else 96.0
+    timers = R["timers"]
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "grid": list(st.n), "species": st.ntype,
+        "metric": METRIC, "value": R["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": R["ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 particles + f64 grids" if head == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "form": head, "grid": list(st.n), "species": st.ntype,
                    "particles_per_species": st.n_particles(), "Bz_T": st.Bconst[2],
-                   "mcc": "Ar 1 Pa 300 K, every 10 steps", "sort_every": sim.nsort,
-                   "l2": "inputs larger than L2 (12.9 GB particle state)",
-                   "particles_at_start": n_start},
-        "mg_vcycles_per_solve": float(np.mean(vcycles)) if vcycles else None,
+                   "mcc": "Ar 1 Pa 300 K, every 10 steps", "sort_every": R["sim"].nsort,
+                   "l2": "inputs larger than L2 (>= 7.5 GB particle state)",
+                   "particles_at_start": R["n_start"]},
+        "phi_err_vs_f64": phi_err,
+        "poisson_iters_per_solve": float(np.mean(R["iters"])) if R["iters"] else None,
         "gpu_launches": int(sum(v[1] for v in timers.values())),
         "kernel_ms": {k: round(v[0], 3) for k, v in sorted(timers.items())},
         "kernel_launches": {k: v[1] for k, v in sorted(timers.items())},
-        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
-                     "algorithmic_bytes_per_launch": bytes_per_launch,
-                     "top_kernel": top[0]},
-        "e2e": {"value": e2e_val, "unit": UNIT, "steps": e2e_steps,
-                "h2d_bytes_per_step": int(phi_host.numel() * 8),
-                "d2h_bytes_per_step": int(out_phi.numel() * 8 + out_cnt.numel() * 4)},
-        "clocks": clocks,
+        "roofline": _roofline(timers, kname, bpp, R["nps"]),
+        "e2e": R["e2e"],
+        "clocks": R["clocks"],
     }
+    if "f64" in res and head != "f64":
+        F = res["f64"]
+        fk = "push_deposit_f64" if "push_deposit_f64" in F["timers"] else "push_f64"
+        line["f64"] = {"value": F["value"], "ms_per_step": F["ms"] / args.steps,
+                       "poisson_vcycles_per_solve": float(np.mean(F["iters"])) if F["iters"] else None,
+                       "kernel_ms": {k: round(v[0], 3) for k, v in sorted(F["timers"].items())},
+                       "roofline": _roofline(F["timers"], fk, 96.0, F["nps"]), "clocks": F["clocks"]}
+        if "e2e" in F:
+            line["f64"]["e2e"] = F["e2e"]
+        line["mixed_over_f64"] = R["value"] / F["value"]
     if args.cpu_baseline and world == 1:
         try:
             line["cpu_baseline"] = cpu_baseline(args.workload, steps=args.cpu_steps, ppc=args.cpu_ppc)
@@ -271,7 +342,10 @@ def main():
     ap.add_argument("--cpu-ppc", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--nsort", type=int, default=None, help="sort cadence (default: the reference's 10)")
-    ap.add_argument("--unfused", action="store_true", help="separate push/compact/deposit kernels")
+    ap.add_argument("--unfused", action="store_true", help="FP64: separate push/compact/deposit kernels")
+    ap.add_argument("--precision", default="both", choices=["both", "mixed", "f64"],
+                    help="both: time the FP64 form, then the mixed form (the headline)")
+    ap.add_argument("--e2e-all", action="store_true", help="also measure e2e for the FP64 form")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -46,6 +46,12 @@ class LepicSpeciesF64(C.Structure):
                 ("key", C.c_void_p), ("flag_dead", C.c_void_p), ("cap", C.c_int)]
 
 
+class LepicSpeciesMixed(C.Structure):
+    _fields_ = [("cell", C.c_void_p), ("p", C.c_void_p), ("cell_alt", C.c_void_p),
+                ("p_alt", C.c_void_p), ("count", C.c_void_p), ("flag_dead", C.c_void_p),
+                ("tile_off", C.c_void_p), ("cap", C.c_int)]
+
+
 class LepicTables(C.Structure):
     _fields_ = [("ncol", C.c_int), ("npt", C.c_int), ("npt_mx", C.c_int),
                 ("sig_Er", C.c_void_p), ("sig", C.c_void_p), ("sig_Eth", C.c_void_p),
@@ -128,6 +134,19 @@ def lib():
         "lepic_dev_collisions": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64), _I,
                                   C.POINTER(LepicTables), C.POINTER(LepicPhys), C.c_ulonglong,
                                   C.c_ulonglong, P_dbl, C.POINTER(C.c_longlong), vp], _I),
+        "lepic_dev_push_deposit_mixed": ([C.POINTER(LepicGrid), vp, C.POINTER(LepicSpeciesMixed), _I,
+                                          _I, C.POINTER(LepicPhys), vp, vp, _I, vp], _I),
+        "lepic_dev_sort_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), _I, vp], _I),
+        "lepic_dev_pack_e32": ([vp, vp, C.c_longlong, vp], _I),
+        "lepic_dev_f64_to_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64),
+                                    C.POINTER(LepicSpeciesMixed), C.c_longlong, vp], _I),
+        "lepic_dev_mixed_to_f64": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), vp,
+                                    C.c_longlong, C.c_longlong, vp], _I),
+        "lepic_dev_pdesolver_mixed": ([C.POINTER(LepicGrid), vp, vp, _D, _D, _I, C.POINTER(LepicPhys),
+                                       _I, _I, _I, _I, P_int, P_dbl, vp], _I),
+        "lepic_dev_collisions_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), _I,
+                                        C.POINTER(LepicTables), C.POINTER(LepicPhys), C.c_ulonglong,
+                                        C.c_ulonglong, P_dbl, C.POINTER(C.c_longlong), vp], _I),
         "lepic_dev_load_uniform": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64), _I,
                                     C.c_longlong, C.POINTER(LepicPhys), C.c_ulonglong, vp], _I),
         "lepic_dev_cell_wall": ([P_int, vp, vp, vp], _I),
@@ -175,7 +194,9 @@ def exported_symbols():
             "lepic_dev_calc_rho", "lepic_dev_calc_efield", "lepic_dev_pdesolver",
             "lepic_dev_pdesolver_noalloc",
             "lepic_dev_part_mover", "lepic_dev_push_deposit", "lepic_dev_charge_deposition", "lepic_dev_part_sorting",
-            "lepic_dev_collisions", "lepic_dev_load_uniform", "lepic_dev_cell_wall",
+            "lepic_dev_collisions", "lepic_dev_push_deposit_mixed", "lepic_dev_sort_mixed",
+            "lepic_dev_pack_e32", "lepic_dev_f64_to_mixed", "lepic_dev_mixed_to_f64",
+            "lepic_dev_pdesolver_mixed", "lepic_dev_collisions_mixed", "lepic_dev_load_uniform", "lepic_dev_cell_wall",
             "lepic_dev_dens_red", "lepic_timing_enable", "lepic_timing_reset", "lepic_timing_read",
             "calc_rho_", "dens_red_", "pdesolver_", "calc_efield_",
             "part_mover_", "charge_deposition_", "part_sorting_", "collisions_",

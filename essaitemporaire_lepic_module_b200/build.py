@@ -19,7 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "liblepic_gpu.so")
-SOURCES = ["context.cu", "timing.cu", "fields.cu", "mg.cu", "particles.cu", "step.cu", "mcc.cu", "capi.cu"]
+SOURCES = ["context.cu", "timing.cu", "fields.cu", "mg.cu", "particles.cu", "step.cu", "mcc.cu", "mixed.cu", "mgmixed.cu",
+           "capi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=default", "--expt-relaxed-constexpr"]

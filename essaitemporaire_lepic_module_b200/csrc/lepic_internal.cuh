@@ -121,6 +121,19 @@ int launch_collisions(const lepic_grid_t &g, lepic_species_f64_t *sp, int ntype,
                       const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
                       unsigned long long call_index, double *nu_max, long long *counts,
                       cudaStream_t s, const RegionCount *rg = nullptr);
+int launch_collisions_mixed(const lepic_grid_t &g, lepic_species_mixed_t *sp, int ntype,
+                            const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
+                            unsigned long long call_index, double *nu_max, long long *counts,
+                            cudaStream_t s);
+// mixed.cu
+int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E32, lepic_species_mixed_t &sp,
+                              int ptype, int ngrid, const lepic_phys_t &P, double *np, double *acc,
+                              int n_hint, cudaStream_t s);
+int launch_sort_mixed(const lepic_grid_t &g, lepic_species_mixed_t &sp, int n_hint, cudaStream_t s);
+// mgmixed.cu
+int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const double *b, const int *bcnd,
+                           double eps, double omega, int ng, double eps0, int max_refine, int nu_pre,
+                           int nu_post, int coarse_sweeps, int *iters, double *res_out, cudaStream_t s);
 
 }  // namespace lepic
 

@@ -6,14 +6,19 @@
 // with probability Pmax = nu_max * ns_coll * dt from a Philox4x32-10 counter
 // keyed by (seed, call, species, particle, sub-stream): the expected number
 // of collisions of each process, nu_r * ns_coll * dt per particle, is the
-// same, and no two threads ever touch the same particle.  The physics of a
-// selected collision follows Src/collisions.f90:437-998 step for step:
-// Maxwellian neutral target (load_gauss form), relative energy in the
-// centre-of-mass frame, linear interpolation of sigma on the merged energy
-// grid, elastic / excitation scattering, ionization with equal-momentum
-// byproducts on equally spaced angles rotated by `scatter`, and charge
-// exchange by velocity swap.  Ionization products are appended at the end of
-// their species' arrays (warp-aggregated atomic slot reservation).
+// same, and no two threads ever touch the same particle.
+//
+// Two passes: k_mcc_select streams the particle indices through the Philox
+// test (no particle data is read) and appends the candidates (a fraction
+// Pmax) to a list; k_mcc_collide then runs the collision physics densely on
+// the candidates only.  The physics follows Src/collisions.f90:437-998 step
+// for step: Maxwellian neutral target (load_gauss form), relative energy in
+// the centre-of-mass frame, linear interpolation of sigma on the merged
+// energy grid, elastic / excitation scattering, ionization with
+// equal-momentum byproducts on equally spaced angles rotated by `scatter`,
+// and charge exchange by velocity swap.  Ionization products are appended at
+// the end of their species' arrays.  The kernels are templated on the
+// particle layout (FP64 SoA or mixed cell + FP32 offsets).
 #include <vector>
 
 #include "lepic_internal.cuh"
@@ -34,17 +39,92 @@ struct MCCConst {
   int tt[MAXR];                 // target species (1-based)
   int rt[MAXR], n_by[MAXR], n_re[MAXR];
   int by[MAXR][MAXBY];
-  int re[MAXR][2];
   double Eth[MAXR], np_t[MAXR];
   double mass[LEPIC_NPART];     // signed masses
   double vt0[LEPIC_NPART];
   int npt, npt_mx;
   unsigned int k0, k1, c2, c3;  // Philox key and counter words
   // region counters of Src/collisions.f90:1005-1013 (drop-in path only)
-  int n_rg, ncol_mx, n1, n2;
+  int n_rg, ncol_mx;
   int ixl[LEPIC_NM_RG], ixr[LEPIC_NM_RG], iyl, iyr, izl, izr;
   double w_rg[LEPIC_NM_RG];     // 1 / np_tot_rg(ptype, i_rg)
   double h0, h1, h2;
+  int n1, n2;
+};
+
+// FP64 SoA layout
+struct AccF64 {
+  double *p[LEPIC_NPART];
+  int *count[LEPIC_NPART];
+  long long cap[LEPIC_NPART];
+  __device__ void load_v(int P, long long i, double &vx, double &vy, double &vz) const {
+    const double *q = p[P];
+    vx = q[3 * cap[P] + i];
+    vy = q[4 * cap[P] + i];
+    vz = q[5 * cap[P] + i];
+  }
+  __device__ void store_v(int P, long long i, double vx, double vy, double vz) const {
+    double *q = p[P];
+    q[3 * cap[P] + i] = vx;
+    q[4 * cap[P] + i] = vy;
+    q[5 * cap[P] + i] = vz;
+  }
+  // new particle j of species B at the position of (P, i)
+  __device__ void append(int P, long long i, int B, long long j, double vx, double vy, double vz) const {
+    const double *s = p[P];
+    double *d = p[B];
+    const long long cs = cap[P], cb = cap[B];
+    d[j] = s[i];
+    d[cb + j] = s[cs + i];
+    d[2 * cb + j] = s[2 * cs + i];
+    d[3 * cb + j] = vx;
+    d[4 * cb + j] = vy;
+    d[5 * cb + j] = vz;
+  }
+  __device__ void cell_of(const MCCConst &c, int P, long long i, int &ix, int &iy, int &iz) const {
+    const double *q = p[P];
+    ix = (int)(q[i] / c.h0) + 1;
+    iy = (int)(q[cap[P] + i] / c.h1) + 1;
+    iz = (int)(q[2 * cap[P] + i] / c.h2) + 1;
+  }
+};
+
+// mixed layout: cell + FP32 offsets and velocities
+struct AccMixed {
+  int *cell[LEPIC_NPART];
+  float *p[LEPIC_NPART];
+  int *count[LEPIC_NPART];
+  long long cap[LEPIC_NPART];
+  __device__ void load_v(int P, long long i, double &vx, double &vy, double &vz) const {
+    const float *q = p[P];
+    vx = q[3 * cap[P] + i];
+    vy = q[4 * cap[P] + i];
+    vz = q[5 * cap[P] + i];
+  }
+  __device__ void store_v(int P, long long i, double vx, double vy, double vz) const {
+    float *q = p[P];
+    q[3 * cap[P] + i] = (float)vx;
+    q[4 * cap[P] + i] = (float)vy;
+    q[5 * cap[P] + i] = (float)vz;
+  }
+  __device__ void append(int P, long long i, int B, long long j, double vx, double vy, double vz) const {
+    const float *s = p[P];
+    float *d = p[B];
+    const long long cs = cap[P], cb = cap[B];
+    cell[B][j] = cell[P][i];
+    d[j] = s[i];
+    d[cb + j] = s[cs + i];
+    d[2 * cb + j] = s[2 * cs + i];
+    d[3 * cb + j] = (float)vx;
+    d[4 * cb + j] = (float)vy;
+    d[5 * cb + j] = (float)vz;
+  }
+  __device__ void cell_of(const MCCConst &c, int P, long long i, int &ix, int &iy, int &iz) const {
+    const int cc = cell[P][i];
+    ix = cc % c.n1 + 1;
+    iy = (cc / c.n1) % c.n2 + 1;
+    iz = cc / (c.n1 * c.n2) + 1;
+  }
 };
 
 // Src/collisions.f90:1022-1050
@@ -85,50 +165,79 @@ __device__ __forceinline__ double sigma_at(const double *__restrict__ Er, const 
   return sL + (E - EL) * (sR - sL) / (ER - EL);
 }
 
-struct SpPtrs {
-  double *p[LEPIC_NPART];
-  int *count[LEPIC_NPART];
-  int cap[LEPIC_NPART];
-};
+__device__ __forceinline__ unsigned lanemask_lt_m() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
 
-__global__ void __launch_bounds__(MB) k_mcc(MCCConst c, SpPtrs S, const double *__restrict__ Er,
-                                            const double *__restrict__ sig, signed char *flag_dead,
-                                            int *add, unsigned long long *counts, double *cnt_col,
-                                            int *err) {
-  const int P = c.ptype - 1;
+// pass 1: Bernoulli(Pmax) per particle, candidates appended to a list
+__global__ void __launch_bounds__(MB) k_mcc_select(MCCConst c, const int *__restrict__ count,
+                                                   int *__restrict__ cand, int *__restrict__ ncand) {
+  const unsigned full = 0xffffffffu;
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int N = *S.count[P];
-  int sel = -1;
-  if (i < N) {
-    U4 ctr = {(uint32_t)i, 0u, c.c2, c.c3};
-    U4 r0 = philox4x32_10(ctr, c.k0, c.k1);
-    if (u01(r0.x) < c.Pmax) {
-      const long long cap = S.cap[P];
-      double *pp = S.p[P];
-      double vx0 = pp[3 * cap + i], vy0 = pp[4 * cap + i], vz0 = pp[5 * cap + i];
+  bool hit = false;
+  if (i < *count) {
+    U4 r0 = philox4x32_10({(uint32_t)i, 0u, c.c2, c.c3}, c.k0, c.k1);
+    hit = u01(r0.x) < c.Pmax;
+  }
+  const unsigned m = __ballot_sync(full, hit);
+  if (m) {
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(ncand, __popc(m));
+    base = __shfl_sync(full, base, leader);
+    if (hit) cand[base + __popc(m & lanemask_lt_m())] = (int)i;
+  }
+}
+
+// pass 2: the collision physics on the candidates (grid-stride over warps so
+// every lane of a warp reaches the warp-wide counter reductions)
+template <class Acc>
+__global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, const int *__restrict__ cand,
+                                                    const int *__restrict__ ncand_p,
+                                                    const double *__restrict__ Er,
+                                                    const double *__restrict__ sig, signed char *flag_dead,
+                                                    int *add, unsigned long long *counts, double *cnt_col,
+                                                    int *err) {
+  const unsigned full = 0xffffffffu;
+  const int P = c.ptype - 1;
+  const int ncand = *ncand_p;
+  const int lane = threadIdx.x & 31;
+  const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long wb = warp0 * 32; wb < ncand; wb += nwarps * 32) {
+    const long long t = wb + lane;
+    int sel = -1;
+    if (t < ncand) {
+      const long long i = cand[t];
+      U4 ctr = {(uint32_t)i, 0u, c.c2, c.c3};
+      const U4 r0 = philox4x32_10(ctr, c.k0, c.k1);
+      double vx0, vy0, vz0;
+      S.load_v(P, i, vx0, vy0, vz0);
       ctr.y = 1u;
-      U4 r1 = philox4x32_10(ctr, c.k0, c.k1);
+      const U4 r1 = philox4x32_10(ctr, c.k0, c.k1);
       // one Maxwellian target per target species (Src/collisions.f90:437-449)
-      double vr_t = 0, Ekr_t = 0, mu_t = 0, vxc = 0, vyc = 0, vzc = 0, tvx = 0, tvy = 0, tvz = 0;
+      double vr_t = 0, mu_t = 0, vxc = 0, vyc = 0, vzc = 0, tvx = 0, tvy = 0, tvz = 0, Ekr_t = 0;
       int cur_tt = -1;
       double nu[MAXR];
       double sum_nu = 0.0;
       for (int r = 0; r < c.nr; ++r) {
-        int tt = c.tt[r];
+        const int tt = c.tt[r];
         if (tt != cur_tt) {
-          double vt = c.vt0[tt - 1];
-          double vp = vt * sqrt(-log(u01(r1.x)));
+          const double vt = c.vt0[tt - 1];
+          const double vp = vt * sqrt(-log(u01(r1.x)));
           double s1, c1;
           sincos(2.0 * c.pi * u01(r1.y), &s1, &c1);
           tvx = vp * c1;
           tvy = vp * s1;
-          double vp2 = vt * sqrt(-log(u01(r1.z)));
+          const double vp2 = vt * sqrt(-log(u01(r1.z)));
           tvz = vp2 * cos(2.0 * c.pi * u01(r1.w));
-          double mt = fabs(c.mass[tt - 1]);
+          const double mt = fabs(c.mass[tt - 1]);
           mu_t = c.m_p * mt / (c.m_p + mt);
           vr_t = sqrt((vx0 - tvx) * (vx0 - tvx) + (vy0 - tvy) * (vy0 - tvy) + (vz0 - tvz) * (vz0 - tvz));
           Ekr_t = (0.5 * mu_t * (vr_t * vr_t)) / c.qe;
-          double sm = c.m_p + mt;
+          const double sm = c.m_p + mt;
           vxc = (c.m_p * vx0 + mt * tvx) / sm;
           vyc = (c.m_p * vy0 + mt * tvy) / sm;
           vzc = (c.m_p * vz0 + mt * tvz) / sm;
@@ -136,11 +245,11 @@ __global__ void __launch_bounds__(MB) k_mcc(MCCConst c, SpPtrs S, const double *
           cur_tt = tt;
         }
         int found;
-        double sp = sigma_at(Er, sig + (long long)c.npt_mx * (c.ind[r] - 1), c.npt, Ekr_t, found);
+        const double sp = sigma_at(Er, sig + (long long)c.npt_mx * (c.ind[r] - 1), c.npt, Ekr_t, found);
         nu[r] = found ? c.np_t[r] * sp * vr_t / c.nu_max : 0.0;
         sum_nu += nu[r];
       }
-      double u = u01(r0.y);
+      const double u = u01(r0.y);
       if (u <= sum_nu) {
         double s = 0.0;
         for (int r = 0; r < c.nr; ++r) {
@@ -155,9 +264,7 @@ __global__ void __launch_bounds__(MB) k_mcc(MCCConst c, SpPtrs S, const double *
         const int rt = c.rt[sel];
         if (rt == 4) {
           // charge exchange: the incident takes the target's velocity
-          pp[3 * cap + i] = tvx;
-          pp[4 * cap + i] = tvy;
-          pp[5 * cap + i] = tvz;
+          S.store_v(P, i, tvx, tvy, tvz);
         } else {
           double Ee = 0.5 * mu_t * (vr_t * vr_t) - c.Eth[sel] * c.qe;
           if (Ee < 0.0) {
@@ -167,76 +274,62 @@ __global__ void __launch_bounds__(MB) k_mcc(MCCConst c, SpPtrs S, const double *
           const int nby = c.n_by[sel];
           double sum_mass = 0.0;
           for (int a = 0; a < nby; ++a) sum_mass = sum_mass + 1.0 / fabs(c.mass[c.by[sel][a] - 1]);
-          double th_add = 2.0 * c.pi / (double)nby;
-          double cos_th = 1.0 - 2.0 * u01(r0.z);
+          const double th_add = 2.0 * c.pi / (double)nby;
+          const double cos_th = 1.0 - 2.0 * u01(r0.z);
           double th = acos(cos_th);
-          double phi = 2.0 * c.pi * u01(r0.w);
+          const double phi = 2.0 * c.pi * u01(r0.w);
           double sin_ph, cos_ph;
           sincos(phi, &sin_ph, &cos_ph);
           ctr.y = 2u;
-          U4 r2 = philox4x32_10(ctr, c.k0, c.k1);
-          double cos_th_s = 1.0 - 2.0 * u01(r2.x);
-          double phi_s = 2.0 * c.pi * u01(r2.y);
-          double xp = pp[i], yp = pp[cap + i], zp = pp[2 * cap + i];
+          const U4 r2 = philox4x32_10(ctr, c.k0, c.k1);
+          const double cos_th_s = 1.0 - 2.0 * u01(r2.x);
+          const double phi_s = 2.0 * c.pi * u01(r2.y);
           bool incident_reused = false;
           for (int a = 0; a < nby; ++a) {
             double sth, cth;
             sincos(th, &sth, &cth);
             th = th + th_add;
-            double ex = cth, ey = sth * sin_ph, ez = sth * cos_ph;
+            const double ex = cth, ey = sth * sin_ph, ez = sth * cos_ph;
             double ex1 = 0, ey1 = 0, ez1 = 0;
             scatter(ex1, ey1, ez1, ex, ey, ez, cos_th_s, phi_s);
-            int bt = c.by[sel][a];
+            const int bt = c.by[sel][a];
             if (c.mass[bt - 1] <= 0) continue;
-            double mb = fabs(c.mass[bt - 1]);
-            double vp = sqrt(2.0 * (Ee / sum_mass) / (mb * mb));
-            double nvx = vxc + vp * ex1, nvy = vyc + vp * ey1, nvz = vzc + vp * ez1;
-            bool reuse = (a == 0 && bt == c.ptype) || ((rt == 1 || rt == 3) && bt == c.ptype);
+            const double mb = fabs(c.mass[bt - 1]);
+            const double vp = sqrt(2.0 * (Ee / sum_mass) / (mb * mb));
+            const double nvx = vxc + vp * ex1, nvy = vyc + vp * ey1, nvz = vzc + vp * ez1;
+            const bool reuse = (a == 0 && bt == c.ptype) || ((rt == 1 || rt == 3) && bt == c.ptype);
             if (reuse) {
-              pp[3 * cap + i] = nvx;
-              pp[4 * cap + i] = nvy;
-              pp[5 * cap + i] = nvz;
+              S.store_v(P, i, nvx, nvy, nvz);
               incident_reused = true;
             } else {
               const int B = bt - 1;
-              int slot = atomicAdd(&add[B], 1);
-              long long j = (long long)*S.count[B] + slot;
-              if (j >= S.cap[B]) {
-                raise_err(err, LEPIC_ERR_CAPACITY, B);
-              } else {
-                const long long cb = S.cap[B];
-                double *qb = S.p[B];
-                qb[j] = xp;
-                qb[cb + j] = yp;
-                qb[2 * cb + j] = zp;
-                qb[3 * cb + j] = nvx;
-                qb[4 * cb + j] = nvy;
-                qb[5 * cb + j] = nvz;
-              }
+              const int slot = atomicAdd(&add[B], 1);
+              const long long j = (long long)*S.count[B] + slot;
+              if (j >= S.cap[B]) raise_err(err, LEPIC_ERR_CAPACITY, B);
+              else S.append(P, i, B, j, nvx, nvy, nvz);
             }
           }
           if (!incident_reused && flag_dead) flag_dead[i] = 1;
         }
         if (cnt_col) {
-          int ix = (int)(pp[i] / c.h0) + 1, iy = (int)(pp[cap + i] / c.h1) + 1,
-              iz = (int)(pp[2 * cap + i] / c.h2) + 1;
-          for (int g = 0; g < c.n_rg; ++g) {
-            if (ix >= c.ixl[g] && ix <= c.ixr[g] && iy >= c.iyl && iy <= c.iyr && iz >= c.izl &&
+          int ix, iy, iz;
+          S.cell_of(c, P, i, ix, iy, iz);
+          for (int gq = 0; gq < c.n_rg; ++gq) {
+            if (ix >= c.ixl[gq] && ix <= c.ixr[gq] && iy >= c.iyl && iy <= c.iyr && iz >= c.izl &&
                 iz <= c.izr) {
-              atomicAdd(&cnt_col[(c.ind[sel] - 1) + (long long)c.ncol_mx * g], c.w_rg[g]);
+              atomicAdd(&cnt_col[(c.ind[sel] - 1) + (long long)c.ncol_mx * gq], c.w_rg[gq]);
               break;
             }
           }
         }
       }
     }
-  }
-  // warp-aggregated collision counters
-  const unsigned mask = __ballot_sync(0xffffffffu, sel >= 0);
-  if (mask) {
-    for (int r = 0; r < c.nr; ++r) {
-      unsigned m = __ballot_sync(0xffffffffu, sel == r);
-      if ((threadIdx.x & 31) == 0 && m) atomicAdd(&counts[c.ind[r] - 1], (unsigned long long)__popc(m));
+    // warp-aggregated collision counters
+    if (__ballot_sync(full, sel >= 0)) {
+      for (int r = 0; r < c.nr; ++r) {
+        const unsigned m = __ballot_sync(full, sel == r);
+        if (lane == 0 && m) atomicAdd(&counts[c.ind[r] - 1], (unsigned long long)__popc(m));
+      }
     }
   }
 }
@@ -247,37 +340,33 @@ __global__ void k_mcc_finalize(int *count0, int *count1, int *count2, const int 
     if (cs[p]) *cs[p] += add[p];
 }
 
-}  // namespace
-
-int launch_collisions(const lepic_grid_t &g, lepic_species_f64_t *sp, int ntype,
-                      const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
-                      unsigned long long call_index, double *nu_max, long long *counts,
-                      cudaStream_t s, const RegionCount *rg) {
+// Host part shared by both layouts: nu_max, Pmax and the per-species
+// constants (Src/collisions.f90:97-165).
+template <class Acc>
+int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed char *const *flag_dead,
+                   int ntype, const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
+                   unsigned long long call_index, double *nu_max, long long *counts, cudaStream_t s,
+                   const RegionCount *rg, const char *tname) {
   if (ntype > 3) return LEPIC_ERR_UNSUPPORTED;
   auto CI = [&](int icol, int info) { return T.col_info_h[(icol - 1) + (long long)T.ncol * (info - 1)]; };
   int *add = (int *)scratch("mcc_add", sizeof(int) * LEPIC_NPART);
   unsigned long long *cnt = (unsigned long long *)scratch("mcc_cnt", sizeof(unsigned long long) * 64);
-  if (!add || !cnt || T.ncol > 64) return LEPIC_ERR_CUDA;
+  int *ncand = (int *)scratch("mcc_ncand", sizeof(int) * LEPIC_NPART);
+  if (!add || !cnt || !ncand || T.ncol > 64) return LEPIC_ERR_CUDA;
   LEPIC_CUDA(cudaMemsetAsync(add, 0, sizeof(int) * LEPIC_NPART, s));
   LEPIC_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 64, s));
-  SpPtrs S;
-  memset(&S, 0, sizeof(S));
-  for (int p = 0; p < ntype; ++p) {
-    S.p[p] = sp[p].p;
-    S.count[p] = sp[p].count;
-    S.cap[p] = sp[p].cap;
-  }
+  LEPIC_CUDA(cudaMemsetAsync(ncand, 0, sizeof(int) * LEPIC_NPART, s));
   std::vector<double> Eth(T.ncol > 0 ? T.ncol : 1, 0.0);
   if (T.ncol > 0)
     LEPIC_CUDA(cudaMemcpyAsync(Eth.data(), T.sig_Eth, sizeof(double) * T.ncol, cudaMemcpyDeviceToHost, s));
   std::vector<int> Nh(ntype, 0);
-  for (int p = 0; p < ntype; ++p) {
-    LEPIC_CUDA(cudaMemcpyAsync(&Nh[p], sp[p].count, sizeof(int), cudaMemcpyDeviceToHost, s));
-  }
+  for (int p = 0; p < ntype; ++p)
+    LEPIC_CUDA(cudaMemcpyAsync(&Nh[p], counts_dev[p], sizeof(int), cudaMemcpyDeviceToHost, s));
   LEPIC_CUDA(cudaStreamSynchronize(s));
+  const Dims d(g.n);
   for (int p = 1; p <= ntype; ++p) {
     nu_max[p - 1] = 0.0;
-    int pn = T.p_ncol[p - 1];
+    const int pn = T.p_ncol[p - 1];
     if (pn == 0 || P.mass[p - 1] <= 0) continue;
     if (pn > MAXR) return LEPIC_ERR_UNSUPPORTED;
     MCCConst c;
@@ -287,22 +376,23 @@ int launch_collisions(const lepic_grid_t &g, lepic_species_f64_t *sp, int ntype,
     c.qe = P.qe;
     c.pi = P.pi;
     c.m_p = fabs(P.mass[p - 1]);
+    c.n1 = d.n1;
+    c.n2 = d.n2;
     for (int q = 0; q < LEPIC_NPART; ++q) {
       c.mass[q] = P.mass[q];
       c.vt0[q] = P.vt0[q];
     }
     double num = 0.0;
     for (int r = 0; r < pn; ++r) {
-      int ind = T.sig_list[(p - 1) + LEPIC_NPART * r];
-      int n_re = CI(ind, 1), n_by = CI(ind, 2);
+      const int ind = T.sig_list[(p - 1) + LEPIC_NPART * r];
+      const int n_re = CI(ind, 1), n_by = CI(ind, 2);
       if (n_by > MAXBY || n_re > 2) return LEPIC_ERR_UNSUPPORTED;
-      int tt = CI(ind, 2 + n_re);
+      const int tt = CI(ind, 2 + n_re);
       if (P.charge[tt - 1] != 0.0) return LEPIC_ERR_UNSUPPORTED;  // DSMC targets
       c.ind[r] = ind;
       c.tt[r] = tt;
       c.n_re[r] = n_re;
       c.n_by[r] = n_by;
-      for (int a = 0; a < n_re; ++a) c.re[r][a] = CI(ind, 3 + a);
       for (int a = 0; a < n_by; ++a) c.by[r][a] = CI(ind, 3 + n_re + a);
       c.rt[r] = CI(ind, 3 + n_re + n_by);
       c.Eth[r] = Eth[ind - 1];
@@ -310,7 +400,7 @@ int launch_collisions(const lepic_grid_t &g, lepic_species_f64_t *sp, int ntype,
       num = num + P.np_mx[tt - 1] * T.sigv_mx[(p - 1) + LEPIC_NPART * (ind - 1)];
     }
     nu_max[p - 1] = num < P.nu_uplim[p - 1] ? num : P.nu_uplim[p - 1];
-    double Pmax = nu_max[p - 1] * (double)(float)P.ns_coll * P.dt;
+    const double Pmax = nu_max[p - 1] * (double)(float)P.ns_coll * P.dt;
     if (Pmax > 1.0) return LEPIC_ERR_PMAX;
     if (Nh[p - 1] == 0 || nu_max[p - 1] <= 0.0) continue;
     c.Pmax = Pmax;
@@ -339,21 +429,77 @@ int launch_collisions(const lepic_grid_t &g, lepic_species_f64_t *sp, int ntype,
       c.izr = rg->izr;
       cc = rg->cnt_col_dev;
     }
-    int tm = timer_start("mcc_f64", s);
-    k_mcc<<<grid_for(Nh[p - 1], MB), MB, 0, s>>>(c, S, T.sig_Er, T.sig, sp[p - 1].flag_dead, add, cnt,
-                                                  cc, ctx().d_err);
+    char nm[32];
+    snprintf(nm, sizeof nm, "mcc_cand%d", p - 1);
+    int *cand = (int *)scratch(nm, sizeof(int) * (size_t)Nh[p - 1]);
+    if (!cand) return LEPIC_ERR_CUDA;
+    int tm = timer_start(tname, s);
+    k_mcc_select<<<grid_for(Nh[p - 1], MB), MB, 0, s>>>(c, counts_dev[p - 1], cand, ncand + (p - 1));
+    k_mcc_collide<Acc><<<ctx().sms * 8, MB, 0, s>>>(c, S, cand, ncand + (p - 1), T.sig_Er, T.sig,
+                                                    flag_dead[p - 1], add, cnt, cc, ctx().d_err);
     timer_stop(tm, s);
     LEPIC_CUDA(cudaGetLastError());
   }
-  k_mcc_finalize<<<1, 1, 0, s>>>(sp[0].count, ntype > 1 ? sp[1].count : nullptr,
-                                 ntype > 2 ? sp[2].count : nullptr, add, ntype);
+  k_mcc_finalize<<<1, 1, 0, s>>>(counts_dev[0], ntype > 1 ? counts_dev[1] : nullptr,
+                                 ntype > 2 ? counts_dev[2] : nullptr, add, ntype);
   LEPIC_CUDA(cudaGetLastError());
   unsigned long long hc[64];
   LEPIC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, s));
-  int rc = check_err(s);
+  const int rc = check_err(s);
   if (counts)
     for (int q = 0; q < T.ncol; ++q) counts[q] += (long long)hc[q];
   return rc;
 }
 
+}  // namespace
+
+int launch_collisions(const lepic_grid_t &g, lepic_species_f64_t *sp, int ntype,
+                      const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
+                      unsigned long long call_index, double *nu_max, long long *counts,
+                      cudaStream_t s, const RegionCount *rg) {
+  if (ntype > 3) return LEPIC_ERR_UNSUPPORTED;
+  AccF64 S;
+  memset(&S, 0, sizeof(S));
+  int *cnts[LEPIC_NPART] = {nullptr};
+  signed char *fd[LEPIC_NPART] = {nullptr};
+  for (int p = 0; p < ntype; ++p) {
+    S.p[p] = sp[p].p;
+    S.count[p] = sp[p].count;
+    S.cap[p] = sp[p].cap;
+    cnts[p] = sp[p].count;
+    fd[p] = sp[p].flag_dead;
+  }
+  return run_collisions(g, S, cnts, fd, ntype, T, P, seed, call_index, nu_max, counts, s, rg, "mcc_f64");
+}
+
+int launch_collisions_mixed(const lepic_grid_t &g, lepic_species_mixed_t *sp, int ntype,
+                            const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
+                            unsigned long long call_index, double *nu_max, long long *counts,
+                            cudaStream_t s) {
+  if (ntype > 3) return LEPIC_ERR_UNSUPPORTED;
+  AccMixed S;
+  memset(&S, 0, sizeof(S));
+  int *cnts[LEPIC_NPART] = {nullptr};
+  signed char *fd[LEPIC_NPART] = {nullptr};
+  for (int p = 0; p < ntype; ++p) {
+    S.cell[p] = sp[p].cell;
+    S.p[p] = sp[p].p;
+    S.count[p] = sp[p].count;
+    S.cap[p] = sp[p].cap;
+    cnts[p] = sp[p].count;
+    fd[p] = sp[p].flag_dead;
+  }
+  return run_collisions(g, S, cnts, fd, ntype, T, P, seed, call_index, nu_max, counts, s, nullptr,
+                        "mcc_mixed");
+}
+
 }  // namespace lepic
+
+extern "C" int lepic_dev_collisions_mixed(const lepic_grid_t *g, lepic_species_mixed_t *sp, int ntype,
+                                          const lepic_tables_t *T, const lepic_phys_t *P,
+                                          unsigned long long seed, unsigned long long call_index,
+                                          double *nu_max, long long *counts, void *stream) {
+  if (!g || !sp || !T || !P || ntype < 1) return LEPIC_ERR_ARG;
+  return lepic::launch_collisions_mixed(*g, sp, ntype, *T, *P, seed, call_index, nu_max, counts,
+                                        (cudaStream_t)stream);
+}

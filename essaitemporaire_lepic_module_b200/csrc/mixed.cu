@@ -1,0 +1,675 @@
+// Mixed-precision particle kernels of the device-resident step loop.
+//
+// Particle state per species (28 B per particle instead of 48):
+//   cell  int32   c = (ix-1) + n1((iy-1) + n2(iz-1)), ix = INT(x/h)+1 of the
+//                 reference (Src/part_expmover.f90:89-91)
+//   p32   float   6 planes: fx, fy, fz in [0,1) (x = (ix-1+fx) h) and
+//                 vx, vy, vz in m/s
+// The push is the reference's gather + Boris + leapfrog
+// (Src/part_expmover.f90:89-246) in FP32 on an FP32 copy of E packed as one
+// float4 per node; the position update is done on the in-cell offset
+// (f += v dt/h, cell += floor(f)), which keeps ~7 significant digits of the
+// position inside its cell.
+//
+// Deposition (Src/part_expmover.f90:591-656) of the new position: the eight
+// CIC weights are computed in FP64 from the FP32 offsets and quantized to
+// integers in units of 2^-24 with the eighth taken as 2^24 minus the other
+// seven, so every particle deposits exactly 2^24 units and integer sums are
+// exact and independent of the summation order.  The sort orders particles
+// by 8x8x8-cell tiles; one block pushes the particles of one tile and sums
+// their weights with 32-bit shared-memory atomics into a node tile covering
+// the tile's cells plus one halo cell on each side (a weight w is split into
+// w >> 12 and w & 4095 held in two tiles, which bounds both sums below 2^31
+// for up to 2^18 particles per flush).  The node tile is then added to the
+// FP64 grid with one atomic per non-zero node; particles outside the box
+// (drifted since the sort, moved by hole filling, appended by collisions) add
+// their quantized weights to the grid directly.  kdep and kq are applied in
+// FP64 to the integer sums.
+//
+// A thread moves four consecutive particles with 16-byte loads and stores
+// and merges the weights of those that end in the same cell before touching
+// shared memory.
+#include <cstring>
+
+#include "lepic_internal.cuh"
+
+namespace lepic {
+
+namespace {
+
+constexpr int MBK = 256;
+constexpr int TC = LEPIC_TILE_CELLS;       // tile edge in cells
+constexpr int TN = TC + 3;                 // node tile edge (halo cell each side)
+constexpr int TT = TN * TN * TN;
+constexpr int CHUNK = 4 * MBK;             // particles per block iteration
+constexpr int FLUSH_CHUNKS = (1 << 18) / CHUNK;
+constexpr double QS = 16777216.0;          // 2^24 weight units per particle
+constexpr double QI = 1.0 / 16777216.0;
+
+__device__ __forceinline__ unsigned lmask_le() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_le;" : "=r"(m));
+  return m;
+}
+__device__ __forceinline__ unsigned lmask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+struct MixedConst {
+  float dth0, dth1, dth2;     // dt / h per direction
+  float k1;                   // dt q / (2 m)
+  float Bx, By, Bz;
+  int boris, flag_pbc, ngrid;
+  double Nm, mass, kdep;      // kdep = Nm / (h1 h2 h3)
+  int ntx, nty, ntiles;       // tile grid
+};
+
+// quantized CIC weights of offsets (gx, gy, gz): w[c] in units of 2^-24,
+// summing to exactly 2^24 (node order of Src/part_expmover.f90:591-656)
+__device__ __forceinline__ void qweights(float gx, float gy, float gz, int w[8]) {
+  const double qx = 1.0 - (double)gx, qy = 1.0 - (double)gy, qz = 1.0 - (double)gz;
+  const double px = 1.0 - qx, py = 1.0 - qy, pz = 1.0 - qz;
+  w[0] = __double2int_rn(qx * qy * qz * QS);
+  w[1] = __double2int_rn(px * qy * qz * QS);
+  w[2] = __double2int_rn(px * py * qz * QS);
+  w[3] = __double2int_rn(qx * py * qz * QS);
+  w[4] = __double2int_rn(qx * qy * pz * QS);
+  w[5] = __double2int_rn(px * qy * pz * QS);
+  w[6] = __double2int_rn(px * py * pz * QS);
+  w[7] = 16777216 - (w[0] + w[1] + w[2] + w[3] + w[4] + w[5] + w[6]);
+}
+
+struct Tile {
+  int *hi, *lo;               // shared node tiles (nullptr: no tile)
+  int bx, by, bz;             // node coordinates of local (0,0,0)
+};
+
+// 8 weights of base node q (grid coordinates jx,jy,jz) into the tile when the
+// cell lies in the box, else into the FP64 grid
+__device__ __forceinline__ void deposit8(const Dims &d, const Tile &T, int jx, int jy, int jz, long long q,
+                                         const int w[8], double kdep, const double *__restrict__ kq,
+                                         double *__restrict__ np) {
+  const int lx = jx - T.bx, ly = jy - T.by, lz = jz - T.bz;
+  if (T.hi && lx >= 0 && lx < TN - 1 && ly >= 0 && ly < TN - 1 && lz >= 0 && lz < TN - 1) {
+    const int t = lx + TN * (ly + TN * lz);
+    const int to[8] = {0, 1, 1 + TN, TN, TN * TN, 1 + TN * TN, 1 + TN + TN * TN, TN + TN * TN};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      atomicAdd(&T.hi[t + to[c]], w[c] >> 12);
+      atomicAdd(&T.lo[t + to[c]], w[c] & 4095);
+    }
+  } else {
+    const long long sy = d.N1, sz = d.N1 * d.N2;
+    const long long o[8] = {0, 1, 1 + sy, sy, sz, 1 + sz, 1 + sy + sz, sy + sz};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) atomicAdd(&np[q + o[c]], __ldg(&kq[q + o[c]]) * (kdep * ((double)w[c] * QI)));
+  }
+}
+
+// the node tile into the FP64 grid (non-zero nodes), then cleared
+__device__ void flush_tile(const Dims &d, const Tile &T, double kdep, const double *__restrict__ kq,
+                           double *__restrict__ np) {
+  for (int e = threadIdx.x; e < TT; e += blockDim.x) {
+    const int h = T.hi[e], l = T.lo[e];
+    if (h | l) {
+      const int lx = e % TN, ly = (e / TN) % TN, lz = e / (TN * TN);
+      const int gx = T.bx + lx, gy = T.by + ly, gz = T.bz + lz;
+      if (gx <= d.n1 + 2 && gy <= d.n2 + 2 && gz <= d.n3 + 2) {
+        const long long node = d.g(gx, gy, gz);
+        const double v = ((double)h * 4096.0 + (double)l) * QI;
+        atomicAdd(&np[node], __ldg(&kq[node]) * (kdep * v));
+      }
+      T.hi[e] = 0;
+      T.lo[e] = 0;
+    }
+  }
+}
+
+// Push + loss test + deposit of the particle quad starting at i0 (a multiple
+// of 4); particles outside [lo, hi) are not touched.  Every lane of the warp
+// must call this (warp-wide hole appends).
+__device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, const Tile &T, long long i0,
+                                          long long lo, long long hi, const float4 *__restrict__ E4,
+                                          const int *__restrict__ bcnd, const unsigned char *__restrict__ cw,
+                                          int *__restrict__ cell, float *__restrict__ p, long long cap,
+                                          signed char *__restrict__ flag, const double *__restrict__ kq,
+                                          double *__restrict__ np, int *__restrict__ holes,
+                                          int *__restrict__ nholes, double *__restrict__ acc,
+                                          int *__restrict__ err) {
+  const unsigned full = 0xffffffffu;
+  const int n1 = d.n1, n2 = d.n2, n3 = d.n3;
+  const int ncell = n1 * n2 * n3;
+  int4 c4 = make_int4(-1, -1, -1, -1);
+  float4 P[6];
+  char4 f4 = make_char4(0, 0, 0, 0);
+  bool in[4] = {false, false, false, false};
+  if (i0 < hi) {
+    // i0 + 3 < cap: cap is a multiple of 4
+    c4 = *reinterpret_cast<const int4 *>(cell + i0);
+    f4 = *reinterpret_cast<const char4 *>(flag + i0);
+#pragma unroll
+    for (int a = 0; a < 6; ++a) P[a] = *reinterpret_cast<const float4 *>(p + a * cap + i0);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) in[k] = (i0 + k >= lo) && (i0 + k < hi);
+  } else {
+#pragma unroll
+    for (int a = 0; a < 6; ++a) P[a] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  const bool full4 = in[0] && in[1] && in[2] && in[3];
+  bool hole[4] = {false, false, false, false};
+  int jx[4], jy[4], jz[4];
+  float gxs[4], gys[4], gzs[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    jx[k] = -1;
+    jy[k] = jz[k] = 0;
+    gxs[k] = gys[k] = gzs[k] = 0.f;
+    if (!in[k]) continue;
+    const int cc = (&c4.x)[k];
+    float vx = (&P[3].x)[k], vy = (&P[4].x)[k], vz = (&P[5].x)[k];
+    if ((&f4.x)[k] == 1) {
+      // killed in a collision: removed here (Src/part_expmover.f90:70-84)
+      atomicAdd(&acc[1], -(0.5 * c.Nm * c.mass * ((double)vx * vx + (double)vy * vy + (double)vz * vz)));
+      hole[k] = true;
+      continue;
+    }
+    if (cc < 0 || cc >= ncell) {
+      raise_err(err, LEPIC_ERR_CELL, (int)(i0 + k));
+      hole[k] = true;
+      continue;
+    }
+    float fx = (&P[0].x)[k], fy = (&P[1].x)[k], fz = (&P[2].x)[k];
+    const int ix = cc % n1 + 1, iy = (cc / n1) % n2 + 1, iz = cc / (n1 * n2) + 1;
+    // gather: left-node weights 1 - f (Src/part_expmover.f90:89-108)
+    const float px = 1.f - fx, py = 1.f - fy, pz = 1.f - fz;
+    const float k0 = px * py * pz, ka = (1.f - px) * py * pz, kb = (1.f - px) * (1.f - py) * pz,
+                kc = px * (1.f - py) * pz, kd = px * py * (1.f - pz), ke = (1.f - px) * py * (1.f - pz),
+                kf = (1.f - px) * (1.f - py) * (1.f - pz), kg = px * (1.f - py) * (1.f - pz);
+    const long long sy = d.N1, sz = d.N1 * d.N2;
+    const long long g0 = d.g(ix, iy, iz);
+    const float4 e0 = __ldg(E4 + g0), e1 = __ldg(E4 + g0 + 1), e2 = __ldg(E4 + g0 + 1 + sy),
+                 e3 = __ldg(E4 + g0 + sy), e4 = __ldg(E4 + g0 + sz), e5 = __ldg(E4 + g0 + 1 + sz),
+                 e6 = __ldg(E4 + g0 + 1 + sy + sz), e7 = __ldg(E4 + g0 + sy + sz);
+    const float Ex = k0 * e0.x + ka * e1.x + kb * e2.x + kc * e3.x + kd * e4.x + ke * e5.x + kf * e6.x + kg * e7.x;
+    const float Ey = k0 * e0.y + ka * e1.y + kb * e2.y + kc * e3.y + kd * e4.y + ke * e5.y + kf * e6.y + kg * e7.y;
+    const float Ez = k0 * e0.z + ka * e1.z + kb * e2.z + kc * e3.z + kd * e4.z + ke * e5.z + kf * e6.z + kg * e7.z;
+    const float k1 = c.k1;
+    if (c.boris) {
+      // Src/part_expmover.f90:128-160
+      const float Bx = c.Bx, By = c.By, Bz = c.Bz;
+      const float B_tot = sqrtf(Bx * Bx + By * By + Bz * Bz);
+      const float kk = k1 * (2.f / (1.f + (k1 * B_tot) * (k1 * B_tot)));
+      const float v1x = vx + k1 * Ex, v1y = vy + k1 * Ey, v1z = vz + k1 * Ez;
+      const float v3x = v1x + k1 * (v1y * Bz - v1z * By);
+      const float v3y = v1y + k1 * (v1z * Bx - v1x * Bz);
+      const float v3z = v1z + k1 * (v1x * By - v1y * Bx);
+      vx = v1x + kk * (v3y * Bz - v3z * By) + k1 * Ex;
+      vy = v1y + kk * (v3z * Bx - v3x * Bz) + k1 * Ey;
+      vz = v1z + kk * (v3x * By - v3y * Bx) + k1 * Ez;
+    } else {
+      vx = vx + 2.f * k1 * Ex;
+      vy = vy + 2.f * k1 * Ey;
+      vz = vz + 2.f * k1 * Ez;
+    }
+    // position on the in-cell offset; the cell moves by floor(f)
+    fx = fx + vx * c.dth0;
+    fy = fy + vy * c.dth1;
+    fz = fz + vz * c.dth2;
+    int sx = (int)floorf(fx), syi = (int)floorf(fy), szi = (int)floorf(fz);
+    fx -= (float)sx;
+    fy -= (float)syi;
+    fz -= (float)szi;
+    if (fx >= 1.f) { fx = 0.f; sx += 1; }
+    if (fy >= 1.f) { fy = 0.f; syi += 1; }
+    if (fz >= 1.f) { fz = 0.f; szi += 1; }
+    int ax = ix + sx, ay = iy + syi, az = iz + szi;
+    if (c.flag_pbc == 1) {
+      if (ay > n2) ay -= n2;
+      if (ay < 1) ay += n2;
+      if (az > n3) az -= n3;
+      if (az < 1) az += n3;
+    }
+    const int cx = ax < 0 ? 0 : (ax > n1 + 1 ? n1 + 1 : ax);
+    const int cy = ay < 0 ? 0 : (ay > n2 + 1 ? n2 + 1 : ay);
+    const int cz = az < 0 ? 0 : (az > n3 + 1 ? n3 + 1 : az);
+    if (cw[d.c(cx, cy, cz)] || ax < 1 || ax > n1 || ay < 1 || ay > n2 || az < 1 || az > n3) {
+      // lost at a wall (Src/part_expmover.f90:275-433): every cell outside
+      // 1..n has only wall nodes in a closed box; a cell inside 1..n is lost
+      // when all of its 8 nodes are walls
+      const double Eki = 0.5 * c.Nm * c.mass * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+      const int igrid = bcnd[d.g(cx, cy, cz)];
+      atomicAdd(&acc[0], Eki);
+      if (igrid >= 0 && igrid <= c.ngrid) {
+        atomicAdd(&acc[2 + 2 * igrid], 1.0);
+        atomicAdd(&acc[3 + 2 * igrid], Eki);
+      }
+      hole[k] = true;
+    } else {
+      (&c4.x)[k] = (ax - 1) + n1 * ((ay - 1) + n2 * (az - 1));
+      jx[k] = ax;
+      jy[k] = ay;
+      jz[k] = az;
+      gxs[k] = fx;
+      gys[k] = fy;
+      gzs[k] = fz;
+    }
+    (&P[0].x)[k] = fx;
+    (&P[1].x)[k] = fy;
+    (&P[2].x)[k] = fz;
+    (&P[3].x)[k] = vx;
+    (&P[4].x)[k] = vy;
+    (&P[5].x)[k] = vz;
+  }
+  // write back (a hole's slot is dead: what is written there is never read)
+  if (full4) {
+    *reinterpret_cast<int4 *>(cell + i0) = c4;
+#pragma unroll
+    for (int a = 0; a < 6; ++a) *reinterpret_cast<float4 *>(p + a * cap + i0) = P[a];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (in[k]) {
+        cell[i0 + k] = (&c4.x)[k];
+#pragma unroll
+        for (int a = 0; a < 6; ++a) p[a * cap + i0 + k] = (&P[a].x)[k];
+      }
+  }
+  // holes: flag 2 and a warp-aggregated append to the hole list
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (hole[k]) flag[i0 + k] = 2;
+    const unsigned hm = __ballot_sync(full, hole[k]);
+    if (hm) {
+      const int leader = __ffs(hm) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(nholes, __popc(hm));
+      base = __shfl_sync(full, base, leader);
+      if (hole[k]) holes[base + __popc(hm & lmask_lt())] = (int)(i0 + k);
+    }
+  }
+  // deposit: merge this lane's particles that end in its first particle's cell
+  int a0 = -1;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (a0 < 0 && jx[k] >= 0) a0 = k;
+  if (a0 < 0) return;
+  int wa[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int ax = jx[a0], ay = jy[a0], az = jz[a0];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (jx[k] < 0) continue;
+    int w[8];
+    qweights(gxs[k], gys[k], gzs[k], w);
+    if (jx[k] == ax && jy[k] == ay && jz[k] == az) {
+#pragma unroll
+      for (int cc = 0; cc < 8; ++cc) wa[cc] += w[cc];
+    } else {
+      deposit8(d, T, jx[k], jy[k], jz[k], d.g(jx[k], jy[k], jz[k]), w, c.kdep, kq, np);
+    }
+  }
+  deposit8(d, T, ax, ay, az, d.g(ax, ay, az), wa, c.kdep, kq, np);
+}
+
+// one block per tile: the particles [tile_off[t], tile_off[t+1]) of the last
+// sort, clipped to the current count
+__global__ void __launch_bounds__(MBK) k_push_deposit_tiles(
+    Dims d, MixedConst c, const float4 *__restrict__ E4, const int *__restrict__ bcnd,
+    const unsigned char *__restrict__ cw, int *__restrict__ cell, float *__restrict__ p, long long cap,
+    const int *__restrict__ count, signed char *__restrict__ flag, const int *__restrict__ tile_off,
+    const double *__restrict__ kq, double *__restrict__ np, int *__restrict__ holes, int *__restrict__ nholes,
+    double *__restrict__ acc, int *__restrict__ err) {
+  __shared__ int s_hi[TT], s_lo[TT];
+  const int t = blockIdx.x;
+  const int tx = t % c.ntx, ty = (t / c.ntx) % c.nty, tz = t / (c.ntx * c.nty);
+  Tile T{s_hi, s_lo, tx * TC, ty * TC, tz * TC};
+  for (int e = threadIdx.x; e < TT; e += MBK) {
+    s_hi[e] = 0;
+    s_lo[e] = 0;
+  }
+  __syncthreads();
+  const long long N = *count;
+  const long long lo = tile_off[t];
+  long long hi = tile_off[t + 1];
+  if (hi > N) hi = N;
+  const long long first = lo & ~3LL;
+  int chunks = 0;
+  for (long long base = first; base < hi; base += CHUNK) {
+    push_quad(d, c, T, base + 4 * threadIdx.x, lo, hi, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes,
+              nholes, acc, err);
+    if (++chunks == FLUSH_CHUNKS && base + CHUNK < hi) {
+      // keep the integer tile sums below 2^31 on very dense tiles
+      chunks = 0;
+      __syncthreads();
+      flush_tile(d, T, c.kdep, kq, np);
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  flush_tile(d, T, c.kdep, kq, np);
+}
+
+// particles past the last tile (appended since the sort), or all of them
+// when no sort has run: deposited straight into the FP64 grid
+__global__ void __launch_bounds__(MBK) k_push_deposit_tail(
+    Dims d, MixedConst c, const float4 *__restrict__ E4, const int *__restrict__ bcnd,
+    const unsigned char *__restrict__ cw, int *__restrict__ cell, float *__restrict__ p, long long cap,
+    const int *__restrict__ count, signed char *__restrict__ flag, const int *__restrict__ tile_off,
+    const double *__restrict__ kq, double *__restrict__ np, int *__restrict__ holes, int *__restrict__ nholes,
+    double *__restrict__ acc, int *__restrict__ err) {
+  const Tile T{nullptr, nullptr, 0, 0, 0};
+  const long long N = *count;
+  const long long lo = tile_off ? tile_off[c.ntiles] : 0;
+  const long long first = lo & ~3LL;
+  for (long long base = first + (long long)blockIdx.x * CHUNK; base < N; base += (long long)gridDim.x * CHUNK)
+    push_quad(d, c, T, base + 4 * threadIdx.x, lo, N, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes,
+              acc, err);
+}
+
+// hole filling for the mixed layout (the FP64 kernels of the same name in
+// step.cu do the same on the FP64 layout)
+__global__ void k_fillm_lists(const int *__restrict__ count, const int *__restrict__ holes,
+                              const signed char *__restrict__ flag, int *side, int *tailA, int *holeH) {
+  const int N = *count, L = side[0], Np = N - L;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < L; t += stride) {
+    const int tail = Np + (int)t;
+    if (flag[tail] != 2) tailA[atomicAdd(&side[1], 1)] = tail;
+    const int h = holes[t];
+    if (h < Np) holeH[atomicAdd(&side[2], 1)] = h;
+  }
+}
+
+__global__ void k_fillm_move(int *__restrict__ cell, float *__restrict__ p, long long cap,
+                             const int *__restrict__ count, signed char *__restrict__ flag, const int *side,
+                             const int *__restrict__ tailA, const int *__restrict__ holeH) {
+  const int N = *count, L = side[0], Np = N - L, na = side[1];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < na; t += stride) {
+    const long long src = tailA[t], dst = holeH[t];
+    cell[dst] = cell[src];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) p[a * cap + dst] = p[a * cap + src];
+    flag[dst] = 0;
+  }
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < L; t += stride)
+    flag[Np + t] = 0;
+}
+
+__global__ void k_fillm_count(int *count, const int *side) { *count = *count - side[0]; }
+
+// ---------------------------------------------------------------- sort
+// sort key: tile (x-fastest over tiles) * 512 + cell inside the tile
+__device__ __forceinline__ int tile_key(int cc, int n1, int n2, int ntx, int nty) {
+  const int cx = cc % n1, cy = (cc / n1) % n2, cz = cc / (n1 * n2);
+  const int tile = (cx / TC) + ntx * ((cy / TC) + nty * (cz / TC));
+  return tile * (TC * TC * TC) + (cx % TC) + TC * ((cy % TC) + TC * (cz % TC));
+}
+
+// run of equal keys among the lanes of the warp
+__device__ __forceinline__ void run_of(int key, bool &head, int &start, int &len) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int prev = __shfl_up_sync(full, key, 1);
+  head = (lane == 0) || (prev != key);
+  const unsigned heads = __ballot_sync(full, head);
+  start = 31 - __clz(heads & lmask_le());
+  const unsigned above = (start == 31) ? 0u : (heads & ~((2u << start) - 1u));
+  len = (above ? __ffs(above) - 1 : 32) - start;
+}
+
+__global__ void k_msort_hist(const int *__restrict__ cell, const int *__restrict__ count, int n1, int n2,
+                             int ntx, int nty, int *cnt) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int k = (i < *count) ? tile_key(cell[i], n1, n2, ntx, nty) : -1;
+  bool head;
+  int start, len;
+  run_of(k, head, start, len);
+  if (head && k >= 0) atomicAdd(&cnt[k], len);
+}
+
+__global__ void k_tile_offsets(const int *__restrict__ off, int ntiles, int *__restrict__ tile_off) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t <= ntiles) tile_off[t] = off[(long long)t * (TC * TC * TC)];
+}
+
+__global__ void k_msort_scatter(const int *__restrict__ cell, const float *__restrict__ p,
+                                int *__restrict__ cell_o, float *__restrict__ p_o, long long cap,
+                                const int *__restrict__ count, int n1, int n2, int ntx, int nty, int *cursor) {
+  const unsigned full = 0xffffffffu;
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int N = *count;
+  const int cc = (i < N) ? cell[i] : -1;
+  const int k = (i < N) ? tile_key(cc, n1, n2, ntx, nty) : -1;
+  bool head;
+  int start, len;
+  run_of(k, head, start, len);
+  int base = 0;
+  if (head && k >= 0) base = atomicAdd(&cursor[k], len);
+  base = __shfl_sync(full, base, start);
+  if (i < N) {
+    const long long j = base + ((threadIdx.x & 31) - start);
+    cell_o[j] = cc;
+#pragma unroll
+    for (int a = 0; a < 6; ++a) p_o[a * cap + j] = p[a * cap + i];
+  }
+}
+
+// E (3, nodes) FP64 -> one float4 (Ex, Ey, Ez, 0) per node
+__global__ void k_pack_e32(const double *__restrict__ Ei, float4 *__restrict__ E4, long long nodes) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < nodes) E4[i] = make_float4((float)Ei[3 * i], (float)Ei[3 * i + 1], (float)Ei[3 * i + 2], 0.f);
+}
+
+// FP64 SoA (x,y,z,vx,vy,vz) -> mixed layout
+__global__ void k_f64_to_mixed(Dims d, double h0, double h1, double h2, const double *__restrict__ pin,
+                               long long capin, int *__restrict__ cell, float *__restrict__ p,
+                               long long cap, long long n, int *err) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double x = pin[i], y = pin[capin + i], z = pin[2 * capin + i];
+  int ix = (int)(x / h0) + 1, iy = (int)(y / h1) + 1, iz = (int)(z / h2) + 1;
+  if (ix < 1 || ix > d.n1 || iy < 1 || iy > d.n2 || iz < 1 || iz > d.n3 || !(x >= 0 && y >= 0 && z >= 0)) {
+    raise_err(err, LEPIC_ERR_CELL, (int)i);
+    ix = ix < 1 ? 1 : (ix > d.n1 ? d.n1 : ix);
+    iy = iy < 1 ? 1 : (iy > d.n2 ? d.n2 : iy);
+    iz = iz < 1 ? 1 : (iz > d.n3 ? d.n3 : iz);
+  }
+  cell[i] = (ix - 1) + d.n1 * ((iy - 1) + d.n2 * (iz - 1));
+  const float fx = (float)(x / h0 - (ix - 1)), fy = (float)(y / h1 - (iy - 1)), fz = (float)(z / h2 - (iz - 1));
+  p[i] = fx >= 1.f ? 0.99999994f : fx;
+  p[cap + i] = fy >= 1.f ? 0.99999994f : fy;
+  p[2 * cap + i] = fz >= 1.f ? 0.99999994f : fz;
+  p[3 * cap + i] = (float)pin[3 * capin + i];
+  p[4 * cap + i] = (float)pin[4 * capin + i];
+  p[5 * cap + i] = (float)pin[5 * capin + i];
+}
+
+// mixed layout -> FP64 SoA (positions x = (ix-1+f) h)
+__global__ void k_mixed_to_f64(Dims d, double h0, double h1, double h2, const int *__restrict__ cell,
+                               const float *__restrict__ p, long long cap, double *__restrict__ pout,
+                               long long capout, long long n) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int cc = cell[i];
+  const int ix = cc % d.n1, iy = (cc / d.n1) % d.n2, iz = cc / (d.n1 * d.n2);
+  pout[i] = ((double)ix + (double)p[i]) * h0;
+  pout[capout + i] = ((double)iy + (double)p[cap + i]) * h1;
+  pout[2 * capout + i] = ((double)iz + (double)p[2 * cap + i]) * h2;
+  pout[3 * capout + i] = p[3 * cap + i];
+  pout[4 * capout + i] = p[4 * cap + i];
+  pout[5 * capout + i] = p[5 * cap + i];
+}
+
+bool aligned16(const void *q) { return ((uintptr_t)q & 15u) == 0; }
+
+int check_layout(const lepic_species_mixed_t &sp) {
+  if (sp.cap % 4 || !aligned16(sp.cell) || !aligned16(sp.p) || !aligned16(sp.cell_alt) || !aligned16(sp.p_alt) ||
+      ((uintptr_t)sp.flag_dead & 3u))
+    return LEPIC_ERR_ARG;
+  return LEPIC_OK;
+}
+
+}  // namespace
+
+int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_species_mixed_t &sp,
+                              int ptype, int ngrid, const lepic_phys_t &P, double *np, double *acc,
+                              int n_hint, cudaStream_t s) {
+  Dims d(g.n);
+  const int p = ptype - 1;
+  if (P.flag_nmn) return LEPIC_ERR_UNSUPPORTED;
+  if (!sp.flag_dead || !aligned16(E4)) return LEPIC_ERR_ARG;
+  if (int rc = check_layout(sp)) return rc;
+  MixedConst c;
+  memset(&c, 0, sizeof(c));
+  c.dth0 = (float)(P.dt / g.h[0]);
+  c.dth1 = (float)(P.dt / g.h[1]);
+  c.dth2 = (float)(P.dt / g.h[2]);
+  c.k1 = (float)(P.dt * P.charge[p] / (2.0 * P.mass[p]));
+  c.Bx = (float)P.Bconst[0];
+  c.By = (float)P.Bconst[1];
+  c.Bz = (float)P.Bconst[2];
+  c.boris = (P.flag_B == 1) ? 1 : 0;
+  if (P.flag_B_pos == 1 && P.charge[p] > 0.0) c.boris = 0;
+  c.flag_pbc = P.flag_pbc;
+  c.ngrid = ngrid;
+  c.Nm = P.Nm[p];
+  c.mass = P.mass[p];
+  c.kdep = P.Nm[p] / (g.h[0] * g.h[1] * g.h[2]);
+  c.ntx = (d.n1 + TC - 1) / TC;
+  c.nty = (d.n2 + TC - 1) / TC;
+  c.ntiles = LEPIC_TILES(g.n);
+  const size_t cap = (size_t)sp.cap;
+  char nm[32];
+  snprintf(nm, sizeof nm, "mixed_holes%d", p);
+  int *holes = (int *)scratch(nm, sizeof(int) * cap);
+  snprintf(nm, sizeof nm, "mixed_tail%d", p);
+  int *tailA = (int *)scratch(nm, sizeof(int) * cap);
+  snprintf(nm, sizeof nm, "mixed_hh%d", p);
+  int *holeH = (int *)scratch(nm, sizeof(int) * cap);
+  snprintf(nm, sizeof nm, "mixed_side%d", p);
+  int *side = (int *)scratch(nm, sizeof(int) * 4);
+  if (!holes || !tailA || !holeH || !side) return LEPIC_ERR_CUDA;
+  LEPIC_CUDA(cudaMemsetAsync(side, 0, sizeof(int) * 4, s));
+  const float4 *E = reinterpret_cast<const float4 *>(E4);
+  int t0 = timer_start("push_deposit_mixed", s);
+  if (sp.tile_off)
+    k_push_deposit_tiles<<<c.ntiles, MBK, 0, s>>>(d, c, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap, sp.count,
+                                                  sp.flag_dead, sp.tile_off, g.kq, np, holes, side, acc,
+                                                  ctx().d_err);
+  // the tail: at most what was appended since the sort unless never sorted
+  long long tail = sp.tile_off ? (long long)ctx().sms * 2 : grid_for(n_hint > 0 ? n_hint : sp.cap, CHUNK);
+  if (tail > (long long)ctx().sms * 8) tail = (long long)ctx().sms * 8;
+  k_push_deposit_tail<<<(int)tail, MBK, 0, s>>>(d, c, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap, sp.count,
+                                               sp.flag_dead, sp.tile_off, g.kq, np, holes, side, acc,
+                                               ctx().d_err);
+  timer_stop(t0, s);
+  LEPIC_CUDA(cudaGetLastError());
+  int t1 = timer_start("fill_holes_mixed", s);
+  const int fb = ctx().sms * 2;
+  k_fillm_lists<<<fb, 256, 0, s>>>(sp.count, holes, sp.flag_dead, side, tailA, holeH);
+  k_fillm_move<<<fb, 256, 0, s>>>(sp.cell, sp.p, sp.cap, sp.count, sp.flag_dead, side, tailA, holeH);
+  k_fillm_count<<<1, 1, 0, s>>>(sp.count, side);
+  timer_stop(t1, s);
+  LEPIC_CUDA(cudaGetLastError());
+  return LEPIC_OK;
+}
+
+int launch_sort_mixed(const lepic_grid_t &g, lepic_species_mixed_t &sp, int n_hint, cudaStream_t s) {
+  Dims d(g.n);
+  if (int rc = check_layout(sp)) return rc;
+  const int ntx = (d.n1 + TC - 1) / TC, nty = (d.n2 + TC - 1) / TC;
+  const int ntiles = LEPIC_TILES(g.n);
+  const long long nkeys = (long long)ntiles * TC * TC * TC;
+  int *cnt = (int *)scratch("msort_cnt", sizeof(int) * (size_t)(nkeys + 1));
+  if (!cnt) return LEPIC_ERR_CUDA;
+  LEPIC_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(nkeys + 1), s));
+  const int nthreads = n_hint > 0 ? n_hint : sp.cap;
+  int t0 = timer_start("sort_hist_mixed", s);
+  k_msort_hist<<<grid_for(nthreads, MBK), MBK, 0, s>>>(sp.cell, sp.count, d.n1, d.n2, ntx, nty, cnt);
+  timer_stop(t0, s);
+  int t1 = timer_start("sort_scan_mixed", s);
+  int rc = exclusive_scan_i32(cnt, cnt, nkeys + 1, s);
+  timer_stop(t1, s);
+  if (rc) return rc;
+  if (sp.tile_off) k_tile_offsets<<<grid_for(ntiles + 1, 256), 256, 0, s>>>(cnt, ntiles, sp.tile_off);
+  int t2 = timer_start("sort_scatter_mixed", s);
+  k_msort_scatter<<<grid_for(nthreads, MBK), MBK, 0, s>>>(sp.cell, sp.p, sp.cell_alt, sp.p_alt, sp.cap,
+                                                          sp.count, d.n1, d.n2, ntx, nty, cnt);
+  timer_stop(t2, s);
+  LEPIC_CUDA(cudaGetLastError());
+  int *tc = sp.cell;
+  sp.cell = sp.cell_alt;
+  sp.cell_alt = tc;
+  float *tp = sp.p;
+  sp.p = sp.p_alt;
+  sp.p_alt = tp;
+  return LEPIC_OK;
+}
+
+int launch_pack_e32(const double *Ei, float *E4, long long nodes, cudaStream_t s) {
+  if (!aligned16(E4)) return LEPIC_ERR_ARG;
+  k_pack_e32<<<grid_for(nodes, 256), 256, 0, s>>>(Ei, reinterpret_cast<float4 *>(E4), nodes);
+  LEPIC_CUDA(cudaGetLastError());
+  return LEPIC_OK;
+}
+
+int launch_convert_f64_to_mixed(const lepic_grid_t &g, const lepic_species_f64_t &in, lepic_species_mixed_t &out,
+                                long long n, cudaStream_t s) {
+  Dims d(g.n);
+  if (n > out.cap) return LEPIC_ERR_CAPACITY;
+  if (n > 0)
+    k_f64_to_mixed<<<grid_for(n, 256), 256, 0, s>>>(d, g.h[0], g.h[1], g.h[2], in.p, in.cap, out.cell, out.p,
+                                                   out.cap, n, ctx().d_err);
+  int nn = (int)n;
+  LEPIC_CUDA(cudaMemcpyAsync(out.count, &nn, sizeof(int), cudaMemcpyHostToDevice, s));
+  if (out.tile_off) LEPIC_CUDA(cudaMemsetAsync(out.tile_off, 0, sizeof(int) * (LEPIC_TILES(g.n) + 1), s));
+  return check_err(s);
+}
+
+int launch_convert_mixed_to_f64(const lepic_grid_t &g, const lepic_species_mixed_t &in, double *out,
+                                long long capout, long long n, cudaStream_t s) {
+  Dims d(g.n);
+  if (n > 0)
+    k_mixed_to_f64<<<grid_for(n, 256), 256, 0, s>>>(d, g.h[0], g.h[1], g.h[2], in.cell, in.p, in.cap, out,
+                                                   capout, n);
+  LEPIC_CUDA(cudaGetLastError());
+  return LEPIC_OK;
+}
+
+}  // namespace lepic
+
+extern "C" {
+
+int lepic_dev_push_deposit_mixed(const lepic_grid_t *g, const float *E4, lepic_species_mixed_t *s,
+                                 int ptype, int ngrid, const lepic_phys_t *P, double *np, double *acc,
+                                 int n_hint, void *stream) {
+  if (!g || !s || !P || ptype < 1 || !acc || !E4 || !np) return LEPIC_ERR_ARG;
+  return lepic::launch_push_deposit_mixed(*g, E4, *s, ptype, ngrid, *P, np, acc, n_hint, (cudaStream_t)stream);
+}
+
+int lepic_dev_sort_mixed(const lepic_grid_t *g, lepic_species_mixed_t *s, int n_hint, void *stream) {
+  if (!g || !s) return LEPIC_ERR_ARG;
+  return lepic::launch_sort_mixed(*g, *s, n_hint, (cudaStream_t)stream);
+}
+
+int lepic_dev_pack_e32(const double *Ei, float *E4, long long nodes, void *stream) {
+  if (!Ei || !E4 || nodes < 0) return LEPIC_ERR_ARG;
+  return lepic::launch_pack_e32(Ei, E4, nodes, (cudaStream_t)stream);
+}
+
+int lepic_dev_f64_to_mixed(const lepic_grid_t *g, const lepic_species_f64_t *in, lepic_species_mixed_t *out,
+                           long long n, void *stream) {
+  if (!g || !in || !out || n < 0) return LEPIC_ERR_ARG;
+  return lepic::launch_convert_f64_to_mixed(*g, *in, *out, n, (cudaStream_t)stream);
+}
+
+int lepic_dev_mixed_to_f64(const lepic_grid_t *g, const lepic_species_mixed_t *in, double *out,
+                           long long capout, long long n, void *stream) {
+  if (!g || !in || !out || n < 0) return LEPIC_ERR_ARG;
+  return lepic::launch_convert_mixed_to_f64(*g, *in, out, capout, n, (cudaStream_t)stream);
+}
+
+}  // extern "C"

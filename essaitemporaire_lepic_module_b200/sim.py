@@ -1,4 +1,4 @@
-"""Device-resident PIC-MCC time stepping on one B200 (FP64 form).
+"""Device-resident PIC-MCC time stepping on one B200 (FP64 and mixed forms).
 
 ``Simulation`` keeps every array of the hot path in HBM (torch tensors used
 as plain device buffers) and advances the legacy timestep of
@@ -15,6 +15,12 @@ Layout in HBM (reference index bases, column-major like the Fortran arrays):
     particles per species  SoA (6, cap) float64 = x, y, z, vx, vy, vz
                            + second buffer (sort target), int32 keys,
                            int8 dead flags, device int32 count
+
+Mixed form (precision="mixed"): particles are int32 cell + (6, cap) float32
+= fx, fy, fz (in-cell offsets), vx, vy, vz (28 B instead of 48 B), the push
+reads an FP32 copy E32 of the field, and the Poisson solve is FP32 V-cycles
+inside FP64 iterative refinement to the same residual tolerance.  rho, phi,
+E and the charge grids stay FP64.
 """
 from __future__ import annotations
 
@@ -24,7 +30,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import LepicGrid, LepicSpeciesF64, LepicTables, check, lib, phys_struct
+from ._lib import (LepicGrid, LepicSpeciesF64, LepicSpeciesMixed, LepicTables, check, lib,
+                   phys_struct)
 
 
 def _ptr(t):
@@ -65,11 +72,56 @@ class Species:
         return self.p[:, :n].t().contiguous().cpu().numpy()
 
 
+def tiles_of(n):
+    """Number of 8x8x8-cell tiles the mixed sort orders particles by."""
+    return ((n[0] + 7) // 8) * ((n[1] + 7) // 8) * ((n[2] + 7) // 8)
+
+
+class SpeciesMixed:
+    """One species' mixed-precision particle store (cell + FP32 planes)."""
+
+    def __init__(self, cap, device, n):
+        self.cap = (int(cap) + 3) // 4 * 4
+        self.cell = torch.zeros(self.cap, dtype=torch.int32, device=device)
+        self.p = torch.zeros((6, self.cap), dtype=torch.float32, device=device)
+        self.cell_alt = torch.zeros(self.cap, dtype=torch.int32, device=device)
+        self.p_alt = torch.zeros((6, self.cap), dtype=torch.float32, device=device)
+        self.count = torch.zeros(1, dtype=torch.int32, device=device)
+        self.flag_dead = torch.zeros(self.cap, dtype=torch.int8, device=device)
+        self.tile_off = torch.zeros(tiles_of(n) + 1, dtype=torch.int32, device=device)
+        self.s = LepicSpeciesMixed()
+        self._sync_struct()
+
+    def _sync_struct(self):
+        s = self.s
+        s.cell, s.p = self.cell.data_ptr(), self.p.data_ptr()
+        s.cell_alt, s.p_alt = self.cell_alt.data_ptr(), self.p_alt.data_ptr()
+        s.count, s.flag_dead, s.cap = self.count.data_ptr(), self.flag_dead.data_ptr(), self.cap
+        s.tile_off = self.tile_off.data_ptr()
+
+    def after_call(self):
+        if self.s.p != self.p.data_ptr():
+            self.p, self.p_alt = self.p_alt, self.p
+            self.cell, self.cell_alt = self.cell_alt, self.cell
+        self._sync_struct()
+
+    def n(self):
+        return int(self.count.item())
+
+
 class Simulation:
     def __init__(self, st, cap=None, device="cuda", seed=123456, nsort=None, ns_coll=None,
-                 fused=True):
+                 fused=True, precision="f64", mg_mixed=None):
+        if precision not in ("f64", "mixed"):
+            raise ValueError(f"precision must be 'f64' or 'mixed', not {precision!r}")
         self.st = st
-        self.fused = fused
+        self.mixed = precision == "mixed"
+        self.precision = precision
+        self.fused = fused or self.mixed
+        # FP32 V-cycle parameters of the mixed Poisson solve
+        self.mg_mixed = dict(max_refine=60, nu_pre=2, nu_post=2, coarse_sweeps=32, omega=1.0)
+        if mg_mixed:
+            self.mg_mixed.update(mg_mixed)
         self._acc = None
         self.dev = torch.device(device)
         self.stream = torch.cuda.current_stream(self.dev)
@@ -99,7 +151,12 @@ class Simulation:
                                         C.c_void_p(self.cw.data_ptr()), self._s()), "cell_wall")
         if cap is None:
             cap = int(st.n_particles() * 1.25) + 1024
-        self.sp = [Species(cap, self.dev) for _ in range(st.ntype)]
+        self.cap = cap
+        if self.mixed:
+            self.sp = [SpeciesMixed(cap, self.dev, st.n) for _ in range(st.ntype)]
+            self.E32 = torch.zeros(tuple(g.bcnd.shape) + (4,), dtype=torch.float32, device=self.dev)
+        else:
+            self.sp = [Species(cap, self.dev) for _ in range(st.ntype)]
         self.sp_arr = (LepicSpeciesF64 * max(st.ntype, 1))()
         self.it = 0
         self.p_mac = np.zeros((st.geom.ngrid + 1, 2, st.ntype))
@@ -137,10 +194,22 @@ class Simulation:
         self._tables = t
 
     # ----------------------------------------------------------- loading
+    def _f64_stage(self):
+        """FP64 species stores the mixed form loads through."""
+        return [Species(self.cap, self.dev) for _ in range(self.st.ntype)]
+
+    def _adopt_f64(self, f64):
+        """Convert FP64 species (positions x, y, z) into the mixed stores."""
+        for s64, sm in zip(f64, self.sp):
+            n = s64.n()
+            check(lib().lepic_dev_f64_to_mixed(C.byref(self.grid), C.byref(s64.s), C.byref(sm.s),
+                                               C.c_longlong(n), self._s()), "f64_to_mixed")
+
     def load_from_host(self, vxp, np_tot, np_grids=None):
         """Initial state from host arrays in the reference layout
         (vxp (ntype, nmax, 6), np_tot, np grids)."""
-        for p, s in enumerate(self.sp):
+        dst = self._f64_stage() if self.mixed else self.sp
+        for p, s in enumerate(dst):
             n = int(np_tot[p])
             assert n <= s.cap
             s.p[:, :n] = torch.as_tensor(np.ascontiguousarray(vxp[p, :n, :].T), device=self.dev)
@@ -148,16 +217,35 @@ class Simulation:
         if np_grids is not None:
             self.np.copy_(torch.as_tensor(np.ascontiguousarray(np_grids), device=self.dev))
         else:
-            self.deposit()
+            self._deposit_f64(dst)
+        if self.mixed:
+            self._adopt_f64(dst)
 
     def load_uniform(self, n_per_species=None, seed=None):
         """GPU Philox loader + initial deposition."""
         n = self.st.n_particles() if n_per_species is None else int(n_per_species)
-        arr = (LepicSpeciesF64 * len(self.sp))(*[s.s for s in self.sp])
-        check(lib().lepic_dev_load_uniform(C.byref(self.grid), arr, len(self.sp), C.c_longlong(n),
+        dst = self._f64_stage() if self.mixed else self.sp
+        arr = (LepicSpeciesF64 * len(dst))(*[s.s for s in dst])
+        check(lib().lepic_dev_load_uniform(C.byref(self.grid), arr, len(dst), C.c_longlong(n),
                                            C.byref(self.P), C.c_ulonglong(seed or self.seed),
                                            self._s()), "load_uniform")
-        self.deposit()
+        self._deposit_f64(dst)
+        if self.mixed:
+            self._adopt_f64(dst)
+            del dst
+            torch.cuda.empty_cache()
+
+    def particles_f64(self, p):
+        """Species p as FP64 (6, n) x, y, z, vx, vy, vz on the device."""
+        s = self.sp[p]
+        n = s.n()
+        if not self.mixed:
+            return s.p[:, :n]
+        out = torch.empty((6, max(n, 1)), dtype=torch.float64, device=self.dev)
+        check(lib().lepic_dev_mixed_to_f64(C.byref(self.grid), C.byref(s.s), _ptr(out),
+                                           C.c_longlong(out.shape[1]), C.c_longlong(n), self._s()),
+              "mixed_to_f64")
+        return out[:, :n]
 
     # ----------------------------------------------------------- kernels
     def calc_rho(self):
@@ -165,6 +253,8 @@ class Simulation:
                                        self.st.ntype, C.byref(self.P), self._s()), "calc_rho")
 
     def pdesolver(self, eps=None, omega=None, ng=None, ncycl=None):
+        if self.mixed:
+            return self.pdesolver_mixed(eps=eps, ng=ng)
         wl = self.st.wl
         k = C.c_int(0)
         ktot = C.c_double(0)
@@ -179,11 +269,40 @@ class Simulation:
         self.mg_last = (k.value, ktot.value, res.value)
         return self.mg_last
 
+    def pdesolver_mixed(self, eps=None, ng=None, **kw):
+        """FP32 V-cycles inside FP64 refinement; returns (refinements, 0, res)."""
+        wl = self.st.wl
+        m = dict(self.mg_mixed)
+        m.update(kw)
+        it = C.c_int(0)
+        res = C.c_double(0)
+        check(lib().lepic_dev_pdesolver_mixed(C.byref(self.grid), _ptr(self.phi), _ptr(self.rhs),
+                                              wl.eps if eps is None else eps, m["omega"],
+                                              self.st.ng if ng is None else ng, C.byref(self.P),
+                                              m["max_refine"], m["nu_pre"], m["nu_post"],
+                                              m["coarse_sweeps"], C.byref(it), C.byref(res),
+                                              self._s()), "pdesolver_mixed")
+        self.mg_last = (it.value, 0.0, res.value)
+        return self.mg_last
+
     def efield(self):
         check(lib().lepic_dev_calc_efield(C.byref(self.grid), _ptr(self.phi), _ptr(self.Ei),
                                           self._s()), "calc_efield")
+        if self.mixed:
+            self.pack_e32()
+
+    def pack_e32(self):
+        """FP32 copy of the current E (one float4 per node) for the mixed push."""
+        check(lib().lepic_dev_pack_e32(_ptr(self.Ei), _ptr(self.E32), C.c_longlong(self.Ei.numel() // 3),
+                                       self._s()), "pack_e32")
 
     def sort(self):
+        if self.mixed:
+            for s in self.sp:
+                check(lib().lepic_dev_sort_mixed(C.byref(self.grid), C.byref(s.s), self._hint(s),
+                                                 self._s()), "sort_mixed")
+                s.after_call()
+            return
         pl_max = self.st.n[0] + self.st.n[0] * (self.st.n[1] + self.st.n[1] * self.st.n[2]) + 1
         if not hasattr(self, "_plist") or self._plist.numel() < pl_max + 1:
             self._plist = torch.zeros(pl_max + 1, dtype=torch.int32, device=self.dev)
@@ -195,12 +314,16 @@ class Simulation:
     def collisions(self):
         if self._tables is None:
             return
-        arr = (LepicSpeciesF64 * len(self.sp))(*[s.s for s in self.sp])
         nu = (C.c_double * 10)()
         cnt = (C.c_longlong * 64)()
-        check(lib().lepic_dev_collisions(C.byref(self.grid), arr, len(self.sp), C.byref(self._tables),
-                                         C.byref(self.P), C.c_ulonglong(self.seed),
-                                         C.c_ulonglong(self.it), nu, cnt, self._s()), "collisions")
+        if self.mixed:
+            arr = (LepicSpeciesMixed * len(self.sp))(*[s.s for s in self.sp])
+            fn, name = lib().lepic_dev_collisions_mixed, "collisions_mixed"
+        else:
+            arr = (LepicSpeciesF64 * len(self.sp))(*[s.s for s in self.sp])
+            fn, name = lib().lepic_dev_collisions, "collisions"
+        check(fn(C.byref(self.grid), arr, len(self.sp), C.byref(self._tables), C.byref(self.P),
+                 C.c_ulonglong(self.seed), C.c_ulonglong(self.it), nu, cnt, self._s()), name)
         self.counts[:64] += np.array(cnt[:], dtype=np.int64)
         self.nu_max[:] = nu[:]
 
@@ -218,8 +341,13 @@ class Simulation:
         self.P_loss += pl
 
     def deposit(self):
+        if self.mixed:
+            raise RuntimeError("the mixed form deposits inside the fused push (move_deposit)")
+        self._deposit_f64(self.sp)
+
+    def _deposit_f64(self, sps):
         self.np.zero_()
-        for p, s in enumerate(self.sp):
+        for p, s in enumerate(sps):
             check(lib().lepic_dev_charge_deposition(C.byref(self.grid), C.byref(s.s), p + 1,
                                                     C.byref(self.P), C.c_void_p(self.np[p].data_ptr()),
                                                     self._s()), "charge_deposition")
@@ -235,6 +363,13 @@ class Simulation:
         self.np.zero_()
         for p, s in enumerate(self.sp):
             if st.charge[p] == 0.0:
+                continue
+            if self.mixed:
+                check(lib().lepic_dev_push_deposit_mixed(
+                    C.byref(self.grid), _ptr(self.E32), C.byref(s.s), p + 1, st.geom.ngrid,
+                    C.byref(self.P), C.c_void_p(self.np[p].data_ptr()),
+                    C.c_void_p(self._acc[p].data_ptr()), int(counts[p]), self._s()),
+                    "push_deposit_mixed")
                 continue
             check(lib().lepic_dev_push_deposit(C.byref(self.grid), _ptr(self.Ei), C.byref(s.s), p + 1,
                                                st.geom.ngrid, C.byref(self.P),
@@ -272,6 +407,9 @@ class Simulation:
         else:
             self.move()
             self.deposit()
+
+    def _hint(self, s):
+        return int(s.count.item())
 
     def counts_host(self):
         return np.array([s.n() for s in self.sp])

@@ -212,6 +212,32 @@ typedef struct {
   int cap;
 } lepic_species_f64_t;
 
+/* One species in the mixed-precision layout (28 B per particle): cell[i] =
+ * (ix-1) + n1((iy-1) + n2(iz-1)) with ix = INT(x/h)+1, and p[a*cap + i] for
+ * a = fx, fy, fz (in-cell offsets in [0,1), x = (ix-1+fx) h) and vx, vy, vz
+ * (m/s), all FP32.  *_alt: sort targets of the same size.  cap must be a
+ * multiple of 4 and the arrays 16-byte aligned (the push moves particles in
+ * groups of four).  The sort orders particles by 8x8x8-cell tiles (cells in
+ * x-fastest order inside a tile, tiles in x-fastest order) and writes the
+ * particle offset of every tile to tile_off (device int[LEPIC_TILES(n)+1],
+ * zero-filled by the caller before the first sort); the push deposits each
+ * tile's particles through an on-chip node tile. */
+typedef struct {
+  int *cell;
+  float *p;
+  int *cell_alt;
+  float *p_alt;
+  int *count;             /* device int                                       */
+  signed char *flag_dead; /* device int8[cap]                                 */
+  int *tile_off;          /* device int[LEPIC_TILES(n)+1]                     */
+  int cap;
+} lepic_species_mixed_t;
+
+/* Number of 8x8x8-cell tiles of an n[3] grid. */
+#define LEPIC_TILE_CELLS 8
+#define LEPIC_TILES(n)                                                        \
+  ((((n)[0] + 7) / 8) * (((n)[1] + 7) / 8) * (((n)[2] + 7) / 8))
+
 /* Src/calc_rho.f90:1 on device grids (nproc = 1). */
 int lepic_dev_calc_rho(const lepic_grid_t *g, double *np, double *rhs, int ntype,
                        const lepic_phys_t *P, void *stream);
@@ -262,6 +288,46 @@ int lepic_dev_part_mover(const lepic_grid_t *g, const double *Ei, lepic_species_
 int lepic_dev_push_deposit(const lepic_grid_t *g, const double *Ei, lepic_species_f64_t *s,
                            int ptype, int ngrid, const lepic_phys_t *P, double *np, double *acc,
                            int n_hint, void *stream);
+
+/* Mixed-precision counterpart of lepic_dev_push_deposit (same reference
+ * lines): FP32 gather from E4 (one float4 Ex,Ey,Ez,0 per node, (n+3)^3
+ * nodes, from lepic_dev_pack_e32), FP32 Boris, position update on the
+ * in-cell offset, CIC weights of the new position quantized to 2^-24 (each
+ * particle deposits exactly 1) and summed exactly in integers per sorted
+ * tile on chip, then added into the FP64 grid np.  Requires a closed box
+ * (cells outside 1..n are walls).  n_hint: an upper bound of the count, used
+ * only before the first sort (<= 0: capacity). */
+int lepic_dev_push_deposit_mixed(const lepic_grid_t *g, const float *E4, lepic_species_mixed_t *s,
+                                 int ptype, int ngrid, const lepic_phys_t *P, double *np, double *acc,
+                                 int n_hint, void *stream);
+/* Src/sorting.f90:97-258 for the mixed layout: counting sort on the stored
+ * cell in tile order (swaps the buffers inside *s, writes s->tile_off). */
+int lepic_dev_sort_mixed(const lepic_grid_t *g, lepic_species_mixed_t *s, int n_hint, void *stream);
+/* E4[i] = (float)Ei(1:3, i), 0 for the nodes i < nodes (FP32 field of the
+ * mixed push; E4 16-byte aligned). */
+int lepic_dev_pack_e32(const double *Ei, float *E4, long long nodes, void *stream);
+/* Layout conversions FP64 SoA <-> mixed (n particles). */
+int lepic_dev_f64_to_mixed(const lepic_grid_t *g, const lepic_species_f64_t *in, lepic_species_mixed_t *out,
+                           long long n, void *stream);
+int lepic_dev_mixed_to_f64(const lepic_grid_t *g, const lepic_species_mixed_t *in, double *out,
+                           long long capout, long long n, void *stream);
+/* Mixed-precision Poisson solve for the operator of Src/pdesolver.f90:1
+ * (Dirichlet walls): FP64 residual r = b - A u, FP32 multigrid V-cycle on
+ * A e = r (nu_pre / nu_post red-black sweeps per level, coarse_sweeps on the
+ * coarsest), u += e in FP64, until sum|r| / alpha < eps, with the sum over
+ * plasma nodes and the alpha of the reference's exit test (or max_refine
+ * refinements).  One cooperative launch.  iters: refinements done; res: the
+ * final sum|r| / alpha. */
+int lepic_dev_pdesolver_mixed(const lepic_grid_t *g, double *u, const double *b, double eps,
+                              double omega, int ng, const lepic_phys_t *P, int max_refine,
+                              int nu_pre, int nu_post, int coarse_sweeps, int *iters, double *res,
+                              void *stream);
+/* lepic_dev_collisions for species in the mixed layout (same physics; the
+ * post-collision velocities are stored in FP32). */
+int lepic_dev_collisions_mixed(const lepic_grid_t *g, lepic_species_mixed_t *sp, int ntype,
+                               const lepic_tables_t *T, const lepic_phys_t *P, unsigned long long seed,
+                               unsigned long long call_index, double *nu_max, long long *counts,
+                               void *stream);
 
 /* Src/part_expmover.f90:570-686 for one species, accumulating into np
  * (device grid of that species). */
