@@ -22,8 +22,12 @@ LIB = os.path.join(HERE, "liblepic_gpu.so")
 SOURCES = ["context.cu", "timing.cu", "fields.cu", "mg.cu", "particles.cu", "step.cu", "mcc.cu", "mixed.cu", "mgmixed.cu",
            "capi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=default", "--expt-relaxed-constexpr"]
+# The FP64 kernels keep the reference's operation order bit for bit, so no
+# multiply-add contraction; the mixed-precision kernels have no bit-parity
+# contract and use fused multiply-adds.
+FMAD = {"mixed.cu": "--fmad=true", "mgmixed.cu": "--fmad=true"}
 
 
 def nvcc():
@@ -50,7 +54,7 @@ def build(force=False, verbose=False):
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(o)
         if force or not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(s), hdr_t):
-            jobs.append([exe, *ARCH, *FLAGS, "-c", s, "-o", o])
+            jobs.append([exe, *ARCH, *FLAGS, FMAD.get(src, "--fmad=false"), "-c", s, "-o", o])
 
     def run(cmd):
         if verbose:

@@ -49,7 +49,6 @@ struct MCCConst {
   int ixl[LEPIC_NM_RG], ixr[LEPIC_NM_RG], iyl, iyr, izl, izr;
   double w_rg[LEPIC_NM_RG];     // 1 / np_tot_rg(ptype, i_rg)
   double h0, h1, h2;
-  int n1, n2;
 };
 
 // FP64 SoA layout
@@ -121,9 +120,9 @@ struct AccMixed {
   }
   __device__ void cell_of(const MCCConst &c, int P, long long i, int &ix, int &iy, int &iz) const {
     const int cc = cell[P][i];
-    ix = cc % c.n1 + 1;
-    iy = (cc / c.n1) % c.n2 + 1;
-    iz = cc / (c.n1 * c.n2) + 1;
+    ix = (cc & (LEPIC_CELL_MAX - 1)) + 1;
+    iy = ((cc >> LEPIC_CELL_BITS) & (LEPIC_CELL_MAX - 1)) + 1;
+    iz = (cc >> (2 * LEPIC_CELL_BITS)) + 1;
   }
 };
 
@@ -363,7 +362,6 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
   for (int p = 0; p < ntype; ++p)
     LEPIC_CUDA(cudaMemcpyAsync(&Nh[p], counts_dev[p], sizeof(int), cudaMemcpyDeviceToHost, s));
   LEPIC_CUDA(cudaStreamSynchronize(s));
-  const Dims d(g.n);
   for (int p = 1; p <= ntype; ++p) {
     nu_max[p - 1] = 0.0;
     const int pn = T.p_ncol[p - 1];
@@ -376,8 +374,6 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
     c.qe = P.qe;
     c.pi = P.pi;
     c.m_p = fabs(P.mass[p - 1]);
-    c.n1 = d.n1;
-    c.n2 = d.n2;
     for (int q = 0; q < LEPIC_NPART; ++q) {
       c.mass[q] = P.mass[q];
       c.vt0[q] = P.vt0[q];

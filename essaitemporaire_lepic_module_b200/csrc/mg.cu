@@ -79,52 +79,64 @@ __device__ double block_sum(double v, double *sh) {
   return r;
 }
 
-// one colour of a red-black sweep, items [t0, items) strided by `stride`
+// Warps that share a loop: warp gw of nw (the whole grid or block 0).
+struct Warps {
+  int gw, nw;
+};
+__device__ __forceinline__ Warps grid_warps() {
+  return {(int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), (int)((gridDim.x * blockDim.x) >> 5)};
+}
+__device__ __forceinline__ Warps block_warps() { return {(int)(threadIdx.x >> 5), (int)(blockDim.x >> 5)}; }
+
+// The grid rows (j, k), j in [j0, j0 + nj), k in [k0, k0 + nk), dealt
+// round-robin to the warps; body(j, k) runs on all 32 lanes of the warp, which
+// split the row along i (coalesced, one 32-bit division per row).
+template <class F>
+__device__ __forceinline__ void for_rows(const Warps &w, int j0, int nj, int k0, int nk, F &&body) {
+  const int rows = nj * nk;
+  for (int r = w.gw; r < rows; r += w.nw) {
+    const int kk = r / nj;
+    body(j0 + (r - kk * nj), k0 + kk);
+  }
+}
+
+// one colour of a red-black sweep
 // colour 0 = red ((i+j+k) odd), 1 = black (Src/sors.f90:87-106, 249-267)
-__device__ __forceinline__ void sweep_colour(const MGLev &L, double omega, int colour, long long t0,
-                                             long long stride) {
-  const long long half = (L.n1 + 2) / 2;  // ceil((n1+1)/2)
-  const long long rows = (long long)(L.n2 + 1) * (L.n3 + 1);
-  const long long items = rows * half;
+__device__ __forceinline__ void sweep_colour(const MGLev &L, double omega, int colour, const Warps &w) {
+  const int lane = threadIdx.x & 31;
   const long long sy = L.N1, sz = L.N1 * L.N2;
-  for (long long t = t0; t < items; t += stride) {
-    long long row = t / half;
-    int ii = (int)(t - row * half);
-    int j = 1 + (int)(row % (L.n2 + 1));
-    int k = 1 + (int)(row / (L.n2 + 1));
+  for_rows(w, 1, L.n2 + 1, 1, L.n3 + 1, [&](int j, int k) {
     int ks = (k % 2 == 0) ? 0 : 1;
     int is;
     if (colour == 0) is = (j % 2 == 0) ? 1 : 2;
     else is = (j % 2 == 0) ? 2 : 1;
     is = is + ks;
     if (is > 2) is = 1;
-    int i = is + 2 * ii;
-    if (i > L.n1 + 1) continue;
-    long long q = L.g(i, j, k);
-    if (L.bc[q] > 0) continue;
-    double tt = L.b[L.r(i, j, k)] - L.aw * L.u[q - 1] - L.an * L.u[q + sy] - L.as * L.u[q - sy] -
-                L.ae * L.u[q + 1] - L.at * L.u[q + sz] - L.ab * L.u[q - sz];
-    L.u[q] = (1.0 - omega) * L.u[q] + omega * tt / L.ac;
-  }
+    for (int i = is + 2 * lane; i <= L.n1 + 1; i += 64) {
+      long long q = L.g(i, j, k);
+      if (L.bc[q] > 0) continue;
+      double tt = L.b[L.r(i, j, k)] - L.aw * L.u[q - 1] - L.an * L.u[q + sy] - L.as * L.u[q - sy] -
+                  L.ae * L.u[q + 1] - L.at * L.u[q + sz] - L.ab * L.u[q - sz];
+      L.u[q] = (1.0 - omega) * L.u[q] + omega * tt / L.ac;
+    }
+  });
 }
 
-// sum of |residual| over plasma nodes handled by this thread
-__device__ __forceinline__ double residual_part(const MGLev &L, long long t0, long long stride) {
-  const long long nx = L.n1 + 1, ny = L.n2 + 1;
-  const long long tot = L.nodes();
+// sum of |residual| over the plasma nodes of this thread's rows
+__device__ __forceinline__ double residual_part(const MGLev &L, const Warps &w) {
+  const int lane = threadIdx.x & 31;
   const long long sy = L.N1, sz = L.N1 * L.N2;
   double acc = 0.0;
-  for (long long t = t0; t < tot; t += stride) {
-    int i = 1 + (int)(t % nx);
-    int j = 1 + (int)((t / nx) % ny);
-    int k = 1 + (int)(t / (nx * ny));
-    long long q = L.g(i, j, k);
-    if (L.bc[q] != -1) continue;
-    double rij = L.b[L.r(i, j, k)] - (L.aw * L.u[q - 1] + L.an * L.u[q + sy] + L.as * L.u[q - sy] +
-                                      L.ae * L.u[q + 1] + L.ac * L.u[q] + L.at * L.u[q + sz] +
-                                      L.ab * L.u[q - sz]);
-    acc += fabs(rij);
-  }
+  for_rows(w, 1, L.n2 + 1, 1, L.n3 + 1, [&](int j, int k) {
+    for (int i = 1 + lane; i <= L.n1 + 1; i += 32) {
+      long long q = L.g(i, j, k);
+      if (L.bc[q] != -1) continue;
+      double rij = L.b[L.r(i, j, k)] - (L.aw * L.u[q - 1] + L.an * L.u[q + sy] + L.as * L.u[q - sy] +
+                                        L.ae * L.u[q + 1] + L.ac * L.u[q] + L.at * L.u[q + sz] +
+                                        L.ab * L.u[q - sz]);
+      acc += fabs(rij);
+    }
+  });
   return acc;
 }
 
@@ -138,12 +150,13 @@ __device__ void sor_rb(const MGArgs &a, const MGLev &L, int kmg, int dig, double
     if (blockIdx.x == 0) {
       double res_s = 0.0, res = 0.0;
       int ksor = 0;
+      const Warps w = block_warps();
       for (long long l = 1; l <= nr; ++l) {
-        sweep_colour(L, a.omega, 0, threadIdx.x, blockDim.x);
+        sweep_colour(L, a.omega, 0, w);
         __syncthreads();
-        sweep_colour(L, a.omega, 1, threadIdx.x, blockDim.x);
+        sweep_colour(L, a.omega, 1, w);
         __syncthreads();
-        res = block_sum(residual_part(L, threadIdx.x, blockDim.x), sh);
+        res = block_sum(residual_part(L, w), sh);
         ksor++;
         bool stop = (dig == 0) ? (res <= eps_abs) : (res_s > 0.0 && (res / res_s) <= eta);
         if (stop) break;
@@ -161,16 +174,15 @@ __device__ void sor_rb(const MGArgs &a, const MGLev &L, int kmg, int dig, double
     grid.sync();  // everyone has read shared_d before it is reused
     return;
   }
-  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long stride = (long long)gridDim.x * blockDim.x;
+  const Warps w = grid_warps();
   double res_s = 0.0, res = 0.0;
   int ksor = 0;
   for (long long l = 1; l <= nr; ++l) {
-    sweep_colour(L, a.omega, 0, tid, stride);
+    sweep_colour(L, a.omega, 0, w);
     grid.sync();
-    sweep_colour(L, a.omega, 1, tid, stride);
+    sweep_colour(L, a.omega, 1, w);
     grid.sync();
-    double part = block_sum(residual_part(L, tid, stride), sh);
+    double part = block_sum(residual_part(L, w), sh);
     if (threadIdx.x == 0) a.partial[blockIdx.x] = part;
     grid.sync();
     // every block sums the partials in the same fixed order
@@ -206,22 +218,18 @@ __device__ __forceinline__ int fmap(int ic, int ncell) {
 
 // Src/mg.f90:248-805 (restriction), fine F -> coarse C
 __device__ void restriction(const MGLev &F, const MGLev &C, cg::grid_group &grid) {
-  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  {
-    const long long nx = F.n1 + 1, ny = F.n2 + 1, tot = F.nodes();
-    for (long long t = tid; t < tot; t += stride) {
-      int i = 1 + (int)(t % nx), j = 1 + (int)((t / nx) % ny), k = 1 + (int)(t / (nx * ny));
+  const Warps w = grid_warps();
+  const int lane = threadIdx.x & 31;
+  for_rows(w, 1, F.n2 + 1, 1, F.n3 + 1, [&](int j, int k) {
+    for (int i = 1 + lane; i <= F.n1 + 1; i += 32) {
       long long q = F.g(i, j, k);
       F.rf[q] = (F.bc[q] > 0) ? 0.0 : getres(F, q, F.b[F.r(i, j, k)]);
     }
-  }
+  });
   grid.sync();
-  {
-    const long long CX = C.n1 + 3, CY = C.n2 + 3, tot = CX * CY * (C.n3 + 3);
-    const long long sy = F.N1, sz = F.N1 * F.N2;
-    for (long long t = tid; t < tot; t += stride) {
-      int i = (int)(t % CX), j = (int)((t / CX) % CY), k = (int)(t / (CX * CY));
+  const long long sy = F.N1, sz = F.N1 * F.N2;
+  for_rows(w, 0, C.n2 + 3, 0, C.n3 + 3, [&](int j, int k) {
+    for (int i = lane; i <= C.n1 + 2; i += 32) {
       long long qc = C.g(i, j, k);
       int bc2 = F.bc[F.g(fmap(i, F.n1), fmap(j, F.n2), fmap(k, F.n3))];
       C.bc[qc] = bc2;
@@ -252,37 +260,37 @@ __device__ void restriction(const MGLev &F, const MGLev &C, cg::grid_group &grid
         C.b[C.r(i, j, k)] = re;
       }
     }
-  }
+  });
   grid.sync();
 }
 
 // Src/mg.f90:849-939 (prolongation): coarse C added into fine F
 __device__ void prolongation(const MGLev &F, const MGLev &C, cg::grid_group &grid) {
-  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  const long long nx = C.n1 + 1, ny = C.n2 + 1, tot = C.nodes();
+  const Warps w = grid_warps();
+  const int lane = threadIdx.x & 31;
   const long long sy = F.N1, sz = F.N1 * F.N2;
   const long long cy = C.N1, cz = C.N1 * C.N2;
-  for (long long t = tid; t < tot; t += stride) {
-    int i = 1 + (int)(t % nx), j = 1 + (int)((t / nx) % ny), k = 1 + (int)(t / (nx * ny));
-    long long c = C.g(i, j, k);
-    const double *E = C.u;
-    double r000 = E[c], r0m0 = E[c - cy], rmm0 = E[c - 1 - cy], rm00 = E[c - 1];
-    double r00m = E[c - cz], r0mm = E[c - cy - cz], rmmm = E[c - 1 - cy - cz], rm0m = E[c - 1 - cz];
-    long long q = F.g(2 * i - 1, 2 * j - 1, 2 * k - 1);
-    double *U = F.u;
-    const int *B = F.bc;
-    if (B[q] <= 0) U[q] = U[q] + r000;
-    if (B[q - sy] <= 0) U[q - sy] = U[q - sy] + (r000 + r0m0) / 2.0;
-    if (B[q - 1 - sy] <= 0) U[q - 1 - sy] = U[q - 1 - sy] + (r000 + r0m0 + rmm0 + rm00) / 4.0;
-    if (B[q - 1] <= 0) U[q - 1] = U[q - 1] + (r000 + rm00) / 2.0;
-    if (B[q - sz] <= 0) U[q - sz] = U[q - sz] + (r000 + r00m) / 2.0;
-    if (B[q - sy - sz] <= 0) U[q - sy - sz] = U[q - sy - sz] + (r000 + r00m + r0mm + r0m0) / 4.0;
-    if (B[q - 1 - sz] <= 0) U[q - 1 - sz] = U[q - 1 - sz] + (r000 + r00m + rm0m + rm00) / 4.0;
-    if (B[q - 1 - sy - sz] <= 0)
-      U[q - 1 - sy - sz] =
-          U[q - 1 - sy - sz] + (r000 + r00m + rm0m + rm00 + r0m0 + r0mm + rmmm + rmm0) / 8.0;
-  }
+  for_rows(w, 1, C.n2 + 1, 1, C.n3 + 1, [&](int j, int k) {
+    for (int i = 1 + lane; i <= C.n1 + 1; i += 32) {
+      long long c = C.g(i, j, k);
+      const double *E = C.u;
+      double r000 = E[c], r0m0 = E[c - cy], rmm0 = E[c - 1 - cy], rm00 = E[c - 1];
+      double r00m = E[c - cz], r0mm = E[c - cy - cz], rmmm = E[c - 1 - cy - cz], rm0m = E[c - 1 - cz];
+      long long q = F.g(2 * i - 1, 2 * j - 1, 2 * k - 1);
+      double *U = F.u;
+      const int *B = F.bc;
+      if (B[q] <= 0) U[q] = U[q] + r000;
+      if (B[q - sy] <= 0) U[q - sy] = U[q - sy] + (r000 + r0m0) / 2.0;
+      if (B[q - 1 - sy] <= 0) U[q - 1 - sy] = U[q - 1 - sy] + (r000 + r0m0 + rmm0 + rm00) / 4.0;
+      if (B[q - 1] <= 0) U[q - 1] = U[q - 1] + (r000 + rm00) / 2.0;
+      if (B[q - sz] <= 0) U[q - sz] = U[q - sz] + (r000 + r00m) / 2.0;
+      if (B[q - sy - sz] <= 0) U[q - sy - sz] = U[q - sy - sz] + (r000 + r00m + r0mm + r0m0) / 4.0;
+      if (B[q - 1 - sz] <= 0) U[q - 1 - sz] = U[q - 1 - sz] + (r000 + r00m + rm0m + rm00) / 4.0;
+      if (B[q - 1 - sy - sz] <= 0)
+        U[q - 1 - sy - sz] =
+            U[q - 1 - sy - sz] + (r000 + r00m + rm0m + rm00 + r0m0 + r0mm + rmmm + rmm0) / 8.0;
+    }
+  });
   grid.sync();
 }
 

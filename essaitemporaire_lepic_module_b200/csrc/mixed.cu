@@ -1,8 +1,8 @@
 // Mixed-precision particle kernels of the device-resident step loop.
 //
 // Particle state per species (28 B per particle instead of 48):
-//   cell  int32   c = (ix-1) + n1((iy-1) + n2(iz-1)), ix = INT(x/h)+1 of the
-//                 reference (Src/part_expmover.f90:89-91)
+//   cell  int32   c = (ix-1) | (iy-1) << 10 | (iz-1) << 20, ix = INT(x/h)+1
+//                 of the reference (Src/part_expmover.f90:89-91)
 //   p32   float   6 planes: fx, fy, fz in [0,1) (x = (ix-1+fx) h) and
 //                 vx, vy, vz in m/s
 // The push is the reference's gather + Boris + leapfrog
@@ -12,19 +12,19 @@
 // position inside its cell.
 //
 // Deposition (Src/part_expmover.f90:591-656) of the new position: the eight
-// CIC weights are computed in FP64 from the FP32 offsets and quantized to
-// integers in units of 2^-24 with the eighth taken as 2^24 minus the other
-// seven, so every particle deposits exactly 2^24 units and integer sums are
-// exact and independent of the summation order.  The sort orders particles
-// by 8x8x8-cell tiles; one block pushes the particles of one tile and sums
-// their weights with 32-bit shared-memory atomics into a node tile covering
-// the tile's cells plus one halo cell on each side (a weight w is split into
-// w >> 12 and w & 4095 held in two tiles, which bounds both sums below 2^31
-// for up to 2^18 particles per flush).  The node tile is then added to the
-// FP64 grid with one atomic per non-zero node; particles outside the box
-// (drifted since the sort, moved by hole filling, appended by collisions) add
-// their quantized weights to the grid directly.  kdep and kq are applied in
-// FP64 to the integer sums.
+// CIC weights are rounded to integers in units of 2^-22 and the rounding
+// residue is added to the weight of the nearest node, so every particle
+// deposits exactly 2^22 units and integer sums are exact and independent of
+// the summation order.  The sort orders particles by 8x8x8-cell tiles; one
+// block pushes the particles of one tile and sums their weights with 32-bit
+// shared-memory atomics into a node tile covering the tile's cells plus one
+// halo cell on each side.  An add that wraps a node's 32-bit sum is seen by
+// the one lane whose atomic returned the value before the wrap; that lane
+// adds the 2^32 units to the FP64 grid, so nothing is lost however dense the
+// tile.  The node tile is then added to the FP64 grid with one atomic per
+// non-zero node; particles outside the box (drifted since the sort, moved by
+// hole filling, appended by collisions) add their integer weights to the grid
+// directly.  kdep and kq are applied in FP64 to the integer sums.
 //
 // A thread moves four consecutive particles with 16-byte loads and stores
 // and merges the weights of those that end in the same cell before touching
@@ -42,9 +42,9 @@ constexpr int TC = LEPIC_TILE_CELLS;       // tile edge in cells
 constexpr int TN = TC + 3;                 // node tile edge (halo cell each side)
 constexpr int TT = TN * TN * TN;
 constexpr int CHUNK = 4 * MBK;             // particles per block iteration
-constexpr int FLUSH_CHUNKS = (1 << 18) / CHUNK;
-constexpr double QS = 16777216.0;          // 2^24 weight units per particle
-constexpr double QI = 1.0 / 16777216.0;
+constexpr int QBITS = 22;                  // 2^22 weight units per particle
+constexpr double QI = 1.0 / 4194304.0;
+constexpr int CB = LEPIC_CELL_BITS, CM = LEPIC_CELL_MAX - 1;
 
 __device__ __forceinline__ unsigned lmask_le() {
   unsigned m;
@@ -66,23 +66,35 @@ struct MixedConst {
   int ntx, nty, ntiles;       // tile grid
 };
 
-// quantized CIC weights of offsets (gx, gy, gz): w[c] in units of 2^-24,
-// summing to exactly 2^24 (node order of Src/part_expmover.f90:591-656)
+// x rounded to the nearest integer for 0 <= x <= 2^22, by the FP32 addition
+// of 1.5 * 2^23 (whose unit in the last place is 1) and integer arithmetic
+__device__ __forceinline__ int round_q(float x) { return __float_as_int(x + 12582912.f) - 0x4B400000; }
+
+// integer CIC weights of offsets (gx, gy, gz) in units of 2^-22 summing to
+// exactly 2^22 (node order of Src/part_expmover.f90:591-656: (0,0,0),
+// (1,0,0), (1,1,0), (0,1,0), then the same at z+1)
 __device__ __forceinline__ void qweights(float gx, float gy, float gz, int w[8]) {
-  const double qx = 1.0 - (double)gx, qy = 1.0 - (double)gy, qz = 1.0 - (double)gz;
-  const double px = 1.0 - qx, py = 1.0 - qy, pz = 1.0 - qz;
-  w[0] = __double2int_rn(qx * qy * qz * QS);
-  w[1] = __double2int_rn(px * qy * qz * QS);
-  w[2] = __double2int_rn(px * py * qz * QS);
-  w[3] = __double2int_rn(qx * py * qz * QS);
-  w[4] = __double2int_rn(qx * qy * pz * QS);
-  w[5] = __double2int_rn(px * qy * pz * QS);
-  w[6] = __double2int_rn(px * py * pz * QS);
-  w[7] = 16777216 - (w[0] + w[1] + w[2] + w[3] + w[4] + w[5] + w[6]);
+  const float S = 4194304.f;
+  const float qx = 1.f - gx, qy = 1.f - gy, qz = 1.f - gz;
+  const float a = qy * qz * S, b = gy * qz * S, e = qy * gz * S, f = gy * gz * S;
+  w[0] = round_q(qx * a);
+  w[1] = round_q(gx * a);
+  w[2] = round_q(gx * b);
+  w[3] = round_q(qx * b);
+  w[4] = round_q(qx * e);
+  w[5] = round_q(gx * e);
+  w[6] = round_q(gx * f);
+  w[7] = round_q(qx * f);
+  const int r = (1 << QBITS) - (w[0] + w[1] + w[2] + w[3] + w[4] + w[5] + w[6] + w[7]);
+  // nearest node: its weight is at least 1/8, so it stays positive
+  const int nx = gx >= 0.5f, ny = gy >= 0.5f, nz = gz >= 0.5f;
+  const int near = (ny ? (nx ? 2 : 3) : (nx ? 1 : 0)) + 4 * nz;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) w[c] += (c == near) ? r : 0;
 }
 
 struct Tile {
-  int *hi, *lo;               // shared node tiles (nullptr: no tile)
+  unsigned *acc;              // shared node tile (nullptr: no tile)
   int bx, by, bz;             // node coordinates of local (0,0,0)
 };
 
@@ -91,18 +103,20 @@ struct Tile {
 __device__ __forceinline__ void deposit8(const Dims &d, const Tile &T, int jx, int jy, int jz, long long q,
                                          const int w[8], double kdep, const double *__restrict__ kq,
                                          double *__restrict__ np) {
+  const long long sy = d.N1, sz = d.N1 * d.N2;
+  const long long o[8] = {0, 1, 1 + sy, sy, sz, 1 + sz, 1 + sy + sz, sy + sz};
   const int lx = jx - T.bx, ly = jy - T.by, lz = jz - T.bz;
-  if (T.hi && lx >= 0 && lx < TN - 1 && ly >= 0 && ly < TN - 1 && lz >= 0 && lz < TN - 1) {
+  if (T.acc && lx >= 0 && lx < TN - 1 && ly >= 0 && ly < TN - 1 && lz >= 0 && lz < TN - 1) {
     const int t = lx + TN * (ly + TN * lz);
     const int to[8] = {0, 1, 1 + TN, TN, TN * TN, 1 + TN * TN, 1 + TN + TN * TN, TN + TN * TN};
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-      atomicAdd(&T.hi[t + to[c]], w[c] >> 12);
-      atomicAdd(&T.lo[t + to[c]], w[c] & 4095);
+      const unsigned add = (unsigned)w[c];
+      const unsigned old = atomicAdd(&T.acc[t + to[c]], add);
+      if (old > 0xFFFFFFFFu - add)  // this add wrapped the 32-bit sum
+        atomicAdd(&np[q + o[c]], __ldg(&kq[q + o[c]]) * (kdep * (4294967296.0 * QI)));
     }
   } else {
-    const long long sy = d.N1, sz = d.N1 * d.N2;
-    const long long o[8] = {0, 1, 1 + sy, sy, sz, 1 + sz, 1 + sy + sz, sy + sz};
 #pragma unroll
     for (int c = 0; c < 8; ++c) atomicAdd(&np[q + o[c]], __ldg(&kq[q + o[c]]) * (kdep * ((double)w[c] * QI)));
   }
@@ -112,17 +126,15 @@ __device__ __forceinline__ void deposit8(const Dims &d, const Tile &T, int jx, i
 __device__ void flush_tile(const Dims &d, const Tile &T, double kdep, const double *__restrict__ kq,
                            double *__restrict__ np) {
   for (int e = threadIdx.x; e < TT; e += blockDim.x) {
-    const int h = T.hi[e], l = T.lo[e];
-    if (h | l) {
+    const unsigned v = T.acc[e];
+    if (v) {
       const int lx = e % TN, ly = (e / TN) % TN, lz = e / (TN * TN);
       const int gx = T.bx + lx, gy = T.by + ly, gz = T.bz + lz;
       if (gx <= d.n1 + 2 && gy <= d.n2 + 2 && gz <= d.n3 + 2) {
         const long long node = d.g(gx, gy, gz);
-        const double v = ((double)h * 4096.0 + (double)l) * QI;
-        atomicAdd(&np[node], __ldg(&kq[node]) * (kdep * v));
+        atomicAdd(&np[node], __ldg(&kq[node]) * (kdep * ((double)v * QI)));
       }
-      T.hi[e] = 0;
-      T.lo[e] = 0;
+      T.acc[e] = 0u;
     }
   }
 }
@@ -140,7 +152,6 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
                                           int *__restrict__ err) {
   const unsigned full = 0xffffffffu;
   const int n1 = d.n1, n2 = d.n2, n3 = d.n3;
-  const int ncell = n1 * n2 * n3;
   int4 c4 = make_int4(-1, -1, -1, -1);
   float4 P[6];
   char4 f4 = make_char4(0, 0, 0, 0);
@@ -175,13 +186,13 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
       hole[k] = true;
       continue;
     }
-    if (cc < 0 || cc >= ncell) {
+    const int ix = (cc & CM) + 1, iy = ((cc >> CB) & CM) + 1, iz = (cc >> (2 * CB)) + 1;
+    if (cc < 0 || ix > n1 || iy > n2 || iz > n3) {
       raise_err(err, LEPIC_ERR_CELL, (int)(i0 + k));
       hole[k] = true;
       continue;
     }
     float fx = (&P[0].x)[k], fy = (&P[1].x)[k], fz = (&P[2].x)[k];
-    const int ix = cc % n1 + 1, iy = (cc / n1) % n2 + 1, iz = cc / (n1 * n2) + 1;
     // gather: left-node weights 1 - f (Src/part_expmover.f90:89-108)
     const float px = 1.f - fx, py = 1.f - fy, pz = 1.f - fz;
     const float k0 = px * py * pz, ka = (1.f - px) * py * pz, kb = (1.f - px) * (1.f - py) * pz,
@@ -217,13 +228,22 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
     fx = fx + vx * c.dth0;
     fy = fy + vy * c.dth1;
     fz = fz + vz * c.dth2;
-    int sx = (int)floorf(fx), syi = (int)floorf(fy), szi = (int)floorf(fz);
-    fx -= (float)sx;
-    fy -= (float)syi;
-    fz -= (float)szi;
-    if (fx >= 1.f) { fx = 0.f; sx += 1; }
-    if (fy >= 1.f) { fy = 0.f; syi += 1; }
-    if (fz >= 1.f) { fz = 0.f; szi += 1; }
+    int sx = 0, syi = 0, szi = 0;
+    if (!(fx >= 0.f && fx < 1.f)) {
+      sx = __float2int_rd(fx);
+      fx -= (float)sx;
+      if (fx >= 1.f) { fx = 0.f; sx += 1; }
+    }
+    if (!(fy >= 0.f && fy < 1.f)) {
+      syi = __float2int_rd(fy);
+      fy -= (float)syi;
+      if (fy >= 1.f) { fy = 0.f; syi += 1; }
+    }
+    if (!(fz >= 0.f && fz < 1.f)) {
+      szi = __float2int_rd(fz);
+      fz -= (float)szi;
+      if (fz >= 1.f) { fz = 0.f; szi += 1; }
+    }
     int ax = ix + sx, ay = iy + syi, az = iz + szi;
     if (c.flag_pbc == 1) {
       if (ay > n2) ay -= n2;
@@ -247,7 +267,7 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
       }
       hole[k] = true;
     } else {
-      (&c4.x)[k] = (ax - 1) + n1 * ((ay - 1) + n2 * (az - 1));
+      (&c4.x)[k] = (ax - 1) | (ay - 1) << CB | (az - 1) << (2 * CB);
       jx[k] = ax;
       jy[k] = ay;
       jz[k] = az;
@@ -315,51 +335,38 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
 
 // one block per tile: the particles [tile_off[t], tile_off[t+1]) of the last
 // sort, clipped to the current count
-__global__ void __launch_bounds__(MBK) k_push_deposit_tiles(
+__global__ void __launch_bounds__(MBK, 3) k_push_deposit_tiles(
     Dims d, MixedConst c, const float4 *__restrict__ E4, const int *__restrict__ bcnd,
     const unsigned char *__restrict__ cw, int *__restrict__ cell, float *__restrict__ p, long long cap,
     const int *__restrict__ count, signed char *__restrict__ flag, const int *__restrict__ tile_off,
     const double *__restrict__ kq, double *__restrict__ np, int *__restrict__ holes, int *__restrict__ nholes,
     double *__restrict__ acc, int *__restrict__ err) {
-  __shared__ int s_hi[TT], s_lo[TT];
+  __shared__ unsigned s_acc[TT];
   const int t = blockIdx.x;
   const int tx = t % c.ntx, ty = (t / c.ntx) % c.nty, tz = t / (c.ntx * c.nty);
-  Tile T{s_hi, s_lo, tx * TC, ty * TC, tz * TC};
-  for (int e = threadIdx.x; e < TT; e += MBK) {
-    s_hi[e] = 0;
-    s_lo[e] = 0;
-  }
+  Tile T{s_acc, tx * TC, ty * TC, tz * TC};
+  for (int e = threadIdx.x; e < TT; e += MBK) s_acc[e] = 0u;
   __syncthreads();
   const long long N = *count;
   const long long lo = tile_off[t];
   long long hi = tile_off[t + 1];
   if (hi > N) hi = N;
-  const long long first = lo & ~3LL;
-  int chunks = 0;
-  for (long long base = first; base < hi; base += CHUNK) {
+  for (long long base = lo & ~3LL; base < hi; base += CHUNK)
     push_quad(d, c, T, base + 4 * threadIdx.x, lo, hi, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes,
               nholes, acc, err);
-    if (++chunks == FLUSH_CHUNKS && base + CHUNK < hi) {
-      // keep the integer tile sums below 2^31 on very dense tiles
-      chunks = 0;
-      __syncthreads();
-      flush_tile(d, T, c.kdep, kq, np);
-      __syncthreads();
-    }
-  }
   __syncthreads();
   flush_tile(d, T, c.kdep, kq, np);
 }
 
 // particles past the last tile (appended since the sort), or all of them
 // when no sort has run: deposited straight into the FP64 grid
-__global__ void __launch_bounds__(MBK) k_push_deposit_tail(
+__global__ void __launch_bounds__(MBK, 3) k_push_deposit_tail(
     Dims d, MixedConst c, const float4 *__restrict__ E4, const int *__restrict__ bcnd,
     const unsigned char *__restrict__ cw, int *__restrict__ cell, float *__restrict__ p, long long cap,
     const int *__restrict__ count, signed char *__restrict__ flag, const int *__restrict__ tile_off,
     const double *__restrict__ kq, double *__restrict__ np, int *__restrict__ holes, int *__restrict__ nholes,
     double *__restrict__ acc, int *__restrict__ err) {
-  const Tile T{nullptr, nullptr, 0, 0, 0};
+  const Tile T{nullptr, 0, 0, 0};
   const long long N = *count;
   const long long lo = tile_off ? tile_off[c.ntiles] : 0;
   const long long first = lo & ~3LL;
@@ -402,8 +409,8 @@ __global__ void k_fillm_count(int *count, const int *side) { *count = *count - s
 
 // ---------------------------------------------------------------- sort
 // sort key: tile (x-fastest over tiles) * 512 + cell inside the tile
-__device__ __forceinline__ int tile_key(int cc, int n1, int n2, int ntx, int nty) {
-  const int cx = cc % n1, cy = (cc / n1) % n2, cz = cc / (n1 * n2);
+__device__ __forceinline__ int tile_key(int cc, int ntx, int nty) {
+  const int cx = cc & CM, cy = (cc >> CB) & CM, cz = cc >> (2 * CB);
   const int tile = (cx / TC) + ntx * ((cy / TC) + nty * (cz / TC));
   return tile * (TC * TC * TC) + (cx % TC) + TC * ((cy % TC) + TC * (cz % TC));
 }
@@ -420,10 +427,10 @@ __device__ __forceinline__ void run_of(int key, bool &head, int &start, int &len
   len = (above ? __ffs(above) - 1 : 32) - start;
 }
 
-__global__ void k_msort_hist(const int *__restrict__ cell, const int *__restrict__ count, int n1, int n2,
-                             int ntx, int nty, int *cnt) {
+__global__ void k_msort_hist(const int *__restrict__ cell, const int *__restrict__ count, int ntx, int nty,
+                             int *cnt) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int k = (i < *count) ? tile_key(cell[i], n1, n2, ntx, nty) : -1;
+  const int k = (i < *count) ? tile_key(cell[i], ntx, nty) : -1;
   bool head;
   int start, len;
   run_of(k, head, start, len);
@@ -437,12 +444,12 @@ __global__ void k_tile_offsets(const int *__restrict__ off, int ntiles, int *__r
 
 __global__ void k_msort_scatter(const int *__restrict__ cell, const float *__restrict__ p,
                                 int *__restrict__ cell_o, float *__restrict__ p_o, long long cap,
-                                const int *__restrict__ count, int n1, int n2, int ntx, int nty, int *cursor) {
+                                const int *__restrict__ count, int ntx, int nty, int *cursor) {
   const unsigned full = 0xffffffffu;
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const int N = *count;
   const int cc = (i < N) ? cell[i] : -1;
-  const int k = (i < N) ? tile_key(cc, n1, n2, ntx, nty) : -1;
+  const int k = (i < N) ? tile_key(cc, ntx, nty) : -1;
   bool head;
   int start, len;
   run_of(k, head, start, len);
@@ -477,7 +484,7 @@ __global__ void k_f64_to_mixed(Dims d, double h0, double h1, double h2, const do
     iy = iy < 1 ? 1 : (iy > d.n2 ? d.n2 : iy);
     iz = iz < 1 ? 1 : (iz > d.n3 ? d.n3 : iz);
   }
-  cell[i] = (ix - 1) + d.n1 * ((iy - 1) + d.n2 * (iz - 1));
+  cell[i] = (ix - 1) | (iy - 1) << CB | (iz - 1) << (2 * CB);
   const float fx = (float)(x / h0 - (ix - 1)), fy = (float)(y / h1 - (iy - 1)), fz = (float)(z / h2 - (iz - 1));
   p[i] = fx >= 1.f ? 0.99999994f : fx;
   p[cap + i] = fy >= 1.f ? 0.99999994f : fy;
@@ -494,7 +501,7 @@ __global__ void k_mixed_to_f64(Dims d, double h0, double h1, double h2, const in
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int cc = cell[i];
-  const int ix = cc % d.n1, iy = (cc / d.n1) % d.n2, iz = cc / (d.n1 * d.n2);
+  const int ix = cc & CM, iy = (cc >> CB) & CM, iz = cc >> (2 * CB);
   pout[i] = ((double)ix + (double)p[i]) * h0;
   pout[capout + i] = ((double)iy + (double)p[cap + i]) * h1;
   pout[2 * capout + i] = ((double)iz + (double)p[2 * cap + i]) * h2;
@@ -505,7 +512,8 @@ __global__ void k_mixed_to_f64(Dims d, double h0, double h1, double h2, const in
 
 bool aligned16(const void *q) { return ((uintptr_t)q & 15u) == 0; }
 
-int check_layout(const lepic_species_mixed_t &sp) {
+int check_layout(const lepic_grid_t &g, const lepic_species_mixed_t &sp) {
+  if (g.n[0] > LEPIC_CELL_MAX || g.n[1] > LEPIC_CELL_MAX || g.n[2] > LEPIC_CELL_MAX) return LEPIC_ERR_UNSUPPORTED;
   if (sp.cap % 4 || !aligned16(sp.cell) || !aligned16(sp.p) || !aligned16(sp.cell_alt) || !aligned16(sp.p_alt) ||
       ((uintptr_t)sp.flag_dead & 3u))
     return LEPIC_ERR_ARG;
@@ -521,7 +529,7 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
   const int p = ptype - 1;
   if (P.flag_nmn) return LEPIC_ERR_UNSUPPORTED;
   if (!sp.flag_dead || !aligned16(E4)) return LEPIC_ERR_ARG;
-  if (int rc = check_layout(sp)) return rc;
+  if (int rc = check_layout(g, sp)) return rc;
   MixedConst c;
   memset(&c, 0, sizeof(c));
   c.dth0 = (float)(P.dt / g.h[0]);
@@ -579,7 +587,7 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
 
 int launch_sort_mixed(const lepic_grid_t &g, lepic_species_mixed_t &sp, int n_hint, cudaStream_t s) {
   Dims d(g.n);
-  if (int rc = check_layout(sp)) return rc;
+  if (int rc = check_layout(g, sp)) return rc;
   const int ntx = (d.n1 + TC - 1) / TC, nty = (d.n2 + TC - 1) / TC;
   const int ntiles = LEPIC_TILES(g.n);
   const long long nkeys = (long long)ntiles * TC * TC * TC;
@@ -588,7 +596,7 @@ int launch_sort_mixed(const lepic_grid_t &g, lepic_species_mixed_t &sp, int n_hi
   LEPIC_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(nkeys + 1), s));
   const int nthreads = n_hint > 0 ? n_hint : sp.cap;
   int t0 = timer_start("sort_hist_mixed", s);
-  k_msort_hist<<<grid_for(nthreads, MBK), MBK, 0, s>>>(sp.cell, sp.count, d.n1, d.n2, ntx, nty, cnt);
+  k_msort_hist<<<grid_for(nthreads, MBK), MBK, 0, s>>>(sp.cell, sp.count, ntx, nty, cnt);
   timer_stop(t0, s);
   int t1 = timer_start("sort_scan_mixed", s);
   int rc = exclusive_scan_i32(cnt, cnt, nkeys + 1, s);
@@ -597,7 +605,7 @@ int launch_sort_mixed(const lepic_grid_t &g, lepic_species_mixed_t &sp, int n_hi
   if (sp.tile_off) k_tile_offsets<<<grid_for(ntiles + 1, 256), 256, 0, s>>>(cnt, ntiles, sp.tile_off);
   int t2 = timer_start("sort_scatter_mixed", s);
   k_msort_scatter<<<grid_for(nthreads, MBK), MBK, 0, s>>>(sp.cell, sp.p, sp.cell_alt, sp.p_alt, sp.cap,
-                                                          sp.count, d.n1, d.n2, ntx, nty, cnt);
+                                                          sp.count, ntx, nty, cnt);
   timer_stop(t2, s);
   LEPIC_CUDA(cudaGetLastError());
   int *tc = sp.cell;

@@ -119,7 +119,7 @@ class Simulation:
         self.precision = precision
         self.fused = fused or self.mixed
         # FP32 V-cycle parameters of the mixed Poisson solve
-        self.mg_mixed = dict(max_refine=60, nu_pre=2, nu_post=2, coarse_sweeps=32, omega=1.0)
+        self.mg_mixed = dict(max_refine=60, nu_pre=2, nu_post=2, coarse_sweeps=16, omega=1.0)
         if mg_mixed:
             self.mg_mixed.update(mg_mixed)
         self._acc = None

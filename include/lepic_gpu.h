@@ -213,15 +213,16 @@ typedef struct {
 } lepic_species_f64_t;
 
 /* One species in the mixed-precision layout (28 B per particle): cell[i] =
- * (ix-1) + n1((iy-1) + n2(iz-1)) with ix = INT(x/h)+1, and p[a*cap + i] for
- * a = fx, fy, fz (in-cell offsets in [0,1), x = (ix-1+fx) h) and vx, vy, vz
- * (m/s), all FP32.  *_alt: sort targets of the same size.  cap must be a
- * multiple of 4 and the arrays 16-byte aligned (the push moves particles in
- * groups of four).  The sort orders particles by 8x8x8-cell tiles (cells in
- * x-fastest order inside a tile, tiles in x-fastest order) and writes the
- * particle offset of every tile to tile_off (device int[LEPIC_TILES(n)+1],
- * zero-filled by the caller before the first sort); the push deposits each
- * tile's particles through an on-chip node tile. */
+ * (ix-1) | (iy-1) << 10 | (iz-1) << 20 with ix = INT(x/h)+1 (so each grid
+ * dimension is at most 1024 cells), and p[a*cap + i] for a = fx, fy, fz
+ * (in-cell offsets in [0,1), x = (ix-1+fx) h) and vx, vy, vz (m/s), all FP32.
+ * *_alt: sort targets of the same size.  cap must be a multiple of 4 and the
+ * arrays 16-byte aligned (the push moves particles in groups of four).  The
+ * sort orders particles by 8x8x8-cell tiles (cells in x-fastest order inside
+ * a tile, tiles in x-fastest order) and writes the particle offset of every
+ * tile to tile_off (device int[LEPIC_TILES(n)+1], zero-filled by the caller
+ * before the first sort); the push deposits each tile's particles through an
+ * on-chip node tile. */
 typedef struct {
   int *cell;
   float *p;
@@ -233,7 +234,9 @@ typedef struct {
   int cap;
 } lepic_species_mixed_t;
 
-/* Number of 8x8x8-cell tiles of an n[3] grid. */
+/* Packed cell index of the mixed layout and the 8x8x8-cell tiles. */
+#define LEPIC_CELL_BITS 10
+#define LEPIC_CELL_MAX (1 << LEPIC_CELL_BITS)
 #define LEPIC_TILE_CELLS 8
 #define LEPIC_TILES(n)                                                        \
   ((((n)[0] + 7) / 8) * (((n)[1] + 7) / 8) * (((n)[2] + 7) / 8))

@@ -81,7 +81,7 @@ def test_layout_roundtrip():
         ix = (o[:, 0] / h[0]).astype(int)
         iy = (o[:, 1] / h[1]).astype(int)
         iz = (o[:, 2] / h[2]).astype(int)
-        np.testing.assert_array_equal(cell_g, ix + st.n[0] * (iy + st.n[1] * iz))
+        np.testing.assert_array_equal(cell_g, ix | (iy << 10) | (iz << 20))
 
 
 def test_sort_tile_order():
@@ -100,7 +100,7 @@ def test_sort_tile_order():
     for p, s in enumerate(sim.sp):
         n = s.n()
         c = s.cell[:n].cpu().numpy().astype(np.int64)
-        cx, cy, cz = c % n1, (c // n1) % n2, c // (n1 * n2)
+        cx, cy, cz = c & 1023, (c >> 10) & 1023, c >> 20
         key = ((cx // 8) + ntx * ((cy // 8) + nty * (cz // 8))) * 512 + (cx % 8) + 8 * ((cy % 8) + 8 * (cz % 8))
         assert np.all(np.diff(key) >= 0)
         toff = s.tile_off.cpu().numpy()
