@@ -225,13 +225,16 @@ def _run_form(args, st, precision, rank, world, dist, torch, e2e=True):
     sim.load_uniform()
     torch.cuda.synchronize()
     n_start = int(sim.counts_host().sum())
+    # the sampler starts before the warm-up so that nvidia-smi's start-up
+    # does not stall the timed steps; it samples through them
+    clk = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clk.start()
     for _ in range(args.warmup):
         sim.step()
     torch.cuda.synchronize()
     _lib.timing(enable=True)
     _lib.timing(reset=True)
-    clk = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
-    clk.start()
+    clk.rows.clear()
     nps, ms, iters = _timed_steps(sim, args.steps, world, dist, torch)
     clocks = clk.stop()
     timers = _lib.timing()

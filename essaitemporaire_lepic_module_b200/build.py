@@ -53,8 +53,12 @@ def build(force=False, verbose=False):
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(o)
-        if force or not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(s), hdr_t):
-            jobs.append([exe, *ARCH, *FLAGS, FMAD.get(src, "--fmad=false"), "-c", s, "-o", o])
+        cmd = [exe, *ARCH, *FLAGS, FMAD.get(src, "--fmad=false"), "-c", s, "-o", o]
+        # an object is stale when its source, a header or its flags changed
+        stamp = o + ".cmd"
+        same = os.path.exists(stamp) and open(stamp).read() == " ".join(cmd)
+        if force or not same or not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(s), hdr_t):
+            jobs.append(cmd)
 
     def run(cmd):
         if verbose:
@@ -68,6 +72,9 @@ def build(force=False, verbose=False):
 
     with cf.ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as ex:
         list(ex.map(run, jobs))
+    for cmd in jobs:
+        with open(cmd[-1] + ".cmd", "w") as f:
+            f.write(" ".join(cmd))
     if jobs or force or not os.path.exists(LIB):
         run([exe, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-ldl", "-lpthread"])
     return LIB

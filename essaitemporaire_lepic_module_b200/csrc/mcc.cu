@@ -425,9 +425,12 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
       c.izr = rg->izr;
       cc = rg->cnt_col_dev;
     }
+    // the candidate list shares the species' work list with the push (hole
+    // list), sized by the capacity, so that the step loop allocates nothing
+    // after its first push
     char nm[32];
-    snprintf(nm, sizeof nm, "mcc_cand%d", p - 1);
-    int *cand = (int *)scratch(nm, sizeof(int) * (size_t)Nh[p - 1]);
+    snprintf(nm, sizeof nm, "work_list%d", p - 1);
+    int *cand = (int *)scratch(nm, sizeof(int) * (size_t)S.cap[p - 1]);
     if (!cand) return LEPIC_ERR_CUDA;
     int tm = timer_start(tname, s);
     k_mcc_select<<<grid_for(Nh[p - 1], MB), MB, 0, s>>>(c, counts_dev[p - 1], cand, ncand + (p - 1));

@@ -12,17 +12,16 @@
 // position inside its cell.
 //
 // Deposition (Src/part_expmover.f90:591-656) of the new position: the eight
-// CIC weights are rounded to integers in units of 2^-22 and the rounding
+// CIC weights are rounded to integers in units of 2^-20 and the rounding
 // residue is added to the weight of the nearest node, so every particle
-// deposits exactly 2^22 units and integer sums are exact and independent of
+// deposits exactly 2^20 units and integer sums are exact and independent of
 // the summation order.  The sort orders particles by 8x8x8-cell tiles; one
 // block pushes the particles of one tile and sums their weights with 32-bit
-// shared-memory atomics into a node tile covering the tile's cells plus one
-// halo cell on each side.  An add that wraps a node's 32-bit sum is seen by
-// the one lane whose atomic returned the value before the wrap; that lane
-// adds the 2^32 units to the FP64 grid, so nothing is lost however dense the
-// tile.  The node tile is then added to the FP64 grid with one atomic per
-// non-zero node; particles outside the box (drifted since the sort, moved by
+// shared-memory adds into a node tile covering the tile's cells plus one halo
+// cell on each side.  The node tile is added to the FP64 grid (one atomic per
+// non-zero node) and cleared after every FLUSH_PARTICLES particles, so a
+// node's sum stays below FLUSH_PARTICLES * 2^20 = 2^31 however the particles
+// are placed.  Particles outside the box (drifted since the sort, moved by
 // hole filling, appended by collisions) add their integer weights to the grid
 // directly.  kdep and kq are applied in FP64 to the integer sums.
 //
@@ -42,8 +41,10 @@ constexpr int TC = LEPIC_TILE_CELLS;       // tile edge in cells
 constexpr int TN = TC + 3;                 // node tile edge (halo cell each side)
 constexpr int TT = TN * TN * TN;
 constexpr int CHUNK = 4 * MBK;             // particles per block iteration
-constexpr int QBITS = 22;                  // 2^22 weight units per particle
-constexpr double QI = 1.0 / 4194304.0;
+constexpr int QBITS = 20;                  // 2^20 weight units per particle
+constexpr double QI = 1.0 / 1048576.0;
+constexpr int FLUSH_PARTICLES = 2048;      // node sums <= 2048 * 2^20 = 2^31
+static_assert(FLUSH_PARTICLES % CHUNK == 0, "flush windows are whole chunks");
 constexpr int CB = LEPIC_CELL_BITS, CM = LEPIC_CELL_MAX - 1;
 
 __device__ __forceinline__ unsigned lmask_le() {
@@ -60,6 +61,7 @@ __device__ __forceinline__ unsigned lmask_lt() {
 struct MixedConst {
   float dth0, dth1, dth2;     // dt / h per direction
   float k1;                   // dt q / (2 m)
+  float kk;                   // Boris rotation factor 2 k1 / (1 + (k1 |B|)^2)
   float Bx, By, Bz;
   int boris, flag_pbc, ngrid;
   double Nm, mass, kdep;      // kdep = Nm / (h1 h2 h3)
@@ -68,13 +70,14 @@ struct MixedConst {
 
 // x rounded to the nearest integer for 0 <= x <= 2^22, by the FP32 addition
 // of 1.5 * 2^23 (whose unit in the last place is 1) and integer arithmetic
+// (weights are at most 2^QBITS <= 2^22)
 __device__ __forceinline__ int round_q(float x) { return __float_as_int(x + 12582912.f) - 0x4B400000; }
 
-// integer CIC weights of offsets (gx, gy, gz) in units of 2^-22 summing to
-// exactly 2^22 (node order of Src/part_expmover.f90:591-656: (0,0,0),
+// integer CIC weights of offsets (gx, gy, gz) in units of 2^-20 summing to
+// exactly 2^20 (node order of Src/part_expmover.f90:591-656: (0,0,0),
 // (1,0,0), (1,1,0), (0,1,0), then the same at z+1)
 __device__ __forceinline__ void qweights(float gx, float gy, float gz, int w[8]) {
-  const float S = 4194304.f;
+  const float S = (float)(1 << QBITS);
   const float qx = 1.f - gx, qy = 1.f - gy, qz = 1.f - gz;
   const float a = qy * qz * S, b = gy * qz * S, e = qy * gz * S, f = gy * gz * S;
   w[0] = round_q(qx * a);
@@ -93,10 +96,23 @@ __device__ __forceinline__ void qweights(float gx, float gy, float gz, int w[8])
   for (int c = 0; c < 8; ++c) w[c] += (c == near) ? r : 0;
 }
 
+// The block's box in shared memory: the nodes bx..bx+TN-1 (and likewise in
+// y, z) of the tile's cells plus one halo cell on each side.
 struct Tile {
-  unsigned *acc;              // shared node tile (nullptr: no tile)
-  int bx, by, bz;             // node coordinates of local (0,0,0)
+  unsigned *acc;              // node weight sums (nullptr: no box, global only)
+  const float4 *E;            // E at the box nodes
+  const unsigned char *cw;    // all-wall flags of the box cells
+  int bx, by, bz;             // grid coordinates of box node (0,0,0)
 };
+
+// box-local coordinates of cell (ix,iy,iz) when the cell's 8 nodes are in the box
+__device__ __forceinline__ bool in_box(const Tile &T, int ix, int iy, int iz, int &lx, int &ly, int &lz) {
+  lx = ix - T.bx;
+  ly = iy - T.by;
+  lz = iz - T.bz;
+  return T.acc && (unsigned)lx < (unsigned)(TN - 1) && (unsigned)ly < (unsigned)(TN - 1) &&
+         (unsigned)lz < (unsigned)(TN - 1);
+}
 
 // 8 weights of base node q (grid coordinates jx,jy,jz) into the tile when the
 // cell lies in the box, else into the FP64 grid
@@ -105,17 +121,12 @@ __device__ __forceinline__ void deposit8(const Dims &d, const Tile &T, int jx, i
                                          double *__restrict__ np) {
   const long long sy = d.N1, sz = d.N1 * d.N2;
   const long long o[8] = {0, 1, 1 + sy, sy, sz, 1 + sz, 1 + sy + sz, sy + sz};
-  const int lx = jx - T.bx, ly = jy - T.by, lz = jz - T.bz;
-  if (T.acc && lx >= 0 && lx < TN - 1 && ly >= 0 && ly < TN - 1 && lz >= 0 && lz < TN - 1) {
+  int lx, ly, lz;
+  if (in_box(T, jx, jy, jz, lx, ly, lz)) {
     const int t = lx + TN * (ly + TN * lz);
     const int to[8] = {0, 1, 1 + TN, TN, TN * TN, 1 + TN * TN, 1 + TN + TN * TN, TN + TN * TN};
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const unsigned add = (unsigned)w[c];
-      const unsigned old = atomicAdd(&T.acc[t + to[c]], add);
-      if (old > 0xFFFFFFFFu - add)  // this add wrapped the 32-bit sum
-        atomicAdd(&np[q + o[c]], __ldg(&kq[q + o[c]]) * (kdep * (4294967296.0 * QI)));
-    }
+    for (int c = 0; c < 8; ++c) atomicAdd(&T.acc[t + to[c]], (unsigned)w[c]);
   } else {
 #pragma unroll
     for (int c = 0; c < 8; ++c) atomicAdd(&np[q + o[c]], __ldg(&kq[q + o[c]]) * (kdep * ((double)w[c] * QI)));
@@ -139,11 +150,43 @@ __device__ void flush_tile(const Dims &d, const Tile &T, double kdep, const doub
   }
 }
 
-// Push + loss test + deposit of the particle quad starting at i0 (a multiple
-// of 4); particles outside [lo, hi) are not touched.  Every lane of the warp
-// must call this (warp-wide hole appends).
+// Four consecutive particles i0..i0+3 (i0 a multiple of 4) and which of
+// them lie in the range being pushed.
+struct Quad {
+  int4 c4;
+  char4 f4;
+  float4 P[6];
+  bool in[4];
+};
+
+__device__ __forceinline__ void quad_range(Quad &Q, long long i0, long long lo, long long hi) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) Q.in[k] = (i0 + k >= lo) && (i0 + k < hi);
+}
+
+// from HBM (i0 + 3 < cap: cap is a multiple of 4)
+__device__ __forceinline__ void load_quad(Quad &Q, long long i0, long long lo, long long hi,
+                                          const int *__restrict__ cell, const float *__restrict__ p,
+                                          long long cap, const signed char *__restrict__ flag) {
+  quad_range(Q, i0, lo, hi);
+  if (i0 < hi) {
+    Q.c4 = *reinterpret_cast<const int4 *>(cell + i0);
+    Q.f4 = *reinterpret_cast<const char4 *>(flag + i0);
+#pragma unroll
+    for (int a = 0; a < 6; ++a) Q.P[a] = *reinterpret_cast<const float4 *>(p + a * cap + i0);
+  } else {
+    Q.c4 = make_int4(-1, -1, -1, -1);
+    Q.f4 = make_char4(0, 0, 0, 0);
+#pragma unroll
+    for (int a = 0; a < 6; ++a) Q.P[a] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+// Push + loss test + deposit of the particle quad Q starting at i0;
+// particles outside the range are not touched.  Every lane of the warp must
+// call this (warp-wide hole appends).
 __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, const Tile &T, long long i0,
-                                          long long lo, long long hi, const float4 *__restrict__ E4,
+                                          Quad &Q, const float4 *__restrict__ E4,
                                           const int *__restrict__ bcnd, const unsigned char *__restrict__ cw,
                                           int *__restrict__ cell, float *__restrict__ p, long long cap,
                                           signed char *__restrict__ flag, const double *__restrict__ kq,
@@ -152,22 +195,10 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
                                           int *__restrict__ err) {
   const unsigned full = 0xffffffffu;
   const int n1 = d.n1, n2 = d.n2, n3 = d.n3;
-  int4 c4 = make_int4(-1, -1, -1, -1);
-  float4 P[6];
-  char4 f4 = make_char4(0, 0, 0, 0);
-  bool in[4] = {false, false, false, false};
-  if (i0 < hi) {
-    // i0 + 3 < cap: cap is a multiple of 4
-    c4 = *reinterpret_cast<const int4 *>(cell + i0);
-    f4 = *reinterpret_cast<const char4 *>(flag + i0);
-#pragma unroll
-    for (int a = 0; a < 6; ++a) P[a] = *reinterpret_cast<const float4 *>(p + a * cap + i0);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) in[k] = (i0 + k >= lo) && (i0 + k < hi);
-  } else {
-#pragma unroll
-    for (int a = 0; a < 6; ++a) P[a] = make_float4(0.f, 0.f, 0.f, 0.f);
-  }
+  int4 &c4 = Q.c4;
+  const char4 f4 = Q.f4;
+  float4 *P = Q.P;
+  const bool *in = Q.in;
   const bool full4 = in[0] && in[1] && in[2] && in[3];
   bool hole[4] = {false, false, false, false};
   int jx[4], jy[4], jz[4];
@@ -198,11 +229,20 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
     const float k0 = px * py * pz, ka = (1.f - px) * py * pz, kb = (1.f - px) * (1.f - py) * pz,
                 kc = px * (1.f - py) * pz, kd = px * py * (1.f - pz), ke = (1.f - px) * py * (1.f - pz),
                 kf = (1.f - px) * (1.f - py) * (1.f - pz), kg = px * (1.f - py) * (1.f - pz);
-    const long long sy = d.N1, sz = d.N1 * d.N2;
-    const long long g0 = d.g(ix, iy, iz);
-    const float4 e0 = __ldg(E4 + g0), e1 = __ldg(E4 + g0 + 1), e2 = __ldg(E4 + g0 + 1 + sy),
-                 e3 = __ldg(E4 + g0 + sy), e4 = __ldg(E4 + g0 + sz), e5 = __ldg(E4 + g0 + 1 + sz),
-                 e6 = __ldg(E4 + g0 + 1 + sy + sz), e7 = __ldg(E4 + g0 + sy + sz);
+    // from the box in shared memory when the cell is in it, else from HBM
+    const float4 *Eb = E4;
+    long long g0 = d.g(ix, iy, iz), sy = d.N1, sz = d.N1 * d.N2;
+    {
+      int lx, ly, lz;
+      if (in_box(T, ix, iy, iz, lx, ly, lz)) {
+        Eb = T.E;
+        g0 = lx + TN * (ly + TN * lz);
+        sy = TN;
+        sz = TN * TN;
+      }
+    }
+    const float4 e0 = Eb[g0], e1 = Eb[g0 + 1], e2 = Eb[g0 + 1 + sy], e3 = Eb[g0 + sy], e4 = Eb[g0 + sz],
+                 e5 = Eb[g0 + 1 + sz], e6 = Eb[g0 + 1 + sy + sz], e7 = Eb[g0 + sy + sz];
     const float Ex = k0 * e0.x + ka * e1.x + kb * e2.x + kc * e3.x + kd * e4.x + ke * e5.x + kf * e6.x + kg * e7.x;
     const float Ey = k0 * e0.y + ka * e1.y + kb * e2.y + kc * e3.y + kd * e4.y + ke * e5.y + kf * e6.y + kg * e7.y;
     const float Ez = k0 * e0.z + ka * e1.z + kb * e2.z + kc * e3.z + kd * e4.z + ke * e5.z + kf * e6.z + kg * e7.z;
@@ -210,8 +250,7 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
     if (c.boris) {
       // Src/part_expmover.f90:128-160
       const float Bx = c.Bx, By = c.By, Bz = c.Bz;
-      const float B_tot = sqrtf(Bx * Bx + By * By + Bz * Bz);
-      const float kk = k1 * (2.f / (1.f + (k1 * B_tot) * (k1 * B_tot)));
+      const float kk = c.kk;
       const float v1x = vx + k1 * Ex, v1y = vy + k1 * Ey, v1z = vz + k1 * Ez;
       const float v3x = v1x + k1 * (v1y * Bz - v1z * By);
       const float v3y = v1y + k1 * (v1z * Bx - v1x * Bz);
@@ -254,7 +293,13 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
     const int cx = ax < 0 ? 0 : (ax > n1 + 1 ? n1 + 1 : ax);
     const int cy = ay < 0 ? 0 : (ay > n2 + 1 ? n2 + 1 : ay);
     const int cz = az < 0 ? 0 : (az > n3 + 1 ? n3 + 1 : az);
-    if (cw[d.c(cx, cy, cz)] || ax < 1 || ax > n1 || ay < 1 || ay > n2 || az < 1 || az > n3) {
+    bool wall;
+    {
+      int lx, ly, lz;
+      wall = in_box(T, cx, cy, cz, lx, ly, lz) ? T.cw[lx + (TN - 1) * (ly + (TN - 1) * lz)] != 0
+                                                : cw[d.c(cx, cy, cz)] != 0;
+    }
+    if (wall || ax < 1 || ax > n1 || ay < 1 || ay > n2 || az < 1 || az > n3) {
       // lost at a wall (Src/part_expmover.f90:275-433): every cell outside
       // 1..n has only wall nodes in a closed box; a cell inside 1..n is lost
       // when all of its 8 nodes are walls
@@ -298,16 +343,18 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
   }
   // holes: flag 2 and a warp-aggregated append to the hole list
   const int lane = threadIdx.x & 31;
+  if (__any_sync(full, hole[0] | hole[1] | hole[2] | hole[3])) {
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (hole[k]) flag[i0 + k] = 2;
-    const unsigned hm = __ballot_sync(full, hole[k]);
-    if (hm) {
-      const int leader = __ffs(hm) - 1;
-      int base = 0;
-      if (lane == leader) base = atomicAdd(nholes, __popc(hm));
-      base = __shfl_sync(full, base, leader);
-      if (hole[k]) holes[base + __popc(hm & lmask_lt())] = (int)(i0 + k);
+    for (int k = 0; k < 4; ++k) {
+      if (hole[k]) flag[i0 + k] = 2;
+      const unsigned hm = __ballot_sync(full, hole[k]);
+      if (hm) {
+        const int leader = __ffs(hm) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(nholes, __popc(hm));
+        base = __shfl_sync(full, base, leader);
+        if (hole[k]) holes[base + __popc(hm & lmask_lt())] = (int)(i0 + k);
+      }
     }
   }
   // deposit: merge this lane's particles that end in its first particle's cell
@@ -334,7 +381,8 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
 }
 
 // one block per tile: the particles [tile_off[t], tile_off[t+1]) of the last
-// sort, clipped to the current count
+// sort, clipped to the current count; E and the wall flags of the tile's box
+// are read into shared memory once
 __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tiles(
     Dims d, MixedConst c, const float4 *__restrict__ E4, const int *__restrict__ bcnd,
     const unsigned char *__restrict__ cw, int *__restrict__ cell, float *__restrict__ p, long long cap,
@@ -342,18 +390,43 @@ __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tiles(
     const double *__restrict__ kq, double *__restrict__ np, int *__restrict__ holes, int *__restrict__ nholes,
     double *__restrict__ acc, int *__restrict__ err) {
   __shared__ unsigned s_acc[TT];
+  __shared__ float4 s_E[TT];
+  __shared__ unsigned char s_cw[(TN - 1) * (TN - 1) * (TN - 1)];
   const int t = blockIdx.x;
   const int tx = t % c.ntx, ty = (t / c.ntx) % c.nty, tz = t / (c.ntx * c.nty);
-  Tile T{s_acc, tx * TC, ty * TC, tz * TC};
-  for (int e = threadIdx.x; e < TT; e += MBK) s_acc[e] = 0u;
+  const Tile T{s_acc, s_E, s_cw, tx * TC, ty * TC, tz * TC};
+  for (int e = threadIdx.x; e < TT; e += MBK) {
+    s_acc[e] = 0u;
+    const int lx = e % TN, ly = (e / TN) % TN, lz = e / (TN * TN);
+    const int gx = T.bx + lx, gy = T.by + ly, gz = T.bz + lz;
+    s_E[e] = (gx <= d.n1 + 2 && gy <= d.n2 + 2 && gz <= d.n3 + 2) ? __ldg(E4 + d.g(gx, gy, gz))
+                                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  for (int e = threadIdx.x; e < (TN - 1) * (TN - 1) * (TN - 1); e += MBK) {
+    const int lx = e % (TN - 1), ly = (e / (TN - 1)) % (TN - 1), lz = e / ((TN - 1) * (TN - 1));
+    const int gx = T.bx + lx, gy = T.by + ly, gz = T.bz + lz;
+    // cells beyond n+1 exist only when n is not a multiple of the tile edge:
+    // they lie outside the grid and count as walls
+    s_cw[e] = (gx <= d.n1 + 1 && gy <= d.n2 + 1 && gz <= d.n3 + 1) ? cw[d.c(gx, gy, gz)] : (unsigned char)1;
+  }
   __syncthreads();
   const long long N = *count;
   const long long lo = tile_off[t];
   long long hi = tile_off[t + 1];
   if (hi > N) hi = N;
-  for (long long base = lo & ~3LL; base < hi; base += CHUNK)
-    push_quad(d, c, T, base + 4 * threadIdx.x, lo, hi, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes,
-              nholes, acc, err);
+  int chunks = 0;
+  for (long long base = lo & ~3LL; base < hi; base += CHUNK) {
+    Quad Q;
+    const long long i0 = base + 4 * threadIdx.x;
+    load_quad(Q, i0, lo, hi, cell, p, cap, flag);
+    push_quad(d, c, T, i0, Q, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes, acc, err);
+    if (++chunks == FLUSH_PARTICLES / CHUNK && base + CHUNK < hi) {
+      chunks = 0;
+      __syncthreads();
+      flush_tile(d, T, c.kdep, kq, np);
+      __syncthreads();
+    }
+  }
   __syncthreads();
   flush_tile(d, T, c.kdep, kq, np);
 }
@@ -366,13 +439,16 @@ __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tail(
     const int *__restrict__ count, signed char *__restrict__ flag, const int *__restrict__ tile_off,
     const double *__restrict__ kq, double *__restrict__ np, int *__restrict__ holes, int *__restrict__ nholes,
     double *__restrict__ acc, int *__restrict__ err) {
-  const Tile T{nullptr, 0, 0, 0};
+  const Tile T{nullptr, nullptr, nullptr, 0, 0, 0};
   const long long N = *count;
   const long long lo = tile_off ? tile_off[c.ntiles] : 0;
   const long long first = lo & ~3LL;
-  for (long long base = first + (long long)blockIdx.x * CHUNK; base < N; base += (long long)gridDim.x * CHUNK)
-    push_quad(d, c, T, base + 4 * threadIdx.x, lo, N, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes,
-              acc, err);
+  for (long long base = first + (long long)blockIdx.x * CHUNK; base < N; base += (long long)gridDim.x * CHUNK) {
+    Quad Q;
+    const long long i0 = base + 4 * threadIdx.x;
+    load_quad(Q, i0, lo, N, cell, p, cap, flag);
+    push_quad(d, c, T, i0, Q, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes, acc, err);
+  }
 }
 
 // hole filling for the mixed layout (the FP64 kernels of the same name in
@@ -536,6 +612,11 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
   c.dth1 = (float)(P.dt / g.h[1]);
   c.dth2 = (float)(P.dt / g.h[2]);
   c.k1 = (float)(P.dt * P.charge[p] / (2.0 * P.mass[p]));
+  {
+    const float k1 = c.k1, Bx = (float)P.Bconst[0], By = (float)P.Bconst[1], Bz = (float)P.Bconst[2];
+    const float B_tot = sqrtf(Bx * Bx + By * By + Bz * Bz);
+    c.kk = k1 * (2.f / (1.f + (k1 * B_tot) * (k1 * B_tot)));
+  }
   c.Bx = (float)P.Bconst[0];
   c.By = (float)P.Bconst[1];
   c.Bz = (float)P.Bconst[2];
@@ -551,7 +632,7 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
   c.ntiles = LEPIC_TILES(g.n);
   const size_t cap = (size_t)sp.cap;
   char nm[32];
-  snprintf(nm, sizeof nm, "mixed_holes%d", p);
+  snprintf(nm, sizeof nm, "work_list%d", p);
   int *holes = (int *)scratch(nm, sizeof(int) * cap);
   snprintf(nm, sizeof nm, "mixed_tail%d", p);
   int *tailA = (int *)scratch(nm, sizeof(int) * cap);

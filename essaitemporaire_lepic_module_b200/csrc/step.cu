@@ -305,7 +305,7 @@ int launch_push_deposit(const lepic_grid_t &g, const double *Ei, lepic_species_f
   if (!sp.flag_dead) return LEPIC_ERR_ARG;
   const size_t cap = (size_t)sp.cap;
   char nm[32];
-  snprintf(nm, sizeof nm, "fused_holes%d", p);
+  snprintf(nm, sizeof nm, "work_list%d", p);
   int *holes = (int *)scratch(nm, sizeof(int) * cap);
   snprintf(nm, sizeof nm, "fused_tail%d", p);
   int *tailA = (int *)scratch(nm, sizeof(int) * cap);
