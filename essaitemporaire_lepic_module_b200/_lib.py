@@ -147,6 +147,15 @@ def lib():
         "lepic_dev_collisions_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), _I,
                                         C.POINTER(LepicTables), C.POINTER(LepicPhys), C.c_ulonglong,
                                         C.c_ulonglong, P_dbl, C.POINTER(C.c_longlong), vp], _I),
+        "lepic_dev_win_push": ([C.POINTER(LepicGrid), vp, vp, _I, _I, vp, _I, C.POINTER(LepicPhys), vp], _I),
+        "lepic_dev_win_deposit": ([C.POINTER(LepicGrid), vp, _I, _I, vp, _I, C.POINTER(LepicPhys), vp, vp], _I),
+        "lepic_dev_adj_push": ([C.POINTER(LepicGrid), vp, vp, _I, _I, vp, vp, vp, _I, _I, C.POINTER(LepicPhys),
+                                vp, vp, vp], _I),
+        "lepic_dev_adj_efield": ([C.POINTER(LepicGrid), vp, vp, vp], _I),
+        "lepic_dev_adj_rhs": ([C.POINTER(LepicGrid), vp, vp, vp], _I),
+        "lepic_dev_adj_walls": ([C.POINTER(LepicGrid), C.POINTER(LepicPhys), _I, vp, vp, vp, vp, _I, vp], _I),
+        "lepic_dev_adj_deposit": ([C.POINTER(LepicGrid), vp, _I, _I, vp, vp, vp, _I, _I, C.POINTER(LepicPhys),
+                                   vp], _I),
         "lepic_dev_load_uniform": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64), _I,
                                     C.c_longlong, C.POINTER(LepicPhys), C.c_ulonglong, vp], _I),
         "lepic_dev_cell_wall": ([P_int, vp, vp, vp], _I),
@@ -196,7 +205,9 @@ def exported_symbols():
             "lepic_dev_part_mover", "lepic_dev_push_deposit", "lepic_dev_charge_deposition", "lepic_dev_part_sorting",
             "lepic_dev_collisions", "lepic_dev_push_deposit_mixed", "lepic_dev_sort_mixed",
             "lepic_dev_pack_e32", "lepic_dev_f64_to_mixed", "lepic_dev_mixed_to_f64",
-            "lepic_dev_pdesolver_mixed", "lepic_dev_collisions_mixed", "lepic_dev_load_uniform", "lepic_dev_cell_wall",
+            "lepic_dev_pdesolver_mixed", "lepic_dev_collisions_mixed", "lepic_dev_load_uniform",
+            "lepic_dev_win_push", "lepic_dev_win_deposit", "lepic_dev_adj_push", "lepic_dev_adj_efield",
+            "lepic_dev_adj_rhs", "lepic_dev_adj_walls", "lepic_dev_adj_deposit", "lepic_dev_cell_wall",
             "lepic_dev_dens_red", "lepic_timing_enable", "lepic_timing_reset", "lepic_timing_read",
             "calc_rho_", "dens_red_", "pdesolver_", "calc_efield_",
             "part_mover_", "charge_deposition_", "part_sorting_", "collisions_",

@@ -18,6 +18,7 @@ set-ups shrunk so the FP64 CPU oracle finishes in seconds):
              captures and tests)
   poisson256 256^3 grid, two 16^3 electrodes at +-100 V, 64 Gaussian blobs
   penning    96x96x192 cells, e- 32 ppc, Bz = 0.1 T, end plates +200 V
+             (electrode labels 2 and 3), side walls 0 V (label 1)
   mcc192     192^3 cells, e- + Ar+ 128 ppc (mixed precision only)
 """
 from __future__ import annotations
@@ -106,8 +107,10 @@ def workload(name: str) -> Workload:
         n = (96, 96, 192) if name == "penning" else (16, 16, 32)
         box = _box(n, 1e-4)
         X, Y, Z = box[3], box[4], box[5]
-        seg = [box + [1], [0.0, 0.0, 0.0, X, Y, 0.0, -2], [0.0, 0.0, Z, X, Y, Z, -2]]
-        return Workload(name, n, 1e-4, seg, [0.0, 0.0, 200.0], [], Te=5.0, n0=1e15, ppc=32,
+        # end plates as separate electrodes (labels 2 at z = 0 and 3 at z = zmax)
+        # so that each has its own voltage parameter
+        seg = [box + [1], [0.0, 0.0, 0.0, X, Y, 0.0, -2], [0.0, 0.0, Z, X, Y, Z, -3]]
+        return Workload(name, n, 1e-4, seg, [0.0, 0.0, 200.0, 200.0], [], Te=5.0, n0=1e15, ppc=32,
                         dt=1e-11, steps=64, B=(0.0, 0.0, 0.1), ng=6 if name == "penning" else 5)
     raise KeyError(name)
 

@@ -367,6 +367,44 @@ int lepic_dev_cell_wall(const int *n, const int *bcnd, unsigned char *cell_wall,
 int lepic_dev_dens_red(const lepic_grid_t *g, const double *np, double *np_red, int ntype,
                        double *np_mx, void *stream);
 
+/* Adjoint window (no counterpart in the reference).  Differentiable K-step
+ * window of the collisionless FP64 step for one species in the FP64 SoA
+ * layout p[a*cap + i] (x,y,z,vx,vy,vz): particles keep their slots and
+ * alive[i] (int8, 1 = alive) marks those still in the domain.
+ *   win_push:    gather + Boris + leapfrog of the alive particles with E
+ *                (3,(n+3)^3); a particle reaching a wall cell gets alive = 0.
+ *   win_deposit: CIC deposition of the alive particles into np (accumulated,
+ *                kq applied).
+ * Adjoint of step n, in reverse order (see the window driver):
+ *   adj_push:    p = state before push n, alive_before/after = the flags
+ *                before/after it; lam (6,lcap) holds (lx, lv) of the outputs
+ *                and receives (lx, lv) of the inputs without the deposit
+ *                term; lE (3,(n+3)^3) += gather^T of the field adjoint;
+ *                *dBz += d/dBz (one device double).
+ *   adj_efield:  lphi = G^T lE (E = G phi of lepic_dev_calc_efield, Dirichlet
+ *                walls); lphi is overwritten, lE is modified (wall
+ *                extrapolations are moved onto the nodes they read).
+ *   adj_rhs:     b ((n+2)^3) = lphi on plasma nodes: the right-hand side of
+ *                the adjoint Poisson solve A mu = b, solved by
+ *                lepic_dev_pdesolver with u = mu = 0 on walls.
+ *   adj_walls:   dV[label-1] += dJ/dV_label for labels 1..nlabel (device
+ *                doubles) from lphi and mu; lnp = -q mu.
+ *   adj_deposit: lam (lx) += deposit^T(lnp) at the state before push n. */
+int lepic_dev_win_push(const lepic_grid_t *g, const double *Ei, double *p, int cap, int n, signed char *alive,
+                       int ptype, const lepic_phys_t *P, void *stream);
+int lepic_dev_win_deposit(const lepic_grid_t *g, const double *p, int cap, int n, const signed char *alive,
+                          int ptype, const lepic_phys_t *P, double *np, void *stream);
+int lepic_dev_adj_push(const lepic_grid_t *g, const double *Ei, const double *p, int cap, int n,
+                       const signed char *alive_before, const signed char *alive_after, double *lam, int lcap,
+                       int ptype, const lepic_phys_t *P, double *lE, double *dBz, void *stream);
+int lepic_dev_adj_efield(const lepic_grid_t *g, double *lE, double *lphi, void *stream);
+int lepic_dev_adj_rhs(const lepic_grid_t *g, const double *lphi, double *b, void *stream);
+int lepic_dev_adj_walls(const lepic_grid_t *g, const lepic_phys_t *P, int ptype, const double *lphi,
+                        const double *mu, double *lnp, double *dV, int nlabel, void *stream);
+int lepic_dev_adj_deposit(const lepic_grid_t *g, const double *p, int cap, int n, const signed char *alive,
+                          const double *lnp, double *lam, int lcap, int ptype, const lepic_phys_t *P,
+                          void *stream);
+
 /* Per-kernel device timers (CUDA events around each named launch).  No
  * counterpart in the reference (its MSTIMER buckets, Src/utils.f90:503-527,
  * time host phases).  read: names '\n'-separated into buf, total ms and

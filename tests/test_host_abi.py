@@ -90,8 +90,9 @@ def test_electrode_and_end_plate_geometry():
     assert np.all(st.geom.phi[st.geom.bcnd == -1] == 0.0)
     pen = config.build("penning_small")
     n1, n2, n3 = pen.n
-    assert np.all(pen.geom.bcnd[0:2] == 2) and np.all(pen.geom.bcnd[n3 + 1:] == 2)
+    assert np.all(pen.geom.bcnd[0:2] == 2) and np.all(pen.geom.bcnd[n3 + 1:] == 3)
     assert np.all(pen.geom.phi[pen.geom.bcnd == 2] == 200.0)
+    assert np.all(pen.geom.phi[pen.geom.bcnd == 3] == 200.0)
     assert np.all(pen.geom.bcnd[2:n3, 2:n2 + 1, 2:n1 + 1] == -1)
 
 
