@@ -17,7 +17,7 @@ value:  the mixed form (int32 cell + FP32 particles, FP32 V-cycles in FP64
         Particle arrays (>= 7.5 GB) are far larger than L2, so no flush is
         needed.
 e2e:    the same steps through the public host API: every step copies the
-        host-owned wall potentials (pinned) in and the potential grid and
+        host's electrode potentials (pinned) in and the potential grid and
         particle counts out.
 roofline: the dominant kernel's algorithmic bytes (mixed: 57 B per
         particle-step = read and write cell + 6 FP32 planes, read the flag;
@@ -25,6 +25,10 @@ roofline: the dominant kernel's algorithmic bytes (mixed: 57 B per
         event-timed duration, against the measured HBM copy bandwidth.
 cpu_baseline: the FP64 CPU oracle (the reference restated in C++) on the
         host cores, on a bounded sample of the same workload.
+adjoint: forward and backward time of the differentiable K-step window on the
+        Penning workload (96x96x192, 5.7e7 electrons, K = 64, checkpoints every
+        8 steps): gradient of the final mean electron energy with respect to the
+        electrode potentials, B_z and the initial velocities.
 """
 from __future__ import annotations
 
@@ -170,13 +174,17 @@ def _timed_steps(sim, steps, world, dist, torch):
 
 
 def _e2e(sim, st, steps, world, dist, torch):
-    """Steps through the public API with host buffers: the host-owned wall
-    potentials (pinned) go in and the potential grid and the particle counts
-    come out every step, inside the timed region."""
-    phi_host = torch.empty(tuple(st.geom.phi.shape), dtype=torch.float64).pin_memory()
-    phi_host.copy_(torch.as_tensor(st.geom.phi))
-    wall = torch.as_tensor(st.geom.bcnd >= 1, device=sim.dev)
-    out_phi = torch.empty_like(phi_host).pin_memory()
+    """Steps through the public API with host buffers: every step the host's
+    electrode potentials (one per wall label, pinned) go in and are applied
+    to the wall nodes, and the potential grid and the particle counts come
+    out, inside the timed region."""
+    nl = int(st.geom.ngrid)
+    v_host = torch.zeros(nl + 2, dtype=torch.float64).pin_memory()
+    for lab in range(1, nl + 1):
+        v_host[lab] = float(st.wl.V[lab]) if lab < len(st.wl.V) else 0.0
+    label = sim.bcnd.long().clamp(0, nl + 1)
+    wall = sim.bcnd >= 1
+    out_phi = torch.empty(tuple(st.geom.phi.shape), dtype=torch.float64).pin_memory()
     out_cnt = torch.empty(len(sim.sp), dtype=torch.int32).pin_memory()
     torch.cuda.synchronize()
     if world > 1:
@@ -184,8 +192,8 @@ def _e2e(sim, st, steps, world, dist, torch):
     t0 = time.perf_counter()
     nps = 0
     for _ in range(steps):
-        dphi = phi_host.to(sim.dev, non_blocking=True)
-        sim.phi[wall] = dphi[wall]
+        v_dev = v_host.to(sim.dev, non_blocking=True)
+        torch.where(wall, v_dev[label], sim.phi, out=sim.phi)
         sim.step()
         out_phi.copy_(sim.phi, non_blocking=True)
         out_cnt.copy_(torch.cat([s.count for s in sim.sp]), non_blocking=True)
@@ -200,7 +208,7 @@ def _e2e(sim, st, steps, world, dist, torch):
         dist.all_reduce(c)
         nps = float(c.item())
     return {"value": nps / e2e_s, "unit": UNIT, "steps": steps,
-            "h2d_bytes_per_step": int(phi_host.numel() * 8),
+            "h2d_bytes_per_step": int(v_host.numel() * 8),
             "d2h_bytes_per_step": int(out_phi.numel() * 8 + out_cnt.numel() * 4)}
 
 
@@ -263,6 +271,43 @@ def _phi_err(sim, st, torch):
     return float((sim.phi - phi64).abs().max() / phi64.abs().max())
 
 
+def run_adjoint(workload, K, every):
+    """Adjoint/forward cost of the differentiable window: the gradient of the
+    final mean electron energy with respect to the electrode potentials, B_z
+    and the initial velocities (FP64 discrete adjoint, checkpoints every
+    `every` steps, recomputed)."""
+    import torch
+    from essaitemporaire_lepic_module_b200 import config
+    from essaitemporaire_lepic_module_b200.adjoint import Window, window_objective
+    st = config.build(workload)
+    win = Window(st, K=K, every=every)
+    win.load_uniform(seed=20240611)
+    V0 = [float(st.wl.V[lab]) if lab < len(st.wl.V) else 0.0 for lab in range(1, win.nlabel + 1)]
+    V = torch.tensor(V0, dtype=torch.float64, requires_grad=True)
+    Bz = torch.tensor(float(st.Bconst[2]), dtype=torch.float64, requires_grad=True)
+    v0 = win.x0[3:6].clone().requires_grad_(True)
+    from essaitemporaire_lepic_module_b200 import _lib
+    win.forward(V0, float(Bz))  # warm-up (allocations)
+    J = window_objective(win, V, Bz, v0)
+    _lib.timing(enable=True)
+    _lib.timing(reset=True)
+    J.backward()
+    timers = _lib.timing()
+    _lib.timing(enable=False)
+    t = dict(win.timing)
+    out = {"workload": f"{workload} {list(st.n)} cells, {win.n} particles of species 1, K={K}, "
+                       f"checkpoint every {every}, FP64",
+           "observable": "mean kinetic energy (eV) after K steps",
+           "J": float(J), "dJ_dV_by_label": [float(x) for x in V.grad], "dJ_dBz": float(Bz.grad),
+           "dJ_dv0_norm": float(v0.grad.norm()),
+           "forward_ms": t["forward_ms"], "backward_ms": t["backward_ms"],
+           "backward_over_forward": t["backward_ms"] / t["forward_ms"],
+           "backward_kernel_ms": {k: round(v[0], 3) for k, v in sorted(timers.items())}}
+    del win, v0
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -323,6 +368,11 @@ def run_ours(args):
         if "e2e" in F:
             line["f64"]["e2e"] = F["e2e"]
         line["mixed_over_f64"] = R["value"] / F["value"]
+    if args.adjoint:
+        del res
+        R = None
+        torch.cuda.empty_cache()
+        line["adjoint"] = run_adjoint(args.adjoint_workload, args.adjoint_k, args.adjoint_every)
     if args.cpu_baseline and world == 1:
         try:
             line["cpu_baseline"] = cpu_baseline(args.workload, steps=args.cpu_steps, ppc=args.cpu_ppc)
@@ -349,6 +399,11 @@ def main():
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "f64"],
                     help="both: time the FP64 form, then the mixed form (the headline)")
     ap.add_argument("--e2e-all", action="store_true", help="also measure e2e for the FP64 form")
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
+                    help="skip the adjoint window measurement")
+    ap.add_argument("--adjoint-workload", default="penning")
+    ap.add_argument("--adjoint-k", type=int, default=64)
+    ap.add_argument("--adjoint-every", type=int, default=8)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -56,20 +56,33 @@ class Window:
         self.timing = {}
 
     # ------------------------------------------------------------ set-up
+    def _adopt(self, p0):
+        """The window's own particle order: sorted by cell, so that the
+        deposition and its transposes of neighbouring threads touch
+        neighbouring nodes.  `order` maps window slots to the input order."""
+        h = self.st.h
+        n1, n2, _ = self.st.n
+        ix = (p0[0] / h[0]).long()
+        iy = (p0[1] / h[1]).long()
+        iz = (p0[2] / h[2]).long()
+        self.order = torch.argsort(ix + n1 * (iy + n2 * iz))
+        self.x0 = p0[:, self.order].contiguous()
+        self.n = int(p0.shape[1])
+
     def load_uniform(self, seed=None):
         """Initial state from the GPU loader (positions, Maxwellian v)."""
         self.sim.load_uniform(seed=seed)
         s = self.sim.sp[self.ptype - 1]
-        self.n = s.n()
-        self.x0 = s.p[:, :self.n].clone()
+        self._adopt(s.p[:, :s.n()])
         self.np_fixed = self.sim.np.clone()
         self.np_fixed[self.ptype - 1].zero_()
 
     def load(self, p0):
         """Initial state (6, n) FP64 device tensor x, y, z, vx, vy, vz of the
-        species; the other species carry no charge."""
-        self.x0 = p0.clone()
-        self.n = int(p0.shape[1])
+        species; the other species carry no charge.  The window keeps the
+        particles in its own order (x0, initial velocities and their
+        gradients are in that order; `order` maps it to p0's)."""
+        self._adopt(p0)
         self.np_fixed = torch.zeros_like(self.sim.np)
 
     def _s(self):
@@ -155,7 +168,6 @@ class Window:
         from .constants import EPS0
         ac = 2.0 * EPS0 * (1.0 / h[0] ** 2 + 1.0 / h[1] ** 2 + 1.0 / h[2] ** 2)
         alpha = (n1 + 1) * (n2 + 1) * (n3 + 1) * ac
-        zeros_phi = torch.zeros_like(sim.phi)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record()
         nseg = len(self.ckpt)
@@ -178,8 +190,8 @@ class Window:
                       "adj_push")
                 check(L.lepic_dev_adj_efield(C.byref(sim.grid), _p(lE), _p(lphi), self._s()), "adj_efield")
                 check(L.lepic_dev_adj_rhs(C.byref(sim.grid), _p(lphi), _p(b), self._s()), "adj_rhs")
+                # warm start: mu of the later step (walls stay 0)
                 r0 = float(b.abs().sum()) / alpha
-                mu.copy_(zeros_phi)
                 if r0 > 0.0:
                     k, kt, res = C.c_int(0), C.c_double(0), C.c_double(0)
                     check(L.lepic_dev_pdesolver(C.byref(sim.grid), _p(mu), _p(b), wl.ncycl, wl.eps * r0,

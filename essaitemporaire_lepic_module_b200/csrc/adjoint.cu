@@ -78,6 +78,40 @@ __device__ __forceinline__ void dweight(const WinConst &k, const Cic &w, int c, 
   gz = fx * fy * sz;
 }
 
+__device__ __forceinline__ unsigned lanemask_le() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_le;" : "=r"(m));
+  return m;
+}
+
+// Sum of v over each run of consecutive lanes with the same key: afterwards
+// the first lane of a run (head) holds the run's totals.  Lanes with key -1
+// contribute zeros.  All 32 lanes must call this.  The window's particles are
+// sorted by cell, so a warp holds few runs and the atomics that follow are
+// one per run instead of one per particle.
+template <int NV>
+__device__ __forceinline__ bool warp_run_sum(long long key, double (&v)[NV]) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const long long prev = __shfl_up_sync(full, key, 1);
+  const bool head = (lane == 0) || prev != key;
+  const unsigned heads = __ballot_sync(full, head);
+  const int rid = __popc(heads & lanemask_le());
+  const unsigned above = heads & ~(0xffffffffu >> (31 - lane));
+  const int len = head ? ((above ? __ffs(above) - 1 : 32) - lane) : 0;
+  const int maxlen = (int)__reduce_max_sync(full, (unsigned)len);
+  for (int o = 1; o < maxlen; o <<= 1) {
+    const int orid = __shfl_down_sync(full, rid, o);
+    const bool same = (lane + o < 32) && orid == rid;
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+      const double t = __shfl_down_sync(full, v[c], o);
+      if (same) v[c] += t;
+    }
+  }
+  return head && key >= 0;
+}
+
 __device__ __forceinline__ void cross(double ax, double ay, double az, double bx, double by, double bz, double &rx,
                                       double &ry, double &rz) {
   rx = ay * bz - az * by;
@@ -143,16 +177,26 @@ __global__ void __launch_bounds__(AB) k_win_deposit(Dims d, WinConst c, const do
                                                     const double *__restrict__ kq, double *__restrict__ np,
                                                     int *err) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= n || !alive[i]) return;
   Cic w;
-  if (!cic(d, c, p[i], p[cap + i], p[2 * cap + i], w)) {
-    raise_err(err, LEPIC_ERR_CELL, (int)i);
-    return;
-  }
+  long long key = -1;
+  double v[8];
 #pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    const long long g = node(d, w, q);
-    atomicAdd(&np[g], kq[g] * (c.kdep * weight(w, q)));
+  for (int q = 0; q < 8; ++q) v[q] = 0.0;
+  if (i < n && alive[i]) {
+    if (cic(d, c, p[i], p[cap + i], p[2 * cap + i], w)) {
+      key = w.g0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = weight(w, q);
+    } else {
+      raise_err(err, LEPIC_ERR_CELL, (int)i);
+    }
+  }
+  if (warp_run_sum<8>(key, v)) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const long long g = node(d, w, q);
+      atomicAdd(&np[g], kq[g] * (c.kdep * v[q]));
+    }
   }
 }
 
@@ -168,6 +212,11 @@ __global__ void __launch_bounds__(AB) k_adj_push(Dims d, WinConst c, const doubl
                                                  double *dBz) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   double gB = 0.0;
+  long long key = -1;
+  Cic g0;
+  double sc[24];
+#pragma unroll
+  for (int q = 0; q < 24; ++q) sc[q] = 0.0;
   if (i < n && alive_before[i]) {
     double lx = lam[i], ly = lam[lcap + i], lz = lam[2 * lcap + i];
     double lvx = lam[3 * lcap + i], lvy = lam[4 * lcap + i], lvz = lam[5 * lcap + i];
@@ -230,14 +279,14 @@ __global__ void __launch_bounds__(AB) k_adj_push(Dims d, WinConst c, const doubl
       lEy = 2.0 * c.k1 * lvy;
       lEz = 2.0 * c.k1 * lvz;
     }
-    // gather^T into lE and the weight gradient into lx
+    // the weight gradient of the gather into lx; gather^T below
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const long long g = node(d, w, q);
       const double wq = weight(w, q);
-      atomicAdd(&lE[3 * g + 0], wq * lEx);
-      atomicAdd(&lE[3 * g + 1], wq * lEy);
-      atomicAdd(&lE[3 * g + 2], wq * lEz);
+      sc[3 * q + 0] = wq * lEx;
+      sc[3 * q + 1] = wq * lEy;
+      sc[3 * q + 2] = wq * lEz;
       double gx, gy, gz;
       dweight(c, w, q, gx, gy, gz);
       const double s = Ei[3 * g] * lEx + Ei[3 * g + 1] * lEy + Ei[3 * g + 2] * lEz;
@@ -245,12 +294,24 @@ __global__ void __launch_bounds__(AB) k_adj_push(Dims d, WinConst c, const doubl
       ly += gy * s;
       lz += gz * s;
     }
+    key = w.g0;
+    g0 = w;
     lam[i] = lx;
     lam[lcap + i] = ly;
     lam[2 * lcap + i] = lz;
     lam[3 * lcap + i] = ux;
     lam[4 * lcap + i] = uy;
     lam[5 * lcap + i] = uz;
+  }
+  // gather^T: lE at the 8 nodes, summed over the runs of the warp
+  if (warp_run_sum<24>(key, sc)) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const long long g = node(d, g0, q);
+      atomicAdd(&lE[3 * g + 0], sc[3 * q + 0]);
+      atomicAdd(&lE[3 * g + 1], sc[3 * q + 1]);
+      atomicAdd(&lE[3 * g + 2], sc[3 * q + 2]);
+    }
   }
   // block sum of the B_z derivative
   for (int o = 16; o > 0; o >>= 1) gB += __shfl_xor_sync(0xffffffffu, gB, o);
