@@ -212,6 +212,13 @@ def _e2e(sim, st, steps, world, dist, torch):
             "d2h_bytes_per_step": int(out_phi.numel() * 8 + out_cnt.numel() * 4)}
 
 
+# DRAM bytes per particle of each push kernel from an ncu capture of one launch
+# on the 96^3 workload (5.7e7 particles per species); the traffic grows in
+# proportion to the particles, so a launch's traffic is this times its
+# particles
+MEASURED_TRAFFIC_PER_PARTICLE = {"push_deposit_mixed": 57.4, "push_deposit_f64": 96.6}
+
+
 def _roofline(timers, kname, bytes_per_particle, nps):
     peak, peak_kind = measured_peaks()
     push = timers.get(kname, (0.0, 0))
@@ -219,9 +226,12 @@ def _roofline(timers, kname, bytes_per_particle, nps):
     per_launch_particles = nps / max(push[1], 1)
     bytes_per_launch = bytes_per_particle * per_launch_particles
     achieved = bytes_per_launch / (push[0] / max(push[1], 1) / 1e3) / 1e9 if push[1] else None
+    tpp = MEASURED_TRAFFIC_PER_PARTICLE.get(kname)
     return {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-            "traffic": None, "algorithmic_bytes_per_launch": bytes_per_launch,
+            "traffic": tpp * per_launch_particles if tpp else None,
+            "traffic_source": "ncu DRAM bytes per particle at 96^3 x particles per launch" if tpp else None,
+            "algorithmic_bytes_per_launch": bytes_per_launch,
             "algorithmic_bytes_per_particle": bytes_per_particle, "top_kernel": top[0]}
 
 
