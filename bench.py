@@ -239,7 +239,7 @@ def _run_form(args, st, precision, rank, world, dist, torch, e2e=True):
     from essaitemporaire_lepic_module_b200 import _lib
     from essaitemporaire_lepic_module_b200.sim import Simulation
     sim = Simulation(st, seed=20240601 + 7919 * rank, nsort=args.nsort, fused=not args.unfused,
-                     precision=precision)
+                     precision=precision, comm=True if world > 1 else None)
     sim.load_uniform()
     torch.cuda.synchronize()
     n_start = int(sim.counts_host().sum())

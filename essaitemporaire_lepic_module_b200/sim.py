@@ -38,6 +38,22 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr())
 
 
+def allreduce_density(np_grids, group=None):
+    """Sum the per-rank density grids over the ranks of `group` in place:
+    every rank holds its own particles over the full grid, and the field
+    needs the density of all of them (the MPI_ALLREDUCE of rho of
+    Src/calc_rho.f90:102).  One collective of the (ntype, nodes) FP64 grids."""
+    import torch.distributed as dist
+    dist.all_reduce(np_grids, op=dist.ReduceOp.SUM, group=group)
+    return np_grids
+
+
+def rank_weight(Nm, world):
+    """Macroparticle weight of each of `world` ranks that each load a full
+    set of particles of weight Nm: Nm / world keeps the plasma density."""
+    return Nm / float(world)
+
+
 class Species:
     """One species' FP64 particle store on the device."""
 
@@ -110,8 +126,13 @@ class SpeciesMixed:
 
 
 class Simulation:
+    """Device-resident timestep.  With `comm` (a torch.distributed process
+    group, or True for the default group) each rank holds its own particles
+    at weight Nm / world, the density grids are all-reduced after every
+    deposition and every rank solves the same field."""
+
     def __init__(self, st, cap=None, device="cuda", seed=123456, nsort=None, ns_coll=None,
-                 fused=True, precision="f64", mg_mixed=None):
+                 fused=True, precision="f64", mg_mixed=None, comm=None):
         if precision not in ("f64", "mixed"):
             raise ValueError(f"precision must be 'f64' or 'mixed', not {precision!r}")
         self.st = st
@@ -129,6 +150,13 @@ class Simulation:
         self.ns_coll = st.wl.ns_coll if ns_coll is None else ns_coll
         self.seed = int(seed)
         self.P = phys_struct(st)
+        self.comm = comm
+        if comm is not None:
+            import torch.distributed as dist
+            self._group = None if comm is True else comm
+            world = dist.get_world_size(self._group)
+            for p in range(st.ntype):
+                self.P.Nm[p] = rank_weight(st.Nm[p], world)
         g = st.geom
         T = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=self.dev)
         self.bcnd = T(g.bcnd, torch.int32)
@@ -351,6 +379,11 @@ class Simulation:
             check(lib().lepic_dev_charge_deposition(C.byref(self.grid), C.byref(s.s), p + 1,
                                                     C.byref(self.P), C.c_void_p(self.np[p].data_ptr()),
                                                     self._s()), "charge_deposition")
+        self._reduce_density()
+
+    def _reduce_density(self):
+        if self.comm is not None:
+            allreduce_density(self.np, self._group)
 
     def move_deposit(self):
         """Fused in-place push + deposition of every species (the step path);
@@ -376,6 +409,7 @@ class Simulation:
                                                C.c_void_p(self.np[p].data_ptr()),
                                                C.c_void_p(self._acc[p].data_ptr()), int(counts[p]),
                                                self._s()), "push_deposit")
+        self._reduce_density()
 
     def loss_stats(self):
         """(p_mac (ngrid+1, 2, ntype), P_loss (ntype, 4)) accumulated so far."""
