@@ -11,17 +11,16 @@
 // (f += v dt/h, cell += floor(f)), which keeps ~7 significant digits of the
 // position inside its cell.
 //
-// Deposition (Src/part_expmover.f90:591-656) of the new position: the eight
-// CIC weights are rounded to integers in units of 2^-20 and the rounding
-// residue is added to the weight of the nearest node, so every particle
-// deposits exactly 2^20 units and integer sums are exact and independent of
-// the summation order.  The sort orders particles by 8x8x8-cell tiles; one
+// Deposition (Src/part_expmover.f90:591-656) of the new position: seven of
+// the eight CIC weights are rounded to integers in units of 2^-20 and the
+// eighth is the remainder, so every particle deposits exactly 2^20 units and
+// integer sums are exact and independent of the summation order.  The sort orders particles by 8x8x8-cell tiles; one
 // block pushes the particles of one tile and sums their weights with 32-bit
 // shared-memory adds into a node tile covering the tile's cells plus one halo
 // cell on each side.  The node tile is added to the FP64 grid (one atomic per
 // non-zero node) and cleared after every FLUSH_PARTICLES particles, so a
-// node's sum stays below FLUSH_PARTICLES * 2^20 = 2^31 however the particles
-// are placed.  Particles outside the box (drifted since the sort, moved by
+// node's sum stays within [-5 FLUSH_PARTICLES, FLUSH_PARTICLES * 2^20 = 2^31]
+// however the particles are placed.  Particles outside the box (drifted since the sort, moved by
 // hole filling, appended by collisions) add their integer weights to the grid
 // directly.  kdep and kq are applied in FP64 to the integer sums.
 //
@@ -75,7 +74,11 @@ __device__ __forceinline__ int round_q(float x) { return __float_as_int(x + 1258
 
 // integer CIC weights of offsets (gx, gy, gz) in units of 2^-20 summing to
 // exactly 2^20 (node order of Src/part_expmover.f90:591-656: (0,0,0),
-// (1,0,0), (1,1,0), (0,1,0), then the same at z+1)
+// (1,0,0), (1,1,0), (0,1,0), then the same at z+1): seven rounded, the
+// eighth the remainder.  The remainder may be a few units below zero for a
+// particle next to the opposite corner (the seven rounding errors are at
+// most 0.7 units each); the 32-bit node sums are exact modulo 2^32 and
+// flush_tile reads them back from that range.
 __device__ __forceinline__ void qweights(float gx, float gy, float gz, int w[8]) {
   const float S = (float)(1 << QBITS);
   const float qx = 1.f - gx, qy = 1.f - gy, qz = 1.f - gz;
@@ -87,13 +90,7 @@ __device__ __forceinline__ void qweights(float gx, float gy, float gz, int w[8])
   w[4] = round_q(qx * e);
   w[5] = round_q(gx * e);
   w[6] = round_q(gx * f);
-  w[7] = round_q(qx * f);
-  const int r = (1 << QBITS) - (w[0] + w[1] + w[2] + w[3] + w[4] + w[5] + w[6] + w[7]);
-  // nearest node: its weight is at least 1/8, so it stays positive
-  const int nx = gx >= 0.5f, ny = gy >= 0.5f, nz = gz >= 0.5f;
-  const int near = (ny ? (nx ? 2 : 3) : (nx ? 1 : 0)) + 4 * nz;
-#pragma unroll
-  for (int c = 0; c < 8; ++c) w[c] += (c == near) ? r : 0;
+  w[7] = (1 << QBITS) - (w[0] + w[1] + w[2] + w[3] + w[4] + w[5] + w[6]);
 }
 
 // The block's box in shared memory: the nodes bx..bx+TN-1 (and likewise in
@@ -143,7 +140,10 @@ __device__ void flush_tile(const Dims &d, const Tile &T, double kdep, const doub
       const int gx = T.bx + lx, gy = T.by + ly, gz = T.bz + lz;
       if (gx <= d.n1 + 2 && gy <= d.n2 + 2 && gz <= d.n3 + 2) {
         const long long node = d.g(gx, gy, gz);
-        atomicAdd(&np[node], __ldg(&kq[node]) * (kdep * ((double)v * QI)));
+        // a node's sum over a window lies in [-5 FLUSH_PARTICLES, 2^31]
+        // (a remainder weight is at least -5 units): read it modulo 2^32
+        const double val = v <= 0x80000000u ? (double)v : (double)v - 4294967296.0;
+        atomicAdd(&np[node], __ldg(&kq[node]) * (kdep * (val * QI)));
       }
       T.acc[e] = 0u;
     }
