@@ -138,6 +138,10 @@ def lib():
                                           _I, C.POINTER(LepicPhys), vp, vp, _I, vp], _I),
         "lepic_dev_sort_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), _I, vp], _I),
         "lepic_dev_pack_e32": ([vp, vp, C.c_longlong, vp], _I),
+        "lepic_dev_load_uniform_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), _I, C.c_longlong,
+                                          C.POINTER(LepicPhys), C.c_ulonglong, vp], _I),
+        "lepic_dev_deposit_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), _I,
+                                     C.POINTER(LepicPhys), vp, _I, vp], _I),
         "lepic_dev_f64_to_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64),
                                     C.POINTER(LepicSpeciesMixed), C.c_longlong, vp], _I),
         "lepic_dev_mixed_to_f64": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), vp,
@@ -204,7 +208,7 @@ def exported_symbols():
             "lepic_dev_pdesolver_noalloc",
             "lepic_dev_part_mover", "lepic_dev_push_deposit", "lepic_dev_charge_deposition", "lepic_dev_part_sorting",
             "lepic_dev_collisions", "lepic_dev_push_deposit_mixed", "lepic_dev_sort_mixed",
-            "lepic_dev_pack_e32", "lepic_dev_f64_to_mixed", "lepic_dev_mixed_to_f64",
+            "lepic_dev_pack_e32", "lepic_dev_load_uniform_mixed", "lepic_dev_deposit_mixed", "lepic_dev_f64_to_mixed", "lepic_dev_mixed_to_f64",
             "lepic_dev_pdesolver_mixed", "lepic_dev_collisions_mixed", "lepic_dev_load_uniform",
             "lepic_dev_win_push", "lepic_dev_win_deposit", "lepic_dev_adj_push", "lepic_dev_adj_efield",
             "lepic_dev_adj_rhs", "lepic_dev_adj_walls", "lepic_dev_adj_deposit", "lepic_dev_cell_wall",

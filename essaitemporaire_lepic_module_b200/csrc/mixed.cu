@@ -586,6 +586,86 @@ __global__ void k_mixed_to_f64(Dims d, double h0, double h1, double h2, const in
   pout[5 * capout + i] = p[5 * cap + i];
 }
 
+// GPU particle loader for the mixed layout: the draws of k_load_uniform
+// (Philox4x32-10 per sample: positions uniform in the loading box outside
+// all-wall cells, co-located species, Maxwellian velocities of the
+// load_gauss form of Src/load_part.f90:233-244) written as cell + FP32
+// offsets and velocities, so that large workloads need no FP64 copy.
+struct LoadMixed {
+  double xl, ym, zm, h0, h1, h2;
+  double vt[LEPIC_NPART];
+  int ntype;
+  unsigned k0, k1;
+  int *cell[LEPIC_NPART];
+  float *p[LEPIC_NPART];
+  long long cap[LEPIC_NPART];
+};
+
+__global__ void k_load_uniform_mixed(Dims d, LoadMixed c, long long n, const unsigned char *__restrict__ cw,
+                                     int *err) {
+  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double x = 0, y = 0, z = 0;
+  int ix = 1, iy = 1, iz = 1;
+  bool ok = false;
+  for (uint32_t tr = 0; tr < 64 && !ok; ++tr) {
+    U4 r = philox4x32_10({(uint32_t)j, (uint32_t)(j >> 32), tr, 0xA5A5u}, c.k0, c.k1);
+    x = u01(r.x) * c.xl;
+    y = u01(r.y) * c.ym;
+    z = u01(r.z) * c.zm;
+    ix = (int)(x / c.h0) + 1;
+    iy = (int)(y / c.h1) + 1;
+    iz = (int)(z / c.h2) + 1;
+    ok = !cw[d.c(ix, iy, iz)];
+  }
+  if (!ok) raise_err(err, LEPIC_ERR_CELL, (int)j);
+  ix = ix > d.n1 ? d.n1 : ix;
+  iy = iy > d.n2 ? d.n2 : iy;
+  iz = iz > d.n3 ? d.n3 : iz;
+  const int cc = (ix - 1) | (iy - 1) << CB | (iz - 1) << (2 * CB);
+  float fx = (float)(x / c.h0 - (ix - 1)), fy = (float)(y / c.h1 - (iy - 1)), fz = (float)(z / c.h2 - (iz - 1));
+  fx = fx >= 1.f ? 0.99999994f : fx;
+  fy = fy >= 1.f ? 0.99999994f : fy;
+  fz = fz >= 1.f ? 0.99999994f : fz;
+  for (int q = 0; q < c.ntype; ++q) {
+    U4 r = philox4x32_10({(uint32_t)j, (uint32_t)(j >> 32), 1000u + q, 0x5A5Au}, c.k0, c.k1);
+    const double vt = c.vt[q];
+    double s1, c1, s2, c2;
+    sincos(2.0 * 3.141592653589793 * u01(r.y), &s1, &c1);
+    sincos(2.0 * 3.141592653589793 * u01(r.w), &s2, &c2);
+    const double vp = vt * sqrt(-log(u01(r.x)));
+    const double vq = vt * sqrt(-log(u01(r.z)));
+    float *P = c.p[q];
+    const long long cap = c.cap[q];
+    c.cell[q][j] = cc;
+    P[j] = fx;
+    P[cap + j] = fy;
+    P[2 * cap + j] = fz;
+    P[3 * cap + j] = (float)(vp * c1);
+    P[4 * cap + j] = (float)(vp * s1);
+    P[5 * cap + j] = (float)(vq * c2);
+  }
+}
+
+// CIC deposition of a mixed-layout species with the integer weights of the
+// push (the initial charge of a loaded state)
+__global__ void k_deposit_mixed(Dims d, double kdep, const int *__restrict__ cell, const float *__restrict__ p,
+                                long long cap, const int *__restrict__ count, const double *__restrict__ kq,
+                                double *__restrict__ np, int *err) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= *count) return;
+  const int cc = cell[i];
+  const int ix = (cc & CM) + 1, iy = ((cc >> CB) & CM) + 1, iz = (cc >> (2 * CB)) + 1;
+  if (cc < 0 || ix > d.n1 || iy > d.n2 || iz > d.n3) {
+    raise_err(err, LEPIC_ERR_CELL, (int)i);
+    return;
+  }
+  int w[8];
+  qweights(p[i], p[cap + i], p[2 * cap + i], w);
+  const Tile T{nullptr, nullptr, nullptr, 0, 0, 0};
+  deposit8(d, T, ix, iy, iz, d.g(ix, iy, iz), w, kdep, kq, np);
+}
+
 bool aligned16(const void *q) { return ((uintptr_t)q & 15u) == 0; }
 
 int check_layout(const lepic_grid_t &g, const lepic_species_mixed_t &sp) {
@@ -698,6 +778,50 @@ int launch_sort_mixed(const lepic_grid_t &g, lepic_species_mixed_t &sp, int n_hi
   return LEPIC_OK;
 }
 
+int launch_load_uniform_mixed(const lepic_grid_t &g, lepic_species_mixed_t *sp, int ntype, long long n,
+                              const lepic_phys_t &P, unsigned long long seed, cudaStream_t s) {
+  Dims d(g.n);
+  if (ntype < 1 || ntype > LEPIC_NPART) return LEPIC_ERR_ARG;
+  LoadMixed c;
+  memset(&c, 0, sizeof(c));
+  c.xl = P.x_load;
+  c.ym = P.ymax;
+  c.zm = P.zmax;
+  c.h0 = g.h[0];
+  c.h1 = g.h[1];
+  c.h2 = g.h[2];
+  for (int q = 0; q < LEPIC_NPART; ++q) c.vt[q] = P.vt0[q];
+  c.ntype = ntype;
+  c.k0 = (unsigned)(seed & 0xffffffffu);
+  c.k1 = (unsigned)(seed >> 32);
+  for (int q = 0; q < ntype; ++q) {
+    if (int rc = check_layout(g, sp[q])) return rc;
+    if (n > sp[q].cap) return LEPIC_ERR_CAPACITY;
+    c.cell[q] = sp[q].cell;
+    c.p[q] = sp[q].p;
+    c.cap[q] = sp[q].cap;
+  }
+  if (n > 0) k_load_uniform_mixed<<<grid_for(n, 256), 256, 0, s>>>(d, c, n, g.cell_wall, ctx().d_err);
+  LEPIC_CUDA(cudaGetLastError());
+  const int nn = (int)n;
+  for (int q = 0; q < ntype; ++q) {
+    LEPIC_CUDA(cudaMemcpyAsync(sp[q].count, &nn, sizeof(int), cudaMemcpyHostToDevice, s));
+    if (sp[q].tile_off) LEPIC_CUDA(cudaMemsetAsync(sp[q].tile_off, 0, sizeof(int) * (LEPIC_TILES(g.n) + 1), s));
+  }
+  return check_err(s);
+}
+
+int launch_deposit_mixed(const lepic_grid_t &g, const lepic_species_mixed_t &sp, int ptype, const lepic_phys_t &P,
+                         double *np, int n_hint, cudaStream_t s) {
+  Dims d(g.n);
+  const double kdep = P.Nm[ptype - 1] / (g.h[0] * g.h[1] * g.h[2]);
+  const int nthreads = n_hint > 0 ? n_hint : sp.cap;
+  k_deposit_mixed<<<grid_for(nthreads, 256), 256, 0, s>>>(d, kdep, sp.cell, sp.p, sp.cap, sp.count, g.kq, np,
+                                                        ctx().d_err);
+  LEPIC_CUDA(cudaGetLastError());
+  return check_err(s);
+}
+
 int launch_pack_e32(const double *Ei, float *E4, long long nodes, cudaStream_t s) {
   if (!aligned16(E4)) return LEPIC_ERR_ARG;
   k_pack_e32<<<grid_for(nodes, 256), 256, 0, s>>>(Ei, reinterpret_cast<float4 *>(E4), nodes);
@@ -742,6 +866,19 @@ int lepic_dev_push_deposit_mixed(const lepic_grid_t *g, const float *E4, lepic_s
 int lepic_dev_sort_mixed(const lepic_grid_t *g, lepic_species_mixed_t *s, int n_hint, void *stream) {
   if (!g || !s) return LEPIC_ERR_ARG;
   return lepic::launch_sort_mixed(*g, *s, n_hint, (cudaStream_t)stream);
+}
+
+int lepic_dev_load_uniform_mixed(const lepic_grid_t *g, lepic_species_mixed_t *sp, int ntype,
+                                 long long n_per_species, const lepic_phys_t *P, unsigned long long seed,
+                                 void *stream) {
+  if (!g || !sp || !P || n_per_species < 0) return LEPIC_ERR_ARG;
+  return lepic::launch_load_uniform_mixed(*g, sp, ntype, n_per_species, *P, seed, (cudaStream_t)stream);
+}
+
+int lepic_dev_deposit_mixed(const lepic_grid_t *g, const lepic_species_mixed_t *s, int ptype, const lepic_phys_t *P,
+                            double *np, int n_hint, void *stream) {
+  if (!g || !s || !P || !np || ptype < 1) return LEPIC_ERR_ARG;
+  return lepic::launch_deposit_mixed(*g, *s, ptype, *P, np, n_hint, (cudaStream_t)stream);
 }
 
 int lepic_dev_pack_e32(const double *Ei, float *E4, long long nodes, void *stream) {

@@ -252,16 +252,23 @@ class Simulation:
     def load_uniform(self, n_per_species=None, seed=None):
         """GPU Philox loader + initial deposition."""
         n = self.st.n_particles() if n_per_species is None else int(n_per_species)
-        dst = self._f64_stage() if self.mixed else self.sp
-        arr = (LepicSpeciesF64 * len(dst))(*[s.s for s in dst])
-        check(lib().lepic_dev_load_uniform(C.byref(self.grid), arr, len(dst), C.c_longlong(n),
+        if self.mixed:
+            arr = (LepicSpeciesMixed * len(self.sp))(*[s.s for s in self.sp])
+            check(lib().lepic_dev_load_uniform_mixed(C.byref(self.grid), arr, len(self.sp), C.c_longlong(n),
+                                                     C.byref(self.P), C.c_ulonglong(seed or self.seed),
+                                                     self._s()), "load_uniform_mixed")
+            self.np.zero_()
+            for p, s in enumerate(self.sp):
+                check(lib().lepic_dev_deposit_mixed(C.byref(self.grid), C.byref(s.s), p + 1, C.byref(self.P),
+                                                    C.c_void_p(self.np[p].data_ptr()), n, self._s()),
+                      "deposit_mixed")
+            self._reduce_density()
+            return
+        arr = (LepicSpeciesF64 * len(self.sp))(*[s.s for s in self.sp])
+        check(lib().lepic_dev_load_uniform(C.byref(self.grid), arr, len(self.sp), C.c_longlong(n),
                                            C.byref(self.P), C.c_ulonglong(seed or self.seed),
                                            self._s()), "load_uniform")
-        self._deposit_f64(dst)
-        if self.mixed:
-            self._adopt_f64(dst)
-            del dst
-            torch.cuda.empty_cache()
+        self._deposit_f64(self.sp)
 
     def particles_f64(self, p):
         """Species p as FP64 (6, n) x, y, z, vx, vy, vz on the device."""

@@ -306,6 +306,16 @@ int lepic_dev_push_deposit_mixed(const lepic_grid_t *g, const float *E4, lepic_s
 /* Src/sorting.f90:97-258 for the mixed layout: counting sort on the stored
  * cell in tile order (swaps the buffers inside *s, writes s->tile_off). */
 int lepic_dev_sort_mixed(const lepic_grid_t *g, lepic_species_mixed_t *s, int n_hint, void *stream);
+/* GPU particle loader for the mixed layout: the same Philox draws as
+ * lepic_dev_load_uniform written as cell + FP32 offsets and velocities (no
+ * FP64 copy); clears s->tile_off. */
+int lepic_dev_load_uniform_mixed(const lepic_grid_t *g, lepic_species_mixed_t *sp, int ntype,
+                                 long long n_per_species, const lepic_phys_t *P, unsigned long long seed,
+                                 void *stream);
+/* CIC deposition of a mixed-layout species into np (accumulated), with the
+ * integer weights of lepic_dev_push_deposit_mixed (exact charge). */
+int lepic_dev_deposit_mixed(const lepic_grid_t *g, const lepic_species_mixed_t *s, int ptype,
+                            const lepic_phys_t *P, double *np, int n_hint, void *stream);
 /* E4[i] = (float)Ei(1:3, i), 0 for the nodes i < nodes (FP32 field of the
  * mixed push; E4 16-byte aligned). */
 int lepic_dev_pack_e32(const double *Ei, float *E4, long long nodes, void *stream);

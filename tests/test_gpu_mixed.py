@@ -84,6 +84,29 @@ def test_layout_roundtrip():
         np.testing.assert_array_equal(cell_g, ix | (iy << 10) | (iz << 20))
 
 
+def test_mixed_loader_matches_f64_loader():
+    """The direct mixed loader draws the FP64 loader's particles (to FP32) and
+    deposits their charge exactly."""
+    import torch
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    st = config.build("mcc32")
+    a = Simulation(st, seed=9)
+    b = Simulation(st, seed=9, precision="mixed")
+    a.load_uniform()
+    b.load_uniform()
+    torch.cuda.synchronize()
+    h = np.asarray(st.h)
+    for p in range(st.ntype):
+        n = a.sp[p].n()
+        assert b.sp[p].n() == n
+        x = a.sp[p].p[:, :n].cpu().numpy()
+        y = b.particles_f64(p).cpu().numpy()
+        assert np.all(np.abs(y[0:3] - x[0:3]).T <= 1.2e-7 * h)
+        assert rel(y[3:6], x[3:6]) <= 1e-7
+        assert rel(b.np[p].cpu().numpy(), a.np[p].cpu().numpy()) <= 1e-6
+    _charge_ok(st, b)
+
+
 def test_sort_tile_order():
     """The mixed sort: tile-major key order, tile offsets, same particles."""
     import torch
