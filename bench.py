@@ -344,6 +344,67 @@ def run_poisson(workload, warm=10):
     return out
 
 
+def run_dropin(workload, steps=4, warm=1):
+    """The reference-facing path: Src/main.f90's timestep as calls to the
+    Fortran-signature entry points over host arrays in the reference layouts
+    (FP64), once with per-call copies (a Fortran build that only relinks) and
+    once with device-resident mirrors (lepic_gpu_set_residency).  Wall-clock
+    particle-steps/s with every host<->device copy inside the timed region;
+    the resident run creates its mirrors in the warm-up step and ends the
+    timed steps with lepic_gpu_sync_to_host, so the host arrays are current
+    at both ends.  Initial particles come from the GPU loader."""
+    import torch
+    from essaitemporaire_lepic_module_b200 import config, dropin
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    st = config.build(workload)
+    nmax = int(st.n_particles() * 1.25)
+    sim = Simulation(st, cap=nmax, precision="f64")
+    sim.load_uniform()
+    vxp0 = np.zeros((st.ntype, nmax, 6))
+    np_tot0 = np.zeros(st.ntype, dtype=np.int32)
+    for p in range(st.ntype):
+        v = sim.sp[p].to_vxp()
+        vxp0[p, :len(v)] = v
+        np_tot0[p] = len(v)
+    np0 = np.ascontiguousarray(sim.np.cpu().numpy())
+    del sim
+    torch.cuda.empty_cache()
+    out = {"workload": f"{workload} {list(st.n)} grid, {int(np_tot0.sum())} particles in host arrays "
+                       f"vxp(6, nmax, {st.ntype}), FP64, MCC every {st.wl.ns_coll} steps",
+           "timing": "wall clock over the drop-in calls, host<->device copies included"}
+    for mode in ("copy", "resident"):
+        vxp, np_tot = vxp0.copy(), np_tot0.copy()
+        fd = np.zeros((st.ntype, nmax), dtype=np.int8)
+        npg = np0.copy()
+        ml = dropin.MainLoop(st, vxp, np_tot, fd, npg, resident=(mode == "resident"))
+        try:
+            for _ in range(warm):
+                ml.step()
+            ml.sync()
+            torch.cuda.synchronize()
+            a = dropin.mirror_stats()
+            t0 = time.perf_counter()
+            nps = 0
+            for _ in range(steps):
+                nps += int(np_tot.sum())
+                ml.step()
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            ml.sync()
+            torch.cuda.synchronize()
+            t = time.perf_counter() - t0
+            b = dropin.mirror_stats()
+        finally:
+            ml.close()
+        out[mode] = {"value": nps / t, "unit": UNIT, "ms_per_step": 1e3 * t / steps, "steps": steps,
+                     "step_ms_without_final_sync": 1e3 * (t1 - t0) / steps,
+                     "final_sync_ms": 1e3 * (t - (t1 - t0)),
+                     "h2d_bytes_per_step": int((b[0] - a[0]) / steps),
+                     "d2h_bytes_per_step": int((b[1] - a[1]) / steps)}
+    out["resident_over_copy"] = out["resident"]["value"] / out["copy"]["value"]
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -412,6 +473,8 @@ def run_ours(args):
         line["poisson"] = run_poisson(args.poisson_workload)
     if args.adjoint:
         line["adjoint"] = run_adjoint(args.adjoint_workload, args.adjoint_k, args.adjoint_every)
+    if args.dropin:
+        line["dropin"] = run_dropin(args.dropin_workload, args.dropin_steps)
     if args.cpu_baseline and world == 1:
         try:
             line["cpu_baseline"] = cpu_baseline(args.workload, steps=args.cpu_steps, ppc=args.cpu_ppc)
@@ -448,6 +511,10 @@ def main():
     ap.add_argument("--adjoint-workload", default="penning")
     ap.add_argument("--adjoint-k", type=int, default=64)
     ap.add_argument("--adjoint-every", type=int, default=8)
+    ap.add_argument("--no-dropin", dest="dropin", action="store_false",
+                    help="skip the drop-in (Fortran-signature) loop, per-call copies vs resident")
+    ap.add_argument("--dropin-workload", default="mcc64")
+    ap.add_argument("--dropin-steps", type=int, default=10)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -117,6 +117,16 @@ def lib():
         "lepic_gpu_last_error": ([], _I),
         "lepic_gpu_strerror": ([_I], C.c_char_p),
         "lepic_build_info": ([], C.c_char_p),
+        "lepic_gpu_set_residency": ([_I], _I),
+        "lepic_gpu_residency": ([], _I),
+        "lepic_gpu_sync_to_host": ([], _I),
+        "lepic_gpu_update_host": ([vp, C.c_size_t], _I),
+        "lepic_gpu_update_device": ([vp, C.c_size_t], _I),
+        "lepic_gpu_release": ([vp, C.c_size_t], _I),
+        "lepic_gpu_release_all": ([], _I),
+        "lepic_gpu_mirror_zero": ([vp, C.c_size_t], _I),
+        "lepic_gpu_mirror_copy": ([vp, vp, C.c_size_t], _I),
+        "lepic_gpu_mirror_stats": ([C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), P_int], _I),
         "lepic_dev_info": ([P_int, C.c_char_p, _I], _I),
         "lepic_dev_calc_rho": ([C.POINTER(LepicGrid), vp, vp, _I, C.POINTER(LepicPhys), vp], _I),
         "lepic_dev_calc_efield": ([C.POINTER(LepicGrid), vp, vp, vp], _I),
@@ -204,6 +214,10 @@ def commons():
 def exported_symbols():
     """Names declared in include/lepic_gpu.h that the library must export."""
     return ["lepic_gpu_last_error", "lepic_gpu_strerror", "lepic_build_info", "lepic_dev_info",
+            "lepic_gpu_set_residency", "lepic_gpu_residency", "lepic_gpu_sync_to_host",
+            "lepic_gpu_update_host", "lepic_gpu_update_device", "lepic_gpu_release",
+            "lepic_gpu_release_all", "lepic_gpu_mirror_zero", "lepic_gpu_mirror_copy",
+            "lepic_gpu_mirror_stats",
             "lepic_dev_calc_rho", "lepic_dev_calc_efield", "lepic_dev_pdesolver",
             "lepic_dev_pdesolver_noalloc",
             "lepic_dev_part_mover", "lepic_dev_push_deposit", "lepic_dev_charge_deposition", "lepic_dev_part_sorting",

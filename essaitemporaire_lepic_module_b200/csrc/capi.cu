@@ -59,31 +59,46 @@ lepic_phys_t phys_from_common(int ntype) {
   return P;
 }
 
-// device staging buffer keyed by name, with a host->device upload
+// Temporary device copy of a host table the call builds itself.
 template <class T>
 T *upload(const char *name, const T *h, size_t n, cudaStream_t s) {
   T *d = (T *)scratch(name, sizeof(T) * (n ? n : 1));
-  if (d && n) cudaMemcpyAsync(d, h, sizeof(T) * n, cudaMemcpyHostToDevice, s);
+  if (d && n && mirror_h2d(d, h, sizeof(T) * n, s)) return nullptr;
   return d;
 }
 
-__global__ void k_aos_to_soa(const double *aos, double *soa, long long n, long long cap) {
-  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= 6 * n) return;
-  long long i = t / 6;
-  int c = (int)(t % 6);
-  soa[c * cap + i] = aos[t];
+// Device view of a Fortran host array for one drop-in call.  Without
+// residency: a named staging buffer, filled from the host unless the call
+// only writes it (WRITE), copied back by host_back.  With residency: the
+// array's device mirror, marked device-newer unless the call only reads it.
+enum Use { READ, WRITE, UPDATE };
+
+template <class T>
+T *dev_view(const char *name, const T *h, size_t n, Use u, cudaStream_t s, int *rc) {
+  *rc = LEPIC_OK;
+  if (residency_on()) {
+    T *d = (T *)mirror_array(h, sizeof(T) * n, u != READ, s, rc);
+    if (!d && !*rc) *rc = LEPIC_ERR_CUDA;
+    return d;
+  }
+  T *d = (T *)scratch(name, sizeof(T) * (n ? n : 1));
+  if (!d) {
+    *rc = LEPIC_ERR_CUDA;
+    return nullptr;
+  }
+  if (u != WRITE) *rc = mirror_h2d(d, h, sizeof(T) * n, s);
+  return *rc ? nullptr : d;
 }
 
-__global__ void k_soa_to_aos(const double *soa, double *aos, long long n, long long cap) {
-  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= 6 * n) return;
-  long long i = t / 6;
-  int c = (int)(t % 6);
-  aos[t] = soa[c * cap + i];
+// Results of a call back into the host array (a mirror keeps them).
+template <class T>
+int host_back(T *h, const T *d, size_t n, cudaStream_t s) {
+  if (residency_on()) return LEPIC_OK;
+  return mirror_d2h(h, d, sizeof(T) * n, s);
 }
 
-// Device-resident copy of one host species slice vxp(6, 1:np, ptype, 1).
+// Per-call staging of one host species slice vxp(6, 1:np, ptype, 1): SoA
+// copies under slot-numbered scratch names.
 struct StagedSpecies {
   lepic_species_f64_t s;
   double *aos = nullptr;
@@ -110,39 +125,62 @@ int stage_species(StagedSpecies &st, const double *vxp_h, int np, int nmax, int 
   st.n = np;
   if (!st.s.p || !st.s.p_alt || !st.s.count || !st.s.key || !st.aos || !st.s.flag_dead)
     return LEPIC_ERR_CUDA;
-  LEPIC_CUDA(cudaMemcpyAsync(st.s.count, &st.n, sizeof(int), cudaMemcpyHostToDevice, s));
-  if (np > 0) {
-    LEPIC_CUDA(cudaMemcpyAsync(st.aos, vxp_h, sizeof(double) * 6 * (size_t)np, cudaMemcpyHostToDevice, s));
-    k_aos_to_soa<<<grid_for(6LL * np, 256), 256, 0, s>>>(st.aos, st.s.p, np, cap);
-  }
-  if (flag_dead_h) {
-    LEPIC_CUDA(cudaMemcpyAsync(st.s.flag_dead, flag_dead_h, (size_t)nmax, cudaMemcpyHostToDevice, s));
-  } else {
-    LEPIC_CUDA(cudaMemsetAsync(st.s.flag_dead, 0, (size_t)nmax, s));
-  }
-  LEPIC_CUDA(cudaGetLastError());
+  int rc = mirror_h2d(st.s.count, &st.n, sizeof(int), s);
+  if (!rc && np > 0) rc = mirror_h2d(st.aos, vxp_h, sizeof(double) * 6 * (size_t)np, s);
+  if (!rc) rc = aos_to_soa(st.aos, st.s.p, 0, np, cap, s);
+  if (rc) return rc;
+  if (flag_dead_h) return mirror_h2d(st.s.flag_dead, flag_dead_h, (size_t)nmax, s);
+  LEPIC_CUDA(cudaMemsetAsync(st.s.flag_dead, 0, (size_t)nmax, s));
   return LEPIC_OK;
 }
 
 int unstage_species(StagedSpecies &st, double *vxp_h, int *np_out, signed char *flag_dead_h,
                     int nmax, cudaStream_t s) {
   int n = 0;
-  LEPIC_CUDA(cudaMemcpyAsync(&n, st.s.count, sizeof(int), cudaMemcpyDeviceToHost, s));
+  int rc = mirror_d2h(&n, st.s.count, sizeof(int), s);
+  if (rc) return rc;
   LEPIC_CUDA(cudaStreamSynchronize(s));
   if (n > nmax) n = nmax;
-  if (n > 0) {
-    k_soa_to_aos<<<grid_for(6LL * n, 256), 256, 0, s>>>(st.s.p, st.aos, n, st.s.cap);
-    LEPIC_CUDA(cudaGetLastError());
-    LEPIC_CUDA(cudaMemcpyAsync(vxp_h, st.aos, sizeof(double) * 6 * (size_t)n, cudaMemcpyDeviceToHost, s));
-  }
-  if (flag_dead_h)
-    LEPIC_CUDA(cudaMemcpyAsync(flag_dead_h, st.s.flag_dead, (size_t)nmax, cudaMemcpyDeviceToHost, s));
+  rc = soa_to_aos(st.s.p, st.aos, n, st.s.cap, s);
+  if (!rc && n > 0) rc = mirror_d2h(vxp_h, st.aos, sizeof(double) * 6 * (size_t)n, s);
+  if (!rc && flag_dead_h) rc = mirror_d2h(flag_dead_h, st.s.flag_dead, (size_t)nmax, s);
+  if (rc) return rc;
   LEPIC_CUDA(cudaStreamSynchronize(s));
   if (np_out) *np_out = n;
   return LEPIC_OK;
 }
 
-// Geometry staging for the drop-ins: bcnd, kq and the cell-wall mask.
+// One species slice on the device for a drop-in call: staged, or the
+// slice's mirror under residency.
+struct SpeciesView {
+  lepic_species_f64_t s{};
+  StagedSpecies st;
+  double *vxp_h = nullptr;
+  bool resident = false;
+};
+
+int acquire_species(SpeciesView &v, double *vxp_h, int np, int nmax, int slot, signed char *fd_h,
+                    cudaStream_t s) {
+  v.vxp_h = vxp_h;
+  v.resident = residency_on();
+  if (v.resident) return mirror_species(vxp_h, np, nmax, fd_h, s, &v.s);
+  int rc = stage_species(v.st, vxp_h, np, nmax, slot, fd_h, s);
+  v.s = v.st.s;
+  return rc;
+}
+
+// After the call: `wrote` = the call changed the particles (and flag_dead,
+// when fd_h names it); np_out receives the count.
+int release_species(SpeciesView &v, int *np_out, signed char *fd_h, int nmax, bool wrote,
+                    cudaStream_t s) {
+  if (v.resident) return mirror_species_done(v.vxp_h, v.s, wrote, wrote && fd_h, np_out, s);
+  v.st.s = v.s;
+  if (!wrote) return LEPIC_OK;
+  return unstage_species(v.st, v.vxp_h, np_out, fd_h, nmax, s);
+}
+
+// Geometry for the drop-ins: bcnd, kq and the cell-wall mask.  Under
+// residency the mask is kept until the bcnd mirror is reloaded.
 int stage_grid(lepic_grid_t &g, const int *n, const double *h, const int *bcnd_h, const double *kq_h,
                cudaStream_t s) {
   Dims d(n);
@@ -150,14 +188,37 @@ int stage_grid(lepic_grid_t &g, const int *n, const double *h, const int *bcnd_h
     g.n[a] = n[a];
     g.h[a] = h ? h[a] : 0.0;
   }
-  g.bcnd = upload("dropin_bcnd", bcnd_h, (size_t)d.cnt(), s);
-  if (!g.bcnd) return LEPIC_ERR_CUDA;
-  g.kq = kq_h ? upload("dropin_kq", kq_h, (size_t)d.cnt(), s) : nullptr;
-  unsigned char *cw = (unsigned char *)scratch("dropin_cw", (size_t)((d.N1 - 1) * (d.N2 - 1) * (d.N3 - 1)));
+  int rc = LEPIC_OK;
+  g.bcnd = dev_view("dropin_bcnd", bcnd_h, (size_t)d.cnt(), READ, s, &rc);
+  if (!g.bcnd) return rc;
+  g.kq = nullptr;
+  if (kq_h) {
+    g.kq = dev_view("dropin_kq", kq_h, (size_t)d.cnt(), READ, s, &rc);
+    if (!g.kq) return rc;
+  }
+  const size_t cells = (size_t)((d.N1 - 1) * (d.N2 - 1) * (d.N3 - 1));
+  if (residency_on()) {
+    static const int *cw_bcnd = nullptr;
+    static const unsigned char *cw_buf = nullptr;
+    static unsigned long long cw_gen = 0;
+    static size_t cw_cells = 0;
+    unsigned char *cw = (unsigned char *)scratch("mirror_cw", cells);
+    if (!cw) return LEPIC_ERR_CUDA;
+    unsigned long long gen = mirror_generation(bcnd_h);
+    g.cell_wall = cw;
+    if (cw == cw_buf && g.bcnd == cw_bcnd && gen == cw_gen && cells == cw_cells) return LEPIC_OK;
+    rc = launch_cell_wall(d, g.bcnd, cw, s);
+    if (rc) return rc;
+    cw_bcnd = g.bcnd;
+    cw_buf = cw;
+    cw_gen = gen;
+    cw_cells = cells;
+    return LEPIC_OK;
+  }
+  unsigned char *cw = (unsigned char *)scratch("dropin_cw", cells);
   if (!cw) return LEPIC_ERR_CUDA;
-  int rc = launch_cell_wall(d, g.bcnd, cw, s);
   g.cell_wall = cw;
-  return rc;
+  return launch_cell_wall(d, g.bcnd, cw, s);
 }
 
 }  // namespace
@@ -273,6 +334,10 @@ int lepic_dev_dens_red(const lepic_grid_t *g, const double *np, double *np_red, 
 }
 
 // ------------------------------------------------------------ drop-ins
+// Every drop-in runs on the legacy default stream and leaves its status in
+// the thread's error word.  Array arguments go through dev_view /
+// acquire_species, so the same bodies serve the per-call copy mode and the
+// residency mode.
 void calc_rho_(const int *n, double *np, double *rhs_dom, const int *bcnd, const int *ntype,
                const int *nproc, const int *nproc_mpi, const int *mpi_rank) {
   (void)mpi_rank;
@@ -281,14 +346,19 @@ void calc_rho_(const int *n, double *np, double *rhs_dom, const int *bcnd, const
   Dims d(n);
   lepic_phys_t P = phys_from_common(*ntype);
   size_t nn = (size_t)d.cnt() * (size_t)*ntype;
-  double *np_d = upload("dropin_np", np, nn, s);
-  int *bc_d = upload("dropin_bcnd", bcnd, (size_t)d.cnt(), s);
-  double *rhs_d = (double *)scratch("dropin_rhs", sizeof(double) * (size_t)d.rcnt());
-  if (!np_d || !bc_d || !rhs_d) return record(LEPIC_ERR_CUDA);
-  int rc = launch_calc_rho(d, np_d, rhs_d, bc_d, *ntype, P, s);
+  int rc = LEPIC_OK;
+  // periodic stitching writes np
+  double *np_d = dev_view("dropin_np", np, nn, P.flag_pbc ? UPDATE : READ, s, &rc);
+  if (!np_d) return record(rc);
+  const int *bc_d = dev_view("dropin_bcnd", bcnd, (size_t)d.cnt(), READ, s, &rc);
+  if (!bc_d) return record(rc);
+  double *rhs_d = dev_view("dropin_rhs", rhs_dom, (size_t)d.rcnt(), WRITE, s, &rc);
+  if (!rhs_d) return record(rc);
+  rc = launch_calc_rho(d, np_d, rhs_d, bc_d, *ntype, P, s);
   if (rc) return record(rc);
-  cudaMemcpyAsync(rhs_dom, rhs_d, sizeof(double) * (size_t)d.rcnt(), cudaMemcpyDeviceToHost, s);
-  if (P.flag_pbc) cudaMemcpyAsync(np, np_d, sizeof(double) * nn, cudaMemcpyDeviceToHost, s);
+  rc = host_back(rhs_dom, rhs_d, (size_t)d.rcnt(), s);
+  if (!rc && P.flag_pbc) rc = host_back(np, np_d, nn, s);
+  record(rc);
   record(check_err(s));
 }
 
@@ -298,14 +368,17 @@ void dens_red_(const int *n, const double *np, double *np_red, const int *bcnd, 
   cudaStream_t s = 0;
   Dims d(n);
   size_t nn = (size_t)d.cnt() * (size_t)*ntype;
-  double *np_d = upload("dropin_np", np, nn, s);
-  int *bc_d = upload("dropin_bcnd", bcnd, (size_t)d.cnt(), s);
-  double *red_d = (double *)scratch("dropin_npred", sizeof(double) * nn);
-  if (!np_d || !bc_d || !red_d) return record(LEPIC_ERR_CUDA);
+  int rc = LEPIC_OK;
+  const double *np_d = dev_view("dropin_np", np, nn, READ, s, &rc);
+  if (!np_d) return record(rc);
+  const int *bc_d = dev_view("dropin_bcnd", bcnd, (size_t)d.cnt(), READ, s, &rc);
+  if (!bc_d) return record(rc);
+  double *red_d = dev_view("dropin_npred", np_red, nn, WRITE, s, &rc);
+  if (!red_d) return record(rc);
   double mx[LEPIC_NPART] = {0};
-  int rc = launch_dens_red(d, np_d, red_d, bc_d, *ntype, mx, s);
+  rc = launch_dens_red(d, np_d, red_d, bc_d, *ntype, mx, s);
   if (rc) return record(rc);
-  cudaMemcpyAsync(np_red, red_d, sizeof(double) * nn, cudaMemcpyDeviceToHost, s);
+  record(host_back(np_red, red_d, nn, s));
   for (int p = 0; p < *ntype; ++p) part_info_dp_3_.np_mx[p] = mx[p];
   record(check_err(s));
 }
@@ -320,13 +393,16 @@ void pdesolver_(double *u, const double *b, const int *bcnd, const double *h, co
   Dims d(n);
   // u(0:n1+2,0:n2+2,-1:n3+2): skip the z = -1 ghost plane (MPI halo only)
   double *u0 = u + d.N1 * d.N2;
-  double *u_d = upload("dropin_u", u0, (size_t)d.cnt(), s);
-  double *b_d = upload("dropin_b", b, (size_t)d.rcnt(), s);
-  int *bc_d = upload("dropin_bcnd", bcnd, (size_t)d.cnt(), s);
-  if (!u_d || !b_d || !bc_d) return record(LEPIC_ERR_CUDA);
-  int rc = launch_pdesolver(d, h, u_d, b_d, bc_d, *ncycl, *eps, *omega, *ng, constants_.eps0, k, ktot,
-                            res, s);
-  cudaMemcpyAsync(u0, u_d, sizeof(double) * (size_t)d.cnt(), cudaMemcpyDeviceToHost, s);
+  int rc = LEPIC_OK;
+  double *u_d = dev_view("dropin_u", u0, (size_t)d.cnt(), UPDATE, s, &rc);
+  if (!u_d) return record(rc);
+  const double *b_d = dev_view("dropin_b", b, (size_t)d.rcnt(), READ, s, &rc);
+  if (!b_d) return record(rc);
+  const int *bc_d = dev_view("dropin_bcnd", bcnd, (size_t)d.cnt(), READ, s, &rc);
+  if (!bc_d) return record(rc);
+  rc = launch_pdesolver(d, h, u_d, b_d, bc_d, *ncycl, *eps, *omega, *ng, constants_.eps0, k, ktot,
+                        res, s);
+  record(host_back(u0, u_d, (size_t)d.cnt(), s));
   record(rc);
   record(check_err(s));
 }
@@ -334,13 +410,17 @@ void pdesolver_(double *u, const double *b, const int *bcnd, const double *h, co
 void calc_efield_(const int *n, const double *h, const double *phi, double *Ei, const int *bcnd) {
   cudaStream_t s = 0;
   Dims d(n);
-  double *phi_d = upload("dropin_u", phi, (size_t)d.cnt(), s);
-  double *E_d = upload("dropin_E", Ei, 3 * (size_t)d.cnt(), s);
-  int *bc_d = upload("dropin_bcnd", bcnd, (size_t)d.cnt(), s);
-  if (!phi_d || !E_d || !bc_d) return record(LEPIC_ERR_CUDA);
-  int rc = launch_efield(d, h, phi_d, E_d, bc_d, s);
+  int rc = LEPIC_OK;
+  const double *phi_d = dev_view("dropin_u", phi, (size_t)d.cnt(), READ, s, &rc);
+  if (!phi_d) return record(rc);
+  // nodes the routine does not write keep the caller's values
+  double *E_d = dev_view("dropin_E", Ei, 3 * (size_t)d.cnt(), UPDATE, s, &rc);
+  if (!E_d) return record(rc);
+  const int *bc_d = dev_view("dropin_bcnd", bcnd, (size_t)d.cnt(), READ, s, &rc);
+  if (!bc_d) return record(rc);
+  rc = launch_efield(d, h, phi_d, E_d, bc_d, s);
   if (rc) return record(rc);
-  cudaMemcpyAsync(Ei, E_d, sizeof(double) * 3 * (size_t)d.cnt(), cudaMemcpyDeviceToHost, s);
+  record(host_back(Ei, E_d, 3 * (size_t)d.cnt(), s));
   record(check_err(s));
 }
 
@@ -375,16 +455,16 @@ void part_mover_(const int *n, const double *h, const double *Ei, const double *
   int rc = stage_grid(g, n, h, bcnd, nullptr, s);
   if (rc) return record(rc);
   const int p = *ptype - 1;
-  const long long slice = 6LL * *nmax * p;
-  StagedSpecies st;
-  rc = stage_species(st, vxp + slice, np_tot[p], *nmax, 0, flag_dead + (long long)*nmax * p, s);
+  double *vxp_p = vxp + 6LL * *nmax * p;
+  signed char *fd_p = flag_dead + (long long)*nmax * p;
+  const double *E_d = dev_view("dropin_E", Ei, 3 * (size_t)d.cnt(), READ, s, &rc);
+  if (!E_d) return record(rc);
+  SpeciesView v;
+  rc = acquire_species(v, vxp_p, np_tot[p], *nmax, 0, fd_p, s);
   if (rc) return record(rc);
-  double *E_d = upload("dropin_E", Ei, 3 * (size_t)d.cnt(), s);
-  if (!E_d) return record(LEPIC_ERR_CUDA);
-  rc = launch_part_mover(g, E_d, st.s, *ptype, *ntype, *ngrid, P, p_mac, P_loss, s);
-  int rc2 = unstage_species(st, vxp + slice, &np_tot[p], flag_dead + (long long)*nmax * p, *nmax, s);
+  rc = launch_part_mover(g, E_d, v.s, *ptype, *ntype, *ngrid, P, p_mac, P_loss, s);
   record(rc);
-  record(rc2);
+  record(release_species(v, &np_tot[p], fd_p, *nmax, true, s));
 }
 
 void charge_deposition_(const int *n, const double *h, const double *vxp, const int *nmax,
@@ -405,17 +485,22 @@ void charge_deposition_(const int *n, const double *h, const double *vxp, const 
   }
   g.bcnd = nullptr;
   g.cell_wall = nullptr;
-  g.kq = upload("dropin_kq", kq, (size_t)d.cnt(), s);
+  int rc = LEPIC_OK;
+  g.kq = dev_view("dropin_kq", kq, (size_t)d.cnt(), READ, s, &rc);
+  if (!g.kq) return record(rc);
   const int p = *ptype - 1;
   double *np_slice = np + (long long)d.cnt() * p;
-  double *np_d = upload("dropin_npdep", np_slice, (size_t)d.cnt(), s);
-  if (!g.kq || !np_d) return record(LEPIC_ERR_CUDA);
-  StagedSpecies st;
-  int rc = stage_species(st, vxp + 6LL * *nmax * p, np_tot[p], *nmax, 0, nullptr, s);
+  double *np_d = dev_view("dropin_npdep", np_slice, (size_t)d.cnt(), UPDATE, s, &rc);
+  if (!np_d) return record(rc);
+  SpeciesView v;
+  // the routine reads the particles only
+  rc = acquire_species(v, const_cast<double *>(vxp) + 6LL * *nmax * p, np_tot[p], *nmax, 0, nullptr, s);
   if (rc) return record(rc);
-  rc = launch_deposit(g, st.s, *ptype, P, np_d, s);
-  if (rc) return record(rc);
-  cudaMemcpyAsync(np_slice, np_d, sizeof(double) * (size_t)d.cnt(), cudaMemcpyDeviceToHost, s);
+  rc = launch_deposit(g, v.s, *ptype, P, np_d, s);
+  record(rc);
+  record(release_species(v, nullptr, nullptr, *nmax, false, s));
+  if (rc) return;
+  record(host_back(np_slice, np_d, (size_t)d.cnt(), s));
   record(check_err(s));
 }
 
@@ -423,6 +508,7 @@ void part_sorting_(double *vxp, double *sorting, const int *nmax, const int *nty
                    const double *h, int *Plist_thd, const int *pl_max, const int *nproc,
                    const int *np_tot, const int *ptype) {
   (void)sorting;
+  (void)ntype;
   if (*nproc != 1) return record(LEPIC_ERR_UNSUPPORTED);
   cudaStream_t s = 0;
   lepic_grid_t g;
@@ -434,19 +520,20 @@ void part_sorting_(double *vxp, double *sorting, const int *nmax, const int *nty
   g.kq = nullptr;
   g.cell_wall = nullptr;
   const int p = *ptype - 1;
-  StagedSpecies st;
-  int rc = stage_species(st, vxp + 6LL * *nmax * p, np_tot[p], *nmax, 0, nullptr, s);
+  const size_t npl = (size_t)(*pl_max + 1);
+  int *pl_h = Plist_thd + (long long)npl * p;
+  int rc = LEPIC_OK;
+  int *pl_d = dev_view("dropin_plist", pl_h, npl, WRITE, s, &rc);
+  if (!pl_d) return record(rc);
+  SpeciesView v;
+  rc = acquire_species(v, vxp + 6LL * *nmax * p, np_tot[p], *nmax, 0, nullptr, s);
   if (rc) return record(rc);
-  int *pl_d = (int *)scratch("dropin_plist", sizeof(int) * (size_t)(*pl_max + 1));
-  if (!pl_d) return record(LEPIC_ERR_CUDA);
-  rc = launch_sort(g, st.s, pl_d, *pl_max, s);
-  if (rc) return record(rc);
+  rc = launch_sort(g, v.s, pl_d, *pl_max, s);
+  record(rc);
   int np_out = 0;
-  rc = unstage_species(st, vxp + 6LL * *nmax * p, &np_out, nullptr, *nmax, s);
-  if (rc) return record(rc);
-  (void)ntype;
-  cudaMemcpy(Plist_thd + (long long)(*pl_max + 1) * p, pl_d, sizeof(int) * (size_t)(*pl_max + 1),
-             cudaMemcpyDeviceToHost);
+  record(release_species(v, &np_out, nullptr, *nmax, true, s));
+  if (rc) return;
+  record(host_back(pl_h, pl_d, npl, s));
   record(check_err(s));
 }
 
@@ -490,9 +577,13 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
   T.ncol = ncol;
   T.npt = part_info_int_.sig_npt_mx;
   T.npt_mx = *npt_mx;
-  T.sig_Er = upload("dropin_sigEr", sig_Er, (size_t)*npt_mx, s);
-  T.sig = upload("dropin_sig", sig, (size_t)*npt_mx * *ncol_mx, s);
-  T.sig_Eth = upload("dropin_sigEth", sig_Eex, (size_t)*ncol_mx, s);  // sig_Eex(:,ind_Eth)
+  int rc = LEPIC_OK;
+  T.sig_Er = dev_view("dropin_sigEr", sig_Er, (size_t)*npt_mx, READ, s, &rc);
+  if (!T.sig_Er) return record(rc);
+  T.sig = dev_view("dropin_sig", sig, (size_t)*npt_mx * *ncol_mx, READ, s, &rc);
+  if (!T.sig) return record(rc);
+  T.sig_Eth = dev_view("dropin_sigEth", sig_Eex, (size_t)*ncol_mx, READ, s, &rc);  // sig_Eex(:,ind_Eth)
+  if (!T.sig_Eth) return record(rc);
   std::vector<int> ci((size_t)ncol * 10);
   for (int c = 0; c < ncol; ++c)
     for (int q = 0; q < 10; ++q) ci[c + (size_t)ncol * q] = col_info[c + (size_t)*ncol_mx * q];
@@ -507,15 +598,6 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
   T.sig_list = sl.data();
   T.sigv_mx = sv.data();
   T.p_ncol = part_info_int_.p_ncol;
-  if (!T.sig_Er || !T.sig || !T.sig_Eth) return record(LEPIC_ERR_CUDA);
-  StagedSpecies st[3];
-  lepic_species_f64_t sp[3];
-  for (int p = 0; p < nt; ++p) {
-    int rc = stage_species(st[p], vxp + 6LL * *nmax * p, np_tot[p], *nmax, p,
-                           flag_dead + (long long)*nmax * p, s);
-    if (rc) return record(rc);
-    sp[p] = st[p].s;
-  }
   // region counters (Src/collisions.f90:153-157, 1005-1013)
   RegionCount rgc;
   memset(&rgc, 0, sizeof(rgc));
@@ -529,6 +611,11 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
   rgc.iyr = part_info_int_.iyr_rg;
   rgc.izl = part_info_int_.izl_rg;
   rgc.izr = part_info_int_.izr_rg;
+  if (rgc.n_rg > 0) {
+    // the region populations read np_red on the host
+    rc = mirror_to_host(np_red, sizeof(double) * (size_t)d.cnt() * nt, s);
+    if (rc) return record(rc);
+  }
   for (int p = 0; p < nt; ++p) {
     double kk = h[0] * h[1] * h[2] / part_info_dp_2_.Nm[p];
     for (int q = 0; q < rgc.n_rg && q < LEPIC_NM_RG; ++q) {
@@ -546,19 +633,27 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
     for (int c = 0; c < *ncol_mx; ++c)
       cc_h[c + (size_t)*ncol_mx * q] = cnt_col[c + (size_t)*ncol_mx * (size_t)(*nproc) * q];
   rgc.cnt_col_dev = upload("dropin_cntcol", cc_h.data(), ncc, s);
+  if (!rgc.cnt_col_dev) return record(LEPIC_ERR_CUDA);
+  SpeciesView v[3];
+  lepic_species_f64_t sp[3];
+  for (int p = 0; p < nt; ++p) {
+    rc = acquire_species(v[p], vxp + 6LL * *nmax * p, np_tot[p], *nmax, p,
+                         flag_dead + (long long)*nmax * p, s);
+    if (rc) return record(rc);
+    sp[p] = v[p].s;
+  }
   double nu_max[LEPIC_NPART] = {0};
   long long counts[64] = {0};
   unsigned long long seed = (unsigned long long)(unsigned)iseed[0];
-  int rc = launch_collisions(g, sp, nt, T, P, seed, (unsigned long long)*it, nu_max, counts, s,
-                             rgc.n_rg > 0 ? &rgc : nullptr);
+  rc = launch_collisions(g, sp, nt, T, P, seed, (unsigned long long)*it, nu_max, counts, s,
+                         rgc.n_rg > 0 ? &rgc : nullptr);
   for (int p = 0; p < nt; ++p) {
-    st[p].s = sp[p];
-    int rc2 = unstage_species(st[p], vxp + 6LL * *nmax * p, &np_tot[p],
-                              flag_dead + (long long)*nmax * p, *nmax, s);
-    record(rc2);
+    v[p].s = sp[p];
+    record(release_species(v[p], &np_tot[p], flag_dead + (long long)*nmax * p, *nmax, true, s));
   }
   if (rgc.n_rg > 0) {
-    cudaMemcpy(cc_h.data(), rgc.cnt_col_dev, sizeof(double) * ncc, cudaMemcpyDeviceToHost);
+    record(mirror_d2h(cc_h.data(), rgc.cnt_col_dev, sizeof(double) * ncc, s));
+    if (cudaStreamSynchronize(s) != cudaSuccess) record(LEPIC_ERR_CUDA);
     for (int q = 0; q < rgc.n_rg; ++q)
       for (int c = 0; c < *ncol_mx; ++c)
         cnt_col[c + (size_t)*ncol_mx * (size_t)(*nproc) * q] = cc_h[c + (size_t)*ncol_mx * q];

@@ -135,6 +135,24 @@ int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const do
                            double eps, double omega, int ng, double eps0, int max_refine, int nu_pre,
                            int nu_post, int coarse_sweeps, int *iters, double *res_out, cudaStream_t s);
 
+// residency.cu: device mirrors of the drop-ins' host arrays
+bool residency_on();
+// device pointer for host range [h, h + bytes) inside its mirror (created and
+// filled from the host on first use); `write` marks the mirror device-newer
+void *mirror_array(const void *h, size_t bytes, bool write, cudaStream_t s, int *rc);
+unsigned long long mirror_generation(const void *h);  // changes on every host reload
+int mirror_to_host(const void *h, size_t bytes, cudaStream_t s);
+// particle slice vxp(6, 1:nmax) with np_h particles on the host side
+int mirror_species(double *vxp_h, int np_h, int nmax, signed char *fd_h, cudaStream_t s,
+                   lepic_species_f64_t *out);
+int mirror_species_done(double *vxp_h, const lepic_species_f64_t &sp, bool wrote, bool fd_wrote,
+                        int *np_out, cudaStream_t s);
+// counted host<->device copies of the drop-in layer
+int mirror_h2d(void *d, const void *h, size_t bytes, cudaStream_t s);
+int mirror_d2h(void *h, const void *d, size_t bytes, cudaStream_t s);
+int aos_to_soa(const double *aos, double *soa, long long first, long long n, long long cap, cudaStream_t s);
+int soa_to_aos(const double *soa, double *aos, long long n, long long cap, cudaStream_t s);
+
 }  // namespace lepic
 
 #define LEPIC_CUDA(call)                                                 \

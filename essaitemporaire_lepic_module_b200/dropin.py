@@ -250,3 +250,168 @@ def collisions(st, it, vxp, np_tot, flag_dead, iseed, np_red=None, ncol_mx=65, n
     check(lib().lepic_gpu_last_error(), "collisions")
     d3 = cm["part_info_dp_3"]
     return np.array([d3.nu_max[i] for i in range(st.ntype)])
+
+
+# ---------------------------------------------------------------- residency
+def set_residency(on):
+    """lepic_gpu_set_residency: device mirrors of the drop-ins' host arrays
+    kept between calls (on) or per-call copies (off; syncs and frees)."""
+    check(lib().lepic_gpu_set_residency(1 if on else 0), "set_residency")
+
+
+def sync_to_host():
+    check(lib().lepic_gpu_sync_to_host(), "sync_to_host")
+
+
+def mirror_stats():
+    """(bytes host->device, bytes device->host, live mirrors) of the drop-in
+    layer since the library loaded."""
+    h2d, d2h, m = C.c_longlong(0), C.c_longlong(0), C.c_int(0)
+    check(lib().lepic_gpu_mirror_stats(C.byref(h2d), C.byref(d2h), C.byref(m)), "mirror_stats")
+    return h2d.value, d2h.value, m.value
+
+
+def _vp(a, offset_bytes=0):
+    return C.c_void_p(a.ctypes.data + offset_bytes)
+
+
+class MainLoop:
+    """The timestep of Src/main.f90:853-1280 through the drop-ins only, over
+    persistent host arrays in the reference layouts -- the calls a Fortran
+    build linked against liblepic_gpu.so makes:
+
+        calc_rho -> pdesolver -> phi = phi_dom (the one-rank MPI_ALLGATHERV,
+        main.f90:977) -> calc_Efield -> part_sorting (MOD(it,nsort) = 1)
+        -> dens_red + collisions (it > 1, MOD(it,ns_coll) = 1)
+        -> part_mover (charged species) -> np(:,:,:,p) = 0 + charge_deposition
+
+    The arrays passed in (vxp (ntype, nmax, 6), np_tot int32 (ntype),
+    flag_dead int8 (ntype, nmax), np_grids (ntype, n3+3, n2+3, n1+3)) are
+    used in place.  resident=True turns the library's residency on: the
+    arrays stay on the GPU between calls, the loop's two host statements on
+    them run as lepic_gpu_mirror_copy / lepic_gpu_mirror_zero, and sync()
+    brings the host arrays up to date."""
+
+    def __init__(self, st, vxp, np_tot, flag_dead, np_grids, resident=False, iseed=4242,
+                 nsort=None, ns_coll=None, collide=True, ncol_mx=65, npt_mx=1300):
+        assert vxp.flags["C_CONTIGUOUS"] and vxp.dtype == np.float64
+        assert np_tot.dtype == np.int32 and flag_dead.dtype == np.int8
+        assert np_grids.flags["C_CONTIGUOUS"] and np_grids.dtype == np.float64
+        self.st = st
+        self.vxp, self.np_tot, self.flag_dead, self.np = vxp, np_tot, flag_dead, np_grids
+        self.resident = bool(resident)
+        self.nsort = st.wl.nsort if nsort is None else nsort
+        self.ns_coll = st.wl.ns_coll if ns_coll is None else ns_coll
+        self.it = 0
+        n1, n2, n3 = st.n
+        N1, N2, N3 = n1 + 3, n2 + 3, n3 + 3
+        self.n = _lib.np_i(st.n).copy()
+        self.h = np.ascontiguousarray(st.h, dtype=np.float64).copy()
+        self.bcnd = _lib.np_i(st.geom.bcnd).copy()
+        self.kq = np.ascontiguousarray(st.kq, dtype=np.float64).copy()
+        self.rhs = np.zeros((n3 + 2, n2 + 2, n1 + 2))
+        self.phi_dom = np.zeros((n3 + 4, N2, N1))          # z from -1
+        self.phi_dom[1:] = st.geom.phi
+        self.phi = np.ascontiguousarray(st.geom.phi, dtype=np.float64).copy()
+        self.Ei = np.zeros((N3, N2, N1, 3))
+        self.np_red = np.zeros_like(np_grids)
+        self.pl_max = pl_max_of(st.n)
+        self.Plist = np.zeros((st.ntype, self.pl_max + 1), dtype=np.int32)
+        ngrid = st.geom.ngrid
+        self.ngrid = ngrid
+        self.p_mac = np.zeros((ngrid + 1, 2, st.ntype))
+        self.P_loss = np.zeros((st.ntype, 4))
+        self.Bi = _bi_uniform(st)
+        self.nB = np.array([1, 1, 1], dtype=np.int32)
+        self.iseed = np.array([iseed], dtype=np.int32)
+        self.zi = np.zeros(16, dtype=np.int32)
+        self.zd = np.zeros(16)
+        self.collide = bool(collide) and st.tables is not None
+        self.ncol = self.npt = 0
+        if self.collide:
+            T = st.tables
+            self.ncol, self.npt = T.sig.shape[0], T.sig_Er.shape[0]
+            self.p_ncol = T.p_ncol
+            self.ncol_mx, self.npt_mx = ncol_mx, npt_mx
+            self.sig = np.zeros((ncol_mx, npt_mx))
+            self.sig[:self.ncol, :self.npt] = T.sig
+            self.sig_Er = np.zeros(npt_mx)
+            self.sig_Er[:self.npt] = T.sig_Er
+            self.sig_list = np.zeros((ncol_mx, 10), dtype=np.int32)
+            self.sig_list[:self.ncol, :] = T.sig_list.T
+            self.sig_Eex = np.zeros((2, ncol_mx))
+            self.sig_Eex[0, :self.ncol] = T.Eth
+            self.sigv = np.zeros((ncol_mx, 10))
+            self.sigv[:self.ncol, :] = T.sigv_mx.T
+            self.col_info = np.zeros((10, ncol_mx), dtype=np.int32)
+            self.col_info[:, :self.ncol] = T.col_info.T
+            self.cnt_col = np.zeros((1, 1, ncol_mx))
+        set_residency(self.resident)
+
+    def _commons(self):
+        if self.collide:
+            set_commons(self.st, ncol=self.ncol, npt=self.npt, p_ncol=self.p_ncol)
+        else:
+            set_commons(self.st)
+
+    def step(self):
+        st, L = self.st, lib()
+        self.it += 1
+        it = self.it
+        self._commons()
+        nt = st.ntype
+        nmax = self.vxp.shape[1]
+        wl = st.wl
+        L.calc_rho_(_pi(self.n), _pd(self.np), _pd(self.rhs), _pi(self.bcnd), _i(nt), _i(1), _i(1), _i(0))
+        check(L.lepic_gpu_last_error(), "calc_rho")
+        k, ktot, res = C.c_int(0), C.c_double(0), C.c_double(0)
+        L.pdesolver_(_pd(self.phi_dom), _pd(self.rhs), _pi(self.bcnd), _pd(self.h), _pi(self.n),
+                     _i(wl.ncycl), _d(wl.eps), _d(wl.omega), C.byref(k), C.byref(ktot), C.byref(res),
+                     _i(st.ng), _i(0), _i(1))
+        check(L.lepic_gpu_last_error(), "pdesolver")
+        plane = self.phi_dom.shape[1] * self.phi_dom.shape[2] * 8
+        check(L.lepic_gpu_mirror_copy(_vp(self.phi), _vp(self.phi_dom, plane), self.phi.nbytes), "phi gather")
+        L.calc_efield_(_pi(self.n), _pd(self.h), _pd(self.phi), _pd(self.Ei), _pi(self.bcnd))
+        check(L.lepic_gpu_last_error(), "calc_efield")
+        if self.nsort and it % self.nsort == 1 % self.nsort:
+            for p in range(1, nt + 1):
+                if self.np_tot[p - 1] > 0:
+                    L.part_sorting_(_pd(self.vxp), _pd(self.zd), _i(nmax), _i(nt), _pi(self.n), _pd(self.h),
+                                    _pi(self.Plist), _i(self.pl_max), _i(1), _pi(self.np_tot), _i(p))
+                    check(L.lepic_gpu_last_error(), "part_sorting")
+        if self.collide and it > 1 and it % self.ns_coll == 1 % self.ns_coll:
+            L.dens_red_(_pi(self.n), _pd(self.np), _pd(self.np_red), _pi(self.bcnd), _i(nt), _i(1), _i(1))
+            check(L.lepic_gpu_last_error(), "dens_red")
+            L.collisions_(_i(it), _pd(self.vxp), _pi(self.n), _pd(self.h), _i(nt), _i(nmax), _pd(self.sig),
+                          _pd(self.sig_Er), _pi(self.sig_list), _pd(self.sig_Eex), _i(self.ncol_mx),
+                          _i(self.npt_mx), _pd(self.cnt_col), _pd(self.zd), _pi(self.zi), _pi(self.zi),
+                          _pi(self.Plist), _i(self.pl_max), _pd(self.sigv), _pi(self.col_info),
+                          _pd(self.np_red), self.flag_dead.ctypes.data_as(_lib.P_i8), _pi(self.zi), _i(1),
+                          _pi(self.np_tot), _pi(self.iseed), _i(1), _i(0), _pd(self.zd), _pd(self.zd),
+                          _pd(self.zd), _i(0))
+            check(L.lepic_gpu_last_error(), "collisions")
+        for p in range(1, nt + 1):
+            if st.charge[p - 1] != 0.0:
+                L.part_mover_(_pi(self.n), _pd(self.h), _pd(self.Ei), _pd(self.Bi), _pd(self.p_mac),
+                              _pd(self.P_loss), _pd(self.vxp), _pi(self.bcnd), _i(nmax), _i(nt),
+                              _i(self.ngrid), self.flag_dead.ctypes.data_as(_lib.P_i8), _i(1),
+                              _pi(self.np_tot), _i(1), _i(p), _pi(self.zi), _pi(self.zi), _pd(self.zd),
+                              _pd(self.zd), _pd(self.zd), _pd(self.zd), _pi(self.zi), _pi(self.zi),
+                              _pi(self.nB), _pd(self.h))
+                check(L.lepic_gpu_last_error(), "part_mover")
+        for p in range(1, nt + 1):
+            check(L.lepic_gpu_mirror_zero(_vp(self.np[p - 1]), self.np[p - 1].nbytes), "np = 0")
+            if self.np_tot[p - 1] > 0:
+                L.charge_deposition_(_pi(self.n), _pd(self.h), _pd(self.vxp), _i(nmax), _i(nt), _pd(self.kq),
+                                     _pd(self.np), _i(1), _pi(self.np_tot), _pd(self.zd), _pi(self.zi), _i(1),
+                                     _i(p))
+                check(L.lepic_gpu_last_error(), "charge_deposition")
+        return k.value, res.value
+
+    def sync(self):
+        """Host arrays up to date (no-op without residency)."""
+        sync_to_host()
+
+    def close(self):
+        """Sync, free the mirrors and turn residency off."""
+        set_residency(False)

@@ -10,7 +10,9 @@
  *    (the routines are external subroutines with implicit interfaces).
  *    Arrays are the Fortran host arrays (column-major, reference index
  *    bases); each call copies its inputs to the GPU, runs the kernels and
- *    copies its outputs back.  Physics constants are read from the Fortran
+ *    copies its outputs back, or, with residency on (lepic_gpu_set_residency),
+ *    works on device mirrors of the arrays that persist between calls.
+ *    Physics constants are read from the Fortran
  *    COMMON blocks declared below, exactly as the Fortran routines read them.
  *    Contract: OMP_NUM_THREADS=1 (nproc = 1) and one MPI rank.
  *
@@ -24,6 +26,8 @@
  */
 #ifndef LEPIC_GPU_H
 #define LEPIC_GPU_H
+
+#include <stddef.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -158,6 +162,55 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
 int lepic_gpu_last_error(void);
 /* Human-readable text for a status code. */
 const char *lepic_gpu_strerror(int code);
+
+/* ------------------------------------------------------------------------ */
+/* Residency of the drop-ins' arrays.  No counterpart in the reference (its  */
+/* arrays live in host memory only).  Off by default: each drop-in copies    */
+/* its array arguments to the GPU and its results back, so a Fortran build   */
+/* links the library with no source change.  On: every host array a drop-in */
+/* touches keeps a device mirror keyed by its host address range, filled    */
+/* from the host on first use and kept between calls; results stay on the   */
+/* device until the caller asks for them.  The Fortran loop then adds:       */
+/*   call lepic_gpu_set_residency(1)          once, before the time loop    */
+/*   lepic_gpu_mirror_zero(np slice)          for np(:,:,:,ptype,iproc)=0,  */
+/*                                            Src/main.f90:1273             */
+/*   lepic_gpu_mirror_copy(phi, phi_dom(0,0,0)) for the one-rank             */
+/*                                            MPI_ALLGATHERV, main.f90:977  */
+/*   lepic_gpu_sync_to_host()                 before host code reads the    */
+/*                                            arrays (write_data, backups,  */
+/*                                            diagnostics, main.f90:1294+)  */
+/*   lepic_gpu_update_device(a, bytes)        after host code writes an     */
+/*                                            array a drop-in reads         */
+/* np_tot(ptype, 1) is updated on the host by every call.  Particles that   */
+/* host code appends behind np_tot (part_injection, part_flux_injection)    */
+/* are uploaded by the next call that sees the larger np_tot.  A host array */
+/* with a mirror must not be freed before lepic_gpu_release covers it.      */
+/* One device per process; the registry is guarded by a lock.               */
+/* ------------------------------------------------------------------------ */
+
+/* on = 1 turns residency on; on = 0 syncs every mirror to the host and frees
+ * them. */
+int lepic_gpu_set_residency(int on);
+int lepic_gpu_residency(void);
+/* Copy every device-newer mirror (arrays, particle slices with their
+ * flag_dead) back to its host array. */
+int lepic_gpu_sync_to_host(void);
+/* The same for the mirrors overlapping host range [h, h + bytes). */
+int lepic_gpu_update_host(const void *h, size_t bytes);
+/* Host code wrote [h, h + bytes): reload that range into its mirrors (a
+ * particle slice mirror is dropped and rebuilt from the host by its next
+ * call). */
+int lepic_gpu_update_device(const void *h, size_t bytes);
+/* Sync and free the mirrors overlapping [h, h + bytes) / all mirrors. */
+int lepic_gpu_release(const void *h, size_t bytes);
+int lepic_gpu_release_all(void);
+/* Device counterparts of host statements on mirrored arrays (host memset /
+ * memcpy when residency is off).  The copy's ranges must not overlap. */
+int lepic_gpu_mirror_zero(void *h, size_t bytes);
+int lepic_gpu_mirror_copy(void *dst, const void *src, size_t bytes);
+/* Bytes the drop-in layer moved host->device and device->host since the
+ * library loaded, and the number of live mirrors. */
+int lepic_gpu_mirror_stats(long long *h2d_bytes, long long *d2h_bytes, int *mirrors);
 
 /* ------------------------------------------------------------------------ */
 /* Device API (layer 2): device pointers, stream as void*.  No counterpart   */

@@ -113,3 +113,26 @@ def test_chemistry_roundtrip(tmp_path):
     mu = 9.10938188e-31 * 39.95 * 1.66053886e-27 / (9.10938188e-31 + 39.95 * 1.66053886e-27)
     vmax = math.sqrt(2 * T.sig_Er[-1] * QE / mu)
     assert abs(T.sigv_mx[0, 0] - 1e-19 * vmax) <= 1e-12 * 1e-19 * vmax
+
+
+def test_residency_switch_and_host_statements_without_mirrors():
+    """With residency off, lepic_gpu_mirror_zero / _copy are the host
+    statements they stand for (np(...) = 0, the one-rank phi gather); the
+    switch and the registry calls make no CUDA call while no mirror exists."""
+    L = _lib.lib()
+    assert L.lepic_gpu_residency() == 0
+    a = np.arange(64, dtype=np.float64)
+    b = np.zeros(64)
+    vp = lambda x, off=0: C.c_void_p(x.ctypes.data + off)
+    assert L.lepic_gpu_mirror_copy(vp(b), vp(a), a.nbytes) == 0
+    assert np.array_equal(a, b)
+    assert L.lepic_gpu_mirror_zero(vp(b, 8 * 16), 8 * 16) == 0
+    assert np.all(b[16:32] == 0) and np.array_equal(b[:16], a[:16]) and np.array_equal(b[32:], a[32:])
+    # overlapping copy ranges are refused
+    assert L.lepic_gpu_mirror_copy(vp(a, 8), vp(a), 16 * 8) == 21
+    assert L.lepic_gpu_set_residency(1) == 0 and L.lepic_gpu_residency() == 1
+    assert L.lepic_gpu_sync_to_host() == 0
+    h2d, d2h, m = C.c_longlong(0), C.c_longlong(0), C.c_int(-1)
+    assert L.lepic_gpu_mirror_stats(C.byref(h2d), C.byref(d2h), C.byref(m)) == 0
+    assert m.value == 0
+    assert L.lepic_gpu_set_residency(0) == 0 and L.lepic_gpu_residency() == 0
