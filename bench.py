@@ -344,6 +344,43 @@ def run_poisson(workload, warm=10):
     return out
 
 
+def run_adjoint(workload, K, every):
+    """Adjoint/forward cost of the differentiable window: the gradient of the
+    final mean electron energy with respect to the electrode potentials, B_z
+    and the initial velocities (FP64 discrete adjoint, checkpoints every
+    `every` steps, recomputed)."""
+    import torch
+    from essaitemporaire_lepic_module_b200 import config
+    from essaitemporaire_lepic_module_b200.adjoint import Window, window_objective
+    st = config.build(workload)
+    win = Window(st, K=K, every=every)
+    win.load_uniform(seed=20240611)
+    V0 = [float(st.wl.V[lab]) if lab < len(st.wl.V) else 0.0 for lab in range(1, win.nlabel + 1)]
+    V = torch.tensor(V0, dtype=torch.float64, requires_grad=True)
+    Bz = torch.tensor(float(st.Bconst[2]), dtype=torch.float64, requires_grad=True)
+    v0 = win.x0[3:6].clone().requires_grad_(True)
+    from essaitemporaire_lepic_module_b200 import _lib
+    win.forward(V0, float(Bz))  # warm-up (allocations)
+    J = window_objective(win, V, Bz, v0)
+    _lib.timing(enable=True)
+    _lib.timing(reset=True)
+    J.backward()
+    timers = _lib.timing()
+    _lib.timing(enable=False)
+    t = dict(win.timing)
+    out = {"workload": f"{workload} {list(st.n)} cells, {win.n} particles of species 1, K={K}, "
+                       f"checkpoint every {every}, FP64",
+           "observable": "mean kinetic energy (eV) after K steps",
+           "J": float(J), "dJ_dV_by_label": [float(x) for x in V.grad], "dJ_dBz": float(Bz.grad),
+           "dJ_dv0_norm": float(v0.grad.norm()),
+           "forward_ms": t["forward_ms"], "backward_ms": t["backward_ms"],
+           "backward_over_forward": t["backward_ms"] / t["forward_ms"],
+           "backward_kernel_ms": {k: round(v[0], 3) for k, v in sorted(timers.items())}}
+    del win, v0
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_dropin(workload, steps=4, warm=1):
     """The reference-facing path: Src/main.f90's timestep as calls to the
     Fortran-signature entry points over host arrays in the reference layouts

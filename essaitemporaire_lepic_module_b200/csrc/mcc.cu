@@ -8,10 +8,11 @@
 // of collisions of each process, nu_r * ns_coll * dt per particle, is the
 // same, and no two threads ever touch the same particle.
 //
-// Two passes: k_mcc_select streams the particle indices through the Philox
-// test (no particle data is read) and appends the candidates (a fraction
-// Pmax) to a list; k_mcc_collide then runs the collision physics densely on
-// the candidates only.  The physics follows Src/collisions.f90:437-998 step
+// Two passes: the select pass appends the candidates (a fraction Pmax of
+// the particle indices; no particle data is read) to a list -- for small
+// Pmax by geometric skipping (k_mcc_select_skip: one draw per candidate),
+// else one Philox test per particle (k_mcc_select) -- and k_mcc_collide then
+// runs the collision physics densely on the candidates only.  The physics follows Src/collisions.f90:437-998 step
 // for step: Maxwellian neutral target (load_gauss form), relative energy in
 // the centre-of-mass frame, linear interpolation of sigma on the merged
 // energy grid, elastic / excitation scattering, ionization with
@@ -187,6 +188,59 @@ __global__ void __launch_bounds__(MB) k_mcc_select(MCCConst c, const int *__rest
     if (lane == leader) base = atomicAdd(ncand, __popc(m));
     base = __shfl_sync(full, base, leader);
     if (hit) cand[base + __popc(m & lanemask_lt_m())] = (int)i;
+  }
+}
+
+// pass 1 for small Pmax: the same Bernoulli(Pmax) sample of the particle
+// indices drawn by geometric skipping.  Within each segment of SKIP_SEG
+// particles the gaps between successive candidates are independent
+// geometric variables, floor(ln U / ln(1 - Pmax)), so one uniform per
+// candidate replaces one per particle.  The draws use Philox counters
+// (segment, 16 + k) that the per-particle streams (particle, 0..2) of the
+// collision pass never use.
+constexpr int SKIP_SEG = 2048;
+constexpr double SKIP_PMAX = 0.25;  // above it: one draw per particle
+
+__global__ void __launch_bounds__(MB) k_mcc_select_skip(MCCConst c, const int *__restrict__ count,
+                                                        double inv_log1m, int *__restrict__ cand,
+                                                        int *__restrict__ ncand) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const long long seg = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long N = *count;
+  const long long lo = seg * SKIP_SEG;
+  const long long hi = lo + SKIP_SEG < N ? lo + SKIP_SEG : N;
+  long long pos = lo - 1;
+  bool live = lo < hi;
+  uint32_t draw = 0;
+  U4 r = {0u, 0u, 0u, 0u};
+  int left = 0;
+  while (__any_sync(full, live)) {
+    long long pick = -1;
+    if (live) {
+      if (left == 0) {
+        r = philox4x32_10({(uint32_t)seg, 16u + draw, c.c2, c.c3}, c.k0, c.k1);
+        ++draw;
+        left = 4;
+      }
+      const uint32_t v = r.x;
+      r.x = r.y;
+      r.y = r.z;
+      r.z = r.w;
+      --left;
+      const double gap = floor(log(u01(v)) * inv_log1m);
+      pos = gap < (double)SKIP_SEG ? pos + 1 + (long long)gap : hi;
+      if (pos < hi) pick = pos;
+      else live = false;
+    }
+    const unsigned m = __ballot_sync(full, pick >= 0);
+    if (m) {
+      const int leader = __ffs(m) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(ncand, __popc(m));
+      base = __shfl_sync(full, base, leader);
+      if (pick >= 0) cand[base + __popc(m & lanemask_lt_m())] = (int)pick;
+    }
   }
 }
 
@@ -432,8 +486,18 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
     snprintf(nm, sizeof nm, "work_list%d", p - 1);
     int *cand = (int *)scratch(nm, sizeof(int) * (size_t)S.cap[p - 1]);
     if (!cand) return LEPIC_ERR_CUDA;
-    int tm = timer_start(tname, s);
-    k_mcc_select<<<grid_for(Nh[p - 1], MB), MB, 0, s>>>(c, counts_dev[p - 1], cand, ncand + (p - 1));
+    char sname[32];
+    snprintf(sname, sizeof sname, "%s_select", tname);
+    int tm = timer_start(sname, s);
+    if (Pmax < SKIP_PMAX) {
+      const long long nseg = (Nh[p - 1] + SKIP_SEG - 1) / SKIP_SEG;
+      k_mcc_select_skip<<<grid_for(nseg, MB), MB, 0, s>>>(c, counts_dev[p - 1], 1.0 / log1p(-Pmax), cand,
+                                                          ncand + (p - 1));
+    } else {
+      k_mcc_select<<<grid_for(Nh[p - 1], MB), MB, 0, s>>>(c, counts_dev[p - 1], cand, ncand + (p - 1));
+    }
+    timer_stop(tm, s);
+    tm = timer_start(tname, s);
     k_mcc_collide<Acc><<<ctx().sms * 8, MB, 0, s>>>(c, S, cand, ncand + (p - 1), T.sig_Er, T.sig,
                                                     flag_dead[p - 1], add, cnt, cc, ctx().d_err);
     timer_stop(tm, s);

@@ -88,21 +88,23 @@ __device__ double bsum(double v, double *sh) {
   return r;
 }
 
-// deterministic grid-wide sum of one value per thread
-__device__ double grid_sum(const XArgs &a, double v, cg::grid_group &grid, double *sh) {
-  double part = bsum(v, sh);
-  if (threadIdx.x == 0) a.partial[blockIdx.x] = part;
+// deterministic grid-wide sum of one value per thread.  The block partials
+// alternate between two halves of a.partial (parity), so one barrier
+// suffices: a half is rewritten two sums later, after further barriers.
+__device__ double grid_sum(const XArgs &a, double v, int parity, cg::grid_group &grid, double *sh) {
+  double *part = a.partial + (parity & 1) * gridDim.x;
+  double p = bsum(v, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = p;
   grid.sync();
   double s = 0.0;
   if (threadIdx.x < 32) {
-    for (int bI = threadIdx.x; bI < (int)gridDim.x; bI += 32) s += a.partial[bI];
+    for (int bI = threadIdx.x; bI < (int)gridDim.x; bI += 32) s += part[bI];
     s = wsum(s);
     if (threadIdx.x == 0) sh[33] = s;
   }
   __syncthreads();
   s = sh[33];
   __syncthreads();
-  grid.sync();  // partials may be reused
   return s;
 }
 
@@ -132,28 +134,36 @@ __device__ __forceinline__ float fine_residual(const XLev &F, int i, int j, int 
 }
 
 // 27-point full weighting of the fine residual onto coarse node (i,j,k)
-// (Src/mg.f90:248-805); C.e cleared
-__device__ __forceinline__ void restrict_node(const XLev &F, const XLev &C, int i, int j, int k) {
-  const long long qc = C.g(i, j, k);
-  C.e[qc] = 0.f;
-  if (i > C.n1 + 1 || j > C.n2 + 1 || k > C.n3 + 1) return;
-  float re = 0.f;
-  if (i >= 1 && j >= 1 && k >= 1 && C.bc[qc] <= 0) {
-    const long long sy = F.N1, sz = (long long)F.N1 * F.N2;
-    const long long q = F.g(2 * i - 1, 2 * j - 1, 2 * k - 1);
-    const float *R = F.rf;
-    re = (8.f * R[q] + 4.f * (R[q + 1] + R[q - 1] + R[q + sy] + R[q - sy] + R[q + sz] + R[q - sz]) +
+// (Src/mg.f90:248-805): loads only; 0 outside the interior and on walls
+__device__ __forceinline__ float restrict_value(const XLev &F, const XLev &C, int i, int j, int k) {
+  if (i < 1 || j < 1 || k < 1 || i > C.n1 + 1 || j > C.n2 + 1 || k > C.n3 + 1) return 0.f;
+  if (C.bc[C.g(i, j, k)] > 0) return 0.f;
+  const long long sy = F.N1, sz = (long long)F.N1 * F.N2;
+  const long long q = F.g(2 * i - 1, 2 * j - 1, 2 * k - 1);
+  const float *R = F.rf;
+  return (8.f * R[q] + 4.f * (R[q + 1] + R[q - 1] + R[q + sy] + R[q - sy] + R[q + sz] + R[q - sz]) +
           2.f * (R[q + 1 + sy] + R[q - 1 + sy] + R[q + 1 - sy] + R[q - 1 - sy] + R[q + 1 + sz] + R[q - 1 + sz] +
                  R[q + sy + sz] + R[q - sy + sz] + R[q + 1 - sz] + R[q - 1 - sz] + R[q + sy - sz] +
                  R[q - sy - sz]) +
           R[q + 1 + sy + sz] + R[q - 1 + sy + sz] + R[q + 1 - sy + sz] + R[q - 1 - sy + sz] + R[q + 1 + sy - sz] +
           R[q - 1 + sy - sz] + R[q + 1 - sy - sz] + R[q - 1 - sy - sz]) *
          (1.f / 64.f);
-  }
-  C.r[C.rr(i, j, k)] = re;
 }
 
-// trilinear prolongation of coarse node (i,j,k) added into F (Src/mg.f90:849-939)
+// coarse node (i,j,k), i,j,k in 0..n+2: right-hand side from the fine
+// residual, correction cleared
+__device__ __forceinline__ void restrict_store(const XLev &C, int i, int j, int k, float re) {
+  C.e[C.g(i, j, k)] = 0.f;
+  if (i <= C.n1 + 1 && j <= C.n2 + 1 && k <= C.n3 + 1) C.r[C.rr(i, j, k)] = re;
+}
+
+__device__ __forceinline__ void restrict_node(const XLev &F, const XLev &C, int i, int j, int k) {
+  restrict_store(C, i, j, k, restrict_value(F, C, i, j, k));
+}
+
+// trilinear prolongation of coarse node (i,j,k) added into F
+// (Src/mg.f90:849-939): the 8 coarse values, the 8 fine masks and the 8 fine
+// values are loaded before the 8 stores
 __device__ __forceinline__ void prolong_node(const XLev &F, const XLev &C, int i, int j, int k) {
   const long long sy = F.N1, sz = (long long)F.N1 * F.N2, cy = C.N1, cz = (long long)C.N1 * C.N2;
   const long long c = C.g(i, j, k);
@@ -163,25 +173,34 @@ __device__ __forceinline__ void prolong_node(const XLev &F, const XLev &C, int i
   const long long q = F.g(2 * i - 1, 2 * j - 1, 2 * k - 1);
   float *U = F.e;
   const int *B = F.bc;
-  if (B[q] <= 0) U[q] += r000;
-  if (B[q - sy] <= 0) U[q - sy] += (r000 + r0m0) * 0.5f;
-  if (B[q - 1 - sy] <= 0) U[q - 1 - sy] += (r000 + r0m0 + rmm0 + rm00) * 0.25f;
-  if (B[q - 1] <= 0) U[q - 1] += (r000 + rm00) * 0.5f;
-  if (B[q - sz] <= 0) U[q - sz] += (r000 + r00m) * 0.5f;
-  if (B[q - sy - sz] <= 0) U[q - sy - sz] += (r000 + r00m + r0mm + r0m0) * 0.25f;
-  if (B[q - 1 - sz] <= 0) U[q - 1 - sz] += (r000 + r00m + rm0m + rm00) * 0.25f;
-  if (B[q - 1 - sy - sz] <= 0)
-    U[q - 1 - sy - sz] += (r000 + r00m + rm0m + rm00 + r0m0 + r0mm + rmmm + rmm0) * 0.125f;
+  const long long o[8] = {0, -sy, -1 - sy, -1, -sz, -sy - sz, -1 - sz, -1 - sy - sz};
+  int bm[8];
+  float uv[8];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    bm[t] = B[q + o[t]];
+    uv[t] = U[q + o[t]];
+  }
+  const float add[8] = {r000,
+                        (r000 + r0m0) * 0.5f,
+                        (r000 + r0m0 + rmm0 + rm00) * 0.25f,
+                        (r000 + rm00) * 0.5f,
+                        (r000 + r00m) * 0.5f,
+                        (r000 + r00m + r0mm + r0m0) * 0.25f,
+                        (r000 + r00m + rm0m + rm00) * 0.25f,
+                        (r000 + r00m + rm0m + rm00 + r0m0 + r0mm + rmmm + rmm0) * 0.125f};
+#pragma unroll
+  for (int t = 0; t < 8; ++t)
+    if (bm[t] <= 0) U[q + o[t]] = uv[t] + add[t];
 }
 
 __device__ __forceinline__ int fmapx(int ic, int ncell) {
   return ic == ncell / 2 + 2 ? ncell + 2 : (ic == 0 ? 0 : 2 * ic - 1);
 }
 
-// ------------------------------------------------------------ grid-wide
 // The rows (j, k), j in [j0, j0 + nj), k in [k0, k0 + nk), dealt round-robin
 // to all warps of the grid; body(j, k) runs on all lanes, which split the row
-// along i (coalesced, one 32-bit division per row).
+// along i.
 template <class F>
 __device__ __forceinline__ void grid_rows(int j0, int nj, int k0, int nk, F &&body) {
   const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -193,36 +212,206 @@ __device__ __forceinline__ void grid_rows(int j0, int nj, int k0, int nk, F &&bo
   }
 }
 
-__device__ void g_smooth(const XLev &L, float omega, int nsweep, cg::grid_group &grid) {
-  const int lane = threadIdx.x & 31;
+// ------------------------------------------------------------ grid-wide
+// The grid levels are small enough to stay in L2 (a 128^3 level of FP32
+// arrays is 9 MB each), so a phase costs the latency of its dependent loads,
+// not bandwidth.  Each thread therefore takes XU slots of a flat index range
+// at once (slot t, t + nth, ...), issues every load of all XU slots before
+// the first arithmetic, then computes and stores: one round trip to L2 per
+// XU slots instead of two per node.
+constexpr int XU = 2;
+
+struct Slots {
+  int tid, nth;
+};
+__device__ __forceinline__ Slots slots() {
+  return {(int)(blockIdx.x * blockDim.x + threadIdx.x), (int)(gridDim.x * blockDim.x)};
+}
+
+// one red-black half-sweep of level L (slots: (m, j, k), i = start + 2m);
+// with u, the finest level's last half-sweep also adds the new correction of
+// its nodes to the FP64 solution
+__device__ __noinline__ void g_half_sweep(const XLev &L, float omega, int colour, Slots S, double *u = nullptr) {
+  const int half = (L.n1 + 2) / 2, nrow = L.n2 + 1;
+  const int total = half * nrow * (L.n3 + 1);
+  const long long sy = L.N1, sz = (long long)L.N1 * L.N2;
   const float rac = 1.f / L.ac;
+  for (int base = S.tid; base < total; base += XU * S.nth) {
+    long long q[XU], rq[XU];
+    bool ok[XU];
+#pragma unroll
+    for (int v = 0; v < XU; ++v) {
+      const int t = base + v * S.nth;
+      ok[v] = false;
+      q[v] = rq[v] = 0;
+      if (t < total) {
+        const int row = t / half, m = t - row * half;
+        const int k = row / nrow + 1, j = row - (k - 1) * nrow + 1;
+        const int i = colour_start(colour, j, k) + 2 * m;
+        if (i <= L.n1 + 1) {
+          ok[v] = true;
+          q[v] = L.g(i, j, k);
+          rq[v] = L.rr(i, j, k);
+        }
+      }
+    }
+    int bc[XU];
+    float r[XU], c0[XU], ew[XU], en[XU], es[XU], ee[XU], et[XU], eb[XU];
+#pragma unroll
+    for (int v = 0; v < XU; ++v) {
+      if (!ok[v]) continue;
+      const long long w = q[v];
+      bc[v] = L.bc[w];
+      r[v] = L.r[rq[v]];
+      c0[v] = L.e[w];
+      ew[v] = L.e[w - 1];
+      en[v] = L.e[w + sy];
+      es[v] = L.e[w - sy];
+      ee[v] = L.e[w + 1];
+      et[v] = L.e[w + sz];
+      eb[v] = L.e[w - sz];
+    }
+    double uo[XU];
+    if (u) {
+#pragma unroll
+      for (int v = 0; v < XU; ++v)
+        if (ok[v] && bc[v] <= 0) uo[v] = u[q[v]];
+    }
+#pragma unroll
+    for (int v = 0; v < XU; ++v) {
+      if (!ok[v] || bc[v] > 0) continue;
+      const float tt = r[v] - L.aw * ew[v] - L.an * en[v] - L.as * es[v] - L.ae * ee[v] - L.at * et[v] -
+                       L.ab * eb[v];
+      const float en1 = (1.f - omega) * c0[v] + omega * tt * rac;
+      L.e[q[v]] = en1;
+      if (u) u[q[v]] = uo[v] + (double)en1;
+    }
+  }
+}
+
+// u += e on the nodes of one colour (their correction is final)
+__device__ __noinline__ void g_add_colour(const XLev &L, int colour, Slots S, double *u) {
+  const int half = (L.n1 + 2) / 2, nrow = L.n2 + 1;
+  const int total = half * nrow * (L.n3 + 1);
+  for (int base = S.tid; base < total; base += XU * S.nth) {
+    long long q[XU];
+    bool ok[XU];
+#pragma unroll
+    for (int v = 0; v < XU; ++v) {
+      const int t = base + v * S.nth;
+      ok[v] = false;
+      q[v] = 0;
+      if (t < total) {
+        const int row = t / half, m = t - row * half;
+        const int k = row / nrow + 1, j = row - (k - 1) * nrow + 1;
+        const int i = colour_start(colour, j, k) + 2 * m;
+        if (i <= L.n1 + 1) {
+          ok[v] = true;
+          q[v] = L.g(i, j, k);
+        }
+      }
+    }
+    int bc[XU];
+    float ev[XU];
+    double uo[XU];
+#pragma unroll
+    for (int v = 0; v < XU; ++v) {
+      if (!ok[v]) continue;
+      bc[v] = L.bc[q[v]];
+      ev[v] = L.e[q[v]];
+      uo[v] = u[q[v]];
+    }
+#pragma unroll
+    for (int v = 0; v < XU; ++v)
+      if (ok[v] && bc[v] <= 0) u[q[v]] = uo[v] + (double)ev[v];
+  }
+}
+
+// nsweep red-black sweeps; with u (finest level, last smoothing of the
+// cycle) the last half-sweep also accumulates u += e on every node
+__device__ __noinline__ void g_smooth(const XLev &L, float omega, int nsweep, cg::grid_group &grid, double *u = nullptr) {
+  const Slots S = slots();
   for (int s = 0; s < nsweep; ++s) {
     for (int colour = 0; colour < 2; ++colour) {
-      grid_rows(1, L.n2 + 1, 1, L.n3 + 1, [&](int j, int k) {
-        for (int i = colour_start(colour, j, k) + 2 * lane; i <= L.n1 + 1; i += 64) relax(L, omega, rac, i, j, k);
-      });
+      const bool last = u && s == nsweep - 1 && colour == 1;
+      g_half_sweep(L, omega, colour, S, last ? u : nullptr);
+      if (last) g_add_colour(L, 0, S, u);
       grid.sync();
     }
   }
 }
 
-__device__ void g_restrict(const XLev &F, const XLev &C, cg::grid_group &grid) {
-  const int lane = threadIdx.x & 31;
-  grid_rows(1, F.n2 + 1, 1, F.n3 + 1, [&](int j, int k) {
-    for (int i = 1 + lane; i <= F.n1 + 1; i += 32) F.rf[F.g(i, j, k)] = fine_residual(F, i, j, k);
-  });
+// fine residual rf = r - A e on the interior nodes (0 on walls)
+__device__ __noinline__ void g_residual(const XLev &F, Slots S) {
+  const int ni = F.n1 + 1, nj = F.n2 + 1;
+  const int total = ni * nj * (F.n3 + 1);
+  const long long sy = F.N1, sz = (long long)F.N1 * F.N2;
+  for (int base = S.tid; base < total; base += XU * S.nth) {
+    long long q[XU], rq[XU];
+    bool ok[XU];
+#pragma unroll
+    for (int u = 0; u < XU; ++u) {
+      const int t = base + u * S.nth;
+      ok[u] = t < total;
+      q[u] = rq[u] = 0;
+      if (ok[u]) {
+        const int row = t / ni, i = t - row * ni + 1;
+        const int k = row / nj + 1, j = row - (k - 1) * nj + 1;
+        q[u] = F.g(i, j, k);
+        rq[u] = F.rr(i, j, k);
+      }
+    }
+    int bc[XU];
+    float r[XU], c0[XU], ew[XU], en[XU], es[XU], ee[XU], et[XU], eb[XU];
+#pragma unroll
+    for (int u = 0; u < XU; ++u) {
+      if (!ok[u]) continue;
+      const long long v = q[u];
+      bc[u] = F.bc[v];
+      r[u] = F.r[rq[u]];
+      c0[u] = F.e[v];
+      ew[u] = F.e[v - 1];
+      en[u] = F.e[v + sy];
+      es[u] = F.e[v - sy];
+      ee[u] = F.e[v + 1];
+      et[u] = F.e[v + sz];
+      eb[u] = F.e[v - sz];
+    }
+#pragma unroll
+    for (int u = 0; u < XU; ++u) {
+      if (!ok[u]) continue;
+      F.rf[q[u]] = bc[u] > 0 ? 0.f
+                             : r[u] - (F.aw * ew[u] + F.ae * ee[u] + F.an * en[u] + F.as * es[u] +
+                                       F.ac * c0[u] + F.at * et[u] + F.ab * eb[u]);
+    }
+  }
+}
+
+__device__ __noinline__ void g_restrict(const XLev &F, const XLev &C, cg::grid_group &grid) {
+  const Slots S = slots();
+  g_residual(F, S);
   grid.sync();
-  grid_rows(0, C.n2 + 3, 0, C.n3 + 3, [&](int j, int k) {
-    for (int i = lane; i <= C.n1 + 2; i += 32) restrict_node(F, C, i, j, k);
-  });
+  const int ni = C.n1 + 3, nj = C.n2 + 3;
+  const int total = ni * nj * (C.n3 + 3);
+  // one coarse node per iteration: its 27 loads are already independent
+  for (int t = S.tid; t < total; t += S.nth) {
+    const int row = t / ni, i = t - row * ni;
+    const int k = row / nj, j = row - k * nj;
+    restrict_node(F, C, i, j, k);
+  }
   grid.sync();
 }
 
-__device__ void g_prolong(const XLev &F, const XLev &C, cg::grid_group &grid) {
-  const int lane = threadIdx.x & 31;
-  grid_rows(1, C.n2 + 1, 1, C.n3 + 1, [&](int j, int k) {
-    for (int i = 1 + lane; i <= C.n1 + 1; i += 32) prolong_node(F, C, i, j, k);
-  });
+__device__ __noinline__ void g_prolong(const XLev &F, const XLev &C, cg::grid_group &grid) {
+  const Slots S = slots();
+  const int ni = C.n1 + 1, nj = C.n2 + 1;
+  const int total = ni * nj * (C.n3 + 1);
+  // one coarse node per iteration: its 24 loads are already independent
+  for (int t = S.tid; t < total; t += S.nth) {
+    const int row = t / ni, i = t - row * ni + 1;
+    const int k = row / nj + 1, j = row - (k - 1) * nj + 1;
+    prolong_node(F, C, i, j, k);
+  }
   grid.sync();
 }
 
@@ -275,11 +464,20 @@ __device__ __forceinline__ XLev smem_level(const XArgs &a, int l, unsigned char 
 }
 
 // the coarse part of the V-cycle, block 0 only: r of level ls+1 in, e out
-__device__ void coarse_cycle(const XArgs &a, unsigned char *sm) {
+__device__ __noinline__ void coarse_cycle(const XArgs &a, unsigned char *sm) {
   const int top = a.ls + 1, ng = a.ng;
   {
+    // four independent loads in flight per thread
     const XLev G = a.L[top], S = smem_level(a, top, sm);
-    for (long long t = threadIdx.x; t < G.nr(); t += blockDim.x) S.r[t] = G.r[t];
+    const int nr = (int)G.nr(), nt = (int)blockDim.x;
+    for (int t0 = threadIdx.x; t0 < nr; t0 += 4 * nt) {
+      float v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = t0 + u * nt < nr ? G.r[t0 + u * nt] : 0.f;
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (t0 + u * nt < nr) S.r[t0 + u * nt] = v[u];
+    }
     for (long long t = threadIdx.x; t < G.nn(); t += blockDim.x) S.e[t] = 0.f;
   }
   __syncthreads();
@@ -301,7 +499,63 @@ __device__ void coarse_cycle(const XArgs &a, unsigned char *sm) {
   __threadfence();
 }
 
-__global__ void __launch_bounds__(XM_BLOCK) k_refine_mixed(const XArgs *__restrict__ ap) {
+// FP64 residual b - A u of the finest level on its interior nodes, written
+// as the FP32 right-hand side of the V-cycle (0 on walls); returns this
+// thread's share of the L1 norm over the plasma nodes (bcnd = -1)
+__device__ __noinline__ double g_residual_f64(const XArgs &a, const XLev &L1, Slots S) {
+  constexpr int U = 2;
+  const int ni = L1.n1 + 1, nj = L1.n2 + 1;
+  const int total = ni * nj * (L1.n3 + 1);
+  const long long sy = L1.N1, sz = (long long)L1.N1 * L1.N2;
+  const double *u = a.u;
+  double acc = 0.0;
+  for (int base = S.tid; base < total; base += U * S.nth) {
+    long long q[U], rq[U];
+    bool ok[U];
+#pragma unroll
+    for (int v = 0; v < U; ++v) {
+      const int t = base + v * S.nth;
+      ok[v] = t < total;
+      q[v] = rq[v] = 0;
+      if (ok[v]) {
+        const int row = t / ni, i = t - row * ni + 1;
+        const int k = row / nj + 1, j = row - (k - 1) * nj + 1;
+        q[v] = L1.g(i, j, k);
+        rq[v] = L1.rr(i, j, k);
+      }
+    }
+    int bc[U];
+    double bv[U], c0[U], uw[U], un[U], us[U], ue[U], ut[U], ub[U];
+#pragma unroll
+    for (int v = 0; v < U; ++v) {
+      if (!ok[v]) continue;
+      const long long w = q[v];
+      bc[v] = L1.bc[w];
+      bv[v] = a.b[rq[v]];
+      c0[v] = u[w];
+      uw[v] = u[w - 1];
+      un[v] = u[w + sy];
+      us[v] = u[w - sy];
+      ue[v] = u[w + 1];
+      ut[v] = u[w + sz];
+      ub[v] = u[w - sz];
+    }
+#pragma unroll
+    for (int v = 0; v < U; ++v) {
+      if (!ok[v]) continue;
+      double rv = 0.0;
+      if (bc[v] <= 0) {
+        rv = bv[v] - (a.aw * uw[v] + a.an * un[v] + a.as * us[v] + a.ae * ue[v] + a.ac * c0[v] + a.at * ut[v] +
+                      a.ab * ub[v]);
+        if (bc[v] == -1) acc += fabs(rv);
+      }
+      L1.r[rq[v]] = (float)rv;
+    }
+  }
+  return acc;
+}
+
+__global__ void __launch_bounds__(XM_BLOCK, 1) k_refine_mixed(const XArgs *__restrict__ ap) {
   cg::grid_group grid = cg::this_grid();
   const XArgs &a = *ap;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -329,30 +583,14 @@ __global__ void __launch_bounds__(XM_BLOCK) k_refine_mixed(const XArgs *__restri
     __syncthreads();
   }
   const XLev &L1 = a.L[1];
-  const long long sy = L1.N1, sz = (long long)L1.N1 * L1.N2;
+  const Slots S = slots();
   double res = 0.0, res0 = -1.0;
   int it = 0, status = 0;
   for (;;) {
     // FP64 residual, FP32 copy as the V-cycle right-hand side, e = 0
-    double acc = 0.0;
-    grid_rows(1, L1.n2 + 1, 1, L1.n3 + 1, [&](int j, int k) {
-      for (int i = 1 + lane; i <= L1.n1 + 1; i += 32) {
-        const long long q = L1.g(i, j, k);
-        double rv = 0.0;
-        const int bc = L1.bc[q];
-        if (bc <= 0) {
-          const double *u = a.u;
-          rv = a.b[L1.rr(i, j, k)] - (a.aw * u[q - 1] + a.an * u[q + sy] + a.as * u[q - sy] +
-                                      a.ae * u[q + 1] + a.ac * u[q] + a.at * u[q + sz] + a.ab * u[q - sz]);
-          if (bc == -1) acc += fabs(rv);
-        }
-        L1.r[L1.rr(i, j, k)] = (float)rv;
-      }
-    });
-    grid_rows(0, L1.n2 + 3, 0, L1.n3 + 3, [&](int j, int k) {
-      for (int i = lane; i <= L1.n1 + 2; i += 32) L1.e[L1.g(i, j, k)] = 0.f;
-    });
-    res = grid_sum(a, acc, grid, sh) / a.alpha;
+    const double acc = g_residual_f64(a, L1, S);
+    for (long long t = S.tid; t < L1.nn(); t += S.nth) L1.e[t] = 0.f;
+    res = grid_sum(a, acc, it, grid, sh) / a.alpha;
     if (res0 < 0.0) res0 = res;
     if (res < a.eps) break;
     if (it >= a.max_refine) {
@@ -364,29 +602,31 @@ __global__ void __launch_bounds__(XM_BLOCK) k_refine_mixed(const XArgs *__restri
       break;
     }
     // FP32 V-cycle on the correction: grid levels down, coarse levels on
-    // chip, grid levels up
+    // chip, grid levels up; the last smoothing of level 1 also applies
+    // u += e (FP64)
     for (int l = 1; l <= ls && l < ng; ++l) {
       g_smooth(a.L[l], a.omega, a.nu_pre, grid);
       g_restrict(a.L[l], a.L[l + 1], grid);
     }
+    bool added = false;
     if (ls < ng) {
       if (blockIdx.x == 0) coarse_cycle(a, smem);
       grid.sync();
     } else {
-      g_smooth(a.L[ng], a.omega, a.coarse_sweeps, grid);
+      added = ng == 1 && a.coarse_sweeps > 0;
+      g_smooth(a.L[ng], a.omega, a.coarse_sweeps, grid, added ? a.u : nullptr);
     }
     for (int l = (ls < ng ? ls : ng - 1); l >= 1; --l) {
       g_prolong(a.L[l], a.L[l + 1], grid);
-      g_smooth(a.L[l], a.omega, a.nu_post, grid);
+      const bool fin = l == 1 && a.nu_post > 0;
+      g_smooth(a.L[l], a.omega, a.nu_post, grid, fin ? a.u : nullptr);
+      added = added || fin;
     }
-    // u += e (FP64)
-    grid_rows(1, L1.n2 + 1, 1, L1.n3 + 1, [&](int j, int k) {
-      for (int i = 1 + lane; i <= L1.n1 + 1; i += 32) {
-        const long long q = L1.g(i, j, k);
-        if (L1.bc[q] <= 0) a.u[q] = a.u[q] + (double)L1.e[q];
-      }
-    });
-    grid.sync();
+    if (!added) {
+      g_add_colour(L1, 0, S, a.u);
+      g_add_colour(L1, 1, S, a.u);
+      grid.sync();
+    }
     ++it;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -482,7 +722,7 @@ int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const do
   LEPIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_refine_mixed, XM_BLOCK, smem));
   if (occ < 1) return LEPIC_ERR_CUDA;
   const int blocks = c.sms * (occ < 2 ? occ : 2);
-  A.partial = (double *)scratch("xm_partial", sizeof(double) * blocks);
+  A.partial = (double *)scratch("xm_partial", sizeof(double) * 2 * blocks);
   A.out_i = (int *)scratch("xm_out_i", sizeof(int) * 4);
   A.out_d = (double *)scratch("xm_out_d", sizeof(double) * 2);
   XArgs *dA = (XArgs *)scratch("xm_args", sizeof(XArgs));

