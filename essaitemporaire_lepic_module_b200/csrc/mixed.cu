@@ -518,25 +518,102 @@ __global__ void k_tile_offsets(const int *__restrict__ off, int ntiles, int *__r
   if (t <= ntiles) tile_off[t] = off[(long long)t * (TC * TC * TC)];
 }
 
-__global__ void k_msort_scatter(const int *__restrict__ cell, const float *__restrict__ p,
-                                int *__restrict__ cell_o, float *__restrict__ p_o, long long cap,
-                                const int *__restrict__ count, int ntx, int nty, int *cursor) {
-  const unsigned full = 0xffffffffu;
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int N = *count;
-  const int cc = (i < N) ? cell[i] : -1;
-  const int k = (i < N) ? tile_key(cc, ntx, nty) : -1;
-  bool head;
-  int start, len;
-  run_of(k, head, start, len);
-  int base = 0;
-  if (head && k >= 0) base = atomicAdd(&cursor[k], len);
-  base = __shfl_sync(full, base, start);
-  if (i < N) {
-    const long long j = base + ((threadIdx.x & 31) - start);
-    cell_o[j] = cc;
+// Scatter of the counting sort, one block per chunk of SC_N consecutive
+// particles.  The block groups its particles by key in shared memory (open
+// addressing on the key, the per-key count giving each particle its rank),
+// reserves one range per distinct key with a single atomic on that key's
+// cursor, stages the particles in key order and writes them out so that
+// consecutive threads store consecutive slots of a key's range.
+constexpr int SC_T = 256, SC_U = 4, SC_N = SC_T * SC_U, SC_H = 1024, SC_HBITS = 10;
+constexpr size_t SC_SMEM = sizeof(int) * (4 * SC_H + 2 * SC_N) + sizeof(float) * 6 * SC_N;
+static_assert(SC_H >= SC_N, "the table holds every distinct key of a chunk");
+
+__global__ void __launch_bounds__(SC_T, 4) k_msort_scatter(const int *__restrict__ cell, const float *__restrict__ p,
+                                                           int *__restrict__ cell_o, float *__restrict__ p_o,
+                                                           long long cap, const int *__restrict__ count, int ntx,
+                                                           int nty, int *__restrict__ cursor) {
+  extern __shared__ __align__(16) int smi[];
+  int *hkey = smi, *hcnt = hkey + SC_H, *hoff = hcnt + SC_H, *hbase = hoff + SC_H;
+  int *sdest = hbase + SC_H, *scell = sdest + SC_N;
+  float *sp = reinterpret_cast<float *>(scell + SC_N);
+  __shared__ int wsum[SC_T / 32];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const long long N = *count;
+  const long long c0 = (long long)blockIdx.x * SC_N;
+  if (c0 >= N) return;  // uniform over the block
+  for (int q = t; q < SC_H; q += SC_T) {
+    hkey[q] = -1;
+    hcnt[q] = 0;
+  }
+  __syncthreads();
+  int cc[SC_U], slot[SC_U], rank[SC_U];
 #pragma unroll
-    for (int a = 0; a < 6; ++a) p_o[a * cap + j] = p[a * cap + i];
+  for (int u = 0; u < SC_U; ++u) {
+    const long long idx = c0 + u * SC_T + t;
+    slot[u] = -1;
+    cc[u] = 0;
+    rank[u] = 0;
+    if (idx < N) {
+      cc[u] = cell[idx];
+      const int key = tile_key(cc[u], ntx, nty);
+      unsigned h = ((unsigned)key * 2654435761u) >> (32 - SC_HBITS);
+      // at most SC_N distinct keys per chunk: a free or matching slot exists
+      for (int probe = 0; probe < SC_H; ++probe) {
+        const int prev = atomicCAS(&hkey[h], -1, key);
+        if (prev == -1 || prev == key) break;
+        h = (h + 1) & (SC_H - 1);
+      }
+      slot[u] = (int)h;
+      rank[u] = atomicAdd(&hcnt[h], 1);
+    }
+  }
+  __syncthreads();
+  {
+    // exclusive scan of the slot counts (four slots per thread), then one
+    // range per distinct key from its global cursor
+    constexpr int PER = SC_H / SC_T;
+    int v[PER];
+    int sum = 0;
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      v[j] = hcnt[t * PER + j];
+      sum += v[j];
+    }
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    int run = incl - sum;
+    for (int w = 0; w < warp; ++w) run += wsum[w];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      hoff[t * PER + j] = run;
+      run += v[j];
+      if (v[j]) hbase[t * PER + j] = atomicAdd(&cursor[hkey[t * PER + j]], v[j]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < SC_U; ++u) {
+    if (slot[u] < 0) continue;
+    const long long idx = c0 + u * SC_T + t;
+    const int lpos = hoff[slot[u]] + rank[u];
+    sdest[lpos] = hbase[slot[u]] + rank[u];
+    scell[lpos] = cc[u];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) sp[a * SC_N + lpos] = p[a * cap + idx];
+  }
+  __syncthreads();
+  const int nv = N - c0 < SC_N ? (int)(N - c0) : SC_N;
+  for (int lp = t; lp < nv; lp += SC_T) {
+    const long long dst = sdest[lp];
+    cell_o[dst] = scell[lp];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) p_o[a * cap + dst] = sp[a * SC_N + lp];
   }
 }
 
@@ -764,9 +841,10 @@ int launch_sort_mixed(const lepic_grid_t &g, lepic_species_mixed_t &sp, int n_hi
   timer_stop(t1, s);
   if (rc) return rc;
   if (sp.tile_off) k_tile_offsets<<<grid_for(ntiles + 1, 256), 256, 0, s>>>(cnt, ntiles, sp.tile_off);
+  LEPIC_CUDA(cudaFuncSetAttribute(k_msort_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SC_SMEM));
   int t2 = timer_start("sort_scatter_mixed", s);
-  k_msort_scatter<<<grid_for(nthreads, MBK), MBK, 0, s>>>(sp.cell, sp.p, sp.cell_alt, sp.p_alt, sp.cap,
-                                                          sp.count, ntx, nty, cnt);
+  k_msort_scatter<<<grid_for(nthreads, SC_N), SC_T, SC_SMEM, s>>>(sp.cell, sp.p, sp.cell_alt, sp.p_alt, sp.cap,
+                                                                  sp.count, ntx, nty, cnt);
   timer_stop(t2, s);
   LEPIC_CUDA(cudaGetLastError());
   int *tc = sp.cell;

@@ -293,7 +293,7 @@ class MainLoop:
     brings the host arrays up to date."""
 
     def __init__(self, st, vxp, np_tot, flag_dead, np_grids, resident=False, iseed=4242,
-                 nsort=None, ns_coll=None, collide=True, ncol_mx=65, npt_mx=1300):
+                 nsort=None, ns_coll=None, collide=True, ncol_mx=65, npt_mx=1300, regions=()):
         assert vxp.flags["C_CONTIGUOUS"] and vxp.dtype == np.float64
         assert np_tot.dtype == np.int32 and flag_dead.dtype == np.int8
         assert np_grids.flags["C_CONTIGUOUS"] and np_grids.dtype == np.float64
@@ -327,6 +327,7 @@ class MainLoop:
         self.zi = np.zeros(16, dtype=np.int32)
         self.zd = np.zeros(16)
         self.collide = bool(collide) and st.tables is not None
+        self.regions = list(regions)  # [(ixl, ixr)]: MCC region counters in cnt_col
         self.ncol = self.npt = 0
         if self.collide:
             T = st.tables
@@ -345,12 +346,17 @@ class MainLoop:
             self.sigv[:self.ncol, :] = T.sigv_mx.T
             self.col_info = np.zeros((10, ncol_mx), dtype=np.int32)
             self.col_info[:, :self.ncol] = T.col_info.T
-            self.cnt_col = np.zeros((1, 1, ncol_mx))
+            self.cnt_col = np.zeros((max(len(self.regions), 1), 1, ncol_mx))
         set_residency(self.resident)
 
     def _commons(self):
         if self.collide:
             set_commons(self.st, ncol=self.ncol, npt=self.npt, p_ncol=self.p_ncol)
+            pi_ = commons()["part_info_int"]
+            pi_.n_rg = len(self.regions)
+            for g, (lo, hi) in enumerate(self.regions):
+                pi_.ixl_rg[g], pi_.ixr_rg[g] = int(lo), int(hi)
+            pi_.iyl_rg, pi_.iyr_rg, pi_.izl_rg, pi_.izr_rg = 1, self.st.n[1] + 1, 1, self.st.n[2] + 1
         else:
             set_commons(self.st)
 

@@ -48,6 +48,27 @@ def allreduce_density(np_grids, group=None):
     return np_grids
 
 
+def sort_intervals(st, nsort, policy="reference"):
+    """Steps between sorts of each species.  "reference": every species every
+    nsort steps (Src/main.f90:1071-1080).  "adaptive": the order only serves
+    the push's memory locality, so a species whose thermal displacement in
+    nsort steps, vt0 dt nsort / h, stays below half a cell is sorted up to
+    ten times less often (a multiple of nsort); fast species keep nsort."""
+    if not nsort:
+        return [0] * st.ntype
+    if policy == "reference":
+        return [int(nsort)] * st.ntype
+    if policy != "adaptive":
+        raise ValueError(f"sort policy must be 'reference' or 'adaptive', not {policy!r}")
+    hmin = float(min(st.h))
+    out = []
+    for p in range(st.ntype):
+        d = float(st.vt0[p]) * float(st.dt) * nsort / hmin
+        m = 10 if d <= 0.05 else max(1, min(10, int(0.5 / d)))
+        out.append(int(nsort) * m)
+    return out
+
+
 def rank_weight(Nm, world):
     """Macroparticle weight of each of `world` ranks that each load a full
     set of particles of weight Nm: Nm / world keeps the plasma density."""
@@ -132,7 +153,7 @@ class Simulation:
     deposition and every rank solves the same field."""
 
     def __init__(self, st, cap=None, device="cuda", seed=123456, nsort=None, ns_coll=None,
-                 fused=True, precision="f64", mg_mixed=None, comm=None):
+                 fused=True, precision="f64", mg_mixed=None, comm=None, sort_policy="reference"):
         if precision not in ("f64", "mixed"):
             raise ValueError(f"precision must be 'f64' or 'mixed', not {precision!r}")
         self.st = st
@@ -151,6 +172,8 @@ class Simulation:
         self.stream = torch.cuda.current_stream(self.dev)
         self.nsort = st.wl.nsort if nsort is None else nsort
         self.ns_coll = st.wl.ns_coll if ns_coll is None else ns_coll
+        self.sort_every = sort_intervals(st, self.nsort, sort_policy)
+        self.sort_policy = sort_policy
         self.seed = int(seed)
         self.P = phys_struct(st)
         self.comm = comm
@@ -334,9 +357,11 @@ class Simulation:
         check(lib().lepic_dev_pack_e32(_ptr(self.Ei), _ptr(self.E32), C.c_longlong(self.Ei.numel() // 3),
                                        self._s()), "pack_e32")
 
-    def sort(self):
+    def sort(self, species=None):
+        """Counting sort by cell of the given species (0-based; all by default)."""
+        todo = [self.sp[p] for p in (range(len(self.sp)) if species is None else species)]
         if self.mixed:
-            for s in self.sp:
+            for s in todo:
                 check(lib().lepic_dev_sort_mixed(C.byref(self.grid), C.byref(s.s), self._hint(s),
                                                  self._s()), "sort_mixed")
                 s.after_call()
@@ -344,7 +369,7 @@ class Simulation:
         pl_max = self.st.n[0] + self.st.n[0] * (self.st.n[1] + self.st.n[1] * self.st.n[2]) + 1
         if not hasattr(self, "_plist") or self._plist.numel() < pl_max + 1:
             self._plist = torch.zeros(pl_max + 1, dtype=torch.int32, device=self.dev)
-        for s in self.sp:
+        for s in todo:
             check(lib().lepic_dev_part_sorting(C.byref(self.grid), C.byref(s.s), _ptr(self._plist),
                                                pl_max, self._s()), "part_sorting")
             s.after_call()
@@ -402,7 +427,9 @@ class Simulation:
         if self._acc is None:
             self._acc = torch.zeros((st.ntype, 2 + 2 * (st.geom.ngrid + 1)), dtype=torch.float64,
                                     device=self.dev)
-        counts = torch.cat([s.count for s in self.sp]).cpu().numpy()
+        # the FP64 push sizes its grid by the counts (a host read); the mixed
+        # push walks its tiles and a grid-stride tail and needs none
+        counts = None if self.mixed else torch.cat([s.count for s in self.sp]).cpu().numpy()
         self.np.zero_()
         for p, s in enumerate(self.sp):
             if st.charge[p] == 0.0:
@@ -411,7 +438,7 @@ class Simulation:
                 check(lib().lepic_dev_push_deposit_mixed(
                     C.byref(self.grid), _ptr(self.E32), C.byref(s.s), p + 1, st.geom.ngrid,
                     C.byref(self.P), C.c_void_p(self.np[p].data_ptr()),
-                    C.c_void_p(self._acc[p].data_ptr()), int(counts[p]), self._s()),
+                    C.c_void_p(self._acc[p].data_ptr()), -1, self._s()),
                     "push_deposit_mixed")
                 continue
             check(lib().lepic_dev_push_deposit(C.byref(self.grid), _ptr(self.Ei), C.byref(s.s), p + 1,
@@ -442,8 +469,9 @@ class Simulation:
         self.calc_rho()
         self.pdesolver()
         self.efield()
-        if self.nsort and it % self.nsort == 1 % self.nsort:
-            self.sort()
+        due = [p for p, k in enumerate(self.sort_every) if k and it % k == 1 % k]
+        if due:
+            self.sort(due)
         if self._tables is not None and it > 1 and it % self.ns_coll == 1 % self.ns_coll:
             self.collisions()
         if self.fused:

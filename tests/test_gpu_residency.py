@@ -9,7 +9,7 @@ Bars, written in each test:
   * after the first step the resident loop moves fewer than 1e-3 of the
     per-call bytes between host and device;
   * host-appended particles (injection) reach the device through np_tot;
-  * MCC under residency: ionizations within 5 sigma of the copy mode.
+  * MCC under residency: counted collisions within 5 sigma of the copy mode.
 """
 import numpy as np
 import pytest
@@ -158,16 +158,26 @@ def test_update_device_and_stale_mirror(box16):
 
 
 def test_mcc_loop_resident():
-    """MCC every step through collisions_ with resident particle mirrors:
-    ions created (np_tot over a collisionless run of the same steps) within
-    5 sigma of the per-call copy mode."""
+    """MCC every step through collisions_ with resident particle mirrors and
+    a region counter over the whole box (which reads np_red back from its
+    mirror): the counted collisions, sum over processes of cnt_col times the
+    region population, within 5 sigma of the per-call copy mode."""
     oracle.set_threads(1)
     st = config.build("mcc32")
     S0 = oracle.load_part(st, nmax=int(st.n_particles() * 1.3))
-    a = run_loop(st, S0, False, 10, collide=True, ns_coll=1)
-    b = run_loop(st, S0, True, 10, collide=True, ns_coll=1)
-    c = run_loop(st, S0, True, 10, collide=False)
-    ga = int(a["np_tot"][1]) - int(c["np_tot"][1])
-    gb = int(b["np_tot"][1]) - int(c["np_tot"][1])
-    assert ga > 0 and gb > 0, (ga, gb)
-    assert abs(ga - gb) <= 5.0 * np.sqrt(ga + gb) + 5
+    reg = [(1, st.n[0] + 1)]
+    res = {}
+    for resident in (False, True):
+        vxp, np_tot, fd, npg = S0.vxp.copy(), S0.np_tot.copy(), S0.flag_dead.copy(), S0.np.copy()
+        ml = dropin.MainLoop(st, vxp, np_tot, fd, npg, resident=resident, collide=True, ns_coll=1,
+                             regions=reg)
+        try:
+            for _ in range(6):
+                ml.step()
+            ml.sync()
+            res[resident] = float(ml.cnt_col.sum()) * float(np_tot[0])
+        finally:
+            ml.close()
+    a, b = res[False], res[True]
+    assert a > 100 and b > 100, (a, b)
+    assert abs(a - b) <= 5.0 * np.sqrt(a + b), (a, b)
