@@ -132,9 +132,11 @@ def cpu_baseline(workload, steps=10, ppc=4):
         ntot += int(S.np_tot.sum())
         Ei, _, _ = oracle.step(st, S, phi, Ei, it)
     dt = time.perf_counter() - t0
+    nsort = sum(1 for it in range(2, steps + 2) if it % 10 == 1)
+    ncoll = nsort if st.tables is not None else 0
     return {"value": ntot / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{workload} grid {st.n}, {ppc} ppc/species ({st.n_particles()} per species), "
-                      f"{steps} steps it=2..{steps + 1} incl. 1 sort + 1 MCC call, {dt:.1f} s"}
+                      f"{steps} steps it=2..{steps + 1} incl. {nsort} sort(s) + {ncoll} MCC call(s), {dt:.1f} s"}
 
 
 def run_reference(args):
