@@ -349,8 +349,10 @@ def run_poisson(workload, warm=10):
 def run_adjoint(workload, K, every):
     """Adjoint/forward cost of the differentiable window: the gradient of the
     final mean electron energy with respect to the electrode potentials, B_z
-    and the initial velocities (FP64 discrete adjoint, checkpoints every
-    `every` steps, recomputed)."""
+    and the initial velocities (discrete adjoint of the FP64 window, adjoint
+    Poisson solves in FP32 V-cycles inside FP64 refinement, checkpoints every
+    `every` steps, recomputed), and its distance from the FP64 reference
+    gradient (FP64 multigrid adjoint solves)."""
     import torch
     from essaitemporaire_lepic_module_b200 import config
     from essaitemporaire_lepic_module_b200.adjoint import Window, window_objective
@@ -370,8 +372,22 @@ def run_adjoint(workload, K, every):
     timers = _lib.timing()
     _lib.timing(enable=False)
     t = dict(win.timing)
+    # the FP64 reference gradient: the same window with FP64 multigrid adjoint solves
+    win.adjoint_solver = "f64"
+    win.forward(V0, float(Bz))
+    rV, rB, rv = win.backward()
+    tf = dict(win.timing)
+    win.adjoint_solver = "mixed"
+    gV = np.array([float(x) for x in V.grad])
+    ref_err = {"dJ_dV": float(np.abs(gV - rV).max() / max(np.abs(rV).max(), 1e-300)),
+               "dJ_dBz": float(abs(float(Bz.grad) - rB) / max(abs(rB), 1e-300)),
+               "dJ_dv0": float((v0.grad - rv).abs().max() / max(float(rv.abs().max()), 1e-300))}
     out = {"workload": f"{workload} {list(st.n)} cells, {win.n} particles of species 1, K={K}, "
-                       f"checkpoint every {every}, FP64",
+                       f"checkpoint every {every}, FP64 forward, adjoint Poisson solves FP32 V-cycles in "
+                       f"FP64 refinement",
+           "grad_rel_err_vs_fp64_reference": ref_err,
+           "fp64_adjoint": {"forward_ms": tf["forward_ms"], "backward_ms": tf["backward_ms"],
+                            "backward_over_forward": tf["backward_ms"] / tf["forward_ms"]},
            "observable": "mean kinetic energy (eV) after K steps",
            "J": float(J), "dJ_dV_by_label": [float(x) for x in V.grad], "dJ_dBz": float(Bz.grad),
            "dJ_dv0_norm": float(v0.grad.norm()),

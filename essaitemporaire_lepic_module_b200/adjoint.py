@@ -10,7 +10,8 @@ window kernels of liblepic_gpu.so, particles keeping their slots (a particle
 that reaches a wall stops being pushed and deposited).  The backward pass is
 the discrete adjoint of that step (adjoint push, gather and deposition as
 each other's transposes, E = -grad phi transposed, and the adjoint Poisson
-solve through the same multigrid), in reverse, from checkpoints of the
+solve -- by default FP32 V-cycles inside FP64 refinement, to the same
+residual test as the FP64 multigrid, or the FP64 multigrid itself), in reverse, from checkpoints of the
 particle state taken every `every` steps (sqrt(K) by default) and recomputed
 forward one segment at a time.
 
@@ -41,13 +42,20 @@ class Window:
     collisionless workload; the other species are not moved (their charge
     stays where it was loaded)."""
 
-    def __init__(self, st, K, every=None, ptype=1, cap=None, device="cuda"):
+    def __init__(self, st, K, every=None, ptype=1, cap=None, device="cuda", adjoint_solver="mixed"):
         if st.geom.flag_pbc or st.geom.flag_nmn:
             raise ValueError("the adjoint window supports Dirichlet walls only")
         self.st = st
         self.K = int(K)
         self.every = int(every) if every else max(1, int(round(math.sqrt(self.K))))
         self.ptype = int(ptype)
+        if adjoint_solver not in ("mixed", "f64"):
+            raise ValueError(f"adjoint_solver must be 'mixed' or 'f64', not {adjoint_solver!r}")
+        # the adjoint Poisson solves: FP32 V-cycles inside FP64 refinement
+        # ("mixed", converged to the same residual test as the FP64
+        # multigrid) or the FP64 multigrid itself ("f64", the reference
+        # gradient); the forward window always runs the FP64 step
+        self.adjoint_solver = adjoint_solver
         self.sim = Simulation(st, cap=cap, device=device, fused=False)
         self.dev = self.sim.dev
         self.nlabel = int(st.geom.ngrid)
@@ -194,9 +202,17 @@ class Window:
                 r0 = float(b.abs().sum()) / alpha
                 if r0 > 0.0:
                     k, kt, res = C.c_int(0), C.c_double(0), C.c_double(0)
-                    check(L.lepic_dev_pdesolver(C.byref(sim.grid), _p(mu), _p(b), wl.ncycl, wl.eps * r0,
-                                                wl.omega, st.ng, C.byref(sim.P), C.byref(k), C.byref(kt),
-                                                C.byref(res), self._s()), "adjoint pdesolver")
+                    if self.adjoint_solver == "mixed":
+                        m = sim.mg_mixed
+                        check(L.lepic_dev_pdesolver_mixed(C.byref(sim.grid), _p(mu), _p(b), wl.eps * r0,
+                                                          m["omega"], st.ng, C.byref(sim.P), m["max_refine"],
+                                                          m["nu_pre"], m["nu_post"], m["coarse_sweeps"],
+                                                          C.byref(k), C.byref(res), self._s()),
+                              "adjoint pdesolver (mixed)")
+                    else:
+                        check(L.lepic_dev_pdesolver(C.byref(sim.grid), _p(mu), _p(b), wl.ncycl, wl.eps * r0,
+                                                    wl.omega, st.ng, C.byref(sim.P), C.byref(k), C.byref(kt),
+                                                    C.byref(res), self._s()), "adjoint pdesolver")
                 check(L.lepic_dev_adj_walls(C.byref(sim.grid), C.byref(sim.P), self.ptype, _p(lphi), _p(mu),
                                             _p(lnp), _p(dV), self.nlabel, self._s()), "adj_walls")
                 check(L.lepic_dev_adj_deposit(C.byref(sim.grid), _p(pn), n, n, _p(an), _p(lnp), _p(lam), n,
