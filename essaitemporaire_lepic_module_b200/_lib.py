@@ -157,7 +157,7 @@ def lib():
         "lepic_dev_mixed_to_f64": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), vp,
                                     C.c_longlong, C.c_longlong, vp], _I),
         "lepic_dev_pdesolver_mixed": ([C.POINTER(LepicGrid), vp, vp, _D, _D, _I, C.POINTER(LepicPhys),
-                                       _I, _I, _I, _I, P_int, P_dbl, vp], _I),
+                                       _I, _I, _I, _I, _I, _I, P_int, P_dbl, vp], _I),
         "lepic_dev_collisions_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), _I,
                                         C.POINTER(LepicTables), C.POINTER(LepicPhys), C.c_ulonglong,
                                         C.c_ulonglong, P_dbl, C.POINTER(C.c_longlong), vp], _I),

@@ -206,7 +206,8 @@ class Window:
                         m = sim.mg_mixed
                         check(L.lepic_dev_pdesolver_mixed(C.byref(sim.grid), _p(mu), _p(b), wl.eps * r0,
                                                           m["omega"], st.ng, C.byref(sim.P), m["max_refine"],
-                                                          m["nu_pre"], m["nu_post"], m["coarse_sweeps"],
+                                                          m["nu_fine_pre"], m["nu_fine_post"], m["nu_pre"],
+                                                          m["nu_post"], m["coarse_sweeps"],
                                                           C.byref(k), C.byref(res), self._s()),
                               "adjoint pdesolver (mixed)")
                     else:

@@ -132,8 +132,9 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E32, lepic_spe
 int launch_sort_mixed(const lepic_grid_t &g, lepic_species_mixed_t &sp, int n_hint, cudaStream_t s);
 // mgmixed.cu
 int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const double *b, const int *bcnd,
-                           double eps, double omega, int ng, double eps0, int max_refine, int nu_pre,
-                           int nu_post, int coarse_sweeps, int *iters, double *res_out, cudaStream_t s);
+                           double eps, double omega, int ng, double eps0, int max_refine, int nu_fine_pre,
+                           int nu_fine_post, int nu_pre, int nu_post, int coarse_sweeps, int *iters,
+                           double *res_out, cudaStream_t s);
 
 // residency.cu: device mirrors of the drop-ins' host arrays
 bool residency_on();

@@ -54,7 +54,7 @@ struct XLev {
 struct XArgs {
   XLev L[XM_MAX + 1];
   int ng, ls;          // levels 1..ls on the grid, ls+1..ng in shared memory
-  int max_refine, nu_pre, nu_post, coarse_sweeps;
+  int max_refine, nu_fine_pre, nu_fine_post, nu_pre, nu_post, coarse_sweeps;  // sweeps: finest level, the others
   float omega;
   double aw, ae, an, as, at, ab, ac;  // FP64 finest coefficients
   double *u;
@@ -605,7 +605,7 @@ __global__ void __launch_bounds__(XM_BLOCK, 1) k_refine_mixed(const XArgs *__res
     // chip, grid levels up; the last smoothing of level 1 also applies
     // u += e (FP64)
     for (int l = 1; l <= ls && l < ng; ++l) {
-      g_smooth(a.L[l], a.omega, a.nu_pre, grid);
+      g_smooth(a.L[l], a.omega, l == 1 ? a.nu_fine_pre : a.nu_pre, grid);
       g_restrict(a.L[l], a.L[l + 1], grid);
     }
     bool added = false;
@@ -618,8 +618,9 @@ __global__ void __launch_bounds__(XM_BLOCK, 1) k_refine_mixed(const XArgs *__res
     }
     for (int l = (ls < ng ? ls : ng - 1); l >= 1; --l) {
       g_prolong(a.L[l], a.L[l + 1], grid);
-      const bool fin = l == 1 && a.nu_post > 0;
-      g_smooth(a.L[l], a.omega, a.nu_post, grid, fin ? a.u : nullptr);
+      const int nu = l == 1 ? a.nu_fine_post : a.nu_post;
+      const bool fin = l == 1 && nu > 0;
+      g_smooth(a.L[l], a.omega, nu, grid, fin ? a.u : nullptr);
       added = added || fin;
     }
     if (!added) {
@@ -642,8 +643,9 @@ size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 }  // namespace
 
 int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const double *b, const int *bcnd,
-                           double eps, double omega, int ng, double eps0, int max_refine, int nu_pre,
-                           int nu_post, int coarse_sweeps, int *iters, double *res_out, cudaStream_t s) {
+                           double eps, double omega, int ng, double eps0, int max_refine, int nu_fine_pre,
+                           int nu_fine_post, int nu_pre, int nu_post, int coarse_sweeps, int *iters,
+                           double *res_out, cudaStream_t s) {
   if (ng < 1 || ng > XM_MAX) return LEPIC_ERR_ARG;
   const int n[3] = {d.n1, d.n2, d.n3};
   for (int q = 0; q < 3; ++q)
@@ -653,6 +655,8 @@ int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const do
   memset(&A, 0, sizeof(A));
   A.ng = ng;
   A.max_refine = max_refine;
+  A.nu_fine_pre = nu_fine_pre;
+  A.nu_fine_post = nu_fine_post;
   A.nu_pre = nu_pre;
   A.nu_post = nu_post;
   A.coarse_sweeps = coarse_sweeps;
@@ -746,11 +750,13 @@ int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const do
 
 extern "C" int lepic_dev_pdesolver_mixed(const lepic_grid_t *g, double *u, const double *b, double eps,
                                          double omega, int ng, const lepic_phys_t *P, int max_refine,
-                                         int nu_pre, int nu_post, int coarse_sweeps, int *iters,
-                                         double *res, void *stream) {
+                                         int nu_fine_pre, int nu_fine_post, int nu_pre, int nu_post,
+                                         int coarse_sweeps, int *iters, double *res, void *stream) {
   if (!g || !P) return LEPIC_ERR_ARG;
   if (P->flag_pbc || P->flag_nmn) return LEPIC_ERR_UNSUPPORTED;
+  if (nu_fine_pre < 0 || nu_fine_post < 0 || nu_pre < 0 || nu_post < 0 || coarse_sweeps < 0 || max_refine < 0)
+    return LEPIC_ERR_ARG;
   return lepic::launch_pdesolver_mixed(lepic::Dims(g->n), g->h, u, b, g->bcnd, eps, omega, ng, P->eps0,
-                                       max_refine, nu_pre, nu_post, coarse_sweeps, iters, res,
-                                       (cudaStream_t)stream);
+                                       max_refine, nu_fine_pre, nu_fine_post, nu_pre, nu_post, coarse_sweeps,
+                                       iters, res, (cudaStream_t)stream);
 }

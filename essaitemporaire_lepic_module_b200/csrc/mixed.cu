@@ -46,11 +46,6 @@ constexpr int FLUSH_PARTICLES = 2048;      // node sums <= 2048 * 2^20 = 2^31
 static_assert(FLUSH_PARTICLES % CHUNK == 0, "flush windows are whole chunks");
 constexpr int CB = LEPIC_CELL_BITS, CM = LEPIC_CELL_MAX - 1;
 
-__device__ __forceinline__ unsigned lmask_le() {
-  unsigned m;
-  asm("mov.u32 %0, %%lanemask_le;" : "=r"(m));
-  return m;
-}
 __device__ __forceinline__ unsigned lmask_lt() {
   unsigned m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -491,28 +486,6 @@ __device__ __forceinline__ int tile_key(int cc, int ntx, int nty) {
   return tile * (TC * TC * TC) + (cx % TC) + TC * ((cy % TC) + TC * (cz % TC));
 }
 
-// run of equal keys among the lanes of the warp
-__device__ __forceinline__ void run_of(int key, bool &head, int &start, int &len) {
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const int prev = __shfl_up_sync(full, key, 1);
-  head = (lane == 0) || (prev != key);
-  const unsigned heads = __ballot_sync(full, head);
-  start = 31 - __clz(heads & lmask_le());
-  const unsigned above = (start == 31) ? 0u : (heads & ~((2u << start) - 1u));
-  len = (above ? __ffs(above) - 1 : 32) - start;
-}
-
-__global__ void k_msort_hist(const int *__restrict__ cell, const int *__restrict__ count, int ntx, int nty,
-                             int *cnt) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int k = (i < *count) ? tile_key(cell[i], ntx, nty) : -1;
-  bool head;
-  int start, len;
-  run_of(k, head, start, len);
-  if (head && k >= 0) atomicAdd(&cnt[k], len);
-}
-
 __global__ void k_tile_offsets(const int *__restrict__ off, int ntiles, int *__restrict__ tile_off) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t <= ntiles) tile_off[t] = off[(long long)t * (TC * TC * TC)];
@@ -546,15 +519,24 @@ __global__ void __launch_bounds__(SC_T, 4) k_msort_scatter(const int *__restrict
     hcnt[q] = 0;
   }
   __syncthreads();
+  // every load of the chunk first (cells and the six planes), so that their
+  // latency overlaps the grouping and the cursor atomics
   int cc[SC_U], slot[SC_U], rank[SC_U];
+  float pv[SC_U][6];
+#pragma unroll
+  for (int u = 0; u < SC_U; ++u) {
+    const long long idx = c0 + u * SC_T + t;
+    const bool in = idx < N;
+    cc[u] = in ? cell[idx] : 0;
+#pragma unroll
+    for (int a = 0; a < 6; ++a) pv[u][a] = in ? p[a * cap + idx] : 0.f;
+  }
 #pragma unroll
   for (int u = 0; u < SC_U; ++u) {
     const long long idx = c0 + u * SC_T + t;
     slot[u] = -1;
-    cc[u] = 0;
     rank[u] = 0;
     if (idx < N) {
-      cc[u] = cell[idx];
       const int key = tile_key(cc[u], ntx, nty);
       unsigned h = ((unsigned)key * 2654435761u) >> (32 - SC_HBITS);
       // at most SC_N distinct keys per chunk: a free or matching slot exists
@@ -600,12 +582,11 @@ __global__ void __launch_bounds__(SC_T, 4) k_msort_scatter(const int *__restrict
 #pragma unroll
   for (int u = 0; u < SC_U; ++u) {
     if (slot[u] < 0) continue;
-    const long long idx = c0 + u * SC_T + t;
     const int lpos = hoff[slot[u]] + rank[u];
     sdest[lpos] = hbase[slot[u]] + rank[u];
     scell[lpos] = cc[u];
 #pragma unroll
-    for (int a = 0; a < 6; ++a) sp[a * SC_N + lpos] = p[a * cap + idx];
+    for (int a = 0; a < 6; ++a) sp[a * SC_N + lpos] = pv[u][a];
   }
   __syncthreads();
   const int nv = N - c0 < SC_N ? (int)(N - c0) : SC_N;
@@ -615,6 +596,45 @@ __global__ void __launch_bounds__(SC_T, 4) k_msort_scatter(const int *__restrict
 #pragma unroll
     for (int a = 0; a < 6; ++a) p_o[a * cap + dst] = sp[a * SC_N + lp];
   }
+}
+
+// Counts per key of the counting sort, one block per chunk of SC_N
+// particles: the chunk's keys are counted in a shared-memory table (open
+// addressing) and each distinct key adds its count to the global histogram
+// once, instead of one atomic per warp run.
+__global__ void __launch_bounds__(SC_T) k_msort_hist(const int *__restrict__ cell, const int *__restrict__ count,
+                                                     int ntx, int nty, int *__restrict__ cnt) {
+  __shared__ int hkey[SC_H], hcnt[SC_H];
+  const int t = threadIdx.x;
+  const long long N = *count;
+  const long long c0 = (long long)blockIdx.x * SC_N;
+  if (c0 >= N) return;  // uniform over the block
+  for (int q = t; q < SC_H; q += SC_T) {
+    hkey[q] = -1;
+    hcnt[q] = 0;
+  }
+  int key[SC_U];
+#pragma unroll
+  for (int u = 0; u < SC_U; ++u) {
+    const long long idx = c0 + u * SC_T + t;
+    key[u] = idx < N ? cell[idx] : -1;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < SC_U; ++u) {
+    if (key[u] < 0) continue;
+    const int k = tile_key(key[u], ntx, nty);
+    unsigned h = ((unsigned)k * 2654435761u) >> (32 - SC_HBITS);
+    for (int probe = 0; probe < SC_H; ++probe) {
+      const int prev = atomicCAS(&hkey[h], -1, k);
+      if (prev == -1 || prev == k) break;
+      h = (h + 1) & (SC_H - 1);
+    }
+    atomicAdd(&hcnt[h], 1);
+  }
+  __syncthreads();
+  for (int q = t; q < SC_H; q += SC_T)
+    if (hcnt[q]) atomicAdd(&cnt[hkey[q]], hcnt[q]);
 }
 
 // E (3, nodes) FP64 -> one float4 (Ex, Ey, Ez, 0) per node
@@ -834,7 +854,7 @@ int launch_sort_mixed(const lepic_grid_t &g, lepic_species_mixed_t &sp, int n_hi
   LEPIC_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(nkeys + 1), s));
   const int nthreads = n_hint > 0 ? n_hint : sp.cap;
   int t0 = timer_start("sort_hist_mixed", s);
-  k_msort_hist<<<grid_for(nthreads, MBK), MBK, 0, s>>>(sp.cell, sp.count, ntx, nty, cnt);
+  k_msort_hist<<<grid_for(nthreads, SC_N), SC_T, 0, s>>>(sp.cell, sp.count, ntx, nty, cnt);
   timer_stop(t0, s);
   int t1 = timer_start("sort_scan_mixed", s);
   int rc = exclusive_scan_i32(cnt, cnt, nkeys + 1, s);

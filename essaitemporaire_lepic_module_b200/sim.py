@@ -162,9 +162,13 @@ class Simulation:
         self.fused = fused or self.mixed
         # FP32 V-cycle parameters of the mixed Poisson solve: over-relaxed
         # red-black smoothing (omega 1.3) reduces the smooth error modes that
-        # the L1 residual test hardly sees; at the workloads' tolerance phi
-        # lands within ~1e-9 of the converged FP64 solution in 4-5 refinements
-        self.mg_mixed = dict(max_refine=60, nu_pre=2, nu_post=2, coarse_sweeps=4, omega=1.3)
+        # the L1 residual test hardly sees; one pre- and three post-sweeps on
+        # the finest level (its sweeps are the dearest, the last one also
+        # accumulates u), two and two on the coarser levels; at the workloads'
+        # tolerance phi lands within ~1e-8 of the converged FP64 solution in
+        # 4-5 refinements
+        self.mg_mixed = dict(max_refine=60, nu_fine_pre=1, nu_fine_post=3, nu_pre=2, nu_post=2,
+                             coarse_sweeps=4, omega=1.3)
         if mg_mixed:
             self.mg_mixed.update(mg_mixed)
         self._acc = None
@@ -340,8 +344,9 @@ class Simulation:
         check(lib().lepic_dev_pdesolver_mixed(C.byref(self.grid), _ptr(self.phi), _ptr(self.rhs),
                                               wl.eps if eps is None else eps, m["omega"],
                                               self.st.ng if ng is None else ng, C.byref(self.P),
-                                              m["max_refine"], m["nu_pre"], m["nu_post"],
-                                              m["coarse_sweeps"], C.byref(it), C.byref(res),
+                                              m["max_refine"], m["nu_fine_pre"], m["nu_fine_post"],
+                                              m["nu_pre"], m["nu_post"], m["coarse_sweeps"],
+                                              C.byref(it), C.byref(res),
                                               self._s()), "pdesolver_mixed")
         self.mg_last = (it.value, 0.0, res.value)
         return self.mg_last

@@ -379,15 +379,16 @@ int lepic_dev_mixed_to_f64(const lepic_grid_t *g, const lepic_species_mixed_t *i
                            long long capout, long long n, void *stream);
 /* Mixed-precision Poisson solve for the operator of Src/pdesolver.f90:1
  * (Dirichlet walls): FP64 residual r = b - A u, FP32 multigrid V-cycle on
- * A e = r (nu_pre / nu_post red-black sweeps per level, coarse_sweeps on the
- * coarsest), u += e in FP64, until sum|r| / alpha < eps, with the sum over
- * plasma nodes and the alpha of the reference's exit test (or max_refine
- * refinements).  One cooperative launch.  iters: refinements done; res: the
- * final sum|r| / alpha. */
+ * A e = r (red-black sweeps: nu_fine_pre / nu_fine_post on the finest level,
+ * nu_pre / nu_post on the coarser ones, coarse_sweeps on the coarsest), u += e
+ * in FP64, until sum|r| / alpha < eps, with the sum over plasma nodes and the
+ * alpha of the reference's exit test (or max_refine refinements).  One
+ * cooperative launch.  iters: refinements done; res: the final
+ * sum|r| / alpha. */
 int lepic_dev_pdesolver_mixed(const lepic_grid_t *g, double *u, const double *b, double eps,
                               double omega, int ng, const lepic_phys_t *P, int max_refine,
-                              int nu_pre, int nu_post, int coarse_sweeps, int *iters, double *res,
-                              void *stream);
+                              int nu_fine_pre, int nu_fine_post, int nu_pre, int nu_post,
+                              int coarse_sweeps, int *iters, double *res, void *stream);
 /* lepic_dev_collisions for species in the mixed layout (same physics; the
  * post-collision velocities are stored in FP32). */
 int lepic_dev_collisions_mixed(const lepic_grid_t *g, lepic_species_mixed_t *sp, int ntype,
