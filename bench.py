@@ -460,6 +460,28 @@ def run_dropin(workload, steps=4, warm=1):
     return out
 
 
+def run_profile_step(args):
+    """One step bracketed by cudaProfilerStart/Stop for `ncu --profile-from-start off`
+    (the steps before it run unprofiled): step `--profile-step` of the workload in
+    the form `--precision` (f64 or mixed)."""
+    import torch
+    from essaitemporaire_lepic_module_b200 import config
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    st = config.build(args.workload)
+    form = "mixed" if args.precision == "both" else args.precision
+    sim = Simulation(st, precision=form, sort_policy=args.sort_policy)
+    sim.load_uniform()
+    for _ in range(args.profile_step - 1):
+        sim.step()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    sim.step()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profiled_step": sim.it, "form": form, "workload": args.workload,
+                      "particles": [s.n() for s in sim.sp]}), flush=True)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -574,8 +596,12 @@ def main():
                     help="skip the drop-in (Fortran-signature) loop, per-call copies vs resident")
     ap.add_argument("--dropin-workload", default="mcc64")
     ap.add_argument("--dropin-steps", type=int, default=10)
+    ap.add_argument("--profile-step", type=int, default=0,
+                    help="run only up to this step, the last one between cudaProfilerStart/Stop (for ncu)")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile_step > 0:
+        run_profile_step(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
