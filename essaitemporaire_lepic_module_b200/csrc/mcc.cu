@@ -192,24 +192,30 @@ __global__ void __launch_bounds__(MB) k_mcc_select(MCCConst c, const int *__rest
 }
 
 // pass 1 for small Pmax: the same Bernoulli(Pmax) sample of the particle
-// indices drawn by geometric skipping.  Within each segment of SKIP_SEG
+// indices drawn by geometric skipping.  Within each segment of `seg`
 // particles the gaps between successive candidates are independent
 // geometric variables, floor(ln U / ln(1 - Pmax)), so one uniform per
 // candidate replaces one per particle.  The draws use Philox counters
 // (segment, 16 + k) that the per-particle streams (particle, 0..2) of the
-// collision pass never use.
-constexpr int SKIP_SEG = 2048;
+// collision pass never use.  The segment is sized for about four candidates
+// per thread (a short serial chain, few threads when Pmax is tiny).
 constexpr double SKIP_PMAX = 0.25;  // above it: one draw per particle
 
+int skip_segment(double Pmax) {
+  int seg = 256;
+  while (seg < 65536 && seg * Pmax < 4.0) seg *= 2;
+  return seg;
+}
+
 __global__ void __launch_bounds__(MB) k_mcc_select_skip(MCCConst c, const int *__restrict__ count,
-                                                        double inv_log1m, int *__restrict__ cand,
+                                                        double inv_log1m, int seg_len, int *__restrict__ cand,
                                                         int *__restrict__ ncand) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const long long seg = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long N = *count;
-  const long long lo = seg * SKIP_SEG;
-  const long long hi = lo + SKIP_SEG < N ? lo + SKIP_SEG : N;
+  const long long lo = seg * seg_len;
+  const long long hi = lo + seg_len < N ? lo + seg_len : N;
   long long pos = lo - 1;
   bool live = lo < hi;
   uint32_t draw = 0;
@@ -229,7 +235,7 @@ __global__ void __launch_bounds__(MB) k_mcc_select_skip(MCCConst c, const int *_
       r.z = r.w;
       --left;
       const double gap = floor(log(u01(v)) * inv_log1m);
-      pos = gap < (double)SKIP_SEG ? pos + 1 + (long long)gap : hi;
+      pos = gap < (double)seg_len ? pos + 1 + (long long)gap : hi;
       if (pos < hi) pick = pos;
       else live = false;
     }
@@ -490,8 +496,9 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
     snprintf(sname, sizeof sname, "%s_select", tname);
     int tm = timer_start(sname, s);
     if (Pmax < SKIP_PMAX) {
-      const long long nseg = (Nh[p - 1] + SKIP_SEG - 1) / SKIP_SEG;
-      k_mcc_select_skip<<<grid_for(nseg, MB), MB, 0, s>>>(c, counts_dev[p - 1], 1.0 / log1p(-Pmax), cand,
+      const int seg = skip_segment(Pmax);
+      const long long nseg = (Nh[p - 1] + seg - 1) / seg;
+      k_mcc_select_skip<<<grid_for(nseg, MB), MB, 0, s>>>(c, counts_dev[p - 1], 1.0 / log1p(-Pmax), seg, cand,
                                                           ncand + (p - 1));
     } else {
       k_mcc_select<<<grid_for(Nh[p - 1], MB), MB, 0, s>>>(c, counts_dev[p - 1], cand, ncand + (p - 1));
