@@ -485,6 +485,54 @@ class Simulation:
             self.move()
             self.deposit()
 
+    def step_host(self, potentials=None, phi_out=None, counts_out=None):
+        """One step with host input and output, pipelined.  `potentials`
+        (FP64, one value per wall label 0..ngrid+1, pinned host memory) are
+        copied in and set on the wall nodes before the step; after it phi and
+        the particle counts are snapshotted on the device and copied into the
+        pinned host tensors `phi_out` (the shape of the node grid) and
+        `counts_out` (one int32 per species) on a separate copy stream, so
+        the copy overlaps the next step.  Returns the CUDA event after which
+        `phi_out` and `counts_out` hold this step's values (and may be
+        reused); two steps may be in flight."""
+        if potentials is not None:
+            if getattr(self, "_wall", None) is None:
+                nl = int(self.st.geom.ngrid)
+                self._label = self.bcnd.long().clamp(0, nl + 1)
+                self._wall = self.bcnd >= 1
+            v = potentials.to(self.dev, non_blocking=True)
+            torch.where(self._wall, v[self._label], self.phi, out=self.phi)
+        self.step()
+        done = torch.cuda.Event()
+        if phi_out is None and counts_out is None:
+            done.record(self.stream)
+            return done
+        if getattr(self, "_io", None) is None:
+            self._io = [(torch.empty_like(self.phi), torch.empty(len(self.sp), dtype=torch.int32, device=self.dev),
+                         None) for _ in range(2)]
+            self._io_slot = 0
+            self._copy_stream = torch.cuda.Stream(self.dev)
+        slot = self._io_slot
+        self._io_slot ^= 1
+        snap_phi, snap_cnt, prev = self._io[slot]
+        if prev is not None:
+            self.stream.wait_event(prev)  # the copy of two steps ago has read this snapshot
+        snap_phi.copy_(self.phi)
+        torch.cat([sp.count for sp in self.sp], out=snap_cnt)
+        ready = torch.cuda.Event()
+        ready.record(self.stream)
+        self._copy_stream.wait_event(ready)
+        with torch.cuda.stream(self._copy_stream):
+            if phi_out is not None:
+                phi_out.copy_(snap_phi, non_blocking=True)
+            if counts_out is not None:
+                counts_out.copy_(snap_cnt, non_blocking=True)
+            done.record(self._copy_stream)
+        snap_phi.record_stream(self._copy_stream)
+        snap_cnt.record_stream(self._copy_stream)
+        self._io[slot] = (snap_phi, snap_cnt, done)
+        return done
+
     def _hint(self, s):
         return int(s.count.item())
 
