@@ -113,10 +113,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(workload, steps=10, ppc=4):
+def cpu_baseline(workload, steps=10, ppc=4, warmup=0):
     """The CPU FP64 oracle on a bounded sample: the workload's grid with
-    `ppc` particles per cell and species, steps it=2..steps+1 (one sort and
-    one MCC call per 10 steps, the reference cadence)."""
+    `ppc` particles per cell and species, `warmup` untimed steps, then
+    `steps` timed ones (one sort and one MCC call per 10 steps, the
+    reference cadence)."""
     import oracle
     from essaitemporaire_lepic_module_b200 import config
     wl = config.workload(workload)
@@ -126,27 +127,32 @@ def cpu_baseline(workload, steps=10, ppc=4):
     S = oracle.load_part(st, nmax=int(st.n_particles() * 1.3) + 1024)
     phi = st.geom.phi.copy()
     Ei = np.zeros(tuple(st.geom.bcnd.shape) + (3,))
+    for it in range(2, warmup + 2):
+        Ei, _, _ = oracle.step(st, S, phi, Ei, it)
+    first = warmup + 2
     ntot = 0
     t0 = time.perf_counter()
-    for it in range(2, steps + 2):
+    for it in range(first, first + steps):
         ntot += int(S.np_tot.sum())
         Ei, _, _ = oracle.step(st, S, phi, Ei, it)
     dt = time.perf_counter() - t0
-    nsort = sum(1 for it in range(2, steps + 2) if it % 10 == 1)
+    nsort = sum(1 for it in range(first, first + steps) if it % 10 == 1)
     ncoll = nsort if st.tables is not None else 0
-    return {"value": ntot / dt, "unit": UNIT, "cores": threads, "kind": "port",
+    return {"value": ntot / dt, "unit": UNIT, "cores": threads, "kind": "port", "ms_per_step": 1e3 * dt / steps,
             "sample": f"{workload} grid {st.n}, {ppc} ppc/species ({st.n_particles()} per species), "
-                      f"{steps} steps it=2..{steps + 1} incl. {nsort} sort(s) + {ncoll} MCC call(s), {dt:.1f} s"}
+                      f"{steps} timed steps it={first}..{first + steps - 1} after {warmup} warm-up, incl. {nsort} "
+                      f"sort(s) + {ncoll} MCC call(s), {dt:.1f} s"}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cb = cpu_baseline(args.workload, steps=args.cpu_steps, ppc=args.cpu_ppc)
+    # the driver's --steps / --warmup, each step a bounded sample (cpu_ppc particles per cell)
+    cb = cpu_baseline(args.workload, steps=args.steps, ppc=args.cpu_ppc, warmup=args.warmup)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
-            "n_gpus": args.gpus, "steps": args.cpu_steps, "warmup": 0,
-            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, "sample": cb["sample"]},
             "cpu_baseline": cb,
