@@ -331,3 +331,39 @@ def test_step_host_pipelined_io():
     for k, ph in got:
         assert np.abs(ph - ref_phi[k]).max() <= 1e-12 * scale, k
     assert np.array_equal(cnts.numpy(), np.array(ref_cnt))
+
+
+def test_mcc_moments_vs_oracle(mcc32):
+    """Ten steps with MCC every step from the same particles, the oracle
+    (serial ran2 picks) against the GPU FP64 step (Philox null collisions):
+    per species the population, the mean kinetic energy and the mean position
+    within 3 sigma of the sampling error (sigma of a mean: std / sqrt(N) of
+    both runs; population: the square root of the particles each run created
+    or lost)."""
+    import os
+    from essaitemporaire_lepic_module_b200.constants import QE
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    st, S0 = mcc32
+    oracle.set_threads(os.cpu_count() or 1)
+    S = S0.copy()
+    sim = Simulation(st, cap=S.vxp.shape[1], seed=777, ns_coll=1)
+    sim.load_from_host(S.vxp, S.np_tot, S.np)
+    phi = st.geom.phi.copy()
+    Ei = np.zeros(tuple(st.geom.bcnd.shape) + (3,))
+    for it in range(1, 11):
+        Ei, _, _ = oracle.step(st, S, phi, Ei, it, ns_coll=1)
+        sim.step()
+    oracle.set_threads(1)
+    for p in range(st.ntype):
+        g = sim.sp[p].to_vxp()
+        o = S.vxp[p, :S.np_tot[p]]
+        n0 = S0.np_tot[p]
+        dn = abs(len(g) - len(o))
+        assert dn <= 3.0 * np.sqrt(abs(len(g) - n0) + abs(len(o) - n0) + 1.0), (p, len(g), len(o), n0)
+        m = abs(st.mass[p])
+        eg = 0.5 * m * (g[:, 3:6] ** 2).sum(axis=1) / QE
+        eo = 0.5 * m * (o[:, 3:6] ** 2).sum(axis=1) / QE
+        qs = [(eg, eo)] + [(g[:, c], o[:, c]) for c in range(3)]
+        for a, b in qs:
+            sig = np.sqrt(a.var() / len(a) + b.var() / len(b))
+            assert abs(a.mean() - b.mean()) <= 3.0 * sig, (p, a.mean(), b.mean(), sig)

@@ -122,6 +122,31 @@ def test_boris_gyration_phase_and_radius():
     assert abs(math.hypot(vx, vy) - v0) < 1e-9 * v0
 
 
+def test_boris_exb_drift():
+    """One electron in uniform Ex and Bz starting at the E x B drift velocity
+    (0, -Ex/Bz, 0): the Boris step keeps it there (the rotation of the drift-
+    frame velocity zero is zero) and the particle moves by v_d dt per step."""
+    st = config.build("penning_small")
+    nmax = 4
+    S = oracle.State(st, nmax)
+    L = st.geom.box
+    Ex, Bz = 1e3, st.Bconst[2]
+    vd = -Ex / Bz
+    y0 = L[1] / 2
+    S.vxp[0, 0] = [L[0] / 2, y0, L[2] / 2, 0.0, vd, 0.0]
+    S.np_tot[0] = 1
+    Ei = np.zeros(tuple(st.geom.bcnd.shape) + (3,))
+    Ei[..., 0] = Ex
+    ng1 = st.geom.ngrid + 1
+    steps = 50
+    for _ in range(steps):
+        oracle.part_mover(st, Ei, S, np.zeros((ng1, 2, 1)), np.zeros((1, 4)), 1)
+    vx, vy, vz = S.vxp[0, 0, 3:6]
+    assert abs(vx) <= 1e-9 * abs(vd) and abs(vz) <= 1e-9 * abs(vd)
+    assert abs(vy - vd) <= 1e-9 * abs(vd)
+    assert abs((S.vxp[0, 0, 1] - y0) - steps * st.dt * vd) <= 1e-9 * abs(steps * st.dt * vd)
+
+
 def test_cic_charge_conservation_and_sort_invariants():
     """Sum over nodes of np/kq * h^3 equals N Nm; the counting sort is a
     permutation, Plist is the inclusive cumulative cell count, keys ascend."""
