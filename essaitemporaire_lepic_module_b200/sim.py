@@ -300,6 +300,26 @@ class Simulation:
                                            self._s()), "load_uniform")
         self._deposit_f64(self.sp)
 
+    def save_bak(self, path, time=0.0):
+        """Particle backup in the reference's DATA.BAK/particlesNNN.bak format
+        (Src/main.f90:1294-1330): time, np_tot and every species' vxp."""
+        from .checkpoint import write_particles_bak
+        arrs = [self.particles_f64(p).t().contiguous().cpu().numpy() for p in range(len(self.sp))]
+        write_particles_bak(path, time, [a.shape[0] for a in arrs], arrs)
+
+    def load_bak(self, path):
+        """Restart from a particle backup of the reference's format
+        (Src/restart.f90:62-70, one process): particles loaded, density
+        deposited; returns the backup's time."""
+        from .checkpoint import read_particles_bak
+        time, npt, arrs, _ = read_particles_bak(path, len(self.sp))
+        nmax = max(1, int(npt.max()))
+        vxp = np.zeros((len(self.sp), nmax, 6))
+        for p, a in enumerate(arrs):
+            vxp[p, :len(a)] = a
+        self.load_from_host(vxp, npt[:, 0])
+        return time
+
     def particles_f64(self, p):
         """Species p as FP64 (6, n) x, y, z, vx, vy, vz on the device."""
         s = self.sp[p]
