@@ -257,6 +257,13 @@ const char *lepic_build_info(void) {
   return buf;
 }
 
+int lepic_dev_check(void *stream, int *detail) {
+  Ctx &c = ctx();
+  const int rc = check_err(S(stream));
+  if (detail) *detail = rc ? c.h_err[1] : 0;
+  return rc;
+}
+
 int lepic_dev_info(int *sm_count, char *name, int name_len) {
   Ctx &c = ctx();
   if (sm_count) *sm_count = c.sms;

@@ -393,10 +393,17 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, const int
   }
 }
 
-__global__ void k_mcc_finalize(int *count0, int *count1, int *count2, const int *add, int ntype) {
+// the appended products enter the counts; appends beyond the capacity were
+// not written (LEPIC_ERR_CAPACITY is raised), so a count stops at its capacity
+__global__ void k_mcc_finalize(int *count0, int *count1, int *count2, const int *add, int ntype, long long cap0,
+                               long long cap1, long long cap2) {
   int *cs[3] = {count0, count1, count2};
+  const long long caps[3] = {cap0, cap1, cap2};
   for (int p = 0; p < ntype && p < 3; ++p)
-    if (cs[p]) *cs[p] += add[p];
+    if (cs[p]) {
+      const long long v = (long long)*cs[p] + add[p];
+      *cs[p] = (int)(v < caps[p] ? v : caps[p]);
+    }
 }
 
 // Host part shared by both layouts: nu_max, Pmax and the per-species
@@ -511,7 +518,8 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
     LEPIC_CUDA(cudaGetLastError());
   }
   k_mcc_finalize<<<1, 1, 0, s>>>(counts_dev[0], ntype > 1 ? counts_dev[1] : nullptr,
-                                 ntype > 2 ? counts_dev[2] : nullptr, add, ntype);
+                                 ntype > 2 ? counts_dev[2] : nullptr, add, ntype, S.cap[0],
+                                 ntype > 1 ? S.cap[1] : 0, ntype > 2 ? S.cap[2] : 0);
   LEPIC_CUDA(cudaGetLastError());
   unsigned long long hc[64];
   LEPIC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, s));

@@ -153,7 +153,8 @@ class Simulation:
     deposition and every rank solves the same field."""
 
     def __init__(self, st, cap=None, device="cuda", seed=123456, nsort=None, ns_coll=None,
-                 fused=True, precision="f64", mg_mixed=None, comm=None, sort_policy="reference"):
+                 fused=True, precision="f64", mg_mixed=None, comm=None, sort_policy="reference",
+                 check_every=1):
         if precision not in ("f64", "mixed"):
             raise ValueError(f"precision must be 'f64' or 'mixed', not {precision!r}")
         self.st = st
@@ -178,6 +179,10 @@ class Simulation:
         self.ns_coll = st.wl.ns_coll if ns_coll is None else ns_coll
         self.sort_every = sort_intervals(st, self.nsort, sort_policy)
         self.sort_policy = sort_policy
+        # steps between reads of the device error word (0: never); a kernel
+        # that met a bad cell, a full particle array or a collision-table
+        # overflow raises LepicError at the next read
+        self.check_every = int(check_every)
         self.seed = int(seed)
         self.P = phys_struct(st)
         self.comm = comm
@@ -504,6 +509,16 @@ class Simulation:
         else:
             self.move()
             self.deposit()
+        if self.check_every and it % self.check_every == 0:
+            self.check_device()
+
+    def check_device(self):
+        """Read and clear the device error word; raise LepicError when a
+        kernel recorded a status since the last read."""
+        detail = C.c_int(0)
+        rc = lib().lepic_dev_check(self._s(), C.byref(detail))
+        if rc:
+            check(rc, f"device status after step {self.it} (detail {detail.value})")
 
     def step_host(self, potentials=None, phi_out=None, counts_out=None):
         """One step with host input and output, pipelined.  `potentials`

@@ -479,6 +479,14 @@ int lepic_timing_read(char *buf, int buflen, double *ms, long long *launches, in
 
 /* Number of SMs, device name; 0 on success. */
 int lepic_dev_info(int *sm_count, char *name, int name_len);
+/* Status of the kernels launched so far: synchronises `stream`, returns the
+ * first status a kernel recorded in the device error word since the last
+ * check (0 = none) and clears it; detail: the recorded particle index or
+ * value.  The device API's launch functions do not all wait for their
+ * kernels, so a step loop calls this once per step (as sim.Simulation
+ * does).  No counterpart in the reference (it stops the run in place,
+ * Src/utils.f90:529-546). */
+int lepic_dev_check(void *stream, int *detail);
 /* Library build identification (nvcc version, arch). */
 const char *lepic_build_info(void);
 
