@@ -279,22 +279,26 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
       if (fz >= 1.f) { fz = 0.f; szi += 1; }
     }
     int ax = ix + sx, ay = iy + syi, az = iz + szi;
-    if (c.flag_pbc == 1) {
-      if (ay > n2) ay -= n2;
-      if (ay < 1) ay += n2;
-      if (az > n3) az -= n3;
-      if (az < 1) az += n3;
-    }
-    const int cx = ax < 0 ? 0 : (ax > n1 + 1 ? n1 + 1 : ax);
-    const int cy = ay < 0 ? 0 : (ay > n2 + 1 ? n2 + 1 : ay);
-    const int cz = az < 0 ? 0 : (az > n3 + 1 ? n3 + 1 : az);
-    bool wall;
-    {
+    int cx = ax, cy = ay, cz = az;
+    bool lost = false;
+    if (sx | syi | szi) {
+      // a new cell: periodic wrap and the loss test (the cell a particle
+      // stays in passed the test when the particle entered it)
+      if (c.flag_pbc == 1) {
+        if (ay > n2) ay -= n2;
+        if (ay < 1) ay += n2;
+        if (az > n3) az -= n3;
+        if (az < 1) az += n3;
+      }
+      cx = ax < 0 ? 0 : (ax > n1 + 1 ? n1 + 1 : ax);
+      cy = ay < 0 ? 0 : (ay > n2 + 1 ? n2 + 1 : ay);
+      cz = az < 0 ? 0 : (az > n3 + 1 ? n3 + 1 : az);
       int lx, ly, lz;
-      wall = in_box(T, cx, cy, cz, lx, ly, lz) ? T.cw[lx + (TN - 1) * (ly + (TN - 1) * lz)] != 0
-                                                : cw[d.c(cx, cy, cz)] != 0;
+      const bool wall = in_box(T, cx, cy, cz, lx, ly, lz) ? T.cw[lx + (TN - 1) * (ly + (TN - 1) * lz)] != 0
+                                                          : cw[d.c(cx, cy, cz)] != 0;
+      lost = wall || ax < 1 || ax > n1 || ay < 1 || ay > n2 || az < 1 || az > n3;
     }
-    if (wall || ax < 1 || ax > n1 || ay < 1 || ay > n2 || az < 1 || az > n3) {
+    if (lost) {
       // lost at a wall (Src/part_expmover.f90:275-433): every cell outside
       // 1..n has only wall nodes in a closed box; a cell inside 1..n is lost
       // when all of its 8 nodes are walls
