@@ -33,7 +33,8 @@ class LepicPhys(C.Structure):
                 ("qe", C.c_double), ("eps0", C.c_double), ("pi", C.c_double),
                 ("flag_B", C.c_int), ("flag_B_pos", C.c_int), ("flag_pbc", C.c_int),
                 ("flag_nmn", C.c_int), ("ns_coll", C.c_int), ("n_cell", C.c_int),
-                ("np_cell", C.c_int), ("Bconst", C.c_double * 3)]
+                ("np_cell", C.c_int), ("Bconst", C.c_double * 3),
+                ("Bmap", C.c_void_p), ("n_B", C.c_int * 3), ("h_B", C.c_double * 3)]
 
 
 class LepicGrid(C.Structure):
@@ -263,8 +264,11 @@ def check(rc, where=""):
         raise LepicError(rc, where)
 
 
-def phys_struct(st, cls=LepicPhys):
-    """Fill a LepicPhys (or the oracle's OPhys, same layout) from a Setup."""
+def phys_struct(st, cls=LepicPhys, bmap_ptr=None):
+    """Fill a LepicPhys (or the oracle's OPhys, same layout) from a Setup.
+    With a B-field map (st.bfield) the map's pointer is ``bmap_ptr`` (a
+    device address for the device API); by default the host array's, which
+    only the CPU oracle may read."""
     from .constants import EPS0, PI, QE
     P = cls()
     P.ntype = st.ntype
@@ -281,7 +285,7 @@ def phys_struct(st, cls=LepicPhys):
     P.x_load = st.x_load
     P.qe, P.eps0, P.pi = QE, EPS0, PI
     P.flag_B = st.flag_B
-    P.flag_B_pos = 0
+    P.flag_B_pos = int(getattr(st, "flag_B_pos", 0))
     P.flag_pbc = st.geom.flag_pbc
     P.flag_nmn = st.geom.flag_nmn
     P.ns_coll = st.wl.ns_coll
@@ -289,6 +293,12 @@ def phys_struct(st, cls=LepicPhys):
     P.np_cell = st.np_cell
     for i in range(3):
         P.Bconst[i] = st.Bconst[i]
+    bf = getattr(st, "bfield", None)
+    if bf is not None:
+        for i in range(3):
+            P.n_B[i] = int(bf.n_B[i])
+            P.h_B[i] = float(bf.h_B[i])
+        P.Bmap = int(bmap_ptr) if bmap_ptr is not None else bf.Bi.ctypes.data
     return P
 
 

@@ -145,6 +145,8 @@ class Setup:
     ngas: float = 0.0
     rhs_blobs: np.ndarray = None    # Poisson-only source (-rho), (n3+2, n2+2, n1+2)
     extra: dict = field(default_factory=dict)
+    bfield: object = None           # bfield.BField (a B-field map) or None (uniform Bconst)
+    flag_B_pos: int = 0             # 1: positive ions not magnetised
 
     @property
     def ncells(self):

@@ -498,7 +498,8 @@ extern "C" {
 int lepic_dev_win_push(const lepic_grid_t *g, const double *Ei, double *p, int cap, int n, signed char *alive,
                        int ptype, const lepic_phys_t *P, void *stream) {
   if (!g || !Ei || !p || !alive || !P || ptype < 1 || n < 0 || n > cap) return LEPIC_ERR_ARG;
-  if (P->flag_pbc || P->flag_nmn) return LEPIC_ERR_UNSUPPORTED;
+  // the window differentiates a uniform B (dJ/dBz): no B-field map
+  if (P->flag_pbc || P->flag_nmn || (P->flag_B == 1 && P->Bmap)) return LEPIC_ERR_UNSUPPORTED;
   const Dims d(g->n);
   cudaStream_t s = (cudaStream_t)stream;
   if (n == 0) return LEPIC_OK;
@@ -530,6 +531,7 @@ int lepic_dev_adj_push(const lepic_grid_t *g, const double *Ei, const double *p,
   if (!g || !Ei || !p || !alive_before || !alive_after || !lam || !P || !lE || !dBz || ptype < 1 || n < 0 ||
       n > cap || n > lcap)
     return LEPIC_ERR_ARG;
+  if (P->flag_B == 1 && P->Bmap) return LEPIC_ERR_UNSUPPORTED;
   const Dims d(g->n);
   cudaStream_t s = (cudaStream_t)stream;
   if (n == 0) return LEPIC_OK;

@@ -445,22 +445,31 @@ void part_mover_(const int *n, const double *h, const double *Ei, const double *
   (void)sum_q_yz;
   (void)dtype;
   (void)iseed;
-  (void)h_B;
   if (*nproc != 1 || *iproc != 1) return record(LEPIC_ERR_UNSUPPORTED);
   if (part_info_int_.flag_die || part_info_int_.tag_neg == *ptype || part_info_dp_1_.gam_sec > 0.0)
     return record(LEPIC_ERR_UNSUPPORTED);
   lepic_phys_t P = phys_from_common(*ntype);
-  if (P.flag_B == 1) {
-    if (n_B[0] != 1) return record(LEPIC_ERR_UNSUPPORTED);  // B-field maps
-    // Bi(1:3,1,1,1) of Bi(4,0:n_B(1)+2,0:n_B(2)+2,0:n_B(3)+2)
-    long long e1 = 4, e2 = 4LL * (n_B[0] + 3), e3 = 4LL * (n_B[0] + 3) * (n_B[1] + 3);
-    for (int c = 0; c < 3; ++c) P.Bconst[c] = Bi[c + e1 + e2 + e3];
-  }
   cudaStream_t s = 0;
   Dims d(n);
   lepic_grid_t g;
   int rc = stage_grid(g, n, h, bcnd, nullptr, s);
   if (rc) return record(rc);
+  if (P.flag_B == 1) {
+    // Bi(4,0:n_B(1)+2,0:n_B(2)+2,0:n_B(3)+2): Bi(1:3,1,1,1) is the uniform
+    // field when n_B(1) = 1, else the whole array is the map
+    const long long e1 = 4, e2 = 4LL * (n_B[0] + 3), e3 = 4LL * (n_B[0] + 3) * (n_B[1] + 3);
+    if (n_B[0] == 1) {
+      for (int c = 0; c < 3; ++c) P.Bconst[c] = Bi[c + e1 + e2 + e3];
+    } else {
+      const size_t nb = 4 * (size_t)(n_B[0] + 3) * (n_B[1] + 3) * (n_B[2] + 3);
+      P.Bmap = dev_view("dropin_Bi", Bi, nb, READ, s, &rc);
+      if (!P.Bmap) return record(rc);
+      for (int c = 0; c < 3; ++c) {
+        P.n_B[c] = n_B[c];
+        P.h_B[c] = h_B[c];
+      }
+    }
+  }
   const int p = *ptype - 1;
   double *vxp_p = vxp + 6LL * *nmax * p;
   signed char *fd_p = flag_dead + (long long)*nmax * p;

@@ -83,6 +83,88 @@ __host__ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t
 // uniform in (0,1) from 32 random bits
 __host__ __device__ __forceinline__ double u01(uint32_t v) { return ((double)v + 0.5) * 2.3283064365386963e-10; }
 
+// ------------------------------------------------------------ B-field map
+// The push's B-field map (Src/part_expmover.f90:148-203):
+// Bi(4, 0:nB1+2, 0:nB2+2, 0:nB3+2), component fastest, Bi(4,...) = |B|.
+struct BMapF64 {
+  const double *B;        // nullptr: uniform field
+  int own;                // 1: own grid (flag_gridB = 1): index and weights from h_B
+  int nb1, nb2, nb3;      // n_B
+  long long N1, N2;       // nB1 + 3, nB2 + 3
+  double h0, h1, h2;      // h_B
+};
+
+// validated map of P for a push on the node grid n; LEPIC_OK also when P has
+// no map (m.B = nullptr)
+inline int bmap_from_phys(const lepic_phys_t &P, const int n[3], BMapF64 &m) {
+  m = BMapF64{};
+  if (P.flag_B != 1 || !P.Bmap) return LEPIC_OK;
+  if (P.n_B[0] < 2 || P.n_B[1] < 1 || P.n_B[2] < 1) return LEPIC_ERR_ARG;
+  m.B = P.Bmap;
+  m.nb1 = P.n_B[0];
+  m.nb2 = P.n_B[1];
+  m.nb3 = P.n_B[2];
+  m.N1 = m.nb1 + 3;
+  m.N2 = m.nb2 + 3;
+  m.own = (m.nb1 != n[0] || m.nb2 != n[1] || m.nb3 != n[2]) ? 1 : 0;
+  m.h0 = P.h_B[0];
+  m.h1 = P.h_B[1];
+  m.h2 = P.h_B[2];
+  if (m.own && !(m.h0 > 0.0 && m.h1 > 0.0 && m.h2 > 0.0)) return LEPIC_ERR_ARG;
+  return LEPIC_OK;
+}
+
+// B at a particle at (xp, yp, zp) whose E gather used cell (ix, iy, iz) and
+// weights k[0..7], in the reference's expression order (FP64 files are built
+// without FMA contraction, so this reproduces the oracle bit for bit).
+// Returns false when |B| at the left map node is not above 1e-5 T: the
+// particle then takes the leapfrog step.  On its own grid the map index is
+// clamped to 0..nB+1, which only changes particles outside the box.
+__device__ __forceinline__ bool bmap_gather_f64(const BMapF64 &m, double xp, double yp, double zp, int ix,
+                                                int iy, int iz, const double (&kE)[8], double &Bx, double &By,
+                                                double &Bz) {
+  double k[8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) k[a] = kE[a];
+  if (m.own) {
+    ix = (int)(xp / m.h0) + 1;
+    iy = (int)(yp / m.h1) + 1;
+    iz = (int)(zp / m.h2) + 1;
+    ix = ix < 0 ? 0 : (ix > m.nb1 + 1 ? m.nb1 + 1 : ix);
+    iy = iy < 0 ? 0 : (iy > m.nb2 + 1 ? m.nb2 + 1 : iy);
+    iz = iz < 0 ? 0 : (iz > m.nb3 + 1 ? m.nb3 + 1 : iz);
+  }
+  const long long q = ix + m.N1 * (iy + m.N2 * (long long)iz);
+  if (!(__ldg(m.B + 4 * q + 3) > 1.e-5)) return false;
+  if (m.own) {
+    const double px = (ix * m.h0 - xp) / m.h0;
+    const double py = (iy * m.h1 - yp) / m.h1;
+    const double pz = (iz * m.h2 - zp) / m.h2;
+    k[0] = px * py * pz;
+    k[1] = (1.0 - px) * py * pz;
+    k[2] = (1.0 - px) * (1.0 - py) * pz;
+    k[3] = px * (1.0 - py) * pz;
+    k[4] = px * py * (1.0 - pz);
+    k[5] = (1.0 - px) * py * (1.0 - pz);
+    k[6] = (1.0 - px) * (1.0 - py) * (1.0 - pz);
+    k[7] = px * (1.0 - py) * (1.0 - pz);
+  }
+  const long long sy = m.N1, sz = m.N1 * m.N2;
+  const long long o[8] = {0, 1, 1 + sy, sy, sz, 1 + sz, 1 + sy + sz, sy + sz};
+  double B[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    double s = k[0] * __ldg(m.B + 4 * (q + o[0]) + a);
+#pragma unroll
+    for (int c = 1; c < 8; ++c) s = s + k[c] * __ldg(m.B + 4 * (q + o[c]) + a);
+    B[a] = s;
+  }
+  Bx = B[0];
+  By = B[1];
+  Bz = B[2];
+  return true;
+}
+
 // ------------------------------------------------------------ launchers
 // fields.cu
 int launch_calc_rho(const Dims &d, double *np, double *rhs, const int *bcnd, int ntype,

@@ -88,6 +88,16 @@ __device__ __forceinline__ void qweights(float gx, float gy, float gz, int w[8])
   w[7] = (1 << QBITS) - (w[0] + w[1] + w[2] + w[3] + w[4] + w[5] + w[6]);
 }
 
+// FP32 copy of the B-field map (Src/part_expmover.f90:148-203): one float4
+// (Bx, By, Bz, |B|) per map node, map nodes indexed like Bi(4, 0:nB1+2, ...).
+struct MixedBMap {
+  const float4 *B;
+  int own;                    // 1: own grid of spacing h_B; 0: the node grid
+  int nb1, nb2, nb3;
+  long long N1, N2;           // nB1 + 3, nB2 + 3
+  float r0, r1, r2;           // h / h_B per direction
+};
+
 // The block's box in shared memory: the nodes bx..bx+TN-1 (and likewise in
 // y, z) of the tile's cells plus one halo cell on each side.
 struct Tile {
@@ -95,6 +105,7 @@ struct Tile {
   const float4 *E;            // E at the box nodes
   const unsigned char *cw;    // all-wall flags of the box cells
   int bx, by, bz;             // grid coordinates of box node (0,0,0)
+  const float4 *B;            // B map at the box nodes (map on the node grid)
 };
 
 // box-local coordinates of cell (ix,iy,iz) when the cell's 8 nodes are in the box
@@ -177,11 +188,58 @@ __device__ __forceinline__ void load_quad(Quad &Q, long long i0, long long lo, l
   }
 }
 
+// B of the map at a particle in cell (ix, iy, iz) at offsets (fx, fy, fz):
+// on the node grid from the E gather's node g0 and weights k[0..7] (in the
+// box Eb = T.E or in HBM); on its own grid at map index INT(x/h_B)+1 with its
+// own weights.  False when |B| at the left map node is not above 1e-5 T.
+__device__ __forceinline__ bool bmap_gather_mixed(const MixedBMap &m, const Tile &T, bool boxed, long long g0,
+                                                  long long sy, long long sz, int ix, int iy, int iz, float fx,
+                                                  float fy, float fz, const float (&kE)[8], float &Bx, float &By,
+                                                  float &Bz) {
+  const float4 *Bb;
+  float k[8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) k[a] = kE[a];
+  if (m.own) {
+    const float xb = ((float)(ix - 1) + fx) * m.r0, yb = ((float)(iy - 1) + fy) * m.r1,
+                zb = ((float)(iz - 1) + fz) * m.r2;
+    int bx = (int)xb, by = (int)yb, bz = (int)zb;
+    bx = bx < 0 ? 0 : (bx > m.nb1 ? m.nb1 : bx);
+    by = by < 0 ? 0 : (by > m.nb2 ? m.nb2 : by);
+    bz = bz < 0 ? 0 : (bz > m.nb3 ? m.nb3 : bz);
+    const float gx = xb - (float)bx, gy = yb - (float)by, gz = zb - (float)bz;
+    const float px = 1.f - gx, py = 1.f - gy, pz = 1.f - gz;
+    k[0] = px * py * pz;
+    k[1] = (1.f - px) * py * pz;
+    k[2] = (1.f - px) * (1.f - py) * pz;
+    k[3] = px * (1.f - py) * pz;
+    k[4] = px * py * (1.f - pz);
+    k[5] = (1.f - px) * py * (1.f - pz);
+    k[6] = (1.f - px) * (1.f - py) * (1.f - pz);
+    k[7] = px * (1.f - py) * (1.f - pz);
+    Bb = m.B;
+    g0 = (bx + 1) + m.N1 * ((by + 1) + m.N2 * (long long)(bz + 1));
+    sy = m.N1;
+    sz = m.N1 * m.N2;
+  } else {
+    Bb = boxed ? T.B : m.B;
+  }
+  const float4 b0 = Bb[g0];
+  if (!(b0.w > 1.e-5f)) return false;
+  const float4 b1 = Bb[g0 + 1], b2 = Bb[g0 + 1 + sy], b3 = Bb[g0 + sy], b4 = Bb[g0 + sz], b5 = Bb[g0 + 1 + sz],
+               b6 = Bb[g0 + 1 + sy + sz], b7 = Bb[g0 + sy + sz];
+  Bx = k[0] * b0.x + k[1] * b1.x + k[2] * b2.x + k[3] * b3.x + k[4] * b4.x + k[5] * b5.x + k[6] * b6.x + k[7] * b7.x;
+  By = k[0] * b0.y + k[1] * b1.y + k[2] * b2.y + k[3] * b3.y + k[4] * b4.y + k[5] * b5.y + k[6] * b6.y + k[7] * b7.y;
+  Bz = k[0] * b0.z + k[1] * b1.z + k[2] * b2.z + k[3] * b3.z + k[4] * b4.z + k[5] * b5.z + k[6] * b6.z + k[7] * b7.z;
+  return true;
+}
+
 // Push + loss test + deposit of the particle quad Q starting at i0;
 // particles outside the range are not touched.  Every lane of the warp must
-// call this (warp-wide hole appends).
-__device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, const Tile &T, long long i0,
-                                          Quad &Q, const float4 *__restrict__ E4,
+// call this (warp-wide hole appends).  BMAP: B from the map m.
+template <bool BMAP>
+__device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, const MixedBMap &m, const Tile &T,
+                                          long long i0, Quad &Q, const float4 *__restrict__ E4,
                                           const int *__restrict__ bcnd, const unsigned char *__restrict__ cw,
                                           int *__restrict__ cell, float *__restrict__ p, long long cap,
                                           signed char *__restrict__ flag, const double *__restrict__ kq,
@@ -227,6 +285,7 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
     // from the box in shared memory when the cell is in it, else from HBM
     const float4 *Eb = E4;
     long long g0 = d.g(ix, iy, iz), sy = d.N1, sz = d.N1 * d.N2;
+    bool boxed = false;
     {
       int lx, ly, lz;
       if (in_box(T, ix, iy, iz, lx, ly, lz)) {
@@ -234,6 +293,7 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
         g0 = lx + TN * (ly + TN * lz);
         sy = TN;
         sz = TN * TN;
+        boxed = true;
       }
     }
     const float4 e0 = Eb[g0], e1 = Eb[g0 + 1], e2 = Eb[g0 + 1 + sy], e3 = Eb[g0 + sy], e4 = Eb[g0 + sz],
@@ -242,10 +302,16 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
     const float Ey = k0 * e0.y + ka * e1.y + kb * e2.y + kc * e3.y + kd * e4.y + ke * e5.y + kf * e6.y + kg * e7.y;
     const float Ez = k0 * e0.z + ka * e1.z + kb * e2.z + kc * e3.z + kd * e4.z + ke * e5.z + kf * e6.z + kg * e7.z;
     const float k1 = c.k1;
-    if (c.boris) {
+    float Bx = c.Bx, By = c.By, Bz = c.Bz, kk = c.kk;
+    bool boris = c.boris;
+    if (BMAP && boris) {
+      const float kE[8] = {k0, ka, kb, kc, kd, ke, kf, kg};
+      boris = bmap_gather_mixed(m, T, boxed, g0, sy, sz, ix, iy, iz, fx, fy, fz, kE, Bx, By, Bz);
+      const float B_tot = sqrtf(Bx * Bx + By * By + Bz * Bz);
+      kk = k1 * (2.f / (1.f + (k1 * B_tot) * (k1 * B_tot)));
+    }
+    if (boris) {
       // Src/part_expmover.f90:128-160
-      const float Bx = c.Bx, By = c.By, Bz = c.Bz;
-      const float kk = c.kk;
       const float v1x = vx + k1 * Ex, v1y = vy + k1 * Ey, v1z = vz + k1 * Ez;
       const float v3x = v1x + k1 * (v1y * Bz - v1z * By);
       const float v3y = v1y + k1 * (v1z * Bx - v1x * Bz);
@@ -382,8 +448,9 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
 // one block per tile: the particles [tile_off[t], tile_off[t+1]) of the last
 // sort, clipped to the current count; E and the wall flags of the tile's box
 // are read into shared memory once
+template <bool BMAP>
 __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tiles(
-    Dims d, MixedConst c, const float4 *__restrict__ E4, const int *__restrict__ bcnd,
+    Dims d, MixedConst c, MixedBMap m, const float4 *__restrict__ E4, const int *__restrict__ bcnd,
     const unsigned char *__restrict__ cw, int *__restrict__ cell, float *__restrict__ p, long long cap,
     const int *__restrict__ count, signed char *__restrict__ flag, const int *__restrict__ tile_off,
     const double *__restrict__ kq, double *__restrict__ np, int *__restrict__ holes, int *__restrict__ nholes,
@@ -391,15 +458,17 @@ __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tiles(
   __shared__ unsigned s_acc[TT];
   __shared__ float4 s_E[TT];
   __shared__ unsigned char s_cw[(TN - 1) * (TN - 1) * (TN - 1)];
+  __shared__ float4 s_B[BMAP ? TT : 1];
   const int t = blockIdx.x;
   const int tx = t % c.ntx, ty = (t / c.ntx) % c.nty, tz = t / (c.ntx * c.nty);
-  const Tile T{s_acc, s_E, s_cw, tx * TC, ty * TC, tz * TC};
+  const Tile T{s_acc, s_E, s_cw, tx * TC, ty * TC, tz * TC, s_B};
   for (int e = threadIdx.x; e < TT; e += MBK) {
     s_acc[e] = 0u;
     const int lx = e % TN, ly = (e / TN) % TN, lz = e / (TN * TN);
     const int gx = T.bx + lx, gy = T.by + ly, gz = T.bz + lz;
-    s_E[e] = (gx <= d.n1 + 2 && gy <= d.n2 + 2 && gz <= d.n3 + 2) ? __ldg(E4 + d.g(gx, gy, gz))
-                                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool ing = gx <= d.n1 + 2 && gy <= d.n2 + 2 && gz <= d.n3 + 2;
+    s_E[e] = ing ? __ldg(E4 + d.g(gx, gy, gz)) : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (BMAP && !m.own) s_B[e] = ing ? __ldg(m.B + d.g(gx, gy, gz)) : make_float4(0.f, 0.f, 0.f, 0.f);
   }
   for (int e = threadIdx.x; e < (TN - 1) * (TN - 1) * (TN - 1); e += MBK) {
     const int lx = e % (TN - 1), ly = (e / (TN - 1)) % (TN - 1), lz = e / ((TN - 1) * (TN - 1));
@@ -418,7 +487,7 @@ __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tiles(
     Quad Q;
     const long long i0 = base + 4 * threadIdx.x;
     load_quad(Q, i0, lo, hi, cell, p, cap, flag);
-    push_quad(d, c, T, i0, Q, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes, acc, err);
+    push_quad<BMAP>(d, c, m, T, i0, Q, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes, acc, err);
     if (++chunks == FLUSH_PARTICLES / CHUNK && base + CHUNK < hi) {
       chunks = 0;
       __syncthreads();
@@ -432,13 +501,14 @@ __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tiles(
 
 // particles past the last tile (appended since the sort), or all of them
 // when no sort has run: deposited straight into the FP64 grid
+template <bool BMAP>
 __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tail(
-    Dims d, MixedConst c, const float4 *__restrict__ E4, const int *__restrict__ bcnd,
+    Dims d, MixedConst c, MixedBMap m, const float4 *__restrict__ E4, const int *__restrict__ bcnd,
     const unsigned char *__restrict__ cw, int *__restrict__ cell, float *__restrict__ p, long long cap,
     const int *__restrict__ count, signed char *__restrict__ flag, const int *__restrict__ tile_off,
     const double *__restrict__ kq, double *__restrict__ np, int *__restrict__ holes, int *__restrict__ nholes,
     double *__restrict__ acc, int *__restrict__ err) {
-  const Tile T{nullptr, nullptr, nullptr, 0, 0, 0};
+  const Tile T{nullptr, nullptr, nullptr, 0, 0, 0, nullptr};
   const long long N = *count;
   const long long lo = tile_off ? tile_off[c.ntiles] : 0;
   const long long first = lo & ~3LL;
@@ -446,7 +516,7 @@ __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tail(
     Quad Q;
     const long long i0 = base + 4 * threadIdx.x;
     load_quad(Q, i0, lo, N, cell, p, cap, flag);
-    push_quad(d, c, T, i0, Q, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes, acc, err);
+    push_quad<BMAP>(d, c, m, T, i0, Q, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes, acc, err);
   }
 }
 
@@ -763,11 +833,18 @@ __global__ void k_deposit_mixed(Dims d, double kdep, const int *__restrict__ cel
   }
   int w[8];
   qweights(p[i], p[cap + i], p[2 * cap + i], w);
-  const Tile T{nullptr, nullptr, nullptr, 0, 0, 0};
+  const Tile T{nullptr, nullptr, nullptr, 0, 0, 0, nullptr};
   deposit8(d, T, ix, iy, iz, d.g(ix, iy, iz), w, kdep, kq, np);
 }
 
 bool aligned16(const void *q) { return ((uintptr_t)q & 15u) == 0; }
+
+// the FP32 copy (Bx, By, Bz, |B|) of the FP64 map Bi(4, ...)
+__global__ void k_pack_b32(const double *__restrict__ Bi, long long nodes, float4 *__restrict__ B4) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nodes; q += stride)
+    B4[q] = make_float4((float)Bi[4 * q], (float)Bi[4 * q + 1], (float)Bi[4 * q + 2], (float)Bi[4 * q + 3]);
+}
 
 int check_layout(const lepic_grid_t &g, const lepic_species_mixed_t &sp) {
   if (g.n[0] > LEPIC_CELL_MAX || g.n[1] > LEPIC_CELL_MAX || g.n[2] > LEPIC_CELL_MAX) return LEPIC_ERR_UNSUPPORTED;
@@ -823,18 +900,55 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
   int *side = (int *)scratch(nm, sizeof(int) * 4);
   if (!holes || !tailA || !holeH || !side) return LEPIC_ERR_CUDA;
   LEPIC_CUDA(cudaMemsetAsync(side, 0, sizeof(int) * 4, s));
+  // B-field map: an FP32 copy made at every call (the map may change
+  // between calls; (n_B+3)^3 x 48 B of traffic)
+  MixedBMap m;
+  memset(&m, 0, sizeof(m));
+  {
+    BMapF64 m64;
+    if (int rc = bmap_from_phys(P, g.n, m64)) return rc;
+    if (m64.B) {
+      const long long nodes = m64.N1 * m64.N2 * (long long)(m64.nb3 + 3);
+      float4 *B4 = (float4 *)scratch("bmap_f32", sizeof(float4) * (size_t)nodes);
+      if (!B4) return LEPIC_ERR_CUDA;
+      k_pack_b32<<<ctx().sms * 4, 256, 0, s>>>(m64.B, nodes, B4);
+      LEPIC_CUDA(cudaGetLastError());
+      m.B = B4;
+      m.own = m64.own;
+      m.nb1 = m64.nb1;
+      m.nb2 = m64.nb2;
+      m.nb3 = m64.nb3;
+      m.N1 = m64.N1;
+      m.N2 = m64.N2;
+      if (m.own) {
+        m.r0 = (float)(g.h[0] / m64.h0);
+        m.r1 = (float)(g.h[1] / m64.h1);
+        m.r2 = (float)(g.h[2] / m64.h2);
+      }
+    }
+  }
   const float4 *E = reinterpret_cast<const float4 *>(E4);
   int t0 = timer_start("push_deposit_mixed", s);
-  if (sp.tile_off)
-    k_push_deposit_tiles<<<c.ntiles, MBK, 0, s>>>(d, c, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap, sp.count,
-                                                  sp.flag_dead, sp.tile_off, g.kq, np, holes, side, acc,
-                                                  ctx().d_err);
   // the tail: at most what was appended since the sort unless never sorted
   long long tail = sp.tile_off ? (long long)ctx().sms * 2 : grid_for(n_hint > 0 ? n_hint : sp.cap, CHUNK);
   if (tail > (long long)ctx().sms * 8) tail = (long long)ctx().sms * 8;
-  k_push_deposit_tail<<<(int)tail, MBK, 0, s>>>(d, c, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap, sp.count,
-                                               sp.flag_dead, sp.tile_off, g.kq, np, holes, side, acc,
-                                               ctx().d_err);
+  if (m.B) {
+    if (sp.tile_off)
+      k_push_deposit_tiles<true><<<c.ntiles, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap,
+                                                          sp.count, sp.flag_dead, sp.tile_off, g.kq, np, holes,
+                                                          side, acc, ctx().d_err);
+    k_push_deposit_tail<true><<<(int)tail, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap,
+                                                        sp.count, sp.flag_dead, sp.tile_off, g.kq, np, holes,
+                                                        side, acc, ctx().d_err);
+  } else {
+    if (sp.tile_off)
+      k_push_deposit_tiles<false><<<c.ntiles, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p,
+                                                           sp.cap, sp.count, sp.flag_dead, sp.tile_off, g.kq, np,
+                                                           holes, side, acc, ctx().d_err);
+    k_push_deposit_tail<false><<<(int)tail, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap,
+                                                         sp.count, sp.flag_dead, sp.tile_off, g.kq, np, holes,
+                                                         side, acc, ctx().d_err);
+  }
   timer_stop(t0, s);
   LEPIC_CUDA(cudaGetLastError());
   int t1 = timer_start("fill_holes_mixed", s);

@@ -31,9 +31,11 @@ struct PushConst {
 
 // gather + Boris/leapfrog + position update of one particle; returns the
 // post-push cell (clamped) for the loss test.  Src/part_expmover.f90:89-272.
-__device__ __forceinline__ void push_one(const Dims &d, const PushConst &c, const double *__restrict__ Ei,
-                                         double &xp, double &yp, double &zp, double &vx, double &vy,
-                                         double &vz, int &ixn, int &iyn, int &izn) {
+// BMAP: B from the map m (else the uniform c.Bx, c.By, c.Bz).
+template <bool BMAP>
+__device__ __forceinline__ void push_one(const Dims &d, const PushConst &c, const BMapF64 &m,
+                                         const double *__restrict__ Ei, double &xp, double &yp, double &zp,
+                                         double &vx, double &vy, double &vz, int &ixn, int &iyn, int &izn) {
   int ix = (int)(xp / c.h0) + 1, iy = (int)(yp / c.h1) + 1, iz = (int)(zp / c.h2) + 1;
   double px = (ix * c.h0 - xp) / c.h0;
   double py = (iy * c.h1 - yp) / c.h1;
@@ -57,8 +59,13 @@ __device__ __forceinline__ void push_one(const Dims &d, const PushConst &c, cons
     E[a] = k0 * __ldg(e0 + a) + kk1 * __ldg(e1 + a) + k2 * __ldg(e2 + a) + k3 * __ldg(e3 + a) +
            k4 * __ldg(e4 + a) + k5 * __ldg(e5 + a) + k6 * __ldg(e6 + a) + k7 * __ldg(e7 + a);
   const double k1 = c.k1;
-  if (c.boris) {
-    const double Bx = c.Bx, By = c.By, Bz = c.Bz;
+  double Bx = c.Bx, By = c.By, Bz = c.Bz;
+  bool boris = c.boris;
+  if (BMAP && boris) {
+    const double kE[8] = {k0, kk1, k2, k3, k4, k5, k6, k7};
+    boris = bmap_gather_f64(m, xp, yp, zp, ix, iy, iz, kE, Bx, By, Bz);
+  }
+  if (boris) {
     double B_tot = sqrt(Bx * Bx + By * By + Bz * Bz);
     double kb = k1 * (2.0 / (1.0 + (k1 * B_tot) * (k1 * B_tot)));
     double v1x = vx + k1 * E[0], v1y = vy + k1 * E[1], v1z = vz + k1 * E[2];
@@ -89,7 +96,8 @@ __device__ __forceinline__ void push_one(const Dims &d, const PushConst &c, cons
 
 // Loss accumulators: acc[0] P_loss(1), acc[1] P_loss(3), acc[2+2g] p_mac
 // count at label g, acc[3+2g] p_mac energy at label g.
-__global__ void __launch_bounds__(PB) k_push_f64(Dims d, PushConst c, const double *__restrict__ Ei,
+template <bool BMAP>
+__global__ void __launch_bounds__(PB) k_push_f64(Dims d, PushConst c, BMapF64 m, const double *__restrict__ Ei,
                                                  const int *__restrict__ bcnd,
                                                  const unsigned char *__restrict__ cw,
                                                  const double *__restrict__ pin, double *__restrict__ pout,
@@ -115,7 +123,7 @@ __global__ void __launch_bounds__(PB) k_push_f64(Dims d, PushConst c, const doub
     return;
   }
   int ix, iy, iz;
-  push_one(d, c, Ei, xp, yp, zp, vx, vy, vz, ix, iy, iz);
+  push_one<BMAP>(d, c, m, Ei, xp, yp, zp, vx, vy, vz, ix, iy, iz);
   if (cw[d.c(ix, iy, iz)]) {
     double Eki = 0.5 * c.Nm * c.mass * (vx * vx + vy * vy + vz * vz);
     int igrid = bcnd[d.g(ix, iy, iz)];
@@ -343,6 +351,8 @@ int launch_part_mover(const lepic_grid_t &g, const double *Ei, lepic_species_f64
   c.ymax = P.ymax;
   c.zmax = P.zmax;
   c.ngrid = ngrid;
+  BMapF64 m;
+  if (int rc = bmap_from_phys(P, g.n, m)) return rc;
   const long long cap = sp.cap;
   int nacc = 2 + 2 * (ngrid + 1);
   double *acc = (double *)scratch("push_acc", sizeof(double) * nacc);
@@ -355,8 +365,12 @@ int launch_part_mover(const lepic_grid_t &g, const double *Ei, lepic_species_f64
   LEPIC_CUDA(cudaStreamSynchronize(s));
   if (N > 0) {
     int t0 = timer_start("push_f64", s);
-    k_push_f64<<<grid_for(N, PB), PB, 0, s>>>(d, c, Ei, g.bcnd, g.cell_wall, sp.p, sp.p_alt, cap,
-                                              sp.count, sp.flag_dead, keep, acc, ctx().d_err);
+    if (m.B)
+      k_push_f64<true><<<grid_for(N, PB), PB, 0, s>>>(d, c, m, Ei, g.bcnd, g.cell_wall, sp.p, sp.p_alt, cap,
+                                                      sp.count, sp.flag_dead, keep, acc, ctx().d_err);
+    else
+      k_push_f64<false><<<grid_for(N, PB), PB, 0, s>>>(d, c, m, Ei, g.bcnd, g.cell_wall, sp.p, sp.p_alt, cap,
+                                                       sp.count, sp.flag_dead, keep, acc, ctx().d_err);
     timer_stop(t0, s);
     LEPIC_CUDA(cudaGetLastError());
     int t1 = timer_start("compact_scan", s);

@@ -57,8 +57,10 @@ __device__ __forceinline__ int run_id(long long key, bool &head) {
   return __popc(heads & lanemask_le());
 }
 
+// BMAP: B from the map m (else the uniform c.Bx, c.By, c.Bz)
+template <bool BMAP>
 __global__ void __launch_bounds__(FB) k_push_deposit_f64(
-    Dims d, FusedConst c, const double *__restrict__ Ei, const int *__restrict__ bcnd,
+    Dims d, FusedConst c, BMapF64 m, const double *__restrict__ Ei, const int *__restrict__ bcnd,
     const unsigned char *__restrict__ cw, double *__restrict__ p, long long cap,
     const int *__restrict__ count, signed char *__restrict__ flag, const double *__restrict__ kq,
     double *__restrict__ np, int *__restrict__ holes, int *__restrict__ nholes,
@@ -102,8 +104,13 @@ __global__ void __launch_bounds__(FB) k_push_deposit_f64(
         E[a] = k0 * __ldg(e0 + a) + ka * __ldg(e1 + a) + kb * __ldg(e2 + a) + kc * __ldg(e3 + a) +
                kd * __ldg(e4 + a) + ke * __ldg(e5 + a) + kf * __ldg(e6 + a) + kg * __ldg(e7 + a);
       const double k1 = c.k1;
-      if (c.boris) {
-        const double Bx = c.Bx, By = c.By, Bz = c.Bz;
+      double Bx = c.Bx, By = c.By, Bz = c.Bz;
+      bool boris = c.boris;
+      if (BMAP && boris) {
+        const double kE[8] = {k0, ka, kb, kc, kd, ke, kf, kg};
+        boris = bmap_gather_f64(m, xp, yp, zp, ix, iy, iz, kE, Bx, By, Bz);
+      }
+      if (boris) {
         double B_tot = sqrt(Bx * Bx + By * By + Bz * Bz);
         double kk = k1 * (2.0 / (1.0 + (k1 * B_tot) * (k1 * B_tot)));
         double v1x = vx + k1 * E[0], v1y = vy + k1 * E[1], v1z = vz + k1 * E[2];
@@ -303,6 +310,8 @@ int launch_push_deposit(const lepic_grid_t &g, const double *Ei, lepic_species_f
   c.zmax = P.zmax;
   c.ngrid = ngrid;
   if (!sp.flag_dead) return LEPIC_ERR_ARG;
+  BMapF64 m;
+  if (int rc = bmap_from_phys(P, g.n, m)) return rc;
   const size_t cap = (size_t)sp.cap;
   char nm[32];
   snprintf(nm, sizeof nm, "work_list%d", p);
@@ -317,9 +326,14 @@ int launch_push_deposit(const lepic_grid_t &g, const double *Ei, lepic_species_f
   LEPIC_CUDA(cudaMemsetAsync(side, 0, sizeof(int) * 4, s));
   const int nthreads = n_hint > 0 ? n_hint : sp.cap;
   int t0 = timer_start("push_deposit_f64", s);
-  k_push_deposit_f64<<<grid_for(nthreads, FB), FB, 0, s>>>(d, c, Ei, g.bcnd, g.cell_wall, sp.p, sp.cap,
-                                                           sp.count, sp.flag_dead, g.kq, np, holes,
-                                                           side, acc_dev, ctx().d_err);
+  if (m.B)
+    k_push_deposit_f64<true><<<grid_for(nthreads, FB), FB, 0, s>>>(d, c, m, Ei, g.bcnd, g.cell_wall, sp.p,
+                                                                   sp.cap, sp.count, sp.flag_dead, g.kq, np,
+                                                                   holes, side, acc_dev, ctx().d_err);
+  else
+    k_push_deposit_f64<false><<<grid_for(nthreads, FB), FB, 0, s>>>(d, c, m, Ei, g.bcnd, g.cell_wall, sp.p,
+                                                                    sp.cap, sp.count, sp.flag_dead, g.kq, np,
+                                                                    holes, side, acc_dev, ctx().d_err);
   timer_stop(t0, s);
   LEPIC_CUDA(cudaGetLastError());
   int t1 = timer_start("fill_holes", s);

@@ -55,6 +55,9 @@ def set_commons(st, ncol=0, npt=0, p_ncol=None):
     pi_.sig_npt_mx = npt
     pi_.n_cell = st.n_cell
     pi_.flag_B = st.flag_B
+    pi_.flag_B_pos = int(getattr(st, "flag_B_pos", 0))
+    bf = getattr(st, "bfield", None)
+    pi_.flag_gridB = int(bf is not None and tuple(bf.n_B) != tuple(st.n))
     pi_.ns_coll = st.wl.ns_coll
     pi_.flag_pbc = st.geom.flag_pbc
     pi_.flag_nmn = st.geom.flag_nmn
@@ -144,10 +147,17 @@ def calc_efield(st, phi, Ei=None):
     return E
 
 
-def _bi_uniform(st):
-    Bi = np.zeros((4, 4, 4, 4))          # Bi(4, 0:3, 0:3, 0:3) with n_B = 1
+def _bi(st):
+    """(Bi, n_B, h_B) as the reference passes them to part_mover: the map of
+    st.bfield, else Bi(4, 0:3, 0:3, 0:3) with n_B = 1 holding the uniform
+    field at (1, 1, 1)."""
+    bf = getattr(st, "bfield", None)
+    if bf is not None:
+        return (np.ascontiguousarray(bf.Bi, dtype=np.float64), np.array(bf.n_B, dtype=np.int32),
+                np.ascontiguousarray(bf.h_B, dtype=np.float64))
+    Bi = np.zeros((4, 4, 4, 4))
     Bi[1, 1, 1, 0:3] = st.Bconst
-    return Bi
+    return Bi, np.array([1, 1, 1], dtype=np.int32), np.ascontiguousarray(st.h, dtype=np.float64)
 
 
 def part_mover(st, Ei, vxp, np_tot, flag_dead, p_mac, P_loss, ptype, ngrid=None):
@@ -157,18 +167,17 @@ def part_mover(st, Ei, vxp, np_tot, flag_dead, p_mac, P_loss, ptype, ngrid=None)
     n = _lib.np_i(st.n)
     h = np.ascontiguousarray(st.h, dtype=np.float64)
     E = np.ascontiguousarray(Ei, dtype=np.float64)
-    Bi = _bi_uniform(st)
+    Bi, nB, hB = _bi(st)
     bc = _lib.np_i(st.geom.bcnd)
     nmax = vxp.shape[1]
     assert vxp.flags["C_CONTIGUOUS"] and np_tot.dtype == np.int32 and flag_dead.dtype == np.int8
     dummy_i = np.zeros(16, dtype=np.int32)
     dummy_d = np.zeros(16)
-    nB = np.array([1, 1, 1], dtype=np.int32)
     lib().part_mover_(_pi(n), _pd(h), _pd(E), _pd(Bi), _pd(p_mac), _pd(P_loss), _pd(vxp), _pi(bc),
                       _i(nmax), _i(st.ntype), _i(ngrid), flag_dead.ctypes.data_as(_lib.P_i8), _i(1),
                       _pi(np_tot), _i(1), _i(ptype), _pi(dummy_i), _pi(dummy_i), _pd(dummy_d),
                       _pd(dummy_d), _pd(dummy_d), _pd(dummy_d), _pi(dummy_i), _pi(dummy_i), _pi(nB),
-                      _pd(h))
+                      _pd(hB))
     check(lib().lepic_gpu_last_error(), "part_mover")
 
 
@@ -321,8 +330,7 @@ class MainLoop:
         self.ngrid = ngrid
         self.p_mac = np.zeros((ngrid + 1, 2, st.ntype))
         self.P_loss = np.zeros((st.ntype, 4))
-        self.Bi = _bi_uniform(st)
-        self.nB = np.array([1, 1, 1], dtype=np.int32)
+        self.Bi, self.nB, self.hB = _bi(st)
         self.iseed = np.array([iseed], dtype=np.int32)
         self.zi = np.zeros(16, dtype=np.int32)
         self.zd = np.zeros(16)
@@ -403,7 +411,7 @@ class MainLoop:
                               _i(self.ngrid), self.flag_dead.ctypes.data_as(_lib.P_i8), _i(1),
                               _pi(self.np_tot), _i(1), _i(p), _pi(self.zi), _pi(self.zi), _pd(self.zd),
                               _pd(self.zd), _pd(self.zd), _pd(self.zd), _pi(self.zi), _pi(self.zi),
-                              _pi(self.nB), _pd(self.h))
+                              _pi(self.nB), _pd(self.hB))
                 check(L.lepic_gpu_last_error(), "part_mover")
         for p in range(1, nt + 1):
             check(L.lepic_gpu_mirror_zero(_vp(self.np[p - 1]), self.np[p - 1].nbytes), "np = 0")

@@ -184,7 +184,12 @@ class Simulation:
         # overflow raises LepicError at the next read
         self.check_every = int(check_every)
         self.seed = int(seed)
-        self.P = phys_struct(st)
+        self.Bmap = None
+        if getattr(st, "bfield", None) is not None:
+            # the B-field map, resident for the run (Bi(4, 0:nB1+2, ...))
+            self.Bmap = torch.as_tensor(np.ascontiguousarray(st.bfield.Bi), dtype=torch.float64,
+                                        device=self.dev)
+        self.P = phys_struct(st, bmap_ptr=None if self.Bmap is None else self.Bmap.data_ptr())
         self.comm = comm
         if comm is not None:
             import torch.distributed as dist

@@ -43,7 +43,7 @@ extern "C" {
 #define LEPIC_ERR_PMAX 3          /* null-collision probability > 1               */
 #define LEPIC_ERR_EKR_TABLE 4     /* collision energy above the sigma table       */
 #define LEPIC_ERR_NEG_ENERGY 5    /* negative CM energy after threshold           */
-#define LEPIC_ERR_UNSUPPORTED 6   /* option outside the GPU path (B maps, ...)    */
+#define LEPIC_ERR_UNSUPPORTED 6   /* option outside the GPU path (dielectrics...) */
 #define LEPIC_ERR_FEW_COLL 7      /* collision time step too small for electrons  */
 #define LEPIC_ERR_CUDA 20         /* CUDA runtime error                          */
 #define LEPIC_ERR_ARG 21          /* invalid argument / size                     */
@@ -119,8 +119,9 @@ void pdesolver_(double *u, const double *b, const int *bcnd, const double *h, co
 void calc_efield_(const int *n, const double *h, const double *phi, double *Ei, const int *bcnd);
 
 /* Src/part_expmover.f90:1 as called at Src/main.f90:1250-1252 (26
- * arguments) -- trilinear gather, Boris (uniform B, n_B(1) = 1) or leapfrog,
- * position update, loss test and in-order compaction of species ptype. */
+ * arguments) -- trilinear gather, Boris (uniform B with n_B(1) = 1, else the
+ * B-field map Bi(4,0:n_B(1)+2,...) of spacing h_B) or leapfrog, position
+ * update, loss test and in-order compaction of species ptype. */
 void part_mover_(const int *n, const double *h, const double *Ei, const double *Bi, double *p_mac,
                  double *P_loss, double *vxp, const int *bcnd, const int *nmax, const int *ntype,
                  const int *ngrid, signed char *flag_dead, const int *nproc, int *np_tot,
@@ -229,6 +230,16 @@ typedef struct {
   int flag_B, flag_B_pos, flag_pbc, flag_nmn;
   int ns_coll, n_cell, np_cell;
   double Bconst[3];
+  /* B-field map (Src/main.f90:361-431, read by Src/part_expmover.f90:148-203),
+   * used when flag_B = 1 and Bmap is not NULL (n_B(1) > 1 in the reference);
+   * Bconst is then ignored.  Bmap = Bi(4, 0:n_B(1)+2, 0:n_B(2)+2, 0:n_B(3)+2)
+   * column-major, component fastest, Bi(4,...) = |B| (device pointer for the
+   * device API).  A map with n_B = n lies on the node grid and reuses the
+   * E-field weights; any other n_B is its own grid of spacing h_B.  A
+   * particle whose left map node has |B| <= 1e-5 T takes the leapfrog step. */
+  const double *Bmap;
+  int n_B[3];
+  double h_B[3];
 } lepic_phys_t;
 
 /* Cross-section tables after Src/read_reactions.f90:ordering, device copies. */

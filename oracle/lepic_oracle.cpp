@@ -604,7 +604,7 @@ void oracle_calc_efield(const int n[3], const double h[3], const double *phi, do
 }
 
 // Src/part_expmover.f90:1-482 (part_mover) without the dbg_* counters, for
-// uniform B (n_B(1) = 1) and metal walls.  p_mac(ntype,2,0:ngrid) and
+// a uniform B (n_B(1) = 1) or a B-field map (:148-203) and metal walls.  p_mac(ntype,2,0:ngrid) and
 // P_loss(4,ntype) are accumulated like the reference (column-major).
 // Dead particles (flag_dead = 1) are removed; lost particles are compacted
 // out in order.  Returns ORACLE_ERR_UNSUPPORTED for periodic/Neumann planes
@@ -663,10 +663,57 @@ int oracle_part_mover(const int n[3], const double h[3], const double *Ei, doubl
     int flag_B_tmp = 0;
     double Bx = 0, By = 0, Bz = 0;
     if (P->flag_B == 1) {
-      Bx = P->Bconst[0];
-      By = P->Bconst[1];
-      Bz = P->Bconst[2];
-      flag_B_tmp = 1;
+      if (!P->Bmap || P->n_B[0] == 1) {
+        Bx = P->Bconst[0];
+        By = P->Bconst[1];
+        Bz = P->Bconst[2];
+        flag_B_tmp = 1;
+      } else {
+        // map on the node grid (flag_gridB = 0): the E gather's cell and
+        // weights; on its own grid: INT(x/h_B)+1 and weights from h_B
+        const int flag_gridB = (P->n_B[0] != d.n1 || P->n_B[1] != d.n2 || P->n_B[2] != d.n3) ? 1 : 0;
+        const long BN1 = P->n_B[0] + 3, BN2 = P->n_B[1] + 3;
+        int bx = ix, by = iy, bz = iz;
+        if (flag_gridB == 1) {
+          bx = (int)(xp / P->h_B[0]) + 1;
+          by = (int)(yp / P->h_B[1]) + 1;
+          bz = (int)(zp / P->h_B[2]) + 1;
+        }
+        auto Bi = [&](int c, int a, int b, int e) { return P->Bmap[c + 4 * (a + BN1 * (b + BN2 * (long)e))]; };
+        if (Bi(3, bx, by, bz) > 1.e-5) {
+          double kb[8];
+          for (int a = 0; a < 8; ++a) kb[a] = ki[a];
+          if (flag_gridB == 1) {
+            double qx = (bx * P->h_B[0] - xp) / P->h_B[0];
+            double qy = (by * P->h_B[1] - yp) / P->h_B[1];
+            double qz = (bz * P->h_B[2] - zp) / P->h_B[2];
+            kb[0] = qx * qy * qz;
+            kb[1] = (1.0 - qx) * qy * qz;
+            kb[2] = (1.0 - qx) * (1.0 - qy) * qz;
+            kb[3] = qx * (1.0 - qy) * qz;
+            kb[4] = qx * qy * (1.0 - qz);
+            kb[5] = (1.0 - qx) * qy * (1.0 - qz);
+            kb[6] = (1.0 - qx) * (1.0 - qy) * (1.0 - qz);
+            kb[7] = qx * (1.0 - qy) * (1.0 - qz);
+          }
+          double Bc[3];
+          for (int c = 0; c < 3; ++c) {
+            double s = kb[0] * Bi(c, bx, by, bz);
+            s = s + kb[1] * Bi(c, bx + 1, by, bz);
+            s = s + kb[2] * Bi(c, bx + 1, by + 1, bz);
+            s = s + kb[3] * Bi(c, bx, by + 1, bz);
+            s = s + kb[4] * Bi(c, bx, by, bz + 1);
+            s = s + kb[5] * Bi(c, bx + 1, by, bz + 1);
+            s = s + kb[6] * Bi(c, bx + 1, by + 1, bz + 1);
+            s = s + kb[7] * Bi(c, bx, by + 1, bz + 1);
+            Bc[c] = s;
+          }
+          Bx = Bc[0];
+          By = Bc[1];
+          Bz = Bc[2];
+          flag_B_tmp = 1;
+        }
+      }
     }
     if (P->flag_B_pos == 1 && q > 0.0) flag_B_tmp = 0;
     if (flag_B_tmp == 1) {

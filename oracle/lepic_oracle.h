@@ -50,11 +50,14 @@ typedef struct OPhys {
   double nu_uplim[ORACLE_NPART];
   double dt, xmax, ymax, zmax, x_load;
   double qe, eps0, pi;
-  int flag_B;                      /* 1: magnetised (uniform B only)        */
+  int flag_B;                      /* 1: magnetised                         */
   int flag_B_pos;                  /* 1: positive ions not magnetised       */
   int flag_pbc, flag_nmn;
   int ns_coll, n_cell, np_cell;
   double Bconst[3];                /* Bi(1:3,1,1,1) with n_B(1)=1           */
+  const double *Bmap;              /* Bi(4,0:nB1+2,0:nB2+2,0:nB3+2) or NULL  */
+  int n_B[3];                      /* map grid (n_B(1) > 1 with a map)       */
+  double h_B[3];                   /* map spacing (xmax/n_B(1), ...)         */
 } OPhys;
 
 /* Cross-section tables after Src/read_reactions.f90:ordering. */
