@@ -20,6 +20,9 @@ set-ups shrunk so the FP64 CPU oracle finishes in seconds):
   penning    96x96x192 cells, e- 32 ppc, Bz = 0.1 T, end plates +200 V
              (electrode labels 2 and 3), side walls 0 V (label 1)
   mcc192     192^3 cells, e- + Ar+ 128 ppc (mixed precision only)
+  pbc16      16^3 cells, e- + Ar+ 16 ppc, walls at both x ends, periodic
+             planes in y and z (pbc32x16: 32 cells in x)
+  nmn16      the same with the Neumann (symmetry) plane at x = 0
 """
 from __future__ import annotations
 
@@ -62,6 +65,7 @@ class Workload:
     blobs: int = 0                  # Poisson-only source: number of Gaussian blobs
     blob_seed: int = 3
     mixed_only: bool = False
+    neumann_x: bool = False         # x = 0 is a Neumann (symmetry) plane
 
 
 def _box(n, dx):
@@ -83,6 +87,12 @@ def workload(name: str) -> Workload:
         return Workload(name, n, 1e-4, [_box(n, 1e-4) + [1]], [0.0, 0.0], _ar_ion(),
                         Te=2.0, n0=1e15, ppc=64 if name != "mcc32" else 32, dt=2e-11, steps=500,
                         B=(0.0, 0.0, 0.01), gas_pressure=1.0, gas_T=300.0)
+    if name in ("pbc16", "pbc32x16", "nmn16"):
+        # walls at both x ends (nmn16: the Neumann plane at x = 0 instead),
+        # periodic planes in y and z (a box segment, then label 0 over it)
+        n = {"pbc16": (16, 16, 16), "pbc32x16": (32, 16, 16), "nmn16": (16, 16, 16)}[name]
+        return Workload(name, n, 1e-4, [_box(n, 1e-4) + [1], _box(n, 1e-4) + [0]], [0.0, 0.0], _ar_ion(),
+                        Te=2.0, n0=1e15, ppc=16, dt=2e-11, steps=200, neumann_x=(name == "nmn16"))
     if name in ("mcc192",):
         n = (192, 192, 192)
         return Workload(name, n, 1e-4, [_box(n, 1e-4) + [1]], [0.0, 0.0], _ar_ion(),
@@ -172,7 +182,9 @@ def build(wl: Workload | str) -> Setup:
         wl = workload(wl)
     n = tuple(wl.n)
     segs = [list(s) for s in wl.segments]
-    box = segs[0][3:6]
+    box = list(segs[0][3:6])
+    if wl.neumann_x:
+        box[0] = -box[0]            # a negative xmax selects the Neumann plane
     geom = generate_boundary(n, box, segs, wl.V)
     h = geom.h.copy()
     ngas = 0.0

@@ -290,9 +290,8 @@ int lepic_dev_pdesolver(const lepic_grid_t *g, double *u, const double *b, int n
                         double omega, int ng, const lepic_phys_t *P, int *k, double *ktot,
                         double *res, void *stream) {
   if (!g || !P) return LEPIC_ERR_ARG;
-  if (P->flag_pbc || P->flag_nmn) return LEPIC_ERR_UNSUPPORTED;
   return launch_pdesolver(Dims(g->n), g->h, u, b, g->bcnd, ncycl, eps, omega, ng, P->eps0, k, ktot,
-                          res, S(stream));
+                          res, S(stream), P->flag_pbc, P->flag_nmn);
 }
 
 int lepic_dev_part_mover(const lepic_grid_t *g, const double *Ei, lepic_species_f64_t *s, int ptype,
@@ -395,7 +394,6 @@ void pdesolver_(double *u, const double *b, const int *bcnd, const double *h, co
                 double *res, const int *ng, const int *rank, const int *nproc) {
   (void)rank;
   if (*nproc != 1) return record(LEPIC_ERR_UNSUPPORTED);
-  if (part_info_int_.flag_pbc || part_info_int_.flag_nmn) return record(LEPIC_ERR_UNSUPPORTED);
   cudaStream_t s = 0;
   Dims d(n);
   // u(0:n1+2,0:n2+2,-1:n3+2): skip the z = -1 ghost plane (MPI halo only)
@@ -408,7 +406,7 @@ void pdesolver_(double *u, const double *b, const int *bcnd, const double *h, co
   const int *bc_d = dev_view("dropin_bcnd", bcnd, (size_t)d.cnt(), READ, s, &rc);
   if (!bc_d) return record(rc);
   rc = launch_pdesolver(d, h, u_d, b_d, bc_d, *ncycl, *eps, *omega, *ng, constants_.eps0, k, ktot,
-                        res, s);
+                        res, s, part_info_int_.flag_pbc, part_info_int_.flag_nmn);
   record(host_back(u0, u_d, (size_t)d.cnt(), s));
   record(rc);
   record(check_err(s));

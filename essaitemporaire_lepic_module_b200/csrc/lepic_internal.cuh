@@ -175,9 +175,10 @@ int launch_efield(const Dims &d, const double h[3], const double *phi, double *E
                   cudaStream_t s);
 int launch_cell_wall(const Dims &d, const int *bcnd, unsigned char *cw, cudaStream_t s);
 // mg.cu
+// pbc: periodic planes in y and z (bcnd 0); nmn: Neumann plane at x = 0 (bcnd -2)
 int launch_pdesolver(const Dims &d, const double h[3], double *u, const double *b, const int *bcnd,
                      int ncycl, double eps, double omega, int ng, double eps0, int *k, double *ktot,
-                     double *res, cudaStream_t s);
+                     double *res, cudaStream_t s, int pbc = 0, int nmn = 0);
 // particles.cu
 int launch_part_mover(const lepic_grid_t &g, const double *Ei, lepic_species_f64_t &sp, int ptype,
                       int ntype, int ngrid, const lepic_phys_t &P, double *p_mac, double *P_loss,

@@ -3,7 +3,7 @@
 // red-black sweep, the residual-ratio exit test of sor_rb and the outer
 // res/alpha < eps loop run on the device; the host sees a single launch.
 //
-// Schedule (identical to the reference, one MPI rank, Dirichlet walls):
+// Schedule (identical to the reference, one MPI rank):
 //   for each V-cycle k: down leg sor_rb(level l, dig<0) + restriction,
 //   coarsest sor_rb(dig=0) (up to 1e6 sweeps in cycle 1 until res <= eps,
 //   4 afterwards) + prolongation, up leg sor_rb(dig>0) + prolongation.
@@ -18,6 +18,12 @@
 //
 // Levels with few nodes (<= SMALL_NODES) are smoothed by block 0 alone with
 // __syncthreads, avoiding grid-wide barriers on the tiny coarse grids.
+//
+// Periodic planes in y and z (bcnd 0) and the Neumann plane at x = 0
+// (bcnd -2) run in a second instance of the kernel (GEN): the node rules of
+// Src/sors.f90:113-125, the ghost-plane refresh after each colour
+// (Src/sors.f90:157-231) and the restriction's periodic wraps
+// (Src/mg.f90:314-805); the Dirichlet instance is unchanged.
 #include <cooperative_groups.h>
 
 #include "lepic_internal.cuh"
@@ -41,6 +47,7 @@ struct MGLev {
   double *b;          // (n+2)^3
   int *bc;            // (n+3)^3
   double *rf;         // (n+3)^3 fine residual scratch (levels that restrict)
+  double *rp;         // (n1+2)(n2+2) residual plane r_pbc of the last z plane (GEN)
   __device__ long long g(int i, int j, int k) const { return i + N1 * (j + N2 * (long long)k); }
   __device__ long long r(int i, int j, int k) const { return i + R1 * (j + R2 * (long long)k); }
   __device__ long long nodes() const { return (long long)(n1 + 1) * (n2 + 1) * (n3 + 1); }
@@ -49,6 +56,7 @@ struct MGLev {
 struct MGArgs {
   MGLev L[MG_MAX + 1];
   int ng, ncycl;
+  int pbc, nmn;       // periodic planes in y and z; Neumann plane at x = 0 (GEN only)
   double alpha, eps, omega;
   double *partial;    // [gridDim.x]
   double *shared_d;   // [4]: small-level results
@@ -101,7 +109,10 @@ __device__ __forceinline__ void for_rows(const Warps &w, int j0, int nj, int k0,
 }
 
 // one colour of a red-black sweep
-// colour 0 = red ((i+j+k) odd), 1 = black (Src/sors.f90:87-106, 249-267)
+// colour 0 = red ((i+j+k) odd), 1 = black (Src/sors.f90:87-106, 249-267).
+// GEN: Neumann nodes (-2) drop the west neighbour and take the east one
+// twice; periodic nodes (0) on the last y or z plane are not updated.
+template <bool GEN>
 __device__ __forceinline__ void sweep_colour(const MGLev &L, double omega, int colour, const Warps &w) {
   const int lane = threadIdx.x & 31;
   const long long sy = L.N1, sz = L.N1 * L.N2;
@@ -114,10 +125,44 @@ __device__ __forceinline__ void sweep_colour(const MGLev &L, double omega, int c
     if (is > 2) is = 1;
     for (int i = is + 2 * lane; i <= L.n1 + 1; i += 64) {
       long long q = L.g(i, j, k);
-      if (L.bc[q] > 0) continue;
+      const int bq = L.bc[q];
+      if (bq > 0) continue;
+      if (GEN) {
+        if (bq == -2) {
+          double tt = L.b[L.r(i, j, k)] - L.an * L.u[q + sy] - L.as * L.u[q - sy] - 2.0 * L.ae * L.u[q + 1] -
+                      L.at * L.u[q + sz] - L.ab * L.u[q - sz];
+          L.u[q] = (1.0 - omega) * L.u[q] + omega * tt / L.ac;
+          continue;
+        }
+        if (bq == 0 && (k == L.n3 + 1 || j == L.n2 + 1)) continue;
+      }
       double tt = L.b[L.r(i, j, k)] - L.aw * L.u[q - 1] - L.an * L.u[q + sy] - L.as * L.u[q - sy] -
                   L.ae * L.u[q + 1] - L.at * L.u[q + sz] - L.ab * L.u[q - sz];
       L.u[q] = (1.0 - omega) * L.u[q] + omega * tt / L.ac;
+    }
+  });
+}
+
+// Periodic ghost planes (Src/sors.f90:157-231), first phase: y ghosts of
+// every z plane; second phase (after a barrier): z ghosts of every y row.
+// A ghost is refreshed where the node next to it is periodic or Neumann.
+__device__ __forceinline__ void ghosts_y(const MGLev &L, const Warps &w) {
+  const int lane = threadIdx.x & 31;
+  for_rows(w, 0, 1, 0, L.n3 + 3, [&](int, int k) {
+    for (int i = lane; i <= L.n1 + 2; i += 32) {
+      const int b1 = L.bc[L.g(i, 1, k)], bn = L.bc[L.g(i, L.n2 + 1, k)];
+      if (b1 == 0 || b1 == -2) L.u[L.g(i, 0, k)] = L.u[L.g(i, L.n2, k)];
+      if (bn == 0 || bn == -2) L.u[L.g(i, L.n2 + 1, k)] = L.u[L.g(i, 1, k)];
+    }
+  });
+}
+__device__ __forceinline__ void ghosts_z(const MGLev &L, const Warps &w) {
+  const int lane = threadIdx.x & 31;
+  for_rows(w, 0, L.n2 + 3, 0, 1, [&](int j, int) {
+    for (int i = lane; i <= L.n1 + 2; i += 32) {
+      const int b1 = L.bc[L.g(i, j, 1)], bm = L.bc[L.g(i, j, L.n3 + 1)];
+      if (b1 == 0 || b1 == -2) L.u[L.g(i, j, 0)] = L.u[L.g(i, j, L.n3)];
+      if (bm == 0 || bm == -2) L.u[L.g(i, j, L.n3 + 1)] = L.u[L.g(i, j, 1)];
     }
   });
 }
@@ -141,8 +186,10 @@ __device__ __forceinline__ double residual_part(const MGLev &L, const Warps &w) 
 }
 
 // Src/sors.f90:1-535, whole grid.  Returns res, ksor (uniform in all threads).
+template <bool GEN>
 __device__ void sor_rb(const MGArgs &a, const MGLev &L, int kmg, int dig, double eps_abs,
                        cg::grid_group &grid, double *sh, double &res_out, int &ksor_out) {
+  const bool pbc = GEN && a.pbc;
   long long nr = 4;
   if (kmg == 1 && dig == 0) nr = 1000000;
   const double eta = 0.6;
@@ -152,10 +199,16 @@ __device__ void sor_rb(const MGArgs &a, const MGLev &L, int kmg, int dig, double
       int ksor = 0;
       const Warps w = block_warps();
       for (long long l = 1; l <= nr; ++l) {
-        sweep_colour(L, a.omega, 0, w);
-        __syncthreads();
-        sweep_colour(L, a.omega, 1, w);
-        __syncthreads();
+        for (int colour = 0; colour < 2; ++colour) {
+          sweep_colour<GEN>(L, a.omega, colour, w);
+          __syncthreads();
+          if (pbc) {
+            ghosts_y(L, w);
+            __syncthreads();
+            ghosts_z(L, w);
+            __syncthreads();
+          }
+        }
         res = block_sum(residual_part(L, w), sh);
         ksor++;
         bool stop = (dig == 0) ? (res <= eps_abs) : (res_s > 0.0 && (res / res_s) <= eta);
@@ -178,10 +231,16 @@ __device__ void sor_rb(const MGArgs &a, const MGLev &L, int kmg, int dig, double
   double res_s = 0.0, res = 0.0;
   int ksor = 0;
   for (long long l = 1; l <= nr; ++l) {
-    sweep_colour(L, a.omega, 0, w);
-    grid.sync();
-    sweep_colour(L, a.omega, 1, w);
-    grid.sync();
+    for (int colour = 0; colour < 2; ++colour) {
+      sweep_colour<GEN>(L, a.omega, colour, w);
+      grid.sync();
+      if (pbc) {
+        ghosts_y(L, w);
+        grid.sync();
+        ghosts_z(L, w);
+        grid.sync();
+      }
+    }
     double part = block_sum(residual_part(L, w), sh);
     if (threadIdx.x == 0) a.partial[blockIdx.x] = part;
     grid.sync();
@@ -264,6 +323,161 @@ __device__ void restriction(const MGLev &F, const MGLev &C, cg::grid_group &grid
   grid.sync();
 }
 
+// Src/mg.f90:808-847 (getres) with its Neumann form: on the plane ir = 1
+// with flag_nmn the west term is dropped (aw = uw = 0) and ae doubled.
+__device__ __forceinline__ double getres_n(const MGLev &L, long long q, double urhs, bool neumann) {
+  const long long sy = L.N1, sz = L.N1 * L.N2;
+  double uij = L.u[q], un = L.u[q + sy], us = L.u[q - sy], ue = L.u[q + 1];
+  double ut = L.u[q + sz], ub = L.u[q - sz];
+  double uw, aw = L.aw, ae = L.ae;
+  if (neumann) {
+    uw = 0.0;
+    aw = 0.0;
+    ae = 2.0 * ae;
+  } else {
+    uw = L.u[q - 1];
+  }
+  return urhs - (aw * uw + ae * ue + L.an * un + L.as * us + L.ac * uij + L.at * ut + L.ab * ub);
+}
+
+// Src/mg.f90:248-805 (restriction) with periodic planes in y and z and/or
+// the Neumann plane.  (1) the fine residual of every node 1..n+1 (no wall
+// mask: the gather tests the neighbours' bcnd as the reference does);
+// (2) with periodic planes, the residual plane r_pbc of the last fine z plane
+// as the reference's loop over coarse nodes leaves it (j outer, i inner, a
+// later write replacing an earlier one: every fine node takes the value of
+// the last coarse node that writes it); (3) the 27-point gather, where a
+// neighbour at jr-1 = 0 takes the residual of its periodic image jr = n2 in
+// the terms the reference wraps and one at kr-1 = 0 takes r_pbc.  Residuals
+// outside 1..n+1 (a wrapped term at ir+1 = n1+2) are zero.
+__device__ void restriction_gen(const MGArgs &a, const MGLev &F, const MGLev &C, cg::grid_group &grid) {
+  const Warps w = grid_warps();
+  const int lane = threadIdx.x & 31;
+  const int n1 = F.n1, n2 = F.n2, m = F.n3;
+  const bool nmn = a.nmn != 0, pbc = a.pbc != 0;
+  for_rows(w, 1, n2 + 1, 1, m + 1, [&](int j, int k) {
+    for (int i = 1 + lane; i <= n1 + 1; i += 32) {
+      long long q = F.g(i, j, k);
+      F.rf[q] = getres_n(F, q, F.b[F.r(i, j, k)], nmn && i == 1);
+    }
+  });
+  grid.sync();
+  auto G = [&](int x, int y, int z) -> double {
+    if (x < 1 || x > n1 + 1 || y < 1 || y > n2 + 1 || z < 1 || z > m + 1) return 0.0;
+    return F.rf[F.g(x, y, z)];
+  };
+  auto BC = [&](int x, int y, int z) -> int { return F.bc[F.g(x, y, z)]; };
+  const long long RP1 = n1 + 2;
+  if (pbc) {
+    for_rows(w, 1, n2 + 1, 0, 1, [&](int b, int) {
+      for (int x = 1 + lane; x <= n1 + 1; x += 32) {
+        double v = 0.0;
+        bool done = false;
+        // coarse writers of (x, b): jr, ir odd within one node, latest first
+        for (int jr = ((b + 1) & 1) ? b + 1 : b; jr >= b - 1 && !done; jr -= 2) {
+          if (jr < 1 || jr > n2 + 1) continue;
+          for (int ir = ((x + 1) & 1) ? x + 1 : x; ir >= x - 1 && !done; ir -= 2) {
+            if (ir < 1 || ir > n1 + 1) continue;
+            const int dx = x - ir, dy = b - jr;
+            const bool le = BC(ir, jr, m + 1) <= 0;
+            bool wr;
+            if (dx == -1) wr = ir != 1 && (dy == -1 ? jr != 1 : (dy == 1 ? jr != n2 + 1 : true));
+            else if (dx == 1) wr = ir != n1 + 1 && (dy == -1 ? jr != 1 : (dy == 1 ? jr != n2 + 1 : true));
+            else wr = dy == -1 ? ((le ? ir != 1 : true) && jr != 1) : (dy == 1 ? jr != n2 + 1 : true);
+            if (wr) {
+              v = le ? F.rf[F.g(x, b, m)] : 0.0;
+              done = true;
+            }
+          }
+        }
+        F.rp[x + RP1 * b] = v;
+      }
+    });
+    grid.sync();
+  }
+  auto RP = [&](int x, int y) -> double { return pbc ? F.rp[x + RP1 * y] : 0.0; };
+  for_rows(w, 0, C.n2 + 3, 0, C.n3 + 3, [&](int j, int k) {
+    for (int i = lane; i <= C.n1 + 2; i += 32) {
+      long long qc = C.g(i, j, k);
+      int bc2 = F.bc[F.g(fmap(i, F.n1), fmap(j, F.n2), fmap(k, F.n3))];
+      C.bc[qc] = bc2;
+      C.u[qc] = 0.0;
+      if (i > C.n1 + 1 || j > C.n2 + 1 || k > C.n3 + 1) continue;
+      double re = 0.0;
+      if (i >= 1 && j >= 1 && k >= 1 && bc2 <= 0) {
+        const int ir = 2 * i - 1, jr = 2 * j - 1, kr = 2 * k - 1;
+        const bool xl = ir != 1, xr = ir != n1 + 1, yl = jr != 1, yr = jr != n2 + 1, zr = kr != m + 1;
+        const bool z0 = kr == 1;
+        double r000 = G(ir, jr, kr);
+        double rpp0 = (xr && yr && BC(ir + 1, jr + 1, kr) <= 0) ? G(ir + 1, jr + 1, kr) : 0.0;
+        double rp00 = (xr && BC(ir + 1, jr, kr) <= 0) ? G(ir + 1, jr, kr) : 0.0;
+        double rpm0 = 0.0;
+        if (BC(ir + 1, jr - 1, kr) <= 0) {
+          if (xr && yl) rpm0 = G(ir + 1, jr - 1, kr);
+          else if (!yl) rpm0 = G(ir + 1, n2, kr);
+        }
+        double r0m0 = 0.0;
+        if (BC(ir, jr - 1, kr) <= 0) r0m0 = yl ? G(ir, jr - 1, kr) : G(ir, n2, kr);
+        double rmm0 = 0.0;
+        if (BC(ir - 1, jr - 1, kr) <= 0 && xl) rmm0 = yl ? G(ir - 1, jr - 1, kr) : G(ir - 1, n2, kr);
+        double rm00 = (xl && BC(ir - 1, jr, kr) <= 0) ? G(ir - 1, jr, kr) : 0.0;
+        double rmp0 = (xl && yr && BC(ir - 1, jr + 1, kr) <= 0) ? G(ir - 1, jr + 1, kr) : 0.0;
+        double r0p0 = (yr && BC(ir, jr + 1, kr) <= 0) ? G(ir, jr + 1, kr) : 0.0;
+        double r00p = (zr && BC(ir, jr, kr + 1) <= 0) ? G(ir, jr, kr + 1) : 0.0;
+        double rppp = (xr && yr && zr && BC(ir + 1, jr + 1, kr + 1) <= 0) ? G(ir + 1, jr + 1, kr + 1) : 0.0;
+        double rp0p = (xr && zr && BC(ir + 1, jr, kr + 1) <= 0) ? G(ir + 1, jr, kr + 1) : 0.0;
+        double rpmp = 0.0;
+        if (BC(ir + 1, jr - 1, kr + 1) <= 0) {
+          if (xr && yl && zr) rpmp = G(ir + 1, jr - 1, kr + 1);
+          else if (!yl && zr) rpmp = G(ir + 1, n2, kr + 1);
+        }
+        double r0mp = 0.0;
+        if (BC(ir, jr - 1, kr + 1) <= 0 && zr) r0mp = yl ? G(ir, jr - 1, kr + 1) : G(ir, n2, kr + 1);
+        double rmmp = 0.0;
+        if (BC(ir - 1, jr - 1, kr + 1) <= 0 && xl && zr)
+          rmmp = yl ? G(ir - 1, jr - 1, kr + 1) : G(ir - 1, n2, kr + 1);
+        double rm0p = (xl && zr && BC(ir - 1, jr, kr + 1) <= 0) ? G(ir - 1, jr, kr + 1) : 0.0;
+        double rmpp = (xl && yr && zr && BC(ir - 1, jr + 1, kr + 1) <= 0) ? G(ir - 1, jr + 1, kr + 1) : 0.0;
+        double r0pp = (yr && zr && BC(ir, jr + 1, kr + 1) <= 0) ? G(ir, jr + 1, kr + 1) : 0.0;
+        double r00m = 0.0;
+        if (BC(ir, jr, kr - 1) <= 0) r00m = z0 ? RP(ir, jr) : G(ir, jr, kr - 1);
+        double rppm = 0.0;
+        if (BC(ir + 1, jr + 1, kr - 1) <= 0 && xr && yr) rppm = z0 ? RP(ir + 1, jr + 1) : G(ir + 1, jr + 1, kr - 1);
+        double rp0m = 0.0;
+        if (BC(ir + 1, jr, kr - 1) <= 0 && xr) rp0m = z0 ? RP(ir + 1, jr) : G(ir + 1, jr, kr - 1);
+        double rpmm = 0.0;
+        if (BC(ir + 1, jr - 1, kr - 1) <= 0) {
+          if (z0) rpmm = (xr && yl) ? RP(ir + 1, jr - 1) : 0.0;
+          else if (yl) rpmm = xr ? G(ir + 1, jr - 1, kr - 1) : 0.0;
+          else rpmm = G(ir + 1, n2, kr - 1);
+        }
+        double r0mm = 0.0;
+        if (BC(ir, jr - 1, kr - 1) <= 0) {
+          if (z0) r0mm = yl ? RP(ir, jr - 1) : 0.0;
+          else r0mm = yl ? G(ir, jr - 1, kr - 1) : G(ir, n2, kr - 1);
+        }
+        double rmmm = 0.0;
+        if (BC(ir - 1, jr - 1, kr - 1) <= 0 && xl) {
+          if (z0) rmmm = yl ? RP(ir - 1, jr - 1) : 0.0;
+          else rmmm = yl ? G(ir - 1, jr - 1, kr - 1) : G(ir - 1, n2, kr - 1);
+        }
+        double rm0m = 0.0;
+        if (BC(ir - 1, jr, kr - 1) <= 0 && xl) rm0m = z0 ? RP(ir - 1, jr) : G(ir - 1, jr, kr - 1);
+        double rmpm = 0.0;
+        if (BC(ir - 1, jr + 1, kr - 1) <= 0 && xl && yr) rmpm = z0 ? RP(ir - 1, jr + 1) : G(ir - 1, jr + 1, kr - 1);
+        double r0pm = 0.0;
+        if (BC(ir, jr + 1, kr - 1) <= 0 && yr) r0pm = z0 ? RP(ir, jr + 1) : G(ir, jr + 1, kr - 1);
+        re = (8.0 * r000 + 4.0 * (rp00 + rm00 + r0p0 + r0m0 + r00p + r00m) +
+              2.0 * (rpp0 + rmp0 + rpm0 + rmm0 + rp0p + rm0p + r0pp + r0mp + rp0m + rm0m + r0pm + r0mm) +
+              rppp + rmpp + rpmp + rmmp + rppm + rmpm + rpmm + rmmm) /
+             64.0;
+      }
+      C.b[C.r(i, j, k)] = re;
+    }
+  });
+  grid.sync();
+}
+
 // Src/mg.f90:849-939 (prolongation): coarse C added into fine F
 __device__ void prolongation(const MGLev &F, const MGLev &C, cg::grid_group &grid) {
   const Warps w = grid_warps();
@@ -294,6 +508,7 @@ __device__ void prolongation(const MGLev &F, const MGLev &C, cg::grid_group &gri
   grid.sync();
 }
 
+template <bool GEN>
 __global__ void __launch_bounds__(MG_BLOCK) k_pdesolver(const MGArgs *__restrict__ ap) {
   cg::grid_group grid = cg::this_grid();
   const MGArgs &a = *ap;
@@ -311,16 +526,19 @@ __global__ void __launch_bounds__(MG_BLOCK) k_pdesolver(const MGArgs *__restrict
       int ksor = 0;
       if (ig < ng) {
         int il = ig;
-        sor_rb(a, a.L[il], k, ig - ng, eps_abs, grid, sh, r, ksor);
+        sor_rb<GEN>(a, a.L[il], k, ig - ng, eps_abs, grid, sh, r, ksor);
         iter[il] += ksor;
-        restriction(a.L[il], a.L[il + 1], grid);
+        if (GEN)
+          restriction_gen(a, a.L[il], a.L[il + 1], grid);
+        else
+          restriction(a.L[il], a.L[il + 1], grid);
       } else if (ig == ng) {
-        sor_rb(a, a.L[ng], k, 0, eps_abs, grid, sh, r, ksor);
+        sor_rb<GEN>(a, a.L[ng], k, 0, eps_abs, grid, sh, r, ksor);
         iter[ng] += ksor;
         if (ng >= 2) prolongation(a.L[ng - 1], a.L[ng], grid);
       } else {
         int il = 2 * ng - ig;
-        sor_rb(a, a.L[il], k, ig - ng, eps_abs, grid, sh, r, ksor);
+        sor_rb<GEN>(a, a.L[il], k, ig - ng, eps_abs, grid, sh, r, ksor);
         iter[il] += ksor;
         if (il >= 2) prolongation(a.L[il - 1], a.L[il], grid);
       }
@@ -351,8 +569,9 @@ __global__ void __launch_bounds__(MG_BLOCK) k_pdesolver(const MGArgs *__restrict
 
 int launch_pdesolver(const Dims &d, const double h[3], double *u, const double *b, const int *bcnd,
                      int ncycl, double eps, double omega, int ng, double eps0, int *k_out,
-                     double *ktot_out, double *res_out, cudaStream_t s) {
+                     double *ktot_out, double *res_out, cudaStream_t s, int pbc, int nmn) {
   if (ng < 1 || ng > MG_MAX) return LEPIC_ERR_ARG;
+  const bool gen = pbc || nmn;
   int n[3] = {d.n1, d.n2, d.n3};
   for (int a = 0; a < 3; ++a)
     if (n[a] % (1 << (ng - 1))) return LEPIC_ERR_ARG;
@@ -363,6 +582,8 @@ int launch_pdesolver(const Dims &d, const double h[3], double *u, const double *
   A.ncycl = ncycl;
   A.eps = eps;
   A.omega = omega;
+  A.pbc = pbc ? 1 : 0;
+  A.nmn = nmn ? 1 : 0;
   char nm[32];
   for (int l = 1; l <= ng; ++l) {
     MGLev &L = A.L[l];
@@ -402,12 +623,18 @@ int launch_pdesolver(const Dims &d, const double h[3], double *u, const double *
       L.rf = (double *)scratch(nm, sizeof(double) * nn);
       if (!L.rf) return LEPIC_ERR_CUDA;
       LEPIC_CUDA(cudaMemsetAsync(L.rf, 0, sizeof(double) * nn, s));
+      if (gen) {
+        snprintf(nm, sizeof nm, "mg_rp%d", l);
+        L.rp = (double *)scratch(nm, sizeof(double) * (size_t)(L.n1 + 2) * (L.n2 + 2));
+        if (!L.rp) return LEPIC_ERR_CUDA;
+      }
     }
   }
   double ac = A.L[1].ac;
   A.alpha = fabs((double)((n[0] + 1) * (n[1] + 1) * (n[2] + 1)) * ac) * 1.0;
+  void *kern = gen ? (void *)k_pdesolver<true> : (void *)k_pdesolver<false>;
   int occ = 0;
-  LEPIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pdesolver, MG_BLOCK, 0));
+  LEPIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, MG_BLOCK, 0));
   if (occ < 1) return LEPIC_ERR_CUDA;
   int blocks = c.sms * (occ < 2 ? occ : 2);
   A.partial = (double *)scratch("mg_partial", sizeof(double) * blocks);
@@ -420,7 +647,7 @@ int launch_pdesolver(const Dims &d, const double h[3], double *u, const double *
   LEPIC_CUDA(cudaMemcpyAsync(dA, &A, sizeof(MGArgs), cudaMemcpyHostToDevice, s));
   void *args[] = {&dA};
   int tm = timer_start("pdesolver_f64", s);
-  LEPIC_CUDA(cudaLaunchCooperativeKernel((void *)k_pdesolver, dim3(blocks), dim3(MG_BLOCK), args, 0, s));
+  LEPIC_CUDA(cudaLaunchCooperativeKernel(kern, dim3(blocks), dim3(MG_BLOCK), args, 0, s));
   timer_stop(tm, s);
   int hi[MG_MAX + 4];
   double hd[2];
@@ -490,7 +717,7 @@ extern "C" int lepic_dev_pdesolver_noalloc(const lepic_grid_t *g, double *u, con
   unsigned char *base = g_noalloc_ptr[dev];
   int sms = 0, occ = 0;
   LEPIC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  LEPIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pdesolver, MG_BLOCK, 0));
+  LEPIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pdesolver<false>, MG_BLOCK, 0));
   if (occ < 1 || sms < 1) return LEPIC_ERR_CUDA;
   const int blocks = sms * (occ < 2 ? occ : 2);
 
@@ -565,7 +792,7 @@ extern "C" int lepic_dev_pdesolver_noalloc(const lepic_grid_t *g, double *u, con
   for (int l = 1; l < ng; ++l) LEPIC_CUDA(cudaMemsetAsync(rf_ptr[l], 0, rf_bytes[l], s));
   LEPIC_CUDA(cudaMemcpyAsync(dA, &A, sizeof(MGArgs), cudaMemcpyHostToDevice, s));
   void *args[] = {&dA};
-  LEPIC_CUDA(cudaLaunchCooperativeKernel((void *)k_pdesolver, dim3(blocks), dim3(MG_BLOCK), args, 0, s));
+  LEPIC_CUDA(cudaLaunchCooperativeKernel((void *)k_pdesolver<false>, dim3(blocks), dim3(MG_BLOCK), args, 0, s));
   int hi[MG_MAX + 4];
   double hd[2];
   LEPIC_CUDA(cudaMemcpyAsync(hi, A.out_i, sizeof(hi), cudaMemcpyDeviceToHost, s));

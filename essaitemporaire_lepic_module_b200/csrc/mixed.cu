@@ -57,7 +57,7 @@ struct MixedConst {
   float k1;                   // dt q / (2 m)
   float kk;                   // Boris rotation factor 2 k1 / (1 + (k1 |B|)^2)
   float Bx, By, Bz;
-  int boris, flag_pbc, ngrid;
+  int boris, flag_pbc, flag_nmn, ngrid;
   double Nm, mass, kdep;      // kdep = Nm / (h1 h2 h3)
   int ntx, nty, ntiles;       // tile grid
 };
@@ -362,6 +362,19 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
       int lx, ly, lz;
       const bool wall = in_box(T, cx, cy, cz, lx, ly, lz) ? T.cw[lx + (TN - 1) * (ly + (TN - 1) * lz)] != 0
                                                           : cw[d.c(cx, cy, cz)] != 0;
+      if (c.flag_nmn == 1 && ax < 1 && !wall) {
+        // specular reflection at the Neumann plane x = 0 (Src/part_expmover.f90:
+        // 437-446): x = (ax - 1 + fx) h < 0 becomes -x, vx changes sign
+        const float g = 1.f - fx;
+        ax = 1 - ax;
+        if (g >= 1.f) {
+          fx = 0.f;
+          ax += 1;
+        } else {
+          fx = g;
+        }
+        vx = -vx;
+      }
       lost = wall || ax < 1 || ax > n1 || ay < 1 || ay > n2 || az < 1 || az > n3;
     }
     if (lost) {
@@ -861,7 +874,6 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
                               int n_hint, cudaStream_t s) {
   Dims d(g.n);
   const int p = ptype - 1;
-  if (P.flag_nmn) return LEPIC_ERR_UNSUPPORTED;
   if (!sp.flag_dead || !aligned16(E4)) return LEPIC_ERR_ARG;
   if (int rc = check_layout(g, sp)) return rc;
   MixedConst c;
@@ -881,6 +893,7 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
   c.boris = (P.flag_B == 1) ? 1 : 0;
   if (P.flag_B_pos == 1 && P.charge[p] > 0.0) c.boris = 0;
   c.flag_pbc = P.flag_pbc;
+  c.flag_nmn = P.flag_nmn;
   c.ngrid = ngrid;
   c.Nm = P.Nm[p];
   c.mass = P.mass[p];

@@ -348,7 +348,10 @@ class Simulation:
                                        self.st.ntype, C.byref(self.P), self._s()), "calc_rho")
 
     def pdesolver(self, eps=None, omega=None, ng=None, ncycl=None):
-        if self.mixed:
+        # the FP32 V-cycles cover Dirichlet walls; with periodic planes or the
+        # Neumann plane the mixed form solves with the FP64 multigrid
+        g = self.st.geom
+        if self.mixed and not (g.flag_pbc or g.flag_nmn):
             return self.pdesolver_mixed(eps=eps, ng=ng)
         wl = self.st.wl
         k = C.c_int(0)

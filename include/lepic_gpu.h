@@ -314,7 +314,9 @@ int lepic_dev_calc_efield(const lepic_grid_t *g, const double *phi, double *Ei, 
 
 /* Src/pdesolver.f90:1 as one persistent cooperative kernel (all V-cycles,
  * all levels, no host round trips).  u: (n+3)^3 device potential (z from 0),
- * b: (n+2)^3.  Blocks until done; k/ktot/res returned like the reference. */
+ * b: (n+2)^3.  Blocks until done; k/ktot/res returned like the reference.
+ * P->flag_pbc: periodic planes in y and z (bcnd 0); P->flag_nmn: the Neumann
+ * plane at x = 0 (bcnd -2), as Src/sors.f90 and Src/mg.f90 treat them. */
 int lepic_dev_pdesolver(const lepic_grid_t *g, double *u, const double *b, int ncycl, double eps,
                         double omega, int ng, const lepic_phys_t *P, int *k, double *ktot,
                         double *res, void *stream);
@@ -332,7 +334,8 @@ int lepic_dev_pdesolver(const lepic_grid_t *g, double *u, const double *b, int n
  * stream capture.  All calls share the array and it keeps the last call's
  * contents (what must start at zero is cleared per call); calls that overlap
  * on the GPU, on any stream, race.  u, b and g->bcnd are the caller's device
- * buffers exactly as for lepic_dev_pdesolver. */
+ * buffers exactly as for lepic_dev_pdesolver; Dirichlet walls only (periodic
+ * or Neumann planes return LEPIC_ERR_UNSUPPORTED). */
 int lepic_dev_pdesolver_noalloc(const lepic_grid_t *g, double *u, const double *b, int ncycl,
                                 double eps, double omega, int ng, const lepic_phys_t *P, int *k,
                                 double *ktot, double *res, void *stream);
@@ -389,7 +392,8 @@ int lepic_dev_f64_to_mixed(const lepic_grid_t *g, const lepic_species_f64_t *in,
 int lepic_dev_mixed_to_f64(const lepic_grid_t *g, const lepic_species_mixed_t *in, double *out,
                            long long capout, long long n, void *stream);
 /* Mixed-precision Poisson solve for the operator of Src/pdesolver.f90:1
- * (Dirichlet walls): FP64 residual r = b - A u, FP32 multigrid V-cycle on
+ * (Dirichlet walls; periodic or Neumann planes return LEPIC_ERR_UNSUPPORTED):
+ * FP64 residual r = b - A u, FP32 multigrid V-cycle on
  * A e = r (red-black sweeps: nu_fine_pre / nu_fine_post on the finest level,
  * nu_pre / nu_post on the coarser ones, coarse_sweeps on the coarsest), u += e
  * in FP64, until sum|r| / alpha < eps, with the sum over plasma nodes and the

@@ -275,8 +275,8 @@ void oracle_dens_red(const int n[3], const double *np, double *np_red, const int
 }
 
 // ---------------------------------------------------------------------------
-// Multigrid: Src/pdesolver.f90, Src/mg.f90, Src/sors.f90 (Dirichlet walls;
-// periodic and Neumann planes are rejected).
+// Multigrid: Src/pdesolver.f90, Src/mg.f90, Src/sors.f90 (Dirichlet walls,
+// periodic planes in y and z, the left-hand Neumann plane in x).
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -288,9 +288,34 @@ struct Level {
   std::vector<int> bc;     // (n+3)^3
 };
 
-// Src/sors.f90:1-535 (sor_rb) for one rank.
+// Src/sors.f90:157-231 (one rank): after each colour the periodic ghost
+// planes are refreshed, first in y for every z plane, then in z for every y
+// row, where the node next to the ghost is periodic (0) or Neumann (-2).
+void pbc_ghosts(double *u, const int *bcnd, const Dims &d) {
+  const int m = d.n3;
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k <= m + 2; ++k)
+    for (int i = 0; i <= d.n1 + 2; ++i) {
+      const int b1 = bcnd[d.g(i, 1, k)], bn = bcnd[d.g(i, d.n2 + 1, k)];
+      if (b1 == 0 || b1 == -2) u[d.g(i, 0, k)] = u[d.g(i, d.n2, k)];
+      if (bn == 0 || bn == -2) u[d.g(i, d.n2 + 1, k)] = u[d.g(i, 1, k)];
+    }
+#pragma omp parallel for schedule(static)
+  for (int j = 0; j <= d.n2 + 2; ++j)
+    for (int i = 0; i <= d.n1 + 2; ++i) {
+      const int b1 = bcnd[d.g(i, j, 1)], bm = bcnd[d.g(i, j, m + 1)];
+      if (b1 == 0 || b1 == -2) u[d.g(i, j, 0)] = u[d.g(i, j, m)];
+      if (bm == 0 || bm == -2) u[d.g(i, j, m + 1)] = u[d.g(i, j, 1)];
+    }
+}
+
+// Src/sors.f90:1-535 (sor_rb) for one rank.  Node kinds (Src/sors.f90:
+// 113-125): Neumann nodes (-2) drop the west neighbour and take the east one
+// twice; periodic nodes (0) on the last plane in y or z are not updated
+// (their ghost copies are); pbc: refresh the ghost planes after each colour.
 void sor_rb(double *u, const double *b, const double h[3], const int *bcnd, double *res_out,
-            const int n[3], double omega, double eps, int *ksor, int kmg, int dig, double eps0) {
+            const int n[3], double omega, double eps, int *ksor, int kmg, int dig, double eps0,
+            int pbc) {
   Dims d(n);
   Coef c(h, eps0);
   double res_s = 0.0, res = 0.0;
@@ -314,12 +339,20 @@ void sor_rb(double *u, const double *b, const double h[3], const int *bcnd, doub
           for (int i = is; i <= d.n1 + 1; i += 2) {
             long q = d.g(i, j, k);
             if (bcnd[q] > 0) continue;
+            if (bcnd[q] == -2) {
+              double t = b[d.r(i, j, k)] - c.an * u[q + d.N1] - c.as * u[q - d.N1] -
+                         2.0 * c.ae * u[q + 1] - c.at * u[q + d.N1 * d.N2] - c.ab * u[q - d.N1 * d.N2];
+              u[q] = (1.0 - omega) * u[q] + omega * t / c.ac;
+              continue;
+            }
+            if (bcnd[q] == 0 && (k == m + 1 || j == d.n2 + 1)) continue;
             double t = b[d.r(i, j, k)] - c.aw * u[q - 1] - c.an * u[q + d.N1] -
                        c.as * u[q - d.N1] - c.ae * u[q + 1] - c.at * u[q + d.N1 * d.N2] -
                        c.ab * u[q - d.N1 * d.N2];
             u[q] = (1.0 - omega) * u[q] + omega * t / c.ac;
           }
         }
+      if (pbc) pbc_ghosts(u, bcnd, d);
     }
     res = 0.0;
     for (int k = 1; k <= m + 1; ++k)
@@ -352,6 +385,159 @@ inline double getres(const double *u, const double *b, const Coef &c, const Dims
   double ut = u[q + d.N1 * d.N2], ub = u[q - d.N1 * d.N2], uw = u[q - 1];
   double urhs = b[d.r(ir, jr, kr)];
   return urhs - (c.aw * uw + c.ae * ue + c.an * un + c.as * us + c.ac * uij + c.at * ut + c.ab * ub);
+}
+
+// Src/mg.f90:808-847 (getres) with its Neumann form: on the plane ir = 1
+// with flag_nmn the west term is dropped (aw = uw = 0) and ae doubled.
+inline double getres_n(const double *u, const double *b, const Coef &c, const Dims &d, int ir, int jr,
+                       int kr, int nmn) {
+  long q = d.g(ir, jr, kr);
+  double uij = u[q], un = u[q + d.N1], us = u[q - d.N1], ue = u[q + 1];
+  double ut = u[q + d.N1 * d.N2], ub = u[q - d.N1 * d.N2];
+  double uw, aw = c.aw, ae = c.ae;
+  if (ir == 1 && nmn == 1) {
+    uw = 0.0;
+    aw = 0.0;
+    ae = 2.0 * ae;
+  } else {
+    uw = u[q - 1];
+  }
+  double urhs = b[d.r(ir, jr, kr)];
+  return urhs - (aw * uw + ae * ue + c.an * un + c.as * us + c.ac * uij + c.at * ut + c.ab * ub);
+}
+
+// Src/mg.f90:248-805 (restriction) for one rank with periodic planes in y
+// and z and/or the Neumann plane.  Beyond the Dirichlet form: a neighbour at
+// jr-1 = 0 takes the residual of its periodic image jr = n2 in the terms the
+// reference wraps, and the neighbours at kr-1 = 0 take the residual plane
+// r_pbc of the last fine plane kr = n3 (Src/mg.f90:314-389), which the
+// reference fills coarse node by coarse node (j outer, i inner), a later
+// write replacing an earlier one; r_pbc is zero without periodic planes
+// (the reference leaves it unset).  A wrapped term at ir+1 = n1+2 (outside
+// the residual's grid) is zero.
+void restriction_gen(const double *u, const double *b, const double h[3], const int *bcnd, int *bcnd2h,
+                     double *r2h, double *e2h, const int n[3], double eps0, int pbc, int nmn) {
+  Dims d(n);
+  int nc[3] = {n[0] / 2, n[1] / 2, n[2] / 2};
+  Dims dc(nc);
+  Coef c(h, eps0);
+  const int n1 = n[0], n2 = n[1], m = n[2];
+  auto fmap = [](int ic, int ncell) { return ic == ncell / 2 + 2 ? ncell + 2 : (ic == 0 ? 0 : 2 * ic - 1); };
+  for (int k = 0; k <= nc[2] + 2; ++k)
+    for (int j = 0; j <= nc[1] + 2; ++j)
+      for (int i = 0; i <= nc[0] + 2; ++i)
+        bcnd2h[dc.g(i, j, k)] = bcnd[d.g(fmap(i, n[0]), fmap(j, n[1]), fmap(k, n[2]))];
+  for (long q = 0; q < dc.cnt(); ++q) e2h[q] = 0.0;
+  for (long q = 0; q < dc.rcnt(); ++q) r2h[q] = 0.0;
+  auto G = [&](int a, int bb, int cc) -> double {
+    if (a < 1 || a > n1 + 1 || bb < 1 || bb > n2 + 1 || cc < 1 || cc > m + 1) return 0.0;
+    return getres_n(u, b, c, d, a, bb, cc, nmn);
+  };
+  auto BC = [&](int a, int bb, int cc) { return bcnd[d.g(a, bb, cc)]; };
+  // r_pbc(1:n1+1, 1:n2+1), serial order of the reference's loop
+  std::vector<double> rp((size_t)(n1 + 2) * (n2 + 2), 0.0);
+  auto RP = [&](int a, int bb) -> double & { return rp[(size_t)a + (size_t)(n1 + 2) * bb]; };
+  if (pbc) {
+    for (int j = 1; j <= n2 / 2 + 1; ++j)
+      for (int i = 1; i <= n1 / 2 + 1; ++i) {
+        const int ir = 2 * i - 1, jr = 2 * j - 1;
+        if (BC(ir, jr, m + 1) <= 0) {
+          if (ir != 1 && jr != 1) RP(ir - 1, jr - 1) = G(ir - 1, jr - 1, m);
+          if (ir != 1) RP(ir - 1, jr) = G(ir - 1, jr, m);
+          if (ir != 1 && jr != n2 + 1) RP(ir - 1, jr + 1) = G(ir - 1, jr + 1, m);
+          if (ir != 1 && jr != 1) RP(ir, jr - 1) = G(ir, jr - 1, m);
+          RP(ir, jr) = G(ir, jr, m);
+          if (jr != n2 + 1) RP(ir, jr + 1) = G(ir, jr + 1, m);
+          if (ir != n1 + 1 && jr != 1) RP(ir + 1, jr - 1) = G(ir + 1, jr - 1, m);
+          if (ir != n1 + 1) RP(ir + 1, jr) = G(ir + 1, jr, m);
+          if (ir != n1 + 1 && jr != n2 + 1) RP(ir + 1, jr + 1) = G(ir + 1, jr + 1, m);
+        } else {
+          if (ir != 1 && jr != 1) RP(ir - 1, jr - 1) = 0.0;
+          if (ir != 1) RP(ir - 1, jr) = 0.0;
+          if (ir != 1 && jr != n2 + 1) RP(ir - 1, jr + 1) = 0.0;
+          if (jr != 1) RP(ir, jr - 1) = 0.0;
+          RP(ir, jr) = 0.0;
+          if (jr != n2 + 1) RP(ir, jr + 1) = 0.0;
+          if (ir != n1 + 1 && jr != 1) RP(ir + 1, jr - 1) = 0.0;
+          if (ir != n1 + 1) RP(ir + 1, jr) = 0.0;
+          if (ir != n1 + 1 && jr != n2 + 1) RP(ir + 1, jr + 1) = 0.0;
+        }
+      }
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= nc[2] + 1; ++k)
+    for (int j = 1; j <= nc[1] + 1; ++j)
+      for (int i = 1; i <= nc[0] + 1; ++i) {
+        const int ir = 2 * i - 1, jr = 2 * j - 1, kr = 2 * k - 1;
+        if (bcnd2h[dc.g(i, j, k)] > 0) continue;
+        const bool xl = ir != 1, xr = ir != n1 + 1, yl = jr != 1, yr = jr != n2 + 1, zr = kr != m + 1;
+        const bool z0 = kr == 1;
+        double r000 = G(ir, jr, kr);
+        double rpp0 = (xr && yr && BC(ir + 1, jr + 1, kr) <= 0) ? G(ir + 1, jr + 1, kr) : 0.0;
+        double rp00 = (xr && BC(ir + 1, jr, kr) <= 0) ? G(ir + 1, jr, kr) : 0.0;
+        double rpm0 = 0.0;
+        if (BC(ir + 1, jr - 1, kr) <= 0) {
+          if (xr && yl) rpm0 = G(ir + 1, jr - 1, kr);
+          else if (!yl) rpm0 = G(ir + 1, n2, kr);
+        }
+        double r0m0 = 0.0;
+        if (BC(ir, jr - 1, kr) <= 0) r0m0 = yl ? G(ir, jr - 1, kr) : G(ir, n2, kr);
+        double rmm0 = 0.0;
+        if (BC(ir - 1, jr - 1, kr) <= 0 && xl) rmm0 = yl ? G(ir - 1, jr - 1, kr) : G(ir - 1, n2, kr);
+        double rm00 = (xl && BC(ir - 1, jr, kr) <= 0) ? G(ir - 1, jr, kr) : 0.0;
+        double rmp0 = (xl && yr && BC(ir - 1, jr + 1, kr) <= 0) ? G(ir - 1, jr + 1, kr) : 0.0;
+        double r0p0 = (yr && BC(ir, jr + 1, kr) <= 0) ? G(ir, jr + 1, kr) : 0.0;
+        double r00p = (zr && BC(ir, jr, kr + 1) <= 0) ? G(ir, jr, kr + 1) : 0.0;
+        double rppp = (xr && yr && zr && BC(ir + 1, jr + 1, kr + 1) <= 0) ? G(ir + 1, jr + 1, kr + 1) : 0.0;
+        double rp0p = (xr && zr && BC(ir + 1, jr, kr + 1) <= 0) ? G(ir + 1, jr, kr + 1) : 0.0;
+        double rpmp = 0.0;
+        if (BC(ir + 1, jr - 1, kr + 1) <= 0) {
+          if (xr && yl && zr) rpmp = G(ir + 1, jr - 1, kr + 1);
+          else if (!yl && zr) rpmp = G(ir + 1, n2, kr + 1);
+        }
+        double r0mp = 0.0;
+        if (BC(ir, jr - 1, kr + 1) <= 0 && zr) r0mp = yl ? G(ir, jr - 1, kr + 1) : G(ir, n2, kr + 1);
+        double rmmp = 0.0;
+        if (BC(ir - 1, jr - 1, kr + 1) <= 0 && xl && zr)
+          rmmp = yl ? G(ir - 1, jr - 1, kr + 1) : G(ir - 1, n2, kr + 1);
+        double rm0p = (xl && zr && BC(ir - 1, jr, kr + 1) <= 0) ? G(ir - 1, jr, kr + 1) : 0.0;
+        double rmpp = (xl && yr && zr && BC(ir - 1, jr + 1, kr + 1) <= 0) ? G(ir - 1, jr + 1, kr + 1) : 0.0;
+        double r0pp = (yr && zr && BC(ir, jr + 1, kr + 1) <= 0) ? G(ir, jr + 1, kr + 1) : 0.0;
+        double r00m = 0.0;
+        if (BC(ir, jr, kr - 1) <= 0) r00m = z0 ? RP(ir, jr) : G(ir, jr, kr - 1);
+        double rppm = 0.0;
+        if (BC(ir + 1, jr + 1, kr - 1) <= 0 && xr && yr) rppm = z0 ? RP(ir + 1, jr + 1) : G(ir + 1, jr + 1, kr - 1);
+        double rp0m = 0.0;
+        if (BC(ir + 1, jr, kr - 1) <= 0 && xr) rp0m = z0 ? RP(ir + 1, jr) : G(ir + 1, jr, kr - 1);
+        double rpmm = 0.0;
+        if (BC(ir + 1, jr - 1, kr - 1) <= 0) {
+          if (z0) rpmm = (xr && yl) ? RP(ir + 1, jr - 1) : 0.0;
+          else if (yl) rpmm = xr ? G(ir + 1, jr - 1, kr - 1) : 0.0;
+          else rpmm = G(ir + 1, n2, kr - 1);
+        }
+        double r0mm = 0.0;
+        if (BC(ir, jr - 1, kr - 1) <= 0) {
+          if (z0) r0mm = yl ? RP(ir, jr - 1) : 0.0;
+          else r0mm = yl ? G(ir, jr - 1, kr - 1) : G(ir, n2, kr - 1);
+        }
+        double rmmm = 0.0;
+        if (BC(ir - 1, jr - 1, kr - 1) <= 0 && xl) {
+          if (z0) rmmm = yl ? RP(ir - 1, jr - 1) : 0.0;
+          else rmmm = yl ? G(ir - 1, jr - 1, kr - 1) : G(ir - 1, n2, kr - 1);
+        }
+        double rm0m = 0.0;
+        if (BC(ir - 1, jr, kr - 1) <= 0 && xl) rm0m = z0 ? RP(ir - 1, jr) : G(ir - 1, jr, kr - 1);
+        double rmpm = 0.0;
+        if (BC(ir - 1, jr + 1, kr - 1) <= 0 && xl && yr) rmpm = z0 ? RP(ir - 1, jr + 1) : G(ir - 1, jr + 1, kr - 1);
+        double r0pm = 0.0;
+        if (BC(ir, jr + 1, kr - 1) <= 0 && yr) r0pm = z0 ? RP(ir, jr + 1) : G(ir, jr + 1, kr - 1);
+        double re = (8.0 * r000 + 4.0 * (rp00 + rm00 + r0p0 + r0m0 + r00p + r00m) +
+                     2.0 * (rpp0 + rmp0 + rpm0 + rmm0 + rp0p + rm0p + r0pp + r0mp + rp0m + rm0m +
+                            r0pm + r0mm) +
+                     rppp + rmpp + rpmp + rmmp + rppm + rmpm + rpmm + rmmm) /
+                    64.0;
+        r2h[dc.r(i, j, k)] = re;
+      }
 }
 
 // Src/mg.f90:248-805 (restriction) for one rank, no periodic planes.
@@ -446,12 +632,13 @@ void prolongation(double *u, const double *e2h, const int *bcnd, const int n[3])
 // u: (n+3)^3 potential with Dirichlet values on wall nodes (updated in place,
 // warm start); b: (n+2)^3 right-hand side (-rho).  Returns 0, or
 // ORACLE_ERR_DIVERGED when the residual grows by more than 10x (the
-// reference's stop_calculation), or ORACLE_ERR_UNSUPPORTED for periodic /
-// Neumann planes.  *k = number of V-cycles + 1 (the reference's exit value).
+// reference's stop_calculation).  *k = number of V-cycles + 1 (the
+// reference's exit value).  P->flag_pbc: periodic planes in y and z;
+// P->flag_nmn: the Neumann plane at x = 0.
 int oracle_pdesolver(double *u, const double *b, const int *bcnd, const double h[3], const int n[3],
                      int ncycl, double eps, double omega, int *k, double *ktot, double *res, int ng,
                      const OPhys *P) {
-  if (P->flag_pbc || P->flag_nmn) return ORACLE_ERR_UNSUPPORTED;
+  const int pbc = P->flag_pbc ? 1 : 0, nmn = P->flag_nmn ? 1 : 0;
   Coef c0(h, P->eps0);
   const double u0 = 1.0;
   double alpha = std::fabs((double)((n[0] + 1) * (n[1] + 1) * (n[2] + 1)) * c0.ac) * u0;
@@ -484,18 +671,22 @@ int oracle_pdesolver(double *u, const double *b, const int *bcnd, const double h
     for (int ig = 1; ig <= 2 * ng - 1; ++ig) {
       if (ig < ng) {
         int il = ig;
-        sor_rb(U(il), B(il), L[il].h, BC(il), &r, L[il].n, omega, eps_abs, &ksor, *k, ig - ng, P->eps0);
+        sor_rb(U(il), B(il), L[il].h, BC(il), &r, L[il].n, omega, eps_abs, &ksor, *k, ig - ng, P->eps0, pbc);
         iter[il] += ksor;
-        restriction(U(il), B(il), L[il].h, BC(il), L[il + 1].bc.data(), L[il + 1].r.data(),
-                    L[il + 1].e.data(), L[il].n, P->eps0);
+        if (pbc || nmn)
+          restriction_gen(U(il), B(il), L[il].h, BC(il), L[il + 1].bc.data(), L[il + 1].r.data(),
+                          L[il + 1].e.data(), L[il].n, P->eps0, pbc, nmn);
+        else
+          restriction(U(il), B(il), L[il].h, BC(il), L[il + 1].bc.data(), L[il + 1].r.data(),
+                      L[il + 1].e.data(), L[il].n, P->eps0);
       } else if (ig == ng) {
         int il = ng;
-        sor_rb(U(il), B(il), L[il].h, BC(il), &r, L[il].n, omega, eps_abs, &ksor, *k, 0, P->eps0);
+        sor_rb(U(il), B(il), L[il].h, BC(il), &r, L[il].n, omega, eps_abs, &ksor, *k, 0, P->eps0, pbc);
         iter[il] += ksor;
         if (ng >= 2) prolongation(U(il - 1), U(il), BC(il - 1), L[il - 1].n);
       } else {
         int il = 2 * ng - ig;
-        sor_rb(U(il), B(il), L[il].h, BC(il), &r, L[il].n, omega, eps_abs, &ksor, *k, ig - ng, P->eps0);
+        sor_rb(U(il), B(il), L[il].h, BC(il), &r, L[il].n, omega, eps_abs, &ksor, *k, ig - ng, P->eps0, pbc);
         iter[il] += ksor;
         if (il >= 2) prolongation(U(il - 1), U(il), BC(il - 1), L[il - 1].n);
       }

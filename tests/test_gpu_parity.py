@@ -62,9 +62,11 @@ def test_calc_rho_bit_exact(box16):
     np.testing.assert_array_equal(r_g, r_o)
 
 
-@pytest.mark.parametrize("name", ["box16", "box32", "poisson32", "penning_small"])
+@pytest.mark.parametrize("name", ["box16", "box32", "poisson32", "penning_small", "pbc16", "nmn16"])
 def test_pdesolver_matches_oracle(name):
-    """Same schedule (V-cycles, sweeps per level) and phi to <= 1e-12."""
+    """Same schedule (V-cycles, sweeps per level) and phi to <= 1e-12
+    (pbc16: periodic planes in y and z; nmn16: the Neumann plane at x = 0
+    as well)."""
     st = config.build(name)
     dropin.set_commons(st)
     if st.rhs_blobs is not None:

@@ -219,3 +219,66 @@ def test_ordering_python_matches_c():
     np.testing.assert_allclose(T.sigv_mx, sv, rtol=1e-15, atol=0)
     np.testing.assert_array_equal(T.sig_list, sl)
     np.testing.assert_array_equal(T.p_ncol, pn)
+
+
+def _periodic_profile(n, m):
+    """A function of the node index that is periodic with period n (node 1 and
+    node n + 1 coincide, ghost 0 is node n)."""
+    j = np.arange(n + 3) - 1.0
+    return m[0] + np.cos(2 * np.pi * j / n) + m[1] * np.sin(4 * np.pi * j / n)
+
+
+def test_pdesolver_periodic_manufactured_solution():
+    """Walls at both x ends, periodic planes in y and z (Src/sors.f90:113-231,
+    Src/mg.f90:314-805): phi_exact periodic in y and z with phi = 0 on the
+    walls, b = A phi_exact; the multigrid returns phi_exact on every
+    unknown node and on the periodic ghosts."""
+    st = config.build("pbc16")
+    n1, n2, n3 = st.n
+    x = np.arange(n1 + 3) - 1.0
+    fx = np.sin(np.pi * x / n1)
+    fx[0] = fx[-1] = 0.0
+    ex = (_periodic_profile(n3, (0.5, 0.3))[:, None, None] * _periodic_profile(n2, (0.2, -0.4))[None, :, None] *
+          fx[None, None, :] * 3.0)
+    # the unknowns and the ghost planes the solver refreshes (y and z indices
+    # 0..n+1; the outer ghosts n+2 are not read)
+    unknown = st.geom.bcnd <= 0
+    unknown[n3 + 2, :, :] = False
+    unknown[:, n2 + 2, :] = False
+    ex = np.where(st.geom.bcnd >= 1, 0.0, ex)
+    b = np.ascontiguousarray(_apply_A(ex, st)[:n3 + 2, :n2 + 2, :n1 + 2])
+    phi = np.zeros_like(ex)
+    k, ktot, res = oracle.pdesolver(st, phi, b, eps=1e-12)
+    assert res < 1e-12
+    assert np.abs(np.where(unknown, phi - ex, 0.0)).max() <= 1e-8 * np.abs(ex).max()
+    # walls keep their Dirichlet value
+    assert not np.where(st.geom.bcnd >= 1, phi, 0.0).any()
+
+
+def test_pdesolver_neumann_plane_is_the_mirror_of_the_full_box():
+    """The Neumann plane at x = 0 (Src/sors.f90:113-117, getres at ir = 1,
+    Src/mg.f90:826-832) makes the half box the mirror image of a box twice as
+    long in x with the source reflected about its middle plane: the two
+    solutions agree on the half box (periodic planes in y and z in both)."""
+    half = config.build("nmn16")
+    full = config.build("pbc32x16")
+    n1, n2, n3 = half.n
+    x = np.arange(n1 + 2) - 1.0
+    src = (np.exp(-(x ** 2) / (2 * 5.0 ** 2))[None, None, :] *
+           _periodic_profile(n2, (1.5, 0.3))[None, :n2 + 2, None] *
+           _periodic_profile(n3, (2.0, -0.2))[:n3 + 2, None, None]) * (-1.6e-19 * 1e15)
+    b_half = np.ascontiguousarray(src)
+    b_full = np.zeros((n3 + 2, n2 + 2, 2 * n1 + 2))
+    for ip in range(1, 2 * n1 + 2):             # full node ip <-> half node |ip - (n1+1)| + 1
+        b_full[:, :, ip] = src[:, :, abs(ip - (n1 + 1)) + 1]
+    phi_h = half.geom.phi.copy()
+    phi_f = full.geom.phi.copy()
+    oracle.pdesolver(half, phi_h, b_half, eps=1e-13)
+    oracle.pdesolver(full, phi_f, b_full, eps=1e-13)
+    mirror = phi_f[:, :, n1 + 1:2 * n1 + 2]       # full x nodes n1+1..2 n1+1 = half nodes 1..n1+1
+    mine = phi_h[:, :, 1:n1 + 2]
+    unknown = half.geom.bcnd[:, :, 1:n1 + 2] <= 0
+    unknown[n3 + 2, :, :] = False
+    unknown[:, n2 + 2, :] = False
+    assert np.abs(np.where(unknown, mine - mirror, 0.0)).max() <= 1e-7 * np.abs(mirror).max()
+    assert np.abs(mirror).max() > 0
