@@ -53,6 +53,12 @@ class LepicSpeciesMixed(C.Structure):
                 ("tile_off", C.c_void_p), ("cap", C.c_int)]
 
 
+class LepicHeat(C.Structure):
+    """lepic_heat_t: electron heating region and rate."""
+    _fields_ = [("ixl_pow", C.c_int), ("ixr_pow", C.c_int), ("flag_circxh", C.c_int), ("flag_ahp", C.c_int),
+                ("R_ahp", C.c_double), ("nudt", C.c_double), ("Pabs", C.c_double), ("nu_h", C.c_double)]
+
+
 class LepicTables(C.Structure):
     _fields_ = [("ncol", C.c_int), ("npt", C.c_int), ("npt_mx", C.c_int),
                 ("sig_Er", C.c_void_p), ("sig", C.c_void_p), ("sig_Eth", C.c_void_p),
@@ -172,6 +178,16 @@ def lib():
         "lepic_dev_adj_walls": ([C.POINTER(LepicGrid), C.POINTER(LepicPhys), _I, vp, vp, vp, vp, _I, vp], _I),
         "lepic_dev_adj_deposit": ([C.POINTER(LepicGrid), vp, _I, _I, vp, vp, vp, _I, _I, C.POINTER(LepicPhys),
                                    vp], _I),
+        "lepic_dev_eheating": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64), C.POINTER(LepicPhys),
+                               C.POINTER(LepicHeat), C.c_double, vp, C.c_ulonglong, C.c_ulonglong, vp, vp], _I),
+        "lepic_dev_eheating_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), C.POINTER(LepicPhys),
+                                     C.POINTER(LepicHeat), C.c_double, vp, C.c_ulonglong, C.c_ulonglong, vp,
+                                     vp], _I),
+        "lepic_dev_heat_stats": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64), C.POINTER(LepicPhys),
+                                  C.POINTER(LepicHeat), vp, vp], _I),
+        "lepic_dev_heat_stats_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), C.POINTER(LepicPhys),
+                                        C.POINTER(LepicHeat), vp, vp], _I),
+        "eheating_": ([P_dbl, P_dbl, P_int, P_int, P_int, P_int, P_int, P_dbl, P_int, P_dbl], None),
         "lepic_dev_load_uniform": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64), _I,
                                     C.c_longlong, C.POINTER(LepicPhys), C.c_ulonglong, vp], _I),
         "lepic_dev_cell_wall": ([P_int, vp, vp, vp], _I),
@@ -230,7 +246,8 @@ def exported_symbols():
             "lepic_dev_adj_rhs", "lepic_dev_adj_walls", "lepic_dev_adj_deposit", "lepic_dev_cell_wall",
             "lepic_dev_dens_red", "lepic_timing_enable", "lepic_timing_reset", "lepic_timing_read",
             "calc_rho_", "dens_red_", "pdesolver_", "calc_efield_",
-            "part_mover_", "charge_deposition_", "part_sorting_", "collisions_",
+            "part_mover_", "charge_deposition_", "part_sorting_", "collisions_", "eheating_",
+            "lepic_dev_eheating", "lepic_dev_eheating_mixed", "lepic_dev_heat_stats", "lepic_dev_heat_stats_mixed",
             "part_info_int_", "part_info_dp_1_", "part_info_dp_2_", "part_info_dp_3_", "constants_"]
 
 

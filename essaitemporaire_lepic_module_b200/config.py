@@ -167,6 +167,41 @@ class Setup:
         return int(round(float(np.float32(self.np_cell * self.n_cell))))
 
 
+@dataclass
+class Heating:
+    """Maxwellian electron heating (Src/read_input.f90:37, 72-74): the region
+    xl_pow..xr_pow in x (m), the absorbed power Pabs (W; <= 0: no
+    self-consistent temperature, the heating speed stays vt0 of the
+    electrons) and the heating frequency nu_h (1/s; < 0: no heating); with
+    flag_circxh the region is also limited to r <= R_ahp (flag_ahp = 0) or
+    r >= R_ahp (flag_ahp = 1) about the box axis."""
+    xl_pow: float
+    xr_pow: float
+    Pabs: float = -1.0
+    nu_h: float = 1.0e7
+    flag_circxh: int = 0
+    flag_ahp: int = 0
+    R_ahp: float = 0.0
+    flag_inj: int = 0
+
+
+def heating_params(st, hz):
+    """What Src/main.f90 derives from the heating input: ns_heat from
+    kt = dt vt0(1) / min(h) (:548-554), nudt = nu_h ns_heat dt (:564), the
+    cell range ixl_pow..ixr_pow (:610-614) and flag_heat (nu_h >= 0)."""
+    kt = st.dt * st.vt0[0] / float(min(st.h))
+    ns_heat = 4
+    if 0.05 <= kt < 0.1:
+        ns_heat = 20
+    if kt < 0.05:
+        ns_heat = 40
+    xmax = float(st.geom.box[0])
+    xr = min(hz.xr_pow, xmax)
+    xl = max(hz.xl_pow, 0.0)
+    return dict(ns_heat=ns_heat, nudt=hz.nu_h * ns_heat * st.dt, ixl_pow=int(xl / st.h[0]) + 1,
+                ixr_pow=int(xr / st.h[0]) + 1, flag_heat=0 if hz.nu_h < 0 else 1)
+
+
 def mg_levels(n, ng_default):
     a = [math.log10(float(np.float32(v))) / math.log10(2.0) for v in n]
     if all(abs(round(x) - x) <= 1e-3 for x in a):

@@ -59,6 +59,24 @@ lepic_phys_t phys_from_common(int ntype) {
   return P;
 }
 
+// LEPIC_OK or the status of a failed runtime call
+int cuda_ok(cudaError_t e, const char *what) { return e == cudaSuccess ? LEPIC_OK : cuda_status(e, what); }
+
+// heating region and rate from the COMMON blocks
+lepic_heat_t heat_from_common() {
+  lepic_heat_t H;
+  memset(&H, 0, sizeof(H));
+  H.ixl_pow = part_info_int_.ixl_pow;
+  H.ixr_pow = part_info_int_.ixr_pow;
+  H.flag_circxh = part_info_int_.flag_circxh;
+  H.flag_ahp = part_info_int_.flag_ahp;
+  H.R_ahp = part_info_dp_2_.R_ahp;
+  H.nudt = part_info_dp_2_.nudt;
+  H.Pabs = part_info_dp_2_.Pabs;
+  H.nu_h = part_info_dp_2_.nu_h;
+  return H;
+}
+
 // Temporary device copy of a host table the call builds itself.
 template <class T>
 T *upload(const char *name, const T *h, size_t n, cudaStream_t s) {
@@ -485,10 +503,7 @@ void charge_deposition_(const int *n, const double *h, const double *vxp, const 
                         const int *ntype, const double *kq, double *np, const int *nproc,
                         const int *np_tot, double *sum_dEk, int *Nh, const int *iproc,
                         const int *ptype) {
-  (void)sum_dEk;
-  (void)Nh;
   if (*nproc != 1 || *iproc != 1) return record(LEPIC_ERR_UNSUPPORTED);
-  if (part_info_dp_2_.Pabs > 0.0 && *ptype == 1) return record(LEPIC_ERR_UNSUPPORTED);
   cudaStream_t s = 0;
   Dims d(n);
   lepic_phys_t P = phys_from_common(*ntype);
@@ -512,10 +527,52 @@ void charge_deposition_(const int *n, const double *h, const double *vxp, const 
   if (rc) return record(rc);
   rc = launch_deposit(g, v.s, *ptype, P, np_d, s);
   record(rc);
+  // heating-region statistics of the electrons (Src/part_expmover.f90:658-681)
+  double hs[2] = {0.0, 0.0};
+  if (!rc && *ptype == 1 && part_info_dp_2_.Pabs > 0.0 && sum_dEk && Nh) {
+    const lepic_heat_t H = heat_from_common();
+    double *st = (double *)scratch("dropin_heat_stats", 2 * sizeof(double));
+    rc = st ? LEPIC_OK : LEPIC_ERR_CUDA;
+    if (!rc) rc = cuda_ok(cudaMemsetAsync(st, 0, 2 * sizeof(double), s), "memset");
+    if (!rc) rc = launch_heat_stats(g, &v.s, nullptr, P, H, st, s);
+    if (!rc) rc = cuda_ok(cudaMemcpyAsync(hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s), "copy");
+    record(rc);
+  }
   record(release_species(v, nullptr, nullptr, *nmax, false, s));
   if (rc) return;
   record(host_back(np_slice, np_d, (size_t)d.cnt(), s));
   record(check_err(s));
+  if (*ptype == 1 && part_info_dp_2_.Pabs > 0.0 && sum_dEk && Nh) {
+    sum_dEk[*iproc - 1] += hs[0];
+    Nh[*iproc - 1] += (int)hs[1];
+  }
+}
+
+void eheating_(const double *h, double *vxp, const int *nmax, const int *ntype, const int *nproc, int *iseed,
+               const int *np_tot, const double *vt, const int *iproc, double *P_loss) {
+  if (*nproc != 1 || *iproc != 1) return record(LEPIC_ERR_UNSUPPORTED);
+  static unsigned long long calls = 0;
+  lepic_phys_t P = phys_from_common(*ntype);
+  const lepic_heat_t H = heat_from_common();
+  cudaStream_t s = 0;
+  lepic_grid_t g;
+  memset(&g, 0, sizeof(g));
+  for (int a = 0; a < 3; ++a) g.h[a] = h[a];
+  double *acc = (double *)scratch("dropin_heat_acc", 3 * sizeof(double));
+  if (!acc) return record(LEPIC_ERR_CUDA);
+  int rc = cuda_ok(cudaMemsetAsync(acc, 0, 3 * sizeof(double), s), "memset");
+  if (rc) return record(rc);
+  SpeciesView v;
+  rc = acquire_species(v, vxp, np_tot[0], *nmax, 0, nullptr, s);
+  if (rc) return record(rc);
+  rc = launch_eheating(g, &v.s, nullptr, P, H, *vt, nullptr, (unsigned long long)(unsigned)*iseed, calls++, acc, s);
+  record(rc);
+  double ha[3] = {0.0, 0.0, 0.0};
+  if (!rc) record(cuda_ok(cudaMemcpyAsync(ha, acc, sizeof(ha), cudaMemcpyDeviceToHost, s), "copy"));
+  int np1 = np_tot[0];
+  record(release_species(v, &np1, nullptr, *nmax, rc == LEPIC_OK, s));
+  record(check_err(s));
+  if (P_loss) P_loss[1] += ha[0];  // P_loss(2, 1, 1)
 }
 
 void part_sorting_(double *vxp, double *sorting, const int *nmax, const int *ntype, const int *n,

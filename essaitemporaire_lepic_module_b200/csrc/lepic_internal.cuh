@@ -219,6 +219,13 @@ int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const do
                            int nu_fine_post, int nu_pre, int nu_post, int coarse_sweeps, int *iters,
                            double *res_out, cudaStream_t s);
 
+// heating.cu (e or m: the electrons in one of the two layouts)
+int launch_eheating(const lepic_grid_t &g, lepic_species_f64_t *e, lepic_species_mixed_t *m, const lepic_phys_t &P,
+                    const lepic_heat_t &H, double vt, const double *stats, unsigned long long seed,
+                    unsigned long long call, double *acc, cudaStream_t s);
+int launch_heat_stats(const lepic_grid_t &g, const lepic_species_f64_t *e, const lepic_species_mixed_t *m,
+                      const lepic_phys_t &P, const lepic_heat_t &H, double *stats, cudaStream_t s);
+
 // residency.cu: device mirrors of the drop-ins' host arrays
 bool residency_on();
 // device pointer for host range [h, h + bytes) inside its mirror (created and

@@ -40,9 +40,20 @@ def _pd(a):
     return a.ctypes.data_as(_lib.P_dbl)
 
 
-def set_commons(st, ncol=0, npt=0, p_ncol=None):
+def heat_struct(st, hz):
+    """lepic_heat_t of a config.Heating on the set-up st."""
+    from .config import heating_params
+    hp = heating_params(st, hz)
+    H = _lib.LepicHeat()
+    H.ixl_pow, H.ixr_pow = hp["ixl_pow"], hp["ixr_pow"]
+    H.flag_circxh, H.flag_ahp = int(hz.flag_circxh), int(hz.flag_ahp)
+    H.R_ahp, H.nudt, H.Pabs, H.nu_h = float(hz.R_ahp), hp["nudt"], float(hz.Pabs), float(hz.nu_h)
+    return H, hp
+
+
+def set_commons(st, ncol=0, npt=0, p_ncol=None, heating=None):
     """Fill the library's COMMON blocks the way read_input/read_reactions/main
-    fill the Fortran ones (Src/main.f90:124-579)."""
+    fill the Fortran ones (Src/main.f90:124-579); heating: a config.Heating."""
     cm = commons()
     pi_, d1, d2, d3, cs = (cm["part_info_int"], cm["part_info_dp_1"], cm["part_info_dp_2"],
                            cm["part_info_dp_3"], cm["constants"])
@@ -82,6 +93,23 @@ def set_commons(st, ncol=0, npt=0, p_ncol=None):
     d2.xmax, d2.ymax, d2.zmax = (float(v) for v in st.geom.box)
     d2.x_load = st.x_load
     cs.qe, cs.eps0, cs.c, cs.pi, cs.amu = QE, EPS0, C_LIGHT, PI, AMU
+    if heating is not None:
+        H, hp = heat_struct(st, heating)
+        pi_.ixl_pow, pi_.ixr_pow = H.ixl_pow, H.ixr_pow
+        pi_.flag_circxh, pi_.flag_ahp = H.flag_circxh, H.flag_ahp
+        pi_.ns_heat, pi_.flag_heat, pi_.flag_inj = hp["ns_heat"], hp["flag_heat"], int(heating.flag_inj)
+        d2.R_ahp, d2.nudt, d2.Pabs, d2.nu_h = H.R_ahp, H.nudt, H.Pabs, H.nu_h
+
+
+def eheating(st, vxp, np_tot, vt, P_loss, iseed=123456):
+    """Src/part_expmover.f90:484 -- heats species 1 of vxp (ntype, nmax, 6)
+    in place; P_loss (ntype, 4) C-order, P_loss[0, 1] gains the energy."""
+    h = np.ascontiguousarray(st.h, dtype=np.float64)
+    assert vxp.flags["C_CONTIGUOUS"] and np_tot.dtype == np.int32 and P_loss.flags["C_CONTIGUOUS"]
+    seed = np.array([iseed], dtype=np.int32)
+    lib().eheating_(_pd(h), _pd(vxp), _i(vxp.shape[1]), _i(st.ntype), _i(1), _pi(seed), _pi(np_tot),
+                    _d(vt), _i(1), _pd(P_loss))
+    check(lib().lepic_gpu_last_error(), "eheating")
 
 
 def calc_rho(st, np_grids):
@@ -182,7 +210,9 @@ def part_mover(st, Ei, vxp, np_tot, flag_dead, p_mac, P_loss, ptype, ngrid=None)
 
 
 def charge_deposition(st, vxp, np_tot, np_grids, ptype):
-    """Src/part_expmover.f90:570 -- accumulates into np_grids[ptype-1]."""
+    """Src/part_expmover.f90:570 -- accumulates into np_grids[ptype-1];
+    returns the heating-region statistics (sum_dEk, Nh) (non-zero for
+    ptype 1 with Pabs > 0 in the COMMON blocks)."""
     n = _lib.np_i(st.n)
     h = np.ascontiguousarray(st.h, dtype=np.float64)
     kq = np.ascontiguousarray(st.kq, dtype=np.float64)
@@ -192,6 +222,7 @@ def charge_deposition(st, vxp, np_tot, np_grids, ptype):
     lib().charge_deposition_(_pi(n), _pd(h), _pd(vxp), _i(vxp.shape[1]), _i(st.ntype), _pd(kq),
                              _pd(np_grids), _i(1), _pi(np_tot), _pd(s), _pi(nh), _i(1), _i(ptype))
     check(lib().lepic_gpu_last_error(), "charge_deposition")
+    return float(s[0]), int(nh[0])
 
 
 def pl_max_of(n):

@@ -154,7 +154,7 @@ class Simulation:
 
     def __init__(self, st, cap=None, device="cuda", seed=123456, nsort=None, ns_coll=None,
                  fused=True, precision="f64", mg_mixed=None, comm=None, sort_policy="reference",
-                 check_every=1):
+                 check_every=1, heating=None):
         if precision not in ("f64", "mixed"):
             raise ValueError(f"precision must be 'f64' or 'mixed', not {precision!r}")
         self.st = st
@@ -235,6 +235,16 @@ class Simulation:
         self._tables = None
         if st.tables is not None:
             self._setup_tables()
+        # Maxwellian electron heating (Src/main.f90:1206-1240): a config.Heating
+        self.heat = None
+        if heating is not None:
+            from .dropin import heat_struct
+            self.heat = heating
+            self._H, self.heat_params = heat_struct(st, heating)
+            self._heat_acc = torch.zeros(3, dtype=torch.float64, device=self.dev)   # dE, heated, vt
+            self._heat_stats = torch.zeros(2, dtype=torch.float64, device=self.dev)  # sum Ek, Nh
+            self._heat_stats_ok = False
+            self._heat_calls = 0
 
     def _s(self):
         return C.c_void_p(self.stream.cuda_stream)
@@ -512,13 +522,49 @@ class Simulation:
             self.sort(due)
         if self._tables is not None and it > 1 and it % self.ns_coll == 1 % self.ns_coll:
             self.collisions()
+        hp = self.heat_params if self.heat is not None else None
+        if hp is not None and hp["flag_heat"] and it % hp["ns_heat"] == 0:
+            self.eheating()
         if self.fused:
             self.move_deposit()
         else:
             self.move()
             self.deposit()
+        if hp is not None and self.heat.Pabs > 0 and (it + 1) % hp["ns_heat"] == 0:
+            self.heat_stats()
         if self.check_every and it % self.check_every == 0:
             self.check_device()
+
+    # ------------------------------------------------------------ heating
+    def heat_stats(self):
+        """Kinetic energy and number of the electrons in the heating region
+        after the push (Src/part_expmover.f90:658-681), for the next heating
+        step's self-consistent temperature."""
+        self._heat_stats.zero_()
+        s = self.sp[0]
+        fn = lib().lepic_dev_heat_stats_mixed if self.mixed else lib().lepic_dev_heat_stats
+        check(fn(C.byref(self.grid), C.byref(s.s), C.byref(self.P), C.byref(self._H),
+                 _ptr(self._heat_stats), self._s()), "heat_stats")
+        self._heat_stats_ok = True
+
+    def eheating(self):
+        """Src/part_expmover.f90:484-568 on the electrons: thermal speed vt0 of
+        the electrons, or with Pabs > 0 the self-consistent one of
+        Src/main.f90:1224-1226 from the last statistics (computed on the
+        device)."""
+        s = self.sp[0]
+        use_stats = self.heat.Pabs > 0 and self._heat_stats_ok and not self.heat.flag_inj
+        fn = lib().lepic_dev_eheating_mixed if self.mixed else lib().lepic_dev_eheating
+        check(fn(C.byref(self.grid), C.byref(s.s), C.byref(self.P), C.byref(self._H), float(self.st.vt0[0]),
+                 _ptr(self._heat_stats) if use_stats else None, C.c_ulonglong(self.seed ^ 0x68656174),
+                 C.c_ulonglong(self._heat_calls), _ptr(self._heat_acc), self._s()), "eheating")
+        self._heat_calls += 1
+
+    def heating_totals(self):
+        """(energy added by heating so far (J, P_loss(2) of the electrons),
+        electrons heated so far, thermal speed of the last heating call)."""
+        a = self._heat_acc.cpu().numpy()
+        return float(a[0]), int(a[1]), float(a[2])
 
     def check_device(self):
         """Read and clear the device error word; raise LepicError when a

@@ -129,7 +129,10 @@ void part_mover_(const int *n, const double *h, const double *Ei, const double *
                  double *beam_div, double *sum_q_xz, double *sum_q_yz, const int *dtype,
                  int *iseed, const int *n_B, const double *h_B);
 
-/* Src/part_expmover.f90:570 -- CIC deposition with kq into np(..,ptype,iproc). */
+/* Src/part_expmover.f90:570 -- CIC deposition with kq into np(..,ptype,iproc);
+ * for ptype 1 with Pabs > 0 also the heating-region statistics:
+ * sum_dEk(iproc) += kinetic energy and Nh(iproc) += number of the electrons
+ * in the heating region (Src/part_expmover.f90:658-681). */
 void charge_deposition_(const int *n, const double *h, const double *vxp, const int *nmax,
                         const int *ntype, const double *kq, double *np, const int *nproc,
                         const int *np_tot, double *sum_dEk, int *Nh, const int *iproc,
@@ -158,6 +161,17 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
                  signed char *flag_dead, int *flag_cex, const int *nproc, int *np_tot, int *iseed,
                  const int *nproc_mpi, const int *mpi_rank, double *ss2D_xy, double *ss2D_xz,
                  double *ss2D_yz, const int *flag_diag);
+
+/* Src/part_expmover.f90:484 (eheating) -- Maxwellian electron heating of
+ * species 1 in the heating region ixl_pow <= ix <= ixr_pow (COMMON
+ * /part_info_int/ ixl_pow, ixr_pow, flag_circxh, flag_ahp; /part_info_dp_2/
+ * R_ahp, nudt): each electron there gets, with probability nudt, a new
+ * Maxwellian velocity of thermal speed *vt; P_loss(2,1,iproc) gains the
+ * energy change.  Draws come from a Philox4x32-10 stream keyed by iseed(1)
+ * and a call counter, not ran2: the reference's statistics, not its
+ * sequence. */
+void eheating_(const double *h, double *vxp, const int *nmax, const int *ntype, const int *nproc, int *iseed,
+               const int *np_tot, const double *vt, const int *iproc, double *P_loss);
 
 /* Status of the last drop-in call on this thread, then cleared. */
 int lepic_gpu_last_error(void);
@@ -428,6 +442,34 @@ int lepic_dev_collisions(const lepic_grid_t *g, lepic_species_f64_t *sp, int nty
                          const lepic_tables_t *T, const lepic_phys_t *P, unsigned long long seed,
                          unsigned long long call_index, double *nu_max, long long *counts,
                          void *stream);
+
+/* Electron heating region and rate: ixl_pow, ixr_pow, flag_circxh, flag_ahp,
+ * R_ahp (Src/main.f90:313, 612-614), nudt = nu_h ns_heat dt (Src/main.f90:
+ * 564), Pabs and nu_h (absorbed power, W, and heating frequency, 1/s). */
+typedef struct {
+  int ixl_pow, ixr_pow, flag_circxh, flag_ahp;
+  double R_ahp, nudt, Pabs, nu_h;
+} lepic_heat_t;
+
+/* Src/part_expmover.f90:484-568 (eheating) on the device electrons (species
+ * 1, either layout).  vt: thermal speed; with stats (device double[2] from
+ * lepic_dev_heat_stats: sum Ek, Nh) and H->Pabs > 0 the speed is the
+ * self-consistent one of Src/main.f90:1206-1227 instead, computed on the
+ * device.  Philox draws keyed by seed, counter (particle, call).  acc: device
+ * double[3]; acc[0] += energy change (P_loss(2)), acc[1] += electrons heated,
+ * acc[2] = the thermal speed used. */
+int lepic_dev_eheating(const lepic_grid_t *g, lepic_species_f64_t *e, const lepic_phys_t *P,
+                       const lepic_heat_t *H, double vt, const double *stats, unsigned long long seed,
+                       unsigned long long call, double *acc, void *stream);
+int lepic_dev_eheating_mixed(const lepic_grid_t *g, lepic_species_mixed_t *e, const lepic_phys_t *P,
+                             const lepic_heat_t *H, double vt, const double *stats, unsigned long long seed,
+                             unsigned long long call, double *acc, void *stream);
+/* Src/part_expmover.f90:658-681: stats[0] += kinetic energy, stats[1] +=
+ * number of the electrons in the heating region (device double[2]). */
+int lepic_dev_heat_stats(const lepic_grid_t *g, const lepic_species_f64_t *e, const lepic_phys_t *P,
+                         const lepic_heat_t *H, double *stats, void *stream);
+int lepic_dev_heat_stats_mixed(const lepic_grid_t *g, const lepic_species_mixed_t *e, const lepic_phys_t *P,
+                               const lepic_heat_t *H, double *stats, void *stream);
 
 /* GPU particle loader (counterpart of Src/load_part.f90:91-194 for the
  * large workloads): n_per_species samples, positions uniform in

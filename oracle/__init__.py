@@ -33,6 +33,46 @@ class OTables(C.Structure):
                 ("sig_list", P_int), ("p_ncol", P_int), ("sigv_mx", P_dbl)]
 
 
+class OHeat(C.Structure):
+    _fields_ = [("ixl_pow", C.c_int), ("ixr_pow", C.c_int), ("flag_circxh", C.c_int), ("flag_ahp", C.c_int),
+                ("R_ahp", C.c_double), ("nudt", C.c_double), ("Pabs", C.c_double)]
+
+
+def _oheat(st, hz):
+    from essaitemporaire_lepic_module_b200.config import heating_params
+    hp = heating_params(st, hz)
+    H = OHeat()
+    H.ixl_pow, H.ixr_pow = hp["ixl_pow"], hp["ixr_pow"]
+    H.flag_circxh, H.flag_ahp = int(hz.flag_circxh), int(hz.flag_ahp)
+    H.R_ahp, H.nudt, H.Pabs = float(hz.R_ahp), hp["nudt"], float(hz.Pabs)
+    return H
+
+
+def eheating(st, S, vt, P_loss, hz):
+    """Src/part_expmover.f90:484-568 on species 1 of S (serial ran2 on
+    S.iseed); P_loss (ntype, 4); returns the number of electrons heated."""
+    h = np.ascontiguousarray(st.h)
+    H = _oheat(st, hz)
+    nh = C.c_int(0)
+    P = ophys(st)
+    lib().oracle_eheating(_pd(h), _pd(S.vxp), C.c_int(S.vxp.shape[1]), _pi(S.iseed), _pi(S.np_tot),
+                          C.c_double(vt), _pd(P_loss), C.byref(P), C.byref(H), C.byref(nh))
+    return nh.value
+
+
+def heat_stats(st, S, hz):
+    """Src/part_expmover.f90:658-681: (sum Ek, Nh) of the electrons in the
+    heating region."""
+    h = np.ascontiguousarray(st.h)
+    H = _oheat(st, hz)
+    s = C.c_double(0)
+    nh = C.c_int(0)
+    P = ophys(st)
+    lib().oracle_heat_stats(_pd(h), _pd(S.vxp), C.c_int(S.vxp.shape[1]), _pi(S.np_tot), C.byref(P),
+                            C.byref(H), C.byref(s), C.byref(nh))
+    return s.value, nh.value
+
+
 def build():
     """Compile the oracle with its Makefile (strict IEEE)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)

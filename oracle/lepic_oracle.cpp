@@ -128,6 +128,76 @@ void oracle_load_gauss(double *vx, double *vy, double vt, const double rnd[2], d
   *vy = vp * std::sin(theta);
 }
 
+// the heating region test of Src/part_expmover.f90:519-530 and 661-672:
+// ixl_pow <= ix <= ixr_pow and, with flag_circxh, inside (flag_ahp = 0) or
+// outside (flag_ahp = 1) the circle of radius R_ahp about the box axis
+static bool in_heat_region(const double *v, const double h[3], const OPhys *P, const OHeat *H) {
+  int ix = (int)(v[0] / h[0]) + 1;
+  if (!(ix >= H->ixl_pow && ix <= H->ixr_pow)) return false;
+  if (H->flag_circxh == 1) {
+    double r2 = (v[1] - P->ymax / 2.0) * (v[1] - P->ymax / 2.0) + (v[2] - P->zmax / 2.0) * (v[2] - P->zmax / 2.0);
+    if (H->flag_ahp == 0) {
+      if (r2 > H->R_ahp * H->R_ahp) return false;
+    } else {
+      if (r2 < H->R_ahp * H->R_ahp) return false;
+    }
+  }
+  return true;
+}
+
+// Src/part_expmover.f90:484-568 (eheating, one thread): every electron in
+// the heating region is, with probability nudt, given a new Maxwellian
+// velocity of thermal speed vt (vz from a second pair, kept for the next
+// heated electron); P_loss(2,1) gains the energy change.
+void oracle_eheating(const double h[3], double *vxp, int nmax, int *iseed, const int *np_tot, double vt,
+                     double *P_loss, const OPhys *P, const OHeat *H, int *nheated) {
+  (void)nmax;
+  double vz_sav = 0.0;
+  int cnt = 0;
+  const double Nm = P->Nm[0], mass = P->mass[0];
+  for (int i = 0; i < np_tot[0]; ++i) {
+    double *v = vxp + (long)i * 6;
+    if (!in_heat_region(v, h, P, H)) continue;
+    double rnd[2];
+    rnd[0] = oracle_ran2(iseed);
+    if (rnd[0] <= H->nudt) {
+      double v2old = v[3] * v[3] + v[4] * v[4] + v[5] * v[5];
+      rnd[0] = oracle_ran2(iseed);
+      rnd[1] = oracle_ran2(iseed);
+      oracle_load_gauss(&v[3], &v[4], vt, rnd, P->pi);
+      if (vz_sav == 0.0) {
+        rnd[0] = oracle_ran2(iseed);
+        rnd[1] = oracle_ran2(iseed);
+        oracle_load_gauss(&v[5], &vz_sav, vt, rnd, P->pi);
+      } else {
+        v[5] = vz_sav;
+        vz_sav = 0.0;
+      }
+      P_loss[1] = P_loss[1] + 0.5 * Nm * mass * (v[3] * v[3] + v[4] * v[4] + v[5] * v[5] - v2old);
+      cnt++;
+    }
+  }
+  *nheated = cnt;
+}
+
+// Src/part_expmover.f90:658-681: the kinetic energy and the number of the
+// electrons in the heating region (the deposition's statistics for the
+// self-consistent heating temperature of Src/main.f90:1206-1227).
+void oracle_heat_stats(const double h[3], const double *vxp, int nmax, const int *np_tot, const OPhys *P,
+                       const OHeat *H, double *sum_dEk, int *Nh) {
+  (void)nmax;
+  double s = 0.0;
+  int c = 0;
+  for (int i = 0; i < np_tot[0]; ++i) {
+    const double *v = vxp + (long)i * 6;
+    if (!in_heat_region(v, h, P, H)) continue;
+    s = s + 0.5 * P->Nm[0] * P->mass[0] * (v[3] * v[3] + v[4] * v[4] + v[5] * v[5]);
+    c++;
+  }
+  *sum_dEk = s;
+  *Nh = c;
+}
+
 // Src/main.f90:336-347 -- kq = 2 on every node that is not plasma.
 void oracle_make_kq(const int n[3], const int *bcnd, double *kq) {
   Dims d(n);

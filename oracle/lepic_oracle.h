@@ -60,6 +60,13 @@ typedef struct OPhys {
   double h_B[3];                   /* map spacing (xmax/n_B(1), ...)         */
 } OPhys;
 
+/* Electron heating region and rate (COMMON /part_info_int/ ixl_pow, ixr_pow,
+ * flag_circxh, flag_ahp; /part_info_dp_2/ R_ahp, nudt, Pabs). */
+typedef struct OHeat {
+  int ixl_pow, ixr_pow, flag_circxh, flag_ahp;
+  double R_ahp, nudt, Pabs;
+} OHeat;
+
 /* Cross-section tables after Src/read_reactions.f90:ordering. */
 typedef struct OTables {
   int ncol;                        /* reactions                              */
@@ -126,6 +133,10 @@ int oracle_collisions(double *vxp, const int n[3], const double h[3], int ntype,
                       long long *cnt_col, int *Nc_out);
 void oracle_scatter(double *vx1, double *vy1, double *vz1, double vx, double vy,
                     double vz, double costheta, double phi);
+void oracle_eheating(const double h[3], double *vxp, int nmax, int *iseed, const int *np_tot,
+                     double vt, double *P_loss, const OPhys *P, const OHeat *H, int *nheated);
+void oracle_heat_stats(const double h[3], const double *vxp, int nmax, const int *np_tot,
+                       const OPhys *P, const OHeat *H, double *sum_dEk, int *Nh);
 
 #ifdef __cplusplus
 }

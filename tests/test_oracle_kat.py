@@ -282,3 +282,32 @@ def test_pdesolver_neumann_plane_is_the_mirror_of_the_full_box():
     unknown[:, n2 + 2, :] = False
     assert np.abs(np.where(unknown, mine - mirror, 0.0)).max() <= 1e-7 * np.abs(mirror).max()
     assert np.abs(mirror).max() > 0
+
+
+def test_eheating_rate_and_temperature():
+    """Src/part_expmover.f90:484-568: of the electrons in the heating region
+    a fraction nudt is heated (binomial, within 4 sigma), their new
+    velocities are Maxwellian of thermal speed vt (<v^2> = 1.5 vt^2, within
+    4 sigma), electrons outside the region are untouched, and P_loss(2)
+    equals the energy change."""
+    st = config.build("box16")
+    hz = config.Heating(xl_pow=0.4e-3, xr_pow=1.2e-3, nu_h=1.5e9)
+    S = oracle.load_part(st, nmax=st.n_particles() + 16)
+    before = S.vxp[0, :S.np_tot[0]].copy()
+    _, nreg = oracle.heat_stats(st, S, hz)
+    nudt = config.heating_params(st, hz)["nudt"]
+    vt = 2.0 * st.vt0[0]
+    P_loss = np.zeros((st.ntype, 4))
+    nh = oracle.eheating(st, S, vt, P_loss, hz)
+    after = S.vxp[0, :S.np_tot[0]]
+    assert abs(nh - nreg * nudt) <= 4 * math.sqrt(nreg * nudt * (1 - nudt))
+    changed = np.any(after != before, axis=1)
+    assert changed.sum() == nh
+    ix = (before[:, 0] / st.h[0]).astype(int) + 1
+    hp = config.heating_params(st, hz)
+    assert not changed[(ix < hp["ixl_pow"]) | (ix > hp["ixr_pow"])].any()
+    v2 = (after[changed, 3:6] ** 2).sum(axis=1)
+    # v^2 / vt^2 of a 3D Maxwellian is Gamma(3/2): mean 1.5, variance 1.5
+    assert abs(v2.mean() / vt ** 2 - 1.5) <= 4 * math.sqrt(1.5 / nh)
+    dE = 0.5 * st.Nm[0] * st.mass[0] * ((after[:, 3:6] ** 2).sum() - (before[:, 3:6] ** 2).sum())
+    assert abs(P_loss[0, 1] - dE) <= 1e-9 * abs(dE)
