@@ -50,7 +50,13 @@ class LepicSpeciesF64(C.Structure):
 class LepicSpeciesMixed(C.Structure):
     _fields_ = [("cell", C.c_void_p), ("p", C.c_void_p), ("cell_alt", C.c_void_p),
                 ("p_alt", C.c_void_p), ("count", C.c_void_p), ("flag_dead", C.c_void_p),
-                ("tile_off", C.c_void_p), ("cap", C.c_int)]
+                ("tile_off", C.c_void_p), ("cap", C.c_int), ("cell_off", C.c_void_p)]
+
+
+class LepicTargets(C.Structure):
+    """lepic_targets_t: charged-target (DSMC) inputs and counters."""
+    _fields_ = [("np", C.c_void_p * NPART), ("cell_off", C.c_void_p * NPART),
+                ("missed", C.c_longlong), ("lost_claims", C.c_longlong)]
 
 
 class LepicHeat(C.Structure):
@@ -169,6 +175,14 @@ def lib():
         "lepic_dev_collisions_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), _I,
                                         C.POINTER(LepicTables), C.POINTER(LepicPhys), C.c_ulonglong,
                                         C.c_ulonglong, P_dbl, C.POINTER(C.c_longlong), vp], _I),
+        "lepic_dev_collisions_targets": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64), _I,
+                                          C.POINTER(LepicTables), C.POINTER(LepicPhys), C.c_ulonglong,
+                                          C.c_ulonglong, P_dbl, C.POINTER(C.c_longlong), C.POINTER(LepicTargets),
+                                          vp], _I),
+        "lepic_dev_collisions_mixed_targets": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), _I,
+                                                C.POINTER(LepicTables), C.POINTER(LepicPhys), C.c_ulonglong,
+                                                C.c_ulonglong, P_dbl, C.POINTER(C.c_longlong),
+                                                C.POINTER(LepicTargets), vp], _I),
         "lepic_dev_win_push": ([C.POINTER(LepicGrid), vp, vp, _I, _I, vp, _I, C.POINTER(LepicPhys), vp], _I),
         "lepic_dev_win_deposit": ([C.POINTER(LepicGrid), vp, _I, _I, vp, _I, C.POINTER(LepicPhys), vp, vp], _I),
         "lepic_dev_adj_push": ([C.POINTER(LepicGrid), vp, vp, _I, _I, vp, vp, vp, _I, _I, C.POINTER(LepicPhys),
@@ -248,6 +262,7 @@ def exported_symbols():
             "calc_rho_", "dens_red_", "pdesolver_", "calc_efield_",
             "part_mover_", "charge_deposition_", "part_sorting_", "collisions_", "eheating_",
             "lepic_dev_eheating", "lepic_dev_eheating_mixed", "lepic_dev_heat_stats", "lepic_dev_heat_stats_mixed",
+            "lepic_dev_collisions_targets", "lepic_dev_collisions_mixed_targets",
             "part_info_int_", "part_info_dp_1_", "part_info_dp_2_", "part_info_dp_3_", "constants_"]
 
 

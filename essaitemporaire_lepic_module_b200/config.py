@@ -23,6 +23,8 @@ set-ups shrunk so the FP64 CPU oracle finishes in seconds):
   pbc16      16^3 cells, e- + Ar+ 16 ppc, walls at both x ends, periodic
              planes in y and z (pbc32x16: 32 cells in x)
   nmn16      the same with the Neumann (symmetry) plane at x = 0
+  dsmc16     16^3 box, e- + Ar+ 16 ppc, e-Ar+ elastic collisions with
+             charged targets (dsmcar16: with the Ar MCC as well)
 """
 from __future__ import annotations
 
@@ -66,6 +68,7 @@ class Workload:
     blob_seed: int = 3
     mixed_only: bool = False
     neumann_x: bool = False         # x = 0 is a Neumann (symmetry) plane
+    coulomb: float = 0.0            # > 0: e-Ar+ elastic (charged target, DSMC) of this sigma0 (m^2)
 
 
 def _box(n, dx):
@@ -87,6 +90,13 @@ def workload(name: str) -> Workload:
         return Workload(name, n, 1e-4, [_box(n, 1e-4) + [1]], [0.0, 0.0], _ar_ion(),
                         Te=2.0, n0=1e15, ppc=64 if name != "mcc32" else 32, dt=2e-11, steps=500,
                         B=(0.0, 0.0, 0.01), gas_pressure=1.0, gas_T=300.0)
+    if name in ("dsmc16", "dsmcar16"):
+        # e-Ar+ elastic collisions with charged targets (dsmcar16: on top of
+        # the Ar MCC of mcc128)
+        n = (16, 16, 16)
+        return Workload(name, n, 1e-4, [_box(n, 1e-4) + [1]], [0.0, 0.0], _ar_ion(),
+                        Te=2.0, n0=1e15, ppc=16, dt=2e-11, steps=200, B=(0.0, 0.0, 0.01),
+                        gas_pressure=1.0 if name == "dsmcar16" else 0.0, gas_T=300.0, coulomb=2e-13)
     if name in ("pbc16", "pbc32x16", "nmn16"):
         # walls at both x ends (nmn16: the Neumann plane at x = 0 instead),
         # periodic planes in y and z (a box segment, then label 0 over it)
@@ -229,6 +239,8 @@ def build(wl: Workload | str) -> Setup:
     if ngas > 0:
         neutrals = [("[Ar]", -39.95, 0.0, KB * wl.gas_T / QE, 1.0)]
     reacts = rx.argon_tables_synthetic() if ngas > 0 else []
+    if wl.coulomb > 0:
+        reacts = [rx.coulomb_table_synthetic(wl.coulomb)] + reacts
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "chem.dat")
         rx.write_dat(path, wl.ions, neutrals, reacts)
@@ -262,7 +274,7 @@ def build(wl: Workload | str) -> Setup:
     n_cell = count_cells(geom.bcnd, n, min(ix_pe, n[0] + 1))
     ng = mg_levels(n, wl.ng or 6)
     kq = np.where(geom.bcnd != -1, 2.0, 1.0)
-    tables = rx.ordering(chem) if (ngas > 0 and len(chem.tables)) else None
+    tables = rx.ordering(chem) if len(chem.tables) else None
     st = Setup(wl=wl, geom=geom, n=n, h=h, ntype=ntype, n_neu=n_neu, names=names, charge=charge,
                mass=mass, Ti=Ti, vt0=vt0, Nm=Nm, np_mx=np_mx, nu_uplim=nu_uplim, ni0=ni0,
                dt=wl.dt, x_load=x_load, n_cell=n_cell, np_cell=np_cell, ng=ng,

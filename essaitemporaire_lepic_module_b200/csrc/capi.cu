@@ -339,6 +339,14 @@ int lepic_dev_collisions(const lepic_grid_t *g, lepic_species_f64_t *sp, int nty
   return launch_collisions(*g, sp, ntype, *T, *P, seed, call_index, nu_max, counts, S(stream));
 }
 
+int lepic_dev_collisions_targets(const lepic_grid_t *g, lepic_species_f64_t *sp, int ntype,
+                                 const lepic_tables_t *T, const lepic_phys_t *P, unsigned long long seed,
+                                 unsigned long long call_index, double *nu_max, long long *counts,
+                                 lepic_targets_t *tg, void *stream) {
+  if (!g || !sp || !T || !P || !tg || ntype < 1) return LEPIC_ERR_ARG;
+  return launch_collisions(*g, sp, ntype, *T, *P, seed, call_index, nu_max, counts, S(stream), nullptr, tg);
+}
+
 int lepic_dev_load_uniform(const lepic_grid_t *g, lepic_species_f64_t *sp, int ntype,
                            long long n_per_species, const lepic_phys_t *P, unsigned long long seed,
                            void *stream) {
@@ -619,8 +627,6 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
   (void)P_loss;
   (void)sour_xy;
   (void)sour_xz;
-  (void)Plist;
-  (void)pl_max;
   (void)flag_cex;
   (void)mpi_rank;
   (void)ss2D_xy;
@@ -713,11 +719,33 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
     if (rc) return record(rc);
     sp[p] = v[p].s;
   }
+  // charged targets (DSMC): the per-cell offsets Plist(0:pl_max,ntype) of the
+  // last part_sorting and the densities np_red of dens_red
+  lepic_targets_t tg;
+  memset(&tg, 0, sizeof(tg));
+  bool charged = false;
+  for (int c = 0; c < ncol; ++c) {
+    const int n_re = ci[c];
+    const int tt = ci[c + (size_t)ncol * (2 + n_re - 1)];
+    if (tt >= 1 && tt <= nt && P.charge[tt - 1] != 0.0) charged = true;
+  }
+  if (charged) {
+    // Plist must cover every cell index of the grid
+    if ((long long)*pl_max < (long long)n[0] * n[1] * n[2]) return record(LEPIC_ERR_ARG);
+    const int *pl_d = dev_view("dropin_plist", Plist, (size_t)(*pl_max + 1) * nt, READ, s, &rc);
+    if (!pl_d) return record(rc);
+    const double *nr_d = dev_view("dropin_npred", np_red, (size_t)d.cnt() * nt, READ, s, &rc);
+    if (!nr_d) return record(rc);
+    for (int p = 0; p < nt; ++p) {
+      tg.cell_off[p] = pl_d + (size_t)(*pl_max + 1) * p;
+      tg.np[p] = nr_d + (size_t)d.cnt() * p;
+    }
+  }
   double nu_max[LEPIC_NPART] = {0};
   long long counts[64] = {0};
   unsigned long long seed = (unsigned long long)(unsigned)iseed[0];
   rc = launch_collisions(g, sp, nt, T, P, seed, (unsigned long long)*it, nu_max, counts, s,
-                         rgc.n_rg > 0 ? &rgc : nullptr);
+                         rgc.n_rg > 0 ? &rgc : nullptr, &tg);
   for (int p = 0; p < nt; ++p) {
     v[p].s = sp[p];
     record(release_species(v[p], &np_tot[p], flag_dead + (long long)*nmax * p, *nmax, true, s));

@@ -102,7 +102,7 @@ __global__ void k_dens_red(Dims d, const double *np, double *np_red, const int *
     v = 0.0 + np[t];
     if (bcnd[q] == -1 && v > 0.0) atomicMax(&mx[p], (unsigned long long)__double_as_longlong(v));
   }
-  np_red[t] = v;
+  if (np_red) np_red[t] = v;
 }
 
 int launch_dens_red(const Dims &d, const double *np, double *np_red, const int *bcnd, int ntype,

@@ -200,14 +200,15 @@ struct RegionCount {
   int ixl[LEPIC_NM_RG], ixr[LEPIC_NM_RG], iyl, iyr, izl, izr;
   double w[LEPIC_NPART][LEPIC_NM_RG];
 };
+// tg: charged-target (DSMC) inputs and outputs, nullptr when the tables have none
 int launch_collisions(const lepic_grid_t &g, lepic_species_f64_t *sp, int ntype,
                       const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
                       unsigned long long call_index, double *nu_max, long long *counts,
-                      cudaStream_t s, const RegionCount *rg = nullptr);
+                      cudaStream_t s, const RegionCount *rg = nullptr, lepic_targets_t *tg = nullptr);
 int launch_collisions_mixed(const lepic_grid_t &g, lepic_species_mixed_t *sp, int ntype,
                             const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
                             unsigned long long call_index, double *nu_max, long long *counts,
-                            cudaStream_t s);
+                            cudaStream_t s, lepic_targets_t *tg = nullptr);
 // mixed.cu
 int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E32, lepic_species_mixed_t &sp,
                               int ptype, int ngrid, const lepic_phys_t &P, double *np, double *acc,

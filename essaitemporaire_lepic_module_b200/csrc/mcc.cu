@@ -1,4 +1,6 @@
-// Null-collision Monte Carlo against neutral targets (Src/collisions.f90).
+// Null-collision Monte Carlo (Src/collisions.f90) against neutral targets
+// (MC: a Maxwellian partner) and charged targets (DSMC: a particle of the
+// target species in the incident's cell).
 //
 // The reference draws Nc = N * nu_max * ns_coll * dt incident particles with
 // replacement from a serial ran2 stream and tests each against
@@ -20,6 +22,20 @@
 // and charge exchange by velocity swap.  Ionization products are appended at
 // the end of their species' arrays.  The kernels are templated on the
 // particle layout (FP64 SoA or mixed cell + FP32 offsets).
+//
+// Charged targets (Src/collisions.f90:335-423, 524-531): the partner is a
+// uniformly chosen particle of the target species in the incident's cell, or
+// in the first non-empty of the cells ici+1, ici-1, ici+n1, ici-n1,
+// ici+n1 n2, ici-n1 n2 (the reference's linear cell index), found through
+// the per-cell offsets of that species' last sort; the target density is the
+// mean of the species' density grid over the cell's 8 nodes.  The collision
+// may change the target's velocity (elastic, excitation, charge exchange) or
+// remove it (other reactions).  The reference runs the collisions one after
+// another; here the incident particles collide concurrently, so a target
+// taken by one collision is claimed (one flag per particle, cleared per
+// call) and a second collision that drew the same target is dropped and
+// counted (lost_claims; rare while collisions per call are few against the
+// targets in a cell).
 #include <vector>
 
 #include "lepic_internal.cuh"
@@ -39,6 +55,8 @@ struct MCCConst {
   int ind[MAXR];                // 1-based reaction index
   int tt[MAXR];                 // target species (1-based)
   int rt[MAXR], n_by[MAXR], n_re[MAXR];
+  int dsmc[MAXR];               // 1: charged target (DSMC)
+  int any_dsmc;
   int by[MAXR][MAXBY];
   double Eth[MAXR], np_t[MAXR];
   double mass[LEPIC_NPART];     // signed masses
@@ -126,6 +144,50 @@ struct AccMixed {
     iz = (cc >> (2 * LEPIC_CELL_BITS)) + 1;
   }
 };
+
+// DSMC state: per species density grids, per-cell offsets of the last sort
+// (FP64 sort: Plist, inclusive ends at the reference's linear cell index;
+// mixed sort: exclusive starts at the 8x8x8-tile key), flag_dead and claims
+struct Targets {
+  const double *np[LEPIC_NPART];
+  const int *off[LEPIC_NPART];
+  signed char *fd[LEPIC_NPART];
+  int *claim[LEPIC_NPART];
+  int tile, n1, n2, n3, ntx, nty;
+  long long pl_max;
+  unsigned long long *stat;     // [0] incident particles with no target, [1] lost claims
+};
+
+// a particle of species T in cell ici (1-based linear index) or its six
+// neighbours in the reference's order; -1 when none
+__device__ __forceinline__ long long pick_target(const Targets &D, int T, long long ici, uint32_t rnd) {
+  const int *off = D.off[T];
+  if (!off) return -1;
+  const long long n12 = (long long)D.n1 * D.n2, ncell = n12 * D.n3;
+  const long long cand[7] = {ici, ici + 1, ici - 1, ici + D.n1, ici - D.n1, ici + n12, ici - n12};
+  for (int k = 0; k < 7; ++k) {
+    const long long ic = cand[k];
+    if (ic < 1 || ic > D.pl_max) continue;
+    long long lo, hi;
+    if (!D.tile) {
+      lo = off[ic - 1];
+      hi = off[ic];
+    } else {
+      if (ic > ncell) continue;
+      const long long l = ic - 1;
+      const int cx = (int)(l % D.n1), cy = (int)((l / D.n1) % D.n2), cz = (int)(l / n12);
+      const long long tile = (cx >> 3) + (long long)D.ntx * ((cy >> 3) + (long long)D.nty * (cz >> 3));
+      const long long key = tile * 512 + (cx & 7) + 8 * ((cy & 7) + 8 * (cz & 7));
+      lo = off[key];
+      hi = off[key + 1];
+    }
+    if (hi > lo) {
+      long long idx = lo + (long long)((double)(hi - lo) * u01(rnd));
+      return idx < hi ? idx : hi - 1;
+    }
+  }
+  return -1;
+}
 
 // Src/collisions.f90:1022-1050
 __device__ __forceinline__ void scatter(double &vx1, double &vy1, double &vz1, double vx, double vy,
@@ -252,8 +314,17 @@ __global__ void __launch_bounds__(MB) k_mcc_select_skip(MCCConst c, const int *_
 
 // pass 2: the collision physics on the candidates (grid-stride over warps so
 // every lane of a warp reaches the warp-wide counter reductions)
+// the partner of the incident particle for target species tt: velocity,
+// reduced mass, relative speed and energy, centre-of-mass velocity
+// (Src/collisions.f90:437-470); idx: the DSMC target's slot
+struct TState {
+  double tvx, tvy, tvz, mu, vr, vxc, vyc, vzc, Ekr;
+  long long idx;
+  bool ok;
+};
+
 template <class Acc>
-__global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, const int *__restrict__ cand,
+__global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D, const int *__restrict__ cand,
                                                     const int *__restrict__ ncand_p,
                                                     const double *__restrict__ Er,
                                                     const double *__restrict__ sig, signed char *flag_dead,
@@ -276,38 +347,78 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, const int
       S.load_v(P, i, vx0, vy0, vz0);
       ctr.y = 1u;
       const U4 r1 = philox4x32_10(ctr, c.k0, c.k1);
-      // one Maxwellian target per target species (Src/collisions.f90:437-449)
-      double vr_t = 0, mu_t = 0, vxc = 0, vyc = 0, vzc = 0, tvx = 0, tvy = 0, tvz = 0, Ekr_t = 0;
+      // the incident's cell (DSMC only)
+      int cix = 1, ciy = 1, ciz = 1;
+      long long ici = 0;
+      if (c.any_dsmc) {
+        S.cell_of(c, P, i, cix, ciy, ciz);
+        ici = (cix - 1) + (long long)D.n1 * ((ciy - 1) + (long long)D.n2 * (ciz - 1)) + 1;
+      }
+      ctr.y = 3u;
+      const U4 r3 = c.any_dsmc ? philox4x32_10(ctr, c.k0, c.k1) : U4{0u, 0u, 0u, 0u};
+      // the partner for target species tt: a Maxwellian neutral
+      // (Src/collisions.f90:437-449; the same draws for every neutral
+      // species) or a particle of a charged species (DSMC)
+      auto partner = [&](int tt, bool charged) {
+        TState t;
+        t.idx = -1;
+        t.ok = true;
+        if (charged) {
+          t.idx = pick_target(D, tt - 1, ici, r3.x);
+          t.ok = t.idx >= 0;
+          if (!t.ok) return t;
+          S.load_v(tt - 1, t.idx, t.tvx, t.tvy, t.tvz);
+        } else {
+          const double vt = c.vt0[tt - 1];
+          const double vp = vt * sqrt(-log(u01(r1.x)));
+          double s1, c1;
+          sincos(2.0 * c.pi * u01(r1.y), &s1, &c1);
+          t.tvx = vp * c1;
+          t.tvy = vp * s1;
+          const double vp2 = vt * sqrt(-log(u01(r1.z)));
+          t.tvz = vp2 * cos(2.0 * c.pi * u01(r1.w));
+        }
+        const double mt = fabs(c.mass[tt - 1]);
+        t.mu = c.m_p * mt / (c.m_p + mt);
+        t.vr = sqrt((vx0 - t.tvx) * (vx0 - t.tvx) + (vy0 - t.tvy) * (vy0 - t.tvy) + (vz0 - t.tvz) * (vz0 - t.tvz));
+        t.Ekr = (0.5 * t.mu * (t.vr * t.vr)) / c.qe;
+        const double sm = c.m_p + mt;
+        t.vxc = (c.m_p * vx0 + mt * t.tvx) / sm;
+        t.vyc = (c.m_p * vy0 + mt * t.tvy) / sm;
+        t.vzc = (c.m_p * vz0 + mt * t.tvz) / sm;
+        if (t.Ekr > Er[c.npt - 1]) raise_err(err, LEPIC_ERR_EKR_TABLE, (int)i);
+        return t;
+      };
+      TState ts;
+      ts.ok = false;
       int cur_tt = -1;
+      unsigned missed = 0u;
       double nu[MAXR];
       double sum_nu = 0.0;
       for (int r = 0; r < c.nr; ++r) {
         const int tt = c.tt[r];
         if (tt != cur_tt) {
-          const double vt = c.vt0[tt - 1];
-          const double vp = vt * sqrt(-log(u01(r1.x)));
-          double s1, c1;
-          sincos(2.0 * c.pi * u01(r1.y), &s1, &c1);
-          tvx = vp * c1;
-          tvy = vp * s1;
-          const double vp2 = vt * sqrt(-log(u01(r1.z)));
-          tvz = vp2 * cos(2.0 * c.pi * u01(r1.w));
-          const double mt = fabs(c.mass[tt - 1]);
-          mu_t = c.m_p * mt / (c.m_p + mt);
-          vr_t = sqrt((vx0 - tvx) * (vx0 - tvx) + (vy0 - tvy) * (vy0 - tvy) + (vz0 - tvz) * (vz0 - tvz));
-          Ekr_t = (0.5 * mu_t * (vr_t * vr_t)) / c.qe;
-          const double sm = c.m_p + mt;
-          vxc = (c.m_p * vx0 + mt * tvx) / sm;
-          vyc = (c.m_p * vy0 + mt * tvy) / sm;
-          vzc = (c.m_p * vz0 + mt * tvz) / sm;
-          if (Ekr_t > Er[c.npt - 1]) raise_err(err, LEPIC_ERR_EKR_TABLE, (int)i);
+          ts = partner(tt, c.dsmc[r] != 0);
+          if (!ts.ok) missed |= 1u << tt;
           cur_tt = tt;
         }
+        nu[r] = 0.0;
+        if (!ts.ok) continue;
         int found;
-        const double sp = sigma_at(Er, sig + (long long)c.npt_mx * (c.ind[r] - 1), c.npt, Ekr_t, found);
-        nu[r] = found ? c.np_t[r] * sp * vr_t / c.nu_max : 0.0;
+        const double sp = sigma_at(Er, sig + (long long)c.npt_mx * (c.ind[r] - 1), c.npt, ts.Ekr, found);
+        double np_t = c.np_t[r];
+        if (c.dsmc[r]) {
+          // the target density at the incident's cell (Src/collisions.f90:524-531)
+          const double *g = D.np[tt - 1];
+          const long long N1 = D.n1 + 3, N2 = D.n2 + 3;
+          const long long q = cix + N1 * (ciy + N2 * (long long)ciz), sy = N1, sz = N1 * N2;
+          np_t = 0.125 * (g[q] + g[q + 1] + g[q + sy] + g[q + 1 + sy] + g[q + sz] + g[q + 1 + sz] + g[q + sy + sz] +
+                          g[q + 1 + sy + sz]);
+        }
+        nu[r] = found ? np_t * sp * ts.vr / c.nu_max : 0.0;
         sum_nu += nu[r];
       }
+      if (missed) atomicAdd(&D.stat[0], (unsigned long long)__popc(missed));
       const double u = u01(r0.y);
       if (u <= sum_nu) {
         double s = 0.0;
@@ -319,11 +430,28 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, const int
           }
         }
       }
+      const bool tgt = sel >= 0 && c.dsmc[sel];
+      if (sel >= 0) {
+        if (c.tt[sel] != cur_tt) ts = partner(c.tt[sel], tgt);
+        // a charged target takes part in one collision per call
+        if (tgt && atomicExch(&D.claim[c.tt[sel] - 1][ts.idx], 1) != 0) {
+          atomicAdd(&D.stat[1], 1ull);
+          sel = -1;
+        }
+      }
       if (sel >= 0) {
         const int rt = c.rt[sel];
+        const int T = c.tt[sel] - 1;
+        const double mu_t = ts.mu, vr_t = ts.vr, vxc = ts.vxc, vyc = ts.vyc, vzc = ts.vzc;
         if (rt == 4) {
-          // charge exchange: the incident takes the target's velocity
-          S.store_v(P, i, tvx, tvy, tvz);
+          // charge exchange (Src/collisions.f90:948-998): the incident takes
+          // the target's velocity, a charged target the incident's
+          for (int a = 0; a < c.n_by[sel]; ++a) {
+            const int bt = c.by[sel][a];
+            if (c.mass[bt - 1] <= 0) continue;
+            if (bt == c.ptype) S.store_v(P, i, ts.tvx, ts.tvy, ts.tvz);
+            else if (tgt && bt - 1 == T) S.store_v(T, ts.idx, vx0, vy0, vz0);
+          }
         } else {
           double Ee = 0.5 * mu_t * (vr_t * vr_t) - c.Eth[sel] * c.qe;
           if (Ee < 0.0) {
@@ -360,6 +488,9 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, const int
             if (reuse) {
               S.store_v(P, i, nvx, nvy, nvz);
               incident_reused = true;
+            } else if ((rt == 1 || rt == 3) && tgt && bt - 1 == T) {
+              // elastic / excitation keep a charged target (Src/collisions.f90:843-851)
+              S.store_v(T, ts.idx, nvx, nvy, nvz);
             } else {
               const int B = bt - 1;
               const int slot = atomicAdd(&add[B], 1);
@@ -369,6 +500,8 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, const int
             }
           }
           if (!incident_reused && flag_dead) flag_dead[i] = 1;
+          // other reactions remove a charged target (Src/collisions.f90:913-938)
+          if (tgt && rt != 1 && rt != 3 && D.fd[T]) D.fd[T][ts.idx] = 1;
         }
         if (cnt_col) {
           int ix, iy, iz;
@@ -412,8 +545,30 @@ template <class Acc>
 int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed char *const *flag_dead,
                    int ntype, const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
                    unsigned long long call_index, double *nu_max, long long *counts, cudaStream_t s,
-                   const RegionCount *rg, const char *tname) {
+                   const RegionCount *rg, const char *tname, lepic_targets_t *tg, int tile) {
   if (ntype > 3) return LEPIC_ERR_UNSUPPORTED;
+  // DSMC state: density grids and sort offsets from the caller, claims here
+  Targets D;
+  memset(&D, 0, sizeof(D));
+  D.tile = tile;
+  D.n1 = g.n[0];
+  D.n2 = g.n[1];
+  D.n3 = g.n[2];
+  D.ntx = (g.n[0] + 7) / 8;
+  D.nty = (g.n[1] + 7) / 8;
+  // cell indices beyond n1 n2 n3 hold no particles: every Plist covering the
+  // grid's cells is read within its bounds
+  D.pl_max = (long long)g.n[0] * g.n[1] * g.n[2];
+  D.stat = (unsigned long long *)scratch("mcc_dsmc_stat", 2 * sizeof(unsigned long long));
+  if (!D.stat) return LEPIC_ERR_CUDA;
+  LEPIC_CUDA(cudaMemsetAsync(D.stat, 0, 2 * sizeof(unsigned long long), s));
+  for (int q = 0; q < ntype; ++q) {
+    D.fd[q] = flag_dead[q];
+    if (tg) {
+      D.np[q] = tg->np[q];
+      D.off[q] = tg->cell_off[q];
+    }
+  }
   auto CI = [&](int icol, int info) { return T.col_info_h[(icol - 1) + (long long)T.ncol * (info - 1)]; };
   int *add = (int *)scratch("mcc_add", sizeof(int) * LEPIC_NPART);
   unsigned long long *cnt = (unsigned long long *)scratch("mcc_cnt", sizeof(unsigned long long) * 64);
@@ -451,7 +606,19 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
       const int n_re = CI(ind, 1), n_by = CI(ind, 2);
       if (n_by > MAXBY || n_re > 2) return LEPIC_ERR_UNSUPPORTED;
       const int tt = CI(ind, 2 + n_re);
-      if (P.charge[tt - 1] != 0.0) return LEPIC_ERR_UNSUPPORTED;  // DSMC targets
+      if (P.charge[tt - 1] != 0.0) {
+        // a charged target: its density grid and sort offsets are needed
+        if (tt > ntype || !D.np[tt - 1] || !D.off[tt - 1] || !D.fd[tt - 1]) return LEPIC_ERR_UNSUPPORTED;
+        c.dsmc[r] = 1;
+        c.any_dsmc = 1;
+        if (!D.claim[tt - 1]) {
+          char cn[32];
+          snprintf(cn, sizeof cn, "mcc_claim%d", tt - 1);
+          D.claim[tt - 1] = (int *)scratch(cn, sizeof(int) * (size_t)S.cap[tt - 1]);
+          if (!D.claim[tt - 1]) return LEPIC_ERR_CUDA;
+          LEPIC_CUDA(cudaMemsetAsync(D.claim[tt - 1], 0, sizeof(int) * (size_t)S.cap[tt - 1], s));
+        }
+      }
       c.ind[r] = ind;
       c.tt[r] = tt;
       c.n_re[r] = n_re;
@@ -512,7 +679,7 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
     }
     timer_stop(tm, s);
     tm = timer_start(tname, s);
-    k_mcc_collide<Acc><<<ctx().sms * 8, MB, 0, s>>>(c, S, cand, ncand + (p - 1), T.sig_Er, T.sig,
+    k_mcc_collide<Acc><<<ctx().sms * 8, MB, 0, s>>>(c, S, D, cand, ncand + (p - 1), T.sig_Er, T.sig,
                                                     flag_dead[p - 1], add, cnt, cc, ctx().d_err);
     timer_stop(tm, s);
     LEPIC_CUDA(cudaGetLastError());
@@ -521,11 +688,16 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
                                  ntype > 2 ? counts_dev[2] : nullptr, add, ntype, S.cap[0],
                                  ntype > 1 ? S.cap[1] : 0, ntype > 2 ? S.cap[2] : 0);
   LEPIC_CUDA(cudaGetLastError());
-  unsigned long long hc[64];
+  unsigned long long hc[64], hs[2];
   LEPIC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, s));
+  LEPIC_CUDA(cudaMemcpyAsync(hs, D.stat, sizeof(hs), cudaMemcpyDeviceToHost, s));
   const int rc = check_err(s);
   if (counts)
     for (int q = 0; q < T.ncol; ++q) counts[q] += (long long)hc[q];
+  if (tg) {
+    tg->missed += (long long)hs[0];
+    tg->lost_claims += (long long)hs[1];
+  }
   return rc;
 }
 
@@ -534,7 +706,7 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
 int launch_collisions(const lepic_grid_t &g, lepic_species_f64_t *sp, int ntype,
                       const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
                       unsigned long long call_index, double *nu_max, long long *counts,
-                      cudaStream_t s, const RegionCount *rg) {
+                      cudaStream_t s, const RegionCount *rg, lepic_targets_t *tg) {
   if (ntype > 3) return LEPIC_ERR_UNSUPPORTED;
   AccF64 S;
   memset(&S, 0, sizeof(S));
@@ -547,13 +719,13 @@ int launch_collisions(const lepic_grid_t &g, lepic_species_f64_t *sp, int ntype,
     cnts[p] = sp[p].count;
     fd[p] = sp[p].flag_dead;
   }
-  return run_collisions(g, S, cnts, fd, ntype, T, P, seed, call_index, nu_max, counts, s, rg, "mcc_f64");
+  return run_collisions(g, S, cnts, fd, ntype, T, P, seed, call_index, nu_max, counts, s, rg, "mcc_f64", tg, 0);
 }
 
 int launch_collisions_mixed(const lepic_grid_t &g, lepic_species_mixed_t *sp, int ntype,
                             const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
                             unsigned long long call_index, double *nu_max, long long *counts,
-                            cudaStream_t s) {
+                            cudaStream_t s, lepic_targets_t *tg) {
   if (ntype > 3) return LEPIC_ERR_UNSUPPORTED;
   AccMixed S;
   memset(&S, 0, sizeof(S));
@@ -568,7 +740,7 @@ int launch_collisions_mixed(const lepic_grid_t &g, lepic_species_mixed_t *sp, in
     fd[p] = sp[p].flag_dead;
   }
   return run_collisions(g, S, cnts, fd, ntype, T, P, seed, call_index, nu_max, counts, s, nullptr,
-                        "mcc_mixed");
+                        "mcc_mixed", tg, 1);
 }
 
 }  // namespace lepic
@@ -579,5 +751,15 @@ extern "C" int lepic_dev_collisions_mixed(const lepic_grid_t *g, lepic_species_m
                                           double *nu_max, long long *counts, void *stream) {
   if (!g || !sp || !T || !P || ntype < 1) return LEPIC_ERR_ARG;
   return lepic::launch_collisions_mixed(*g, sp, ntype, *T, *P, seed, call_index, nu_max, counts,
-                                        (cudaStream_t)stream);
+                                        (cudaStream_t)stream, nullptr);
+}
+
+extern "C" int lepic_dev_collisions_mixed_targets(const lepic_grid_t *g, lepic_species_mixed_t *sp, int ntype,
+                                                  const lepic_tables_t *T, const lepic_phys_t *P,
+                                                  unsigned long long seed, unsigned long long call_index,
+                                                  double *nu_max, long long *counts, lepic_targets_t *tg,
+                                                  void *stream) {
+  if (!g || !sp || !T || !P || !tg || ntype < 1) return LEPIC_ERR_ARG;
+  return lepic::launch_collisions_mixed(*g, sp, ntype, *T, *P, seed, call_index, nu_max, counts,
+                                        (cudaStream_t)stream, tg);
 }

@@ -992,6 +992,9 @@ int launch_sort_mixed(const lepic_grid_t &g, lepic_species_mixed_t &sp, int n_hi
   timer_stop(t1, s);
   if (rc) return rc;
   if (sp.tile_off) k_tile_offsets<<<grid_for(ntiles + 1, 256), 256, 0, s>>>(cnt, ntiles, sp.tile_off);
+  // the start of every cell, kept for charged-target collisions
+  if (sp.cell_off)
+    LEPIC_CUDA(cudaMemcpyAsync(sp.cell_off, cnt, sizeof(int) * (size_t)(nkeys + 1), cudaMemcpyDeviceToDevice, s));
   LEPIC_CUDA(cudaFuncSetAttribute(k_msort_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SC_SMEM));
   int t2 = timer_start("sort_scatter_mixed", s);
   k_msort_scatter<<<grid_for(nthreads, SC_N), SC_T, SC_SMEM, s>>>(sp.cell, sp.p, sp.cell_alt, sp.p_alt, sp.cap,

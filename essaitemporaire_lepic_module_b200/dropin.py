@@ -245,10 +245,13 @@ def part_sorting(st, vxp, np_tot, ptype):
 
 
 def collisions(st, it, vxp, np_tot, flag_dead, iseed, np_red=None, ncol_mx=65, npt_mx=1300,
-               regions=(), cnt_col=None):
+               regions=(), cnt_col=None, Plist=None):
     """Src/collisions.f90:1 -- in place on vxp / np_tot / flag_dead.
     regions: [(ixl, ixr)] x-ranges of the counting regions (n_rg of them)
     sharing the y/z range of the whole grid, like conditions.inp's regions.
+    Charged targets (DSMC) need Plist, the per-species cell offsets of the
+    last part_sorting (ntype rows of pl_max+1), and np_red, the densities:
+    dens_red runs on np_red first, as in Src/main.f90:1194, to set np_mx.
     Returns the per-species nu_max written to COMMON /part_info_dp_3/."""
     T = st.tables
     ncol = T.sig.shape[0]
@@ -279,12 +282,19 @@ def collisions(st, it, vxp, np_tot, flag_dead, iseed, np_red=None, ncol_mx=65, n
         cnt_col = np.zeros((max(n_rg, 1), 1, ncol_mx))
     if np_red is None:
         np_red = np.zeros((st.ntype,) + tuple(st.geom.bcnd.shape))
+    else:
+        np_red = np.ascontiguousarray(np_red, dtype=np.float64)
+        dens_red(st, np_red)
     zi = np.zeros(16, dtype=np.int32)
     zd = np.zeros(16)
-    pl = np.zeros(1, dtype=np.int32)
+    if Plist is None:
+        pl, plm = np.zeros(1, dtype=np.int32), 0
+    else:
+        pl = np.ascontiguousarray(np.stack([np.asarray(r, dtype=np.int32) for r in Plist]))
+        plm = pl.shape[1] - 1
     lib().collisions_(_i(it), _pd(vxp), _pi(n), _pd(h), _i(st.ntype), _i(vxp.shape[1]), _pd(sig),
                       _pd(sig_Er), _pi(sig_list), _pd(sig_Eex), _i(ncol_mx), _i(npt_mx), _pd(cnt_col),
-                      _pd(zd), _pi(zi), _pi(zi), _pi(pl), _i(0), _pd(sigv), _pi(col_info), _pd(np_red),
+                      _pd(zd), _pi(zi), _pi(zi), _pi(pl), _i(plm), _pd(sigv), _pi(col_info), _pd(np_red),
                       flag_dead.ctypes.data_as(_lib.P_i8), _pi(zi), _i(1), _pi(np_tot), _pi(iseed),
                       _i(1), _i(0), _pd(zd), _pd(zd), _pd(zd), _i(0))
     check(lib().lepic_gpu_last_error(), "collisions")

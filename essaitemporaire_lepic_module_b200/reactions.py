@@ -204,6 +204,17 @@ def ordering(chem: Chemistry, qe=QE):
                   Eth=chem.Eth.copy(), col_info=chem.col_info.copy())
 
 
+def coulomb_table_synthetic(sigma0, E0=1.0, npts=400, emax=1000.0):
+    """A synthetic e-Ar+ elastic reaction with a charged target (DSMC): sigma =
+    sigma0 below E0 eV and sigma0 (E0/E)^2 above, the Coulomb-like fall of the
+    reference's [e]+[Ar+]->[e]+[Ar+] table."""
+    E = np.concatenate([[0.0], np.geomspace(1e-3, emax, npts)])
+    S = np.full_like(E, sigma0)
+    m = E > E0
+    S[m] = sigma0 * (E0 / E[m]) ** 2
+    return ("[e]+[Ar+]->[e]+[Ar+]", 0.0, 0.0, 1.0, 1.0, "COLLISION", E, S)
+
+
 def argon_tables_synthetic(npts=400, emax=1000.0):
     """The synthetic analytic e-Ar / Ar+-Ar cross sections of the 128^3
     benchmark: elastic 1e-19 m^2, excitation 1.5e-21 m^2 above 11.5 eV,

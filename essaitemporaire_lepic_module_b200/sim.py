@@ -30,7 +30,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import (LepicGrid, LepicSpeciesF64, LepicSpeciesMixed, LepicTables, check, lib,
+from ._lib import (LepicGrid, LepicSpeciesF64, LepicSpeciesMixed, LepicTables, LepicTargets, check, lib,
                    phys_struct)
 
 
@@ -126,8 +126,16 @@ class SpeciesMixed:
         self.count = torch.zeros(1, dtype=torch.int32, device=device)
         self.flag_dead = torch.zeros(self.cap, dtype=torch.int8, device=device)
         self.tile_off = torch.zeros(tiles_of(n) + 1, dtype=torch.int32, device=device)
+        self.cell_off = None        # per-cell starts of the last sort (charged targets)
         self.s = LepicSpeciesMixed()
         self._sync_struct()
+
+    def keep_cell_offsets(self, n):
+        """Have every sort keep the start of each cell (for charged-target
+        collisions): LEPIC_TILES(n) * 512 + 1 ints."""
+        if self.cell_off is None:
+            self.cell_off = torch.zeros(tiles_of(n) * 512 + 1, dtype=torch.int32, device=self.count.device)
+            self._sync_struct()
 
     def _sync_struct(self):
         s = self.s
@@ -135,6 +143,7 @@ class SpeciesMixed:
         s.cell_alt, s.p_alt = self.cell_alt.data_ptr(), self.p_alt.data_ptr()
         s.count, s.flag_dead, s.cap = self.count.data_ptr(), self.flag_dead.data_ptr(), self.cap
         s.tile_off = self.tile_off.data_ptr()
+        s.cell_off = None if self.cell_off is None else self.cell_off.data_ptr()
 
     def after_call(self):
         if self.s.p != self.p.data_ptr():
@@ -270,6 +279,18 @@ class Simulation:
         t.sigv_mx = self._sv_h.ctypes.data
         t.col_info_h = self._ci_h.ctypes.data
         self._tables = t
+        # charged target species (DSMC): sorted on every collision step, their
+        # per-cell offsets kept (Src/collisions.f90:335-423)
+        st = self.st
+        self.dsmc_targets = sorted({int(T.col_info[c, 2 + T.col_info[c, 0] - 1]) - 1
+                                    for c in range(ncol)
+                                    if st.charge[int(T.col_info[c, 2 + T.col_info[c, 0] - 1]) - 1] != 0.0})
+        self._targets = None
+        if self.dsmc_targets:
+            self._targets = LepicTargets()
+            if self.mixed:
+                for q in self.dsmc_targets:
+                    self.sp[q].keep_cell_offsets(st.n)
 
     # ----------------------------------------------------------- loading
     def _f64_stage(self):
@@ -415,10 +436,12 @@ class Simulation:
                 s.after_call()
             return
         pl_max = self.st.n[0] + self.st.n[0] * (self.st.n[1] + self.st.n[1] * self.st.n[2]) + 1
-        if not hasattr(self, "_plist") or self._plist.numel() < pl_max + 1:
-            self._plist = torch.zeros(pl_max + 1, dtype=torch.int32, device=self.dev)
+        if not hasattr(self, "_plist_sp"):
+            # per-species cell offsets (Plist) of the last sort
+            self._plist_sp = [torch.zeros(pl_max + 1, dtype=torch.int32, device=self.dev) for _ in self.sp]
         for s in todo:
-            check(lib().lepic_dev_part_sorting(C.byref(self.grid), C.byref(s.s), _ptr(self._plist),
+            q = self.sp.index(s)
+            check(lib().lepic_dev_part_sorting(C.byref(self.grid), C.byref(s.s), _ptr(self._plist_sp[q]),
                                                pl_max, self._s()), "part_sorting")
             s.after_call()
 
@@ -427,14 +450,34 @@ class Simulation:
             return
         nu = (C.c_double * 10)()
         cnt = (C.c_longlong * 64)()
+        tg = self._targets
+        if tg is not None:
+            # dens_red before the collisions (Src/main.f90:1194): np_mx of the
+            # charged species for nu_max; the density grids and the offsets of
+            # the target species' sort of this step
+            mx = (C.c_double * 10)()
+            check(lib().lepic_dev_dens_red(C.byref(self.grid), _ptr(self.np), None, self.st.ntype, mx,
+                                           self._s()), "dens_red")
+            for q in range(self.st.ntype):
+                self.P.np_mx[q] = mx[q]
+            for q in self.dsmc_targets:
+                tg.np[q] = self.np[q].data_ptr()
+                tg.cell_off[q] = (self.sp[q].cell_off.data_ptr() if self.mixed else self._plist_sp[q].data_ptr())
         if self.mixed:
             arr = (LepicSpeciesMixed * len(self.sp))(*[s.s for s in self.sp])
             fn, name = lib().lepic_dev_collisions_mixed, "collisions_mixed"
+            if tg is not None:
+                fn, name = lib().lepic_dev_collisions_mixed_targets, "collisions_mixed_targets"
         else:
             arr = (LepicSpeciesF64 * len(self.sp))(*[s.s for s in self.sp])
             fn, name = lib().lepic_dev_collisions, "collisions"
-        check(fn(C.byref(self.grid), arr, len(self.sp), C.byref(self._tables), C.byref(self.P),
-                 C.c_ulonglong(self.seed), C.c_ulonglong(self.it), nu, cnt, self._s()), name)
+            if tg is not None:
+                fn, name = lib().lepic_dev_collisions_targets, "collisions_targets"
+        args = [C.byref(self.grid), arr, len(self.sp), C.byref(self._tables), C.byref(self.P),
+                C.c_ulonglong(self.seed), C.c_ulonglong(self.it), nu, cnt]
+        if tg is not None:
+            args.append(C.byref(tg))
+        check(fn(*args, self._s()), name)
         self.counts[:64] += np.array(cnt[:], dtype=np.int64)
         self.nu_max[:] = nu[:]
 
@@ -518,9 +561,13 @@ class Simulation:
         self.pdesolver()
         self.efield()
         due = [p for p, k in enumerate(self.sort_every) if k and it % k == 1 % k]
+        mcc = self._tables is not None and it > 1 and it % self.ns_coll == 1 % self.ns_coll
+        if mcc and self._targets is not None:
+            # charged targets are picked from the cells of this step's sort
+            due = sorted(set(due) | set(self.dsmc_targets))
         if due:
             self.sort(due)
-        if self._tables is not None and it > 1 and it % self.ns_coll == 1 % self.ns_coll:
+        if mcc:
             self.collisions()
         hp = self.heat_params if self.heat is not None else None
         if hp is not None and hp["flag_heat"] and it % hp["ns_heat"] == 0:

@@ -147,7 +147,9 @@ void part_sorting_(double *vxp, double *sorting, const int *nmax, const int *nty
                    const int *np_tot, const int *ptype);
 
 /* Src/collisions.f90:1 -- null-collision Monte Carlo against neutral
- * targets.  Same 29 arguments.  The GPU draws from a Philox4x32-10 counter
+ * targets (MC) and charged targets (DSMC, picked in the incident's cell with
+ * Plist from part_sorting_ and weighted by np_red from dens_red).  Same 29
+ * arguments.  The GPU draws from a Philox4x32-10 counter
  * stream keyed by iseed(1) instead of the serial ran2 stream, so results
  * agree with the reference statistically (collision counts per process,
  * moments), not bit for bit.  cnt_col(ncol_mx,nproc,nm_rg) region counters
@@ -310,6 +312,8 @@ typedef struct {
   signed char *flag_dead; /* device int8[cap]                                 */
   int *tile_off;          /* device int[LEPIC_TILES(n)+1]                     */
   int cap;
+  int *cell_off;          /* device int[LEPIC_TILES(n)*512+1] or NULL: the sort
+                             writes the start of every cell (tile-key order)  */
 } lepic_species_mixed_t;
 
 /* Packed cell index of the mixed layout and the 8x8x8-cell tiles. */
@@ -471,6 +475,37 @@ int lepic_dev_heat_stats(const lepic_grid_t *g, const lepic_species_f64_t *e, co
 int lepic_dev_heat_stats_mixed(const lepic_grid_t *g, const lepic_species_mixed_t *e, const lepic_phys_t *P,
                                const lepic_heat_t *H, double *stats, void *stream);
 
+/* Charged targets (DSMC, Src/collisions.f90:335-423, 524-531) for the
+ * collision calls below.  Per species: np[p], the device density grid of the
+ * last deposition (np_red, (n1+3)(n2+3)(n3+3)); cell_off[p], the device
+ * per-cell offsets of that species' last sort: for the FP64 layout the Plist
+ * of lepic_dev_part_sorting (inclusive ends at the reference's linear cell
+ * index, pl_max+1 entries), for the mixed layout the cell_off of
+ * lepic_species_mixed_t (exclusive starts at the 8x8x8-tile key).  A target
+ * is a particle of its species in the incident's cell, else in the first
+ * non-empty neighbour cell in the reference's order; the species must not
+ * have moved since that sort.  The target density is the mean of np over the
+ * cell's 8 nodes; nu_max uses P->np_mx of the target species (dens_red's
+ * maximum, set by the caller).  A collision may change the target's
+ * velocity or remove it (flag_dead of the target species).  The outputs
+ * accumulate: missed, incident particles that found no target in reach (the
+ * reference's err_coll); lost_claims, collisions dropped because another
+ * incident particle of the same call had taken the target (the reference runs
+ * its collisions one after another). */
+typedef struct {
+  const double *np[LEPIC_NPART];
+  const int *cell_off[LEPIC_NPART];
+  long long missed, lost_claims;
+} lepic_targets_t;
+int lepic_dev_collisions_targets(const lepic_grid_t *g, lepic_species_f64_t *sp, int ntype,
+                                 const lepic_tables_t *T, const lepic_phys_t *P, unsigned long long seed,
+                                 unsigned long long call_index, double *nu_max, long long *counts,
+                                 lepic_targets_t *tg, void *stream);
+int lepic_dev_collisions_mixed_targets(const lepic_grid_t *g, lepic_species_mixed_t *sp, int ntype,
+                                       const lepic_tables_t *T, const lepic_phys_t *P, unsigned long long seed,
+                                       unsigned long long call_index, double *nu_max, long long *counts,
+                                       lepic_targets_t *tg, void *stream);
+
 /* GPU particle loader (counterpart of Src/load_part.f90:91-194 for the
  * large workloads): n_per_species samples, positions uniform in
  * [0,x_load) x [0,ymax) x [0,zmax) outside all-wall cells, shared by all
@@ -484,7 +519,8 @@ int lepic_dev_load_uniform(const lepic_grid_t *g, lepic_species_f64_t *sp, int n
  * cell_wall((n1+2)(n2+2)(n3+2)) from bcnd, both device. */
 int lepic_dev_cell_wall(const int *n, const int *bcnd, unsigned char *cell_wall, void *stream);
 
-/* Src/calc_rho.f90:116 (dens_red) on device grids; np_mx host [ntype]. */
+/* Src/calc_rho.f90:116 (dens_red) on device grids; np_mx host [ntype];
+ * np_red may be NULL (only np_mx wanted). */
 int lepic_dev_dens_red(const lepic_grid_t *g, const double *np, double *np_red, int ntype,
                        double *np_mx, void *stream);
 

@@ -129,6 +129,7 @@ class State:
         self.flag_dead = np.zeros((st.ntype, nmax), dtype=np.int8)
         self.np = np.zeros((st.ntype,) + tuple(st.geom.bcnd.shape))
         self.iseed = np.array([123456], dtype=np.int32)
+        self.Plist = None          # (ntype, pl_max+1) per-cell offsets of the last sort
 
     def copy(self):
         o = object.__new__(State)
@@ -137,6 +138,7 @@ class State:
         o.flag_dead = self.flag_dead.copy()
         o.np = self.np.copy()
         o.iseed = self.iseed.copy()
+        o.Plist = None if self.Plist is None else self.Plist.copy()
         return o
 
 
@@ -258,20 +260,37 @@ def tables_struct(T, keep):
     return OTables(ncol, npt, npt, _pd(Er), _pd(sig), _pd(Eth), _pi(ci), _pi(sl), _pi(pn), _pd(sv))
 
 
-def collisions(st, S):
-    """Src/collisions.f90 with one thread; returns (nu_max, counts, Nc)."""
+def pl_max_of(st):
+    return st.n[0] + st.n[0] * (st.n[1] + st.n[1] * st.n[2]) + 1
+
+
+def collisions(st, S, err=None):
+    """Src/collisions.f90 with one thread, after dens_red (Src/main.f90:1194:
+    np_mx of the charged species is the maximum of their density over the
+    plasma nodes); charged targets (DSMC) are picked with the per-cell
+    offsets S.Plist of the last sort.  Returns (nu_max, counts, Nc); err
+    (int64[ntype]) counts the incident particles that found no target."""
     keep = []
     T = tables_struct(st.tables, keep)
     n = np.array(st.n, dtype=np.int32)
     h = np.ascontiguousarray(st.h)
     P = ophys(st)
+    _, mx = dens_red(st, S.np)
+    for p in range(st.ntype):
+        P.np_mx[p] = mx[p]
     nu = np.zeros(10)
     cnt = np.zeros(64, dtype=np.int64)
     Nc = np.zeros(10, dtype=np.int32)
+    pl_max = pl_max_of(st)
+    if S.Plist is None:
+        S.Plist = np.zeros((st.ntype, pl_max + 1), dtype=np.int32)
+    if err is None:
+        err = np.zeros(st.ntype, dtype=np.int64)
     rc = lib().oracle_collisions(_pd(S.vxp), _pi(n), _pd(h), C.c_int(st.ntype),
                                  C.c_int(S.vxp.shape[1]), C.byref(T), S.flag_dead.ctypes.data_as(P_i8),
                                  _pi(S.np_tot), _pi(S.iseed), C.byref(P), _pd(nu),
-                                 cnt.ctypes.data_as(P_ll), _pi(Nc))
+                                 cnt.ctypes.data_as(P_ll), _pi(Nc), _pi(S.Plist), C.c_int(pl_max),
+                                 _pd(S.np), err.ctypes.data_as(P_ll))
     if rc:
         raise RuntimeError(f"oracle collisions status {rc}")
     return nu[:st.ntype], cnt[:T.ncol], Nc[:st.ntype]
@@ -319,7 +338,10 @@ def step(st, S, phi, Ei, it, p_mac=None, P_loss=None, nsort=10, ns_coll=10, mg=N
     if nsort and it % nsort == 1 % nsort:
         for p in range(1, st.ntype + 1):
             if S.np_tot[p - 1] > 0:
-                part_sorting(st, S, p)
+                pl = part_sorting(st, S, p)
+                if S.Plist is None:
+                    S.Plist = np.zeros((st.ntype, len(pl)), dtype=np.int32)
+                S.Plist[p - 1] = pl
     mcc = None
     if st.tables is not None and it > 1 and it % ns_coll == 1 % ns_coll:
         mcc = collisions(st, S)

@@ -1257,10 +1257,13 @@ void oracle_scatter(double *vx1, double *vy1, double *vz1, double vx, double vy,
 // of each reaction; Nc_out[ptype] the number of picks.
 int oracle_collisions(double *vxp, const int n[3], const double h[3], int ntype, int nmax,
                       const OTables *T, signed char *flag_dead, int *np_tot, int *iseed,
-                      const OPhys *P, double *nu_max, long long *cnt_col, int *Nc_out) {
-  (void)n;
-  (void)h;
+                      const OPhys *P, double *nu_max, long long *cnt_col, int *Nc_out,
+                      const int *Plist, int pl_max, const double *np_red, long long *err_coll) {
   const double qe = P->qe, pi = P->pi;
+  Dims d(n);
+  // Plist(0:pl_max, ntype) column-major; np_red(0:n1+2, 0:n2+2, 0:n3+2, ntype)
+  auto PL = [&](int ic, int t) { return Plist[ic + (long)(pl_max + 1) * (t - 1)]; };
+  auto NR = [&](int a, int b, int c, int t) { return np_red[d.g(a, b, c) + d.cnt() * (long)(t - 1)]; };
   auto CI = [&](int icol, int info) { return T->col_info[(icol - 1) + (long)T->ncol * (info - 1)]; };
   auto SL = [&](int p, int icol) { return T->sig_list[(p - 1) + ORACLE_NPART * (long)(icol - 1)]; };
   auto SVM = [&](int p, int icol) { return T->sigv_mx[(p - 1) + ORACLE_NPART * (long)(icol - 1)]; };
@@ -1303,7 +1306,10 @@ int oracle_collisions(double *vxp, const int n[3], const double h[3], int ntype,
       if (ip == np_tot[p - 1] + 1) return ORACLE_ERR_BAD_PICK;
       double *vi = vxp + ((long)(p - 1) * nmax + (ip - 1)) * 6;
       double vx[2] = {vi[3], 0}, vy[2] = {vi[4], 0}, vz[2] = {vi[5], 0};
-      int flag_ttype[ORACLE_NPART + 1] = {0};
+      int flag_ttype[ORACLE_NPART + 1] = {0}, flag_err[ORACLE_NPART + 1] = {0}, sav_it[ORACLE_NPART + 1] = {0};
+      // cell of the incident particle (Src/collisions.f90:289-300)
+      const int cix = (int)(vi[0] / h[0]) + 1, ciy = (int)(vi[1] / h[1]) + 1, ciz = (int)(vi[2] / h[2]) + 1;
+      const int ici = (cix - 1) + n[0] * ((ciy - 1) + n[1] * (ciz - 1)) + 1;
       double vr[ORACLE_NPART + 1] = {0}, Ekr[ORACLE_NPART + 1] = {0}, mu[ORACLE_NPART + 1] = {0};
       double vxc[ORACLE_NPART + 1] = {0}, vyc[ORACLE_NPART + 1] = {0}, vzc[ORACLE_NPART + 1] = {0};
       std::vector<double> nu(pn + 1, 0.0), sort_arr(pn, 0.0);
@@ -1311,18 +1317,45 @@ int oracle_collisions(double *vxp, const int n[3], const double h[3], int ntype,
       for (int icol = 1; icol <= pn; ++icol) {
         int ind = SL(p, icol);
         int tt = sav_ttype[ind];
+        if (flag_err[tt] == 1) continue;
         if (flag_ttype[tt] == 0) {
-          if (P->charge[tt - 1] != 0.0) return ORACLE_ERR_UNSUPPORTED;
-          rnd[0] = oracle_ran2(iseed);
-          rnd[1] = oracle_ran2(iseed);
-          oracle_load_gauss(&vx[1], &vy[1], P->vt0[tt - 1], rnd, pi);
-          if (vz_sav == 0.0) {
+          if (P->charge[tt - 1] != 0.0) {
+            // DSMC: a particle of the target species in the incident's cell,
+            // else in the first non-empty of the cells ici+1, ici-1, ici+n1,
+            // ici-n1, ici+n1 n2, ici-n1 n2 (Src/collisions.f90:335-423)
+            if (!Plist || !np_red) return ORACLE_ERR_UNSUPPORTED;
+            int ict = ici;
+            auto cnt_of = [&](int c) { return (c > 0 && c <= pl_max) ? PL(c, tt) - PL(c - 1, tt) : 0; };
+            int cnt = cnt_of(ict);
+            const int nb[6] = {ici + 1, ici - 1, ici + n[0], ici - n[0], ici + n[0] * n[1], ici - n[0] * n[1]};
+            for (int k = 0; k < 6 && cnt == 0; ++k) {
+              ict = nb[k];
+              cnt = cnt_of(ict);
+            }
+            if (cnt == 0) {
+              flag_err[tt] = 1;
+              if (err_coll) err_coll[p - 1] += 1;
+              continue;
+            }
+            rnd[0] = oracle_ran2(iseed);
+            int it = (int)(PL(ict, tt) * (1.0 - rnd[0]) + PL(ict - 1, tt) * rnd[0] + 1);
+            sav_it[tt] = it;
+            const double *vt = vxp + ((long)(tt - 1) * nmax + (it - 1)) * 6;
+            vx[1] = vt[3];
+            vy[1] = vt[4];
+            vz[1] = vt[5];
+          } else {
             rnd[0] = oracle_ran2(iseed);
             rnd[1] = oracle_ran2(iseed);
-            oracle_load_gauss(&vz[1], &vz_sav, P->vt0[tt - 1], rnd, pi);
-          } else {
-            vz[1] = vz_sav;
-            vz_sav = 0.0;
+            oracle_load_gauss(&vx[1], &vy[1], P->vt0[tt - 1], rnd, pi);
+            if (vz_sav == 0.0) {
+              rnd[0] = oracle_ran2(iseed);
+              rnd[1] = oracle_ran2(iseed);
+              oracle_load_gauss(&vz[1], &vz_sav, P->vt0[tt - 1], rnd, pi);
+            } else {
+              vz[1] = vz_sav;
+              vz_sav = 0.0;
+            }
           }
           mu[tt] = absm(p) * absm(tt) / (absm(p) + absm(tt));
           vr[tt] = std::sqrt((vx[0] - vx[1]) * (vx[0] - vx[1]) + (vy[0] - vy[1]) * (vy[0] - vy[1]) +
@@ -1348,6 +1381,11 @@ int oracle_collisions(double *vxp, const int n[3], const double h[3], int ntype,
             double sL = SIG(ipt - 1, ind), sR = SIG(ipt, ind);
             double sig_p = sL + (Ekr[tt] - EL) * (sR - sL) / (ER - EL);
             double np_t = P->np_mx[tt - 1];
+            if (P->charge[tt - 1] != 0.0)
+              np_t = 0.125 * (NR(cix, ciy, ciz, tt) + NR(cix + 1, ciy, ciz, tt) + NR(cix, ciy + 1, ciz, tt) +
+                              NR(cix + 1, ciy + 1, ciz, tt) + NR(cix, ciy, ciz + 1, tt) +
+                              NR(cix + 1, ciy, ciz + 1, tt) + NR(cix, ciy + 1, ciz + 1, tt) +
+                              NR(cix + 1, ciy + 1, ciz + 1, tt));
             nu[icol] = np_t * sig_p * vr[tt] / nu_max_omp;
             sum_nu = sum_nu + nu[icol];
             sort_arr[icol - 1] = nu[icol];
@@ -1411,7 +1449,10 @@ int oracle_collisions(double *vxp, const int n[3], const double h[3], int ntype,
           }
           if (rt == 1 || rt == 3) {
             if (bt == p) ib = ip;
-            if (bt == tt) return ORACLE_ERR_UNSUPPORTED;  // charged target reuse
+            if (bt == tt) {
+              if (P->charge[tt - 1] == 0.0) return ORACLE_ERR_UNSUPPORTED;  // a neutral target has no slot
+              ib = sav_it[tt];
+            }
             opt_add = 0;
             flag_add[1] = flag_add[2] = 0;
           }
@@ -1439,6 +1480,7 @@ int oracle_collisions(double *vxp, const int n[3], const double h[3], int ntype,
           }
           if (flag_add[i_re] == -1) {
             if (ct == p) flag_dead[(long)(ct - 1) * nmax + (ip - 1)] = 1;
+            else if (ct == tt && P->charge[tt - 1] != 0.0) flag_dead[(long)(ct - 1) * nmax + (sav_it[tt] - 1)] = 1;
             else return ORACLE_ERR_UNSUPPORTED;
           }
         }
@@ -1446,12 +1488,21 @@ int oracle_collisions(double *vxp, const int n[3], const double h[3], int ntype,
         for (int i_by = 1; i_by <= n_by; ++i_by) {
           int bt = CI(c_ind, 2 + n_re + i_by);
           if (P->mass[bt - 1] <= 0) continue;
-          if (bt != p) return ORACLE_ERR_UNSUPPORTED;
-          // ind_ce = 1 + 1 -> 2: the incident particle takes the target's
-          // velocity (Src/collisions.f90:956-971)
-          vi[3] = vx[1];
-          vi[4] = vy[1];
-          vi[5] = vz[1];
+          if (bt == p) {
+            // ind_ce = 1 + 1 -> 2: the incident particle takes the target's
+            // velocity (Src/collisions.f90:956-971)
+            vi[3] = vx[1];
+            vi[4] = vy[1];
+            vi[5] = vz[1];
+          } else if (bt == tt && P->charge[tt - 1] != 0.0) {
+            // ind_ce = 2 + 1 -> 1: a charged target takes the incident's
+            double *vb = vxp + ((long)(tt - 1) * nmax + (sav_it[tt] - 1)) * 6;
+            vb[3] = vx[0];
+            vb[4] = vy[0];
+            vb[5] = vz[0];
+          } else {
+            return ORACLE_ERR_UNSUPPORTED;
+          }
         }
       }
     }

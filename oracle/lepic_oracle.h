@@ -130,7 +130,8 @@ int oracle_ordering(int ncol, const int *sig_npt, const double *sig_tmp_E,
 int oracle_collisions(double *vxp, const int n[3], const double h[3], int ntype,
                       int nmax, const OTables *T, signed char *flag_dead,
                       int *np_tot, int *iseed, const OPhys *P, double *nu_max,
-                      long long *cnt_col, int *Nc_out);
+                      long long *cnt_col, int *Nc_out, const int *Plist,
+                      int pl_max, const double *np_red, long long *err_coll);
 void oracle_scatter(double *vx1, double *vy1, double *vz1, double vx, double vy,
                     double vz, double costheta, double phi);
 void oracle_eheating(const double h[3], double *vxp, int nmax, int *iseed, const int *np_tot,
