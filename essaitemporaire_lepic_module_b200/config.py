@@ -222,7 +222,10 @@ def mg_levels(n, ng_default):
     return ng_default
 
 
-def build(wl: Workload | str) -> Setup:
+def build(wl: Workload | str, chem=None) -> Setup:
+    """The set-up of a workload; chem: a reactions.Chemistry that replaces
+    the workload's own species and reactions (e.g. a chemistry file of the
+    reference read with reactions.read_dat)."""
     if isinstance(wl, str):
         wl = workload(wl)
     n = tuple(wl.n)
@@ -241,10 +244,11 @@ def build(wl: Workload | str) -> Setup:
     reacts = rx.argon_tables_synthetic() if ngas > 0 else []
     if wl.coulomb > 0:
         reacts = [rx.coulomb_table_synthetic(wl.coulomb)] + reacts
-    with tempfile.TemporaryDirectory() as td:
-        path = os.path.join(td, "chem.dat")
-        rx.write_dat(path, wl.ions, neutrals, reacts)
-        chem = rx.read_dat(path, wl.Te, ngas)
+    if chem is None:
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "chem.dat")
+            rx.write_dat(path, wl.ions, neutrals, reacts)
+            chem = rx.read_dat(path, wl.Te, ngas)
     ntype = chem.ntype
     n_neu = chem.n_neu
     charge = np.zeros(NPART)

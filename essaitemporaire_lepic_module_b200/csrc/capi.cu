@@ -634,7 +634,7 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
   (void)ss2D_yz;
   if (*nproc != 1 || *nproc_mpi != 1 || *flag_diag != 0) return record(LEPIC_ERR_UNSUPPORTED);
   const int nt = *ntype;
-  if (nt > 3) return record(LEPIC_ERR_UNSUPPORTED);
+  if (nt < 1 || nt > LEPIC_NPART) return record(LEPIC_ERR_ARG);
   cudaStream_t s = 0;
   Dims d(n);
   lepic_phys_t P = phys_from_common(nt);
@@ -711,8 +711,8 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
       cc_h[c + (size_t)*ncol_mx * q] = cnt_col[c + (size_t)*ncol_mx * (size_t)(*nproc) * q];
   rgc.cnt_col_dev = upload("dropin_cntcol", cc_h.data(), ncc, s);
   if (!rgc.cnt_col_dev) return record(LEPIC_ERR_CUDA);
-  SpeciesView v[3];
-  lepic_species_f64_t sp[3];
+  SpeciesView v[LEPIC_NPART];
+  lepic_species_f64_t sp[LEPIC_NPART];
   for (int p = 0; p < nt; ++p) {
     rc = acquire_species(v[p], vxp + 6LL * *nmax * p, np_tot[p], *nmax, p,
                          flag_dead + (long long)*nmax * p, s);

@@ -45,7 +45,7 @@ namespace lepic {
 namespace {
 
 constexpr int MB = 256;
-constexpr int MAXR = 8;   // reactions per incident species
+constexpr int MAXR = 48;  // reactions per incident species (hydrogen.dat's electrons: 40)
 constexpr int MAXBY = 4;  // byproducts per reaction
 
 struct MCCConst {
@@ -528,11 +528,15 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
 
 // the appended products enter the counts; appends beyond the capacity were
 // not written (LEPIC_ERR_CAPACITY is raised), so a count stops at its capacity
-__global__ void k_mcc_finalize(int *count0, int *count1, int *count2, const int *add, int ntype, long long cap0,
-                               long long cap1, long long cap2) {
-  int *cs[3] = {count0, count1, count2};
-  const long long caps[3] = {cap0, cap1, cap2};
-  for (int p = 0; p < ntype && p < 3; ++p)
+struct Counts {
+  int *count[LEPIC_NPART];
+  long long cap[LEPIC_NPART];
+};
+
+__global__ void k_mcc_finalize(Counts C, const int *add, int ntype) {
+  int *const *cs = C.count;
+  const long long *caps = C.cap;
+  for (int p = 0; p < ntype && p < LEPIC_NPART; ++p)
     if (cs[p]) {
       const long long v = (long long)*cs[p] + add[p];
       *cs[p] = (int)(v < caps[p] ? v : caps[p]);
@@ -546,7 +550,7 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
                    int ntype, const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
                    unsigned long long call_index, double *nu_max, long long *counts, cudaStream_t s,
                    const RegionCount *rg, const char *tname, lepic_targets_t *tg, int tile) {
-  if (ntype > 3) return LEPIC_ERR_UNSUPPORTED;
+  if (ntype < 1 || ntype > LEPIC_NPART) return LEPIC_ERR_ARG;
   // DSMC state: density grids and sort offsets from the caller, claims here
   Targets D;
   memset(&D, 0, sizeof(D));
@@ -588,7 +592,10 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
     nu_max[p - 1] = 0.0;
     const int pn = T.p_ncol[p - 1];
     if (pn == 0 || P.mass[p - 1] <= 0) continue;
-    if (pn > MAXR) return LEPIC_ERR_UNSUPPORTED;
+    if (pn > MAXR) {
+      fprintf(stderr, "lepic_gpu: collisions: species %d has %d reactions (at most %d)\n", p, pn, MAXR);
+      return LEPIC_ERR_UNSUPPORTED;
+    }
     MCCConst c;
     memset(&c, 0, sizeof(c));
     c.ptype = p;
@@ -604,11 +611,21 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
     for (int r = 0; r < pn; ++r) {
       const int ind = T.sig_list[(p - 1) + LEPIC_NPART * r];
       const int n_re = CI(ind, 1), n_by = CI(ind, 2);
-      if (n_by > MAXBY || n_re > 2) return LEPIC_ERR_UNSUPPORTED;
+      if (n_by > MAXBY || n_re > 2) {
+        fprintf(stderr, "lepic_gpu: collisions: reaction %d has %d reactants and %d byproducts (at most 2 and %d)\n",
+                ind, n_re, n_by, MAXBY);
+        return LEPIC_ERR_UNSUPPORTED;
+      }
       const int tt = CI(ind, 2 + n_re);
       if (P.charge[tt - 1] != 0.0) {
         // a charged target: its density grid and sort offsets are needed
-        if (tt > ntype || !D.np[tt - 1] || !D.off[tt - 1] || !D.fd[tt - 1]) return LEPIC_ERR_UNSUPPORTED;
+        if (tt > ntype || !D.np[tt - 1] || !D.off[tt - 1] || !D.fd[tt - 1]) {
+          fprintf(stderr,
+                  "lepic_gpu: collisions: reaction %d has the charged target species %d without its density "
+                  "grid, sort offsets or flag_dead (lepic_targets_t)\n",
+                  ind, tt);
+          return LEPIC_ERR_UNSUPPORTED;
+        }
         c.dsmc[r] = 1;
         c.any_dsmc = 1;
         if (!D.claim[tt - 1]) {
@@ -684,9 +701,13 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
     timer_stop(tm, s);
     LEPIC_CUDA(cudaGetLastError());
   }
-  k_mcc_finalize<<<1, 1, 0, s>>>(counts_dev[0], ntype > 1 ? counts_dev[1] : nullptr,
-                                 ntype > 2 ? counts_dev[2] : nullptr, add, ntype, S.cap[0],
-                                 ntype > 1 ? S.cap[1] : 0, ntype > 2 ? S.cap[2] : 0);
+  Counts fc;
+  memset(&fc, 0, sizeof(fc));
+  for (int q = 0; q < ntype; ++q) {
+    fc.count[q] = counts_dev[q];
+    fc.cap[q] = S.cap[q];
+  }
+  k_mcc_finalize<<<1, 1, 0, s>>>(fc, add, ntype);
   LEPIC_CUDA(cudaGetLastError());
   unsigned long long hc[64], hs[2];
   LEPIC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, s));
@@ -707,7 +728,7 @@ int launch_collisions(const lepic_grid_t &g, lepic_species_f64_t *sp, int ntype,
                       const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
                       unsigned long long call_index, double *nu_max, long long *counts,
                       cudaStream_t s, const RegionCount *rg, lepic_targets_t *tg) {
-  if (ntype > 3) return LEPIC_ERR_UNSUPPORTED;
+  if (ntype < 1 || ntype > LEPIC_NPART) return LEPIC_ERR_ARG;
   AccF64 S;
   memset(&S, 0, sizeof(S));
   int *cnts[LEPIC_NPART] = {nullptr};
@@ -726,7 +747,7 @@ int launch_collisions_mixed(const lepic_grid_t &g, lepic_species_mixed_t *sp, in
                             const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
                             unsigned long long call_index, double *nu_max, long long *counts,
                             cudaStream_t s, lepic_targets_t *tg) {
-  if (ntype > 3) return LEPIC_ERR_UNSUPPORTED;
+  if (ntype < 1 || ntype > LEPIC_NPART) return LEPIC_ERR_ARG;
   AccMixed S;
   memset(&S, 0, sizeof(S));
   int *cnts[LEPIC_NPART] = {nullptr};

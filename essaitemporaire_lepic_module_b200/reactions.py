@@ -146,6 +146,31 @@ def read_dat(path, Te, ngas):
                      Eth=np.array(Eth, dtype=np.float64), tables=tables)
 
 
+def chemistry_from_arrays(d, Te, ngas):
+    """A Chemistry from the arrays a chemistry fixture stores (species name,
+    mass in amu, charge in e, T in eV, n/n0; reaction label, col_info row,
+    threshold, E / sigma table), with the electron temperature Te and the
+    neutral density ngas applied as read_dat applies them."""
+    species = []
+    for k, name in enumerate(d["sp_name"]):
+        name = str(name)
+        if k == 0 and name == "[e]":
+            species.append(Species("[e]", ME, -QE, float(Te), 1.0))
+            continue
+        m, q, T, n = (float(d["sp_mass_amu"][k]) * AMU, float(d["sp_charge_e"][k]) * QE,
+                      float(d["sp_T"][k]), float(d["sp_n"][k]))
+        if q == 0.0:
+            n = n * ngas
+            m = -abs(m)
+        species.append(Species(name, m, q, T, n))
+    off = d["tab_off"]
+    tables = [(np.array(d["tab_E"][off[c]:off[c + 1]]), np.array(d["tab_S"][off[c]:off[c + 1]]))
+              for c in range(len(off) - 1)]
+    return Chemistry(species=species, labels=[str(x) for x in d["labels"]],
+                     col_info=np.array(d["col_info"], dtype=np.int32).reshape(-1, 10),
+                     Eth=np.array(d["Eth"], dtype=np.float64), tables=tables)
+
+
 @dataclass
 class Tables:
     sig_Er: np.ndarray     # merged energy grid (npt,)

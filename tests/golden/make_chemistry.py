@@ -1,0 +1,45 @@
+"""Generate the chemistry fixture of the reference's hydrogen source model.
+
+Reads the reference's input_dir/hydrogen.dat (5 charged species, 2 neutrals,
+60 reactions of every type, charged targets included) with the package's
+restatement of Src/read_reactions.f90 and stores the parsed chemistry in
+hydrogen_chem.npz: the species (name, mass in amu, charge in e, T in eV,
+n/n0 as the file gives them) and every reaction (label, col_info row,
+threshold, scaled E / sigma table).  The tests rebuild a Chemistry from it
+with reactions.chemistry_from_arrays, so they need no reference tree.
+
+Run here (the reference tree is read only):
+    python tests/golden/make_chemistry.py [/path/to/reference]
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from essaitemporaire_lepic_module_b200 import reactions as rx  # noqa: E402
+from essaitemporaire_lepic_module_b200.constants import AMU, QE  # noqa: E402
+
+
+def main(ref):
+    chem = rx.read_dat(os.path.join(ref, "input_dir", "hydrogen.dat"), Te=1.0, ngas=1.0)
+    sp = chem.species
+    E = [t[0] for t in chem.tables]
+    S = [t[1] for t in chem.tables]
+    off = np.concatenate([[0], np.cumsum([len(e) for e in E])]).astype(np.int64)
+    np.savez_compressed(
+        os.path.join(HERE, "hydrogen_chem.npz"),
+        sp_name=np.array([s.name for s in sp]),
+        sp_mass_amu=np.array([abs(s.mass) / AMU for s in sp]),
+        sp_charge_e=np.array([s.charge / QE for s in sp]),
+        sp_T=np.array([s.T for s in sp]),
+        sp_n=np.array([s.ni0 for s in sp]),
+        labels=np.array(chem.labels), col_info=chem.col_info, Eth=chem.Eth,
+        tab_off=off, tab_E=np.concatenate(E), tab_S=np.concatenate(S))
+    print("wrote", os.path.join(HERE, "hydrogen_chem.npz"), len(chem.labels), "reactions")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
