@@ -48,17 +48,24 @@ constexpr int MB = 256;
 constexpr int MAXR = 48;  // reactions per incident species (hydrogen.dat's electrons: 40)
 constexpr int MAXBY = 4;  // byproducts per reaction
 
+// one reaction of the incident species; the table lives in device memory
+// (runtime-indexed arrays in the kernel's parameters would be copied to
+// every thread's local memory)
+struct Reac {
+  int ind;                      // 1-based reaction index
+  int tt;                       // target species (1-based)
+  int rt, n_by, n_re;
+  int dsmc;                     // 1: charged target (DSMC)
+  int by[MAXBY];
+  double Eth, np_t;
+};
+
 struct MCCConst {
   int ptype, nr;
   double Pmax, nu_max, qe, pi;
   double m_p;                   // |mass| of incident
-  int ind[MAXR];                // 1-based reaction index
-  int tt[MAXR];                 // target species (1-based)
-  int rt[MAXR], n_by[MAXR], n_re[MAXR];
-  int dsmc[MAXR];               // 1: charged target (DSMC)
+  const Reac *R;                // device Reac[nr]
   int any_dsmc;
-  int by[MAXR][MAXBY];
-  double Eth[MAXR], np_t[MAXR];
   double mass[LEPIC_NPART];     // signed masses
   double vt0[LEPIC_NPART];
   int npt, npt_mx;
@@ -210,20 +217,23 @@ __device__ __forceinline__ void scatter(double &vx1, double &vy1, double &vz1, d
   }
 }
 
-// sigma(Ekr) on the merged grid: the unique interval Er[j-1] < E <= Er[j]
-// (Src/collisions.f90:485-521); 0 when E <= Er[0].
-__device__ __forceinline__ double sigma_at(const double *__restrict__ Er, const double *__restrict__ sig,
-                                           int npt, double E, int &found) {
-  found = 0;
-  if (!(E > Er[0]) || E > Er[npt - 1]) return 0.0;
+// the interval j of the merged grid with Er[j-1] < E <= Er[j], or -1 when
+// E <= Er[0] or E > Er[npt-1] (sigma 0), Src/collisions.f90:485-507
+__device__ __forceinline__ int energy_segment(const double *__restrict__ Er, int npt, double E) {
+  if (!(E > Er[0]) || E > Er[npt - 1]) return -1;
   int lo = 0, hi = npt - 1;  // Er[lo] < E <= Er[hi]
   while (hi - lo > 1) {
     int mid = (lo + hi) >> 1;
     if (E > Er[mid]) lo = mid;
     else hi = mid;
   }
-  found = 1;
-  double EL = Er[lo], ER = Er[hi], sL = sig[lo], sR = sig[hi];
+  return hi;
+}
+
+// linear interpolation of one table in interval j (Src/collisions.f90:510-521)
+__device__ __forceinline__ double sigma_in(const double *__restrict__ Er, const double *__restrict__ sig, int j,
+                                           double E) {
+  const double EL = Er[j - 1], ER = Er[j], sL = sig[j - 1], sR = sig[j];
   return sL + (E - EL) * (sR - sL) / (ER - EL);
 }
 
@@ -323,7 +333,7 @@ struct TState {
   bool ok;
 };
 
-template <class Acc>
+template <class Acc, bool DSMC>
 __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D, const int *__restrict__ cand,
                                                     const int *__restrict__ ncand_p,
                                                     const double *__restrict__ Er,
@@ -350,12 +360,12 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
       // the incident's cell (DSMC only)
       int cix = 1, ciy = 1, ciz = 1;
       long long ici = 0;
-      if (c.any_dsmc) {
+      if (DSMC) {
         S.cell_of(c, P, i, cix, ciy, ciz);
         ici = (cix - 1) + (long long)D.n1 * ((ciy - 1) + (long long)D.n2 * (ciz - 1)) + 1;
       }
       ctr.y = 3u;
-      const U4 r3 = c.any_dsmc ? philox4x32_10(ctr, c.k0, c.k1) : U4{0u, 0u, 0u, 0u};
+      const U4 r3 = DSMC ? philox4x32_10(ctr, c.k0, c.k1) : U4{0u, 0u, 0u, 0u};
       // the partner for target species tt: a Maxwellian neutral
       // (Src/collisions.f90:437-449; the same draws for every neutral
       // species) or a particle of a charged species (DSMC)
@@ -363,7 +373,7 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
         TState t;
         t.idx = -1;
         t.ok = true;
-        if (charged) {
+        if (DSMC && charged) {
           t.idx = pick_target(D, tt - 1, ici, r3.x);
           t.ok = t.idx >= 0;
           if (!t.ok) return t;
@@ -391,23 +401,23 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
       };
       TState ts;
       ts.ok = false;
-      int cur_tt = -1;
+      int cur_tt = -1, seg = -1;
       unsigned missed = 0u;
-      double nu[MAXR];
-      double sum_nu = 0.0;
-      for (int r = 0; r < c.nr; ++r) {
-        const int tt = c.tt[r];
+      // nu_r / nu_max of reaction r; the partner and the interval of the
+      // merged energy grid (shared by all tables) change with the target
+      // species only
+      auto nu_of = [&](int r) -> double {
+        const int tt = c.R[r].tt;
         if (tt != cur_tt) {
-          ts = partner(tt, c.dsmc[r] != 0);
+          ts = partner(tt, c.R[r].dsmc != 0);
           if (!ts.ok) missed |= 1u << tt;
+          seg = ts.ok ? energy_segment(Er, c.npt, ts.Ekr) : -1;
           cur_tt = tt;
         }
-        nu[r] = 0.0;
-        if (!ts.ok) continue;
-        int found;
-        const double sp = sigma_at(Er, sig + (long long)c.npt_mx * (c.ind[r] - 1), c.npt, ts.Ekr, found);
-        double np_t = c.np_t[r];
-        if (c.dsmc[r]) {
+        if (seg < 0) return 0.0;
+        const double sp = sigma_in(Er, sig + (long long)c.npt_mx * (c.R[r].ind - 1), seg, ts.Ekr);
+        double np_t = c.R[r].np_t;
+        if (DSMC && c.R[r].dsmc) {
           // the target density at the incident's cell (Src/collisions.f90:524-531)
           const double *g = D.np[tt - 1];
           const long long N1 = D.n1 + 3, N2 = D.n2 + 3;
@@ -415,52 +425,56 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
           np_t = 0.125 * (g[q] + g[q + 1] + g[q + sy] + g[q + 1 + sy] + g[q + sz] + g[q + 1 + sz] + g[q + sy + sz] +
                           g[q + 1 + sy + sz]);
         }
-        nu[r] = found ? np_t * sp * ts.vr / c.nu_max : 0.0;
-        sum_nu += nu[r];
-      }
-      if (missed) atomicAdd(&D.stat[0], (unsigned long long)__popc(missed));
+        return np_t * sp * ts.vr / c.nu_max;
+      };
+      // pass 1: sum_r nu_r; pass 2 (a collision): the same partial sums in
+      // the same order up to the drawn u (Src/collisions.f90:714-737)
+      double sum_nu = 0.0;
+      for (int r = 0; r < c.nr; ++r) sum_nu += nu_of(r);
+      if (DSMC && missed) atomicAdd(&D.stat[0], (unsigned long long)__popc(missed));
       const double u = u01(r0.y);
       if (u <= sum_nu) {
         double s = 0.0;
+        cur_tt = -1;
         for (int r = 0; r < c.nr; ++r) {
-          s += nu[r];
+          s += nu_of(r);
           if (u <= s) {
             sel = r;
             break;
           }
         }
       }
-      const bool tgt = sel >= 0 && c.dsmc[sel];
+      const bool tgt = DSMC && sel >= 0 && c.R[sel].dsmc;
       if (sel >= 0) {
-        if (c.tt[sel] != cur_tt) ts = partner(c.tt[sel], tgt);
+        if (c.R[sel].tt != cur_tt) ts = partner(c.R[sel].tt, tgt);
         // a charged target takes part in one collision per call
-        if (tgt && atomicExch(&D.claim[c.tt[sel] - 1][ts.idx], 1) != 0) {
+        if (tgt && atomicExch(&D.claim[c.R[sel].tt - 1][ts.idx], 1) != 0) {
           atomicAdd(&D.stat[1], 1ull);
           sel = -1;
         }
       }
       if (sel >= 0) {
-        const int rt = c.rt[sel];
-        const int T = c.tt[sel] - 1;
+        const int rt = c.R[sel].rt;
+        const int T = c.R[sel].tt - 1;
         const double mu_t = ts.mu, vr_t = ts.vr, vxc = ts.vxc, vyc = ts.vyc, vzc = ts.vzc;
         if (rt == 4) {
           // charge exchange (Src/collisions.f90:948-998): the incident takes
           // the target's velocity, a charged target the incident's
-          for (int a = 0; a < c.n_by[sel]; ++a) {
-            const int bt = c.by[sel][a];
+          for (int a = 0; a < c.R[sel].n_by; ++a) {
+            const int bt = c.R[sel].by[a];
             if (c.mass[bt - 1] <= 0) continue;
             if (bt == c.ptype) S.store_v(P, i, ts.tvx, ts.tvy, ts.tvz);
             else if (tgt && bt - 1 == T) S.store_v(T, ts.idx, vx0, vy0, vz0);
           }
         } else {
-          double Ee = 0.5 * mu_t * (vr_t * vr_t) - c.Eth[sel] * c.qe;
+          double Ee = 0.5 * mu_t * (vr_t * vr_t) - c.R[sel].Eth * c.qe;
           if (Ee < 0.0) {
             raise_err(err, LEPIC_ERR_NEG_ENERGY, (int)i);
             Ee = 0.0;
           }
-          const int nby = c.n_by[sel];
+          const int nby = c.R[sel].n_by;
           double sum_mass = 0.0;
-          for (int a = 0; a < nby; ++a) sum_mass = sum_mass + 1.0 / fabs(c.mass[c.by[sel][a] - 1]);
+          for (int a = 0; a < nby; ++a) sum_mass = sum_mass + 1.0 / fabs(c.mass[c.R[sel].by[a] - 1]);
           const double th_add = 2.0 * c.pi / (double)nby;
           const double cos_th = 1.0 - 2.0 * u01(r0.z);
           double th = acos(cos_th);
@@ -479,7 +493,7 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
             const double ex = cth, ey = sth * sin_ph, ez = sth * cos_ph;
             double ex1 = 0, ey1 = 0, ez1 = 0;
             scatter(ex1, ey1, ez1, ex, ey, ez, cos_th_s, phi_s);
-            const int bt = c.by[sel][a];
+            const int bt = c.R[sel].by[a];
             if (c.mass[bt - 1] <= 0) continue;
             const double mb = fabs(c.mass[bt - 1]);
             const double vp = sqrt(2.0 * (Ee / sum_mass) / (mb * mb));
@@ -509,7 +523,7 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
           for (int gq = 0; gq < c.n_rg; ++gq) {
             if (ix >= c.ixl[gq] && ix <= c.ixr[gq] && iy >= c.iyl && iy <= c.iyr && iz >= c.izl &&
                 iz <= c.izr) {
-              atomicAdd(&cnt_col[(c.ind[sel] - 1) + (long long)c.ncol_mx * gq], c.w_rg[gq]);
+              atomicAdd(&cnt_col[(c.R[sel].ind - 1) + (long long)c.ncol_mx * gq], c.w_rg[gq]);
               break;
             }
           }
@@ -520,7 +534,7 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
     if (__ballot_sync(full, sel >= 0)) {
       for (int r = 0; r < c.nr; ++r) {
         const unsigned m = __ballot_sync(full, sel == r);
-        if (lane == 0 && m) atomicAdd(&counts[c.ind[r] - 1], (unsigned long long)__popc(m));
+        if (lane == 0 && m) atomicAdd(&counts[c.R[r].ind - 1], (unsigned long long)__popc(m));
       }
     }
   }
@@ -598,6 +612,8 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
     }
     MCCConst c;
     memset(&c, 0, sizeof(c));
+    Reac hr[MAXR];
+    memset(hr, 0, sizeof(hr));
     c.ptype = p;
     c.nr = pn;
     c.qe = P.qe;
@@ -626,7 +642,7 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
                   ind, tt);
           return LEPIC_ERR_UNSUPPORTED;
         }
-        c.dsmc[r] = 1;
+        hr[r].dsmc = 1;
         c.any_dsmc = 1;
         if (!D.claim[tt - 1]) {
           char cn[32];
@@ -636,14 +652,14 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
           LEPIC_CUDA(cudaMemsetAsync(D.claim[tt - 1], 0, sizeof(int) * (size_t)S.cap[tt - 1], s));
         }
       }
-      c.ind[r] = ind;
-      c.tt[r] = tt;
-      c.n_re[r] = n_re;
-      c.n_by[r] = n_by;
-      for (int a = 0; a < n_by; ++a) c.by[r][a] = CI(ind, 3 + n_re + a);
-      c.rt[r] = CI(ind, 3 + n_re + n_by);
-      c.Eth[r] = Eth[ind - 1];
-      c.np_t[r] = P.np_mx[tt - 1];
+      hr[r].ind = ind;
+      hr[r].tt = tt;
+      hr[r].n_re = n_re;
+      hr[r].n_by = n_by;
+      for (int a = 0; a < n_by; ++a) hr[r].by[a] = CI(ind, 3 + n_re + a);
+      hr[r].rt = CI(ind, 3 + n_re + n_by);
+      hr[r].Eth = Eth[ind - 1];
+      hr[r].np_t = P.np_mx[tt - 1];
       num = num + P.np_mx[tt - 1] * T.sigv_mx[(p - 1) + LEPIC_NPART * (ind - 1)];
     }
     nu_max[p - 1] = num < P.nu_uplim[p - 1] ? num : P.nu_uplim[p - 1];
@@ -676,6 +692,13 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
       c.izr = rg->izr;
       cc = rg->cnt_col_dev;
     }
+    // the reaction table of this species, in device memory
+    char rn[32];
+    snprintf(rn, sizeof rn, "mcc_reac%d", p - 1);
+    Reac *R = (Reac *)scratch(rn, sizeof(Reac) * MAXR);
+    if (!R) return LEPIC_ERR_CUDA;
+    LEPIC_CUDA(cudaMemcpyAsync(R, hr, sizeof(Reac) * (size_t)pn, cudaMemcpyHostToDevice, s));
+    c.R = R;
     // the candidate list shares the species' work list with the push (hole
     // list), sized by the capacity, so that the step loop allocates nothing
     // after its first push
@@ -696,8 +719,12 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
     }
     timer_stop(tm, s);
     tm = timer_start(tname, s);
-    k_mcc_collide<Acc><<<ctx().sms * 8, MB, 0, s>>>(c, S, D, cand, ncand + (p - 1), T.sig_Er, T.sig,
-                                                    flag_dead[p - 1], add, cnt, cc, ctx().d_err);
+    if (c.any_dsmc)
+      k_mcc_collide<Acc, true><<<ctx().sms * 8, MB, 0, s>>>(c, S, D, cand, ncand + (p - 1), T.sig_Er, T.sig,
+                                                            flag_dead[p - 1], add, cnt, cc, ctx().d_err);
+    else
+      k_mcc_collide<Acc, false><<<ctx().sms * 8, MB, 0, s>>>(c, S, D, cand, ncand + (p - 1), T.sig_Er, T.sig,
+                                                             flag_dead[p - 1], add, cnt, cc, ctx().d_err);
     timer_stop(tm, s);
     LEPIC_CUDA(cudaGetLastError());
   }
