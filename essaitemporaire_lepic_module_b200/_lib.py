@@ -65,6 +65,15 @@ class LepicHeat(C.Structure):
                 ("R_ahp", C.c_double), ("nudt", C.c_double), ("Pabs", C.c_double), ("nu_h", C.c_double)]
 
 
+class LepicInject(C.Structure):
+    """lepic_inject_t: particle injection."""
+    _fields_ = [("opt_inj", C.c_int), ("ns_inj", C.c_int), ("n_cath", C.c_int), ("dir_sec", C.c_int),
+                ("tag_beam", C.c_int), ("flag_pbcz", C.c_int), ("I_inj", C.c_double),
+                ("xl", C.c_double), ("xr", C.c_double), ("yl", C.c_double), ("yr", C.c_double),
+                ("zl", C.c_double), ("zr", C.c_double), ("THm", C.c_double), ("zg_sec", C.c_double * 2),
+                ("ni0", C.c_double * NPART)]
+
+
 class LepicTables(C.Structure):
     _fields_ = [("ncol", C.c_int), ("npt", C.c_int), ("npt_mx", C.c_int),
                 ("sig_Er", C.c_void_p), ("sig", C.c_void_p), ("sig_Eth", C.c_void_p),
@@ -202,6 +211,15 @@ def lib():
         "lepic_dev_heat_stats_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), C.POINTER(LepicPhys),
                                         C.POINTER(LepicHeat), vp, vp], _I),
         "eheating_": ([P_dbl, P_dbl, P_int, P_int, P_int, P_int, P_int, P_dbl, P_int, P_dbl], None),
+        "part_injection_": ([P_int, P_dbl, P_int, P_dbl, P_int, P_int, P_int, P_int, P_int, P_dbl, P_dbl, P_dbl,
+                             P_dbl, P_dbl, P_dbl, P_dbl, P_int, P_int, P_int, P_int, P_int, P_int, P_dbl, P_dbl,
+                             P_dbl], None),
+        "lepic_dev_inject": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64), _I, C.POINTER(LepicPhys),
+                              C.POINTER(LepicInject), C.c_longlong, C.c_ulonglong, C.c_ulonglong, vp, vp, P_dbl,
+                              C.POINTER(C.c_longlong), vp], _I),
+        "lepic_dev_inject_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), _I, C.POINTER(LepicPhys),
+                                    C.POINTER(LepicInject), C.c_longlong, C.c_ulonglong, C.c_ulonglong, vp, vp,
+                                    P_dbl, C.POINTER(C.c_longlong), vp], _I),
         "lepic_dev_load_uniform": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64), _I,
                                     C.c_longlong, C.POINTER(LepicPhys), C.c_ulonglong, vp], _I),
         "lepic_dev_cell_wall": ([P_int, vp, vp, vp], _I),
@@ -263,6 +281,7 @@ def exported_symbols():
             "part_mover_", "charge_deposition_", "part_sorting_", "collisions_", "eheating_",
             "lepic_dev_eheating", "lepic_dev_eheating_mixed", "lepic_dev_heat_stats", "lepic_dev_heat_stats_mixed",
             "lepic_dev_collisions_targets", "lepic_dev_collisions_mixed_targets",
+            "part_injection_", "lepic_dev_inject", "lepic_dev_inject_mixed",
             "part_info_int_", "part_info_dp_1_", "part_info_dp_2_", "part_info_dp_3_", "constants_"]
 
 

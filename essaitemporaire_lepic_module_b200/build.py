@@ -20,7 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "liblepic_gpu.so")
 SOURCES = ["context.cu", "timing.cu", "fields.cu", "mg.cu", "particles.cu", "step.cu", "mcc.cu", "mixed.cu", "mgmixed.cu",
-           "adjoint.cu", "residency.cu", "heating.cu", "capi.cu"]
+           "adjoint.cu", "residency.cu", "heating.cu", "injection.cu", "capi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=default", "--expt-relaxed-constexpr"]

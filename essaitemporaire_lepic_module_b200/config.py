@@ -195,6 +195,31 @@ class Heating:
     flag_inj: int = 0
 
 
+@dataclass
+class Injection:
+    """Particle injection (Src/read_input.f90:75, Src/part_injection.f90):
+    opt_inj 1 (uniform in the box xl..zr, m), -1 (cosine / flat-top profile),
+    2 (as many events as ions lost to the walls), +-3 (electron beam of energy
+    THm eV), +-4 (cathode emission at the planes zg_sec); I_inj the injected
+    current (A); every ns_inj steps; ni0: the probability that an event
+    injects each species (default: the set-up's n/n0)."""
+    opt_inj: int
+    I_inj: float
+    xl: float
+    xr: float
+    yl: float
+    yr: float
+    zl: float
+    zr: float
+    ns_inj: int = 1
+    THm: float = 0.0
+    zg_sec: tuple = (0.0, 0.0)
+    n_cath: int = 1
+    dir_sec: int = 1
+    tag_beam: int = 0
+    ni0: tuple = None
+
+
 def heating_params(st, hz):
     """What Src/main.f90 derives from the heating input: ns_heat from
     kt = dt vt0(1) / min(h) (:548-554), nudt = nu_h ns_heat dt (:564), the

@@ -556,6 +556,66 @@ void charge_deposition_(const int *n, const double *h, const double *vxp, const 
   }
 }
 
+void part_injection_(const int *n, const double *h, const int *bcnd, double *vxp, int *sour_xy, int *sour_xz,
+                     int *sour_yz, const int *ntype, const int *nmax, const double *I_inj, const double *xl_pow,
+                     const double *xr_pow, const double *yl_pow, const double *yr_pow, const double *zl_pow,
+                     const double *zr_pow, int *np_tot, const int *nproc, int *iseed, const int *nproc_mpi,
+                     int *N_inj, const int *iproc, double *P_loss, const double *phi, const double *ni0) {
+  (void)sour_xy;
+  (void)sour_xz;
+  (void)sour_yz;
+  if (*nproc != 1 || *iproc != 1 || *nproc_mpi != 1) return record(LEPIC_ERR_UNSUPPORTED);
+  const int nt = *ntype;
+  if (nt < 1 || nt > LEPIC_NPART) return record(LEPIC_ERR_ARG);
+  static unsigned long long calls = 0;
+  lepic_phys_t P = phys_from_common(nt);
+  lepic_inject_t I;
+  memset(&I, 0, sizeof(I));
+  I.opt_inj = part_info_int_.opt_inj;
+  I.ns_inj = part_info_int_.ns_inj > 0 ? part_info_int_.ns_inj : 1;
+  I.n_cath = part_info_int_.n_cath;
+  I.dir_sec = part_info_int_.dir_sec;
+  I.tag_beam = part_info_int_.tag_beam;
+  I.flag_pbcz = part_info_int_.flag_pbcz;
+  I.I_inj = *I_inj;
+  I.xl = *xl_pow;
+  I.xr = *xr_pow;
+  I.yl = *yl_pow;
+  I.yr = *yr_pow;
+  I.zl = *zl_pow;
+  I.zr = *zr_pow;
+  I.THm = part_info_dp_1_.THm;
+  I.zg_sec[0] = part_info_dp_1_.zg_sec[0];
+  I.zg_sec[1] = part_info_dp_1_.zg_sec[1];
+  for (int p = 0; p < nt; ++p) I.ni0[p] = ni0[p];
+  cudaStream_t s = 0;
+  Dims d(n);
+  lepic_grid_t g;
+  int rc = stage_grid(g, n, h, bcnd, nullptr, s);
+  if (rc) return record(rc);
+  const double *phi_d = dev_view("dropin_u", phi, (size_t)d.cnt(), READ, s, &rc);
+  if (!phi_d) return record(rc);
+  SpeciesView v[LEPIC_NPART];
+  lepic_species_f64_t sp[LEPIC_NPART];
+  for (int p = 0; p < nt; ++p) {
+    rc = acquire_species(v[p], vxp + 6LL * *nmax * p, np_tot[p], *nmax, p, nullptr, s);
+    if (rc) return record(rc);
+    sp[p] = v[p].s;
+  }
+  // opt_inj 2: as many events as ions were lost to the walls (N_inj(2,iproc))
+  const long long nev = (I.opt_inj == 2 || I.opt_inj == -2) ? (nt > 1 ? N_inj[1] : 0) : -1;
+  double pl4[LEPIC_NPART] = {0};
+  rc = launch_inject(g, sp, nullptr, nt, P, I, nev, (unsigned long long)(unsigned)iseed[0], calls++, nullptr, phi_d,
+                     pl4, nullptr, s);
+  record(rc);
+  for (int p = 0; p < nt; ++p) {
+    v[p].s = sp[p];
+    record(release_species(v[p], &np_tot[p], nullptr, *nmax, true, s));
+  }
+  if (P_loss)
+    for (int p = 0; p < nt; ++p) P_loss[3 + 4 * p] += pl4[p];  // P_loss(4, p, 1)
+}
+
 void eheating_(const double *h, double *vxp, const int *nmax, const int *ntype, const int *nproc, int *iseed,
                const int *np_tot, const double *vt, const int *iproc, double *P_loss) {
   if (*nproc != 1 || *iproc != 1) return record(LEPIC_ERR_UNSUPPORTED);

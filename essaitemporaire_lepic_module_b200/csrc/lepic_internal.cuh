@@ -227,6 +227,12 @@ int launch_eheating(const lepic_grid_t &g, lepic_species_f64_t *e, lepic_species
 int launch_heat_stats(const lepic_grid_t &g, const lepic_species_f64_t *e, const lepic_species_mixed_t *m,
                       const lepic_phys_t &P, const lepic_heat_t &H, double *stats, cudaStream_t s);
 
+// injection.cu (e64 or m: the species in one of the two layouts)
+int launch_inject(const lepic_grid_t &g, lepic_species_f64_t *e64, lepic_species_mixed_t *m, int ntype,
+                  const lepic_phys_t &P, const lepic_inject_t &I, long long n_events, unsigned long long seed,
+                  unsigned long long call, double *const *np, const double *phi, double *P_loss4,
+                  long long *injected, cudaStream_t s);
+
 // residency.cu: device mirrors of the drop-ins' host arrays
 bool residency_on();
 // device pointer for host range [h, h + bytes) inside its mirror (created and

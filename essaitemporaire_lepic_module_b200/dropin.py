@@ -101,6 +101,49 @@ def set_commons(st, ncol=0, npt=0, p_ncol=None, heating=None):
         d2.R_ahp, d2.nudt, d2.Pabs, d2.nu_h = H.R_ahp, H.nudt, H.Pabs, H.nu_h
 
 
+def inject_struct(st, inj):
+    """lepic_inject_t of a config.Injection on the set-up st."""
+    I = _lib.LepicInject()
+    I.opt_inj, I.ns_inj, I.n_cath = int(inj.opt_inj), int(inj.ns_inj), int(inj.n_cath)
+    I.dir_sec, I.tag_beam, I.flag_pbcz = int(inj.dir_sec), int(inj.tag_beam), int(st.geom.flag_pbcz)
+    I.I_inj = float(inj.I_inj)
+    I.xl, I.xr, I.yl, I.yr, I.zl, I.zr = (float(v) for v in (inj.xl, inj.xr, inj.yl, inj.yr, inj.zl, inj.zr))
+    I.THm = float(inj.THm)
+    I.zg_sec[0], I.zg_sec[1] = (float(v) for v in inj.zg_sec)
+    ni0 = st.ni0 if inj.ni0 is None else inj.ni0
+    for i in range(st.ntype):
+        I.ni0[i] = float(ni0[i])
+    return I
+
+
+def part_injection(st, inj, vxp, np_tot, phi, P_loss, N_inj_ions=0, iseed=123456):
+    """Src/part_injection.f90:1 -- appends to vxp (ntype, nmax, 6) behind
+    np_tot; P_loss (ntype, 4) C-order, P_loss[p, 3] gains the injected power."""
+    cm = commons()
+    pi_, d1, d2 = cm["part_info_int"], cm["part_info_dp_1"], cm["part_info_dp_2"]
+    pi_.opt_inj, pi_.ns_inj, pi_.n_cath = int(inj.opt_inj), int(inj.ns_inj), int(inj.n_cath)
+    pi_.dir_sec, pi_.tag_beam, pi_.flag_pbcz = int(inj.dir_sec), int(inj.tag_beam), int(st.geom.flag_pbcz)
+    pi_.flag_inj = 1
+    d1.THm = float(inj.THm)
+    d1.zg_sec[0], d1.zg_sec[1] = (float(v) for v in inj.zg_sec)
+    n = _lib.np_i(st.n)
+    h = np.ascontiguousarray(st.h, dtype=np.float64)
+    bc = _lib.np_i(st.geom.bcnd)
+    assert vxp.flags["C_CONTIGUOUS"] and np_tot.dtype == np.int32 and P_loss.flags["C_CONTIGUOUS"]
+    ni0 = np.ascontiguousarray(st.ni0 if inj.ni0 is None else np.array(inj.ni0), dtype=np.float64)
+    f = np.ascontiguousarray(phi, dtype=np.float64)
+    zi = np.zeros(16, dtype=np.int32)
+    N_inj = np.zeros((1, st.ntype), dtype=np.int32)
+    if st.ntype > 1:
+        N_inj[0, 1] = int(N_inj_ions)
+    seed = np.array([iseed], dtype=np.int32)
+    lib().part_injection_(_pi(n), _pd(h), _pi(bc), _pd(vxp), _pi(zi), _pi(zi), _pi(zi), _i(st.ntype),
+                          _i(vxp.shape[1]), _d(inj.I_inj), _d(inj.xl), _d(inj.xr), _d(inj.yl), _d(inj.yr),
+                          _d(inj.zl), _d(inj.zr), _pi(np_tot), _i(1), _pi(seed), _i(1), _pi(N_inj), _i(1),
+                          _pd(P_loss), _pd(f), _pd(ni0))
+    check(lib().lepic_gpu_last_error(), "part_injection")
+
+
 def eheating(st, vxp, np_tot, vt, P_loss, iseed=123456):
     """Src/part_expmover.f90:484 -- heats species 1 of vxp (ntype, nmax, 6)
     in place; P_loss (ntype, 4) C-order, P_loss[0, 1] gains the energy."""

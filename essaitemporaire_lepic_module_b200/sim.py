@@ -163,7 +163,7 @@ class Simulation:
 
     def __init__(self, st, cap=None, device="cuda", seed=123456, nsort=None, ns_coll=None,
                  fused=True, precision="f64", mg_mixed=None, comm=None, sort_policy="reference",
-                 check_every=1, heating=None):
+                 check_every=1, heating=None, injection=None):
         if precision not in ("f64", "mixed"):
             raise ValueError(f"precision must be 'f64' or 'mixed', not {precision!r}")
         self.st = st
@@ -245,6 +245,19 @@ class Simulation:
         if st.tables is not None:
             self._setup_tables()
         # Maxwellian electron heating (Src/main.f90:1206-1240): a config.Heating
+        # particle injection after the push (Src/main.f90:1261-1267): a config.Injection
+        self.inj = None
+        if injection is not None:
+            from .dropin import inject_struct
+            self.inj = injection
+            self._I = inject_struct(st, injection)
+            if comm is not None:
+                # every rank holds the whole population at weight Nm / world
+                import torch.distributed as dist
+                self._I.I_inj = injection.I_inj / dist.get_world_size(None if comm is True else comm)
+            self._inj_calls = 0
+            self._inj_lost_seen = 0.0
+            self.injected = np.zeros(st.ntype, dtype=np.int64)
         self.heat = None
         if heating is not None:
             from .dropin import heat_struct
@@ -511,9 +524,10 @@ class Simulation:
         if self.comm is not None:
             allreduce_density(self.np, self._group)
 
-    def move_deposit(self):
+    def move_deposit(self, reduce=True):
         """Fused in-place push + deposition of every species (the step path);
-        lost particles are removed by hole filling."""
+        lost particles are removed by hole filling.  reduce: all-reduce the
+        density grids over the ranks (deferred while an injection follows)."""
         st = self.st
         if self._acc is None:
             self._acc = torch.zeros((st.ntype, 2 + 2 * (st.geom.ngrid + 1)), dtype=torch.float64,
@@ -537,7 +551,8 @@ class Simulation:
                                                C.c_void_p(self.np[p].data_ptr()),
                                                C.c_void_p(self._acc[p].data_ptr()), int(counts[p]),
                                                self._s()), "push_deposit")
-        self._reduce_density()
+        if reduce:
+            self._reduce_density()
 
     def loss_stats(self):
         """(p_mac (ngrid+1, 2, ntype), P_loss (ntype, 4)) accumulated so far."""
@@ -572,15 +587,50 @@ class Simulation:
         hp = self.heat_params if self.heat is not None else None
         if hp is not None and hp["flag_heat"] and it % hp["ns_heat"] == 0:
             self.eheating()
+        inj_due = self.inj is not None and it % max(int(self.inj.ns_inj), 1) == 0
         if self.fused:
-            self.move_deposit()
+            self.move_deposit(reduce=not inj_due)
         else:
             self.move()
             self.deposit()
+        if inj_due:
+            self.inject()
+            if self.fused:
+                self._reduce_density()
         if hp is not None and self.heat.Pabs > 0 and (it + 1) % hp["ns_heat"] == 0:
             self.heat_stats()
         if self.check_every and it % self.check_every == 0:
             self.check_device()
+
+    # ---------------------------------------------------------- injection
+    def inject(self):
+        """Src/part_injection.f90 after the push; the new particles are
+        deposited into the density grids as well (the fused push has already
+        deposited the others).  opt_inj 2: as many events as ions were lost to
+        the walls since the last injection."""
+        st = self.st
+        nev = -1
+        if abs(int(self.inj.opt_inj)) == 2:
+            pm, _ = self.loss_stats()
+            lost = float(pm[:, 0, 1].sum()) if st.ntype > 1 else 0.0
+            nev = int(round(lost - self._inj_lost_seen))
+            self._inj_lost_seen = lost
+        pl4 = (C.c_double * 10)()
+        got = (C.c_longlong * 10)()
+        nps = (C.c_void_p * 10)(*[self.np[p].data_ptr() for p in range(st.ntype)])
+        if self.mixed:
+            arr = (LepicSpeciesMixed * len(self.sp))(*[s.s for s in self.sp])
+            fn = lib().lepic_dev_inject_mixed
+        else:
+            arr = (LepicSpeciesF64 * len(self.sp))(*[s.s for s in self.sp])
+            fn = lib().lepic_dev_inject
+        check(fn(C.byref(self.grid), arr, st.ntype, C.byref(self.P), C.byref(self._I), nev,
+                 C.c_ulonglong(self.seed ^ 0x696E6A), C.c_ulonglong(self._inj_calls), nps, _ptr(self.phi), pl4, got,
+                 self._s()), "inject")
+        self._inj_calls += 1
+        for p in range(st.ntype):
+            self.P_loss[p, 3] += pl4[p]
+            self.injected[p] += got[p]
 
     # ------------------------------------------------------------ heating
     def heat_stats(self):

@@ -175,6 +175,20 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
 void eheating_(const double *h, double *vxp, const int *nmax, const int *ntype, const int *nproc, int *iseed,
                const int *np_tot, const double *vt, const int *iproc, double *P_loss);
 
+/* Src/part_injection.f90:1 -- injection of electron-ion pairs (opt_inj 1:
+ * uniform in the injection box, -1: cosine / flat-top profile, 2: as many
+ * events as ions were lost to the walls, N_inj(2,iproc)), of an electron beam
+ * (+-3) or of cathode electrons (+-4), appended behind np_tot; P_loss(4,:)
+ * gains the injected power.  COMMON: opt_inj, ns_inj, n_cath, dir_sec,
+ * tag_beam, flag_pbcz, THm, zg_sec, dt, Nm, vt0.  Draws come from a Philox
+ * stream keyed by iseed(1) and a call counter, not ran2.  The sour_xy,
+ * sour_xz, sour_yz planes are left untouched. */
+void part_injection_(const int *n, const double *h, const int *bcnd, double *vxp, int *sour_xy, int *sour_xz,
+                     int *sour_yz, const int *ntype, const int *nmax, const double *I_inj, const double *xl_pow,
+                     const double *xr_pow, const double *yl_pow, const double *yr_pow, const double *zl_pow,
+                     const double *zr_pow, int *np_tot, const int *nproc, int *iseed, const int *nproc_mpi,
+                     int *N_inj, const int *iproc, double *P_loss, const double *phi, const double *ni0);
+
 /* Status of the last drop-in call on this thread, then cleared. */
 int lepic_gpu_last_error(void);
 /* Human-readable text for a status code. */
@@ -446,6 +460,32 @@ int lepic_dev_collisions(const lepic_grid_t *g, lepic_species_f64_t *sp, int nty
                          const lepic_tables_t *T, const lepic_phys_t *P, unsigned long long seed,
                          unsigned long long call_index, double *nu_max, long long *counts,
                          void *stream);
+
+/* Particle injection (Src/part_injection.f90, Src/main.f90:1261-1267). */
+typedef struct {
+  int opt_inj;            /* 1, -1, 2, +-3, +-4 (see part_injection_)        */
+  int ns_inj;             /* steps between injections                        */
+  int n_cath, dir_sec, tag_beam, flag_pbcz;
+  double I_inj;           /* injected current, A                             */
+  double xl, xr, yl, yr, zl, zr; /* injection box xl_pow..zr_pow, m          */
+  double THm;             /* beam / cathode energy, eV                        */
+  double zg_sec[2];       /* emissive planes of the cathodes, m              */
+  double ni0[LEPIC_NPART]; /* probability that an event injects a species    */
+} lepic_inject_t;
+
+/* The injection on the device particles of either layout: n_events events
+ * (n_events < 0: the current I_inj ns_inj dt / (qe Nm(1)), rounded
+ * stochastically).  np: per-species device density grids to deposit the new
+ * particles into (the step loop, whose deposition ran before), or NULL.
+ * phi: device potential (beam power), or NULL.  P_loss4 (host [ntype]) and
+ * injected (host [ntype]) accumulate. */
+int lepic_dev_inject(const lepic_grid_t *g, lepic_species_f64_t *sp, int ntype, const lepic_phys_t *P,
+                     const lepic_inject_t *I, long long n_events, unsigned long long seed, unsigned long long call,
+                     double *const *np, const double *phi, double *P_loss4, long long *injected, void *stream);
+int lepic_dev_inject_mixed(const lepic_grid_t *g, lepic_species_mixed_t *sp, int ntype, const lepic_phys_t *P,
+                           const lepic_inject_t *I, long long n_events, unsigned long long seed,
+                           unsigned long long call, double *const *np, const double *phi, double *P_loss4,
+                           long long *injected, void *stream);
 
 /* Electron heating region and rate: ixl_pow, ixr_pow, flag_circxh, flag_ahp,
  * R_ahp (Src/main.f90:313, 612-614), nudt = nu_h ns_heat dt (Src/main.f90:

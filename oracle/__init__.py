@@ -60,6 +60,34 @@ def eheating(st, S, vt, P_loss, hz):
     return nh.value
 
 
+class OInject(C.Structure):
+    _fields_ = [("opt_inj", C.c_int), ("ns_inj", C.c_int), ("n_cath", C.c_int), ("dir_sec", C.c_int),
+                ("tag_beam", C.c_int), ("flag_pbcz", C.c_int), ("I_inj", C.c_double),
+                ("xl", C.c_double), ("xr", C.c_double), ("yl", C.c_double), ("yr", C.c_double),
+                ("zl", C.c_double), ("zr", C.c_double), ("THm", C.c_double), ("zg_sec", C.c_double * 2)]
+
+
+def part_injection(st, S, inj, phi, P_loss, N_inj_ions=0):
+    """Src/part_injection.f90 on S (serial ran2 on S.iseed); P_loss (ntype, 4)."""
+    I = OInject()
+    I.opt_inj, I.ns_inj, I.n_cath = int(inj.opt_inj), int(inj.ns_inj), int(inj.n_cath)
+    I.dir_sec, I.tag_beam, I.flag_pbcz = int(inj.dir_sec), int(inj.tag_beam), int(st.geom.flag_pbcz)
+    I.I_inj = float(inj.I_inj)
+    I.xl, I.xr, I.yl, I.yr, I.zl, I.zr = (float(v) for v in (inj.xl, inj.xr, inj.yl, inj.yr, inj.zl, inj.zr))
+    I.THm = float(inj.THm)
+    I.zg_sec[0], I.zg_sec[1] = (float(v) for v in inj.zg_sec)
+    n = np.array(st.n, dtype=np.int32)
+    h = np.ascontiguousarray(st.h)
+    bc = np.ascontiguousarray(st.geom.bcnd, dtype=np.int32)
+    ni0 = np.ascontiguousarray(st.ni0 if inj.ni0 is None else np.array(inj.ni0), dtype=np.float64)
+    P = ophys(st)
+    rc = lib().oracle_part_injection(_pi(n), _pd(h), _pi(bc), _pd(S.vxp), C.c_int(st.ntype),
+                                     C.c_int(S.vxp.shape[1]), _pi(S.np_tot), _pi(S.iseed), C.c_int(N_inj_ions),
+                                     _pd(P_loss), _pd(np.ascontiguousarray(phi)), _pd(ni0), C.byref(P), C.byref(I))
+    if rc:
+        raise RuntimeError(f"oracle part_injection status {rc}")
+
+
 def heat_stats(st, S, hz):
     """Src/part_expmover.f90:658-681: (sum Ek, Nh) of the electrons in the
     heating region."""

@@ -180,6 +180,154 @@ void oracle_eheating(const double h[3], double *vxp, int nmax, int *iseed, const
   *nheated = cnt;
 }
 
+// Src/part_injection.f90:1-293 (one thread, one MPI rank): injection of
+// electron-ion pairs (opt_inj 1 / -1 / 2), an electron beam (+-3) or
+// cathode electrons (+-4), appended behind np_tot.  P_loss(4,ntype).
+int oracle_part_injection(const int n[3], const double h[3], const int *bcnd, double *vxp, int ntype, int nmax,
+                          int *np_tot, int *iseed, int N_inj_ions, double *P_loss, const double *phi,
+                          const double *ni0, const OPhys *P, const OInject *I) {
+  Dims d(n);
+  const double pi = P->pi, qe = P->qe, dt = P->dt;
+  std::vector<double> vz_sav(ntype + 1, 0.0);
+  const double xm = (I->xl + I->xr) / 2.0, dx = I->xr - I->xl;
+  const double ym = (I->yl + I->yr) / 2.0, dy = I->yr - I->yl;
+  const double zm = (I->zl + I->zr) / 2.0, dz = I->zr - I->zl;
+  const double Rb = std::min(dx, dy) / 2.0;
+  int ng_sec = 1;
+  int dir_sec = I->dir_sec;
+  if (dir_sec == -1) ng_sec = 2;
+  const int aopt = std::abs(I->opt_inj);
+  double vb = 0.0, vt = 0.0, fmax = 0.0;
+  if (aopt == 3 || aopt == 4) {
+    vb = std::sqrt(2.0 * qe * I->THm / std::fabs(P->mass[0]));
+    vt = P->vt0[0];
+    double vmax = (vb + std::sqrt(vb * vb + 2.0 * vt * vt)) / 2.0;
+    fmax = vmax * std::exp(-(vmax - vb) * (vmax - vb) / (vt * vt));
+  }
+  int N;
+  if (aopt != 2) {
+    double dN = I->I_inj * I->ns_inj * dt / (qe * P->Nm[0]);
+    N = (int)dN;
+    double r = oracle_ran2(iseed);
+    if (r <= dN - N) N = N + 1;
+  } else {
+    N = N_inj_ions;
+  }
+  for (int i = 1; i <= N; ++i) {
+    double x, y, z;
+    for (;;) {
+      double r1 = oracle_ran2(iseed), r2 = oracle_ran2(iseed), r3 = oracle_ran2(iseed);
+      if (I->opt_inj > 0) {
+        x = -r1 * dx + I->xr;
+        y = -r2 * dy + I->yr;
+        z = -r3 * dz + I->zr;
+      } else {
+        x = xm + (dx / pi) * std::asin(2.0 * r1 - 1.0);
+        if (P->flag_pbc == 0 || (P->flag_pbc == 1 && I->flag_pbcz == 1)) y = ym + (dy / pi) * std::asin(2.0 * r2 - 1.0);
+        else y = -r2 * dy + I->yr;
+        if (P->flag_pbc == 0) z = zm + (P->zmax / pi) * std::asin(2.0 * r3 - 1.0);
+        else z = -r3 * dz + I->zr;
+      }
+      if ((aopt == 3 || aopt == 4) && ((x - xm) * (x - xm) + (y - ym) * (y - ym)) > Rb * Rb) continue;
+      int ix = (int)std::floor(x / h[0]) + 1, iy = (int)std::floor(y / h[1]) + 1, iz = (int)std::floor(z / h[2]) + 1;
+      if (ix < 0 || ix > d.n1 + 1 || iy < 0 || iy > d.n2 + 1 || iz < 0 || iz > d.n3 + 1) continue;
+      if (bcnd[d.g(ix, iy, iz)] >= 1 && bcnd[d.g(ix + 1, iy, iz)] >= 1 && bcnd[d.g(ix + 1, iy + 1, iz)] >= 1 &&
+          bcnd[d.g(ix, iy + 1, iz)] >= 1 && bcnd[d.g(ix, iy, iz + 1)] >= 1 && bcnd[d.g(ix + 1, iy, iz + 1)] >= 1 &&
+          bcnd[d.g(ix + 1, iy + 1, iz + 1)] >= 1 && bcnd[d.g(ix, iy + 1, iz + 1)] >= 1)
+        continue;
+      break;
+    }
+    for (int p = 1; p <= ntype; ++p) {
+      if (aopt == 3 || aopt == 4) {
+        if (I->tag_beam == 0) {
+          if (p >= 2) continue;
+        } else if (p != I->tag_beam) {
+          continue;
+        }
+        if (I->n_cath == 2 && aopt == 4) {
+          ng_sec = ng_sec + 1;
+          if (ng_sec > 2) ng_sec = 1;
+          dir_sec = (ng_sec == 1) ? 1 : -1;
+        }
+        z = I->zg_sec[ng_sec - 1];
+      }
+      double r = oracle_ran2(iseed);
+      if (r > ni0[p - 1]) continue;
+      np_tot[p - 1] += 1;
+      double vtp = P->vt0[p - 1];
+      int k = np_tot[p - 1];
+      if (k > nmax) return ORACLE_ERR_CAPACITY;
+      double vx, vy, vz;
+      if (aopt == 3 || aopt == 4) {
+        double z_tmp = z;
+        for (;;) {
+          double rr[2];
+          if (aopt == 3) {
+            double vmn = std::max(0.0, vb - 4.0 * vtp), vpx = vb + 4.0 * vtp;
+            for (;;) {
+              double a = oracle_ran2(iseed), b = oracle_ran2(iseed);
+              vz = vmn + a * (vpx - vmn);
+              double f = vz * std::exp(-(vz - vb) * (vz - vb) / (vtp * vtp));
+              if (!(b > f / fmax)) break;
+            }
+            rr[0] = oracle_ran2(iseed);
+            rr[1] = oracle_ran2(iseed);
+            oracle_load_gauss(&vx, &vy, vtp, rr, pi);
+          } else {
+            double a = oracle_ran2(iseed);
+            vz = (double)dir_sec * vb * std::sqrt(-std::log(1 - a));
+            rr[0] = oracle_ran2(iseed);
+            rr[1] = oracle_ran2(iseed);
+            oracle_load_gauss(&vx, &vy, vb, rr, pi);
+          }
+          double a = oracle_ran2(iseed);
+          double dt_tmp = a * ((double)I->ns_inj * dt);
+          z = z_tmp + vz * dt_tmp;
+          if (!(z < 0.0 || z > P->zmax)) break;
+        }
+      } else {
+        double rr[2];
+        rr[0] = oracle_ran2(iseed);
+        rr[1] = oracle_ran2(iseed);
+        oracle_load_gauss(&vx, &vy, vtp, rr, pi);
+        if (vz_sav[p] == 0.0) {
+          double a, b;
+          rr[0] = oracle_ran2(iseed);
+          rr[1] = oracle_ran2(iseed);
+          oracle_load_gauss(&a, &b, vtp, rr, pi);
+          vz = a;
+          vz_sav[p] = b;
+        } else {
+          vz = vz_sav[p];
+          vz_sav[p] = 0.0;
+        }
+      }
+      double *v = vxp + ((long)(p - 1) * nmax + (k - 1)) * 6;
+      v[0] = x;
+      v[1] = y;
+      v[2] = z;
+      v[3] = vx;
+      v[4] = vy;
+      v[5] = vz;
+      P_loss[3 + 4 * (p - 1)] += 0.5 * P->Nm[p - 1] * P->mass[p - 1] * (vx * vx + vy * vy + vz * vz);
+      if (aopt == 3 && phi) {
+        int ix = (int)std::floor(x / h[0]) + 1, iy = (int)std::floor(y / h[1]) + 1, iz = (int)std::floor(z / h[2]) + 1;
+        double px = (ix * h[0] - x) / h[0], py = (iy * h[1] - y) / h[1], pz = (iz * h[2] - z) / h[2];
+        double ki[8] = {px * py * pz,         (1 - px) * py * pz,         (1 - px) * (1 - py) * pz,
+                        px * (1 - py) * pz,   px * py * (1 - pz),         (1 - px) * py * (1 - pz),
+                        (1 - px) * (1 - py) * (1 - pz), px * (1 - py) * (1 - pz)};
+        long nd[8] = {d.g(ix, iy, iz),         d.g(ix + 1, iy, iz),         d.g(ix + 1, iy + 1, iz),
+                      d.g(ix, iy + 1, iz),     d.g(ix, iy, iz + 1),         d.g(ix + 1, iy, iz + 1),
+                      d.g(ix + 1, iy + 1, iz + 1), d.g(ix, iy + 1, iz + 1)};
+        double ph = 0.0;
+        for (int a = 0; a < 8; ++a) ph += ki[a] * phi[nd[a]];
+        P_loss[3 + 4 * (p - 1)] += P->Nm[p - 1] * P->charge[p - 1] * ph;
+      }
+    }
+  }
+  return ORACLE_OK;
+}
+
 // Src/part_expmover.f90:658-681: the kinetic energy and the number of the
 // electrons in the heating region (the deposition's statistics for the
 // self-consistent heating temperature of Src/main.f90:1206-1227).

@@ -67,6 +67,12 @@ typedef struct OHeat {
   double R_ahp, nudt, Pabs;
 } OHeat;
 
+/* Particle injection (Src/part_injection.f90): the COMMON values it reads. */
+typedef struct OInject {
+  int opt_inj, ns_inj, n_cath, dir_sec, tag_beam, flag_pbcz;
+  double I_inj, xl, xr, yl, yr, zl, zr, THm, zg_sec[2];
+} OInject;
+
 /* Cross-section tables after Src/read_reactions.f90:ordering. */
 typedef struct OTables {
   int ncol;                        /* reactions                              */
@@ -134,6 +140,9 @@ int oracle_collisions(double *vxp, const int n[3], const double h[3], int ntype,
                       int pl_max, const double *np_red, long long *err_coll);
 void oracle_scatter(double *vx1, double *vy1, double *vz1, double vx, double vy,
                     double vz, double costheta, double phi);
+int oracle_part_injection(const int n[3], const double h[3], const int *bcnd, double *vxp, int ntype,
+                          int nmax, int *np_tot, int *iseed, int N_inj_ions, double *P_loss,
+                          const double *phi, const double *ni0, const OPhys *P, const OInject *I);
 void oracle_eheating(const double h[3], double *vxp, int nmax, int *iseed, const int *np_tot,
                      double vt, double *P_loss, const OPhys *P, const OHeat *H, int *nheated);
 void oracle_heat_stats(const double h[3], const double *vxp, int nmax, const int *np_tot,
