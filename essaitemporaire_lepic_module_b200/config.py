@@ -103,6 +103,16 @@ def workload(name: str) -> Workload:
         n = {"pbc16": (16, 16, 16), "pbc32x16": (32, 16, 16), "nmn16": (16, 16, 16)}[name]
         return Workload(name, n, 1e-4, [_box(n, 1e-4) + [1], _box(n, 1e-4) + [0]], [0.0, 0.0], _ar_ion(),
                         Te=2.0, n0=1e15, ppc=16, dt=2e-11, steps=200, neumann_x=(name == "nmn16"))
+    if name == "die16":
+        # metal box plus two dielectric walls: the y = ymax plane (label 2,
+        # a Y = const dielectric) and the x = xmax plane (label 3, the first
+        # X = const dielectric)
+        n = (16, 16, 16)
+        box = _box(n, 1e-4)
+        X, Y, Z = box[3], box[4], box[5]
+        seg = [box + [1], [0.0, Y, 0.0, X, -Y, Z, -2], [X, 0.0, 0.0, -X, Y, Z, -3]]
+        return Workload(name, n, 1e-4, seg, [0.0, 0.0, 0.0, 0.0], _ar_ion(), Te=2.0, n0=1e15, ppc=16,
+                        dt=2e-11, steps=200)
     if name in ("mcc192",):
         n = (192, 192, 192)
         return Workload(name, n, 1e-4, [_box(n, 1e-4) + [1]], [0.0, 0.0], _ar_ion(),

@@ -465,13 +465,9 @@ void part_mover_(const int *n, const double *h, const double *Ei, const double *
   (void)cnt_cex;
   (void)cnt_dead;
   (void)beam_div;
-  (void)sum_q_xz;
-  (void)sum_q_yz;
-  (void)dtype;
   (void)iseed;
   if (*nproc != 1 || *iproc != 1) return record(LEPIC_ERR_UNSUPPORTED);
-  if (part_info_int_.flag_die || part_info_int_.tag_neg == *ptype || part_info_dp_1_.gam_sec > 0.0)
-    return record(LEPIC_ERR_UNSUPPORTED);
+  if (part_info_int_.tag_neg == *ptype || part_info_dp_1_.gam_sec > 0.0) return record(LEPIC_ERR_UNSUPPORTED);
   lepic_phys_t P = phys_from_common(*ntype);
   cudaStream_t s = 0;
   Dims d(n);
@@ -499,12 +495,38 @@ void part_mover_(const int *n, const double *h, const double *Ei, const double *
   signed char *fd_p = flag_dead + (long long)*nmax * p;
   const double *E_d = dev_view("dropin_E", Ei, 3 * (size_t)d.cnt(), READ, s, &rc);
   if (!E_d) return record(rc);
+  // dielectric walls: the surface charges of this species' lost particles
+  // (sum_q_xz(0:n1+2,0:n3+2,ntype,nproc), sum_q_yz(2,0:n2+2,0:n3+2,ntype,nproc))
+  const bool die = part_info_int_.flag_die == 1 && dtype && sum_q_xz && sum_q_yz;
+  const size_t nxz = (size_t)(n[0] + 3) * (n[2] + 3), nyz = 2 * (size_t)(n[1] + 3) * (n[2] + 3);
+  const int *dt_d = nullptr;
+  double *qxz_d = nullptr, *qyz_d = nullptr;
+  if (die) {
+    dt_d = upload("dropin_dtype", dtype, (size_t)*ngrid + 1, s);
+    qxz_d = (double *)scratch("dropin_qxz", sizeof(double) * nxz);
+    qyz_d = (double *)scratch("dropin_qyz", sizeof(double) * nyz);
+    if (!dt_d || !qxz_d || !qyz_d) return record(LEPIC_ERR_CUDA);
+    rc = cuda_ok(cudaMemsetAsync(qxz_d, 0, sizeof(double) * nxz, s), "memset");
+    if (!rc) rc = cuda_ok(cudaMemsetAsync(qyz_d, 0, sizeof(double) * nyz, s), "memset");
+    if (rc) return record(rc);
+  }
   SpeciesView v;
   rc = acquire_species(v, vxp_p, np_tot[p], *nmax, 0, fd_p, s);
   if (rc) return record(rc);
-  rc = launch_part_mover(g, E_d, v.s, *ptype, *ntype, *ngrid, P, p_mac, P_loss, s);
+  rc = launch_part_mover(g, E_d, v.s, *ptype, *ntype, *ngrid, P, p_mac, P_loss, s, dt_d, qxz_d, qyz_d);
   record(rc);
   record(release_species(v, &np_tot[p], fd_p, *nmax, true, s));
+  if (die && !rc) {
+    std::vector<double> hxz(nxz), hyz(nyz);
+    rc = cuda_ok(cudaMemcpyAsync(hxz.data(), qxz_d, sizeof(double) * nxz, cudaMemcpyDeviceToHost, s), "copy");
+    if (!rc) rc = cuda_ok(cudaMemcpyAsync(hyz.data(), qyz_d, sizeof(double) * nyz, cudaMemcpyDeviceToHost, s), "copy");
+    if (!rc) rc = cuda_ok(cudaStreamSynchronize(s), "sync");
+    record(rc);
+    if (!rc) {
+      for (size_t q = 0; q < nxz; ++q) sum_q_xz[q + nxz * p] += hxz[q];
+      for (size_t q = 0; q < nyz; ++q) sum_q_yz[q + nyz * p] += hyz[q];
+    }
+  }
 }
 
 void charge_deposition_(const int *n, const double *h, const double *vxp, const int *nmax,

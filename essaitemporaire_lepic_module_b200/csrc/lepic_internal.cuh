@@ -180,9 +180,12 @@ int launch_pdesolver(const Dims &d, const double h[3], double *u, const double *
                      int ncycl, double eps, double omega, int ng, double eps0, int *k, double *ktot,
                      double *res, cudaStream_t s, int pbc = 0, int nmn = 0);
 // particles.cu
+// dtype_dev (device dtype(0:ngrid)) with qxz_dev / qyz_dev (device planes of
+// the species pushed): the charge of particles lost on dielectric walls
 int launch_part_mover(const lepic_grid_t &g, const double *Ei, lepic_species_f64_t &sp, int ptype,
                       int ntype, int ngrid, const lepic_phys_t &P, double *p_mac, double *P_loss,
-                      cudaStream_t s);
+                      cudaStream_t s, const int *dtype_dev = nullptr, double *qxz_dev = nullptr,
+                      double *qyz_dev = nullptr);
 int launch_deposit(const lepic_grid_t &g, const lepic_species_f64_t &sp, int ptype,
                    const lepic_phys_t &P, double *np, cudaStream_t s);
 int launch_sort(const lepic_grid_t &g, lepic_species_f64_t &sp, int *Plist, int pl_max,

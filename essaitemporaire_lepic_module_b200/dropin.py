@@ -231,9 +231,12 @@ def _bi(st):
     return Bi, np.array([1, 1, 1], dtype=np.int32), np.ascontiguousarray(st.h, dtype=np.float64)
 
 
-def part_mover(st, Ei, vxp, np_tot, flag_dead, p_mac, P_loss, ptype, ngrid=None):
+def part_mover(st, Ei, vxp, np_tot, flag_dead, p_mac, P_loss, ptype, ngrid=None, sum_q=None):
     """Src/part_expmover.f90:1 -- in place on vxp / np_tot / flag_dead /
-    p_mac (ntype, 2, 0:ngrid) C-order (ngrid+1, 2, ntype) / P_loss (ntype, 4)."""
+    p_mac (ntype, 2, 0:ngrid) C-order (ngrid+1, 2, ntype) / P_loss (ntype, 4).
+    sum_q: (sum_q_xz, sum_q_yz), the surface charges of the dielectric walls
+    (flag_die = 1), C-order (ntype, n3+3, n1+3) and (ntype, n3+3, n2+3, 2),
+    accumulated for ptype."""
     ngrid = st.geom.ngrid if ngrid is None else ngrid
     n = _lib.np_i(st.n)
     h = np.ascontiguousarray(st.h, dtype=np.float64)
@@ -244,10 +247,20 @@ def part_mover(st, Ei, vxp, np_tot, flag_dead, p_mac, P_loss, ptype, ngrid=None)
     assert vxp.flags["C_CONTIGUOUS"] and np_tot.dtype == np.int32 and flag_dead.dtype == np.int8
     dummy_i = np.zeros(16, dtype=np.int32)
     dummy_d = np.zeros(16)
+    qxz = qyz = dummy_d
+    dt = dummy_i
+    if st.geom.flag_die:
+        n1, n2, n3 = st.n
+        if sum_q is None:
+            sum_q = (np.zeros((st.ntype, n3 + 3, n1 + 3)), np.zeros((st.ntype, n3 + 3, n2 + 3, 2)))
+        qxz, qyz = sum_q
+        assert qxz.shape == (st.ntype, n3 + 3, n1 + 3) and qyz.shape == (st.ntype, n3 + 3, n2 + 3, 2)
+        assert qxz.flags["C_CONTIGUOUS"] and qyz.flags["C_CONTIGUOUS"] and qxz.dtype == np.float64
+        dt = st.geom.dtype_array()
     lib().part_mover_(_pi(n), _pd(h), _pd(E), _pd(Bi), _pd(p_mac), _pd(P_loss), _pd(vxp), _pi(bc),
                       _i(nmax), _i(st.ntype), _i(ngrid), flag_dead.ctypes.data_as(_lib.P_i8), _i(1),
                       _pi(np_tot), _i(1), _i(ptype), _pi(dummy_i), _pi(dummy_i), _pd(dummy_d),
-                      _pd(dummy_d), _pd(dummy_d), _pd(dummy_d), _pi(dummy_i), _pi(dummy_i), _pi(nB),
+                      _pd(dummy_d), _pd(qxz), _pd(qyz), _pi(dt), _pi(dummy_i), _pi(nB),
                       _pd(hB))
     check(lib().lepic_gpu_last_error(), "part_mover")
 

@@ -31,6 +31,14 @@ class Geometry:
     flag_die: int = 0
     ngrid: int = 1
 
+    def dtype_array(self) -> np.ndarray:
+        """dtype(0:ngrid) as the reference passes it: 0 for unused labels."""
+        a = np.zeros(self.ngrid + 1, dtype=np.int32)
+        for g, t in self.dtype.items():
+            if 0 <= g <= self.ngrid:
+                a[g] = t
+        return a
+
 
 def generate_boundary(n, box_cm, segments, V):
     """Build the mask like Src/generate_boundary.f90 does from geometry.inp.

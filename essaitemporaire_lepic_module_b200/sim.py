@@ -166,6 +166,11 @@ class Simulation:
                  check_every=1, heating=None, injection=None):
         if precision not in ("f64", "mixed"):
             raise ValueError(f"precision must be 'f64' or 'mixed', not {precision!r}")
+        if st.geom.flag_die:
+            # the surface charge of dielectric walls is accumulated by the
+            # drop-in mover only; the device step loop has no dielectric
+            # boundary condition (Src/main.f90:856-925)
+            raise NotImplementedError("dielectric walls: use the part_mover_ drop-in")
         self.st = st
         self.mixed = precision == "mixed"
         self.precision = precision

@@ -121,7 +121,11 @@ void calc_efield_(const int *n, const double *h, const double *phi, double *Ei, 
 /* Src/part_expmover.f90:1 as called at Src/main.f90:1250-1252 (26
  * arguments) -- trilinear gather, Boris (uniform B with n_B(1) = 1, else the
  * B-field map Bi(4,0:n_B(1)+2,...) of spacing h_B) or leapfrog, position
- * update, loss test and in-order compaction of species ptype. */
+ * update, loss test and in-order compaction of species ptype.  With
+ * flag_die = 1 in COMMON /part_info_int/ the charge of the particles lost
+ * on dielectric walls (dtype(igrid) = 2: Y = const plane, 3 / 4: X = const
+ * planes) is added to sum_q_xz(0:n1+2,0:n3+2,ntype,nproc) and
+ * sum_q_yz(2,0:n2+2,0:n3+2,ntype,nproc) (Src/part_expmover.f90:302-348). */
 void part_mover_(const int *n, const double *h, const double *Ei, const double *Bi, double *p_mac,
                  double *P_loss, double *vxp, const int *bcnd, const int *nmax, const int *ntype,
                  const int *ngrid, signed char *flag_dead, const int *nproc, int *np_tot,

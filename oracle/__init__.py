@@ -239,7 +239,9 @@ def calc_efield(st, phi, Ei=None):
     return E
 
 
-def part_mover(st, Ei, S, p_mac, P_loss, ptype, ngrid=None):
+def part_mover(st, Ei, S, p_mac, P_loss, ptype, ngrid=None, sum_q=None):
+    """sum_q: (sum_q_xz (ntype, n3+3, n1+3), sum_q_yz (ntype, n3+3, n2+3, 2))
+    C-order, accumulated for the dielectric walls (flag_die = 1)."""
     ngrid = st.geom.ngrid if ngrid is None else ngrid
     n = np.array(st.n, dtype=np.int32)
     h = np.ascontiguousarray(st.h)
@@ -248,9 +250,18 @@ def part_mover(st, Ei, S, p_mac, P_loss, ptype, ngrid=None):
     rc = lib().oracle_part_mover(_pi(n), _pd(h), _pd(np.ascontiguousarray(Ei)), _pd(p_mac),
                                  _pd(P_loss), _pd(S.vxp), _pi(bc), C.c_int(S.vxp.shape[1]),
                                  C.c_int(st.ntype), C.c_int(ngrid), S.flag_dead.ctypes.data_as(P_i8),
-                                 _pi(S.np_tot), C.c_int(ptype), C.byref(P))
+                                 _pi(S.np_tot), C.c_int(ptype), C.byref(P), *_die_args(st, sum_q))
     if rc:
         raise RuntimeError(f"oracle part_mover status {rc}")
+
+
+def _die_args(st, sum_q):
+    if sum_q is None or not st.geom.flag_die:
+        return (None, None, None)
+    qxz, qyz = sum_q
+    assert qxz.flags["C_CONTIGUOUS"] and qyz.flags["C_CONTIGUOUS"]
+    assert qxz.dtype == np.float64 and qyz.dtype == np.float64
+    return (_pi(st.geom.dtype_array()), _pd(qxz), _pd(qyz))   # data_as keeps the array alive
 
 
 def charge_deposition(st, S, ptype):

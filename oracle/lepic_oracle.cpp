@@ -1018,9 +1018,50 @@ void oracle_calc_efield(const int n[3], const double h[3], const double *phi, do
 // Dead particles (flag_dead = 1) are removed; lost particles are compacted
 // out in order.  Returns ORACLE_ERR_UNSUPPORTED for periodic/Neumann planes
 // combined with negative ions or dielectric walls (out of scope).
+// Src/part_expmover.f90:302-348: the charge k3 of a particle lost on a
+// dielectric wall of type dt (2: Y = const plane, 3 and 4: X = const planes)
+// spread bilinearly on the plane's nodes: sum_q_xz(0:n1+2, 0:n3+2) or
+// sum_q_yz(2, 0:n2+2, 0:n3+2) of the species.  x: the new position, c: its
+// cell (ix, iy, iz).
+static void die_charge(const Dims &d, const double h[3], const OPhys *P, int dt, double k3, const double *x,
+                       const int *c, double *qxz, double *qyz) {
+  double zp = x[2];
+  int iz = c[2];
+  if (P->flag_pbc == 1) {
+    if (zp >= P->zmax) {
+      zp = zp - P->zmax;
+      iz = (int)std::floor(zp / h[2]) + 1;
+    }
+    if (zp <= 0.0) {
+      zp = P->zmax + zp;
+      iz = (int)std::floor(zp / h[2]) + 1;
+    }
+  }
+  const double pz = (iz * h[2] - zp) / h[2];
+  if (dt == 2) {
+    const int ix = c[0];
+    const long N1 = d.n1 + 3;
+    const double px = (ix * h[0] - x[0]) / h[0];
+    qxz[ix + N1 * iz] += k3 * px * pz;
+    qxz[ix + 1 + N1 * iz] += k3 * (1.0 - px) * pz;
+    qxz[ix + 1 + N1 * (iz + 1)] += k3 * (1.0 - px) * (1.0 - pz);
+    qxz[ix + N1 * (iz + 1)] += k3 * px * (1.0 - pz);
+  } else if (dt == 3 || dt == 4) {
+    const int iy = c[1];
+    const long N2 = d.n2 + 3;
+    const double py = (iy * h[1] - x[1]) / h[1];
+    double *q = qyz + (dt - 3);
+    q[2 * (iy + N2 * iz)] += k3 * py * pz;
+    q[2 * (iy + 1 + N2 * iz)] += k3 * (1.0 - py) * pz;
+    q[2 * (iy + 1 + N2 * (iz + 1))] += k3 * (1.0 - py) * (1.0 - pz);
+    q[2 * (iy + N2 * (iz + 1))] += k3 * py * (1.0 - pz);
+  }
+}
+
 int oracle_part_mover(const int n[3], const double h[3], const double *Ei, double *p_mac,
                       double *P_loss, double *vxp, const int *bcnd, int nmax, int ntype, int ngrid,
-                      signed char *flag_dead, int *np_tot, int ptype, const OPhys *P) {
+                      signed char *flag_dead, int *np_tot, int ptype, const OPhys *P,
+                      const int *dtype, double *sum_q_xz, double *sum_q_yz) {
   // Two passes: the push of every particle (independent, OpenMP over
   // contiguous particle slices like the reference's thread slices), then the
   // in-order compaction i_shift = i - np_lost (Src/part_expmover.f90:454-470).
@@ -1036,6 +1077,10 @@ int oracle_part_mover(const int n[3], const double h[3], const double *Ei, doubl
   std::vector<signed char> state(N);  // 0 kept, 1 dead, 2 lost
   std::vector<int> lost_grid(N, 0);
   std::vector<double> lost_E(N, 0.0);
+  // dielectric walls: the new position and cell of each lost particle
+  const bool die = dtype && sum_q_xz && sum_q_yz;
+  std::vector<double> lost_x(die ? 3L * N : 0);
+  std::vector<int> lost_c(die ? 3L * N : 0);
   int bad = 0;
 #pragma omp parallel for schedule(static) reduction(| : bad)
   for (int i = 0; i < N; ++i) {
@@ -1164,6 +1209,14 @@ int oracle_part_mover(const int n[3], const double h[3], const double *Ei, doubl
       lost_E[i] = 0.5 * Nm * mass * (vx * vx + vy * vy + vz * vz);
       lost_grid[i] = bcnd[d.g(ix, iy, iz)];
       if (lost_grid[i] > ngrid) bad = 1;
+      if (die) {
+        lost_x[3L * i] = xp;
+        lost_x[3L * i + 1] = yp;
+        lost_x[3L * i + 2] = zp;
+        lost_c[3L * i] = ix;
+        lost_c[3L * i + 1] = iy;
+        lost_c[3L * i + 2] = iz;
+      }
       continue;
     }
     if (P->flag_nmn == 1 && xp <= 0.0) {
@@ -1199,6 +1252,9 @@ int oracle_part_mover(const int n[3], const double h[3], const double *Ei, doubl
       PL(0) = PL(0) + lost_E[i];
       pm(0, lost_grid[i]) = pm(0, lost_grid[i]) + 1.0;
       pm(1, lost_grid[i]) = pm(1, lost_grid[i]) + lost_E[i];
+      if (die && dtype[lost_grid[i]] > 1) die_charge(d, h, P, dtype[lost_grid[i]], Nm * q, &lost_x[3L * i],
+                                                     &lost_c[3L * i], sum_q_xz + (long)p * (d.n1 + 3) * (d.n3 + 3),
+                                                     sum_q_yz + (long)p * 2 * (d.n2 + 3) * (d.n3 + 3));
     } else if (np_lost) {
       std::memcpy(V + (long)(i - np_lost) * 6, V + (long)i * 6, 6 * sizeof(double));
     }

@@ -120,7 +120,8 @@ int oracle_part_mover(const int n[3], const double h[3], const double *Ei,
                       double *p_mac, double *P_loss, double *vxp,
                       const int *bcnd, int nmax, int ntype, int ngrid,
                       signed char *flag_dead, int *np_tot, int ptype,
-                      const OPhys *P);
+                      const OPhys *P, const int *dtype, double *sum_q_xz,
+                      double *sum_q_yz);
 void oracle_charge_deposition(const int n[3], const double h[3],
                               const double *vxp, int nmax, int ntype,
                               const double *kq, double *np, const int *np_tot,
