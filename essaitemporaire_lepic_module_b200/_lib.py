@@ -34,7 +34,8 @@ class LepicPhys(C.Structure):
                 ("flag_B", C.c_int), ("flag_B_pos", C.c_int), ("flag_pbc", C.c_int),
                 ("flag_nmn", C.c_int), ("ns_coll", C.c_int), ("n_cell", C.c_int),
                 ("np_cell", C.c_int), ("Bconst", C.c_double * 3),
-                ("Bmap", C.c_void_p), ("n_B", C.c_int * 3), ("h_B", C.c_double * 3)]
+                ("Bmap", C.c_void_p), ("n_B", C.c_int * 3), ("h_B", C.c_double * 3),
+                ("dtype", C.c_void_p), ("sum_q_xz", C.c_void_p), ("sum_q_yz", C.c_void_p)]
 
 
 class LepicGrid(C.Structure):
@@ -223,6 +224,7 @@ def lib():
         "lepic_dev_load_uniform": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64), _I,
                                     C.c_longlong, C.POINTER(LepicPhys), C.c_ulonglong, vp], _I),
         "lepic_dev_cell_wall": ([P_int, vp, vp, vp], _I),
+        "lepic_dev_dielectric_phi": ([C.POINTER(LepicGrid), vp, C.POINTER(LepicPhys), _I, C.c_double, vp], _I),
         "lepic_dev_dens_red": ([C.POINTER(LepicGrid), vp, vp, _I, P_dbl, vp], _I),
         "lepic_timing_enable": ([_I], None),
         "lepic_timing_reset": ([], None),
@@ -276,6 +278,7 @@ def exported_symbols():
             "lepic_dev_pdesolver_mixed", "lepic_dev_collisions_mixed", "lepic_dev_load_uniform",
             "lepic_dev_win_push", "lepic_dev_win_deposit", "lepic_dev_adj_push", "lepic_dev_adj_efield",
             "lepic_dev_adj_rhs", "lepic_dev_adj_walls", "lepic_dev_adj_deposit", "lepic_dev_cell_wall",
+            "lepic_dev_dielectric_phi",
             "lepic_dev_dens_red", "lepic_timing_enable", "lepic_timing_reset", "lepic_timing_read",
             "calc_rho_", "dens_red_", "pdesolver_", "calc_efield_",
             "part_mover_", "charge_deposition_", "part_sorting_", "collisions_", "eheating_",

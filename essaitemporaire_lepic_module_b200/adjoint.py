@@ -43,8 +43,8 @@ class Window:
     stays where it was loaded)."""
 
     def __init__(self, st, K, every=None, ptype=1, cap=None, device="cuda", adjoint_solver="mixed"):
-        if st.geom.flag_pbc or st.geom.flag_nmn:
-            raise ValueError("the adjoint window supports Dirichlet walls only")
+        if st.geom.flag_pbc or st.geom.flag_nmn or st.geom.flag_die:
+            raise ValueError("the adjoint window supports Dirichlet (metal) walls only")
         self.st = st
         self.K = int(K)
         self.every = int(every) if every else max(1, int(round(math.sqrt(self.K))))

@@ -69,6 +69,7 @@ class Workload:
     mixed_only: bool = False
     neumann_x: bool = False         # x = 0 is a Neumann (symmetry) plane
     coulomb: float = 0.0            # > 0: e-Ar+ elastic (charged target, DSMC) of this sigma0 (m^2)
+    Ca: float = 0.0                 # capacitance of the dielectric walls, F/m^2
 
 
 def _box(n, dx):
@@ -112,7 +113,7 @@ def workload(name: str) -> Workload:
         X, Y, Z = box[3], box[4], box[5]
         seg = [box + [1], [0.0, Y, 0.0, X, -Y, Z, -2], [X, 0.0, 0.0, -X, Y, Z, -3]]
         return Workload(name, n, 1e-4, seg, [0.0, 0.0, 0.0, 0.0], _ar_ion(), Te=2.0, n0=1e15, ppc=16,
-                        dt=2e-11, steps=200)
+                        dt=2e-11, steps=200, Ca=2e-8)
     if name in ("mcc192",):
         n = (192, 192, 192)
         return Workload(name, n, 1e-4, [_box(n, 1e-4) + [1]], [0.0, 0.0], _ar_ion(),
@@ -177,6 +178,7 @@ class Setup:
     extra: dict = field(default_factory=dict)
     bfield: object = None           # bfield.BField (a B-field map) or None (uniform Bconst)
     flag_B_pos: int = 0             # 1: positive ions not magnetised
+    Ca: float = 0.0                 # dielectric walls: capacitance per cell (F), Src/main.f90:572
 
     @property
     def ncells(self):
@@ -321,6 +323,8 @@ def build(wl: Workload | str, chem=None) -> Setup:
                Bconst=np.array(wl.B, dtype=np.float64), kq=kq, tables=tables, ngas=ngas)
     if wl.blobs:
         st.rhs_blobs = gaussian_blobs(n, h, wl.blobs, wl.blob_seed)
+    if geom.flag_die:
+        st.Ca = wl.Ca * h[0] * h[2]     # Farads per grid cell (Src/main.f90:572)
     return st
 
 

@@ -354,6 +354,12 @@ int lepic_dev_load_uniform(const lepic_grid_t *g, lepic_species_f64_t *sp, int n
   return launch_load_uniform(*g, sp, ntype, n_per_species, *P, seed, S(stream));
 }
 
+int lepic_dev_dielectric_phi(const lepic_grid_t *g, double *phi, const lepic_phys_t *P, int ngrid, double Ca,
+                             void *stream) {
+  if (!g || !phi || !P || P->ntype < 1 || P->ntype > LEPIC_NPART) return LEPIC_ERR_ARG;
+  return launch_dielectric_phi(Dims(g->n), phi, g->bcnd, *P, ngrid, Ca, S(stream));
+}
+
 int lepic_dev_cell_wall(const int *n, const int *bcnd, unsigned char *cell_wall, void *stream) {
   if (!n || !bcnd || !cell_wall) return LEPIC_ERR_ARG;
   return launch_cell_wall(Dims(n), bcnd, cell_wall, S(stream));

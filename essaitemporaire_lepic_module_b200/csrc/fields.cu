@@ -270,6 +270,59 @@ __global__ void k_cell_wall(Dims d, const int *bcnd, unsigned char *cw) {
   cw[t] = w ? 1 : 0;
 }
 
+// Src/main.f90:859-949 (one rank, one thread slice): the potential of the
+// dielectric walls' nodes rises by the surface charge over the capacitance
+// per cell Ca, species by species in ptype order: Q/(2 Ca) on Y = const
+// planes (sum_q_xz), Q/Ca on X = const planes (sum_q_yz).  With periodic z
+// planes the sums of rows 1 and n3+1 count twice, row 0 reads twice row n3
+// and row n3+2 twice row 2 (the boundary cell collects half the charge).
+__global__ void k_dielectric_phi(Dims d, double *phi, const int *__restrict__ bcnd,
+                                 const int *__restrict__ dtype, int ngrid, const double *__restrict__ qxz,
+                                 const double *__restrict__ qyz, int ntype, double Ca, int pbc) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= d.cnt()) return;
+  const int igrid = bcnd[t];
+  if (igrid <= 0 || igrid > ngrid) return;
+  const int dt = dtype[igrid];
+  if (dt < 2 || dt > 4) return;
+  const int ix = (int)(t % d.N1), iy = (int)((t / d.N1) % d.N2), iz = (int)(t / (d.N1 * d.N2));
+  int jz = iz;
+  bool twice = false;
+  if (pbc == 1) {
+    twice = true;
+    if (iz == 0)
+      jz = d.n3;
+    else if (iz == d.n3 + 2)
+      jz = 2;
+    else if (iz != 1 && iz != d.n3 + 1)
+      twice = false;
+  }
+  const long long nxz = d.N1 * d.N3, nyz = 2 * d.N2 * d.N3;
+  double v = phi[t];
+  for (int p = 0; p < ntype; ++p) {
+    if (dt == 2) {
+      const double q = qxz[p * nxz + ix + d.N1 * jz];
+      v = v + (twice ? 2.0 * q : q) / (2.0 * Ca);
+    } else {
+      const double q = qyz[p * nyz + (dt - 3) + 2 * (iy + d.N2 * jz)];
+      v = v + (twice ? 2.0 * q : q) / Ca;
+    }
+  }
+  phi[t] = v;
+}
+
+int launch_dielectric_phi(const Dims &d, double *phi, const int *bcnd, const lepic_phys_t &P, int ngrid,
+                          double Ca, cudaStream_t s) {
+  if (!P.dtype || !P.sum_q_xz || !P.sum_q_yz || !(Ca > 0.0) || d.n3 < 2) return LEPIC_ERR_ARG;
+  k_dielectric_phi<<<grid_for(d.cnt(), 256), 256, 0, s>>>(d, phi, bcnd, P.dtype, ngrid, P.sum_q_xz,
+                                                          P.sum_q_yz, P.ntype, Ca, P.flag_pbc);
+  LEPIC_CUDA(cudaGetLastError());
+  // Src/main.f90:912-914: the counters restart from zero
+  LEPIC_CUDA(cudaMemsetAsync(P.sum_q_xz, 0, sizeof(double) * P.ntype * d.N1 * d.N3, s));
+  LEPIC_CUDA(cudaMemsetAsync(P.sum_q_yz, 0, sizeof(double) * P.ntype * 2 * d.N2 * d.N3, s));
+  return LEPIC_OK;
+}
+
 int launch_cell_wall(const Dims &d, const int *bcnd, unsigned char *cw, cudaStream_t s) {
   long long nc = (d.N1 - 1) * (d.N2 - 1) * (d.N3 - 1);
   k_cell_wall<<<grid_for(nc, 256), 256, 0, s>>>(d, bcnd, cw);

@@ -165,8 +165,78 @@ __device__ __forceinline__ bool bmap_gather_f64(const BMapF64 &m, double xp, dou
   return true;
 }
 
+// Dielectric walls (Src/part_expmover.f90:302-348): the charge of a particle
+// lost on a wall whose type dtype(igrid) is 2 (Y = const plane) or 3, 4
+// (X = const planes #1, #2) is spread bilinearly on that plane's node sums.
+struct Dielectric {
+  const int *dtype;   // device dtype(0:ngrid), nullptr: no dielectric walls
+  double *qxz;        // sum_q_xz(0:n1+2, 0:n3+2) of the species pushed
+  double *qyz;        // sum_q_yz(2, 0:n2+2, 0:n3+2) of the species pushed
+  double k3;          // Nm charge
+};
+
+// The walls of P (device API) for species ptype; die.dtype stays nullptr
+// when P has none.
+inline Dielectric dielectric_from_phys(const lepic_phys_t &P, const int n[3], int ptype) {
+  Dielectric die{};
+  if (P.dtype && P.sum_q_xz && P.sum_q_yz) {
+    const int p = ptype - 1;
+    die.dtype = P.dtype;
+    die.qxz = P.sum_q_xz + (size_t)p * (n[0] + 3) * (n[2] + 3);
+    die.qyz = P.sum_q_yz + (size_t)p * 2 * (n[1] + 3) * (n[2] + 3);
+    die.k3 = P.Nm[p] * P.charge[p];
+  }
+  return die;
+}
+
+// A particle lost at the new position (xp, yp, zp) in cell (ix, iy, iz)
+// (clamped to 0..n+1) on wall label igrid: its charge on the wall's plane
+// sums when the wall is a dielectric.  pbc: periodic planes along z (the
+// position wraps first).
+__device__ __forceinline__ void dielectric_charge(const Dielectric &die, const Dims &d, int igrid, double xp,
+                                                  double yp, double zp, int ix, int iy, int iz, double h0,
+                                                  double h1, double h2, int pbc, double zmax) {
+  const int dt = die.dtype ? die.dtype[igrid] : 0;
+  if (dt <= 1) return;
+  double zq = zp;
+  int iq = iz;
+  if (pbc == 1) {
+    if (zq >= zmax) {
+      zq = zq - zmax;
+      iq = (int)floor(zq / h2) + 1;
+    }
+    if (zq <= 0.0) {
+      zq = zmax + zq;
+      iq = (int)floor(zq / h2) + 1;
+    }
+  }
+  iq = iq < 0 ? 0 : (iq > d.n3 + 1 ? d.n3 + 1 : iq);
+  const double pz = (iq * h2 - zq) / h2;
+  if (dt == 2) {
+    const double px = (ix * h0 - xp) / h0;
+    double *q = die.qxz;
+    const long long NX = d.N1;
+    atomicAdd(&q[ix + NX * iq], die.k3 * px * pz);
+    atomicAdd(&q[ix + 1 + NX * iq], die.k3 * (1.0 - px) * pz);
+    atomicAdd(&q[ix + 1 + NX * (iq + 1)], die.k3 * (1.0 - px) * (1.0 - pz));
+    atomicAdd(&q[ix + NX * (iq + 1)], die.k3 * px * (1.0 - pz));
+  } else if (dt == 3 || dt == 4) {
+    const double py = (iy * h1 - yp) / h1;
+    double *q = die.qyz + (dt - 3);
+    const long long NY = d.N2;
+    atomicAdd(&q[2 * (iy + NY * iq)], die.k3 * py * pz);
+    atomicAdd(&q[2 * (iy + 1 + NY * iq)], die.k3 * (1.0 - py) * pz);
+    atomicAdd(&q[2 * (iy + 1 + NY * (iq + 1))], die.k3 * (1.0 - py) * (1.0 - pz));
+    atomicAdd(&q[2 * (iy + NY * (iq + 1))], die.k3 * py * (1.0 - pz));
+  }
+}
+
 // ------------------------------------------------------------ launchers
 // fields.cu
+// Src/main.f90:859-949 for one rank: the dielectric walls' potential update
+// from the summed surface charges of every species, then the sums cleared
+int launch_dielectric_phi(const Dims &d, double *phi, const int *bcnd, const lepic_phys_t &P, int ngrid,
+                          double Ca, cudaStream_t s);
 int launch_calc_rho(const Dims &d, double *np, double *rhs, const int *bcnd, int ntype,
                     const lepic_phys_t &P, cudaStream_t s);
 int launch_dens_red(const Dims &d, const double *np, double *np_red, const int *bcnd, int ntype,
@@ -182,6 +252,7 @@ int launch_pdesolver(const Dims &d, const double h[3], double *u, const double *
 // particles.cu
 // dtype_dev (device dtype(0:ngrid)) with qxz_dev / qyz_dev (device planes of
 // the species pushed): the charge of particles lost on dielectric walls
+// (without them, the walls of P, if any)
 int launch_part_mover(const lepic_grid_t &g, const double *Ei, lepic_species_f64_t &sp, int ptype,
                       int ntype, int ngrid, const lepic_phys_t &P, double *p_mac, double *P_loss,
                       cudaStream_t s, const int *dtype_dev = nullptr, double *qxz_dev = nullptr,

@@ -876,6 +876,7 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
   const int p = ptype - 1;
   if (!sp.flag_dead || !aligned16(E4)) return LEPIC_ERR_ARG;
   if (int rc = check_layout(g, sp)) return rc;
+  if (P.dtype) return LEPIC_ERR_UNSUPPORTED;  // dielectric walls: FP64 push only
   MixedConst c;
   memset(&c, 0, sizeof(c));
   c.dth0 = (float)(P.dt / g.h[0]);

@@ -20,16 +20,6 @@ namespace {
 
 constexpr int PB = 256;
 
-// Dielectric walls (Src/part_expmover.f90:302-348): the charge of a particle
-// lost on a wall whose type dtype(igrid) is 2 (Y = const plane) or 3, 4
-// (X = const planes #1, #2) is spread bilinearly on that plane's node sums.
-struct Dielectric {
-  const int *dtype;   // device dtype(0:ngrid), nullptr: no dielectric walls
-  double *qxz;        // sum_q_xz(0:n1+2, 0:n3+2) of the species pushed
-  double *qyz;        // sum_q_yz(2, 0:n2+2, 0:n3+2) of the species pushed
-  double k3;          // Nm charge
-};
-
 struct PushConst {
   double h0, h1, h2, dt, k1, Nm, mass;
   double Bx, By, Bz;
@@ -142,41 +132,7 @@ __global__ void __launch_bounds__(PB) k_push_f64(Dims d, PushConst c, BMapF64 m,
     if (igrid >= 0 && igrid <= c.ngrid) {
       atomicAdd(&acc[2 + 2 * igrid], 1.0);
       atomicAdd(&acc[3 + 2 * igrid], Eki);
-      const int dt = die.dtype ? die.dtype[igrid] : 0;
-      if (dt > 1) {
-        // with periodic planes along z the position wraps first
-        double zq = zp;
-        int iq = iz;
-        if (c.flag_pbc == 1) {
-          if (zq >= c.zmax) {
-            zq = zq - c.zmax;
-            iq = (int)floor(zq / c.h2) + 1;
-          }
-          if (zq <= 0.0) {
-            zq = c.zmax + zq;
-            iq = (int)floor(zq / c.h2) + 1;
-          }
-        }
-        iq = iq < 0 ? 0 : (iq > d.n3 + 1 ? d.n3 + 1 : iq);
-        const double pz = (iq * c.h2 - zq) / c.h2;
-        if (dt == 2) {
-          const double px = (ix * c.h0 - xp) / c.h0;
-          const long long NX = d.N1;
-          double *q = die.qxz;
-          atomicAdd(&q[ix + NX * iq], die.k3 * px * pz);
-          atomicAdd(&q[ix + 1 + NX * iq], die.k3 * (1.0 - px) * pz);
-          atomicAdd(&q[ix + 1 + NX * (iq + 1)], die.k3 * (1.0 - px) * (1.0 - pz));
-          atomicAdd(&q[ix + NX * (iq + 1)], die.k3 * px * (1.0 - pz));
-        } else if (dt == 3 || dt == 4) {
-          const double py = (iy * c.h1 - yp) / c.h1;
-          const long long NY = d.N2;
-          double *q = die.qyz + (dt - 3);
-          atomicAdd(&q[2 * (iy + NY * iq)], die.k3 * py * pz);
-          atomicAdd(&q[2 * (iy + 1 + NY * iq)], die.k3 * (1.0 - py) * pz);
-          atomicAdd(&q[2 * (iy + 1 + NY * (iq + 1))], die.k3 * (1.0 - py) * (1.0 - pz));
-          atomicAdd(&q[2 * (iy + NY * (iq + 1))], die.k3 * py * (1.0 - pz));
-        }
-      }
+      dielectric_charge(die, d, igrid, xp, yp, zp, ix, iy, iz, c.h0, c.h1, c.h2, c.flag_pbc, c.zmax);
     }
     keep[i] = 0;
     return;
@@ -399,8 +355,7 @@ int launch_part_mover(const lepic_grid_t &g, const double *Ei, lepic_species_f64
   c.ngrid = ngrid;
   BMapF64 m;
   if (int rc = bmap_from_phys(P, g.n, m)) return rc;
-  Dielectric die;
-  memset(&die, 0, sizeof(die));
+  Dielectric die = dielectric_from_phys(P, g.n, ptype);
   if (dtype_dev) {
     if (!qxz_dev || !qyz_dev) return LEPIC_ERR_ARG;
     die.dtype = dtype_dev;

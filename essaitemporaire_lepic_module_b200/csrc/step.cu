@@ -60,7 +60,7 @@ __device__ __forceinline__ int run_id(long long key, bool &head) {
 // BMAP: B from the map m (else the uniform c.Bx, c.By, c.Bz)
 template <bool BMAP>
 __global__ void __launch_bounds__(FB) k_push_deposit_f64(
-    Dims d, FusedConst c, BMapF64 m, const double *__restrict__ Ei, const int *__restrict__ bcnd,
+    Dims d, FusedConst c, BMapF64 m, Dielectric die, const double *__restrict__ Ei, const int *__restrict__ bcnd,
     const unsigned char *__restrict__ cw, double *__restrict__ p, long long cap,
     const int *__restrict__ count, signed char *__restrict__ flag, const double *__restrict__ kq,
     double *__restrict__ np, int *__restrict__ holes, int *__restrict__ nholes,
@@ -143,6 +143,7 @@ __global__ void __launch_bounds__(FB) k_push_deposit_f64(
         if (igrid >= 0 && igrid <= c.ngrid) {
           atomicAdd(&acc[2 + 2 * igrid], 1.0);
           atomicAdd(&acc[3 + 2 * igrid], Eki);
+          dielectric_charge(die, d, igrid, xp, yp, zp, jx, jy, jz, c.h0, c.h1, c.h2, c.flag_pbc, c.zmax);
         }
         hole = true;
       } else {
@@ -312,6 +313,7 @@ int launch_push_deposit(const lepic_grid_t &g, const double *Ei, lepic_species_f
   if (!sp.flag_dead) return LEPIC_ERR_ARG;
   BMapF64 m;
   if (int rc = bmap_from_phys(P, g.n, m)) return rc;
+  const Dielectric die = dielectric_from_phys(P, g.n, ptype);
   const size_t cap = (size_t)sp.cap;
   char nm[32];
   snprintf(nm, sizeof nm, "work_list%d", p);
@@ -327,11 +329,11 @@ int launch_push_deposit(const lepic_grid_t &g, const double *Ei, lepic_species_f
   const int nthreads = n_hint > 0 ? n_hint : sp.cap;
   int t0 = timer_start("push_deposit_f64", s);
   if (m.B)
-    k_push_deposit_f64<true><<<grid_for(nthreads, FB), FB, 0, s>>>(d, c, m, Ei, g.bcnd, g.cell_wall, sp.p,
+    k_push_deposit_f64<true><<<grid_for(nthreads, FB), FB, 0, s>>>(d, c, m, die, Ei, g.bcnd, g.cell_wall, sp.p,
                                                                    sp.cap, sp.count, sp.flag_dead, g.kq, np,
                                                                    holes, side, acc_dev, ctx().d_err);
   else
-    k_push_deposit_f64<false><<<grid_for(nthreads, FB), FB, 0, s>>>(d, c, m, Ei, g.bcnd, g.cell_wall, sp.p,
+    k_push_deposit_f64<false><<<grid_for(nthreads, FB), FB, 0, s>>>(d, c, m, die, Ei, g.bcnd, g.cell_wall, sp.p,
                                                                     sp.cap, sp.count, sp.flag_dead, g.kq, np,
                                                                     holes, side, acc_dev, ctx().d_err);
   timer_stop(t0, s);

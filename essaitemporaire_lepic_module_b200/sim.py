@@ -166,11 +166,12 @@ class Simulation:
                  check_every=1, heating=None, injection=None):
         if precision not in ("f64", "mixed"):
             raise ValueError(f"precision must be 'f64' or 'mixed', not {precision!r}")
-        if st.geom.flag_die:
-            # the surface charge of dielectric walls is accumulated by the
-            # drop-in mover only; the device step loop has no dielectric
-            # boundary condition (Src/main.f90:856-925)
-            raise NotImplementedError("dielectric walls: use the part_mover_ drop-in")
+        if st.geom.flag_die and precision == "mixed":
+            # the surface charge of dielectric walls is summed by the FP64
+            # pushes only
+            raise NotImplementedError("dielectric walls: the step loop runs them in the f64 form")
+        if st.geom.flag_die and not st.Ca > 0.0:
+            raise ValueError("dielectric walls need a capacitance Ca > 0")
         self.st = st
         self.mixed = precision == "mixed"
         self.precision = precision
@@ -211,6 +212,17 @@ class Simulation:
             world = dist.get_world_size(self._group)
             for p in range(st.ntype):
                 self.P.Nm[p] = rank_weight(st.Nm[p], world)
+        self.die = None
+        if st.geom.flag_die:
+            # dielectric walls: dtype(0:ngrid) and the surface-charge sums of
+            # every species, sum_q_xz (ntype, n3+3, n1+3) and sum_q_yz
+            # (ntype, n3+3, n2+3, 2), which the FP64 pushes add to
+            n1, n2, n3 = st.n
+            f64 = dict(dtype=torch.float64, device=self.dev)
+            self.die = (torch.as_tensor(st.geom.dtype_array(), device=self.dev),
+                        torch.zeros((st.ntype, n3 + 3, n1 + 3), **f64),
+                        torch.zeros((st.ntype, n3 + 3, n2 + 3, 2), **f64))
+            self.P.dtype, self.P.sum_q_xz, self.P.sum_q_yz = (t.data_ptr() for t in self.die)
         g = st.geom
         T = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=self.dev)
         self.bcnd = T(g.bcnd, torch.int32)
@@ -396,6 +408,19 @@ class Simulation:
         check(lib().lepic_dev_calc_rho(C.byref(self.grid), _ptr(self.np), _ptr(self.rhs),
                                        self.st.ntype, C.byref(self.P), self._s()), "calc_rho")
 
+    def dielectric_phi(self):
+        """Src/main.f90:859-949: the dielectric walls' potential rises by
+        the surface charge the pushes summed since the last call (summed over
+        the ranks first, the MPI_ALLREDUCE of Src/main.f90:888-892); the
+        sums restart from zero."""
+        if self.comm is not None:
+            import torch.distributed as dist
+            for t in self.die[1:]:
+                dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self._group)
+        check(lib().lepic_dev_dielectric_phi(C.byref(self.grid), _ptr(self.phi), C.byref(self.P),
+                                             self.st.geom.ngrid, C.c_double(self.st.Ca), self._s()),
+              "dielectric_phi")
+
     def pdesolver(self, eps=None, omega=None, ng=None, ncycl=None):
         # the FP32 V-cycles cover Dirichlet walls; with periodic planes or the
         # Neumann plane the mixed form solves with the FP64 multigrid
@@ -578,6 +603,8 @@ class Simulation:
         self.it += 1
         it = self.it
         self.calc_rho()
+        if self.die is not None:
+            self.dielectric_phi()
         self.pdesolver()
         self.efield()
         due = [p for p, k in enumerate(self.sort_every) if k and it % k == 1 % k]

@@ -274,6 +274,14 @@ typedef struct {
   const double *Bmap;
   int n_B[3];
   double h_B[3];
+  /* Dielectric walls (Src/part_expmover.f90:302-348), device pointers, all
+   * NULL when there are none: dtype(0:ngrid) (2: Y = const plane, 3 and 4:
+   * X = const planes) and the surface-charge sums of every species,
+   * sum_q_xz(0:n1+2,0:n3+2,ntype) and sum_q_yz(2,0:n2+2,0:n3+2,ntype), to
+   * which the FP64 pushes add the charge of the particles lost on them. */
+  const int *dtype;
+  double *sum_q_xz;
+  double *sum_q_yz;
 } lepic_phys_t;
 
 /* Cross-section tables after Src/read_reactions.f90:ordering, device copies. */
@@ -375,6 +383,17 @@ int lepic_dev_pdesolver(const lepic_grid_t *g, double *u, const double *b, int n
 int lepic_dev_pdesolver_noalloc(const lepic_grid_t *g, double *u, const double *b, int ncycl,
                                 double eps, double omega, int ng, const lepic_phys_t *P, int *k,
                                 double *ktot, double *res, void *stream);
+
+/* Src/main.f90:859-949 with one rank: the potential of the dielectric walls'
+ * nodes (dtype 2, 3, 4 of P->dtype) rises by the surface charge of every
+ * species over the capacitance per cell Ca (F; the input Ca times h(1) h(3),
+ * Src/main.f90:572) -- Q/(2 Ca) on Y = const planes, Q/Ca on X = const
+ * planes, with the periodic-z doubling of the boundary rows -- and the sums
+ * P->sum_q_xz / P->sum_q_yz are cleared.  phi device (0:n1+2,0:n2+2,0:n3+2).
+ * Multi-rank callers sum the per-rank sums first (the MPI_ALLREDUCE of
+ * Src/main.f90:888-892). */
+int lepic_dev_dielectric_phi(const lepic_grid_t *g, double *phi, const lepic_phys_t *P, int ngrid, double Ca,
+                             void *stream);
 
 /* Src/part_expmover.f90:1-482 for one species: push + loss + in-order
  * compaction.  Ei device (3,(n+3)^3).  p_mac: host (ntype,2,0:ngrid),

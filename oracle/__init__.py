@@ -158,6 +158,9 @@ class State:
         self.np = np.zeros((st.ntype,) + tuple(st.geom.bcnd.shape))
         self.iseed = np.array([123456], dtype=np.int32)
         self.Plist = None          # (ntype, pl_max+1) per-cell offsets of the last sort
+        n1, n2, n3 = st.n
+        # surface-charge sums of the dielectric walls (sum_q_xz, sum_q_yz) C-order
+        self.sum_q = (np.zeros((st.ntype, n3 + 3, n1 + 3)), np.zeros((st.ntype, n3 + 3, n2 + 3, 2)))
 
     def copy(self):
         o = object.__new__(State)
@@ -167,6 +170,7 @@ class State:
         o.np = self.np.copy()
         o.iseed = self.iseed.copy()
         o.Plist = None if self.Plist is None else self.Plist.copy()
+        o.sum_q = tuple(a.copy() for a in self.sum_q)
         return o
 
 
@@ -367,11 +371,27 @@ def ordering(chem, npt_mx=4000):
     return sig_Er[:k], sig[:, :k], sv.T, sl.T, pn
 
 
+def dielectric_phi(st, phi, sum_q):
+    """Src/main.f90:859-949 (one rank): phi of the dielectric walls' nodes
+    rises by the surface charges over the capacitance per cell st.Ca; the
+    sums are cleared."""
+    qxz, qyz = sum_q
+    assert phi.flags["C_CONTIGUOUS"] and qxz.flags["C_CONTIGUOUS"] and qyz.flags["C_CONTIGUOUS"]
+    n = np.array(st.n, dtype=np.int32)
+    bc = np.ascontiguousarray(st.geom.bcnd, dtype=np.int32)
+    lib().oracle_dielectric_phi(_pi(n), _pd(phi), _pi(bc), _pi(st.geom.dtype_array()),
+                                C.c_int(st.geom.ngrid), _pd(qxz), _pd(qyz), C.c_int(st.ntype),
+                                C.c_double(st.Ca), C.c_int(st.geom.flag_pbc))
+
+
 def step(st, S, phi, Ei, it, p_mac=None, P_loss=None, nsort=10, ns_coll=10, mg=None):
     """One legacy timestep in the order of Src/main.f90:853-1277:
-    calc_rho -> pdesolver -> calc_Efield -> (sort) -> (collisions) ->
-    part_mover -> charge_deposition.  Returns (Ei, mg result, MCC result)."""
+    calc_rho -> (dielectric walls' potential) -> pdesolver -> calc_Efield ->
+    (sort) -> (collisions) -> part_mover -> charge_deposition.  Returns
+    (Ei, mg result, MCC result)."""
     rhs = calc_rho(st, S.np)
+    if st.geom.flag_die:
+        dielectric_phi(st, phi, S.sum_q)
     mg_out = pdesolver(st, phi, rhs, **(mg or {}))
     Ei = calc_efield(st, phi, Ei)
     if nsort and it % nsort == 1 % nsort:
@@ -391,7 +411,7 @@ def step(st, S, phi, Ei, it, p_mac=None, P_loss=None, nsort=10, ns_coll=10, mg=N
         P_loss = np.zeros((st.ntype, 4))
     for p in range(1, st.ntype + 1):
         if st.charge[p - 1] != 0.0:
-            part_mover(st, Ei, S, p_mac, P_loss, p)
+            part_mover(st, Ei, S, p_mac, P_loss, p, sum_q=S.sum_q)
     for p in range(1, st.ntype + 1):
         S.np[p - 1] = 0.0
         if S.np_tot[p - 1] > 0:

@@ -1058,6 +1058,54 @@ static void die_charge(const Dims &d, const double h[3], const OPhys *P, int dt,
   }
 }
 
+// Src/main.f90:859-949 with one rank and nproc = 1: the reduction of the
+// surface-charge sums (0 + the one slice), the periodic-z doubling of the
+// boundary rows in place, the potential update of the dielectric walls'
+// nodes in the reference's loop order (iz, iy, ix, then ptype) and the
+// counters cleared.  qxz: sum_q_xz(0:n1+2,0:n3+2,ntype),
+// qyz: sum_q_yz(2,0:n2+2,0:n3+2,ntype); Ca: capacitance per cell.
+void oracle_dielectric_phi(const int n[3], double *phi, const int *bcnd, const int *dtype, int ngrid,
+                           double *qxz, double *qyz, int ntype, double Ca, int flag_pbc) {
+  Dims d(n);
+  const long N1 = d.n1 + 3, N2 = d.n2 + 3, N3 = d.n3 + 3;
+  const long nxz = N1 * N3, nyz = 2 * N2 * N3;
+  std::vector<double> rxz(ntype * nxz), ryz(ntype * nyz);
+  for (long t = 0; t < ntype * nxz; ++t) rxz[t] = 0.0 + qxz[t];
+  for (long t = 0; t < ntype * nyz; ++t) ryz[t] = 0.0 + qyz[t];
+  if (flag_pbc == 1) {
+    for (int p = 0; p < ntype; ++p) {
+      double *a = &rxz[p * nxz];
+      double *b = &ryz[p * nyz];
+      for (long x = 0; x < N1; ++x) {
+        a[x + N1 * 1] = 2.0 * a[x + N1 * 1];
+        a[x + N1 * (d.n3 + 1)] = 2.0 * a[x + N1 * (d.n3 + 1)];
+        a[x + N1 * 0] = 2.0 * a[x + N1 * d.n3];
+        a[x + N1 * (d.n3 + 2)] = 2.0 * a[x + N1 * 2];
+      }
+      for (long y = 0; y < 2 * N2; ++y) {
+        b[y + 2 * N2 * 1] = 2.0 * b[y + 2 * N2 * 1];
+        b[y + 2 * N2 * (d.n3 + 1)] = 2.0 * b[y + 2 * N2 * (d.n3 + 1)];
+        b[y + 2 * N2 * 0] = 2.0 * b[y + 2 * N2 * d.n3];
+        b[y + 2 * N2 * (d.n3 + 2)] = 2.0 * b[y + 2 * N2 * 2];
+      }
+    }
+  }
+  for (int iz = 0; iz <= d.n3 + 2; ++iz)
+    for (int iy = 0; iy <= d.n2 + 2; ++iy)
+      for (int ix = 0; ix <= d.n1 + 2; ++ix) {
+        const long g = d.g(ix, iy, iz);
+        const int igrid = bcnd[g];
+        if (igrid <= 0 || igrid > ngrid) continue;
+        for (int p = 0; p < ntype; ++p) {
+          if (dtype[igrid] == 2) phi[g] = phi[g] + rxz[p * nxz + ix + N1 * iz] / (2.0 * Ca);
+          if (dtype[igrid] == 3) phi[g] = phi[g] + ryz[p * nyz + 0 + 2 * (iy + N2 * iz)] / Ca;
+          if (dtype[igrid] == 4) phi[g] = phi[g] + ryz[p * nyz + 1 + 2 * (iy + N2 * iz)] / Ca;
+        }
+      }
+  std::memset(qxz, 0, sizeof(double) * ntype * nxz);
+  std::memset(qyz, 0, sizeof(double) * ntype * nyz);
+}
+
 int oracle_part_mover(const int n[3], const double h[3], const double *Ei, double *p_mac,
                       double *P_loss, double *vxp, const int *bcnd, int nmax, int ntype, int ngrid,
                       signed char *flag_dead, int *np_tot, int ptype, const OPhys *P,

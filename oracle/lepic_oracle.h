@@ -116,6 +116,9 @@ int oracle_pdesolver(double *u, const double *b, const int *bcnd,
                      const OPhys *P);
 void oracle_calc_efield(const int n[3], const double h[3], const double *phi,
                         double *Ei, const int *bcnd);
+void oracle_dielectric_phi(const int n[3], double *phi, const int *bcnd,
+                           const int *dtype, int ngrid, double *qxz,
+                           double *qyz, int ntype, double Ca, int flag_pbc);
 int oracle_part_mover(const int n[3], const double h[3], const double *Ei,
                       double *p_mac, double *P_loss, double *vxp,
                       const int *bcnd, int nmax, int ntype, int ngrid,

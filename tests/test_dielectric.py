@@ -75,7 +75,61 @@ def test_dielectric_charge_conservation():
         assert not qyz[p, ..., 1].any()
 
 
-def test_step_loop_rejects_dielectric_walls():
+def test_step_loop_dielectric_guards():
+    """the mixed form does not sum surface charge, and the walls need Ca"""
     from essaitemporaire_lepic_module_b200.sim import Simulation
+    st = config.build("die16")
+    assert abs(st.Ca - 2e-8 * st.h[0] * st.h[2]) <= 1e-30
     with pytest.raises(NotImplementedError):
-        Simulation(config.build("die16"), cap=1000, device="cpu")
+        Simulation(st, cap=1000, device="cpu", precision="mixed")
+    st.Ca = 0.0
+    with pytest.raises(ValueError):
+        Simulation(st, cap=1000, device="cpu")
+
+
+def _random_sums(st, seed):
+    rng = np.random.default_rng(seed)
+    qxz, qyz = _sums(st)
+    qxz[...] = rng.normal(0.0, 1e-17, qxz.shape)
+    qyz[...] = rng.normal(0.0, 1e-17, qyz.shape)
+    return qxz, qyz
+
+
+@pytest.mark.parametrize("pbc", [0, 1])
+def test_dielectric_phi_known_answer(pbc):
+    """Src/main.f90:859-949: Q/(2 Ca) per species on the Y plane's nodes,
+    Q/Ca on the X plane's, the periodic-z doubling of rows 1, n3+1 and the
+    copies into rows 0 and n3+2, nothing elsewhere, the sums cleared."""
+    st = config.build("die16")
+    st.geom.flag_pbc = pbc
+    n1, n2, n3 = st.n
+    qxz, qyz = _random_sums(st, 3)
+    rxz, ryz = qxz.copy(), qyz.copy()
+    phi = st.geom.phi.copy()
+    oracle.dielectric_phi(st, phi, (qxz, qyz))
+    assert not qxz.any() and not qyz.any()
+    Ca = st.Ca
+
+    def row(iz):
+        if not pbc:
+            return iz, 1.0
+        if iz == 0:
+            return n3, 2.0
+        if iz == n3 + 2:
+            return 2, 2.0
+        return iz, 2.0 if iz in (1, n3 + 1) else 1.0
+
+    for iz in (0, 1, 2, 7, n3, n3 + 1, n3 + 2):
+        jz, f = row(iz)
+        # a Y-plane node (label 2) and an X-plane node (label 3)
+        want = st.geom.phi[iz, n2 + 1, 5]
+        for p in range(st.ntype):
+            want = want + (f * rxz[p, jz, 5]) / (2.0 * Ca)
+        assert phi[iz, n2 + 1, 5] == want
+        want = st.geom.phi[iz, 6, n1 + 1]
+        for p in range(st.ntype):
+            want = want + (f * ryz[p, jz, 6, 0]) / Ca
+        assert phi[iz, 6, n1 + 1] == want
+    other = st.geom.bcnd != 2
+    other &= st.geom.bcnd != 3
+    np.testing.assert_array_equal(phi[other], st.geom.phi[other])

@@ -48,3 +48,63 @@ def test_dielectric_dropin_vs_oracle():
         assert scale > 0
         np.testing.assert_allclose(a, b, rtol=0, atol=1e-12 * scale)
 
+
+
+@pytest.mark.parametrize("pbc", [0, 1])
+def test_dielectric_phi_device_bit_exact(pbc):
+    """lepic_dev_dielectric_phi (Src/main.f90:859-949) against the oracle on
+    random surface charges: phi bit for bit, the sums cleared."""
+    import torch
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    st = config.build("die16")
+    st.geom.flag_pbc = pbc
+    rng = np.random.default_rng(11 + pbc)
+    qo = _sums(st)
+    for a in qo:
+        a[...] = rng.normal(0.0, 1e-17, a.shape)
+    sim = Simulation(st, cap=1000)
+    sim.die[1].copy_(torch.as_tensor(qo[0]))
+    sim.die[2].copy_(torch.as_tensor(qo[1]))
+    phi_o = st.geom.phi.copy()
+    oracle.dielectric_phi(st, phi_o, qo)
+    sim.dielectric_phi()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(sim.phi.cpu().numpy(), phi_o)
+    assert not sim.die[1].any() and not sim.die[2].any()
+    assert (phi_o != st.geom.phi).sum() > 100
+
+
+@pytest.mark.parametrize("fused", [True, False])
+def test_step_loop_dielectric(fused):
+    """20 device steps of the FP64 loop on die16 (surface charge summed by the
+    push, the walls' potential raised before each field solve) against 20
+    oracle steps: particles and phi within 1e-10, the walls charged."""
+    import torch
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    oracle.set_threads(1)
+    st = config.build("die16")
+    nmax = st.n_particles() + 4096
+    S = oracle.load_part(st, nmax=nmax)
+    sim = Simulation(st, cap=nmax, fused=fused)
+    sim.load_from_host(S.vxp, S.np_tot, S.np)
+    phi = st.geom.phi.copy()
+    Ei = np.zeros(tuple(st.geom.bcnd.shape) + (3,))
+    for it in range(1, 21):
+        Ei, _, _ = oracle.step(st, S, phi, Ei, it)
+        sim.step()
+    torch.cuda.synchronize()
+    for p in range(st.ntype):
+        g = sim.sp[p].to_vxp()
+        o = S.vxp[p, :S.np_tot[p]]
+        assert g.shape == o.shape
+        ko = np.lexsort((o[:, 2], o[:, 1], o[:, 0]))
+        kg = np.lexsort((g[:, 2], g[:, 1], g[:, 0]))
+        scale = np.abs(o).max(axis=0)
+        assert (np.abs(g[kg] - o[ko]) <= 1e-10 * scale).all(), p
+    phg = sim.phi.cpu().numpy()
+    assert np.abs(phg - phi).max() <= 1e-10 * np.abs(phi).max()
+    n1, n2, n3 = st.n
+    assert np.abs(phi[:, n2 + 1, :]).max() > 1e-3       # the Y plane charged
+    assert np.abs(phi[:, :, n1 + 1]).max() > 1e-3       # the X plane charged
+    for a, b in zip(sim.die[1:], S.sum_q):
+        np.testing.assert_allclose(a.cpu().numpy(), b, rtol=0, atol=1e-10 * max(np.abs(b).max(), 1e-30))
