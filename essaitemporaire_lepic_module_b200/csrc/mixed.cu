@@ -27,6 +27,7 @@
 // A thread moves four consecutive particles with 16-byte loads and stores
 // and merges the weights of those that end in the same cell before touching
 // shared memory.
+#include <type_traits>
 #include <cstring>
 
 #include "lepic_internal.cuh"
@@ -60,7 +61,41 @@ struct MixedConst {
   int boris, flag_pbc, flag_nmn, ngrid;
   double Nm, mass, kdep;      // kdep = Nm / (h1 h2 h3)
   int ntx, nty, ntiles;       // tile grid
+  Dielectric die;             // dielectric walls (die.dtype nullptr: none)
 };
+
+// The charge of a particle lost on a dielectric wall (Src/part_expmover.f90:
+// 302-348) from its cell coordinates: new cell (ax, ay, az) (z already
+// wrapped with periodic planes) with offsets (fx, fy, fz) in [0, 1), clamped
+// to (cx, cy, cz).  The reference's weight (ix h - x) / h is
+// cx - (ax - 1 + fx) here, evaluated in FP64.
+// Out of line and with its arguments by value: the branch is rare, and the
+// kernel parameters' addresses are never taken (which would copy them to
+// local memory).
+__device__ __noinline__ void dielectric_charge_cells(Dielectric die, long long N1, long long N2, int igrid,
+                                                     int ax, int ay, int az, float fx, float fy, float fz,
+                                                     int cx, int cy, int cz) {
+  const int dt = die.dtype[igrid];
+  if (dt <= 1) return;
+  const double pz = (double)cz - ((double)(az - 1) + (double)fz);
+  if (dt == 2) {
+    const double px = (double)cx - ((double)(ax - 1) + (double)fx);
+    double *q = die.qxz;
+    const long long NX = N1;
+    atomicAdd(&q[cx + NX * cz], die.k3 * px * pz);
+    atomicAdd(&q[cx + 1 + NX * cz], die.k3 * (1.0 - px) * pz);
+    atomicAdd(&q[cx + 1 + NX * (cz + 1)], die.k3 * (1.0 - px) * (1.0 - pz));
+    atomicAdd(&q[cx + NX * (cz + 1)], die.k3 * px * (1.0 - pz));
+  } else if (dt == 3 || dt == 4) {
+    const double py = (double)cy - ((double)(ay - 1) + (double)fy);
+    double *q = die.qyz + (dt - 3);
+    const long long NY = N2;
+    atomicAdd(&q[2 * (cy + NY * cz)], die.k3 * py * pz);
+    atomicAdd(&q[2 * (cy + 1 + NY * cz)], die.k3 * (1.0 - py) * pz);
+    atomicAdd(&q[2 * (cy + 1 + NY * (cz + 1))], die.k3 * (1.0 - py) * (1.0 - pz));
+    atomicAdd(&q[2 * (cy + NY * (cz + 1))], die.k3 * py * (1.0 - pz));
+  }
+}
 
 // x rounded to the nearest integer for 0 <= x <= 2^22, by the FP32 addition
 // of 1.5 * 2^23 (whose unit in the last place is 1) and integer arithmetic
@@ -237,7 +272,7 @@ __device__ __forceinline__ bool bmap_gather_mixed(const MixedBMap &m, const Tile
 // Push + loss test + deposit of the particle quad Q starting at i0;
 // particles outside the range are not touched.  Every lane of the warp must
 // call this (warp-wide hole appends).  BMAP: B from the map m.
-template <bool BMAP>
+template <bool BMAP, bool DIE>
 __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, const MixedBMap &m, const Tile &T,
                                           long long i0, Quad &Q, const float4 *__restrict__ E4,
                                           const int *__restrict__ bcnd, const unsigned char *__restrict__ cw,
@@ -387,6 +422,10 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
       if (igrid >= 0 && igrid <= c.ngrid) {
         atomicAdd(&acc[2 + 2 * igrid], 1.0);
         atomicAdd(&acc[3 + 2 * igrid], Eki);
+        if (DIE) {
+          const Dielectric die = {c.die.dtype, c.die.qxz, c.die.qyz, c.die.k3};
+          dielectric_charge_cells(die, d.N1, d.N2, igrid, ax, ay, az, fx, fy, fz, cx, cy, cz);
+        }
       }
       hole[k] = true;
     } else {
@@ -461,7 +500,7 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
 // one block per tile: the particles [tile_off[t], tile_off[t+1]) of the last
 // sort, clipped to the current count; E and the wall flags of the tile's box
 // are read into shared memory once
-template <bool BMAP>
+template <bool BMAP, bool DIE>
 __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tiles(
     Dims d, MixedConst c, MixedBMap m, const float4 *__restrict__ E4, const int *__restrict__ bcnd,
     const unsigned char *__restrict__ cw, int *__restrict__ cell, float *__restrict__ p, long long cap,
@@ -500,7 +539,7 @@ __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tiles(
     Quad Q;
     const long long i0 = base + 4 * threadIdx.x;
     load_quad(Q, i0, lo, hi, cell, p, cap, flag);
-    push_quad<BMAP>(d, c, m, T, i0, Q, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes, acc, err);
+    push_quad<BMAP, DIE>(d, c, m, T, i0, Q, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes, acc, err);
     if (++chunks == FLUSH_PARTICLES / CHUNK && base + CHUNK < hi) {
       chunks = 0;
       __syncthreads();
@@ -514,7 +553,7 @@ __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tiles(
 
 // particles past the last tile (appended since the sort), or all of them
 // when no sort has run: deposited straight into the FP64 grid
-template <bool BMAP>
+template <bool BMAP, bool DIE>
 __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tail(
     Dims d, MixedConst c, MixedBMap m, const float4 *__restrict__ E4, const int *__restrict__ bcnd,
     const unsigned char *__restrict__ cw, int *__restrict__ cell, float *__restrict__ p, long long cap,
@@ -529,7 +568,7 @@ __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tail(
     Quad Q;
     const long long i0 = base + 4 * threadIdx.x;
     load_quad(Q, i0, lo, N, cell, p, cap, flag);
-    push_quad<BMAP>(d, c, m, T, i0, Q, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes, acc, err);
+    push_quad<BMAP, DIE>(d, c, m, T, i0, Q, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes, acc, err);
   }
 }
 
@@ -876,7 +915,6 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
   const int p = ptype - 1;
   if (!sp.flag_dead || !aligned16(E4)) return LEPIC_ERR_ARG;
   if (int rc = check_layout(g, sp)) return rc;
-  if (P.dtype) return LEPIC_ERR_UNSUPPORTED;  // dielectric walls: FP64 push only
   MixedConst c;
   memset(&c, 0, sizeof(c));
   c.dth0 = (float)(P.dt / g.h[0]);
@@ -896,6 +934,7 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
   c.flag_pbc = P.flag_pbc;
   c.flag_nmn = P.flag_nmn;
   c.ngrid = ngrid;
+  c.die = dielectric_from_phys(P, g.n, ptype);
   c.Nm = P.Nm[p];
   c.mass = P.mass[p];
   c.kdep = P.Nm[p] / (g.h[0] * g.h[1] * g.h[2]);
@@ -946,23 +985,27 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
   // the tail: at most what was appended since the sort unless never sorted
   long long tail = sp.tile_off ? (long long)ctx().sms * 2 : grid_for(n_hint > 0 ? n_hint : sp.cap, CHUNK);
   if (tail > (long long)ctx().sms * 8) tail = (long long)ctx().sms * 8;
-  if (m.B) {
+  // four instances: B map or uniform B, dielectric walls or none (the
+  // uniform kernels without walls keep their registers)
+  auto run = [&](auto bmap, auto die) {
+    constexpr bool B = decltype(bmap)::value, D = decltype(die)::value;
     if (sp.tile_off)
-      k_push_deposit_tiles<true><<<c.ntiles, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap,
+      k_push_deposit_tiles<B, D><<<c.ntiles, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap,
                                                           sp.count, sp.flag_dead, sp.tile_off, g.kq, np, holes,
                                                           side, acc, ctx().d_err);
-    k_push_deposit_tail<true><<<(int)tail, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap,
+    k_push_deposit_tail<B, D><<<(int)tail, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap,
                                                         sp.count, sp.flag_dead, sp.tile_off, g.kq, np, holes,
                                                         side, acc, ctx().d_err);
-  } else {
-    if (sp.tile_off)
-      k_push_deposit_tiles<false><<<c.ntiles, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p,
-                                                           sp.cap, sp.count, sp.flag_dead, sp.tile_off, g.kq, np,
-                                                           holes, side, acc, ctx().d_err);
-    k_push_deposit_tail<false><<<(int)tail, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap,
-                                                         sp.count, sp.flag_dead, sp.tile_off, g.kq, np, holes,
-                                                         side, acc, ctx().d_err);
-  }
+  };
+  const bool die = c.die.dtype != nullptr;
+  if (m.B && die)
+    run(std::true_type{}, std::true_type{});
+  else if (m.B)
+    run(std::true_type{}, std::false_type{});
+  else if (die)
+    run(std::false_type{}, std::true_type{});
+  else
+    run(std::false_type{}, std::false_type{});
   timer_stop(t0, s);
   LEPIC_CUDA(cudaGetLastError());
   int t1 = timer_start("fill_holes_mixed", s);

@@ -166,10 +166,6 @@ class Simulation:
                  check_every=1, heating=None, injection=None):
         if precision not in ("f64", "mixed"):
             raise ValueError(f"precision must be 'f64' or 'mixed', not {precision!r}")
-        if st.geom.flag_die and precision == "mixed":
-            # the surface charge of dielectric walls is summed by the FP64
-            # pushes only
-            raise NotImplementedError("dielectric walls: the step loop runs them in the f64 form")
         if st.geom.flag_die and not st.Ca > 0.0:
             raise ValueError("dielectric walls need a capacitance Ca > 0")
         self.st = st
@@ -216,7 +212,7 @@ class Simulation:
         if st.geom.flag_die:
             # dielectric walls: dtype(0:ngrid) and the surface-charge sums of
             # every species, sum_q_xz (ntype, n3+3, n1+3) and sum_q_yz
-            # (ntype, n3+3, n2+3, 2), which the FP64 pushes add to
+            # (ntype, n3+3, n2+3, 2), which the pushes add to
             n1, n2, n3 = st.n
             f64 = dict(dtype=torch.float64, device=self.dev)
             self.die = (torch.as_tensor(st.geom.dtype_array(), device=self.dev),

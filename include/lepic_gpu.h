@@ -409,7 +409,9 @@ int lepic_dev_part_mover(const lepic_grid_t *g, const double *Ei, lepic_species_
  * slots (order not kept; the periodic sort restores cell order).  np: device
  * grid of this species (accumulated); acc: device doubles [2 + 2(ngrid+1)]
  * accumulating P_loss(1), P_loss(3) and p_mac(count, energy) per wall label.
- * n_hint: an upper bound of the species' count (grid size), <= 0 = capacity. */
+ * n_hint: an upper bound of the species' count (grid size), <= 0 = capacity.
+ * With P->dtype set, the surface charge of the particles lost on dielectric
+ * walls is added to P->sum_q_xz / P->sum_q_yz. */
 int lepic_dev_push_deposit(const lepic_grid_t *g, const double *Ei, lepic_species_f64_t *s,
                            int ptype, int ngrid, const lepic_phys_t *P, double *np, double *acc,
                            int n_hint, void *stream);
@@ -421,7 +423,8 @@ int lepic_dev_push_deposit(const lepic_grid_t *g, const double *Ei, lepic_specie
  * particle deposits exactly 1) and summed exactly in integers per sorted
  * tile on chip, then added into the FP64 grid np.  Requires a closed box
  * (cells outside 1..n are walls).  n_hint: an upper bound of the count, used
- * only before the first sort (<= 0: capacity). */
+ * only before the first sort (<= 0: capacity).  Dielectric walls of P as in
+ * lepic_dev_push_deposit (weights from the FP32 offsets, summed in FP64). */
 int lepic_dev_push_deposit_mixed(const lepic_grid_t *g, const float *E4, lepic_species_mixed_t *s,
                                  int ptype, int ngrid, const lepic_phys_t *P, double *np, double *acc,
                                  int n_hint, void *stream);

@@ -2,8 +2,8 @@
 the CPU oracle: the labels of generate_boundary (Src/generate_boundary.f90:
 yr < 0 a Y = const dielectric, xr < 0 an X = const one), a hand-computed
 known answer for one electron on each plane, and charge conservation --
-each lost particle puts exactly Nm q on its plane.  The device step loop
-refuses the geometry instead of ignoring the walls' charge."""
+each lost particle puts exactly Nm q on its plane; the potential update of
+the walls from the sums (Src/main.f90:859-949)."""
 import numpy as np
 import pytest
 
@@ -76,12 +76,10 @@ def test_dielectric_charge_conservation():
 
 
 def test_step_loop_dielectric_guards():
-    """the mixed form does not sum surface charge, and the walls need Ca"""
+    """the walls need a capacitance"""
     from essaitemporaire_lepic_module_b200.sim import Simulation
     st = config.build("die16")
     assert abs(st.Ca - 2e-8 * st.h[0] * st.h[2]) <= 1e-30
-    with pytest.raises(NotImplementedError):
-        Simulation(st, cap=1000, device="cpu", precision="mixed")
     st.Ca = 0.0
     with pytest.raises(ValueError):
         Simulation(st, cap=1000, device="cpu")

@@ -108,3 +108,42 @@ def test_step_loop_dielectric(fused):
     assert np.abs(phi[:, :, n1 + 1]).max() > 1e-3       # the X plane charged
     for a, b in zip(sim.die[1:], S.sum_q):
         np.testing.assert_allclose(a.cpu().numpy(), b, rtol=0, atol=1e-10 * max(np.abs(b).max(), 1e-30))
+
+
+def test_step_loop_dielectric_mixed():
+    """The mixed step loop on die16: the surface charge of one step equals
+    Nm q times the particles it lost on each dielectric label (1e-12), and
+    after 10 steps the walls' potential is within 10 % of the FP64 loop's
+    from the same particles (FP32 trajectories lose a few particles at other
+    steps)."""
+    import torch
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    oracle.set_threads(1)
+    st = config.build("die16")
+    nmax = st.n_particles() + 4096
+    S = oracle.load_part(st, nmax=nmax)
+    runs = {}
+    for prec in ("mixed", "f64"):
+        sim = Simulation(st, cap=nmax, precision=prec)
+        sim.load_from_host(S.vxp, S.np_tot, S.np)
+        for _ in range(9):
+            sim.step()
+        pm0, _ = sim.loss_stats()
+        sim.step()
+        torch.cuda.synchronize()
+        pm1, _ = sim.loss_stats()
+        runs[prec] = sim.phi.cpu().numpy()
+        if prec != "mixed":
+            continue
+        qxz, qyz = (t.cpu().numpy() for t in sim.die[1:])
+        for p in range(st.ntype):
+            k3 = st.Nm[p] * st.charge[p]
+            d2, d3 = pm1[2, 0, p] - pm0[2, 0, p], pm1[3, 0, p] - pm0[3, 0, p]
+            assert abs(qxz[p].sum() - k3 * d2) <= 1e-12 * abs(k3) * max(d2, 1)
+            assert abs(qyz[p, ..., 0].sum() - k3 * d3) <= 1e-12 * abs(k3) * max(d3, 1)
+            assert not qyz[p, ..., 1].any()
+        assert pm1[2, 0, 0] > 20 and pm1[3, 0, 0] > 20
+    wall = (st.geom.bcnd == 2) | (st.geom.bcnd == 3)
+    a, b = runs["mixed"][wall], runs["f64"][wall]
+    assert np.abs(b).max() > 1e-3
+    assert np.abs(a - b).max() <= 0.1 * np.abs(b).max()
