@@ -131,3 +131,39 @@ def test_dielectric_phi_known_answer(pbc):
     other = st.geom.bcnd != 2
     other &= st.geom.bcnd != 3
     np.testing.assert_array_equal(phi[other], st.geom.phi[other])
+
+
+def _corner_electron(st):
+    """an electron that leaves through the y = ymax dielectric and z = zmax
+    at once (the corner cell carries label 2)"""
+    h, L = st.h, st.geom.box
+    S = oracle.State(st, 4)
+    S.vxp[0, 0] = [5.3 * h[0], L[1] - 0.1 * h[1], L[2] - 0.2 * h[2], 0.0, 0.5 * h[1] / st.dt,
+                   0.5 * h[2] / st.dt]
+    S.np_tot[0] = 1
+    return S
+
+
+def test_dielectric_periodic_z_wrap():
+    """Src/part_expmover.f90:306-316: with periodic z planes the position of
+    a particle lost on a dielectric wraps before the weights (z - zmax, row
+    floor(z/h)+1)."""
+    st = config.build("die16")
+    st.geom.flag_pbc = 1
+    S = _corner_electron(st)
+    Ei = np.zeros(tuple(st.geom.bcnd.shape) + (3,))
+    qxz, qyz = _sums(st)
+    pm = np.zeros((st.geom.ngrid + 1, 2, st.ntype))
+    oracle.part_mover(st, Ei, S, pm, np.zeros((st.ntype, 4)), 1, sum_q=(qxz, qyz))
+    assert S.np_tot[0] == 0 and pm[2, 0, 0] == 1
+    k3 = st.Nm[0] * st.charge[0]
+    zq = (st.geom.box[2] - 0.2 * st.h[2] + 0.5 * st.h[2]) - st.geom.box[2]
+    iq = int(np.floor(zq / st.h[2])) + 1
+    assert iq == 1
+    px, pz = 6 - 5.3, (iq * st.h[2] - zq) / st.h[2]
+    want = np.zeros_like(qxz[0])
+    want[1, 6] = k3 * px * pz
+    want[1, 7] = k3 * (1 - px) * pz
+    want[2, 7] = k3 * (1 - px) * (1 - pz)
+    want[2, 6] = k3 * px * (1 - pz)
+    np.testing.assert_allclose(qxz[0], want, rtol=1e-9, atol=0)

@@ -147,3 +147,24 @@ def test_step_loop_dielectric_mixed():
     a, b = runs["mixed"][wall], runs["f64"][wall]
     assert np.abs(b).max() > 1e-3
     assert np.abs(a - b).max() <= 0.1 * np.abs(b).max()
+
+
+def test_dielectric_periodic_z_wrap_dropin():
+    """the z wrap of a particle lost on a dielectric (periodic z planes): the
+    drop-in's plane sums equal the oracle's"""
+    from tests.test_dielectric import _corner_electron
+    st = config.build("die16")
+    st.geom.flag_pbc = 1
+    dropin.set_commons(st)
+    So = _corner_electron(st)
+    Sg = So.copy()
+    Ei = np.zeros(tuple(st.geom.bcnd.shape) + (3,))
+    ng1 = st.geom.ngrid + 1
+    qo, qg = _sums(st), _sums(st)
+    oracle.part_mover(st, Ei, So, np.zeros((ng1, 2, st.ntype)), np.zeros((st.ntype, 4)), 1, sum_q=qo)
+    dropin.part_mover(st, Ei, Sg.vxp, Sg.np_tot, Sg.flag_dead, np.zeros((ng1, 2, st.ntype)),
+                      np.zeros((st.ntype, 4)), 1, sum_q=qg)
+    assert So.np_tot[0] == 0 and Sg.np_tot[0] == 0
+    assert qo[0][0, 1:3].any()
+    np.testing.assert_array_equal(qg[0], qo[0])
+    np.testing.assert_array_equal(qg[1], qo[1])
