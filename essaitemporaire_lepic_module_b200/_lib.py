@@ -57,7 +57,7 @@ class LepicSpeciesMixed(C.Structure):
 class LepicTargets(C.Structure):
     """lepic_targets_t: charged-target (DSMC) inputs and counters."""
     _fields_ = [("np", C.c_void_p * NPART), ("cell_off", C.c_void_p * NPART),
-                ("missed", C.c_longlong), ("lost_claims", C.c_longlong)]
+                ("missed", C.c_longlong), ("lost_claims", C.c_longlong), ("replayed", C.c_longlong)]
 
 
 class LepicHeat(C.Structure):

@@ -24,7 +24,9 @@ set-ups shrunk so the FP64 CPU oracle finishes in seconds):
              planes in y and z (pbc32x16: 32 cells in x)
   nmn16      the same with the Neumann (symmetry) plane at x = 0
   dsmc16     16^3 box, e- + Ar+ 16 ppc, e-Ar+ elastic collisions with
-             charged targets (dsmcar16: with the Ar MCC as well)
+             charged targets (dsmcar16: with the Ar MCC as well; dsmc32:
+             32^3 box, 40 ppc and a cross section 20 times larger, about
+             1e5 collisions per call, several on one ion in many cells)
 """
 from __future__ import annotations
 
@@ -91,13 +93,14 @@ def workload(name: str) -> Workload:
         return Workload(name, n, 1e-4, [_box(n, 1e-4) + [1]], [0.0, 0.0], _ar_ion(),
                         Te=2.0, n0=1e15, ppc=64 if name != "mcc32" else 32, dt=2e-11, steps=500,
                         B=(0.0, 0.0, 0.01), gas_pressure=1.0, gas_T=300.0)
-    if name in ("dsmc16", "dsmcar16"):
+    if name in ("dsmc16", "dsmcar16", "dsmc32"):
         # e-Ar+ elastic collisions with charged targets (dsmcar16: on top of
-        # the Ar MCC of mcc128)
-        n = (16, 16, 16)
+        # the Ar MCC of mcc128; dsmc32: dense, nu_max at its cap nu_uplim)
+        n = (32, 32, 32) if name == "dsmc32" else (16, 16, 16)
         return Workload(name, n, 1e-4, [_box(n, 1e-4) + [1]], [0.0, 0.0], _ar_ion(),
-                        Te=2.0, n0=1e15, ppc=16, dt=2e-11, steps=200, B=(0.0, 0.0, 0.01),
-                        gas_pressure=1.0 if name == "dsmcar16" else 0.0, gas_T=300.0, coulomb=2e-13)
+                        Te=2.0, n0=1e15, ppc=40 if name == "dsmc32" else 16, dt=2e-11, steps=200,
+                        B=(0.0, 0.0, 0.01), gas_pressure=1.0 if name == "dsmcar16" else 0.0, gas_T=300.0,
+                        coulomb=4e-12 if name == "dsmc32" else 2e-13)
     if name in ("pbc16", "pbc32x16", "nmn16"):
         # walls at both x ends (nmn16: the Neumann plane at x = 0 instead),
         # periodic planes in y and z (a box segment, then label 0 over it)

@@ -31,11 +31,17 @@
 // mean of the species' density grid over the cell's 8 nodes.  The collision
 // may change the target's velocity (elastic, excitation, charge exchange) or
 // remove it (other reactions).  The reference runs the collisions one after
-// another; here the incident particles collide concurrently, so a target
-// taken by one collision is claimed (one flag per particle, cleared per
-// call) and a second collision that drew the same target is dropped and
-// counted (lost_claims; rare while collisions per call are few against the
-// targets in a cell).
+// another, so a target drawn by two incident particles takes part in both,
+// the second seeing the velocity the first left.  Here the incident
+// particles collide concurrently in rounds: a collision claims its target
+// with the round's tag (one word per particle, cleared per call); one that
+// finds its target claimed in the same round changes nothing, goes to the
+// next round's list and is evaluated again from its own draws (same target,
+// same uniform) once the first collision is done -- the order of a serial
+// loop in which the winner came first.  Every drawn collision happens; the
+// rounds end when no collision is left over (lost_claims counts those still
+// left at the round cap, and stays zero while a target is hit by fewer
+// collisions than there are rounds).
 #include <vector>
 
 #include "lepic_internal.cuh"
@@ -47,6 +53,11 @@ namespace {
 constexpr int MB = 256;
 constexpr int MAXR = 48;  // reactions per incident species (hydrogen.dat's electrons: 40)
 constexpr int MAXBY = 4;  // byproducts per reaction
+// DSMC rounds per species and call (a target hit by more collisions than
+// this in one call leaves the excess undone, counted as lost_claims), and
+// rounds launched between two reads of the count left
+constexpr int DSMC_ROUNDS = 256;
+constexpr int DSMC_BATCH = 8;
 
 // one reaction of the incident species; the table lives in device memory
 // (runtime-indexed arrays in the kernel's parameters would be copied to
@@ -162,7 +173,9 @@ struct Targets {
   int *claim[LEPIC_NPART];
   int tile, n1, n2, n3, ntx, nty;
   long long pl_max;
-  unsigned long long *stat;     // [0] incident particles with no target, [1] lost claims
+  // [0] incident particles with no target, [1] collisions left at the round
+  // cap, [2] collisions deferred to a later round (target taken first)
+  unsigned long long *stat;
 };
 
 // a particle of species T in cell ici (1-based linear index) or its six
@@ -333,13 +346,24 @@ struct TState {
   bool ok;
 };
 
+// DSMC rounds: `tag` marks the claims of this round (claims of earlier
+// rounds hold smaller tags); a collision whose target carries this round's
+// tag appends its particle to `defer` (counter *ndefer) for the next round.
+// first: the first round of the call (the only one that counts misses).
+struct Round {
+  int *defer;
+  int *ndefer;
+  int tag;
+  int first;
+};
+
 template <class Acc, bool DSMC>
 __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D, const int *__restrict__ cand,
                                                     const int *__restrict__ ncand_p,
                                                     const double *__restrict__ Er,
                                                     const double *__restrict__ sig, signed char *flag_dead,
                                                     int *add, unsigned long long *counts, double *cnt_col,
-                                                    int *err) {
+                                                    int *err, Round rd) {
   const unsigned full = 0xffffffffu;
   const int P = c.ptype - 1;
   const int ncand = *ncand_p;
@@ -431,7 +455,7 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
       // the same order up to the drawn u (Src/collisions.f90:714-737)
       double sum_nu = 0.0;
       for (int r = 0; r < c.nr; ++r) sum_nu += nu_of(r);
-      if (DSMC && missed) atomicAdd(&D.stat[0], (unsigned long long)__popc(missed));
+      if (DSMC && missed && rd.first) atomicAdd(&D.stat[0], (unsigned long long)__popc(missed));
       const double u = u01(r0.y);
       if (u <= sum_nu) {
         double s = 0.0;
@@ -447,9 +471,11 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
       const bool tgt = DSMC && sel >= 0 && c.R[sel].dsmc;
       if (sel >= 0) {
         if (c.R[sel].tt != cur_tt) ts = partner(c.R[sel].tt, tgt);
-        // a charged target takes part in one collision per call
-        if (tgt && atomicExch(&D.claim[c.R[sel].tt - 1][ts.idx], 1) != 0) {
-          atomicAdd(&D.stat[1], 1ull);
+        // a charged target takes part in one collision per round; a later
+        // collision on it is evaluated again in the next round
+        if (tgt && atomicExch(&D.claim[c.R[sel].tt - 1][ts.idx], rd.tag) == rd.tag) {
+          rd.defer[atomicAdd(rd.ndefer, 1)] = (int)i;
+          atomicAdd(&D.stat[2], 1ull);
           sel = -1;
         }
       }
@@ -577,9 +603,11 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
   // cell indices beyond n1 n2 n3 hold no particles: every Plist covering the
   // grid's cells is read within its bounds
   D.pl_max = (long long)g.n[0] * g.n[1] * g.n[2];
-  D.stat = (unsigned long long *)scratch("mcc_dsmc_stat", 2 * sizeof(unsigned long long));
+  D.stat = (unsigned long long *)scratch("mcc_dsmc_stat", 3 * sizeof(unsigned long long));
   if (!D.stat) return LEPIC_ERR_CUDA;
-  LEPIC_CUDA(cudaMemsetAsync(D.stat, 0, 2 * sizeof(unsigned long long), s));
+  LEPIC_CUDA(cudaMemsetAsync(D.stat, 0, 3 * sizeof(unsigned long long), s));
+  int tag = 0;                  // claim tag of the last DSMC round launched
+  unsigned long long left_over = 0;
   for (int q = 0; q < ntype; ++q) {
     D.fd[q] = flag_dead[q];
     if (tg) {
@@ -633,6 +661,12 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
         return LEPIC_ERR_UNSUPPORTED;
       }
       const int tt = CI(ind, 2 + n_re);
+      if (P.charge[tt - 1] != 0.0 && tt == p) {
+        // the incident would have to be claimed as well as its target
+        fprintf(stderr, "lepic_gpu: collisions: reaction %d has a charged target of the incident's own species\n",
+                ind);
+        return LEPIC_ERR_UNSUPPORTED;
+      }
       if (P.charge[tt - 1] != 0.0) {
         // a charged target: its density grid and sort offsets are needed
         if (tt > ntype || !D.np[tt - 1] || !D.off[tt - 1] || !D.fd[tt - 1]) {
@@ -719,12 +753,47 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
     }
     timer_stop(tm, s);
     tm = timer_start(tname, s);
-    if (c.any_dsmc)
-      k_mcc_collide<Acc, true><<<ctx().sms * 8, MB, 0, s>>>(c, S, D, cand, ncand + (p - 1), T.sig_Er, T.sig,
-                                                            flag_dead[p - 1], add, cnt, cc, ctx().d_err);
-    else
+    if (c.any_dsmc) {
+      // rounds until no collision is deferred: the list of round r is read
+      // from one buffer while the deferrals of the round go to the other
+      // (the candidate list and a deferral list of the same capacity);
+      // rc[r] counts the collisions of round r >= 1
+      snprintf(nm, sizeof nm, "mcc_defer%d", p - 1);
+      int *defer = (int *)scratch(nm, sizeof(int) * (size_t)S.cap[p - 1]);
+      int *rc = (int *)scratch("mcc_round_cnt", sizeof(int) * (DSMC_ROUNDS + 1));
+      if (!defer || !rc) return LEPIC_ERR_CUDA;
+      LEPIC_CUDA(cudaMemsetAsync(rc, 0, sizeof(int) * (DSMC_ROUNDS + 1), s));
+      int r = 0;
+      for (;;) {
+        // a batch of rounds without a host round trip (an empty round
+        // returns at once), then the count left for the next round
+        const int stop = r + DSMC_BATCH < DSMC_ROUNDS ? r + DSMC_BATCH : DSMC_ROUNDS;
+        for (; r < stop; ++r) {
+          Round rd;
+          rd.defer = (r & 1) ? cand : defer;
+          rd.ndefer = rc + r + 1;
+          rd.tag = ++tag;
+          rd.first = r == 0;
+          const int *in = (r & 1) ? defer : cand;
+          const int *nin = r == 0 ? ncand + (p - 1) : rc + r;
+          k_mcc_collide<Acc, true><<<ctx().sms * 8, MB, 0, s>>>(c, S, D, in, nin, T.sig_Er, T.sig,
+                                                                flag_dead[p - 1], add, cnt, cc, ctx().d_err, rd);
+          LEPIC_CUDA(cudaGetLastError());
+        }
+        int left = 0;
+        LEPIC_CUDA(cudaMemcpyAsync(&left, rc + r, sizeof(int), cudaMemcpyDeviceToHost, s));
+        LEPIC_CUDA(cudaStreamSynchronize(s));
+        if (left == 0) break;
+        if (r >= DSMC_ROUNDS) {
+          left_over += (unsigned long long)left;
+          break;
+        }
+      }
+    } else {
+      Round rd{nullptr, nullptr, 0, 1};
       k_mcc_collide<Acc, false><<<ctx().sms * 8, MB, 0, s>>>(c, S, D, cand, ncand + (p - 1), T.sig_Er, T.sig,
-                                                             flag_dead[p - 1], add, cnt, cc, ctx().d_err);
+                                                             flag_dead[p - 1], add, cnt, cc, ctx().d_err, rd);
+    }
     timer_stop(tm, s);
     LEPIC_CUDA(cudaGetLastError());
   }
@@ -736,7 +805,7 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
   }
   k_mcc_finalize<<<1, 1, 0, s>>>(fc, add, ntype);
   LEPIC_CUDA(cudaGetLastError());
-  unsigned long long hc[64], hs[2];
+  unsigned long long hc[64], hs[3];
   LEPIC_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, s));
   LEPIC_CUDA(cudaMemcpyAsync(hs, D.stat, sizeof(hs), cudaMemcpyDeviceToHost, s));
   const int rc = check_err(s);
@@ -744,7 +813,8 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
     for (int q = 0; q < T.ncol; ++q) counts[q] += (long long)hc[q];
   if (tg) {
     tg->missed += (long long)hs[0];
-    tg->lost_claims += (long long)hs[1];
+    tg->lost_claims += (long long)left_over;
+    tg->replayed += (long long)hs[2];
   }
   return rc;
 }

@@ -383,14 +383,10 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
     int cx = ax, cy = ay, cz = az;
     bool lost = false;
     if (sx | syi | szi) {
-      // a new cell: periodic wrap and the loss test (the cell a particle
-      // stays in passed the test when the particle entered it)
-      if (c.flag_pbc == 1) {
-        if (ay > n2) ay -= n2;
-        if (ay < 1) ay += n2;
-        if (az > n3) az -= n3;
-        if (az < 1) az += n3;
-      }
+      // a new cell: the loss test on the clamped cell before any periodic
+      // wrap, as Src/part_expmover.f90:250-275 (the cell a particle stays in
+      // passed the test when the particle entered it), then the wrap of the
+      // particles that stay (:460-465)
       cx = ax < 0 ? 0 : (ax > n1 + 1 ? n1 + 1 : ax);
       cy = ay < 0 ? 0 : (ay > n2 + 1 ? n2 + 1 : ay);
       cz = az < 0 ? 0 : (az > n3 + 1 ? n3 + 1 : az);
@@ -410,7 +406,17 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
         }
         vx = -vx;
       }
-      lost = wall || ax < 1 || ax > n1 || ay < 1 || ay > n2 || az < 1 || az > n3;
+      lost = wall || ax < 1 || ax > n1;
+      if (c.flag_pbc == 1) {
+        if (!lost) {
+          if (ay > n2) ay -= n2;
+          if (ay < 1) ay += n2;
+          if (az > n3) az -= n3;
+          if (az < 1) az += n3;
+        }
+      } else {
+        lost = lost || ay < 1 || ay > n2 || az < 1 || az > n3;
+      }
     }
     if (lost) {
       // lost at a wall (Src/part_expmover.f90:275-433): every cell outside
@@ -423,8 +429,15 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
         atomicAdd(&acc[2 + 2 * igrid], 1.0);
         atomicAdd(&acc[3 + 2 * igrid], Eki);
         if (DIE) {
+          // periodic planes: z wraps for the wall charge, y does not
+          // (Src/part_expmover.f90:306-316)
+          int aw = az, cw_z = cz;
+          if (c.flag_pbc == 1 && (az > n3 || az < 1)) {
+            aw = az > n3 ? az - n3 : az + n3;
+            cw_z = aw < 0 ? 0 : (aw > n3 + 1 ? n3 + 1 : aw);
+          }
           const Dielectric die = {c.die.dtype, c.die.qxz, c.die.qyz, c.die.k3};
-          dielectric_charge_cells(die, d.N1, d.N2, igrid, ax, ay, az, fx, fy, fz, cx, cy, cz);
+          dielectric_charge_cells(die, d.N1, d.N2, igrid, ax, ay, aw, fx, fy, fz, cx, cy, cw_z);
         }
       }
       hole[k] = true;

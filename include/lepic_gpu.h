@@ -375,7 +375,9 @@ int lepic_dev_pdesolver(const lepic_grid_t *g, double *u, const double *b, int n
  * the process exits, which fits grids up to 64^3 cells; larger grids return
  * LEPIC_ERR_SCRATCH_LIMIT.  The first call on each device looks up the
  * array's device address (cudaGetSymbolAddress) and should be made before any
- * stream capture.  All calls share the array and it keeps the last call's
+ * stream capture.  Every call waits on the stream until its solve is done and
+ * reads k, ktot and res back from the device into host memory of its own
+ * stack.  All calls share the array and it keeps the last call's
  * contents (what must start at zero is cleared per call); calls that overlap
  * on the GPU, on any stream, race.  u, b and g->bcnd are the caller's device
  * buffers exactly as for lepic_dev_pdesolver; Dirichlet walls only (periodic
@@ -553,15 +555,20 @@ int lepic_dev_heat_stats_mixed(const lepic_grid_t *g, const lepic_species_mixed_
  * have moved since that sort.  The target density is the mean of np over the
  * cell's 8 nodes; nu_max uses P->np_mx of the target species (dens_red's
  * maximum, set by the caller).  A collision may change the target's
- * velocity or remove it (flag_dead of the target species).  The outputs
- * accumulate: missed, incident particles that found no target in reach (the
- * reference's err_coll); lost_claims, collisions dropped because another
- * incident particle of the same call had taken the target (the reference runs
- * its collisions one after another). */
+ * velocity or remove it (flag_dead of the target species).  The reference
+ * runs its collisions one after another; here they run concurrently in
+ * rounds, and a collision whose target another collision of the same round
+ * took is evaluated again in the next round, from its own draws, against the
+ * target as that collision left it, so every drawn collision happens.  A
+ * charged target of the incident's own species is LEPIC_ERR_UNSUPPORTED.
+ * The outputs accumulate: missed, incident particles that found no target in
+ * reach (the reference's err_coll); lost_claims, collisions still deferred
+ * after 256 rounds (not done; zero unless one target is drawn by more than
+ * 256 collisions of a call); replayed, the deferrals. */
 typedef struct {
   const double *np[LEPIC_NPART];
   const int *cell_off[LEPIC_NPART];
-  long long missed, lost_claims;
+  long long missed, lost_claims, replayed;
 } lepic_targets_t;
 int lepic_dev_collisions_targets(const lepic_grid_t *g, lepic_species_f64_t *sp, int ntype,
                                  const lepic_tables_t *T, const lepic_phys_t *P, unsigned long long seed,

@@ -12,9 +12,9 @@ and the GPU do (LEPIC_ERR_NEG_ENERGY).  The test keeps the other 56.
 
 Bars (statistical: Philox per particle against the serial ran2): over six
 calls, the collisions of every incident species and of every reaction the
-oracle sees at least 30 times within 4 sigma; the incident particles that
-find no charged target (no H- is loaded) within 4 sigma of the oracle's;
-nu_max equal (1e-12).
+oracle sees at least 30 times within 3 sigma; the incident particles that
+find no charged target (no H- is loaded) within 3 sigma of the oracle's;
+nu_max equal (1e-12); no drawn collision left undone (lost_claims 0).
 """
 import dataclasses
 import math
@@ -58,7 +58,7 @@ def _sorted_copy(st, S0):
 
 
 def _close(a, b):
-    return abs(a - b) <= 4 * math.sqrt(max(a + b, 1.0))
+    return abs(a - b) <= 3 * math.sqrt(max(a + b, 1.0))
 
 
 @pytest.mark.parametrize("precision", ["f64", "mixed"])
@@ -94,6 +94,7 @@ def test_hydrogen_chemistry_vs_oracle(precision):
         torch.cuda.synchronize()
         got += sim.counts[:ncol]
         miss_g += sim._targets.missed
+        assert sim._targets.lost_claims == 0
         np.testing.assert_allclose(sim.nu_max[:st.ntype], nu_o, rtol=1e-12, atol=0)
     ci = st.tables.col_info
     for p in range(1, st.ntype + 1):

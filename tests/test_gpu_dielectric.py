@@ -168,3 +168,38 @@ def test_dielectric_periodic_z_wrap_dropin():
     assert qo[0][0, 1:3].any()
     np.testing.assert_array_equal(qg[0], qo[0])
     np.testing.assert_array_equal(qg[1], qo[1])
+
+
+@pytest.mark.parametrize("precision", ["mixed", "f64"])
+def test_dielectric_periodic_corner_push(precision):
+    """The step loop's push with periodic y and z planes: an electron that
+    leaves through x = xmax (the X = const dielectric, label 3) while it
+    crosses y = ymax and z = zmax.  As in Src/part_expmover.f90:250-348 the
+    wall label and the y weight come from the clamped cell before any wrap
+    (row n2+1) and only z wraps (row 1): sum_q_yz node for node equal to the
+    oracle's (FP32 offsets in the mixed form: 1e-6 of the charge)."""
+    import torch
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    oracle.set_threads(1)
+    st = config.build("die16")
+    st.geom.flag_pbc = 1
+    h, L = st.h, st.geom.box
+    So = oracle.State(st, 4)
+    So.vxp[0, 0] = [L[0] - 0.1 * h[0], L[1] - 0.1 * h[1], L[2] - 0.2 * h[2],
+                    0.5 * h[0] / st.dt, 0.5 * h[1] / st.dt, 0.5 * h[2] / st.dt]
+    So.np_tot[0] = 1
+    sim = Simulation(st, cap=1024, precision=precision)
+    sim.load_from_host(So.vxp, So.np_tot)
+    sim.move_deposit()
+    torch.cuda.synchronize()
+    qo = _sums(st)
+    Ei = np.zeros(tuple(st.geom.bcnd.shape) + (3,))
+    ng1 = st.geom.ngrid + 1
+    oracle.part_mover(st, Ei, So, np.zeros((ng1, 2, st.ntype)), np.zeros((st.ntype, 4)), 1, sum_q=qo)
+    assert So.np_tot[0] == 0 and int(sim.counts_host()[0]) == 0
+    n2 = st.n[1]
+    k3 = abs(st.Nm[0] * st.charge[0])
+    assert np.abs(qo[1][0, 1:3, n2 + 1:n2 + 3, 0]).sum() > 0.99 * k3     # rows n2+1, n2+2 at z rows 1, 2
+    qyz = sim.die[2].cpu().numpy()
+    np.testing.assert_allclose(qyz[0], qo[1][0], rtol=0, atol=1e-6 * k3)
+    assert not sim.die[1].cpu().numpy().any()

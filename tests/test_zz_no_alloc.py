@@ -86,3 +86,39 @@ def test_noalloc_rejects_grid_beyond_limit():
                                            C.byref(k), C.byref(kt), C.byref(r),
                                            C.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert rc == 24   # LEPIC_ERR_SCRATCH_LIMIT, raised before any device work
+
+
+def test_noalloc_allocates_no_device_memory():
+    """The property the entry point exists for: after one call has set the
+    device up, further calls (two grid sizes, two calls each) leave the
+    device's free memory unchanged -- no cudaMalloc behind the caller's
+    back.  Every input is allocated before the first reading."""
+    import torch
+    from essaitemporaire_lepic_module_b200 import config
+    from essaitemporaire_lepic_module_b200._lib import LepicGrid, lib, phys_struct
+
+    dev = torch.device("cuda")
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    cases = []
+    for name in ("poisson32", "poisson64"):
+        st = config.build(name)
+        bc = torch.as_tensor(np.ascontiguousarray(st.geom.bcnd), dtype=torch.int32, device=dev)
+        rhs = torch.as_tensor(np.ascontiguousarray(st.rhs_blobs), dtype=torch.float64, device=dev)
+        phi = torch.as_tensor(np.ascontiguousarray(st.geom.phi), dtype=torch.float64, device=dev)
+        grid = LepicGrid()
+        for a in range(3):
+            grid.n[a] = st.n[a]
+            grid.h[a] = float(st.h[a])
+        grid.bcnd = bc.data_ptr()
+        cases.append((st, grid, phi, rhs, phys_struct(st), bc))
+    L = lib()
+    st, grid, phi, rhs, P, _ = cases[0]
+    assert _solve(L.lepic_dev_pdesolver_noalloc, grid, phi, rhs, P, st, stream)[0] == 0   # set-up call
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        for st, grid, phi, rhs, P, _ in reversed(cases):
+            phi.zero_()
+            assert _solve(L.lepic_dev_pdesolver_noalloc, grid, phi, rhs, P, st, stream)[0] == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
