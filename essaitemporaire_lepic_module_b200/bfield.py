@@ -76,9 +76,11 @@ def gaussian(bf, B0, x0, Lx, B_dir):
 
 # Franzen et al., Plasma Phys. Control. Fusion 56 (2014) 025007, Fig. 5: the
 # filter-field profile of the ELISE source in G against x in cm, a quartic up
-# to 39 cm and a straight line beyond (the fit of Src/Bfield.f90:83-92)
-_PG_QUARTIC = (0.0175596, 0.0227362, 0.00193113, -8.51235e-05, 9.58673e-07)
-_PG_LINE = (15.7416, -0.377132)
+# to 39 cm and a straight line beyond (the fit of Src/Bfield.f90:83-92).  The
+# reference writes the coefficients as default-real (single precision)
+# literals, so its doubles hold their float32 roundings; so do these.
+_PG_QUARTIC = tuple(float(np.float32(v)) for v in (0.0175596, 0.0227362, 0.00193113, -8.51235e-05, 9.58673e-07))
+_PG_LINE = tuple(float(np.float32(v)) for v in (15.7416, -0.377132))
 
 
 def pg_current(bf, B0, B_dir):

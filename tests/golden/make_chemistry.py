@@ -9,7 +9,7 @@ threshold, scaled E / sigma table).  The tests rebuild a Chemistry from it
 with reactions.chemistry_from_arrays, so they need no reference tree.
 
 Run here (the reference tree is read only):
-    python tests/golden/make_chemistry.py [/path/to/reference]
+    python tests/golden/make_chemistry.py /path/to/reference   (or LEPIC_REFERENCE=...)
 """
 import os
 import sys
@@ -42,4 +42,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LEPIC_REFERENCE")
+    if not ref:
+        sys.exit("usage: python tests/golden/make_chemistry.py <reference tree> (or set LEPIC_REFERENCE)")
+    main(ref)

@@ -14,7 +14,7 @@ Src/write_data.f90:322-430) and stores them in ref_default_planes.npz:
   E-field stencil (Src/Efield.f90) to the printed precision (6 digits).
 
 Run here (the reference tree is read only):
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference   (or LEPIC_REFERENCE=...)
 """
 import os
 import sys
@@ -69,4 +69,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LEPIC_REFERENCE")
+    if not ref:
+        sys.exit("usage: python tests/golden/make_golden.py <reference tree> (or set LEPIC_REFERENCE)")
+    main(ref)

@@ -151,10 +151,16 @@ def test_map_builders():
     pg.h_B[:] = 0.39 / 10.0
     bfield.pg_current(pg, 1.0, 1)
     x = 39.0
-    quart = 0.0175596 + 0.0227362 * x + 0.00193113 * x ** 2 - 8.51235e-05 * x ** 3 + 9.58673e-07 * x ** 4
-    assert pg.Bi[0, 0, 11, 0] == pytest.approx(quart, rel=1e-12)
-    assert pg.Bi[0, 0, 12, 0] == pytest.approx(15.7416 - 0.377132 * 42.9, rel=1e-12)
-    assert abs(quart - (15.7416 - 0.377132 * x)) < 0.05      # nearly continuous at 39 cm
+    # Src/Bfield.f90:85-92 writes the coefficients as single-precision
+    # literals: the doubles of the fit are their float32 roundings
+    a = [float(np.float32(v)) for v in (0.0175596, 0.0227362, 0.00193113, -8.51235e-05, 9.58673e-07)]
+    b = [float(np.float32(v)) for v in (15.7416, -0.377132)]
+    quart = a[0] + a[1] * x + a[2] * x ** 2 + a[3] * x ** 3 + a[4] * x ** 4
+    assert pg.Bi[0, 0, 11, 0] == pytest.approx(quart, rel=1e-14)
+    assert pg.Bi[0, 0, 12, 0] == pytest.approx(b[0] + b[1] * 42.9, rel=1e-14)
+    exact = 0.0175596 + 0.0227362 * x + 0.00193113 * x ** 2 - 8.51235e-05 * x ** 3 + 9.58673e-07 * x ** 4
+    assert 1e-9 < abs(quart - exact) / exact < 1e-6           # the single-precision rounding shows
+    assert abs(quart - (b[0] + b[1] * x)) < 0.05               # nearly continuous at 39 cm
 
 
 def test_read_map_file(tmp_path):
