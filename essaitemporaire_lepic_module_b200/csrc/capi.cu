@@ -712,14 +712,13 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
                  signed char *flag_dead, int *flag_cex, const int *nproc, int *np_tot, int *iseed,
                  const int *nproc_mpi, const int *mpi_rank, double *ss2D_xy, double *ss2D_xz,
                  double *ss2D_yz, const int *flag_diag) {
-  (void)P_loss;
-  (void)sour_xy;
-  (void)sour_xz;
   (void)flag_cex;
   (void)mpi_rank;
   (void)ss2D_xy;
   (void)ss2D_xz;
   (void)ss2D_yz;
+  // flag_diag = 1 turns the routine into a diagnostic pass over every
+  // particle (the source maps ss2D_*, no collision): not built here
   if (*nproc != 1 || *nproc_mpi != 1 || *flag_diag != 0) return record(LEPIC_ERR_UNSUPPORTED);
   const int nt = *ntype;
   if (nt < 1 || nt > LEPIC_NPART) return record(LEPIC_ERR_ARG);
@@ -799,6 +798,21 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
       cc_h[c + (size_t)*ncol_mx * q] = cnt_col[c + (size_t)*ncol_mx * (size_t)(*nproc) * q];
   rgc.cnt_col_dev = upload("dropin_cntcol", cc_h.data(), ncc, s);
   if (!rgc.cnt_col_dev) return record(LEPIC_ERR_CUDA);
+  // P_loss(3, :, 1) and the source planes sour_xy / sour_xz of the created
+  // particles (Src/collisions.f90:862-869, 894-902, 982-990)
+  const size_t nsxy = (size_t)(n[0] + 3) * (n[1] + 3) * nt, nsxz = (size_t)(n[0] + 3) * (n[2] + 3) * nt;
+  rgc.ploss3_dev = (double *)scratch("dropin_ploss3", sizeof(double) * LEPIC_NPART);
+  if (!rgc.ploss3_dev) return record(LEPIC_ERR_CUDA);
+  rc = cuda_ok(cudaMemsetAsync(rgc.ploss3_dev, 0, sizeof(double) * LEPIC_NPART, s), "memset");
+  if (rc) return record(rc);
+  if (sour_xy && sour_xz) {
+    rgc.sour_xy_dev = dev_view("dropin_sourxy", sour_xy, nsxy, UPDATE, s, &rc);
+    if (!rgc.sour_xy_dev) return record(rc);
+    rgc.sour_xz_dev = dev_view("dropin_sourxz", sour_xz, nsxz, UPDATE, s, &rc);
+    if (!rgc.sour_xz_dev) return record(rc);
+  }
+  rgc.iz_pl = part_info_int_.iz_pl;
+  rgc.iy_pl = n[1] / 2 + 1;
   SpeciesView v[LEPIC_NPART];
   lepic_species_f64_t sp[LEPIC_NPART];
   for (int p = 0; p < nt; ++p) {
@@ -832,8 +846,7 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
   double nu_max[LEPIC_NPART] = {0};
   long long counts[64] = {0};
   unsigned long long seed = (unsigned long long)(unsigned)iseed[0];
-  rc = launch_collisions(g, sp, nt, T, P, seed, (unsigned long long)*it, nu_max, counts, s,
-                         rgc.n_rg > 0 ? &rgc : nullptr, &tg);
+  rc = launch_collisions(g, sp, nt, T, P, seed, (unsigned long long)*it, nu_max, counts, s, &rgc, &tg);
   for (int p = 0; p < nt; ++p) {
     v[p].s = sp[p];
     record(release_species(v[p], &np_tot[p], flag_dead + (long long)*nmax * p, *nmax, true, s));
@@ -845,6 +858,15 @@ void collisions_(const int *it, double *vxp, const int *n, const double *h, cons
       for (int c = 0; c < *ncol_mx; ++c)
         cnt_col[c + (size_t)*ncol_mx * (size_t)(*nproc) * q] = cc_h[c + (size_t)*ncol_mx * q];
   }
+  if (rgc.sour_xy_dev) {
+    record(host_back(sour_xy, rgc.sour_xy_dev, nsxy, s));
+    record(host_back(sour_xz, rgc.sour_xz_dev, nsxz, s));
+  }
+  double pl3[LEPIC_NPART] = {0};
+  record(mirror_d2h(pl3, rgc.ploss3_dev, sizeof(pl3), s));
+  if (cudaStreamSynchronize(s) != cudaSuccess) record(LEPIC_ERR_CUDA);
+  if (P_loss)
+    for (int p = 0; p < nt; ++p) P_loss[2 + 4 * p] += pl3[p];  // P_loss(3, p, 1)
   for (int p = 0; p < nt; ++p) part_info_dp_3_.nu_max[p] = nu_max[p];
   record(rc);
 }

@@ -268,11 +268,20 @@ int exclusive_scan_i32(const int *in, int *out, long long n, cudaStream_t s);
 // Region counters of the drop-in path (Src/collisions.f90:1005-1013):
 // cnt_col(c, 1, i_rg) += 1/np_tot_rg(ptype, i_rg) for the first region that
 // contains the incident particle's cell.
+// The same path's per-collision bookkeeping (Src/collisions.f90:862-869,
+// 894-902, 982-990): ploss3_dev (device double[LEPIC_NPART]) += the kinetic
+// energy change of every particle a collision sets, P_loss(3, btype);
+// sour_xy_dev / sour_xz_dev (device int planes (0:n1+2, 0:n2+2, ntype) /
+// (0:n1+2, 0:n3+2, ntype)) += 1 per particle created in the incident's cell
+// when its iz is iz_pl / its iy is iy_pl.  nullptr: not kept.
 struct RegionCount {
   double *cnt_col_dev;          // device (ncol_mx, n_rg) slice for iproc = 1
   int n_rg, ncol_mx;
   int ixl[LEPIC_NM_RG], ixr[LEPIC_NM_RG], iyl, iyr, izl, izr;
   double w[LEPIC_NPART][LEPIC_NM_RG];
+  double *ploss3_dev;
+  int *sour_xy_dev, *sour_xz_dev;
+  int iz_pl, iy_pl;
 };
 // tg: charged-target (DSMC) inputs and outputs, nullptr when the tables have none
 int launch_collisions(const lepic_grid_t &g, lepic_species_f64_t *sp, int ntype,

@@ -86,6 +86,11 @@ struct MCCConst {
   int ixl[LEPIC_NM_RG], ixr[LEPIC_NM_RG], iyl, iyr, izl, izr;
   double w_rg[LEPIC_NM_RG];     // 1 / np_tot_rg(ptype, i_rg)
   double h0, h1, h2;
+  // energy and source bookkeeping of the drop-in path (RegionCount)
+  double *ploss3;
+  int *sxy, *sxz;
+  int iz_pl, iy_pl, n1, n2, n3;
+  double Nm[LEPIC_NPART];
 };
 
 // FP64 SoA layout
@@ -483,14 +488,30 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
         const int rt = c.R[sel].rt;
         const int T = c.R[sel].tt - 1;
         const double mu_t = ts.mu, vr_t = ts.vr, vxc = ts.vxc, vyc = ts.vyc, vzc = ts.vzc;
+        // P_loss(3, B) += the kinetic energy change of a particle of species
+        // B set to (nx, ny, nz) from a speed squared of o2 (0: created)
+        auto energy = [&](int B, double nx, double ny, double nz, double o2) {
+          if (c.ploss3)
+            atomicAdd(&c.ploss3[B], 0.5 * c.Nm[B] * c.mass[B] * (nx * nx + ny * ny + nz * nz - o2));
+        };
+        auto speed2 = [&](int B, long long k) {
+          double ox, oy, oz;
+          S.load_v(B, k, ox, oy, oz);
+          return ox * ox + oy * oy + oz * oz;
+        };
         if (rt == 4) {
           // charge exchange (Src/collisions.f90:948-998): the incident takes
           // the target's velocity, a charged target the incident's
           for (int a = 0; a < c.R[sel].n_by; ++a) {
             const int bt = c.R[sel].by[a];
             if (c.mass[bt - 1] <= 0) continue;
-            if (bt == c.ptype) S.store_v(P, i, ts.tvx, ts.tvy, ts.tvz);
-            else if (tgt && bt - 1 == T) S.store_v(T, ts.idx, vx0, vy0, vz0);
+            if (bt == c.ptype) {
+              if (c.ploss3) energy(P, ts.tvx, ts.tvy, ts.tvz, speed2(P, i));
+              S.store_v(P, i, ts.tvx, ts.tvy, ts.tvz);
+            } else if (tgt && bt - 1 == T) {
+              if (c.ploss3) energy(T, vx0, vy0, vz0, speed2(T, ts.idx));
+              S.store_v(T, ts.idx, vx0, vy0, vz0);
+            }
           }
         } else {
           double Ee = 0.5 * mu_t * (vr_t * vr_t) - c.R[sel].Eth * c.qe;
@@ -526,17 +547,30 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
             const double nvx = vxc + vp * ex1, nvy = vyc + vp * ey1, nvz = vzc + vp * ez1;
             const bool reuse = (a == 0 && bt == c.ptype) || ((rt == 1 || rt == 3) && bt == c.ptype);
             if (reuse) {
+              if (c.ploss3) energy(P, nvx, nvy, nvz, speed2(P, i));
               S.store_v(P, i, nvx, nvy, nvz);
               incident_reused = true;
             } else if ((rt == 1 || rt == 3) && tgt && bt - 1 == T) {
               // elastic / excitation keep a charged target (Src/collisions.f90:843-851)
+              if (c.ploss3) energy(T, nvx, nvy, nvz, speed2(T, ts.idx));
               S.store_v(T, ts.idx, nvx, nvy, nvz);
             } else {
               const int B = bt - 1;
               const int slot = atomicAdd(&add[B], 1);
               const long long j = (long long)*S.count[B] + slot;
-              if (j >= S.cap[B]) raise_err(err, LEPIC_ERR_CAPACITY, B);
-              else S.append(P, i, B, j, nvx, nvy, nvz);
+              if (j >= S.cap[B]) {
+                raise_err(err, LEPIC_ERR_CAPACITY, B);
+              } else {
+                S.append(P, i, B, j, nvx, nvy, nvz);
+                energy(B, nvx, nvy, nvz, 0.0);
+                if (c.sxy) {
+                  // the new particle's source count on the two plot planes
+                  int sx, sy, sz;
+                  S.cell_of(c, P, i, sx, sy, sz);
+                  if (sz == c.iz_pl) atomicAdd(&c.sxy[sx + (c.n1 + 3) * (sy + (long long)(c.n2 + 3) * B)], 1);
+                  if (sy == c.iy_pl) atomicAdd(&c.sxz[sx + (c.n1 + 3) * (sz + (long long)(c.n3 + 3) * B)], 1);
+                }
+              }
             }
           }
           if (!incident_reused && flag_dead) flag_dead[i] = 1;
@@ -726,6 +760,17 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
       c.izr = rg->izr;
       cc = rg->cnt_col_dev;
     }
+    if (rg) {
+      c.ploss3 = rg->ploss3_dev;
+      c.sxy = rg->sour_xy_dev;
+      c.sxz = rg->sour_xz_dev;
+      c.iz_pl = rg->iz_pl;
+      c.iy_pl = rg->iy_pl;
+      for (int q = 0; q < LEPIC_NPART; ++q) c.Nm[q] = P.Nm[q];
+    }
+    c.n1 = g.n[0];
+    c.n2 = g.n[1];
+    c.n3 = g.n[2];
     // the reaction table of this species, in device memory
     char rn[32];
     snprintf(rn, sizeof rn, "mcc_reac%d", p - 1);

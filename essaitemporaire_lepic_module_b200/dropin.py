@@ -73,6 +73,7 @@ def set_commons(st, ncol=0, npt=0, p_ncol=None, heating=None):
     pi_.flag_pbc = st.geom.flag_pbc
     pi_.flag_nmn = st.geom.flag_nmn
     pi_.flag_die = st.geom.flag_die
+    pi_.iz_pl = st.n[2] // 2 + 1            # the XY plot plane (Src/main.f90:570)
     if p_ncol is not None:
         for i in range(len(p_ncol)):
             pi_.p_ncol[i] = int(p_ncol[i])
@@ -301,13 +302,18 @@ def part_sorting(st, vxp, np_tot, ptype):
 
 
 def collisions(st, it, vxp, np_tot, flag_dead, iseed, np_red=None, ncol_mx=65, npt_mx=1300,
-               regions=(), cnt_col=None, Plist=None):
+               regions=(), cnt_col=None, Plist=None, P_loss=None, sour=None):
     """Src/collisions.f90:1 -- in place on vxp / np_tot / flag_dead.
     regions: [(ixl, ixr)] x-ranges of the counting regions (n_rg of them)
     sharing the y/z range of the whole grid, like conditions.inp's regions.
     Charged targets (DSMC) need Plist, the per-species cell offsets of the
     last part_sorting (ntype rows of pl_max+1), and np_red, the densities:
     dens_red runs on np_red first, as in Src/main.f90:1194, to set np_mx.
+    P_loss (ntype, 4), accumulated: column 3 gains the kinetic energy change
+    of every particle the collisions set (created ones from zero).  sour:
+    (sour_xy (ntype, n2+3, n1+3), sour_xz (ntype, n3+3, n1+3)) int32,
+    accumulated: the particles created in the cells of the plot planes
+    iz = n3/2+1 and iy = n2/2+1.
     Returns the per-species nu_max written to COMMON /part_info_dp_3/."""
     T = st.tables
     ncol = T.sig.shape[0]
@@ -343,6 +349,16 @@ def collisions(st, it, vxp, np_tot, flag_dead, iseed, np_red=None, ncol_mx=65, n
         dens_red(st, np_red)
     zi = np.zeros(16, dtype=np.int32)
     zd = np.zeros(16)
+    n1, n2, n3 = st.n
+    if P_loss is None:
+        P_loss = np.zeros((st.ntype, 4))
+    assert P_loss.shape == (st.ntype, 4) and P_loss.dtype == np.float64 and P_loss.flags.c_contiguous
+    if sour is None:
+        sour = (np.zeros((st.ntype, n2 + 3, n1 + 3), dtype=np.int32),
+                np.zeros((st.ntype, n3 + 3, n1 + 3), dtype=np.int32))
+    sxy, sxz = sour
+    assert sxy.shape == (st.ntype, n2 + 3, n1 + 3) and sxz.shape == (st.ntype, n3 + 3, n1 + 3)
+    assert sxy.dtype == np.int32 and sxz.dtype == np.int32 and sxy.flags.c_contiguous and sxz.flags.c_contiguous
     if Plist is None:
         pl, plm = np.zeros(1, dtype=np.int32), 0
     else:
@@ -350,7 +366,7 @@ def collisions(st, it, vxp, np_tot, flag_dead, iseed, np_red=None, ncol_mx=65, n
         plm = pl.shape[1] - 1
     lib().collisions_(_i(it), _pd(vxp), _pi(n), _pd(h), _i(st.ntype), _i(vxp.shape[1]), _pd(sig),
                       _pd(sig_Er), _pi(sig_list), _pd(sig_Eex), _i(ncol_mx), _i(npt_mx), _pd(cnt_col),
-                      _pd(zd), _pi(zi), _pi(zi), _pi(pl), _i(plm), _pd(sigv), _pi(col_info), _pd(np_red),
+                      _pd(P_loss), _pi(sxy), _pi(sxz), _pi(pl), _i(plm), _pd(sigv), _pi(col_info), _pd(np_red),
                       flag_dead.ctypes.data_as(_lib.P_i8), _pi(zi), _i(1), _pi(np_tot), _pi(iseed),
                       _i(1), _i(0), _pd(zd), _pd(zd), _pd(zd), _i(0))
     check(lib().lepic_gpu_last_error(), "collisions")
@@ -431,6 +447,8 @@ class MainLoop:
         self.iseed = np.array([iseed], dtype=np.int32)
         self.zi = np.zeros(16, dtype=np.int32)
         self.zd = np.zeros(16)
+        self.sour_xy = np.zeros((st.ntype, N2, N1), dtype=np.int32)   # sour_xy(0:n1+2, 0:n2+2, ntype, 1)
+        self.sour_xz = np.zeros((st.ntype, N3, N1), dtype=np.int32)   # sour_xz(0:n1+2, 0:n3+2, ntype, 1)
         self.collide = bool(collide) and st.tables is not None
         self.regions = list(regions)  # [(ixl, ixr)]: MCC region counters in cnt_col
         self.ncol = self.npt = 0
@@ -495,8 +513,8 @@ class MainLoop:
             check(L.lepic_gpu_last_error(), "dens_red")
             L.collisions_(_i(it), _pd(self.vxp), _pi(self.n), _pd(self.h), _i(nt), _i(nmax), _pd(self.sig),
                           _pd(self.sig_Er), _pi(self.sig_list), _pd(self.sig_Eex), _i(self.ncol_mx),
-                          _i(self.npt_mx), _pd(self.cnt_col), _pd(self.zd), _pi(self.zi), _pi(self.zi),
-                          _pi(self.Plist), _i(self.pl_max), _pd(self.sigv), _pi(self.col_info),
+                          _i(self.npt_mx), _pd(self.cnt_col), _pd(self.P_loss), _pi(self.sour_xy),
+                          _pi(self.sour_xz), _pi(self.Plist), _i(self.pl_max), _pd(self.sigv), _pi(self.col_info),
                           _pd(self.np_red), self.flag_dead.ctypes.data_as(_lib.P_i8), _pi(self.zi), _i(1),
                           _pi(self.np_tot), _pi(self.iseed), _i(1), _i(0), _pd(self.zd), _pd(self.zd),
                           _pd(self.zd), _i(0))

@@ -1,8 +1,10 @@
-"""The collisions with the reference's hydrogen source chemistry
+"""The collisions with the reference's own chemistry files on the GPU
+against the CPU oracle, from the same seeded particles.
+
+The hydrogen source chemistry
 (input_dir/hydrogen.dat: 5 charged species, 2 neutrals, 60 reactions of the
 five types, charged targets among them; the parsed tables come from the
-fixture tests/golden/hydrogen_chem.npz) on the GPU against the CPU oracle,
-from the same seeded particles.
+fixture tests/golden/hydrogen_chem.npz).
 
 Four reactions of the file have a table that is non-zero below their
 threshold (e.g. [e]+[H2]->[e]+[H]+[H], sigma > 0 from 8.07 eV, Eth 10.5 eV);
@@ -15,6 +17,13 @@ calls, the collisions of every incident species and of every reaction the
 oracle sees at least 30 times within 3 sigma; the incident particles that
 find no charged target (no H- is loaded) within 3 sigma of the oracle's;
 nu_max equal (1e-12); no drawn collision left undone (lost_claims 0).
+
+The argon chemistry (input_dir/argon.dat, fixture tests/golden/
+argon_chem.npz): the e-Ar+ Coulomb collision (charged target: the partner is
+an ion of the electron's cell, Src/collisions.f90:336-423), e-Ar elastic,
+excitation and ionization, Ar+-Ar elastic and charge exchange, at a plasma
+density (1e18 m^-3) and gas pressure (0.5 Pa) where the Coulomb collision
+is a third of the electrons' collisions; the same bars.
 """
 import dataclasses
 import math
@@ -33,6 +42,7 @@ pytestmark = [pytest.mark.gpu,
 
 CALLS = 6
 FIX = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "hydrogen_chem.npz")
+ARFIX = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "argon_chem.npz")
 
 
 def hydrogen_setup():
@@ -61,13 +71,33 @@ def _close(a, b):
     return abs(a - b) <= 3 * math.sqrt(max(a + b, 1.0))
 
 
+def argon_setup():
+    wl = dataclasses.replace(config.workload("box32"), name="ar32", gas_pressure=0.5, Te=6.0, n0=1e18,
+                             B=(0.0, 0.0, 0.01))
+    ngas = wl.gas_pressure / (KB * wl.gas_T)
+    return config.build(wl, chem=rx.chemistry_from_arrays(np.load(ARFIX), wl.Te, ngas))
+
+
 @pytest.mark.parametrize("precision", ["f64", "mixed"])
 def test_hydrogen_chemistry_vs_oracle(precision):
+    st = hydrogen_setup()
+    assert st.ntype == 5 and st.tables.sig.shape[0] == 56
+    _chemistry_vs_oracle(st, precision, CALLS, min_total=500)
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_argon_chemistry_vs_oracle(precision):
+    st = argon_setup()
+    assert st.ntype == 2 and st.tables.sig.shape[0] == 6
+    got, want = _chemistry_vs_oracle(st, precision, 8, min_total=20000)
+    assert want[0] > 5000 and got[0] > 5000          # the Coulomb collisions with ions
+    assert want[5] >= 30                             # Ar+ charge exchange seen
+
+
+def _chemistry_vs_oracle(st, precision, calls, min_total):
     import torch
     from essaitemporaire_lepic_module_b200.sim import Simulation
     oracle.set_threads(4)
-    st = hydrogen_setup()
-    assert st.ntype == 5 and st.tables.sig.shape[0] == 56
     nmax = int(st.n_particles() * 1.5)
     S0 = oracle.load_part(st, nmax=nmax)
     ncol = st.tables.sig.shape[0]
@@ -75,7 +105,7 @@ def test_hydrogen_chemistry_vs_oracle(precision):
     miss_o = 0
     seed = S0.iseed.copy()
     nu_o = None
-    for _ in range(CALLS):
+    for _ in range(calls):
         S = _sorted_copy(st, S0)
         S.iseed = seed
         err = np.zeros(st.ntype, dtype=np.int64)
@@ -85,7 +115,7 @@ def test_hydrogen_chemistry_vs_oracle(precision):
         miss_o += int(err.sum())
     got = np.zeros(ncol, dtype=np.int64)
     miss_g = 0
-    for call in range(CALLS):
+    for call in range(calls):
         sim = Simulation(st, cap=nmax, precision=precision, seed=500 + call)
         sim.load_from_host(S0.vxp, S0.np_tot, S0.np)
         sim.sort()
@@ -103,5 +133,57 @@ def test_hydrogen_chemistry_vs_oracle(precision):
     for c in range(ncol):
         if want[c] >= 30:
             assert _close(got[c], want[c]), (c, st.tables and got[c], want[c])
-    assert want.sum() > 500
+    assert want.sum() > min_total
     assert _close(miss_g, miss_o), (miss_g, miss_o)
+    return got, want
+
+
+def test_collisions_dropin_energy_and_sources():
+    """collisions_ (the drop-in) keeps the reference's per-collision
+    bookkeeping (Src/collisions.f90:862-869, 894-902, 982-990): P_loss(3, p)
+    gains the kinetic energy change of every particle of species p that a
+    collision sets (a created one from zero), and sour_xy / sour_xz count the
+    particles created in the cells of the plot planes iz = n3/2+1 and
+    iy = n2/2+1.  Checked on the argon chemistry (ionization creates
+    electrons and ions; Coulomb collisions change ions) against the particle
+    arrays themselves, over four calls from the same particles: energies to
+    1e-9 of the species' total, counts exact."""
+    from essaitemporaire_lepic_module_b200 import dropin
+    oracle.set_threads(4)
+    st = argon_setup()
+    T = st.tables
+    nmax = int(st.n_particles() * 1.5)
+    S0 = oracle.load_part(st, nmax=nmax)
+    dropin.set_commons(st, ncol=T.sig.shape[0], npt=T.sig_Er.shape[0], p_ncol=T.p_ncol)
+    n1, n2, n3 = st.n
+    h = st.h
+    seen = np.zeros((st.ntype, 3), dtype=np.int64)
+    for call in range(4):
+        S = S0.copy()
+        pls = [dropin.part_sorting(st, S.vxp, S.np_tot, p) for p in range(1, st.ntype + 1)]
+        n0 = S.np_tot.copy()
+        v0 = [S.vxp[p, :n0[p], 3:6].copy() for p in range(st.ntype)]
+        PL = np.zeros((st.ntype, 4))
+        sxy = np.zeros((st.ntype, n2 + 3, n1 + 3), dtype=np.int32)
+        sxz = np.zeros((st.ntype, n3 + 3, n1 + 3), dtype=np.int32)
+        dropin.collisions(st, 11, S.vxp, S.np_tot, S.flag_dead, np.array([4321 + 7 * call], dtype=np.int32),
+                          np_red=S.np, Plist=pls, P_loss=PL, sour=(sxy, sxz))
+        for p in range(st.ntype):
+            k = 0.5 * st.Nm[p] * st.mass[p]
+            kept, new = S.vxp[p, :n0[p], 3:6], S.vxp[p, n0[p]:S.np_tot[p], 3:6]
+            dE = k * ((kept ** 2).sum() - (v0[p] ** 2).sum() + (new ** 2).sum())
+            assert abs(PL[p, 2] - dE) <= 1e-9 * k * (kept ** 2).sum(), (p, PL[p, 2], dE)
+            assert not PL[p, [0, 1, 3]].any()
+            x = S.vxp[p, n0[p]:S.np_tot[p], 0:3]
+            ix, iy, iz = ((x[:, a] / h[a]).astype(np.int64) + 1 for a in range(3))
+            want_xy = np.zeros_like(sxy[p])
+            want_xz = np.zeros_like(sxz[p])
+            m = iz == n3 // 2 + 1
+            np.add.at(want_xy, (iy[m], ix[m]), 1)
+            m = iy == n2 // 2 + 1
+            np.add.at(want_xz, (iz[m], ix[m]), 1)
+            np.testing.assert_array_equal(sxy[p], want_xy)
+            np.testing.assert_array_equal(sxz[p], want_xz)
+            seen[p] += [len(new), want_xy.sum(), int(np.any(kept != v0[p], axis=1).sum())]
+    assert np.all(seen[:, 0] > 40) and np.all(seen[:, 1] > 0), seen   # ionization products, some in the plane
+    assert np.all(seen[:, 2] > 100), seen                               # electrons and ions changed

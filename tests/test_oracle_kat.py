@@ -5,6 +5,8 @@ Each test states the analytic or independent answer it checks against.
 """
 import math
 
+import os
+
 import numpy as np
 import pytest
 
@@ -219,6 +221,29 @@ def test_ordering_python_matches_c():
     np.testing.assert_allclose(T.sigv_mx, sv, rtol=1e-15, atol=0)
     np.testing.assert_array_equal(T.sig_list, sl)
     np.testing.assert_array_equal(T.p_ncol, pn)
+
+
+def test_ordering_of_the_reference_argon_file():
+    """The reference's own input_dir/argon.dat (fixture tests/golden/
+    argon_chem.npz: e, Ar+, Ar; the e-Ar+ Coulomb collision with a charged
+    target, e-Ar elastic, excitation and ionization, Ar+-Ar elastic and
+    charge exchange): the host and oracle restatements of ordering() agree,
+    and the parsed reactions are the file's."""
+    from essaitemporaire_lepic_module_b200.constants import KB
+    path = os.path.join(os.path.dirname(__file__), "golden", "argon_chem.npz")
+    chem = reactions.chemistry_from_arrays(np.load(path), 6.0, 0.5 / (KB * 300.0))
+    assert [s.name for s in chem.species] == ["[e]", "[Ar+]", "[Ar]"]
+    assert chem.labels[0] == "[e]+[Ar+]->[e]+[Ar+]" and chem.col_info[0, 3] == 2   # charged target
+    assert [int(r[2 + r[0] + r[1]]) for r in chem.col_info] == [1, 1, 3, 2, 1, 4]   # reaction types
+    np.testing.assert_array_equal(chem.Eth, [0.0, 0.0, 11.5, 15.8, 0.0, 0.0])
+    T = reactions.ordering(chem)
+    Er, sig, sv, sl, pn = oracle.ordering(chem)
+    np.testing.assert_array_equal(T.sig_Er, Er)
+    np.testing.assert_array_equal(T.sig, sig)
+    np.testing.assert_allclose(T.sigv_mx, sv, rtol=1e-15, atol=0)
+    np.testing.assert_array_equal(T.sig_list, sl)
+    np.testing.assert_array_equal(T.p_ncol, pn)
+    assert list(pn[:2]) == [4, 2]
 
 
 def _periodic_profile(n, m):
