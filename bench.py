@@ -30,6 +30,11 @@ cpu_baseline: the FP64 CPU oracle (the reference restated in C++) on the
 poisson: the Poisson stress configuration (256^3, two electrodes at +-100 V, 64
         Gaussian blobs): cold and warm solve times of the FP64 multigrid and of
         the mixed solve, and phi of the mixed solve against the FP64 one.
+large:  the large mixed-precision configuration (192^3 cells, e- + Ar+ at 128
+        ppc = 2 x 9.06e8 FP32 particles, the MCC of the 128^3 workload; the
+        FP64 form does not fit in HBM): after 3 warm-up steps, 500 steps timed
+        with CUDA events as one region (50 electron sorts and 50 MCC calls),
+        with its roofline, clocks and phi error against the FP64 multigrid.
 adjoint: forward and backward time of the differentiable K-step window on the
         Penning workload (96x96x192, 5.7e7 electrons, K = 64, checkpoints every
         8 steps): gradient of the final mean electron energy with respect to the
@@ -200,16 +205,21 @@ def _timed_steps(sim, steps, world, dist, torch):
         dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    nps = 0
+    # the particles each step pushes (the counts before it), summed on the
+    # device: no host read of the counts inside the timed region
+    acc = torch.zeros(1, dtype=torch.int64, device="cuda")
+    counts = [s.count for s in sim.sp]
     vcycles = []
     e0.record()
     for _ in range(steps):
-        nps += int(sum(s.n() for s in sim.sp))
+        for c in counts:
+            acc += c
         sim.step()
         vcycles.append(sim.mg_last[0])
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    nps = int(acc.item())
     if world > 1:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -442,6 +452,33 @@ def run_adjoint(workload, K, every):
     return out
 
 
+def run_large(args):
+    """The large mixed-precision configuration: `--large-steps` steps of the
+    mixed form timed as one region after 3 warm-up steps."""
+    import torch
+    from essaitemporaire_lepic_module_b200 import config
+    st = config.build(args.large_workload)
+    a = argparse.Namespace(**vars(args))
+    a.warmup, a.steps = 3, args.large_steps
+    R = _run_form(a, st, "mixed", 0, 1, None, torch, e2e=False)
+    perr = _phi_err(R["sim"], st, torch)
+    timers = R["timers"]
+    out = {"workload": f"{args.large_workload} {list(st.n)} cells, {st.ntype} species x {st.n_particles()} "
+                       f"FP32 particles, MCC every {st.wl.ns_coll} steps, 3 warm-up + {a.steps} timed steps",
+           "value": R["value"], "unit": UNIT, "steps": a.steps, "ms_per_step": R["ms"] / a.steps,
+           "particles_at_start": R["n_start"],
+           "particles_at_end": int(R["sim"].counts_host().sum()),
+           "phi_err_vs_f64": perr["mixed"], "phi_err_detail": perr,
+           "poisson_iters_per_solve": float(np.mean(R["iters"])) if R["iters"] else None,
+           "roofline": _roofline(timers, "push_deposit_mixed", 57.0, R["nps"]),
+           "kernel_ms": {k: round(v[0], 3) for k, v in sorted(timers.items())},
+           "kernel_launches": {k: v[1] for k, v in sorted(timers.items())},
+           "clocks": R["clocks"]}
+    del R
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_dropin(workload, steps=4, warm=1):
     """The reference-facing path: Src/main.f90's timestep as calls to the
     Fortran-signature entry points over host arrays in the reference layouts
@@ -590,6 +627,8 @@ def run_ours(args):
     del res
     R = None
     torch.cuda.empty_cache()
+    if args.large and world == 1:
+        line["large"] = run_large(args)
     if args.poisson:
         line["poisson"] = run_poisson(args.poisson_workload)
     if args.adjoint:
@@ -627,6 +666,10 @@ def main():
     ap.add_argument("--e2e-all", action="store_true", help="also measure e2e for the FP64 form")
     ap.add_argument("--cap-factor", type=float, default=None,
                     help="particle capacity per species / particles loaded (default 1.25)")
+    ap.add_argument("--no-large", dest="large", action="store_false",
+                    help="skip the large mixed-precision configuration (192^3, 2 x 9.06e8 particles)")
+    ap.add_argument("--large-workload", default="mcc192")
+    ap.add_argument("--large-steps", type=int, default=500)
     ap.add_argument("--no-poisson", dest="poisson", action="store_false",
                     help="skip the Poisson stress measurement")
     ap.add_argument("--poisson-workload", default="poisson256")
