@@ -10,17 +10,38 @@
 // Src/mg.f90 27-point full-weighting restriction and trilinear
 // prolongation), evaluated in FP32 on the correction; only the residual and
 // the accumulation of u are FP64, so u converges to the FP64 solution while
-// the V-cycle moves half the bytes.  The level masks are injected from the
-// finest mask once per call.
+// the V-cycle moves half the bytes.
 //
-// The fine levels are swept by the whole grid (warps take grid rows, lanes
-// split a row, grid-wide barriers between phases).  The coarse levels, from
-// the first one whose arrays fit in shared memory down to the coarsest, live
-// in block 0's shared memory for the whole call: each V-cycle block 0 loads
-// the restricted right-hand side of the top coarse level, runs the coarse
-// part of the cycle on chip with block barriers only, and stores the
-// correction back for the grid to prolongate.
+// Wall nodes are marked in the FP32 right-hand side itself: r = +inf on a
+// wall or ghost node (never updated; its correction stays 0), so the FP32
+// levels carry no mask arrays.  The coarse masks are the reference's
+// injection (Src/mg.f90:429-436): a coarse node is a wall when the fine node
+// it sits on is one.
+//
+// Grid levels (those too large for one SM's shared memory) are processed in
+// 3D tiles of 32 x 8 x 8 nodes staged in shared memory by the tensor memory
+// accelerator: per tile a block loads the boxes of e and r covering the tile
+// and two halo layers with cp.async.bulk.tensor (double-buffered: the next
+// tile's copy is in flight while the current one is computed, completion on
+// an mbarrier), and works on chip:
+//   sweep      red nodes of tile + 1 halo layer, then black nodes of the tile
+//              (a full red-black sweep per grid phase; the halo's red values
+//              are computed redundantly by the neighbouring tiles);
+//   restrict   the fine residual on tile + 1 halo layer, then the 27-point
+//              weighting onto the coarse nodes whose fine twin lies in the
+//              tile (one grid phase instead of two);
+//   prolong    the coarse correction's box is staged as well and added before
+//              the first post-sweep of the level, in the same phase.
+// The last post-sweep of level 1 also adds the correction to u (FP64).  The
+// coarse levels, from the first one whose arrays fit in shared memory down
+// to the coarsest, run in block 0 alone for each V-cycle, with block
+// barriers only, in the same shared memory.
+//
+// Every wait on a tile copy is bounded (one second); a copy that never
+// completes sets LEPIC_ERR_TIMEOUT in the device error word, the block stops
+// issuing copies and computing, and still meets every grid barrier.
 #include <cooperative_groups.h>
+#include <cuda.h>
 
 #include <cstring>
 
@@ -32,40 +53,76 @@ namespace lepic {
 
 namespace {
 
-constexpr int XM_MAX = 13;
+constexpr int XM_MAX = 13;      // multigrid levels
+constexpr int GMAX = 6;         // levels in global memory (tiled)
 constexpr int XM_BLOCK = 512;
-constexpr size_t XM_SMEM_BUDGET = 160 * 1024;  // coarse levels in block 0's shared memory
+constexpr size_t XM_SMEM_COARSE = 160 * 1024;   // budget of the on-chip coarse levels
 
-struct XLev {
+// tile of updated nodes; the last tile of a row takes the remainder, up to
+// T + 1 nodes (the node n + 1)
+constexpr int TX = 32, TY = 8, TZ = 8;
+// staged boxes: the fine box is the tile with two halo layers on each side
+// (one more for a last tile), the coarse box covers what the fine box's
+// nodes interpolate from
+constexpr int BX = TX + 8, BY = TY + 5, BZ = TZ + 5;
+constexpr int CBX = TX / 2 + 4, CBY = TY / 2 + 4, CBZ = TZ / 2 + 4;
+constexpr int BXY = BX * BY;
+constexpr unsigned BOX_BYTES = BX * BY * BZ * 4u;
+constexpr unsigned CBOX_BYTES = CBX * CBY * CBZ * 4u;
+constexpr unsigned BOX_STRIDE = (BOX_BYTES + 127u) / 128u * 128u;
+constexpr unsigned CBOX_STRIDE = (CBOX_BYTES + 127u) / 128u * 128u;
+constexpr unsigned STAGE_BYTES = 2 * BOX_STRIDE + CBOX_STRIDE;  // e box, r box, coarse e box
+constexpr unsigned TILE_SMEM = 2 * STAGE_BYTES + BOX_STRIDE;     // two stages + the residual box
+
+// A level in global memory: FP32 e and r over nodes 0..n+2 per axis, node
+// (i, j, k) at column i + 1 of a row padded to a multiple of 4 floats (so
+// that every tile box starts on a 16-byte boundary, x = 32 t).
+struct GLev {
   int n1, n2, n3;
-  int N1, N2;          // n+3
-  int R1, R2;          // n+2
-  float aw, ae, an, as, at, ab, ac;
-  float *e;            // (n+3)^3 correction
-  float *r;            // (n+2)^3 right-hand side
-  float *rf;           // (n+3)^3 residual scratch
-  int *bc;             // (n+3)^3 mask (level 1: caller's bcnd)
-  __device__ long long g(int i, int j, int k) const { return i + (long long)N1 * (j + (long long)N2 * k); }
-  __device__ long long rr(int i, int j, int k) const { return i + (long long)R1 * (j + (long long)R2 * k); }
-  __host__ __device__ long long nn() const { return (long long)N1 * N2 * (n3 + 3); }
-  __host__ __device__ long long nr() const { return (long long)R1 * R2 * (n3 + 2); }
+  int P1;              // row pitch, floats
+  int ntx, nty, ntz;   // tiles per axis
+  float aw, an, at, ac;
+  float *e, *r;
+  __host__ __device__ long long g(int i, int j, int k) const {
+    return (long long)(i + 1) + (long long)P1 * (j + (long long)(n2 + 3) * k);
+  }
+  __host__ __device__ long long nn() const { return (long long)P1 * (n2 + 3) * (n3 + 3); }
+};
+
+// A coarse level in block 0's shared memory: nodes 0..n+2, x fastest.
+struct SLev {
+  int n1, n2, n3;
+  int N1, N2;          // n + 3
+  float aw, an, at, ac;
+  float *e, *r, *rf;
+  __device__ int g(int i, int j, int k) const { return i + N1 * (j + N2 * k); }
 };
 
 struct XArgs {
-  XLev L[XM_MAX + 1];
+  GLev G[GMAX + 2];    // levels 1..min(ls + 1, ng): the grid levels and the exchange level
+  SLev S[XM_MAX + 1];  // levels ls + 1..ng on chip (pointers are shared-memory offsets, set per block)
+  unsigned so_e[XM_MAX + 1], so_r[XM_MAX + 1], so_rf[XM_MAX + 1];
   int ng, ls;          // levels 1..ls on the grid, ls+1..ng in shared memory
-  int max_refine, nu_fine_pre, nu_fine_post, nu_pre, nu_post, coarse_sweeps;  // sweeps: finest level, the others
+  int max_refine, nu_fine_pre, nu_fine_post, nu_pre, nu_post, coarse_sweeps;
   float omega;
-  double aw, ae, an, as, at, ab, ac;  // FP64 finest coefficients
+  double aw, an, at, ac;  // FP64 finest coefficients (ae = aw, as = an, ab = at)
   double *u;
   const double *b;
+  const int *bcnd;
   double alpha, eps;
   double *partial;
   int *out_i;      // [0] refinement iterations, [1] status
   double *out_d;   // [0] res/alpha, [1] first res/alpha
-  // shared-memory offsets (bytes) of e, r, rf, bc of the coarse levels
-  unsigned so_e[XM_MAX + 1], so_r[XM_MAX + 1], so_rf[XM_MAX + 1], so_bc[XM_MAX + 1];
+  int *err;        // device error word
 };
+
+// tensor maps of the tile boxes (a __grid_constant__ kernel parameter)
+struct XMaps {
+  CUtensorMap fe[GMAX + 1], fr[GMAX + 1];  // fine boxes of e and r, levels 1..ls
+  CUtensorMap ce[GMAX + 2];                // coarse boxes of e, levels 2..ls + 1
+};
+
+__device__ __forceinline__ bool wall(float r) { return isinf(r); }
 
 __device__ __forceinline__ double wsum(double v) {
 #pragma unroll
@@ -108,310 +165,268 @@ __device__ double grid_sum(const XArgs &a, double v, int parity, cg::grid_group 
   return s;
 }
 
-// red-black colour start: colour 0 = red ((i+j+k) odd), 1 = black
-// (Src/sors.f90:87-106, 249-267)
-__device__ __forceinline__ int colour_start(int colour, int j, int k) {
-  int is = (colour == 0) ? ((j % 2 == 0) ? 1 : 2) : ((j % 2 == 0) ? 2 : 1);
-  is += (k % 2 == 0) ? 0 : 1;
-  return is > 2 ? 1 : is;
+// ------------------------------------------------------------ tile copies
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long gtime() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
 }
 
-__device__ __forceinline__ void relax(const XLev &L, float omega, float rac, int i, int j, int k) {
-  const long long sy = L.N1, sz = (long long)L.N1 * L.N2;
-  const long long q = L.g(i, j, k);
-  if (L.bc[q] > 0) return;
-  const float tt = L.r[L.rr(i, j, k)] - L.aw * L.e[q - 1] - L.an * L.e[q + sy] - L.as * L.e[q - sy] -
-                   L.ae * L.e[q + 1] - L.at * L.e[q + sz] - L.ab * L.e[q - sz];
-  L.e[q] = (1.f - omega) * L.e[q] + omega * tt * rac;
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
 }
 
-__device__ __forceinline__ float fine_residual(const XLev &F, int i, int j, int k) {
-  const long long sy = F.N1, sz = (long long)F.N1 * F.N2;
-  const long long q = F.g(i, j, k);
-  if (F.bc[q] > 0) return 0.f;
-  return F.r[F.rr(i, j, k)] - (F.aw * F.e[q - 1] + F.ae * F.e[q + 1] + F.an * F.e[q + sy] +
-                               F.as * F.e[q - sy] + F.ac * F.e[q] + F.at * F.e[q + sz] + F.ab * F.e[q - sz]);
+// wait for phase `parity` of the mbarrier, at most one second
+__device__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = gtime();
+  while (!mbar_try(bar, parity))
+    if (gtime() - t0 > 1000000000ull) return false;
+  return true;
 }
 
-// 27-point full weighting of the fine residual onto coarse node (i,j,k)
-// (Src/mg.f90:248-805): loads only; 0 outside the interior and on walls
-__device__ __forceinline__ float restrict_value(const XLev &F, const XLev &C, int i, int j, int k) {
-  if (i < 1 || j < 1 || k < 1 || i > C.n1 + 1 || j > C.n2 + 1 || k > C.n3 + 1) return 0.f;
-  if (C.bc[C.g(i, j, k)] > 0) return 0.f;
-  const long long sy = F.N1, sz = (long long)F.N1 * F.N2;
-  const long long q = F.g(2 * i - 1, 2 * j - 1, 2 * k - 1);
-  const float *R = F.rf;
-  return (8.f * R[q] + 4.f * (R[q + 1] + R[q - 1] + R[q + sy] + R[q - sy] + R[q + sz] + R[q - sz]) +
-          2.f * (R[q + 1 + sy] + R[q - 1 + sy] + R[q + 1 - sy] + R[q - 1 - sy] + R[q + 1 + sz] + R[q - 1 + sz] +
-                 R[q + sy + sz] + R[q - sy + sz] + R[q + 1 - sz] + R[q - 1 - sz] + R[q + sy - sz] +
-                 R[q - sy - sz]) +
-          R[q + 1 + sy + sz] + R[q - 1 + sy + sz] + R[q + 1 - sy + sz] + R[q - 1 - sy + sz] + R[q + 1 + sy - sz] +
-          R[q - 1 + sy - sz] + R[q + 1 - sy - sz] + R[q - 1 - sy - sz]) *
+__device__ __forceinline__ void tma_box(uint32_t dst, const CUtensorMap *m, int x, int y, int z, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(m)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+
+// The double-buffered tile copies of one block.
+struct Pipe {
+  unsigned char *stage[2];
+  float *rf;              // residual box (restriction)
+  uint32_t bar[2];        // mbarriers in shared memory
+  unsigned uses[2];       // completed phases per mbarrier
+  bool fail;
+};
+
+enum { K_SWEEP = 1, K_PRO = 2, K_RESTRICT = 4, K_ADDU = 8 };
+
+struct Tile {
+  int tx, ty, tz;
+  int i0, j0, k0;   // node of box index 0 on each axis
+  int w, h, d;      // tile nodes per axis
+};
+
+__device__ __forceinline__ Tile tile_of(const GLev &L, int tau) {
+  Tile t;
+  t.tx = tau % L.ntx;
+  const int q = tau / L.ntx;
+  t.ty = q % L.nty;
+  t.tz = q / L.nty;
+  t.i0 = TX * t.tx - 1;
+  t.j0 = TY * t.ty - 1;
+  t.k0 = TZ * t.tz - 1;
+  t.w = t.tx == L.ntx - 1 ? L.n1 + 1 - TX * t.tx : TX;
+  t.h = t.ty == L.nty - 1 ? L.n2 + 1 - TY * t.ty : TY;
+  t.d = t.tz == L.ntz - 1 ? L.n3 + 1 - TZ * t.tz : TZ;
+  return t;
+}
+
+// thread 0: the copies of tile tau of level l into stage s
+__device__ void issue(const XMaps &maps, int l, int kind, const GLev &L, int tau, Pipe &pp, int s) {
+  const Tile t = tile_of(L, tau);
+  const unsigned bytes = 2 * BOX_BYTES + ((kind & K_PRO) ? CBOX_BYTES : 0u);
+  // earlier generic accesses of this stage and of the global arrays come
+  // before the asynchronous copies
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(pp.bar[s]), "r"(bytes) : "memory");
+  const uint32_t dst = smem_addr(pp.stage[s]);
+  tma_box(dst, &maps.fe[l], TX * t.tx, t.j0, t.k0, pp.bar[s]);
+  tma_box(dst + BOX_STRIDE, &maps.fr[l], TX * t.tx, t.j0, t.k0, pp.bar[s]);
+  if (kind & K_PRO)
+    tma_box(dst + 2 * BOX_STRIDE, &maps.ce[l + 1], (TX / 2) * t.tx, (TY / 2) * t.ty - 1, (TZ / 2) * t.tz - 1,
+            pp.bar[s]);
+}
+
+// red-black colour: red = (i + j + k) odd (Src/sors.f90:87-106)
+// one relaxation of box node q (Src/sors.f90 update, in FP32)
+__device__ __forceinline__ void relax_box(float *E, const float *R, int q, const GLev &L, float omega, float rac) {
+  const float rv = R[q];
+  if (wall(rv)) return;
+  const float tt = rv - L.aw * E[q - 1] - L.an * E[q + BX] - L.an * E[q - BX] - L.aw * E[q + 1] -
+                   L.at * E[q + BXY] - L.at * E[q - BXY];
+  E[q] = (1.f - omega) * E[q] + omega * tt * rac;
+}
+
+// nodes of one colour in the box region [x0, x0 + nx) x [y0, y0 + ny) x
+// [z0, z0 + nz); odd = true: (i + j + k) odd
+template <class F>
+__device__ __forceinline__ void colour_loop(const Tile &t, int x0, int nx, int y0, int ny, int z0, int nz, bool odd,
+                                            F &&body) {
+  const int hx = (nx + 1) >> 1;
+  const int tot = hx * ny * nz;
+  for (int v = threadIdx.x; v < tot; v += blockDim.x) {
+    const int row = v / hx, m = v - row * hx;
+    const int zz = row / ny, yy = row - zz * ny;
+    const int by = y0 + yy, bz = z0 + zz;
+    const int par = (t.i0 + x0 + t.j0 + by + t.k0 + bz) & 1;   // parity of the row's first node
+    const int bx = x0 + ((par == (odd ? 1 : 0)) ? 0 : 1) + 2 * m;
+    if (bx < x0 + nx) body(bx + BX * (by + BY * bz));
+  }
+}
+
+// trilinear prolongation (Src/mg.f90:849-939) of the coarse box onto fine
+// box node (bx, by, bz) = fine node (i, j, k): a fine node on a coarse node
+// takes its value, one between coarse nodes their mean
+__device__ __forceinline__ float prolong_value(const float *CE, const Tile &t, int i, int j, int k) {
+  const int ci = (i + 1) >> 1, cj = (j + 1) >> 1, ck = (k + 1) >> 1;
+  const int ex = (i & 1) ^ 1, ey = (j & 1) ^ 1, ez = (k & 1) ^ 1;
+  const int cx = ci - ((TX / 2) * t.tx - 1), cy = cj - ((TY / 2) * t.ty - 1), cz = ck - ((TZ / 2) * t.tz - 1);
+  const int c0 = cx + CBX * (cy + CBY * cz);
+  float s = 0.f;
+#pragma unroll
+  for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+      for (int dx = 0; dx < 2; ++dx)
+        if (dx <= ex && dy <= ey && dz <= ez) s += CE[c0 + dx + CBX * (dy + CBY * dz)];
+  const float wgt = (ex + ey + ez) == 0 ? 1.f : ((ex + ey + ez) == 1 ? 0.5f : ((ex + ey + ez) == 2 ? 0.25f : 0.125f));
+  return s * wgt;
+}
+
+// fine residual of box node q (0 on walls)
+__device__ __forceinline__ float box_residual(const float *E, const float *R, int q, const GLev &L) {
+  const float rv = R[q];
+  if (wall(rv)) return 0.f;
+  return rv - (L.aw * E[q - 1] + L.aw * E[q + 1] + L.an * E[q + BX] + L.an * E[q - BX] + L.ac * E[q] +
+               L.at * E[q + BXY] + L.at * E[q - BXY]);
+}
+
+// 27-point full weighting (Src/mg.f90:696-702) of the residual box around q
+__device__ __forceinline__ float weigh27(const float *F, int q) {
+  const int sy = BX, sz = BXY;
+  return (8.f * F[q] + 4.f * (F[q + 1] + F[q - 1] + F[q + sy] + F[q - sy] + F[q + sz] + F[q - sz]) +
+          2.f * (F[q + 1 + sy] + F[q - 1 + sy] + F[q + 1 - sy] + F[q - 1 - sy] + F[q + 1 + sz] + F[q - 1 + sz] +
+                 F[q + sy + sz] + F[q - sy + sz] + F[q + 1 - sz] + F[q - 1 - sz] + F[q + sy - sz] +
+                 F[q - sy - sz]) +
+          F[q + 1 + sy + sz] + F[q - 1 + sy + sz] + F[q + 1 - sy + sz] + F[q - 1 - sy + sz] + F[q + 1 + sy - sz] +
+          F[q - 1 + sy - sz] + F[q + 1 - sy - sz] + F[q - 1 - sy - sz]) *
          (1.f / 64.f);
 }
 
-// coarse node (i,j,k), i,j,k in 0..n+2: right-hand side from the fine
-// residual, correction cleared
-__device__ __forceinline__ void restrict_store(const XLev &C, int i, int j, int k, float re) {
-  C.e[C.g(i, j, k)] = 0.f;
-  if (i <= C.n1 + 1 && j <= C.n2 + 1 && k <= C.n3 + 1) C.r[C.rr(i, j, k)] = re;
-}
-
-__device__ __forceinline__ void restrict_node(const XLev &F, const XLev &C, int i, int j, int k) {
-  restrict_store(C, i, j, k, restrict_value(F, C, i, j, k));
-}
-
-// trilinear prolongation of coarse node (i,j,k) added into F
-// (Src/mg.f90:849-939): the 8 coarse values, the 8 fine masks and the 8 fine
-// values are loaded before the 8 stores
-__device__ __forceinline__ void prolong_node(const XLev &F, const XLev &C, int i, int j, int k) {
-  const long long sy = F.N1, sz = (long long)F.N1 * F.N2, cy = C.N1, cz = (long long)C.N1 * C.N2;
-  const long long c = C.g(i, j, k);
-  const float *E = C.e;
-  const float r000 = E[c], r0m0 = E[c - cy], rmm0 = E[c - 1 - cy], rm00 = E[c - 1];
-  const float r00m = E[c - cz], r0mm = E[c - cy - cz], rmmm = E[c - 1 - cy - cz], rm0m = E[c - 1 - cz];
-  const long long q = F.g(2 * i - 1, 2 * j - 1, 2 * k - 1);
-  float *U = F.e;
-  const int *B = F.bc;
-  const long long o[8] = {0, -sy, -1 - sy, -1, -sz, -sy - sz, -1 - sz, -1 - sy - sz};
-  int bm[8];
-  float uv[8];
-#pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    bm[t] = B[q + o[t]];
-    uv[t] = U[q + o[t]];
+// the work of one staged tile
+__device__ void tile_work(const XArgs &a, int l, int kind, const Tile &t, float *E, const float *R, const float *CE,
+                          float *RF) {
+  const GLev &L = a.G[l];
+  if (kind & K_PRO) {
+    // the coarse correction onto every non-wall node of the box inside the grid
+    const int tot = (t.w + 4) * (t.h + 4) * (t.d + 4);
+    for (int v = threadIdx.x; v < tot; v += blockDim.x) {
+      const int nx = t.w + 4, ny = t.h + 4;
+      const int row = v / nx, bx = v - row * nx;
+      const int bz = row / ny, by = row - bz * ny;
+      const int i = t.i0 + bx, j = t.j0 + by, k = t.k0 + bz;
+      if (i < 0 || j < 0 || k < 0 || i > L.n1 + 1 || j > L.n2 + 1 || k > L.n3 + 1) continue;
+      const int q = bx + BX * (by + BY * bz);
+      if (wall(R[q])) continue;
+      E[q] += prolong_value(CE, t, i, j, k);
+    }
+    __syncthreads();
   }
-  const float add[8] = {r000,
-                        (r000 + r0m0) * 0.5f,
-                        (r000 + r0m0 + rmm0 + rm00) * 0.25f,
-                        (r000 + rm00) * 0.5f,
-                        (r000 + r00m) * 0.5f,
-                        (r000 + r00m + r0mm + r0m0) * 0.25f,
-                        (r000 + r00m + rm0m + rm00) * 0.25f,
-                        (r000 + r00m + rm0m + rm00 + r0m0 + r0mm + rmmm + rmm0) * 0.125f};
-#pragma unroll
-  for (int t = 0; t < 8; ++t)
-    if (bm[t] <= 0) U[q + o[t]] = uv[t] + add[t];
-}
-
-__device__ __forceinline__ int fmapx(int ic, int ncell) {
-  return ic == ncell / 2 + 2 ? ncell + 2 : (ic == 0 ? 0 : 2 * ic - 1);
-}
-
-// The rows (j, k), j in [j0, j0 + nj), k in [k0, k0 + nk), dealt round-robin
-// to all warps of the grid; body(j, k) runs on all lanes, which split the row
-// along i.
-template <class F>
-__device__ __forceinline__ void grid_rows(int j0, int nj, int k0, int nk, F &&body) {
-  const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
-  const int rows = nj * nk;
-  for (int r = gw; r < rows; r += nw) {
-    const int kk = r / nj;
-    body(j0 + (r - kk * nj), k0 + kk);
+  if (kind & K_SWEEP) {
+    const float om = a.omega, rac = 1.f / L.ac;
+    // red on the tile and one halo layer, then black on the tile
+    colour_loop(t, 1, t.w + 2, 1, t.h + 2, 1, t.d + 2, true, [&](int q) { relax_box(E, R, q, L, om, rac); });
+    __syncthreads();
+    colour_loop(t, 2, t.w, 2, t.h, 2, t.d, false, [&](int q) { relax_box(E, R, q, L, om, rac); });
+    __syncthreads();
   }
-}
-
-// ------------------------------------------------------------ grid-wide
-// The grid levels are small enough to stay in L2 (a 128^3 level of FP32
-// arrays is 9 MB each), so a phase costs the latency of its dependent loads,
-// not bandwidth.  Each thread therefore takes XU slots of a flat index range
-// at once (slot t, t + nth, ...), issues every load of all XU slots before
-// the first arithmetic, then computes and stores: one round trip to L2 per
-// XU slots instead of two per node.
-constexpr int XU = 2;
-
-struct Slots {
-  int tid, nth;
-};
-__device__ __forceinline__ Slots slots() {
-  return {(int)(blockIdx.x * blockDim.x + threadIdx.x), (int)(gridDim.x * blockDim.x)};
-}
-
-// one red-black half-sweep of level L (slots: (m, j, k), i = start + 2m);
-// with u, the finest level's last half-sweep also adds the new correction of
-// its nodes to the FP64 solution
-__device__ __noinline__ void g_half_sweep(const XLev &L, float omega, int colour, Slots S, double *u = nullptr) {
-  const int half = (L.n1 + 2) / 2, nrow = L.n2 + 1;
-  const int total = half * nrow * (L.n3 + 1);
-  const long long sy = L.N1, sz = (long long)L.N1 * L.N2;
-  const float rac = 1.f / L.ac;
-  for (int base = S.tid; base < total; base += XU * S.nth) {
-    long long q[XU], rq[XU];
-    bool ok[XU];
-#pragma unroll
-    for (int v = 0; v < XU; ++v) {
-      const int t = base + v * S.nth;
-      ok[v] = false;
-      q[v] = rq[v] = 0;
-      if (t < total) {
-        const int row = t / half, m = t - row * half;
-        const int k = row / nrow + 1, j = row - (k - 1) * nrow + 1;
-        const int i = colour_start(colour, j, k) + 2 * m;
-        if (i <= L.n1 + 1) {
-          ok[v] = true;
-          q[v] = L.g(i, j, k);
-          rq[v] = L.rr(i, j, k);
-        }
+  if (kind & K_RESTRICT) {
+    // residual on the tile and one halo layer, then the coarse nodes whose
+    // fine twin (2I-1, 2J-1, 2K-1) lies in the tile (the first and last tiles
+    // of a row also set the coarse ghost nodes)
+    const int nx = t.w + 2, ny = t.h + 2;
+    const int tot = nx * ny * (t.d + 2);
+    for (int v = threadIdx.x; v < tot; v += blockDim.x) {
+      const int row = v / nx, bx = 1 + v - row * nx;
+      const int bz = 1 + row / ny, by = 1 + row % ny;
+      const int q = bx + BX * (by + BY * bz);
+      RF[q] = box_residual(E, R, q, L);
+    }
+    __syncthreads();
+    const GLev &C = a.G[l + 1];
+    const int I0 = t.tx == 0 ? 0 : (TX / 2) * t.tx + 1, I1 = t.tx == L.ntx - 1 ? C.n1 + 2 : (TX / 2) * (t.tx + 1);
+    const int J0 = t.ty == 0 ? 0 : (TY / 2) * t.ty + 1, J1 = t.ty == L.nty - 1 ? C.n2 + 2 : (TY / 2) * (t.ty + 1);
+    const int K0 = t.tz == 0 ? 0 : (TZ / 2) * t.tz + 1, K1 = t.tz == L.ntz - 1 ? C.n3 + 2 : (TZ / 2) * (t.tz + 1);
+    const int cx = I1 - I0 + 1, cy = J1 - J0 + 1;
+    const int ctot = cx * cy * (K1 - K0 + 1);
+    for (int v = threadIdx.x; v < ctot; v += blockDim.x) {
+      const int row = v / cx, I = I0 + v - row * cx;
+      const int K = K0 + row / cy, J = J0 + row % cy;
+      float rv = INFINITY;
+      if (I >= 1 && J >= 1 && K >= 1 && I <= C.n1 + 1 && J <= C.n2 + 1 && K <= C.n3 + 1) {
+        const int q = (2 * I - 1 - t.i0) + BX * ((2 * J - 1 - t.j0) + BY * (2 * K - 1 - t.k0));
+        if (!wall(R[q])) rv = weigh27(RF, q);
+      }
+      const long long o = C.g(I, J, K);
+      C.r[o] = rv;
+      C.e[o] = 0.f;
+    }
+  } else {
+    // the tile's correction back to the grid (and, last post-sweep of
+    // level 1, into the FP64 solution)
+    const int tot = t.w * t.h * t.d;
+    const long long U1 = (long long)L.n1 + 3, U2 = (long long)L.n2 + 3;
+    for (int v = threadIdx.x; v < tot; v += blockDim.x) {
+      const int row = v / t.w, bx = 2 + v - row * t.w;
+      const int bz = 2 + row / t.h, by = 2 + row % t.h;
+      const int q = bx + BX * (by + BY * bz);
+      const int i = t.i0 + bx, j = t.j0 + by, k = t.k0 + bz;
+      const float ev = E[q];
+      L.e[L.g(i, j, k)] = ev;
+      if ((kind & K_ADDU) && !wall(R[q])) {
+        double *uq = a.u + i + U1 * (j + U2 * k);
+        *uq = *uq + (double)ev;
       }
     }
-    int bc[XU];
-    float r[XU], c0[XU], ew[XU], en[XU], es[XU], ee[XU], et[XU], eb[XU];
-#pragma unroll
-    for (int v = 0; v < XU; ++v) {
-      if (!ok[v]) continue;
-      const long long w = q[v];
-      bc[v] = L.bc[w];
-      r[v] = L.r[rq[v]];
-      c0[v] = L.e[w];
-      ew[v] = L.e[w - 1];
-      en[v] = L.e[w + sy];
-      es[v] = L.e[w - sy];
-      ee[v] = L.e[w + 1];
-      et[v] = L.e[w + sz];
-      eb[v] = L.e[w - sz];
-    }
-    double uo[XU];
-    if (u) {
-#pragma unroll
-      for (int v = 0; v < XU; ++v)
-        if (ok[v] && bc[v] <= 0) uo[v] = u[q[v]];
-    }
-#pragma unroll
-    for (int v = 0; v < XU; ++v) {
-      if (!ok[v] || bc[v] > 0) continue;
-      const float tt = r[v] - L.aw * ew[v] - L.an * en[v] - L.as * es[v] - L.ae * ee[v] - L.at * et[v] -
-                       L.ab * eb[v];
-      const float en1 = (1.f - omega) * c0[v] + omega * tt * rac;
-      L.e[q[v]] = en1;
-      if (u) u[q[v]] = uo[v] + (double)en1;
-    }
   }
 }
 
-// u += e on the nodes of one colour (their correction is final)
-__device__ __noinline__ void g_add_colour(const XLev &L, int colour, Slots S, double *u) {
-  const int half = (L.n1 + 2) / 2, nrow = L.n2 + 1;
-  const int total = half * nrow * (L.n3 + 1);
-  for (int base = S.tid; base < total; base += XU * S.nth) {
-    long long q[XU];
-    bool ok[XU];
-#pragma unroll
-    for (int v = 0; v < XU; ++v) {
-      const int t = base + v * S.nth;
-      ok[v] = false;
-      q[v] = 0;
-      if (t < total) {
-        const int row = t / half, m = t - row * half;
-        const int k = row / nrow + 1, j = row - (k - 1) * nrow + 1;
-        const int i = colour_start(colour, j, k) + 2 * m;
-        if (i <= L.n1 + 1) {
-          ok[v] = true;
-          q[v] = L.g(i, j, k);
-        }
+// one pass of `kind` over the tiles of grid level l, ending at a grid barrier
+__device__ __noinline__ void tile_pass(const XArgs &a, const XMaps &maps, int l, int kind, Pipe &pp,
+                                       cg::grid_group &grid) {
+  const GLev &L = a.G[l];
+  const int NT = L.ntx * L.nty * L.ntz;
+  int tau = blockIdx.x;
+  if (tau < NT && threadIdx.x == 0 && !pp.fail) issue(maps, l, kind, L, tau, pp, 0);
+  for (int m = 0; tau < NT; tau += gridDim.x, ++m) {
+    const int s = m & 1;
+    const int nxt = tau + gridDim.x;
+    if (nxt < NT && threadIdx.x == 0 && !pp.fail) issue(maps, l, kind, L, nxt, pp, s ^ 1);
+    __shared__ int ok;
+    if (threadIdx.x == 0) {
+      ok = !pp.fail && mbar_wait(pp.bar[s], pp.uses[s] & 1u);
+      if (!ok && !pp.fail) {
+        pp.fail = true;
+        raise_err(a.err, LEPIC_ERR_TIMEOUT, l);
       }
     }
-    int bc[XU];
-    float ev[XU];
-    double uo[XU];
-#pragma unroll
-    for (int v = 0; v < XU; ++v) {
-      if (!ok[v]) continue;
-      bc[v] = L.bc[q[v]];
-      ev[v] = L.e[q[v]];
-      uo[v] = u[q[v]];
+    __syncthreads();
+    pp.uses[s] += 1;
+    const bool good = ok != 0;
+    if (good) {
+      unsigned char *st = pp.stage[s];
+      tile_work(a, l, kind, tile_of(L, tau), reinterpret_cast<float *>(st),
+                reinterpret_cast<const float *>(st + BOX_STRIDE),
+                reinterpret_cast<const float *>(st + 2 * BOX_STRIDE), pp.rf);
     }
-#pragma unroll
-    for (int v = 0; v < XU; ++v)
-      if (ok[v] && bc[v] <= 0) u[q[v]] = uo[v] + (double)ev[v];
+    __syncthreads();
   }
-}
-
-// nsweep red-black sweeps; with u (finest level, last smoothing of the
-// cycle) the last half-sweep also accumulates u += e on every node
-__device__ __noinline__ void g_smooth(const XLev &L, float omega, int nsweep, cg::grid_group &grid, double *u = nullptr) {
-  const Slots S = slots();
-  for (int s = 0; s < nsweep; ++s) {
-    for (int colour = 0; colour < 2; ++colour) {
-      const bool last = u && s == nsweep - 1 && colour == 1;
-      g_half_sweep(L, omega, colour, S, last ? u : nullptr);
-      if (last) g_add_colour(L, 0, S, u);
-      grid.sync();
-    }
-  }
-}
-
-// fine residual rf = r - A e on the interior nodes (0 on walls)
-__device__ __noinline__ void g_residual(const XLev &F, Slots S) {
-  const int ni = F.n1 + 1, nj = F.n2 + 1;
-  const int total = ni * nj * (F.n3 + 1);
-  const long long sy = F.N1, sz = (long long)F.N1 * F.N2;
-  for (int base = S.tid; base < total; base += XU * S.nth) {
-    long long q[XU], rq[XU];
-    bool ok[XU];
-#pragma unroll
-    for (int u = 0; u < XU; ++u) {
-      const int t = base + u * S.nth;
-      ok[u] = t < total;
-      q[u] = rq[u] = 0;
-      if (ok[u]) {
-        const int row = t / ni, i = t - row * ni + 1;
-        const int k = row / nj + 1, j = row - (k - 1) * nj + 1;
-        q[u] = F.g(i, j, k);
-        rq[u] = F.rr(i, j, k);
-      }
-    }
-    int bc[XU];
-    float r[XU], c0[XU], ew[XU], en[XU], es[XU], ee[XU], et[XU], eb[XU];
-#pragma unroll
-    for (int u = 0; u < XU; ++u) {
-      if (!ok[u]) continue;
-      const long long v = q[u];
-      bc[u] = F.bc[v];
-      r[u] = F.r[rq[u]];
-      c0[u] = F.e[v];
-      ew[u] = F.e[v - 1];
-      en[u] = F.e[v + sy];
-      es[u] = F.e[v - sy];
-      ee[u] = F.e[v + 1];
-      et[u] = F.e[v + sz];
-      eb[u] = F.e[v - sz];
-    }
-#pragma unroll
-    for (int u = 0; u < XU; ++u) {
-      if (!ok[u]) continue;
-      F.rf[q[u]] = bc[u] > 0 ? 0.f
-                             : r[u] - (F.aw * ew[u] + F.ae * ee[u] + F.an * en[u] + F.as * es[u] +
-                                       F.ac * c0[u] + F.at * et[u] + F.ab * eb[u]);
-    }
-  }
-}
-
-__device__ __noinline__ void g_restrict(const XLev &F, const XLev &C, cg::grid_group &grid) {
-  const Slots S = slots();
-  g_residual(F, S);
-  grid.sync();
-  const int ni = C.n1 + 3, nj = C.n2 + 3;
-  const int total = ni * nj * (C.n3 + 3);
-  // one coarse node per iteration: its 27 loads are already independent
-  for (int t = S.tid; t < total; t += S.nth) {
-    const int row = t / ni, i = t - row * ni;
-    const int k = row / nj, j = row - k * nj;
-    restrict_node(F, C, i, j, k);
-  }
-  grid.sync();
-}
-
-__device__ __noinline__ void g_prolong(const XLev &F, const XLev &C, cg::grid_group &grid) {
-  const Slots S = slots();
-  const int ni = C.n1 + 1, nj = C.n2 + 1;
-  const int total = ni * nj * (C.n3 + 1);
-  // one coarse node per iteration: its 24 loads are already independent
-  for (int t = S.tid; t < total; t += S.nth) {
-    const int row = t / ni, i = t - row * ni + 1;
-    const int k = row / nj + 1, j = row - (k - 1) * nj + 1;
-    prolong_node(F, C, i, j, k);
-  }
+  // stores of this phase before the next phase's copies read them
+  asm volatile("fence.proxy.async.global;" ::: "memory");
   grid.sync();
 }
 
@@ -426,102 +441,169 @@ __device__ __forceinline__ void block_box(int i0, int ni, int j0, int nj, int k0
   }
 }
 
-__device__ void b_smooth(const XLev &L, float omega, int nsweep) {
+// red-black colour start: colour 0 = red ((i+j+k) odd), 1 = black
+// (Src/sors.f90:87-106, 249-267)
+__device__ __forceinline__ int colour_start(int colour, int j, int k) {
+  int is = (colour == 0) ? ((j % 2 == 0) ? 1 : 2) : ((j % 2 == 0) ? 2 : 1);
+  is += (k % 2 == 0) ? 0 : 1;
+  return is > 2 ? 1 : is;
+}
+
+__device__ void b_smooth(const SLev &L, float omega, int nsweep) {
   const float rac = 1.f / L.ac;
   const int half = (L.n1 + 2) / 2;
+  const int sy = L.N1, sz = L.N1 * L.N2;
   for (int s = 0; s < nsweep; ++s) {
     for (int colour = 0; colour < 2; ++colour) {
       block_box(0, half, 1, L.n2 + 1, 1, L.n3 + 1, [&](int ii, int j, int k) {
         const int i = colour_start(colour, j, k) + 2 * ii;
-        if (i <= L.n1 + 1) relax(L, omega, rac, i, j, k);
+        if (i > L.n1 + 1) return;
+        const int q = L.g(i, j, k);
+        const float rv = L.r[q];
+        if (wall(rv)) return;
+        const float tt = rv - L.aw * L.e[q - 1] - L.an * L.e[q + sy] - L.an * L.e[q - sy] - L.aw * L.e[q + 1] -
+                         L.at * L.e[q + sz] - L.at * L.e[q - sz];
+        L.e[q] = (1.f - omega) * L.e[q] + omega * tt * rac;
       });
       __syncthreads();
     }
   }
 }
 
-__device__ void b_restrict(const XLev &F, const XLev &C) {
-  block_box(1, F.n1 + 1, 1, F.n2 + 1, 1, F.n3 + 1,
-            [&](int i, int j, int k) { F.rf[F.g(i, j, k)] = fine_residual(F, i, j, k); });
+__device__ void b_restrict(const SLev &F, const SLev &C) {
+  const int sy = F.N1, sz = F.N1 * F.N2;
+  // the residual on every node, 0 on ghosts and walls
+  block_box(0, F.n1 + 3, 0, F.n2 + 3, 0, F.n3 + 3, [&](int i, int j, int k) {
+    const int q = F.g(i, j, k);
+    float v = 0.f;
+    if (i >= 1 && j >= 1 && k >= 1 && i <= F.n1 + 1 && j <= F.n2 + 1 && k <= F.n3 + 1) {
+      const float rv = F.r[q];
+      if (!wall(rv))
+        v = rv - (F.aw * F.e[q - 1] + F.aw * F.e[q + 1] + F.an * F.e[q + sy] + F.an * F.e[q - sy] + F.ac * F.e[q] +
+                  F.at * F.e[q + sz] + F.at * F.e[q - sz]);
+    }
+    F.rf[q] = v;
+  });
   __syncthreads();
-  block_box(0, C.n1 + 3, 0, C.n2 + 3, 0, C.n3 + 3, [&](int i, int j, int k) { restrict_node(F, C, i, j, k); });
+  block_box(0, C.n1 + 3, 0, C.n2 + 3, 0, C.n3 + 3, [&](int i, int j, int k) {
+    float rv = INFINITY;
+    if (i >= 1 && j >= 1 && k >= 1 && i <= C.n1 + 1 && j <= C.n2 + 1 && k <= C.n3 + 1) {
+      const int q = F.g(2 * i - 1, 2 * j - 1, 2 * k - 1);
+      if (!wall(F.r[q])) {
+        const float *R = F.rf;
+        rv = (8.f * R[q] + 4.f * (R[q + 1] + R[q - 1] + R[q + sy] + R[q - sy] + R[q + sz] + R[q - sz]) +
+              2.f * (R[q + 1 + sy] + R[q - 1 + sy] + R[q + 1 - sy] + R[q - 1 - sy] + R[q + 1 + sz] +
+                     R[q - 1 + sz] + R[q + sy + sz] + R[q - sy + sz] + R[q + 1 - sz] + R[q - 1 - sz] +
+                     R[q + sy - sz] + R[q - sy - sz]) +
+              R[q + 1 + sy + sz] + R[q - 1 + sy + sz] + R[q + 1 - sy + sz] + R[q - 1 - sy + sz] +
+              R[q + 1 + sy - sz] + R[q - 1 + sy - sz] + R[q + 1 - sy - sz] + R[q - 1 - sy - sz]) *
+             (1.f / 64.f);
+      }
+    }
+    const int o = C.g(i, j, k);
+    C.r[o] = rv;
+    C.e[o] = 0.f;
+  });
   __syncthreads();
 }
 
-__device__ void b_prolong(const XLev &F, const XLev &C) {
-  block_box(1, C.n1 + 1, 1, C.n2 + 1, 1, C.n3 + 1, [&](int i, int j, int k) { prolong_node(F, C, i, j, k); });
+// trilinear prolongation of C into F on F's non-wall nodes 0..n+1
+__device__ void b_prolong(const SLev &F, const SLev &C) {
+  block_box(0, F.n1 + 2, 0, F.n2 + 2, 0, F.n3 + 2, [&](int i, int j, int k) {
+    const int q = F.g(i, j, k);
+    if (wall(F.r[q])) return;
+    const int ci = (i + 1) >> 1, cj = (j + 1) >> 1, ck = (k + 1) >> 1;
+    const int ex = (i & 1) ^ 1, ey = (j & 1) ^ 1, ez = (k & 1) ^ 1;
+    const int c0 = C.g(ci, cj, ck);
+    float s = 0.f;
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+      for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < 2; ++dx)
+          if (dx <= ex && dy <= ey && dz <= ez) s += C.e[c0 + dx + C.N1 * (dy + C.N2 * dz)];
+    const int ne = ex + ey + ez;
+    F.e[q] += s * (ne == 0 ? 1.f : (ne == 1 ? 0.5f : (ne == 2 ? 0.25f : 0.125f)));
+  });
   __syncthreads();
 }
 
 // the coarse levels' view in block 0's shared memory
-__device__ __forceinline__ XLev smem_level(const XArgs &a, int l, unsigned char *sm) {
-  XLev S = a.L[l];
+__device__ __forceinline__ SLev smem_level(const XArgs &a, int l, unsigned char *sm) {
+  SLev S = a.S[l];
   S.e = reinterpret_cast<float *>(sm + a.so_e[l]);
   S.r = reinterpret_cast<float *>(sm + a.so_r[l]);
   S.rf = reinterpret_cast<float *>(sm + a.so_rf[l]);
-  S.bc = reinterpret_cast<int *>(sm + a.so_bc[l]);
   return S;
 }
 
-// the coarse part of the V-cycle, block 0 only: r of level ls+1 in, e out
+// the coarse part of the V-cycle, block 0 only: r of level ls+1 in from the
+// grid (its exchange arrays), e out
 __device__ __noinline__ void coarse_cycle(const XArgs &a, unsigned char *sm) {
   const int top = a.ls + 1, ng = a.ng;
   {
-    // four independent loads in flight per thread
-    const XLev G = a.L[top], S = smem_level(a, top, sm);
-    const int nr = (int)G.nr(), nt = (int)blockDim.x;
-    for (int t0 = threadIdx.x; t0 < nr; t0 += 4 * nt) {
-      float v[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) v[u] = t0 + u * nt < nr ? G.r[t0 + u * nt] : 0.f;
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-        if (t0 + u * nt < nr) S.r[t0 + u * nt] = v[u];
-    }
-    for (long long t = threadIdx.x; t < G.nn(); t += blockDim.x) S.e[t] = 0.f;
+    const GLev &G = a.G[top];
+    const SLev S = smem_level(a, top, sm);
+    block_box(0, S.N1, 0, S.N2, 0, S.n3 + 3, [&](int i, int j, int k) {
+      const int q = S.g(i, j, k);
+      S.r[q] = G.r[G.g(i, j, k)];
+      S.e[q] = 0.f;
+    });
   }
   __syncthreads();
   for (int l = top; l < ng; ++l) {
-    const XLev F = smem_level(a, l, sm), C = smem_level(a, l + 1, sm);
+    const SLev F = smem_level(a, l, sm), C = smem_level(a, l + 1, sm);
     b_smooth(F, a.omega, a.nu_pre);
     b_restrict(F, C);
   }
   b_smooth(smem_level(a, ng, sm), a.omega, a.coarse_sweeps);
   for (int l = ng - 1; l >= top; --l) {
-    const XLev F = smem_level(a, l, sm), C = smem_level(a, l + 1, sm);
+    const SLev F = smem_level(a, l, sm), C = smem_level(a, l + 1, sm);
     b_prolong(F, C);
     b_smooth(F, a.omega, a.nu_post);
   }
   {
-    const XLev G = a.L[top], S = smem_level(a, top, sm);
-    for (long long t = threadIdx.x; t < G.nn(); t += blockDim.x) G.e[t] = S.e[t];
+    const GLev &G = a.G[top];
+    const SLev S = smem_level(a, top, sm);
+    block_box(0, S.N1, 0, S.N2, 0, S.n3 + 3, [&](int i, int j, int k) { G.e[G.g(i, j, k)] = S.e[S.g(i, j, k)]; });
   }
-  __threadfence();
+  asm volatile("fence.proxy.async.global;" ::: "memory");
 }
 
+// ------------------------------------------------------------ level 1, FP64
 // FP64 residual b - A u of the finest level on its interior nodes, written
-// as the FP32 right-hand side of the V-cycle (0 on walls); returns this
-// thread's share of the L1 norm over the plasma nodes (bcnd = -1)
-__device__ __noinline__ double g_residual_f64(const XArgs &a, const XLev &L1, Slots S) {
+// as the FP32 right-hand side of the V-cycle (+inf on walls), the correction
+// cleared; returns this thread's share of the L1 norm over the plasma nodes
+// (bcnd = -1).  Each thread takes U nodes at once and issues all their
+// loads before any arithmetic.
+__device__ __noinline__ double g_residual_f64(const XArgs &a, const GLev &L1) {
   constexpr int U = 2;
+  const int tid = (int)(blockIdx.x * blockDim.x + threadIdx.x), nth = (int)(gridDim.x * blockDim.x);
   const int ni = L1.n1 + 1, nj = L1.n2 + 1;
   const int total = ni * nj * (L1.n3 + 1);
-  const long long sy = L1.N1, sz = (long long)L1.N1 * L1.N2;
+  const long long sy = L1.n1 + 3, sz = (long long)(L1.n1 + 3) * (L1.n2 + 3);
+  const long long ry = L1.n1 + 2, rz = (long long)(L1.n1 + 2) * (L1.n2 + 2);
   const double *u = a.u;
   double acc = 0.0;
-  for (int base = S.tid; base < total; base += U * S.nth) {
+  for (int base = tid; base < total; base += U * nth) {
     long long q[U], rq[U];
+    int ii[U], jj[U], kk[U];
     bool ok[U];
 #pragma unroll
     for (int v = 0; v < U; ++v) {
-      const int t = base + v * S.nth;
+      const int t = base + v * nth;
       ok[v] = t < total;
       q[v] = rq[v] = 0;
+      ii[v] = jj[v] = kk[v] = 1;
       if (ok[v]) {
         const int row = t / ni, i = t - row * ni + 1;
         const int k = row / nj + 1, j = row - (k - 1) * nj + 1;
-        q[v] = L1.g(i, j, k);
-        rq[v] = L1.rr(i, j, k);
+        ii[v] = i;
+        jj[v] = j;
+        kk[v] = k;
+        q[v] = i + sy * j + sz * k;
+        rq[v] = i + ry * j + rz * k;
       }
     }
     int bc[U];
@@ -530,7 +612,7 @@ __device__ __noinline__ double g_residual_f64(const XArgs &a, const XLev &L1, Sl
     for (int v = 0; v < U; ++v) {
       if (!ok[v]) continue;
       const long long w = q[v];
-      bc[v] = L1.bc[w];
+      bc[v] = a.bcnd[w];
       bv[v] = a.b[rq[v]];
       c0[v] = u[w];
       uw[v] = u[w - 1];
@@ -543,53 +625,86 @@ __device__ __noinline__ double g_residual_f64(const XArgs &a, const XLev &L1, Sl
 #pragma unroll
     for (int v = 0; v < U; ++v) {
       if (!ok[v]) continue;
-      double rv = 0.0;
+      float rf = INFINITY;
       if (bc[v] <= 0) {
-        rv = bv[v] - (a.aw * uw[v] + a.an * un[v] + a.as * us[v] + a.ae * ue[v] + a.ac * c0[v] + a.at * ut[v] +
-                      a.ab * ub[v]);
+        const double rv = bv[v] - (a.aw * uw[v] + a.an * un[v] + a.an * us[v] + a.aw * ue[v] + a.ac * c0[v] +
+                                   a.at * ut[v] + a.at * ub[v]);
         if (bc[v] == -1) acc += fabs(rv);
+        rf = (float)rv;
       }
-      L1.r[rq[v]] = (float)rv;
+      const long long o = L1.g(ii[v], jj[v], kk[v]);
+      L1.r[o] = rf;
+      L1.e[o] = 0.f;
     }
   }
   return acc;
 }
 
-__global__ void __launch_bounds__(XM_BLOCK, 1) k_refine_mixed(const XArgs *__restrict__ ap) {
+// r = +inf on the ghost nodes of level 1 (never updated, correction 0)
+__device__ __noinline__ void g_ghosts(const GLev &L) {
+  const int tid = (int)(blockIdx.x * blockDim.x + threadIdx.x), nth = (int)(gridDim.x * blockDim.x);
+  const int N1 = L.n1 + 3, N2 = L.n2 + 3, N3 = L.n3 + 3;
+  const int total = N1 * N2 * N3;
+  // the ghost faces: planes k = 0, n3+2, rows j = 0, n2+2, columns i = 0, n1+2
+  for (int t = tid; t < total; t += nth) {
+    const int row = t / N1, i = t - row * N1;
+    const int k = row / N2, j = row - k * N2;
+    if (i == 0 || j == 0 || k == 0 || i == N1 - 1 || j == N2 - 1 || k == N3 - 1) {
+      L.r[L.g(i, j, k)] = INFINITY;
+      L.e[L.g(i, j, k)] = 0.f;
+    }
+  }
+}
+
+// u += e on the non-wall nodes of level 1 (when no post-sweep of level 1 did it)
+__device__ __noinline__ void g_add_u(const XArgs &a, const GLev &L1) {
+  const int tid = (int)(blockIdx.x * blockDim.x + threadIdx.x), nth = (int)(gridDim.x * blockDim.x);
+  const int ni = L1.n1 + 1, nj = L1.n2 + 1;
+  const int total = ni * nj * (L1.n3 + 1);
+  for (int t = tid; t < total; t += nth) {
+    const int row = t / ni, i = t - row * ni + 1;
+    const int k = row / nj + 1, j = row - (k - 1) * nj + 1;
+    const long long o = L1.g(i, j, k);
+    if (!wall(L1.r[o])) {
+      double *uq = a.u + i + (long long)(L1.n1 + 3) * (j + (long long)(L1.n2 + 3) * k);
+      *uq = *uq + (double)L1.e[o];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(XM_BLOCK, 1)
+    k_refine_mixed(const XArgs *__restrict__ ap, const __grid_constant__ XMaps maps) {
   cg::grid_group grid = cg::this_grid();
   const XArgs &a = *ap;
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ unsigned char smem_raw[];
   __shared__ double sh[40];
-  const int lane = threadIdx.x & 31;
+  __shared__ __align__(8) unsigned long long bars[2];
+  unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<size_t>(smem_raw) + 127) & ~(size_t)127);
   const int ng = a.ng, ls = a.ls;
-  // level masks by injection from the finest mask (Src/mg.f90:429-436)
-  for (int l = 2; l <= ng; ++l) {
-    const XLev &F = a.L[l - 1], &C = a.L[l];
-    grid_rows(0, C.n2 + 3, 0, C.n3 + 3, [&](int j, int k) {
-      for (int i = lane; i <= C.n1 + 2; i += 32)
-        C.bc[C.g(i, j, k)] = F.bc[F.g(fmapx(i, F.n1), fmapx(j, F.n2), fmapx(k, F.n3))];
-    });
-    grid.sync();
+  Pipe pp;
+  pp.stage[0] = smem;
+  pp.stage[1] = smem + STAGE_BYTES;
+  pp.rf = reinterpret_cast<float *>(smem + 2 * STAGE_BYTES);
+  pp.bar[0] = smem_addr(&bars[0]);
+  pp.bar[1] = smem_addr(&bars[1]);
+  pp.uses[0] = pp.uses[1] = 0;
+  pp.fail = false;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(pp.bar[0]) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(pp.bar[1]) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (blockIdx.x == 0 && ls < ng) {
-    // coarse masks and zero residual halos, resident for the whole call
-    for (int l = ls + 1; l <= ng; ++l) {
-      const XLev G = a.L[l], S = smem_level(a, l, smem);
-      for (long long t = threadIdx.x; t < G.nn(); t += blockDim.x) {
-        S.bc[t] = G.bc[t];
-        S.rf[t] = 0.f;
-      }
-    }
-    __syncthreads();
-  }
-  const XLev &L1 = a.L[1];
-  const Slots S = slots();
+  __syncthreads();
+  const GLev &L1 = a.G[1];
+  g_ghosts(L1);
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+  grid.sync();
   double res = 0.0, res0 = -1.0;
   int it = 0, status = 0;
   for (;;) {
     // FP64 residual, FP32 copy as the V-cycle right-hand side, e = 0
-    const double acc = g_residual_f64(a, L1, S);
-    for (long long t = S.tid; t < L1.nn(); t += S.nth) L1.e[t] = 0.f;
+    const double acc = g_residual_f64(a, L1);
+    asm volatile("fence.proxy.async.global;" ::: "memory");
     res = grid_sum(a, acc, it, grid, sh) / a.alpha;
     if (res0 < 0.0) res0 = res;
     if (res < a.eps) break;
@@ -601,34 +716,50 @@ __global__ void __launch_bounds__(XM_BLOCK, 1) k_refine_mixed(const XArgs *__res
       status = LEPIC_ERR_DIVERGED;
       break;
     }
-    // FP32 V-cycle on the correction: grid levels down, coarse levels on
-    // chip, grid levels up; the last smoothing of level 1 also applies
-    // u += e (FP64)
-    for (int l = 1; l <= ls && l < ng; ++l) {
-      g_smooth(a.L[l], a.omega, l == 1 ? a.nu_fine_pre : a.nu_pre, grid);
-      g_restrict(a.L[l], a.L[l + 1], grid);
+    // FP32 V-cycle on the correction: grid levels down (sweeps, fused
+    // residual + restriction), coarse levels on chip, grid levels up (the
+    // first post-sweep prolongs), the last sweep of level 1 adds u += e
+    const int ldown = ls < ng ? ls : ng - 1;   // the last level restricted from
+    for (int l = 1; l <= ldown; ++l) {
+      const int nu = l == 1 ? a.nu_fine_pre : a.nu_pre;
+      for (int s = 0; s < nu; ++s) tile_pass(a, maps, l, K_SWEEP, pp, grid);
+      tile_pass(a, maps, l, K_RESTRICT, pp, grid);
     }
     bool added = false;
     if (ls < ng) {
       if (blockIdx.x == 0) coarse_cycle(a, smem);
       grid.sync();
     } else {
-      added = ng == 1 && a.coarse_sweeps > 0;
-      g_smooth(a.L[ng], a.omega, a.coarse_sweeps, grid, added ? a.u : nullptr);
+      // the coarsest level is a grid level: its sweeps (ng = 1: the last one
+      // adds u += e)
+      for (int s = 0; s < a.coarse_sweeps; ++s) {
+        const bool last = ng == 1 && s == a.coarse_sweeps - 1;
+        tile_pass(a, maps, ng, K_SWEEP | (last ? K_ADDU : 0), pp, grid);
+        added = added || last;
+      }
     }
     for (int l = (ls < ng ? ls : ng - 1); l >= 1; --l) {
-      g_prolong(a.L[l], a.L[l + 1], grid);
       const int nu = l == 1 ? a.nu_fine_post : a.nu_post;
-      const bool fin = l == 1 && nu > 0;
-      g_smooth(a.L[l], a.omega, nu, grid, fin ? a.u : nullptr);
-      added = added || fin;
+      if (nu == 0) {
+        tile_pass(a, maps, l, K_PRO, pp, grid);
+        continue;
+      }
+      for (int s = 0; s < nu; ++s) {
+        const bool last = l == 1 && s == nu - 1;
+        tile_pass(a, maps, l, K_SWEEP | (s == 0 ? K_PRO : 0) | (last ? K_ADDU : 0), pp, grid);
+        added = added || last;
+      }
     }
     if (!added) {
-      g_add_colour(L1, 0, S, a.u);
-      g_add_colour(L1, 1, S, a.u);
+      g_add_u(a, L1);
       grid.sync();
     }
     ++it;
+  }
+  if (pp.fail && threadIdx.x == 0) {
+    // copies possibly in flight: one more bounded wait on each stage
+    mbar_wait(pp.bar[0], pp.uses[0] & 1u);
+    mbar_wait(pp.bar[1], pp.uses[1] & 1u);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.out_i[0] = it;
@@ -639,6 +770,44 @@ __global__ void __launch_bounds__(XM_BLOCK, 1) k_refine_mixed(const XArgs *__res
 }
 
 size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// tensor map of array `base` of level L with a box of bx x by x bz floats
+int box_map(CUtensorMap *m, float *base, const GLev &L, unsigned bx, unsigned by, unsigned bz) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) {
+    fprintf(stderr, "lepic_gpu: cuTensorMapEncodeTiled not available\n");
+    return LEPIC_ERR_CUDA;
+  }
+  const cuuint64_t dims[3] = {(cuuint64_t)L.P1, (cuuint64_t)(L.n2 + 3), (cuuint64_t)(L.n3 + 3)};
+  const cuuint64_t strides[2] = {(cuuint64_t)L.P1 * 4, (cuuint64_t)L.P1 * (L.n2 + 3) * 4};
+  const cuuint32_t box[3] = {bx, by, bz};
+  const cuuint32_t es[3] = {1, 1, 1};
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    fprintf(stderr, "lepic_gpu: cuTensorMapEncodeTiled failed (%d) for a %d x %d x %d level\n", (int)r, L.n1, L.n2,
+            L.n3);
+    return LEPIC_ERR_CUDA;
+  }
+  return LEPIC_OK;
+}
 
 }  // namespace
 
@@ -663,76 +832,113 @@ int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const do
   A.omega = (float)omega;
   A.u = u;
   A.b = b;
+  A.bcnd = bcnd;
   A.eps = eps;
-  char nm[32];
+  A.err = c.d_err;
+  // coefficients per level (Src/mg.h) and the coarse levels that fit in
+  // shared memory (level 1 stays on the grid)
+  float co[XM_MAX + 1][4];
   for (int l = 1; l <= ng; ++l) {
-    XLev &L = A.L[l];
-    L.n1 = n[0] >> (l - 1);
-    L.n2 = n[1] >> (l - 1);
-    L.n3 = n[2] >> (l - 1);
-    L.N1 = L.n1 + 3;
-    L.N2 = L.n2 + 3;
-    L.R1 = L.n1 + 2;
-    L.R2 = L.n2 + 2;
     double hl[3];
     for (int q = 0; q < 3; ++q) hl[q] = h[q] * (double)(1 << (l - 1));
     const double aw = eps0 / (hl[0] * hl[0]), an = eps0 / (hl[1] * hl[1]), at = eps0 / (hl[2] * hl[2]);
     const double ac = -(an + an + aw + aw + at + at);
     if (l == 1) {
-      A.aw = A.ae = aw;
-      A.an = A.as = an;
-      A.at = A.ab = at;
+      A.aw = aw;
+      A.an = an;
+      A.at = at;
       A.ac = ac;
     }
-    L.aw = L.ae = (float)aw;
-    L.an = L.as = (float)an;
-    L.at = L.ab = (float)at;
-    L.ac = (float)ac;
-    const size_t nn = (size_t)L.nn(), nr = (size_t)L.nr();
-    snprintf(nm, sizeof nm, "xm_e%d", l);
-    L.e = (float *)scratch(nm, sizeof(float) * nn);
-    snprintf(nm, sizeof nm, "xm_r%d", l);
-    L.r = (float *)scratch(nm, sizeof(float) * nr);
-    snprintf(nm, sizeof nm, "xm_rf%d", l);
-    L.rf = (float *)scratch(nm, sizeof(float) * nn);
-    if (l == 1) {
-      L.bc = const_cast<int *>(bcnd);
-    } else {
-      snprintf(nm, sizeof nm, "xm_bc%d", l);
-      L.bc = (int *)scratch(nm, sizeof(int) * nn);
-    }
-    if (!L.e || !L.r || !L.rf || !L.bc) return LEPIC_ERR_CUDA;
-    LEPIC_CUDA(cudaMemsetAsync(L.rf, 0, sizeof(float) * nn, s));
-    LEPIC_CUDA(cudaMemsetAsync(L.e, 0, sizeof(float) * nn, s));
+    co[l][0] = (float)aw;
+    co[l][1] = (float)an;
+    co[l][2] = (float)at;
+    co[l][3] = (float)ac;
   }
-  // the coarse levels that fit in shared memory (level 1 stays on the grid)
-  size_t smem = 0;
+  size_t csm = 0;
   A.ls = ng;
   for (int l = ng; l >= 2; --l) {
-    const XLev &L = A.L[l];
-    const size_t need = align16(4 * L.nn()) * 3 + align16(4 * L.nr());
-    if (smem + need > XM_SMEM_BUDGET) break;
-    A.so_e[l] = (unsigned)smem;
-    A.so_rf[l] = (unsigned)(smem + align16(4 * L.nn()));
-    A.so_bc[l] = (unsigned)(smem + 2 * align16(4 * L.nn()));
-    A.so_r[l] = (unsigned)(smem + 3 * align16(4 * L.nn()));
-    smem += need;
+    const size_t nn = (size_t)(n[0] / (1 << (l - 1)) + 3) * (n[1] / (1 << (l - 1)) + 3) * (n[2] / (1 << (l - 1)) + 3);
+    const size_t need = align16(4 * nn) * 3;
+    if (csm + need > XM_SMEM_COARSE) break;
+    A.so_e[l] = (unsigned)csm;
+    A.so_r[l] = (unsigned)(csm + align16(4 * nn));
+    A.so_rf[l] = (unsigned)(csm + 2 * align16(4 * nn));
+    csm += need;
     A.ls = l - 1;
   }
-  if (A.ls == ng) smem = 0;
+  if (A.ls == ng) csm = 0;
+  const int ngl = A.ls < ng ? A.ls + 1 : ng;   // levels with global arrays
+  if (A.ls > GMAX) {
+    fprintf(stderr, "lepic_gpu: mixed solve: %d grid levels (at most %d)\n", A.ls, GMAX);
+    return LEPIC_ERR_UNSUPPORTED;
+  }
+  char nm[32];
+  for (int l = 1; l <= ng; ++l) {
+    const int m1 = n[0] >> (l - 1), m2 = n[1] >> (l - 1), m3 = n[2] >> (l - 1);
+    if (l <= ngl) {
+      GLev &L = A.G[l];
+      L.n1 = m1;
+      L.n2 = m2;
+      L.n3 = m3;
+      L.P1 = (m1 + 4 + 3) & ~3;
+      L.ntx = (m1 + TX - 1) / TX;
+      L.nty = (m2 + TY - 1) / TY;
+      L.ntz = (m3 + TZ - 1) / TZ;
+      L.aw = co[l][0];
+      L.an = co[l][1];
+      L.at = co[l][2];
+      L.ac = co[l][3];
+      snprintf(nm, sizeof nm, "xm_e%d", l);
+      L.e = (float *)scratch(nm, sizeof(float) * (size_t)L.nn());
+      snprintf(nm, sizeof nm, "xm_r%d", l);
+      L.r = (float *)scratch(nm, sizeof(float) * (size_t)L.nn());
+      if (!L.e || !L.r) return LEPIC_ERR_CUDA;
+      // every node of e and r is written by the kernel before it is read
+      // (the ghosts of level 1 at its start, the others by the restriction);
+      // the padding columns are never read as nodes
+      LEPIC_CUDA(cudaMemsetAsync(L.e, 0, sizeof(float) * (size_t)L.nn(), s));
+    }
+    if (l > A.ls) {
+      SLev &S = A.S[l];
+      S.n1 = m1;
+      S.n2 = m2;
+      S.n3 = m3;
+      S.N1 = m1 + 3;
+      S.N2 = m2 + 3;
+      S.aw = co[l][0];
+      S.an = co[l][1];
+      S.at = co[l][2];
+      S.ac = co[l][3];
+    }
+  }
+  XMaps M;
+  memset(&M, 0, sizeof(M));
+  for (int l = 1; l <= ngl; ++l) {
+    const GLev &L = A.G[l];
+    if (l <= A.ls) {
+      int rc = box_map(&M.fe[l], L.e, L, BX, BY, BZ);
+      if (!rc) rc = box_map(&M.fr[l], L.r, L, BX, BY, BZ);
+      if (rc) return rc;
+    }
+    if (l >= 2) {
+      const int rc = box_map(&M.ce[l], L.e, L, CBX, CBY, CBZ);
+      if (rc) return rc;
+    }
+  }
   A.alpha = fabs((double)((n[0] + 1) * (n[1] + 1) * (n[2] + 1)) * A.ac) * 1.0;
+  const size_t smem = (csm > TILE_SMEM ? csm : TILE_SMEM) + 128;
   LEPIC_CUDA(cudaFuncSetAttribute(k_refine_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
   LEPIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_refine_mixed, XM_BLOCK, smem));
   if (occ < 1) return LEPIC_ERR_CUDA;
-  const int blocks = c.sms * (occ < 2 ? occ : 2);
+  const int blocks = c.sms;
   A.partial = (double *)scratch("xm_partial", sizeof(double) * 2 * blocks);
   A.out_i = (int *)scratch("xm_out_i", sizeof(int) * 4);
   A.out_d = (double *)scratch("xm_out_d", sizeof(double) * 2);
   XArgs *dA = (XArgs *)scratch("xm_args", sizeof(XArgs));
   if (!A.partial || !A.out_i || !A.out_d || !dA) return LEPIC_ERR_CUDA;
   LEPIC_CUDA(cudaMemcpyAsync(dA, &A, sizeof(XArgs), cudaMemcpyHostToDevice, s));
-  void *args[] = {&dA};
+  void *args[] = {&dA, &M};
   int tm = timer_start("pdesolver_mixed", s);
   LEPIC_CUDA(cudaLaunchCooperativeKernel((void *)k_refine_mixed, dim3(blocks), dim3(XM_BLOCK), args, smem, s));
   timer_stop(tm, s);
@@ -743,6 +949,7 @@ int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const do
   LEPIC_CUDA(cudaStreamSynchronize(s));
   if (iters) *iters = hi[0];
   if (res_out) *res_out = hd[0];
+  // a copy that timed out stays in the device error word (lepic_dev_check)
   return hi[1];
 }
 

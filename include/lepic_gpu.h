@@ -51,6 +51,8 @@ extern "C" {
 #define LEPIC_ERR_NOT_CONVERGED 23 /* iteration cap reached                      */
 #define LEPIC_ERR_SCRATCH_LIMIT 24 /* grid too large for the static scratch of
                                       lepic_dev_pdesolver_noalloc               */
+#define LEPIC_ERR_TIMEOUT 25       /* a bounded device wait ran out (a tile copy
+                                      that never completed)                     */
 
 /* ------------------------------------------------------------------------ */
 /* Fortran COMMON blocks of Src/particle_info.h:53-70 and Src/constants.h,   */
