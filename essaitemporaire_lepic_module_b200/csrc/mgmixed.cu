@@ -59,7 +59,11 @@ constexpr int XM_BLOCK = 512;
 constexpr size_t XM_SMEM_COARSE = 160 * 1024;   // budget of the on-chip coarse levels
 
 // tile of updated nodes; the last tile of a row takes the remainder, up to
-// T + 1 nodes (the node n + 1)
+// T + 1 nodes (the node n + 1).  TX = 32 puts every fine box on a 16-byte
+// boundary (column 32 t) and every coarse box too (column 16 t); a row of one
+// colour of the tile and its halo (at most 18 nodes) is one warp's.  (A
+// 24-node tile with a row per half-warp was slower at 128^3: 6 tiles per
+// row of 129 nodes instead of 4.)
 constexpr int TX = 32, TY = 8, TZ = 8;
 // staged boxes: the fine box is the tile with two halo layers on each side
 // (one more for a last tile), the coarse box covers what the fine box's
@@ -82,7 +86,8 @@ struct GLev {
   int P1;              // row pitch, floats
   int ntx, nty, ntz;   // tiles per axis
   float aw, an, at, ac;
-  float *e, *r;
+  float *e[2];         // the correction, two buffers (a sweep reads one, writes the other)
+  float *r;
   __host__ __device__ long long g(int i, int j, int k) const {
     return (long long)(i + 1) + (long long)P1 * (j + (long long)(n2 + 3) * k);
   }
@@ -118,8 +123,8 @@ struct XArgs {
 
 // tensor maps of the tile boxes (a __grid_constant__ kernel parameter)
 struct XMaps {
-  CUtensorMap fe[GMAX + 1], fr[GMAX + 1];  // fine boxes of e and r, levels 1..ls
-  CUtensorMap ce[GMAX + 2];                // coarse boxes of e, levels 2..ls + 1
+  CUtensorMap fe[GMAX + 1][2], fr[GMAX + 1];  // fine boxes of e (both buffers) and r, levels 1..ls
+  CUtensorMap ce[GMAX + 2][2];                // coarse boxes of e, levels 2..ls + 1
 };
 
 __device__ __forceinline__ bool wall(float r) { return isinf(r); }
@@ -201,10 +206,14 @@ __device__ __forceinline__ void tma_box(uint32_t dst, const CUtensorMap *m, int 
       : "memory");
 }
 
+// The dynamic shared memory of the kernel: the tile stages (grid phases) or
+// the coarse levels (block 0's coarse cycle).  Box pointers are formed from
+// this symbol so that the compiler addresses them as shared memory.
+extern __shared__ __align__(128) unsigned char xm_smem[];
+
 // The double-buffered tile copies of one block.
 struct Pipe {
-  unsigned char *stage[2];
-  float *rf;              // residual box (restriction)
+  int base;               // offset of the first 128-byte boundary in xm_smem
   uint32_t bar[2];        // mbarriers in shared memory
   unsigned uses[2];       // completed phases per mbarrier
   bool fail;
@@ -233,76 +242,70 @@ __device__ __forceinline__ Tile tile_of(const GLev &L, int tau) {
   return t;
 }
 
-// thread 0: the copies of tile tau of level l into stage s
-__device__ void issue(const XMaps &maps, int l, int kind, const GLev &L, int tau, Pipe &pp, int s) {
+// thread 0: the copies of tile tau of level l into stage s; ein / cin: the
+// e buffers read (level l, level l + 1)
+__device__ void issue(const XMaps &maps, int l, int kind, const GLev &L, int tau, Pipe &pp, int s, int ein,
+                      int cin) {
   const Tile t = tile_of(L, tau);
   const unsigned bytes = 2 * BOX_BYTES + ((kind & K_PRO) ? CBOX_BYTES : 0u);
-  // earlier generic accesses of this stage and of the global arrays come
-  // before the asynchronous copies
+  // earlier generic accesses of this stage come before the asynchronous copy
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  asm volatile("fence.proxy.async.global;" ::: "memory");
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(pp.bar[s]), "r"(bytes) : "memory");
-  const uint32_t dst = smem_addr(pp.stage[s]);
-  tma_box(dst, &maps.fe[l], TX * t.tx, t.j0, t.k0, pp.bar[s]);
+  const uint32_t dst = smem_addr(xm_smem + pp.base + s * STAGE_BYTES);
+  tma_box(dst, &maps.fe[l][ein], TX * t.tx, t.j0, t.k0, pp.bar[s]);
   tma_box(dst + BOX_STRIDE, &maps.fr[l], TX * t.tx, t.j0, t.k0, pp.bar[s]);
   if (kind & K_PRO)
-    tma_box(dst + 2 * BOX_STRIDE, &maps.ce[l + 1], (TX / 2) * t.tx, (TY / 2) * t.ty - 1, (TZ / 2) * t.tz - 1,
+    tma_box(dst + 2 * BOX_STRIDE, &maps.ce[l + 1][cin], (TX / 2) * t.tx, (TY / 2) * t.ty - 1, (TZ / 2) * t.tz - 1,
             pp.bar[s]);
 }
 
-// red-black colour: red = (i + j + k) odd (Src/sors.f90:87-106)
-// one relaxation of box node q (Src/sors.f90 update, in FP32)
-__device__ __forceinline__ void relax_box(float *E, const float *R, int q, const GLev &L, float omega, float rac) {
-  const float rv = R[q];
-  if (wall(rv)) return;
-  const float tt = rv - L.aw * E[q - 1] - L.an * E[q + BX] - L.an * E[q - BX] - L.aw * E[q + 1] -
-                   L.at * E[q + BXY] - L.at * E[q - BXY];
-  E[q] = (1.f - omega) * E[q] + omega * tt * rac;
-}
-
-// nodes of one colour in the box region [x0, x0 + nx) x [y0, y0 + ny) x
-// [z0, z0 + nz); odd = true: (i + j + k) odd
+// The rows (y, z) of the region [x0, x0 + nx) x [y0, y0 + ny) x [z0, z0 + nz)
+// dealt to the warps of the block, the lanes along x: body(x, y, z).  The
+// row coordinates advance by the warp count without divisions.
 template <class F>
-__device__ __forceinline__ void colour_loop(const Tile &t, int x0, int nx, int y0, int ny, int z0, int nz, bool odd,
-                                            F &&body) {
-  const int hx = (nx + 1) >> 1;
-  const int tot = hx * ny * nz;
-  for (int v = threadIdx.x; v < tot; v += blockDim.x) {
-    const int row = v / hx, m = v - row * hx;
-    const int zz = row / ny, yy = row - zz * ny;
-    const int by = y0 + yy, bz = z0 + zz;
-    const int par = (t.i0 + x0 + t.j0 + by + t.k0 + bz) & 1;   // parity of the row's first node
-    const int bx = x0 + ((par == (odd ? 1 : 0)) ? 0 : 1) + 2 * m;
-    if (bx < x0 + nx) body(bx + BX * (by + BY * bz));
+__device__ __forceinline__ void box_rows(int x0, int nx, int y0, int ny, int z0, int nz, F &&body) {
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int zz = wp / ny, yy = wp - zz * ny;
+#pragma unroll 2
+  for (; zz < nz;) {
+    const int y = y0 + yy, z = z0 + zz;
+    for (int x = x0 + lane; x < x0 + nx; x += 32) body(x, y, z);
+    yy += nw;
+    while (yy >= ny) {
+      yy -= ny;
+      ++zz;
+    }
   }
 }
 
-// trilinear prolongation (Src/mg.f90:849-939) of the coarse box onto fine
-// box node (bx, by, bz) = fine node (i, j, k): a fine node on a coarse node
-// takes its value, one between coarse nodes their mean
-__device__ __forceinline__ float prolong_value(const float *CE, const Tile &t, int i, int j, int k) {
-  const int ci = (i + 1) >> 1, cj = (j + 1) >> 1, ck = (k + 1) >> 1;
-  const int ex = (i & 1) ^ 1, ey = (j & 1) ^ 1, ez = (k & 1) ^ 1;
-  const int cx = ci - ((TX / 2) * t.tx - 1), cy = cj - ((TY / 2) * t.ty - 1), cz = ck - ((TZ / 2) * t.tz - 1);
-  const int c0 = cx + CBX * (cy + CBY * cz);
-  float s = 0.f;
-#pragma unroll
-  for (int dz = 0; dz < 2; ++dz)
-#pragma unroll
-    for (int dy = 0; dy < 2; ++dy)
-#pragma unroll
-      for (int dx = 0; dx < 2; ++dx)
-        if (dx <= ex && dy <= ey && dz <= ez) s += CE[c0 + dx + CBX * (dy + CBY * dz)];
-  const float wgt = (ex + ey + ez) == 0 ? 1.f : ((ex + ey + ez) == 1 ? 0.5f : ((ex + ey + ez) == 2 ? 0.25f : 0.125f));
-  return s * wgt;
-}
-
-// fine residual of box node q (0 on walls)
-__device__ __forceinline__ float box_residual(const float *E, const float *R, int q, const GLev &L) {
-  const float rv = R[q];
-  if (wall(rv)) return 0.f;
-  return rv - (L.aw * E[q - 1] + L.aw * E[q + 1] + L.an * E[q + BX] + L.an * E[q - BX] + L.ac * E[q] +
-               L.at * E[q + BXY] + L.at * E[q - BXY]);
+// one red-black colour (red = (i + j + k) odd, Src/sors.f90:87-106) of the box
+// region [x0, x0 + nx) x ... relaxed in place (the Src/sors.f90 update, in
+// FP32): each warp takes a row (at most 32 nodes of one colour: nx <= 64),
+// its rows advance by the warp count.  Every load of a node is issued before
+// its wall test; walls keep their value.
+__device__ __forceinline__ void relax_colour(float *E, const float *R, const Tile &t, int x0, int nx, int y0, int ny,
+                                             int z0, int nz, bool red, float aw, float an, float at, float om,
+                                             float rac) {
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int p0 = (t.i0 + x0 + t.j0 + y0 + t.k0 + z0 + (red ? 1 : 0)) & 1;   // 1: the row's first node is off colour
+  int zz = wp / ny, yy = wp - zz * ny;
+#pragma unroll 2
+  for (; zz < nz;) {
+    const int bx = x0 + ((p0 + yy + zz) & 1) + 2 * lane;
+    const int q = bx + BX * (y0 + yy + BY * (z0 + zz));
+    if (bx < x0 + nx) {
+      const float rv = R[q], e0 = E[q], ew = E[q - 1], ee = E[q + 1], en = E[q + BX], es = E[q - BX],
+                  et = E[q + BXY], eb = E[q - BXY];
+      const float tt = rv - aw * ew - an * en - an * es - aw * ee - at * et - at * eb;
+      const float v = (1.f - om) * e0 + om * tt * rac;
+      if (!wall(rv)) E[q] = v;
+    }
+    yy += nw;
+    while (yy >= ny) {
+      yy -= ny;
+      ++zz;
+    }
+  }
 }
 
 // 27-point full weighting (Src/mg.f90:696-702) of the residual box around q
@@ -317,95 +320,119 @@ __device__ __forceinline__ float weigh27(const float *F, int q) {
          (1.f / 64.f);
 }
 
-// the work of one staged tile
-__device__ void tile_work(const XArgs &a, int l, int kind, const Tile &t, float *E, const float *R, const float *CE,
-                          float *RF) {
-  const GLev &L = a.G[l];
+// the work of one staged tile (stage s): sweep / prolong+sweep / restrict;
+// eout: the e buffer of level l written
+__device__ void tile_work(const GLev &L, const GLev &C, double *u, float omega, int kind, const Tile &t, int base,
+                          int s, int eout, int cout) {
+  float *E = reinterpret_cast<float *>(xm_smem + base + s * STAGE_BYTES);
+  const float *R = reinterpret_cast<const float *>(xm_smem + base + s * STAGE_BYTES + BOX_STRIDE);
+  const float aw = L.aw, an = L.an, at = L.at, ac = L.ac;
+  const int n1 = L.n1, n2 = L.n2, n3 = L.n3;
   if (kind & K_PRO) {
-    // the coarse correction onto every non-wall node of the box inside the grid
-    const int tot = (t.w + 4) * (t.h + 4) * (t.d + 4);
-    for (int v = threadIdx.x; v < tot; v += blockDim.x) {
-      const int nx = t.w + 4, ny = t.h + 4;
-      const int row = v / nx, bx = v - row * nx;
-      const int bz = row / ny, by = row - bz * ny;
+    // trilinear prolongation (Src/mg.f90:849-939) of the coarse box onto
+    // every non-wall node of the fine box inside the grid: a fine node on a
+    // coarse node takes its value, one between coarse nodes their mean
+    const float *CE = reinterpret_cast<const float *>(xm_smem + base + s * STAGE_BYTES + 2 * BOX_STRIDE);
+    const int cx0 = (TX / 2) * t.tx - 1, cy0 = (TY / 2) * t.ty - 1, cz0 = (TZ / 2) * t.tz - 1;
+    box_rows(0, t.w + 4, 0, t.h + 4, 0, t.d + 4, [&](int bx, int by, int bz) {
       const int i = t.i0 + bx, j = t.j0 + by, k = t.k0 + bz;
-      if (i < 0 || j < 0 || k < 0 || i > L.n1 + 1 || j > L.n2 + 1 || k > L.n3 + 1) continue;
+      if (i < 0 || j < 0 || k < 0 || i > n1 + 1 || j > n2 + 1 || k > n3 + 1) return;
       const int q = bx + BX * (by + BY * bz);
-      if (wall(R[q])) continue;
-      E[q] += prolong_value(CE, t, i, j, k);
-    }
+      if (wall(R[q])) return;
+      const int c = (((i + 1) >> 1) - cx0) + CBX * ((((j + 1) >> 1) - cy0) + CBY * (((k + 1) >> 1) - cz0));
+      // weights of the upper neighbour per axis: 0.5 between coarse nodes, 0 on one
+      const float wx = (i & 1) ? 0.f : 0.5f, wy = (j & 1) ? 0.f : 0.5f, wz = (k & 1) ? 0.f : 0.5f;
+      const float vx = 1.f - wx, vy = 1.f - wy, vz = 1.f - wz;
+      const float s0 = vx * CE[c] + wx * CE[c + 1];
+      const float s1 = vx * CE[c + CBX] + wx * CE[c + 1 + CBX];
+      const float s2 = vx * CE[c + CBX * CBY] + wx * CE[c + 1 + CBX * CBY];
+      const float s3 = vx * CE[c + CBX + CBX * CBY] + wx * CE[c + 1 + CBX + CBX * CBY];
+      E[q] += vz * (vy * s0 + wy * s1) + wz * (vy * s2 + wy * s3);
+    });
     __syncthreads();
   }
   if (kind & K_SWEEP) {
-    const float om = a.omega, rac = 1.f / L.ac;
+    const float om = omega, rac = 1.f / ac;
     // red on the tile and one halo layer, then black on the tile
-    colour_loop(t, 1, t.w + 2, 1, t.h + 2, 1, t.d + 2, true, [&](int q) { relax_box(E, R, q, L, om, rac); });
+    relax_colour(E, R, t, 1, t.w + 2, 1, t.h + 2, 1, t.d + 2, true, aw, an, at, om, rac);
     __syncthreads();
-    colour_loop(t, 2, t.w, 2, t.h, 2, t.d, false, [&](int q) { relax_box(E, R, q, L, om, rac); });
+    relax_colour(E, R, t, 2, t.w, 2, t.h, 2, t.d, false, aw, an, at, om, rac);
     __syncthreads();
   }
   if (kind & K_RESTRICT) {
-    // residual on the tile and one halo layer, then the coarse nodes whose
-    // fine twin (2I-1, 2J-1, 2K-1) lies in the tile (the first and last tiles
-    // of a row also set the coarse ghost nodes)
-    const int nx = t.w + 2, ny = t.h + 2;
-    const int tot = nx * ny * (t.d + 2);
-    for (int v = threadIdx.x; v < tot; v += blockDim.x) {
-      const int row = v / nx, bx = 1 + v - row * nx;
-      const int bz = 1 + row / ny, by = 1 + row % ny;
+    // residual on the tile and one halo layer (0 on walls), then the coarse
+    // nodes whose fine twin (2I-1, 2J-1, 2K-1) lies in the tile (the first
+    // and last tiles of a row also set the coarse ghost nodes)
+    float *RF = reinterpret_cast<float *>(xm_smem + base + 2 * STAGE_BYTES);
+    box_rows(1, t.w + 2, 1, t.h + 2, 1, t.d + 2, [&](int bx, int by, int bz) {
       const int q = bx + BX * (by + BY * bz);
-      RF[q] = box_residual(E, R, q, L);
-    }
+      const float rv = R[q], e0 = E[q], ew = E[q - 1], ee = E[q + 1], en = E[q + BX], es = E[q - BX],
+                  et = E[q + BXY], eb = E[q - BXY];
+      const float v = rv - (aw * ew + aw * ee + an * en + an * es + ac * e0 + at * et + at * eb);
+      RF[q] = wall(rv) ? 0.f : v;
+    });
     __syncthreads();
-    const GLev &C = a.G[l + 1];
-    const int I0 = t.tx == 0 ? 0 : (TX / 2) * t.tx + 1, I1 = t.tx == L.ntx - 1 ? C.n1 + 2 : (TX / 2) * (t.tx + 1);
-    const int J0 = t.ty == 0 ? 0 : (TY / 2) * t.ty + 1, J1 = t.ty == L.nty - 1 ? C.n2 + 2 : (TY / 2) * (t.ty + 1);
-    const int K0 = t.tz == 0 ? 0 : (TZ / 2) * t.tz + 1, K1 = t.tz == L.ntz - 1 ? C.n3 + 2 : (TZ / 2) * (t.tz + 1);
-    const int cx = I1 - I0 + 1, cy = J1 - J0 + 1;
-    const int ctot = cx * cy * (K1 - K0 + 1);
-    for (int v = threadIdx.x; v < ctot; v += blockDim.x) {
-      const int row = v / cx, I = I0 + v - row * cx;
-      const int K = K0 + row / cy, J = J0 + row % cy;
+    float *Cr = C.r, *Ce = C.e[cout];
+    const int m1 = C.n1, m2 = C.n2, m3 = C.n3, P1 = C.P1;
+    const int I0 = t.tx == 0 ? 0 : (TX / 2) * t.tx + 1, I1 = t.tx == L.ntx - 1 ? m1 + 2 : (TX / 2) * (t.tx + 1);
+    const int J0 = t.ty == 0 ? 0 : (TY / 2) * t.ty + 1, J1 = t.ty == L.nty - 1 ? m2 + 2 : (TY / 2) * (t.ty + 1);
+    const int K0 = t.tz == 0 ? 0 : (TZ / 2) * t.tz + 1, K1 = t.tz == L.ntz - 1 ? m3 + 2 : (TZ / 2) * (t.tz + 1);
+    box_rows(I0, I1 - I0 + 1, J0, J1 - J0 + 1, K0, K1 - K0 + 1, [&](int I, int J, int K) {
       float rv = INFINITY;
-      if (I >= 1 && J >= 1 && K >= 1 && I <= C.n1 + 1 && J <= C.n2 + 1 && K <= C.n3 + 1) {
+      if (I >= 1 && J >= 1 && K >= 1 && I <= m1 + 1 && J <= m2 + 1 && K <= m3 + 1) {
         const int q = (2 * I - 1 - t.i0) + BX * ((2 * J - 1 - t.j0) + BY * (2 * K - 1 - t.k0));
         if (!wall(R[q])) rv = weigh27(RF, q);
       }
-      const long long o = C.g(I, J, K);
-      C.r[o] = rv;
-      C.e[o] = 0.f;
-    }
+      const long long o = (long long)(I + 1) + (long long)P1 * (J + (long long)(m2 + 3) * K);
+      Cr[o] = rv;
+      Ce[o] = 0.f;
+    });
   } else {
     // the tile's correction back to the grid (and, last post-sweep of
     // level 1, into the FP64 solution)
-    const int tot = t.w * t.h * t.d;
-    const long long U1 = (long long)L.n1 + 3, U2 = (long long)L.n2 + 3;
-    for (int v = threadIdx.x; v < tot; v += blockDim.x) {
-      const int row = v / t.w, bx = 2 + v - row * t.w;
-      const int bz = 2 + row / t.h, by = 2 + row % t.h;
+    float *Le = L.e[eout];
+    const int P1 = L.P1;
+    const long long U1 = (long long)n1 + 3, U2 = (long long)n2 + 3;
+    box_rows(2, t.w, 2, t.h, 2, t.d, [&](int bx, int by, int bz) {
       const int q = bx + BX * (by + BY * bz);
       const int i = t.i0 + bx, j = t.j0 + by, k = t.k0 + bz;
       const float ev = E[q];
-      L.e[L.g(i, j, k)] = ev;
+      Le[(long long)(i + 1) + (long long)P1 * (j + (long long)(n2 + 3) * k)] = ev;
       if ((kind & K_ADDU) && !wall(R[q])) {
-        double *uq = a.u + i + U1 * (j + U2 * k);
+        double *uq = u + i + U1 * (j + U2 * k);
         *uq = *uq + (double)ev;
       }
-    }
+    });
   }
 }
 
-// one pass of `kind` over the tiles of grid level l, ending at a grid barrier
+// One pass of `kind` over the tiles of grid level l, ending at a grid
+// barrier.  cur: bit m = the e buffer of level m that holds its correction;
+// a sweep reads it and writes the other one, which becomes current (no
+// block reads what another block of the same phase writes).
 __device__ __noinline__ void tile_pass(const XArgs &a, const XMaps &maps, int l, int kind, Pipe &pp,
-                                       cg::grid_group &grid) {
-  const GLev &L = a.G[l];
+                                       cg::grid_group &grid, unsigned &cur) {
+  // the level descriptors in shared memory for the whole pass
+  __shared__ GLev sL, sC;
+  __shared__ double *su;
+  __shared__ float som;
+  if (threadIdx.x == 0) {
+    sL = a.G[l];
+    if (kind & K_RESTRICT) sC = a.G[l + 1];
+    su = a.u;
+    som = a.omega;
+  }
+  __syncthreads();
+  const GLev &L = sL;
   const int NT = L.ntx * L.nty * L.ntz;
+  const int ein = (cur >> l) & 1, cin = (cur >> (l + 1)) & 1;
+  const int eout = (kind & K_RESTRICT) ? ein : ein ^ 1;
   int tau = blockIdx.x;
-  if (tau < NT && threadIdx.x == 0 && !pp.fail) issue(maps, l, kind, L, tau, pp, 0);
+  if (tau < NT && threadIdx.x == 0 && !pp.fail) issue(maps, l, kind, L, tau, pp, 0, ein, cin);
   for (int m = 0; tau < NT; tau += gridDim.x, ++m) {
     const int s = m & 1;
     const int nxt = tau + gridDim.x;
-    if (nxt < NT && threadIdx.x == 0 && !pp.fail) issue(maps, l, kind, L, nxt, pp, s ^ 1);
+    if (nxt < NT && threadIdx.x == 0 && !pp.fail) issue(maps, l, kind, L, nxt, pp, s ^ 1, ein, cin);
     __shared__ int ok;
     if (threadIdx.x == 0) {
       ok = !pp.fail && mbar_wait(pp.bar[s], pp.uses[s] & 1u);
@@ -416,16 +443,11 @@ __device__ __noinline__ void tile_pass(const XArgs &a, const XMaps &maps, int l,
     }
     __syncthreads();
     pp.uses[s] += 1;
-    const bool good = ok != 0;
-    if (good) {
-      unsigned char *st = pp.stage[s];
-      tile_work(a, l, kind, tile_of(L, tau), reinterpret_cast<float *>(st),
-                reinterpret_cast<const float *>(st + BOX_STRIDE),
-                reinterpret_cast<const float *>(st + 2 * BOX_STRIDE), pp.rf);
-    }
+    if (ok) tile_work(L, sC, su, som, kind, tile_of(L, tau), pp.base, s, eout, cin);
     __syncthreads();
   }
-  // stores of this phase before the next phase's copies read them
+  if (!(kind & K_RESTRICT)) cur ^= 1u << l;
+  // this phase's stores before the next phase's copies read them
   asm volatile("fence.proxy.async.global;" ::: "memory");
   grid.sync();
 }
@@ -566,7 +588,7 @@ __device__ __noinline__ void coarse_cycle(const XArgs &a, unsigned char *sm) {
   {
     const GLev &G = a.G[top];
     const SLev S = smem_level(a, top, sm);
-    block_box(0, S.N1, 0, S.N2, 0, S.n3 + 3, [&](int i, int j, int k) { G.e[G.g(i, j, k)] = S.e[S.g(i, j, k)]; });
+    block_box(0, S.N1, 0, S.N2, 0, S.n3 + 3, [&](int i, int j, int k) { G.e[0][G.g(i, j, k)] = S.e[S.g(i, j, k)]; });
   }
   asm volatile("fence.proxy.async.global;" ::: "memory");
 }
@@ -577,7 +599,7 @@ __device__ __noinline__ void coarse_cycle(const XArgs &a, unsigned char *sm) {
 // cleared; returns this thread's share of the L1 norm over the plasma nodes
 // (bcnd = -1).  Each thread takes U nodes at once and issues all their
 // loads before any arithmetic.
-__device__ __noinline__ double g_residual_f64(const XArgs &a, const GLev &L1) {
+__device__ __noinline__ double g_residual_f64(const XArgs &a, const GLev &L1, float *e1) {
   constexpr int U = 2;
   const int tid = (int)(blockIdx.x * blockDim.x + threadIdx.x), nth = (int)(gridDim.x * blockDim.x);
   const int ni = L1.n1 + 1, nj = L1.n2 + 1;
@@ -634,7 +656,7 @@ __device__ __noinline__ double g_residual_f64(const XArgs &a, const GLev &L1) {
       }
       const long long o = L1.g(ii[v], jj[v], kk[v]);
       L1.r[o] = rf;
-      L1.e[o] = 0.f;
+      e1[o] = 0.f;
     }
   }
   return acc;
@@ -651,13 +673,14 @@ __device__ __noinline__ void g_ghosts(const GLev &L) {
     const int k = row / N2, j = row - k * N2;
     if (i == 0 || j == 0 || k == 0 || i == N1 - 1 || j == N2 - 1 || k == N3 - 1) {
       L.r[L.g(i, j, k)] = INFINITY;
-      L.e[L.g(i, j, k)] = 0.f;
+      L.e[0][L.g(i, j, k)] = 0.f;
+      L.e[1][L.g(i, j, k)] = 0.f;
     }
   }
 }
 
 // u += e on the non-wall nodes of level 1 (when no post-sweep of level 1 did it)
-__device__ __noinline__ void g_add_u(const XArgs &a, const GLev &L1) {
+__device__ __noinline__ void g_add_u(const XArgs &a, const GLev &L1, const float *e1) {
   const int tid = (int)(blockIdx.x * blockDim.x + threadIdx.x), nth = (int)(gridDim.x * blockDim.x);
   const int ni = L1.n1 + 1, nj = L1.n2 + 1;
   const int total = ni * nj * (L1.n3 + 1);
@@ -667,7 +690,7 @@ __device__ __noinline__ void g_add_u(const XArgs &a, const GLev &L1) {
     const long long o = L1.g(i, j, k);
     if (!wall(L1.r[o])) {
       double *uq = a.u + i + (long long)(L1.n1 + 3) * (j + (long long)(L1.n2 + 3) * k);
-      *uq = *uq + (double)L1.e[o];
+      *uq = *uq + (double)e1[o];
     }
   }
 }
@@ -676,15 +699,11 @@ __global__ void __launch_bounds__(XM_BLOCK, 1)
     k_refine_mixed(const XArgs *__restrict__ ap, const __grid_constant__ XMaps maps) {
   cg::grid_group grid = cg::this_grid();
   const XArgs &a = *ap;
-  extern __shared__ unsigned char smem_raw[];
   __shared__ double sh[40];
   __shared__ __align__(8) unsigned long long bars[2];
-  unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<size_t>(smem_raw) + 127) & ~(size_t)127);
   const int ng = a.ng, ls = a.ls;
   Pipe pp;
-  pp.stage[0] = smem;
-  pp.stage[1] = smem + STAGE_BYTES;
-  pp.rf = reinterpret_cast<float *>(smem + 2 * STAGE_BYTES);
+  pp.base = (int)((128u - (smem_addr(xm_smem) & 127u)) & 127u);
   pp.bar[0] = smem_addr(&bars[0]);
   pp.bar[1] = smem_addr(&bars[1]);
   pp.uses[0] = pp.uses[1] = 0;
@@ -695,6 +714,8 @@ __global__ void __launch_bounds__(XM_BLOCK, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  unsigned char *smem = xm_smem + pp.base;
+  unsigned cur = 0;   // bit l: the e buffer of level l holding its correction
   const GLev &L1 = a.G[1];
   g_ghosts(L1);
   asm volatile("fence.proxy.async.global;" ::: "memory");
@@ -703,7 +724,7 @@ __global__ void __launch_bounds__(XM_BLOCK, 1)
   int it = 0, status = 0;
   for (;;) {
     // FP64 residual, FP32 copy as the V-cycle right-hand side, e = 0
-    const double acc = g_residual_f64(a, L1);
+    const double acc = g_residual_f64(a, L1, L1.e[(cur >> 1) & 1]);
     asm volatile("fence.proxy.async.global;" ::: "memory");
     res = grid_sum(a, acc, it, grid, sh) / a.alpha;
     if (res0 < 0.0) res0 = res;
@@ -722,8 +743,8 @@ __global__ void __launch_bounds__(XM_BLOCK, 1)
     const int ldown = ls < ng ? ls : ng - 1;   // the last level restricted from
     for (int l = 1; l <= ldown; ++l) {
       const int nu = l == 1 ? a.nu_fine_pre : a.nu_pre;
-      for (int s = 0; s < nu; ++s) tile_pass(a, maps, l, K_SWEEP, pp, grid);
-      tile_pass(a, maps, l, K_RESTRICT, pp, grid);
+      for (int s = 0; s < nu; ++s) tile_pass(a, maps, l, K_SWEEP, pp, grid, cur);
+      tile_pass(a, maps, l, K_RESTRICT, pp, grid, cur);
     }
     bool added = false;
     if (ls < ng) {
@@ -734,24 +755,24 @@ __global__ void __launch_bounds__(XM_BLOCK, 1)
       // adds u += e)
       for (int s = 0; s < a.coarse_sweeps; ++s) {
         const bool last = ng == 1 && s == a.coarse_sweeps - 1;
-        tile_pass(a, maps, ng, K_SWEEP | (last ? K_ADDU : 0), pp, grid);
+        tile_pass(a, maps, ng, K_SWEEP | (last ? K_ADDU : 0), pp, grid, cur);
         added = added || last;
       }
     }
     for (int l = (ls < ng ? ls : ng - 1); l >= 1; --l) {
       const int nu = l == 1 ? a.nu_fine_post : a.nu_post;
       if (nu == 0) {
-        tile_pass(a, maps, l, K_PRO, pp, grid);
+        tile_pass(a, maps, l, K_PRO, pp, grid, cur);
         continue;
       }
       for (int s = 0; s < nu; ++s) {
         const bool last = l == 1 && s == nu - 1;
-        tile_pass(a, maps, l, K_SWEEP | (s == 0 ? K_PRO : 0) | (last ? K_ADDU : 0), pp, grid);
+        tile_pass(a, maps, l, K_SWEEP | (s == 0 ? K_PRO : 0) | (last ? K_ADDU : 0), pp, grid, cur);
         added = added || last;
       }
     }
     if (!added) {
-      g_add_u(a, L1);
+      g_add_u(a, L1, L1.e[(cur >> 1) & 1]);
       grid.sync();
     }
     ++it;
@@ -888,15 +909,17 @@ int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const do
       L.an = co[l][1];
       L.at = co[l][2];
       L.ac = co[l][3];
-      snprintf(nm, sizeof nm, "xm_e%d", l);
-      L.e = (float *)scratch(nm, sizeof(float) * (size_t)L.nn());
+      for (int q = 0; q < 2; ++q) {
+        snprintf(nm, sizeof nm, "xm_e%d_%d", l, q);
+        L.e[q] = (float *)scratch(nm, sizeof(float) * (size_t)L.nn());
+        if (!L.e[q]) return LEPIC_ERR_CUDA;
+        // the nodes a sweep never writes (ghosts; walls stay at the 0 the
+        // residual or the restriction gave them) hold 0 in both buffers
+        LEPIC_CUDA(cudaMemsetAsync(L.e[q], 0, sizeof(float) * (size_t)L.nn(), s));
+      }
       snprintf(nm, sizeof nm, "xm_r%d", l);
       L.r = (float *)scratch(nm, sizeof(float) * (size_t)L.nn());
-      if (!L.e || !L.r) return LEPIC_ERR_CUDA;
-      // every node of e and r is written by the kernel before it is read
-      // (the ghosts of level 1 at its start, the others by the restriction);
-      // the padding columns are never read as nodes
-      LEPIC_CUDA(cudaMemsetAsync(L.e, 0, sizeof(float) * (size_t)L.nn(), s));
+      if (!L.r) return LEPIC_ERR_CUDA;
     }
     if (l > A.ls) {
       SLev &S = A.S[l];
@@ -916,12 +939,14 @@ int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const do
   for (int l = 1; l <= ngl; ++l) {
     const GLev &L = A.G[l];
     if (l <= A.ls) {
-      int rc = box_map(&M.fe[l], L.e, L, BX, BY, BZ);
+      int rc = box_map(&M.fe[l][0], L.e[0], L, BX, BY, BZ);
+      if (!rc) rc = box_map(&M.fe[l][1], L.e[1], L, BX, BY, BZ);
       if (!rc) rc = box_map(&M.fr[l], L.r, L, BX, BY, BZ);
       if (rc) return rc;
     }
     if (l >= 2) {
-      const int rc = box_map(&M.ce[l], L.e, L, CBX, CBY, CBZ);
+      int rc = box_map(&M.ce[l][0], L.e[0], L, CBX, CBY, CBZ);
+      if (!rc) rc = box_map(&M.ce[l][1], L.e[1], L, CBX, CBY, CBZ);
       if (rc) return rc;
     }
   }
