@@ -54,6 +54,21 @@ class LepicSpeciesMixed(C.Structure):
                 ("tile_off", C.c_void_p), ("cap", C.c_int), ("cell_off", C.c_void_p)]
 
 
+class LepicWinSpecies(C.Structure):
+    """lepic_win_species_t: one species of the differentiable collisional window."""
+    _fields_ = [("cell", C.c_void_p), ("p", C.c_void_p), ("lam", C.c_void_p), ("bl", C.c_void_p),
+                ("count", C.c_void_p), ("cap", C.c_int), ("fp64", C.c_int)]
+
+
+class LepicWinEvent(C.Structure):
+    """lepic_win_event_t: one recorded collision of the window."""
+    _fields_ = [("step", C.c_int), ("P", C.c_int), ("i", C.c_int), ("r", C.c_int),
+                ("rt", C.c_int), ("nby", C.c_int), ("ind", C.c_int), ("pad", C.c_int),
+                ("by", C.c_int * 4), ("slot", C.c_int * 4), ("e1", C.c_float * 12),
+                ("tv", C.c_double * 3), ("vold", C.c_double * 3), ("m_t", C.c_double), ("Eth", C.c_double),
+                ("sum_mass", C.c_double), ("pad2", C.c_double)]
+
+
 class LepicTargets(C.Structure):
     """lepic_targets_t: charged-target (DSMC) inputs and counters."""
     _fields_ = [("np", C.c_void_p * NPART), ("cell_off", C.c_void_p * NPART),
@@ -202,6 +217,23 @@ def lib():
         "lepic_dev_adj_walls": ([C.POINTER(LepicGrid), C.POINTER(LepicPhys), _I, vp, vp, vp, vp, _I, vp], _I),
         "lepic_dev_adj_deposit": ([C.POINTER(LepicGrid), vp, _I, _I, vp, vp, vp, _I, _I, C.POINTER(LepicPhys),
                                    vp], _I),
+        "lepic_dev_cw_deposit": ([C.POINTER(LepicGrid), C.POINTER(LepicWinSpecies), _I, C.POINTER(LepicPhys),
+                                  _I, vp, vp], _I),
+        "lepic_dev_cw_push": ([C.POINTER(LepicGrid), vp, C.POINTER(LepicWinSpecies), _I, C.POINTER(LepicPhys),
+                               _I, vp, vp], _I),
+        "lepic_dev_cw_reverse": ([C.POINTER(LepicGrid), vp, C.POINTER(LepicWinSpecies), _I,
+                                  C.POINTER(LepicPhys), _I, vp], _I),
+        "lepic_dev_cw_adj_push": ([C.POINTER(LepicGrid), vp, C.POINTER(LepicWinSpecies), _I,
+                                   C.POINTER(LepicPhys), _I, _D, vp, vp, vp], _I),
+        "lepic_dev_cw_adj_deposit": ([C.POINTER(LepicGrid), C.POINTER(LepicWinSpecies), _I,
+                                      C.POINTER(LepicPhys), _I, vp, vp], _I),
+        "lepic_dev_win_collisions": ([C.POINTER(LepicGrid), C.POINTER(LepicWinSpecies), _I,
+                                      C.POINTER(LepicTables), C.POINTER(LepicPhys), C.c_ulonglong, C.c_ulonglong,
+                                      _I, vp, _I, vp, P_dbl, C.POINTER(C.c_longlong), vp], _I),
+        "lepic_dev_cw_replay": ([C.POINTER(LepicGrid), C.POINTER(LepicWinSpecies), _I, C.POINTER(LepicPhys),
+                                 vp, _I, vp], _I),
+        "lepic_dev_cw_adj_collide": ([C.POINTER(LepicGrid), C.POINTER(LepicWinSpecies), _I,
+                                      C.POINTER(LepicPhys), vp, _I, vp], _I),
         "lepic_dev_eheating": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesF64), C.POINTER(LepicPhys),
                                C.POINTER(LepicHeat), C.c_double, vp, C.c_ulonglong, C.c_ulonglong, vp, vp], _I),
         "lepic_dev_eheating_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), C.POINTER(LepicPhys),
@@ -278,6 +310,9 @@ def exported_symbols():
             "lepic_dev_pdesolver_mixed", "lepic_dev_collisions_mixed", "lepic_dev_load_uniform",
             "lepic_dev_win_push", "lepic_dev_win_deposit", "lepic_dev_adj_push", "lepic_dev_adj_efield",
             "lepic_dev_adj_rhs", "lepic_dev_adj_walls", "lepic_dev_adj_deposit", "lepic_dev_cell_wall",
+            "lepic_dev_cw_deposit", "lepic_dev_cw_push", "lepic_dev_cw_reverse", "lepic_dev_cw_adj_push",
+            "lepic_dev_cw_adj_deposit", "lepic_dev_win_collisions", "lepic_dev_cw_replay",
+            "lepic_dev_cw_adj_collide",
             "lepic_dev_dielectric_phi",
             "lepic_dev_dens_red", "lepic_timing_enable", "lepic_timing_reset", "lepic_timing_read",
             "calc_rho_", "dens_red_", "pdesolver_", "calc_efield_",

@@ -28,7 +28,7 @@ import math
 import numpy as np
 import torch
 
-from ._lib import check, lib
+from ._lib import LepicWinEvent, LepicWinSpecies, check, lib
 from .constants import QE
 from .sim import Simulation
 
@@ -244,3 +244,332 @@ def window_objective(window, V, Bz, v0):
     V (nlabel,) FP64 CPU tensor of wall potentials by label, Bz FP64 scalar
     tensor, v0 (3, n) FP64 device tensor of initial velocities."""
     return _WindowFn.apply(V, Bz, v0, window)
+
+
+# ----------------------------------------------------------------------------
+# The differentiable window of the collisional step
+# ----------------------------------------------------------------------------
+_ALIVE_BL = -1 & 0xffff | (0x7fff << 16)     # born -1 (present at the start), not lost
+
+
+class CollisionWindow:
+    """K-step differentiable window of the full collisional step (no
+    counterpart in the reference) on the particles of a mixed-precision
+    Simulation: every charged species is deposited and pushed, the
+    null-collision MCC against the neutral gas runs every ns_coll steps
+    (Src/main.f90:1116-1122) and its collisions are recorded, so that every
+    later pass -- the backward pass, finite differences, the FP64 reference --
+    replays exactly those events (which particle, which reaction, the target's
+    velocity and the scattering directions; the velocities themselves follow
+    from the replayed state).
+
+    Observables (scalar J):
+      "energy"  mean kinetic energy (eV) of species 1 after K steps,
+      "probe"   the potential (V) at the node nearest the box centre after K
+                steps (a field solve of the final charge),
+      "flux"    the kinetic energy (J) carried to the walls by the
+                macroparticles lost during the window (P_loss(1) of
+                Src/part_expmover.f90:290-296 summed over the steps).
+    Gradients: dJ/dV per wall label, dJ/dB_z (uniform B) and dJ/dv0 (the
+    initial velocities of species 1, in its slot order).
+
+    fp64=False runs in place on the simulation's FP32 stores (the adjoint in
+    the particle-state arrays the sort uses as its second buffer, the window
+    history in the second cell array) with FP32 pushes and the mixed Poisson
+    solve; fp64=True runs on FP64 copies of the same initial particles with
+    the FP64 multigrid: the FP64 reference of the same events.  The backward
+    pass needs no particle checkpoints: it undoes each push (the inverse
+    Boris rotation), each collision (from its record), and keeps only the
+    potential of every step."""
+
+    def __init__(self, sim, K, fp64=False, ns_coll=None, first_it=None, log_cap=None, keep_initial=False,
+                 seed=None):
+        st = sim.st
+        if not sim.mixed:
+            raise ValueError("the collisional window runs on a mixed-precision Simulation")
+        if st.geom.flag_pbc or st.geom.flag_nmn or st.geom.flag_die:
+            raise ValueError("the collisional window supports Dirichlet (metal) walls only")
+        if st.bfield is not None:
+            raise ValueError("the collisional window differentiates a uniform B, not a B-field map")
+        self.sim, self.st, self.K, self.fp64 = sim, st, int(K), bool(fp64)
+        self.dev = sim.dev
+        self.ntype = st.ntype
+        self.nlabel = int(st.geom.ngrid)
+        self.ns_coll = int(ns_coll or st.wl.ns_coll)
+        self.first_it = int(sim.it + 1 if first_it is None else first_it)
+        self.seed = int(sim.seed if seed is None else seed)
+        self.ws = (LepicWinSpecies * self.ntype)()
+        self.stores = []
+        for p in range(self.ntype):
+            sp = sim.sp[p]
+            if self.fp64:
+                d = dict(cell=sp.cell.clone(), p=sp.p.to(torch.float64), lam=torch.zeros((6, sp.cap),
+                         dtype=torch.float64, device=self.dev), bl=torch.empty(sp.cap, dtype=torch.int32,
+                         device=self.dev), count=sp.count.clone())
+            else:
+                d = dict(cell=sp.cell, p=sp.p, lam=sp.p_alt, bl=sp.cell_alt, count=sp.count)
+            d["cap"] = sp.cap
+            self.stores.append(d)
+            w = self.ws[p]
+            w.cell, w.p, w.lam = d["cell"].data_ptr(), d["p"].data_ptr(), d["lam"].data_ptr()
+            w.bl, w.count, w.cap, w.fp64 = d["bl"].data_ptr(), d["count"].data_ptr(), d["cap"], int(self.fp64)
+        self.count0 = [int(d["count"].item()) for d in self.stores]
+        self.initial = None
+        if keep_initial:
+            self.initial = [(d["cell"].clone(), d["p"].clone(), d["count"].clone()) for d in self.stores]
+        n1, n2, n3 = st.n
+        self.centre = (n3 // 2 + 1, n2 // 2 + 1, n1 // 2 + 1)
+        self.phis = torch.empty((self.K + 1,) + tuple(sim.phi.shape), dtype=torch.float64, device=self.dev)
+        self.wall_acc = torch.zeros(self.ntype, dtype=torch.float64, device=self.dev)
+        cap = log_cap or max(4096, int(0.05 * sum(self.count0) * max(1, self.K // self.ns_coll + 1)))
+        self.log = torch.zeros(cap * C.sizeof(LepicWinEvent), dtype=torch.uint8, device=self.dev)
+        self.log_cap = cap
+        self.nlog = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self.ev_range = {}            # step -> (first record, end)
+        self.recorded = False
+        self.timing = {}
+        self.counts = np.zeros(64, dtype=np.int64)
+
+    # ------------------------------------------------------------ helpers
+    def _s(self):
+        return self.sim._s()
+
+    def _E(self):
+        return self.sim.Ei if self.fp64 else self.sim.E32
+
+    def _events(self, step):
+        a, b = self.ev_range.get(step, (0, 0))
+        return C.c_void_p(self.log.data_ptr() + a * C.sizeof(LepicWinEvent)), b - a
+
+    def use_log_of(self, other):
+        """Replay the collisions another window of the same initial state
+        recorded (the FP64 reference of a mixed window)."""
+        self.log = other.log.clone()
+        self.log_cap = other.log_cap
+        self.ev_range = dict(other.ev_range)
+        self.recorded = True
+
+    def _solve(self, u, rhs, eps=None):
+        """A u = rhs on plasma nodes (u holds the wall values and the start):
+        the FP64 multigrid for the FP64 window, FP32 V-cycles in FP64
+        refinement for the mixed one."""
+        sim, st = self.sim, self.st
+        eps = st.wl.eps if eps is None else eps
+        if self.fp64:
+            k, kt, res = C.c_int(0), C.c_double(0), C.c_double(0)
+            check(lib().lepic_dev_pdesolver(C.byref(sim.grid), _p(u), _p(rhs), st.wl.ncycl, eps, st.wl.omega,
+                                            st.ng, C.byref(sim.P), C.byref(k), C.byref(kt), C.byref(res),
+                                            self._s()), "pdesolver")
+        else:
+            m = sim.mg_mixed
+            it, res = C.c_int(0), C.c_double(0)
+            check(lib().lepic_dev_pdesolver_mixed(C.byref(sim.grid), _p(u), _p(rhs), eps, m["omega"], st.ng,
+                                                  C.byref(sim.P), m["max_refine"], m["nu_fine_pre"],
+                                                  m["nu_fine_post"], m["nu_pre"], m["nu_post"], m["coarse_sweeps"],
+                                                  C.byref(it), C.byref(res), self._s()), "pdesolver_mixed")
+
+    def _field(self):
+        self.sim.calc_rho()
+        self._solve(self.sim.phi, self.sim.rhs)
+
+    def _efield(self):
+        sim = self.sim
+        check(lib().lepic_dev_calc_efield(C.byref(sim.grid), _p(sim.phi), _p(sim.Ei), self._s()), "calc_efield")
+        if not self.fp64:
+            sim.pack_e32()
+
+    def _deposit(self, step):
+        sim, L = self.sim, lib()
+        sim.np.zero_()
+        for p in range(self.ntype):
+            if self.st.charge[p] != 0.0:
+                check(L.lepic_dev_cw_deposit(C.byref(sim.grid), C.byref(self.ws[p]), p + 1, C.byref(sim.P), step,
+                                             _p(sim.np[p]), self._s()), "cw_deposit")
+
+    def _set_params(self, V, Bz):
+        st, sim = self.st, self.sim
+        phi = torch.as_tensor(st.geom.phi, device=self.dev).clone()
+        for lab in range(1, self.nlabel + 1):
+            phi[sim.bcnd == lab] = float(V[lab - 1])
+        self.phi0 = phi
+        sim.P.Bconst[2] = float(Bz)
+        if float(Bz) != 0.0:
+            sim.P.flag_B = 1
+
+    # ------------------------------------------------------------ forward
+    def forward(self, V, Bz, v0=None, observable="energy"):
+        """Run the window from its initial state; returns J.  The first call
+        records the collisions, later calls replay them."""
+        if observable not in ("energy", "probe", "flux"):
+            raise ValueError(f"observable must be energy, probe or flux, not {observable!r}")
+        sim, L, st = self.sim, lib(), self.st
+        self.observable = observable
+        self._set_params(V, Bz)
+        if self.initial is not None:
+            for d, (c0, p0, n0) in zip(self.stores, self.initial):
+                d["cell"].copy_(c0)
+                d["p"].copy_(p0)
+                d["count"].copy_(n0)
+        for d in self.stores:
+            d["bl"].fill_(_ALIVE_BL)
+        if v0 is not None:
+            self.stores[0]["p"][3:6, :self.count0[0]] = v0.to(self.stores[0]["p"].dtype)
+        self.wall_acc.zero_()
+        sim.phi.copy_(self.phi0)
+        record = not self.recorded
+        if record:
+            self.nlog.zero_()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for n in range(self.K):
+            self._deposit(n)
+            self._field()
+            self.phis[n].copy_(sim.phi)
+            self._efield()
+            it = self.first_it + n
+            if st.tables is not None and it > 1 and it % self.ns_coll == 1 % self.ns_coll:
+                if record:
+                    a = int(self.nlog.item())
+                    nu = (C.c_double * 10)()
+                    cnt = (C.c_longlong * 64)()
+                    check(L.lepic_dev_win_collisions(C.byref(sim.grid), self.ws, self.ntype, C.byref(sim._tables),
+                                                     C.byref(sim.P), C.c_ulonglong(self.seed), C.c_ulonglong(it), n,
+                                                     _p(self.log), self.log_cap, _p(self.nlog), nu, cnt, self._s()),
+                          "win_collisions")
+                    self.counts[:64] += np.array(cnt[:], dtype=np.int64)
+                    self.ev_range[n] = (a, int(self.nlog.item()))
+                else:
+                    evp, ne = self._events(n)
+                    check(L.lepic_dev_cw_replay(C.byref(sim.grid), self.ws, self.ntype, C.byref(sim.P), evp, ne,
+                                                self._s()), "cw_replay")
+            for p in range(self.ntype):
+                if st.charge[p] != 0.0:
+                    check(L.lepic_dev_cw_push(C.byref(sim.grid), _p(self._E()), C.byref(self.ws[p]), p + 1,
+                                              C.byref(sim.P), n, _p(self.wall_acc[p:]), self._s()), "cw_push")
+        if observable == "probe":
+            self._deposit(self.K)
+            self._field()
+            self.phis[self.K].copy_(sim.phi)
+        ev1.record()
+        torch.cuda.synchronize()
+        self.recorded = True
+        self.timing["forward_ms"] = ev0.elapsed_time(ev1)
+        self.V, self.Bz = [float(v) for v in V], float(Bz)
+        return self._objective()
+
+    def _alive(self, p):
+        d = self.stores[p]
+        n = int(d["count"].item())
+        return n, ((d["bl"][:n] >> 16) == 0x7fff)
+
+    def _objective(self):
+        st = self.st
+        if self.observable == "energy":
+            n, a = self._alive(0)
+            v = self.stores[0]["p"][3:6, :n].to(torch.float64)
+            m = abs(st.mass[0])
+            self.n_alive = int(a.sum())
+            ke = 0.5 * m * (v ** 2).sum(dim=0) / QE
+            return float((ke * a).sum()) / self.n_alive
+        if self.observable == "probe":
+            k, j, i = self.centre
+            return float(self.phis[self.K][k, j, i])
+        return float(self.wall_acc.sum())
+
+    # ------------------------------------------------------------ backward
+    def backward(self, gJ=1.0):
+        """Adjoint of the last forward: (dJ/dV per label, dJ/dBz, dJ/dv0)."""
+        sim, L, st = self.sim, lib(), self.st
+        dev = self.dev
+        wl = st.wl
+        for d in self.stores:
+            d["lam"].zero_()
+        dV = torch.zeros(max(self.nlabel, 1), dtype=torch.float64, device=dev)
+        dBz = torch.zeros(1, dtype=torch.float64, device=dev)
+        lE = torch.zeros_like(sim.Ei)
+        lphi = torch.zeros_like(sim.phi)
+        mu = torch.zeros_like(sim.phi)
+        lnp = torch.zeros_like(sim.phi)
+        b = torch.zeros_like(sim.rhs)
+        from .constants import EPS0
+        h = st.h
+        n1, n2, n3 = st.n
+        ac = 2.0 * EPS0 * (1.0 / h[0] ** 2 + 1.0 / h[1] ** 2 + 1.0 / h[2] ** 2)
+        alpha = (n1 + 1) * (n2 + 1) * (n3 + 1) * ac
+
+        def field_adjoint(step):
+            # lphi -> mu (A mu = lphi on plasma nodes), dJ/dV, and the deposit
+            # adjoint of the particles deposited at `step`
+            check(L.lepic_dev_adj_rhs(C.byref(sim.grid), _p(lphi), _p(b), self._s()), "adj_rhs")
+            r0 = float(b.abs().sum()) / alpha
+            if r0 > 0.0:
+                self._solve(mu, b, eps=wl.eps * r0)   # warm start: mu of the later step (walls 0)
+            check(L.lepic_dev_adj_walls(C.byref(sim.grid), C.byref(sim.P), 1, _p(lphi), _p(mu), _p(lnp), _p(dV),
+                                        self.nlabel, self._s()), "adj_walls")
+            for p in range(self.ntype):
+                if st.charge[p] != 0.0:
+                    check(L.lepic_dev_cw_adj_deposit(C.byref(sim.grid), C.byref(self.ws[p]), p + 1, C.byref(sim.P),
+                                                     step, _p(mu), self._s()), "cw_adj_deposit")
+
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        wflux = 0.0
+        if self.observable == "energy":
+            n, a = self._alive(0)
+            m = abs(st.mass[0])
+            d = self.stores[0]
+            d["lam"][3:6, :n] = ((gJ * m / (QE * self.n_alive)) * d["p"][3:6, :n].to(torch.float64)
+                                 * a.to(torch.float64)).to(d["lam"].dtype)
+        elif self.observable == "probe":
+            lphi.zero_()
+            k, j, i = self.centre
+            lphi[k, j, i] = gJ
+            field_adjoint(self.K)
+        else:
+            wflux = gJ
+        for n in reversed(range(self.K)):
+            sim.phi.copy_(self.phis[n])
+            self._efield()
+            for p in range(self.ntype):
+                if st.charge[p] != 0.0:
+                    check(L.lepic_dev_cw_reverse(C.byref(sim.grid), _p(self._E()), C.byref(self.ws[p]), p + 1,
+                                                 C.byref(sim.P), n, self._s()), "cw_reverse")
+            lE.zero_()
+            for p in range(self.ntype):
+                if st.charge[p] != 0.0:
+                    check(L.lepic_dev_cw_adj_push(C.byref(sim.grid), _p(self._E()), C.byref(self.ws[p]), p + 1,
+                                                  C.byref(sim.P), n, C.c_double(wflux), _p(lE), _p(dBz),
+                                                  self._s()), "cw_adj_push")
+            if n in self.ev_range:
+                evp, ne = self._events(n)
+                check(L.lepic_dev_cw_adj_collide(C.byref(sim.grid), self.ws, self.ntype, C.byref(sim.P), evp, ne,
+                                                 self._s()), "cw_adj_collide")
+            check(L.lepic_dev_adj_efield(C.byref(sim.grid), _p(lE), _p(lphi), self._s()), "adj_efield")
+            field_adjoint(n)
+        ev1.record()
+        torch.cuda.synchronize()
+        self.timing["backward_ms"] = ev0.elapsed_time(ev1)
+        lam = self.stores[0]["lam"]
+        return (dV.cpu().numpy()[:self.nlabel].copy(), float(dBz.item()),
+                lam[3:6, :self.count0[0]].to(torch.float64).clone())
+
+
+class _CollisionWindowFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, V, Bz, v0, window, observable):
+        J = window.forward(V.detach().cpu().numpy(), float(Bz), v0.detach(), observable=observable)
+        ctx.window = window
+        return torch.tensor(J, dtype=torch.float64)
+
+    @staticmethod
+    def backward(ctx, gJ):
+        dV, dBz, dv0 = ctx.window.backward(float(gJ))
+        return (torch.as_tensor(dV, dtype=torch.float64), torch.tensor(dBz, dtype=torch.float64), dv0, None, None)
+
+
+def collision_window_objective(window, V, Bz, v0, observable="energy"):
+    """J(V, Bz, v0) through a CollisionWindow as a torch.autograd.Function:
+    V (nlabel,) FP64 CPU tensor of wall potentials by label, Bz FP64 scalar
+    tensor, v0 (3, n) FP64 device tensor of the initial velocities of
+    species 1 (its slot order)."""
+    return _CollisionWindowFn.apply(V, Bz, v0, window, observable)

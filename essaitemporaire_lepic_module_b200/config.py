@@ -14,8 +14,8 @@ Workloads (sizes from the benchmark definition; ``*_small`` are the same
 set-ups shrunk so the FP64 CPU oracle finishes in seconds):
   box32      32^3 cells, e- + Ar+ 16 ppc, walls 0 V, no B, no collisions
   mcc128     128^3 cells, e- + Ar+ 64 ppc, Bz = 0.01 T, Ar 1 Pa / 300 K MCC
-             (mcc96, mcc64, mcc32: the same on smaller grids, for profiling
-             captures and tests)
+             (mcc96, mcc64, mcc32, mcc16: the same on smaller grids, for
+             profiling captures and tests)
   poisson256 256^3 grid, two 16^3 electrodes at +-100 V, 64 Gaussian blobs
   penning    96x96x192 cells, e- 32 ppc, Bz = 0.1 T, end plates +200 V
              (electrode labels 2 and 3), side walls 0 V (label 1)
@@ -88,8 +88,8 @@ def workload(name: str) -> Workload:
         n = (32, 32, 32) if name == "box32" else (16, 16, 16)
         return Workload(name, n, 1e-4, [_box(n, 1e-4) + [1]], [0.0, 0.0], _ar_ion(),
                         Te=2.0, n0=1e15, ppc=16, dt=2e-11, steps=200)
-    if name in ("mcc128", "mcc32", "mcc64", "mcc96"):
-        n = {"mcc128": (128,) * 3, "mcc32": (32,) * 3, "mcc64": (64,) * 3, "mcc96": (96,) * 3}[name]
+    if name in ("mcc128", "mcc32", "mcc64", "mcc96", "mcc16"):
+        n = {"mcc128": (128,) * 3, "mcc32": (32,) * 3, "mcc64": (64,) * 3, "mcc96": (96,) * 3, "mcc16": (16,) * 3}[name]
         return Workload(name, n, 1e-4, [_box(n, 1e-4) + [1]], [0.0, 0.0], _ar_ion(),
                         Te=2.0, n0=1e15, ppc=64 if name != "mcc32" else 32, dt=2e-11, steps=500,
                         B=(0.0, 0.0, 0.01), gas_pressure=1.0, gas_T=300.0)

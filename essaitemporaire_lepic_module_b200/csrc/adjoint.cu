@@ -36,6 +36,7 @@ constexpr int MAX_LABEL = 16;
 struct WinConst {
   double h0, h1, h2, dt, k1, kk, Bx, By, Bz, kdep, q, mass;
   double dkk;       // d kk / d Bz
+  double Nm;        // macroparticle weight
   int boris;
 };
 
@@ -484,7 +485,562 @@ WinConst win_const(const lepic_grid_t &g, const lepic_phys_t &P, int ptype) {
   c.kdep = P.Nm[p] / (g.h[0] * g.h[1] * g.h[2]);
   c.q = P.charge[p];
   c.mass = P.mass[p];
+  c.Nm = P.Nm[p];
   return c;
+}
+
+// ============================================================ collisional window
+// The differentiable window of the collisional step in the mixed layout
+// (lepic_win_species_t): particles keep their slots, positions are a packed
+// cell and offsets in [0,1), real type R = float (the mixed form) or double
+// (its FP64 reference).  Step n maps (x^n, v^{n-1/2}) to (x^{n+1}, v^{n+1/2}):
+// deposit x^n, field solve, E^n, collisions of step n (v^{n-1/2} -> v+),
+// push.  The backward pass runs the steps in reverse without checkpoints:
+// the push is reversed exactly up to rounding (x^n = x^{n+1} - dt v^{n+1/2},
+// then the inverse Boris rotation with E^n gathered at x^n), a collision is
+// undone from its record (the incident's velocity before it), a particle a
+// wall took kept its state from before that push, and a particle a collision
+// created does not exist before its step.  Only the fields phi^n of every
+// step are kept.
+constexpr int WALIVE = 0x7fff;
+__device__ __forceinline__ int born_of(int b) { return (short)(b & 0xffff); }
+__device__ __forceinline__ int lost_of(int b) { return b >> 16; }
+
+template <class R>
+struct WinS {
+  int *cell;
+  R *p;
+  R *lam;
+  int *bl;
+  long long cap;
+};
+
+template <class R>
+WinS<R> win_view(const lepic_win_species_t &w) {
+  WinS<R> v;
+  v.cell = w.cell;
+  v.p = (R *)w.p;
+  v.lam = (R *)w.lam;
+  v.bl = w.bl;
+  v.cap = w.cap;
+  return v;
+}
+
+// cell (1-based) and offsets of a packed window particle
+__device__ __forceinline__ void unpack_cell(int cc, int &ix, int &iy, int &iz) {
+  ix = (cc & (LEPIC_CELL_MAX - 1)) + 1;
+  iy = ((cc >> LEPIC_CELL_BITS) & (LEPIC_CELL_MAX - 1)) + 1;
+  iz = (cc >> (2 * LEPIC_CELL_BITS)) + 1;
+}
+__device__ __forceinline__ int pack_cell(int ix, int iy, int iz) {
+  return (ix - 1) | ((iy - 1) << LEPIC_CELL_BITS) | ((iz - 1) << (2 * LEPIC_CELL_BITS));
+}
+
+// the eight left-node weights (the order of Src/part_expmover.f90:100-108)
+// of offsets (fx, fy, fz): the left-node factor is 1 - f
+template <class R>
+__device__ __forceinline__ void weights8(R fx, R fy, R fz, R (&w)[8]) {
+  const R px = R(1) - fx, py = R(1) - fy, pz = R(1) - fz;
+  w[0] = px * py * pz;
+  w[1] = (R(1) - px) * py * pz;
+  w[2] = (R(1) - px) * (R(1) - py) * pz;
+  w[3] = px * (R(1) - py) * pz;
+  w[4] = px * py * (R(1) - pz);
+  w[5] = (R(1) - px) * py * (R(1) - pz);
+  w[6] = (R(1) - px) * (R(1) - py) * (R(1) - pz);
+  w[7] = px * (R(1) - py) * (R(1) - pz);
+}
+
+// E at node g: FP32 (Ex, Ey, Ez, 0) per node for the mixed form, FP64 (3 per
+// node) for its reference
+template <class R>
+__device__ __forceinline__ void node_E(const void *E, long long g, R &ex, R &ey, R &ez);
+template <>
+__device__ __forceinline__ void node_E<float>(const void *E, long long g, float &ex, float &ey, float &ez) {
+  const float4 e = reinterpret_cast<const float4 *>(E)[g];
+  ex = e.x;
+  ey = e.y;
+  ez = e.z;
+}
+template <>
+__device__ __forceinline__ void node_E<double>(const void *E, long long g, double &ex, double &ey, double &ez) {
+  const double *e = reinterpret_cast<const double *>(E) + 3 * g;
+  ex = e[0];
+  ey = e[1];
+  ez = e[2];
+}
+
+template <class R>
+__device__ __forceinline__ void gather_E(const Dims &d, const void *E, long long g0, const R (&w)[8], R &Ex, R &Ey,
+                                         R &Ez) {
+  Ex = Ey = Ez = R(0);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    R ex, ey, ez;
+    node_E<R>(E, g0 + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q)), ex, ey, ez);
+    Ex += w[q] * ex;
+    Ey += w[q] * ey;
+    Ez += w[q] * ez;
+  }
+}
+
+// the Boris rotation (Src/part_expmover.f90:214-240) and its inverse
+template <class R>
+__device__ __forceinline__ void boris(const WinConst &c, R Ex, R Ey, R Ez, R &vx, R &vy, R &vz) {
+  const R k1 = (R)c.k1;
+  if (c.boris) {
+    const R Bx = (R)c.Bx, By = (R)c.By, Bz = (R)c.Bz, kk = (R)c.kk;
+    const R v1x = vx + k1 * Ex, v1y = vy + k1 * Ey, v1z = vz + k1 * Ez;
+    const R v3x = v1x + k1 * (v1y * Bz - v1z * By), v3y = v1y + k1 * (v1z * Bx - v1x * Bz),
+            v3z = v1z + k1 * (v1x * By - v1y * Bx);
+    vx = v1x + kk * (v3y * Bz - v3z * By) + k1 * Ex;
+    vy = v1y + kk * (v3z * Bx - v3x * Bz) + k1 * Ey;
+    vz = v1z + kk * (v3x * By - v3y * Bx) + k1 * Ez;
+  } else {
+    vx = vx + R(2) * k1 * Ex;
+    vy = vy + R(2) * k1 * Ey;
+    vz = vz + R(2) * k1 * Ez;
+  }
+}
+template <class R>
+__device__ __forceinline__ void boris_inverse(const WinConst &c, R Ex, R Ey, R Ez, R &vx, R &vy, R &vz) {
+  const R k1 = (R)c.k1;
+  if (c.boris) {
+    const R Bx = (R)c.Bx, By = (R)c.By, Bz = (R)c.Bz, kk = (R)c.kk;
+    const R v2x = vx - k1 * Ex, v2y = vy - k1 * Ey, v2z = vz - k1 * Ez;
+    const R v3x = v2x - k1 * (v2y * Bz - v2z * By), v3y = v2y - k1 * (v2z * Bx - v2x * Bz),
+            v3z = v2z - k1 * (v2x * By - v2y * Bx);
+    vx = v2x - kk * (v3y * Bz - v3z * By) - k1 * Ex;
+    vy = v2y - kk * (v3z * Bx - v3x * Bz) - k1 * Ey;
+    vz = v2z - kk * (v3x * By - v3y * Bx) - k1 * Ez;
+  } else {
+    vx = vx - R(2) * k1 * Ex;
+    vy = vy - R(2) * k1 * Ey;
+    vz = vz - R(2) * k1 * Ez;
+  }
+}
+
+// offset f moved by s cells of (possibly negative) displacement df: the
+// new offset in [0,1) and the cell shift
+template <class R>
+__device__ __forceinline__ int move_offset(R &f, R df) {
+  f = f + df;
+  int sh = 0;
+  if (!(f >= R(0) && f < R(1))) {
+    sh = (int)floor((double)f);
+    f = f - (R)sh;
+    if (f >= R(1)) {
+      f = R(0);
+      sh += 1;
+    }
+    if (f < R(0)) f = R(0);
+  }
+  return sh;
+}
+
+// block-reduced FP64 atomic add
+__device__ __forceinline__ void block_add(double v, double *dst) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __shared__ double sh[AB / 32];
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int k = 0; k < AB / 32; ++k) s += sh[k];
+    if (s != 0.0) atomicAdd(dst, s);
+  }
+}
+
+// deposit of the particles of step `step` (created before it, not lost
+// before its push) into np, kq applied
+template <class R>
+__global__ void __launch_bounds__(AB) k_cw_deposit(Dims d, WinConst c, WinS<R> S, const int *__restrict__ count,
+                                                   int step, const double *__restrict__ kq, double *__restrict__ np) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long key = -1;
+  double v[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) v[q] = 0.0;
+  if (i < *count) {
+    const int b = S.bl[i];
+    if (born_of(b) < step && lost_of(b) >= step) {
+      int ix, iy, iz;
+      unpack_cell(S.cell[i], ix, iy, iz);
+      R w[8];
+      weights8<R>(S.p[i], S.p[S.cap + i], S.p[2 * S.cap + i], w);
+      key = d.g(ix, iy, iz);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = (double)w[q];
+    }
+  }
+  if (warp_run_sum<8>(key, v)) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const long long g = key + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
+      atomicAdd(&np[g], kq[g] * (c.kdep * v[q]));
+    }
+  }
+}
+
+// push of step `step`; a particle whose new cell is a wall cell (or outside
+// the grid) is lost at this step and keeps its state from before the push;
+// wall_acc += the kinetic energy (J) the lost macroparticles carry
+template <class R>
+__global__ void __launch_bounds__(AB) k_cw_push(Dims d, WinConst c, const void *__restrict__ E,
+                                                const unsigned char *__restrict__ cw, WinS<R> S,
+                                                const int *__restrict__ count, int step, double *wall_acc) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double wl = 0.0;
+  if (i < *count) {
+    const int b = S.bl[i];
+    if (born_of(b) <= step && lost_of(b) >= step) {
+      int ix, iy, iz;
+      unpack_cell(S.cell[i], ix, iy, iz);
+      const long long cap = S.cap;
+      R fx = S.p[i], fy = S.p[cap + i], fz = S.p[2 * cap + i];
+      R vx = S.p[3 * cap + i], vy = S.p[4 * cap + i], vz = S.p[5 * cap + i];
+      R w[8];
+      weights8<R>(fx, fy, fz, w);
+      R Ex, Ey, Ez;
+      gather_E<R>(d, E, d.g(ix, iy, iz), w, Ex, Ey, Ez);
+      boris<R>(c, Ex, Ey, Ez, vx, vy, vz);
+      const int ax = ix + move_offset<R>(fx, vx * (R)(c.dt / c.h0));
+      const int ay = iy + move_offset<R>(fy, vy * (R)(c.dt / c.h1));
+      const int az = iz + move_offset<R>(fz, vz * (R)(c.dt / c.h2));
+      const int cx = ax < 0 ? 0 : (ax > d.n1 + 1 ? d.n1 + 1 : ax);
+      const int cy = ay < 0 ? 0 : (ay > d.n2 + 1 ? d.n2 + 1 : ay);
+      const int cz = az < 0 ? 0 : (az > d.n3 + 1 ? d.n3 + 1 : az);
+      const bool lost = ax < 1 || ay < 1 || az < 1 || ax > d.n1 || ay > d.n2 || az > d.n3 || cw[d.c(cx, cy, cz)];
+      if (lost) {
+        S.bl[i] = (b & 0xffff) | (step << 16);
+        wl = 0.5 * c.Nm * c.mass * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+      } else {
+        S.cell[i] = pack_cell(ax, ay, az);
+        S.p[i] = fx;
+        S.p[cap + i] = fy;
+        S.p[2 * cap + i] = fz;
+        S.p[3 * cap + i] = vx;
+        S.p[4 * cap + i] = vy;
+        S.p[5 * cap + i] = vz;
+      }
+    }
+  }
+  block_add(wl, wall_acc);
+}
+
+// the push of step `step` undone for the particles it kept: x^n from
+// x^{n+1} and v^{n+1/2}, then v+ by the inverse rotation with E^n at x^n
+template <class R>
+__global__ void __launch_bounds__(AB) k_cw_reverse(Dims d, WinConst c, const void *__restrict__ E, WinS<R> S,
+                                                   const int *__restrict__ count, int step) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= *count) return;
+  const int b = S.bl[i];
+  if (!(born_of(b) <= step && lost_of(b) > step)) return;
+  int ix, iy, iz;
+  unpack_cell(S.cell[i], ix, iy, iz);
+  const long long cap = S.cap;
+  R fx = S.p[i], fy = S.p[cap + i], fz = S.p[2 * cap + i];
+  R vx = S.p[3 * cap + i], vy = S.p[4 * cap + i], vz = S.p[5 * cap + i];
+  ix += move_offset<R>(fx, -vx * (R)(c.dt / c.h0));
+  iy += move_offset<R>(fy, -vy * (R)(c.dt / c.h1));
+  iz += move_offset<R>(fz, -vz * (R)(c.dt / c.h2));
+  ix = ix < 1 ? 1 : (ix > d.n1 ? d.n1 : ix);
+  iy = iy < 1 ? 1 : (iy > d.n2 ? d.n2 : iy);
+  iz = iz < 1 ? 1 : (iz > d.n3 ? d.n3 : iz);
+  R w[8];
+  weights8<R>(fx, fy, fz, w);
+  R Ex, Ey, Ez;
+  gather_E<R>(d, E, d.g(ix, iy, iz), w, Ex, Ey, Ez);
+  boris_inverse<R>(c, Ex, Ey, Ez, vx, vy, vz);
+  S.cell[i] = pack_cell(ix, iy, iz);
+  S.p[i] = fx;
+  S.p[cap + i] = fy;
+  S.p[2 * cap + i] = fz;
+  S.p[3 * cap + i] = vx;
+  S.p[4 * cap + i] = vy;
+  S.p[5 * cap + i] = vz;
+}
+
+// adjoint of the push of step `step` at the state (x^n, v+) for the
+// particles it moved: lam (dJ/dx^{n+1}, dJ/dv^{n+1/2}) -> (the push's part of
+// dJ/dx^n, dJ/dv+), lE += gather^T, dBz.  A particle lost at this step has no
+// later use except the wall-flux observable: wflux Nm m v^{n+1/2}.
+template <class R>
+__global__ void __launch_bounds__(AB) k_cw_adj_push(Dims d, WinConst c, const void *__restrict__ E, WinS<R> S,
+                                                    const int *__restrict__ count, int step, double wflux,
+                                                    double *__restrict__ lE, double *dBz) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double gB = 0.0;
+  long long key = -1;
+  double sc[24];
+#pragma unroll
+  for (int q = 0; q < 24; ++q) sc[q] = 0.0;
+  if (i < *count) {
+    const int b = S.bl[i];
+    if (born_of(b) <= step && lost_of(b) >= step) {
+      const long long cap = S.cap;
+      int ix, iy, iz;
+      unpack_cell(S.cell[i], ix, iy, iz);
+      const R fx = S.p[i], fy = S.p[cap + i], fz = S.p[2 * cap + i];
+      const R vx = S.p[3 * cap + i], vy = S.p[4 * cap + i], vz = S.p[5 * cap + i];
+      R w[8];
+      weights8<R>(fx, fy, fz, w);
+      const long long g0 = d.g(ix, iy, iz);
+      R Ex, Ey, Ez;
+      gather_E<R>(d, E, g0, w, Ex, Ey, Ez);
+      R lx, ly, lz, lvx, lvy, lvz;
+      if (lost_of(b) == step) {
+        lx = ly = lz = R(0);
+        lvx = lvy = lvz = R(0);
+        if (wflux != 0.0) {
+          R ux = vx, uy = vy, uz = vz;
+          boris<R>(c, Ex, Ey, Ez, ux, uy, uz);
+          const R k = (R)(wflux * c.Nm * c.mass);
+          lvx = k * ux;
+          lvy = k * uy;
+          lvz = k * uz;
+        }
+      } else {
+        lx = S.lam[i];
+        ly = S.lam[cap + i];
+        lz = S.lam[2 * cap + i];
+        lvx = S.lam[3 * cap + i];
+        lvy = S.lam[4 * cap + i];
+        lvz = S.lam[5 * cap + i];
+      }
+      // x^{n+1} = x^n + dt v^{n+1/2}
+      const R dt = (R)c.dt, k1 = (R)c.k1, kk = (R)c.kk;
+      lvx += dt * lx;
+      lvy += dt * ly;
+      lvz += dt * lz;
+      R lEx, lEy, lEz, ux, uy, uz;
+      if (c.boris) {
+        const R Bx = (R)c.Bx, By = (R)c.By, Bz = (R)c.Bz;
+        const R v1x = vx + k1 * Ex, v1y = vy + k1 * Ey, v1z = vz + k1 * Ez;
+        const R v3x = v1x + k1 * (v1y * Bz - v1z * By), v3y = v1y + k1 * (v1z * Bx - v1x * Bz),
+                v3z = v1z + k1 * (v1x * By - v1y * Bx);
+        // d v^{n+1/2} / d Bz: v2 = v1 + kk (v3 x B), v3 = v1 + k1 (v1 x B)
+        const R ax = v3y * Bz - v3z * By, ay = v3z * Bx - v3x * Bz, az = v3x * By - v3y * Bx;   // v3 x B
+        const R bx = v1y, by = -v1x;                                                            // v1 x e_z
+        const R cx = k1 * (by * Bz), cy = k1 * (-bx * Bz), cz = k1 * (bx * By - by * Bx);     // (k1 v1 x e_z) x B
+        const R ex = v3y, ey = -v3x;                                                            // v3 x e_z
+        const R dkk = (R)c.dkk;
+        gB = (double)(lvx * (dkk * ax + kk * (cx + ex)) + lvy * (dkk * ay + kk * (cy + ey)) + lvz * (dkk * az + kk * cz));
+        lEx = k1 * lvx;
+        lEy = k1 * lvy;
+        lEz = k1 * lvz;
+        // l3 = kk (B x lv), u = lv + l3 + k1 (B x l3)
+        const R l3x = kk * (By * lvz - Bz * lvy), l3y = kk * (Bz * lvx - Bx * lvz), l3z = kk * (Bx * lvy - By * lvx);
+        ux = lvx + l3x + k1 * (By * l3z - Bz * l3y);
+        uy = lvy + l3y + k1 * (Bz * l3x - Bx * l3z);
+        uz = lvz + l3z + k1 * (Bx * l3y - By * l3x);
+        lEx += k1 * ux;
+        lEy += k1 * uy;
+        lEz += k1 * uz;
+      } else {
+        ux = lvx;
+        uy = lvy;
+        uz = lvz;
+        lEx = R(2) * k1 * lvx;
+        lEy = R(2) * k1 * lvy;
+        lEz = R(2) * k1 * lvz;
+      }
+      // gather^T (below) and the weight gradient of the gather into lx
+      const R px = R(1) - fx, py = R(1) - fy, pz = R(1) - fz;
+      const R hx = (R)(1.0 / c.h0), hy = (R)(1.0 / c.h1), hz = (R)(1.0 / c.h2);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        sc[3 * q + 0] = (double)(w[q] * lEx);
+        sc[3 * q + 1] = (double)(w[q] * lEy);
+        sc[3 * q + 2] = (double)(w[q] * lEz);
+        const R ax_ = ox(q) ? R(1) - px : px, ay_ = oy(q) ? R(1) - py : py, az_ = oz(q) ? R(1) - pz : pz;
+        const R sx = ox(q) ? hx : -hx, sy = oy(q) ? hy : -hy, sz = oz(q) ? hz : -hz;
+        R ex_, ey_, ez_;
+        node_E<R>(E, g0 + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q)), ex_, ey_, ez_);
+        const R s = ex_ * lEx + ey_ * lEy + ez_ * lEz;
+        lx += sx * ay_ * az_ * s;
+        ly += ax_ * sy * az_ * s;
+        lz += ax_ * ay_ * sz * s;
+      }
+      key = g0;
+      S.lam[i] = lx;
+      S.lam[cap + i] = ly;
+      S.lam[2 * cap + i] = lz;
+      S.lam[3 * cap + i] = ux;
+      S.lam[4 * cap + i] = uy;
+      S.lam[5 * cap + i] = uz;
+    }
+  }
+  if (warp_run_sum<24>(key, sc)) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const long long g = key + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
+      atomicAdd(&lE[3 * g + 0], sc[3 * q + 0]);
+      atomicAdd(&lE[3 * g + 1], sc[3 * q + 1]);
+      atomicAdd(&lE[3 * g + 2], sc[3 * q + 2]);
+    }
+  }
+  block_add(gB, dBz);
+}
+
+// lx += deposit^T of the adjoint potential mu for the particles deposited at
+// `step`: the deposit adds kq kdep w to np, rhs = -q np, so
+// dJ/dx += -q kdep sum_c kq mu grad w_c
+template <class R>
+__global__ void __launch_bounds__(AB) k_cw_adj_deposit(Dims d, WinConst c, WinS<R> S, const int *__restrict__ count,
+                                                       int step, const double *__restrict__ kq,
+                                                       const double *__restrict__ mu) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= *count) return;
+  const int b = S.bl[i];
+  if (!(born_of(b) < step && lost_of(b) >= step)) return;
+  int ix, iy, iz;
+  unpack_cell(S.cell[i], ix, iy, iz);
+  const long long cap = S.cap;
+  const double fx = S.p[i], fy = S.p[cap + i], fz = S.p[2 * cap + i];
+  const double px = 1.0 - fx, py = 1.0 - fy, pz = 1.0 - fz;
+  const long long g0 = d.g(ix, iy, iz);
+  double lx = 0.0, ly = 0.0, lz = 0.0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const long long g = g0 + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
+    const double s = -c.q * c.kdep * kq[g] * mu[g];
+    const double ax = ox(q) ? 1.0 - px : px, ay = oy(q) ? 1.0 - py : py, az = oz(q) ? 1.0 - pz : pz;
+    const double sx = ox(q) ? 1.0 / c.h0 : -1.0 / c.h0, sy = oy(q) ? 1.0 / c.h1 : -1.0 / c.h1,
+                 sz = oz(q) ? 1.0 / c.h2 : -1.0 / c.h2;
+    lx += sx * ay * az * s;
+    ly += ax * sy * az * s;
+    lz += ax * ay * sz * s;
+  }
+  S.lam[i] += (R)lx;
+  S.lam[cap + i] += (R)ly;
+  S.lam[2 * cap + i] += (R)lz;
+}
+
+// every species of the window, for the collision kernels
+template <class R>
+struct CwSet {
+  WinS<R> S[LEPIC_NPART];
+  int *count[LEPIC_NPART];
+  double mass[LEPIC_NPART];
+};
+
+// the recorded collisions of one step applied again (a later forward pass:
+// finite differences, the FP64 reference): each byproduct from the
+// incident's current velocity, the recorded target and directions; the
+// incident's velocity before is written back into the record
+template <class R>
+__global__ void __launch_bounds__(AB) k_cw_replay(lepic_win_event_t *ev, int ne, CwSet<R> set, double qe) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ne) return;
+  lepic_win_event_t &e = ev[k];
+  const WinS<R> A = set.S[e.P];
+  const long long i = e.i, ca = A.cap;
+  const double vx = A.p[3 * ca + i], vy = A.p[4 * ca + i], vz = A.p[5 * ca + i];
+  e.vold[0] = vx;
+  e.vold[1] = vy;
+  e.vold[2] = vz;
+  const double mp = fabs(set.mass[e.P]), mt = e.m_t, M = mp + mt, mu = mp * mt / M;
+  const double rx = vx - e.tv[0], ry = vy - e.tv[1], rz = vz - e.tv[2];
+  const double vcx = (mp * vx + mt * e.tv[0]) / M, vcy = (mp * vy + mt * e.tv[1]) / M,
+               vcz = (mp * vz + mt * e.tv[2]) / M;
+  double Ee = 0.5 * mu * (rx * rx + ry * ry + rz * rz) - e.Eth * qe;
+  if (Ee < 0.0) Ee = 0.0;
+  for (int a = 0; a < e.nby && a < 4; ++a) {
+    const int B = e.by[a];
+    if (B < 0) continue;
+    double nx, ny, nz;
+    if (e.rt == 4) {
+      if (B != e.P) continue;
+      nx = e.tv[0];
+      ny = e.tv[1];
+      nz = e.tv[2];
+    } else {
+      const double mb = fabs(set.mass[B]);
+      const double vp = sqrt(2.0 * (Ee / e.sum_mass) / (mb * mb));
+      nx = vcx + vp * e.e1[a][0];
+      ny = vcy + vp * e.e1[a][1];
+      nz = vcz + vp * e.e1[a][2];
+    }
+    const WinS<R> Bs = set.S[B];
+    long long j = e.slot[a];
+    if (j < 0) {
+      j = i;
+    } else {
+      const long long cb = Bs.cap;
+      Bs.cell[j] = A.cell[i];
+      Bs.p[j] = A.p[i];
+      Bs.p[cb + j] = A.p[ca + i];
+      Bs.p[2 * cb + j] = A.p[2 * ca + i];
+      Bs.bl[j] = (e.step & 0xffff) | (WALIVE << 16);
+      atomicMax(set.count[B], (int)j + 1);
+    }
+    const long long cb = Bs.cap;
+    Bs.p[3 * cb + j] = (R)nx;
+    Bs.p[4 * cb + j] = (R)ny;
+    Bs.p[5 * cb + j] = (R)nz;
+  }
+}
+
+// adjoint of the recorded collisions of one step, then the collisions undone
+// (the incident's velocity before them back in its slot): the byproducts'
+// dJ/dv through v_b = v_cm + vp_b e1_b (v_cm = (m_p v + m_t v_t)/(m_p + m_t),
+// vp_b from the centre-of-mass energy of v - v_t), the products' dJ/dx onto
+// the incident's position (they were created there), charge exchange
+// (v = v_t) passing nothing back
+template <class R>
+__global__ void __launch_bounds__(AB) k_cw_adj_collide(const lepic_win_event_t *ev, int ne, CwSet<R> set,
+                                                       double qe) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ne) return;
+  const lepic_win_event_t &e = ev[k];
+  const WinS<R> A = set.S[e.P];
+  const long long i = e.i, ca = A.cap;
+  const double vx = e.vold[0], vy = e.vold[1], vz = e.vold[2];
+  const double mp = fabs(set.mass[e.P]), mt = e.m_t, M = mp + mt, mu = mp * mt / M;
+  const double rx = vx - e.tv[0], ry = vy - e.tv[1], rz = vz - e.tv[2];
+  double Ee = 0.5 * mu * (rx * rx + ry * ry + rz * rz) - e.Eth * qe;
+  const bool pos = Ee > 0.0;
+  if (!pos) Ee = 0.0;
+  double gx = 0.0, gy = 0.0, gz = 0.0;   // dJ/dv before
+  double px = 0.0, py = 0.0, pz = 0.0;   // dJ/dx from the products
+  for (int a = 0; a < e.nby && a < 4; ++a) {
+    const int B = e.by[a];
+    if (B < 0) continue;
+    if (e.rt == 4 && B != e.P) continue;
+    const WinS<R> Bs = set.S[B];
+    const long long j = e.slot[a] < 0 ? i : e.slot[a], cb = Bs.cap;
+    const double lx = Bs.lam[3 * cb + j], ly = Bs.lam[4 * cb + j], lz = Bs.lam[5 * cb + j];
+    if (e.slot[a] >= 0) {
+      px += Bs.lam[j];
+      py += Bs.lam[cb + j];
+      pz += Bs.lam[2 * cb + j];
+      for (int q = 0; q < 6; ++q) Bs.lam[q * cb + j] = R(0);
+    }
+    if (e.rt == 4) continue;
+    const double mb = fabs(set.mass[B]);
+    const double vp = sqrt(2.0 * (Ee / e.sum_mass) / (mb * mb));
+    gx += (mp / M) * lx;
+    gy += (mp / M) * ly;
+    gz += (mp / M) * lz;
+    if (pos && vp > 0.0) {
+      const double el = e.e1[a][0] * lx + e.e1[a][1] * ly + e.e1[a][2] * lz;
+      const double s = el * mu / (vp * e.sum_mass * mb * mb);
+      gx += s * rx;
+      gy += s * ry;
+      gz += s * rz;
+    }
+  }
+  A.lam[i] += (R)px;
+  A.lam[ca + i] += (R)py;
+  A.lam[2 * ca + i] += (R)pz;
+  A.lam[3 * ca + i] = (R)gx;
+  A.lam[4 * ca + i] = (R)gy;
+  A.lam[5 * ca + i] = (R)gz;
+  A.p[3 * ca + i] = (R)vx;
+  A.p[4 * ca + i] = (R)vy;
+  A.p[5 * ca + i] = (R)vz;
 }
 
 }  // namespace
@@ -577,6 +1133,153 @@ int lepic_dev_adj_rhs(const lepic_grid_t *g, const double *lphi, double *b, void
   const Dims d(g->n);
   cudaStream_t s = (cudaStream_t)stream;
   lepic::k_adj_rhs<<<lepic::grid_for(d.rcnt(), 256), 256, 0, s>>>(d, g->bcnd, lphi, b);
+  LEPIC_CUDA(cudaGetLastError());
+  return LEPIC_OK;
+}
+
+int lepic_dev_cw_deposit(const lepic_grid_t *g, const lepic_win_species_t *ws, int ptype, const lepic_phys_t *P,
+                         int step, double *np, void *stream) {
+  if (!g || !ws || !P || !np || ptype < 1 || ptype > LEPIC_NPART) return LEPIC_ERR_ARG;
+  const Dims d(g->n);
+  cudaStream_t s = (cudaStream_t)stream;
+  const lepic::WinConst c = lepic::win_const(*g, *P, ptype);
+  int tm = lepic::timer_start("cw_deposit", s);
+  if (ws->fp64)
+    lepic::k_cw_deposit<double><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, lepic::win_view<double>(*ws), ws->count, step, g->kq, np);
+  else
+    lepic::k_cw_deposit<float><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, lepic::win_view<float>(*ws), ws->count, step, g->kq, np);
+  lepic::timer_stop(tm, s);
+  LEPIC_CUDA(cudaGetLastError());
+  return LEPIC_OK;
+}
+
+int lepic_dev_cw_push(const lepic_grid_t *g, const void *E, lepic_win_species_t *ws, int ptype,
+                      const lepic_phys_t *P, int step, double *wall_acc, void *stream) {
+  if (!g || !E || !ws || !P || !wall_acc || ptype < 1 || ptype > LEPIC_NPART || !g->cell_wall) return LEPIC_ERR_ARG;
+  if (P->flag_pbc || P->flag_nmn || (P->flag_B == 1 && P->Bmap)) return LEPIC_ERR_UNSUPPORTED;
+  const Dims d(g->n);
+  cudaStream_t s = (cudaStream_t)stream;
+  const lepic::WinConst c = lepic::win_const(*g, *P, ptype);
+  int tm = lepic::timer_start("cw_push", s);
+  if (ws->fp64)
+    lepic::k_cw_push<double><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, E, g->cell_wall, lepic::win_view<double>(*ws), ws->count, step, wall_acc);
+  else
+    lepic::k_cw_push<float><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, E, g->cell_wall, lepic::win_view<float>(*ws), ws->count, step, wall_acc);
+  lepic::timer_stop(tm, s);
+  LEPIC_CUDA(cudaGetLastError());
+  return LEPIC_OK;
+}
+
+int lepic_dev_cw_reverse(const lepic_grid_t *g, const void *E, lepic_win_species_t *ws, int ptype,
+                         const lepic_phys_t *P, int step, void *stream) {
+  if (!g || !E || !ws || !P || ptype < 1 || ptype > LEPIC_NPART) return LEPIC_ERR_ARG;
+  const Dims d(g->n);
+  cudaStream_t s = (cudaStream_t)stream;
+  const lepic::WinConst c = lepic::win_const(*g, *P, ptype);
+  int tm = lepic::timer_start("cw_reverse", s);
+  if (ws->fp64)
+    lepic::k_cw_reverse<double><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, E, lepic::win_view<double>(*ws), ws->count, step);
+  else
+    lepic::k_cw_reverse<float><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, E, lepic::win_view<float>(*ws), ws->count, step);
+  lepic::timer_stop(tm, s);
+  LEPIC_CUDA(cudaGetLastError());
+  return LEPIC_OK;
+}
+
+int lepic_dev_cw_adj_push(const lepic_grid_t *g, const void *E, lepic_win_species_t *ws, int ptype,
+                          const lepic_phys_t *P, int step, double wflux, double *lE, double *dBz, void *stream) {
+  if (!g || !E || !ws || !P || !lE || !dBz || ptype < 1 || ptype > LEPIC_NPART) return LEPIC_ERR_ARG;
+  const Dims d(g->n);
+  cudaStream_t s = (cudaStream_t)stream;
+  const lepic::WinConst c = lepic::win_const(*g, *P, ptype);
+  int tm = lepic::timer_start("cw_adj_push", s);
+  if (ws->fp64)
+    lepic::k_cw_adj_push<double><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, E, lepic::win_view<double>(*ws), ws->count, step, wflux, lE, dBz);
+  else
+    lepic::k_cw_adj_push<float><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, E, lepic::win_view<float>(*ws), ws->count, step, wflux, lE, dBz);
+  lepic::timer_stop(tm, s);
+  LEPIC_CUDA(cudaGetLastError());
+  return LEPIC_OK;
+}
+
+int lepic_dev_cw_adj_deposit(const lepic_grid_t *g, lepic_win_species_t *ws, int ptype, const lepic_phys_t *P,
+                             int step, const double *mu, void *stream) {
+  if (!g || !ws || !P || !mu || ptype < 1 || ptype > LEPIC_NPART) return LEPIC_ERR_ARG;
+  const Dims d(g->n);
+  cudaStream_t s = (cudaStream_t)stream;
+  const lepic::WinConst c = lepic::win_const(*g, *P, ptype);
+  int tm = lepic::timer_start("cw_adj_deposit", s);
+  if (ws->fp64)
+    lepic::k_cw_adj_deposit<double><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, lepic::win_view<double>(*ws), ws->count, step, g->kq, mu);
+  else
+    lepic::k_cw_adj_deposit<float><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, lepic::win_view<float>(*ws), ws->count, step, g->kq, mu);
+  lepic::timer_stop(tm, s);
+  LEPIC_CUDA(cudaGetLastError());
+  return LEPIC_OK;
+}
+
+extern "C++" {
+template <class R>
+static lepic::CwSet<R> cw_set(lepic_win_species_t *ws, int ntype, const lepic_phys_t &P) {
+  lepic::CwSet<R> set;
+  memset(&set, 0, sizeof(set));
+  for (int p = 0; p < ntype; ++p) {
+    set.S[p] = lepic::win_view<R>(ws[p]);
+    set.count[p] = ws[p].count;
+  }
+  for (int p = 0; p < LEPIC_NPART; ++p) set.mass[p] = P.mass[p];
+  return set;
+}
+
+static bool cw_uniform(const lepic_win_species_t *ws, int ntype) {
+  for (int p = 1; p < ntype; ++p)
+    if (ws[p].fp64 != ws[0].fp64) return false;
+  return true;
+}
+}  // extern "C++"
+
+int lepic_dev_cw_replay(const lepic_grid_t *g, lepic_win_species_t *ws, int ntype, const lepic_phys_t *P,
+                        lepic_win_event_t *events, int ne, void *stream) {
+  if (!g || !ws || !P || ntype < 1 || ntype > LEPIC_NPART || ne < 0 || (ne > 0 && !events) ||
+      !cw_uniform(ws, ntype))
+    return LEPIC_ERR_ARG;
+  if (ne == 0) return LEPIC_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (ws[0].fp64)
+    lepic::k_cw_replay<double><<<lepic::grid_for(ne, lepic::AB), lepic::AB, 0, s>>>(
+        events, ne, cw_set<double>(ws, ntype, *P), P->qe);
+  else
+    lepic::k_cw_replay<float><<<lepic::grid_for(ne, lepic::AB), lepic::AB, 0, s>>>(
+        events, ne, cw_set<float>(ws, ntype, *P), P->qe);
+  LEPIC_CUDA(cudaGetLastError());
+  return LEPIC_OK;
+}
+
+int lepic_dev_cw_adj_collide(const lepic_grid_t *g, lepic_win_species_t *ws, int ntype, const lepic_phys_t *P,
+                             const lepic_win_event_t *events, int ne, void *stream) {
+  if (!g || !ws || !P || ntype < 1 || ntype > LEPIC_NPART || ne < 0 || (ne > 0 && !events) ||
+      !cw_uniform(ws, ntype))
+    return LEPIC_ERR_ARG;
+  if (ne == 0) return LEPIC_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  int tm = lepic::timer_start("cw_adj_collide", s);
+  if (ws[0].fp64)
+    lepic::k_cw_adj_collide<double><<<lepic::grid_for(ne, lepic::AB), lepic::AB, 0, s>>>(
+        events, ne, cw_set<double>(ws, ntype, *P), P->qe);
+  else
+    lepic::k_cw_adj_collide<float><<<lepic::grid_for(ne, lepic::AB), lepic::AB, 0, s>>>(
+        events, ne, cw_set<float>(ws, ntype, *P), P->qe);
+  lepic::timer_stop(tm, s);
   LEPIC_CUDA(cudaGetLastError());
   return LEPIC_OK;
 }

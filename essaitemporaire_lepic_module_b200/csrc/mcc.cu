@@ -86,6 +86,10 @@ struct MCCConst {
   int ixl[LEPIC_NM_RG], ixr[LEPIC_NM_RG], iyl, iyr, izl, izr;
   double w_rg[LEPIC_NM_RG];     // 1 / np_tot_rg(ptype, i_rg)
   double h0, h1, h2;
+  // event log of the differentiable window (nullptr: not recorded)
+  lepic_win_event_t *log;
+  int *nlog;
+  int log_cap, step;
   // energy and source bookkeeping of the drop-in path (RegionCount)
   double *ploss3;
   int *sxy, *sxz;
@@ -128,6 +132,7 @@ struct AccF64 {
     iy = (int)(q[cap[P] + i] / c.h1) + 1;
     iz = (int)(q[2 * cap[P] + i] / c.h2) + 1;
   }
+  __device__ bool live(int, long long) const { return true; }
 };
 
 // mixed layout: cell + FP32 offsets and velocities
@@ -165,6 +170,57 @@ struct AccMixed {
     ix = (cc & (LEPIC_CELL_MAX - 1)) + 1;
     iy = ((cc >> LEPIC_CELL_BITS) & (LEPIC_CELL_MAX - 1)) + 1;
     iz = (cc >> (2 * LEPIC_CELL_BITS)) + 1;
+  }
+  __device__ bool live(int, long long) const { return true; }
+};
+
+// the differentiable window's particles (lepic_win_species_t): the mixed
+// layout in FP32 or FP64 planes, slots kept, the window history in bl; a
+// particle takes part in the collisions of `step` when it is not lost and
+// was not created by them
+constexpr int WIN_ALIVE = 0x7fff;
+template <class T>
+struct AccWin {
+  int *cell[LEPIC_NPART];
+  T *p[LEPIC_NPART];
+  int *bl[LEPIC_NPART];
+  int *count[LEPIC_NPART];
+  long long cap[LEPIC_NPART];
+  int step;
+  __device__ void load_v(int P, long long i, double &vx, double &vy, double &vz) const {
+    const T *q = p[P];
+    vx = q[3 * cap[P] + i];
+    vy = q[4 * cap[P] + i];
+    vz = q[5 * cap[P] + i];
+  }
+  __device__ void store_v(int P, long long i, double vx, double vy, double vz) const {
+    T *q = p[P];
+    q[3 * cap[P] + i] = (T)vx;
+    q[4 * cap[P] + i] = (T)vy;
+    q[5 * cap[P] + i] = (T)vz;
+  }
+  __device__ void append(int P, long long i, int B, long long j, double vx, double vy, double vz) const {
+    const T *s = p[P];
+    T *d = p[B];
+    const long long cs = cap[P], cb = cap[B];
+    cell[B][j] = cell[P][i];
+    d[j] = s[i];
+    d[cb + j] = s[cs + i];
+    d[2 * cb + j] = s[2 * cs + i];
+    d[3 * cb + j] = (T)vx;
+    d[4 * cb + j] = (T)vy;
+    d[5 * cb + j] = (T)vz;
+    bl[B][j] = (step & 0xffff) | (WIN_ALIVE << 16);
+  }
+  __device__ void cell_of(const MCCConst &c, int P, long long i, int &ix, int &iy, int &iz) const {
+    const int cc = cell[P][i];
+    ix = (cc & (LEPIC_CELL_MAX - 1)) + 1;
+    iy = ((cc >> LEPIC_CELL_BITS) & (LEPIC_CELL_MAX - 1)) + 1;
+    iz = (cc >> (2 * LEPIC_CELL_BITS)) + 1;
+  }
+  __device__ bool live(int P, long long i) const {
+    const int b = bl[P][i];
+    return (b >> 16) == WIN_ALIVE && (short)(b & 0xffff) < step;
   }
 };
 
@@ -462,7 +518,7 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
       for (int r = 0; r < c.nr; ++r) sum_nu += nu_of(r);
       if (DSMC && missed && rd.first) atomicAdd(&D.stat[0], (unsigned long long)__popc(missed));
       const double u = u01(r0.y);
-      if (u <= sum_nu) {
+      if (u <= sum_nu && S.live(P, i)) {
         double s = 0.0;
         cur_tt = -1;
         for (int r = 0; r < c.nr; ++r) {
@@ -488,6 +544,35 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
         const int rt = c.R[sel].rt;
         const int T = c.R[sel].tt - 1;
         const double mu_t = ts.mu, vr_t = ts.vr, vxc = ts.vxc, vyc = ts.vyc, vzc = ts.vzc;
+        // the window's record of this collision
+        lepic_win_event_t *ev = nullptr;
+        if (c.log) {
+          const int k = atomicAdd(c.nlog, 1);
+          if (k < c.log_cap) {
+            ev = c.log + k;
+            ev->step = c.step;
+            ev->P = P;
+            ev->i = (int)i;
+            ev->r = sel;
+            ev->rt = rt;
+            ev->nby = c.R[sel].n_by;
+            ev->ind = c.R[sel].ind;
+            ev->tv[0] = ts.tvx;
+            ev->tv[1] = ts.tvy;
+            ev->tv[2] = ts.tvz;
+            ev->vold[0] = vx0;
+            ev->vold[1] = vy0;
+            ev->vold[2] = vz0;
+            ev->m_t = fabs(c.mass[T]);
+            ev->Eth = c.R[sel].Eth;
+            for (int a = 0; a < MAXBY; ++a) {
+              ev->by[a] = -1;
+              ev->slot[a] = -1;
+            }
+          } else {
+            raise_err(err, LEPIC_ERR_CAPACITY, -1);
+          }
+        }
         // P_loss(3, B) += the kinetic energy change of a particle of species
         // B set to (nx, ny, nz) from a speed squared of o2 (0: created)
         auto energy = [&](int B, double nx, double ny, double nz, double o2) {
@@ -505,6 +590,7 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
           for (int a = 0; a < c.R[sel].n_by; ++a) {
             const int bt = c.R[sel].by[a];
             if (c.mass[bt - 1] <= 0) continue;
+            if (ev && bt == c.ptype) ev->by[a] = bt - 1;
             if (bt == c.ptype) {
               if (c.ploss3) energy(P, ts.tvx, ts.tvy, ts.tvz, speed2(P, i));
               S.store_v(P, i, ts.tvx, ts.tvy, ts.tvz);
@@ -522,6 +608,7 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
           const int nby = c.R[sel].n_by;
           double sum_mass = 0.0;
           for (int a = 0; a < nby; ++a) sum_mass = sum_mass + 1.0 / fabs(c.mass[c.R[sel].by[a] - 1]);
+          if (ev) ev->sum_mass = sum_mass;
           const double th_add = 2.0 * c.pi / (double)nby;
           const double cos_th = 1.0 - 2.0 * u01(r0.z);
           double th = acos(cos_th);
@@ -542,6 +629,12 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
             scatter(ex1, ey1, ez1, ex, ey, ez, cos_th_s, phi_s);
             const int bt = c.R[sel].by[a];
             if (c.mass[bt - 1] <= 0) continue;
+            if (ev) {
+              ev->by[a] = bt - 1;
+              ev->e1[a][0] = (float)ex1;
+              ev->e1[a][1] = (float)ey1;
+              ev->e1[a][2] = (float)ez1;
+            }
             const double mb = fabs(c.mass[bt - 1]);
             const double vp = sqrt(2.0 * (Ee / sum_mass) / (mb * mb));
             const double nvx = vxc + vp * ex1, nvy = vyc + vp * ey1, nvz = vzc + vp * ez1;
@@ -562,6 +655,7 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
                 raise_err(err, LEPIC_ERR_CAPACITY, B);
               } else {
                 S.append(P, i, B, j, nvx, nvy, nvz);
+                if (ev) ev->slot[a] = (int)j;
                 energy(B, nvx, nvy, nvz, 0.0);
                 if (c.sxy) {
                   // the new particle's source count on the two plot planes
@@ -619,11 +713,19 @@ __global__ void k_mcc_finalize(Counts C, const int *add, int ntype) {
 
 // Host part shared by both layouts: nu_max, Pmax and the per-species
 // constants (Src/collisions.f90:97-165).
+// The differentiable window's collisions: the log they are recorded in.
+struct WinLog {
+  lepic_win_event_t *log;
+  int *nlog;   // device int: records written (continues across calls)
+  int cap, step;
+};
+
 template <class Acc>
 int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed char *const *flag_dead,
                    int ntype, const lepic_tables_t &T, const lepic_phys_t &P, unsigned long long seed,
                    unsigned long long call_index, double *nu_max, long long *counts, cudaStream_t s,
-                   const RegionCount *rg, const char *tname, lepic_targets_t *tg, int tile) {
+                   const RegionCount *rg, const char *tname, lepic_targets_t *tg, int tile,
+                   const WinLog *wlog = nullptr) {
   if (ntype < 1 || ntype > LEPIC_NPART) return LEPIC_ERR_ARG;
   // DSMC state: density grids and sort offsets from the caller, claims here
   Targets D;
@@ -695,6 +797,17 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
         return LEPIC_ERR_UNSUPPORTED;
       }
       const int tt = CI(ind, 2 + n_re);
+      if (wlog) {
+        // the window keeps every particle's slot: no charged targets, and
+        // the incident survives (elastic, excitation, charge exchange, or
+        // a reaction whose first byproduct is the incident's species)
+        const int rt = CI(ind, 3 + n_re + n_by);
+        const bool kept = rt == 1 || rt == 3 || rt == 4 || (n_by > 0 && CI(ind, 3 + n_re) == p);
+        if (P.charge[tt - 1] != 0.0 || !kept) {
+          fprintf(stderr, "lepic_gpu: window collisions: reaction %d (charged target or incident removed)\n", ind);
+          return LEPIC_ERR_UNSUPPORTED;
+        }
+      }
       if (P.charge[tt - 1] != 0.0 && tt == p) {
         // the incident would have to be claimed as well as its target
         fprintf(stderr, "lepic_gpu: collisions: reaction %d has a charged target of the incident's own species\n",
@@ -745,6 +858,12 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
     c.h0 = g.h[0];
     c.h1 = g.h[1];
     c.h2 = g.h[2];
+    if (wlog) {
+      c.log = wlog->log;
+      c.nlog = wlog->nlog;
+      c.log_cap = wlog->cap;
+      c.step = wlog->step;
+    }
     double *cc = nullptr;
     if (rg && rg->cnt_col_dev) {
       c.n_rg = rg->n_rg;
@@ -906,7 +1025,46 @@ int launch_collisions_mixed(const lepic_grid_t &g, lepic_species_mixed_t *sp, in
                         "mcc_mixed", tg, 1);
 }
 
+// the differentiable window's collisions, recorded in the log (ws in FP32 or
+// FP64 planes, fp64 taken from ws[0])
+template <class R>
+int run_window_collisions(const lepic_grid_t &g, lepic_win_species_t *ws, int ntype, const lepic_tables_t &T,
+                          const lepic_phys_t &P, unsigned long long seed, unsigned long long call_index,
+                          double *nu_max, long long *counts, const WinLog &wl, cudaStream_t s) {
+  AccWin<R> S;
+  memset(&S, 0, sizeof(S));
+  int *cnts[LEPIC_NPART] = {nullptr};
+  signed char *fd[LEPIC_NPART] = {nullptr};
+  for (int p = 0; p < ntype; ++p) {
+    S.cell[p] = ws[p].cell;
+    S.p[p] = (R *)ws[p].p;
+    S.bl[p] = ws[p].bl;
+    S.count[p] = ws[p].count;
+    S.cap[p] = ws[p].cap;
+    cnts[p] = ws[p].count;
+  }
+  S.step = wl.step;
+  return run_collisions(g, S, cnts, fd, ntype, T, P, seed, call_index, nu_max, counts, s, nullptr,
+                        ws[0].fp64 ? "mcc_window_f64" : "mcc_window", nullptr, 1, &wl);
+}
+
 }  // namespace lepic
+
+extern "C" int lepic_dev_win_collisions(const lepic_grid_t *g, lepic_win_species_t *ws, int ntype,
+                                        const lepic_tables_t *T, const lepic_phys_t *P, unsigned long long seed,
+                                        unsigned long long call_index, int step, lepic_win_event_t *log,
+                                        int log_cap, int *nlog, double *nu_max, long long *counts, void *stream) {
+  if (!g || !ws || !T || !P || !log || !nlog || ntype < 1 || ntype > LEPIC_NPART || log_cap < 0 || step < 0)
+    return LEPIC_ERR_ARG;
+  for (int p = 1; p < ntype; ++p)
+    if (ws[p].fp64 != ws[0].fp64) return LEPIC_ERR_ARG;
+  lepic::WinLog wl{log, nlog, log_cap, step};
+  if (ws[0].fp64)
+    return lepic::run_window_collisions<double>(*g, ws, ntype, *T, *P, seed, call_index, nu_max, counts, wl,
+                                                (cudaStream_t)stream);
+  return lepic::run_window_collisions<float>(*g, ws, ntype, *T, *P, seed, call_index, nu_max, counts, wl,
+                                             (cudaStream_t)stream);
+}
 
 extern "C" int lepic_dev_collisions_mixed(const lepic_grid_t *g, lepic_species_mixed_t *sp, int ntype,
                                           const lepic_tables_t *T, const lepic_phys_t *P,

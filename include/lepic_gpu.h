@@ -581,6 +581,46 @@ int lepic_dev_collisions_mixed_targets(const lepic_grid_t *g, lepic_species_mixe
                                        unsigned long long call_index, double *nu_max, long long *counts,
                                        lepic_targets_t *tg, void *stream);
 
+/* Differentiable window of the collisional step (no counterpart in the
+ * reference).  The particles of each species keep their slots for the whole
+ * window, in the mixed layout (packed cell, offsets in [0,1) and velocities as
+ * six planes of `cap`, FP32 or FP64): lam holds the adjoint (d J / d x in
+ * J per m for x, y, z, d J / d v for vx, vy, vz), bl the particle's window
+ * history: born = (short)(bl & 0xffff) the step whose collisions created it
+ * (-1: present at the start), lost = bl >> 16 the step whose push took it to
+ * a wall (0x7fff: not lost).  A lost particle keeps its state from before that
+ * push. */
+typedef struct {
+  int *cell;
+  void *p;
+  void *lam;
+  int *bl;
+  int *count;             /* device int                                       */
+  int cap;
+  int fp64;               /* 1: p and lam are double planes, 0: float         */
+} lepic_win_species_t;
+
+/* One collision of the window's MCC (neutral targets), recorded by the
+ * forward pass and replayed by later passes: the incident (species P, slot i)
+ * collided at `step` through reaction `r` (position in the species' list;
+ * `ind` the global 1-based index, `rt` its type) with a target of velocity
+ * tv and mass m_t; vold is the incident's velocity before.  Byproduct a of
+ * species by[a] (-1: not a particle, a neutral) got the velocity
+ * v_cm + vp e1[a], vp = sqrt(2 (E_cm - Eth) / sum_mass) / |m_b|, and lives in
+ * slot[a] (-1: the incident itself). */
+typedef struct {
+  int step, P, i, r;
+  int rt, nby, ind, pad;
+  int by[4];
+  int slot[4];
+  float e1[4][3];
+  double tv[3];
+  double vold[3];
+  double m_t, Eth;
+  double sum_mass;        /* sum over the byproducts of 1 / |mass|            */
+  double pad2;
+} lepic_win_event_t;
+
 /* GPU particle loader (counterpart of Src/load_part.f90:91-194 for the
  * large workloads): n_per_species samples, positions uniform in
  * [0,x_load) x [0,ymax) x [0,zmax) outside all-wall cells, shared by all
@@ -633,6 +673,50 @@ int lepic_dev_adj_efield(const lepic_grid_t *g, double *lE, double *lphi, void *
 int lepic_dev_adj_rhs(const lepic_grid_t *g, const double *lphi, double *b, void *stream);
 int lepic_dev_adj_walls(const lepic_grid_t *g, const lepic_phys_t *P, int ptype, const double *lphi,
                         const double *mu, double *lnp, double *dV, int nlabel, void *stream);
+
+/* The differentiable window of the collisional step (no counterpart in the
+ * reference; the forward operations are those of the step loop:
+ * Src/part_expmover.f90:89-250, 570-686, Src/collisions.f90:437-998), one
+ * species per call, FP32 or FP64 planes (ws->fp64).  Step n: deposit, field
+ * solve, E^n, collisions, push.  E: the FP32 node field (float4 per node,
+ * lepic_dev_pack_e32) for FP32 planes, the FP64 field (3 per node) for FP64.
+ *   cw_deposit:     np += the CIC charge of the particles of step n (created
+ *                   before it, not lost before its push), kq applied.
+ *   cw_push:        gather + Boris + leapfrog of step n; a particle reaching a
+ *                   wall cell is lost at n (it keeps its state from before the
+ *                   push) and *wall_acc += its kinetic energy (J, weight Nm).
+ *   cw_reverse:     the push of step n undone for the particles it kept
+ *                   (x^n = x^{n+1} - dt v^{n+1/2}, inverse rotation with E^n).
+ *   cw_adj_push:    adjoint of the push of step n at (x^n, v+): lam from
+ *                   (dJ/dx^{n+1}, dJ/dv^{n+1/2}) to the push's part of dJ/dx^n
+ *                   and dJ/dv+; lE += gather^T (device (3,(n+3)^3)), *dBz +=;
+ *                   a particle lost at n starts from wflux Nm m v^{n+1/2}.
+ *   cw_adj_deposit: lam(x) += -q kdep sum kq mu grad w for the particles
+ *                   deposited at step n (mu: the adjoint potential).
+ * The collisions of step n (neutral targets only; the incident survives
+ * every reaction) are drawn by lepic_dev_win_collisions, which records each
+ * in log (the step's records continue at *nlog, at most log_cap), or applied
+ * again from records by cw_replay (which writes the incident's velocity
+ * before into vold); cw_adj_collide is the records' adjoint, after which the
+ * incidents hold their velocities before again. */
+int lepic_dev_cw_deposit(const lepic_grid_t *g, const lepic_win_species_t *ws, int ptype, const lepic_phys_t *P,
+                         int step, double *np, void *stream);
+int lepic_dev_cw_push(const lepic_grid_t *g, const void *E, lepic_win_species_t *ws, int ptype,
+                      const lepic_phys_t *P, int step, double *wall_acc, void *stream);
+int lepic_dev_cw_reverse(const lepic_grid_t *g, const void *E, lepic_win_species_t *ws, int ptype,
+                         const lepic_phys_t *P, int step, void *stream);
+int lepic_dev_cw_adj_push(const lepic_grid_t *g, const void *E, lepic_win_species_t *ws, int ptype,
+                          const lepic_phys_t *P, int step, double wflux, double *lE, double *dBz, void *stream);
+int lepic_dev_cw_adj_deposit(const lepic_grid_t *g, lepic_win_species_t *ws, int ptype, const lepic_phys_t *P,
+                             int step, const double *mu, void *stream);
+int lepic_dev_win_collisions(const lepic_grid_t *g, lepic_win_species_t *ws, int ntype, const lepic_tables_t *T,
+                             const lepic_phys_t *P, unsigned long long seed, unsigned long long call_index, int step,
+                             lepic_win_event_t *log, int log_cap, int *nlog, double *nu_max, long long *counts,
+                             void *stream);
+int lepic_dev_cw_replay(const lepic_grid_t *g, lepic_win_species_t *ws, int ntype, const lepic_phys_t *P,
+                        lepic_win_event_t *events, int ne, void *stream);
+int lepic_dev_cw_adj_collide(const lepic_grid_t *g, lepic_win_species_t *ws, int ntype, const lepic_phys_t *P,
+                             const lepic_win_event_t *events, int ne, void *stream);
 int lepic_dev_adj_deposit(const lepic_grid_t *g, const double *p, int cap, int n, const signed char *alive,
                           const double *lnp, double *lam, int lcap, int ptype, const lepic_phys_t *P,
                           void *stream);

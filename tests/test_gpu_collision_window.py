@@ -1,0 +1,140 @@
+"""The differentiable window of the collisional step (adjoint.CollisionWindow):
+electrons and Ar+ of a Penning-like box (16x16x32 cells, end plates at
+200 V, B_z = 0.1 T) with the Ar null-collision MCC (elastic, excitation,
+ionization, charge exchange) every 4 steps of a 12-step window, the
+collisions recorded by the first forward pass and replayed by every later
+one.
+
+Bars:
+  * the backward pass undoes the window: after it the particles are back at
+    their initial state (cells equal, offsets within 1e-5, velocities within
+    1e-4 of the species' largest speed; FP32 rounding of the reversed pushes);
+  * the FP64 adjoint (the same events, FP64 particles and multigrid) against
+    central finite differences of the FP64 window (events replayed):
+    dJ/dV per wall label and dJ/dB_z within 1e-4, a directional derivative in
+    the initial velocities within 1e-3, for the mean electron energy and the
+    probe potential at the box centre;
+  * the mixed-precision adjoint (FP32 particles and pushes, FP32 V-cycles in
+    FP64 refinement) within 1e-4 of the FP64 adjoint for all three
+    observables (energy, probe potential, wall energy flux);
+  * the torch.autograd.Function returns the window's own gradients.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from tests.conftest import have_gpu
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not have_gpu(), reason="needs a CUDA GPU")]
+
+
+@pytest.fixture(scope="module")
+def windows():
+    import torch
+    from essaitemporaire_lepic_module_b200 import config
+    from essaitemporaire_lepic_module_b200.adjoint import CollisionWindow
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    wl = dataclasses.replace(config.workload("penning_small"), name="mccpen16",
+                             ions=[("[Ar+]", 39.95, 1.0, 0.026, 1.0)], gas_pressure=20.0)
+    st = config.build(wl)
+    sim = Simulation(st, precision="mixed", seed=7)
+    sim.load_uniform()
+    for _ in range(3):
+        sim.step()
+    torch.cuda.synchronize()
+    w64 = CollisionWindow(sim, K=12, ns_coll=4, fp64=True, keep_initial=True)
+    w32 = CollisionWindow(sim, K=12, ns_coll=4, keep_initial=True)
+    V = [float(st.wl.V[lab]) for lab in range(1, st.geom.ngrid + 1)]
+    Bz = float(st.Bconst[2])
+    w32.forward(V, Bz)                  # records the collisions
+    w64.use_log_of(w32)
+    return st, w32, w64, V, Bz
+
+
+def _close(a, b, rel):
+    a, b = np.atleast_1d(a), np.atleast_1d(b)
+    scale = max(np.abs(b).max(), 1e-300)
+    return np.abs(a - b).max() <= rel * scale
+
+
+def test_events_recorded(windows):
+    st, w32, _, _, _ = windows
+    assert len(w32.ev_range) == 3                         # steps 1, 5, 9
+    assert all(b - a > 1000 for a, b in w32.ev_range.values())
+    T = st.tables
+    types = {int(T.col_info[c, 2 + T.col_info[c, 0] + T.col_info[c, 1]]) for c in range(T.sig.shape[0])
+             if w32.counts[c] > 0}
+    assert types == {1, 3, 2, 4}, types                   # elastic, excitation, ionization, charge exchange
+
+
+def test_backward_returns_to_the_initial_state(windows):
+    _, w32, _, V, Bz = windows
+    w32.forward(V, Bz, observable="energy")
+    w32.backward()
+    for p, (c0, p0, _) in enumerate(w32.initial):
+        n = w32.count0[p]
+        d = w32.stores[p]
+        x = (d["cell"][:n] & 1023).double() + d["p"][0, :n].double()
+        x0 = (c0[:n] & 1023).double() + p0[0, :n].double()
+        assert float((x - x0).abs().max()) <= 1e-5
+        vmax = float(p0[3:6, :n].abs().max())
+        assert float((d["p"][3:6, :n] - p0[3:6, :n]).abs().max()) <= 1e-4 * vmax
+
+
+@pytest.mark.parametrize("observable", ["energy", "probe"])
+def test_fp64_adjoint_vs_central_differences(windows, observable):
+    import torch
+    _, _, w64, V, Bz = windows
+    w64.forward(V, Bz, observable=observable)
+    gV, gB, gv = w64.backward()
+    fd = []
+    for lab in range(len(V)):
+        Vp, Vm = list(V), list(V)
+        Vp[lab] += 1e-3
+        Vm[lab] -= 1e-3
+        fd.append((w64.forward(Vp, Bz, observable=observable) - w64.forward(Vm, Bz, observable=observable)) / 2e-3)
+    assert _close(gV, np.array(fd), 1e-4), (gV, fd)
+    fB = (w64.forward(V, Bz + 1e-6, observable=observable) - w64.forward(V, Bz - 1e-6, observable=observable)) / 2e-6
+    assert _close(gB, fB, 1e-4), (gB, fB)
+    torch.manual_seed(0)
+    n0 = w64.count0[0]
+    dv = torch.randn((3, n0), dtype=torch.float64, device="cuda")
+    v0 = w64.initial[0][1][3:6, :n0].clone()
+    fv = (w64.forward(V, Bz, v0=v0 + dv, observable=observable)
+          - w64.forward(V, Bz, v0=v0 - dv, observable=observable)) / 2.0
+    assert _close(float((gv * dv).sum()), fv, 1e-3), (float((gv * dv).sum()), fv)
+
+
+@pytest.mark.parametrize("observable", ["energy", "probe", "flux"])
+def test_mixed_adjoint_vs_fp64_adjoint(windows, observable):
+    import torch
+    _, w32, w64, V, Bz = windows
+    J32 = w32.forward(V, Bz, observable=observable)
+    g32 = w32.backward()
+    J64 = w64.forward(V, Bz, observable=observable)
+    g64 = w64.backward()
+    assert abs(J32 - J64) <= 1e-4 * abs(J64)
+    assert _close(g32[0], g64[0], 1e-4), (g32[0], g64[0])
+    assert _close(g32[1], g64[1], 1e-4), (g32[1], g64[1])
+    torch.manual_seed(1)
+    dv = torch.randn(g64[2].shape, dtype=torch.float64, device="cuda")
+    assert _close(float((g32[2] * dv).sum()), float((g64[2] * dv).sum()), 1e-4)
+    # backward no dearer than 3 forward passes of the window
+    assert w32.timing["backward_ms"] <= 3.0 * w32.timing["forward_ms"] + 5.0
+
+
+def test_autograd_function(windows):
+    import torch
+    from essaitemporaire_lepic_module_b200.adjoint import collision_window_objective
+    _, w32, _, V, Bz = windows
+    Vt = torch.tensor(V, dtype=torch.float64, requires_grad=True)
+    Bt = torch.tensor(Bz, dtype=torch.float64, requires_grad=True)
+    v0 = w32.initial[0][1][3:6, :w32.count0[0]].to(torch.float64).clone().requires_grad_(True)
+    J = collision_window_objective(w32, Vt, Bt, v0, observable="probe")
+    J.backward()
+    gV, gB, gv = w32.backward()
+    np.testing.assert_allclose(Vt.grad.numpy(), gV, rtol=1e-12, atol=0)
+    assert float(Bt.grad) == pytest.approx(gB, rel=1e-12)
+    assert torch.allclose(v0.grad, gv, rtol=1e-6, atol=0)
