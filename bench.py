@@ -34,7 +34,11 @@ large:  the large mixed-precision configuration (192^3 cells, e- + Ar+ at 128
         ppc = 2 x 9.06e8 FP32 particles, the MCC of the 128^3 workload; the
         FP64 form does not fit in HBM): after 3 warm-up steps, 500 steps timed
         with CUDA events as one region (50 electron sorts and 50 MCC calls),
-        with its roofline, clocks and phi error against the FP64 multigrid.
+        with its roofline, clocks and phi error against the FP64 multigrid;
+        then the differentiable window of the next 32 steps (collisions
+        recorded and replayed): the gradient of the potential at the box
+        centre after them with respect to the wall potential, B_z and the
+        electrons' initial velocities, forward and backward times.
 adjoint: forward and backward time of the differentiable K-step window on the
         Penning workload (96x96x192, 5.7e7 electrons, K = 64, checkpoints every
         8 steps): gradient of the final mean electron energy with respect to the
@@ -474,7 +478,49 @@ def run_large(args):
            "kernel_ms": {k: round(v[0], 3) for k, v in sorted(timers.items())},
            "kernel_launches": {k: v[1] for k, v in sorted(timers.items())},
            "clocks": R["clocks"]}
+    if args.large_adjoint:
+        out["adjoint"] = run_window_adjoint(R["sim"], st, K=32, observable="probe",
+                                            production_ms_per_step=R["ms"] / a.steps)
     del R
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_window_adjoint(sim, st, K, observable, production_ms_per_step):
+    """The differentiable window of the collisional step over the next K steps
+    of `sim` (mixed form, in place): the first forward records the collisions,
+    the backward replays them; gradient of the observable with respect to the
+    wall potentials, B_z and the electrons' initial velocities."""
+    import torch
+    from essaitemporaire_lepic_module_b200 import _lib
+    from essaitemporaire_lepic_module_b200.adjoint import CollisionWindow
+    win = CollisionWindow(sim, K=K)
+    V = [float(st.wl.V[lab]) if lab < len(st.wl.V) else 0.0 for lab in range(1, win.nlabel + 1)]
+    Bz = float(st.Bconst[2])
+    _lib.timing(enable=True)
+    _lib.timing(reset=True)
+    J = win.forward(V, Bz, observable=observable)
+    fwd = _lib.timing()
+    _lib.timing(reset=True)
+    gV, gB, gv = win.backward()
+    bwd = _lib.timing()
+    _lib.timing(enable=False)
+    t = dict(win.timing)
+    events = sum(b - a for a, b in win.ev_range.values())
+    out = {"window": f"{K} steps after the timed run, {win.ntype} species, {sum(win.count0)} particles (FP32, "
+                     f"slots kept), MCC every {win.ns_coll} steps with {events} collisions recorded and replayed, "
+                     f"no particle checkpoints (pushes and collisions undone in the backward pass)",
+           "observable": {"probe": "phi at the box centre after the window (V)",
+                          "energy": "mean electron kinetic energy after the window (eV)",
+                          "flux": "kinetic energy carried to the walls in the window (J)"}[observable],
+           "J": J, "dJ_dV_by_label": [float(x) for x in gV], "dJ_dBz": gB, "dJ_dv0_norm": float(gv.norm()),
+           "forward_ms": t["forward_ms"], "backward_ms": t["backward_ms"],
+           "backward_over_forward": t["backward_ms"] / t["forward_ms"],
+           "production_forward_ms": production_ms_per_step * K,
+           "backward_over_production_forward": t["backward_ms"] / (production_ms_per_step * K),
+           "forward_kernel_ms": {k: round(v[0], 3) for k, v in sorted(fwd.items())},
+           "backward_kernel_ms": {k: round(v[0], 3) for k, v in sorted(bwd.items())}}
+    del win
     torch.cuda.empty_cache()
     return out
 
@@ -670,6 +716,8 @@ def main():
                     help="skip the large mixed-precision configuration (192^3, 2 x 9.06e8 particles)")
     ap.add_argument("--large-workload", default="mcc192")
     ap.add_argument("--large-steps", type=int, default=500)
+    ap.add_argument("--no-large-adjoint", dest="large_adjoint", action="store_false",
+                    help="skip the differentiable window after the large run")
     ap.add_argument("--no-poisson", dest="poisson", action="store_false",
                     help="skip the Poisson stress measurement")
     ap.add_argument("--poisson-workload", default="poisson256")

@@ -321,7 +321,14 @@ class CollisionWindow:
         self.centre = (n3 // 2 + 1, n2 // 2 + 1, n1 // 2 + 1)
         self.phis = torch.empty((self.K + 1,) + tuple(sim.phi.shape), dtype=torch.float64, device=self.dev)
         self.wall_acc = torch.zeros(self.ntype, dtype=torch.float64, device=self.dev)
-        cap = log_cap or max(4096, int(0.05 * sum(self.count0) * max(1, self.K // self.ns_coll + 1)))
+        # records: about 0.35 % of the particles collide per call at 1 Pa (the
+        # electrons' null-collision probability is 1.4 %); the default leaves
+        # room for 3 % per call, at most 8 GB of records (a call that finds
+        # the log full raises LEPIC_ERR_CAPACITY)
+        calls = sum(1 for n in range(self.K) if (self.first_it + n) > 1
+                    and (self.first_it + n) % self.ns_coll == 1 % self.ns_coll)
+        cap = log_cap or min(4096 + int(0.03 * sum(self.count0) * max(calls, 1)),
+                             (8 << 30) // C.sizeof(LepicWinEvent))
         self.log = torch.zeros(cap * C.sizeof(LepicWinEvent), dtype=torch.uint8, device=self.dev)
         self.log_cap = cap
         self.nlog = torch.zeros(1, dtype=torch.int32, device=self.dev)
