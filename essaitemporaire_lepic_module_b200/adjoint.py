@@ -556,9 +556,10 @@ class CollisionWindow:
         ev1.record()
         torch.cuda.synchronize()
         self.timing["backward_ms"] = ev0.elapsed_time(ev1)
+        # dJ/dv0 is a view of the adjoint planes (the window's precision),
+        # valid until the window's next pass
         lam = self.stores[0]["lam"]
-        return (dV.cpu().numpy()[:self.nlabel].copy(), float(dBz.item()),
-                lam[3:6, :self.count0[0]].to(torch.float64).clone())
+        return dV.cpu().numpy()[:self.nlabel].copy(), float(dBz.item()), lam[3:6, :self.count0[0]]
 
 
 class _CollisionWindowFn(torch.autograd.Function):
@@ -571,7 +572,8 @@ class _CollisionWindowFn(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gJ):
         dV, dBz, dv0 = ctx.window.backward(float(gJ))
-        return (torch.as_tensor(dV, dtype=torch.float64), torch.tensor(dBz, dtype=torch.float64), dv0, None, None)
+        return (torch.as_tensor(dV, dtype=torch.float64), torch.tensor(dBz, dtype=torch.float64),
+                dv0.to(torch.float64).clone(), None, None)
 
 
 def collision_window_objective(window, V, Bz, v0, observable="energy"):

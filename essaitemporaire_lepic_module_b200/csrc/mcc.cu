@@ -512,19 +512,36 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
         }
         return np_t * sp * ts.vr / c.nu_max;
       };
-      // pass 1: sum_r nu_r; pass 2 (a collision): the same partial sums in
-      // the same order up to the drawn u (Src/collisions.f90:714-737)
+      // pass 1: sum_r nu_r; pass 2 (a collision): the partial sums up to the
+      // drawn u over the reactions in ascending order of nu_r, as the
+      // reference sorts them (Src/collisions.f90:711-737).  The order
+      // matters when sum_r nu_r exceeds 1 (nu_max held at nu_uplim): the
+      // smallest frequencies then keep their full share.
       double sum_nu = 0.0;
       for (int r = 0; r < c.nr; ++r) sum_nu += nu_of(r);
       if (DSMC && missed && rd.first) atomicAdd(&D.stat[0], (unsigned long long)__popc(missed));
       const double u = u01(r0.y);
       if (u <= sum_nu && S.live(P, i)) {
-        double s = 0.0;
+        double nu[MAXR];
+        unsigned char ord[MAXR];
         cur_tt = -1;
         for (int r = 0; r < c.nr; ++r) {
-          s += nu_of(r);
+          // insertion by value; equal values keep the table order
+          const double v = nu_of(r);
+          int k = r;
+          while (k > 0 && nu[k - 1] > v) {
+            nu[k] = nu[k - 1];
+            ord[k] = ord[k - 1];
+            --k;
+          }
+          nu[k] = v;
+          ord[k] = (unsigned char)r;
+        }
+        double s = 0.0;
+        for (int k = 0; k < c.nr; ++k) {
+          s += nu[k];
           if (u <= s) {
-            sel = r;
+            sel = ord[k];
             break;
           }
         }

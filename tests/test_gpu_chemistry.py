@@ -187,3 +187,20 @@ def test_collisions_dropin_energy_and_sources():
             seen[p] += [len(new), want_xy.sum(), int(np.any(kept != v0[p], axis=1).sum())]
     assert np.all(seen[:, 0] > 40) and np.all(seen[:, 1] > 0), seen   # ionization products, some in the plane
     assert np.all(seen[:, 2] > 100), seen                               # electrons and ions changed
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_saturated_frequency_order(precision):
+    """At 20 Pa the electrons' collision frequency bound is held at its cap
+    (nu_uplim = 5e8 1/s, Src/main.f90:565-566), so the sum of nu_r / nu_max
+    exceeds 1 for most electrons and the reaction drawn depends on the order
+    of the partial sums: the reference adds them in ascending order of nu_r
+    (Src/collisions.f90:711-737), which keeps excitation and ionization at
+    their share next to the dominant elastic collisions.  Counts of every
+    reaction over six calls within 3 sigma of the oracle's."""
+    from essaitemporaire_lepic_module_b200.reactions import argon_tables_synthetic  # noqa: F401
+    wl = dataclasses.replace(config.workload("penning_small"), name="mccpen16",
+                             ions=[("[Ar+]", 39.95, 1.0, 0.026, 1.0)], gas_pressure=20.0)
+    st = config.build(wl)
+    got, want = _chemistry_vs_oracle(st, precision, CALLS, min_total=10000)
+    assert want[1] > 300 and want[2] > 300, want          # excitation and ionization seen

@@ -137,4 +137,4 @@ def test_autograd_function(windows):
     gV, gB, gv = w32.backward()
     np.testing.assert_allclose(Vt.grad.numpy(), gV, rtol=1e-12, atol=0)
     assert float(Bt.grad) == pytest.approx(gB, rel=1e-12)
-    assert torch.allclose(v0.grad, gv, rtol=1e-6, atol=0)
+    assert torch.allclose(v0.grad, gv.to(torch.float64), rtol=1e-6, atol=0)
