@@ -123,8 +123,9 @@ def _chemistry_vs_oracle(st, precision, calls, min_total):
         sim.collisions()
         torch.cuda.synchronize()
         got += sim.counts[:ncol]
-        miss_g += sim._targets.missed
-        assert sim._targets.lost_claims == 0
+        if sim._targets is not None:
+            miss_g += sim._targets.missed
+            assert sim._targets.lost_claims == 0
         np.testing.assert_allclose(sim.nu_max[:st.ntype], nu_o, rtol=1e-12, atol=0)
     ci = st.tables.col_info
     for p in range(1, st.ntype + 1):
@@ -198,7 +199,6 @@ def test_saturated_frequency_order(precision):
     (Src/collisions.f90:711-737), which keeps excitation and ionization at
     their share next to the dominant elastic collisions.  Counts of every
     reaction over six calls within 3 sigma of the oracle's."""
-    from essaitemporaire_lepic_module_b200.reactions import argon_tables_synthetic  # noqa: F401
     wl = dataclasses.replace(config.workload("penning_small"), name="mccpen16",
                              ions=[("[Ar+]", 39.95, 1.0, 0.026, 1.0)], gas_pressure=20.0)
     st = config.build(wl)
