@@ -39,6 +39,10 @@ large:  the large mixed-precision configuration (192^3 cells, e- + Ar+ at 128
         recorded and replayed): the gradient of the potential at the box
         centre after them with respect to the wall potential, B_z and the
         electrons' initial velocities, forward and backward times.
+mixed_vs_f64_error: the mixed form against the FP64 form after 10 and 100
+        steps from the same particles (64^3 workload, collisions replayed): phi
+        (every step), E, per-particle positions and velocities, density and
+        energy moments.
 adjoint: forward and backward time of the differentiable K-step window on the
         Penning workload (96x96x192, 5.7e7 electrons, K = 64, checkpoints every
         8 steps): gradient of the final mean electron energy with respect to the
@@ -525,6 +529,78 @@ def run_window_adjoint(sim, st, K, observable, production_ms_per_step):
     return out
 
 
+def run_precision(workload, steps=(10, 100)):
+    """The mixed form against the FP64 form after N steps from the same
+    particles: both run the collisional window (particles keep their slots, so
+    each particle is compared with itself), the mixed one recording its
+    collisions and the FP64 one replaying them; the errors of phi (every step),
+    E, positions, velocities and the species' density and energy moments."""
+    import torch
+    from essaitemporaire_lepic_module_b200 import config
+    from essaitemporaire_lepic_module_b200.adjoint import CollisionWindow
+    from essaitemporaire_lepic_module_b200.constants import QE
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    st = config.build(workload)
+    sim = Simulation(st, precision="mixed", seed=20240612)
+    sim.load_uniform()
+    for _ in range(3):
+        sim.step()
+    torch.cuda.synchronize()
+    V = [float(st.wl.V[lab]) if lab < len(st.wl.V) else 0.0 for lab in range(1, st.geom.ngrid + 1)]
+    Bz = float(st.Bconst[2])
+    out = {"workload": f"{workload} {list(st.n)} cells, {st.ntype} species, {sum(s.n() for s in sim.sp)} particles, "
+                       f"Bz {Bz} T, MCC every {st.wl.ns_coll} steps (the mixed run's collisions replayed by the "
+                       f"FP64 run)"}
+    h = st.h
+    for K in steps:
+        w64 = CollisionWindow(sim, K=K, fp64=True)
+        w32 = CollisionWindow(sim, K=K, keep_initial=True)
+        w32.forward(V, Bz)
+        w64.use_log_of(w32)
+        w64.forward(V, Bz)
+        dphi = [float((w32.phis[n] - w64.phis[n]).abs().max() / w64.phis[n].abs().max()) for n in range(K)]
+        Es = []
+        for w in (w32, w64):
+            sim.phi.copy_(w.phis[K - 1])
+            sim.efield()
+            Es.append(sim.Ei.clone())
+        res = {"phi_rel_err_last_step": dphi[-1], "phi_rel_err_max_over_steps": max(dphi),
+               "E_rel_err_last_step": float((Es[0] - Es[1]).abs().max() / Es[1].abs().max()),
+               "collisions_replayed": sum(b - a for a, b in w32.ev_range.values())}
+        for p in range(st.ntype):
+            a, b = w32.stores[p], w64.stores[p]
+            n = int(b["count"].item())
+            both = ((a["bl"][:n] >> 16) == 0x7fff) & ((b["bl"][:n] >> 16) == 0x7fff)
+            xa = torch.stack([((a["cell"][:n] >> (10 * k)) & 1023).double() + a["p"][k, :n].double()
+                              for k in range(3)])
+            xb = torch.stack([((b["cell"][:n] >> (10 * k)) & 1023).double() + b["p"][k, :n] for k in range(3)])
+            dx = (xa - xb)[:, both].abs()
+            va, vb = a["p"][3:6, :n].double(), b["p"][3:6, :n]
+            vmax = float(vb.abs().max())
+            m = abs(st.mass[p])
+            ke_a = float((0.5 * m * (va[:, both] ** 2).sum(dim=0)).mean() / QE)
+            ke_b = float((0.5 * m * (vb[:, both] ** 2).sum(dim=0)).mean() / QE)
+            mom_a = [float((xa[k, both] * h[k]).mean()) for k in range(3)]
+            mom_b = [float((xb[k, both] * h[k]).mean()) for k in range(3)]
+            res[st.names[p]] = {
+                "particles_compared": int(both.sum()), "lost_in_one_form_only": int((((a["bl"][:n] >> 16) == 0x7fff)
+                                                                                    != ((b["bl"][:n] >> 16) == 0x7fff)).sum()),
+                "position_err_max_cells": float(dx.max()), "position_err_rms_cells": float((dx ** 2).mean().sqrt()),
+                "velocity_rel_err_max": float((va - vb)[:, both].abs().max()) / vmax,
+                "energy_moment_rel_err": abs(ke_a - ke_b) / ke_b,
+                "density_moment_err_m": max(abs(x - y) for x, y in zip(mom_a, mom_b))}
+        out[f"after_{K}_steps"] = res
+        for d, (c0, p0, n0) in zip(w32.stores, w32.initial):
+            d["cell"].copy_(c0)
+            d["p"].copy_(p0)
+            d["count"].copy_(n0)
+        del w32, w64
+        torch.cuda.empty_cache()
+    del sim
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_dropin(workload, steps=4, warm=1):
     """The reference-facing path: Src/main.f90's timestep as calls to the
     Fortran-signature entry points over host arrays in the reference layouts
@@ -675,6 +751,8 @@ def run_ours(args):
     torch.cuda.empty_cache()
     if args.large and world == 1:
         line["large"] = run_large(args)
+    if args.precision_leg and world == 1:
+        line["mixed_vs_f64_error"] = run_precision(args.precision_workload)
     if args.poisson:
         line["poisson"] = run_poisson(args.poisson_workload)
     if args.adjoint:
@@ -718,6 +796,9 @@ def main():
     ap.add_argument("--large-steps", type=int, default=500)
     ap.add_argument("--no-large-adjoint", dest="large_adjoint", action="store_false",
                     help="skip the differentiable window after the large run")
+    ap.add_argument("--no-precision", dest="precision_leg", action="store_false",
+                    help="skip the mixed-vs-FP64 error after 10 and 100 steps")
+    ap.add_argument("--precision-workload", default="mcc64")
     ap.add_argument("--no-poisson", dest="poisson", action="store_false",
                     help="skip the Poisson stress measurement")
     ap.add_argument("--poisson-workload", default="poisson256")

@@ -227,6 +227,43 @@ def _gpu_counts(st, S, it, seed):
     return sim.counts[:st.tables.sig.shape[0]].astype(float)
 
 
+def test_box32_100_steps_at_its_own_size():
+    """The plain FP64 benchmark case at its own size (32^3 cells, electrons
+    and Ar+ at 16 per cell: 524,288 each, walls at 0 V, no B, no collisions):
+    100 device steps of the step loop against 100 oracle steps in the
+    reference's order from the same loaded particles -- particle counts
+    equal, every position and velocity within 1e-10 of the largest, phi
+    within 1e-10 of its largest value (the deposit's atomics sum in another
+    order than the oracle: 1e-16 per step, grown over 100 steps), the
+    multigrid schedule (V-cycles of the last solve) equal."""
+    import os
+    import torch
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    oracle.set_threads(os.cpu_count() or 1)
+    st = config.build("box32")
+    assert st.n_particles() == 524288
+    nmax = st.n_particles() + 4096
+    S = oracle.load_part(st, nmax=nmax)
+    sim = Simulation(st, cap=nmax)
+    sim.load_from_host(S.vxp, S.np_tot, S.np)
+    phi = st.geom.phi.copy()
+    Ei = np.zeros(tuple(st.geom.bcnd.shape) + (3,))
+    for it in range(1, 101):
+        Ei, mg_o, _ = oracle.step(st, S, phi, Ei, it)
+        sim.step()
+    torch.cuda.synchronize()
+    assert list(sim.counts_host()) == list(S.np_tot)
+    assert sim.mg_last[0] == mg_o[0], (sim.mg_last, mg_o)
+    for p in range(st.ntype):
+        g = sim.sp[p].to_vxp()
+        o = S.vxp[p, :S.np_tot[p]]
+        ko = np.lexsort((o[:, 2], o[:, 1], o[:, 0]))
+        kg = np.lexsort((g[:, 2], g[:, 1], g[:, 0]))
+        for c in range(6):
+            assert rel(g[kg, c], o[ko, c]) <= 1e-10, (p, c, rel(g[kg, c], o[ko, c]))
+    assert rel(sim.phi.cpu().numpy(), phi) <= 1e-10
+
+
 @pytest.mark.parametrize("fused", [True, False])
 def test_step_loop_trajectories_100_steps(fused):
     """Collisionless box: 100 device-resident steps vs 100 oracle steps in
