@@ -113,6 +113,36 @@ __device__ __forceinline__ bool warp_run_sum(long long key, double (&v)[NV]) {
   return head && key >= 0;
 }
 
+// The same after a bitonic sort of (key, lane) across the warp: the lanes of
+// one key form one run wherever they sat, so particles that left their
+// sorted order since the last sort still share one atomic per cell.  key and
+// v become the sorted lane's.
+template <int NV>
+__device__ __forceinline__ bool warp_sorted_run_sum(long long &key, double (&v)[NV]) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  long long sk = key < 0 ? (long long)0x7fffffffffffffffLL : key;
+  int sl = lane;
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const long long ok = __shfl_xor_sync(full, sk, j);
+      const int ol = __shfl_xor_sync(full, sl, j);
+      const bool up = (lane & k) == 0, lower = (lane & j) == 0;
+      const bool mine_first = sk < ok || (sk == ok && sl < ol);
+      if (((lower == up) ? mine_first : !mine_first) == false) {
+        sk = ok;
+        sl = ol;
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NV; ++c) v[c] = __shfl_sync(full, v[c], sl);
+  key = sk == (long long)0x7fffffffffffffffLL ? -1 : sk;
+  return warp_run_sum<NV>(key, v);
+}
+
 __device__ __forceinline__ void cross(double ax, double ay, double az, double bx, double by, double bz, double &rx,
                                       double &ry, double &rz) {
   rx = ay * bz - az * by;
@@ -673,7 +703,7 @@ __global__ void __launch_bounds__(AB) k_cw_deposit(Dims d, WinConst c, WinS<R> S
       for (int q = 0; q < 8; ++q) v[q] = (double)w[q];
     }
   }
-  if (warp_run_sum<8>(key, v)) {
+  if (warp_sorted_run_sum<8>(key, v)) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const long long g = key + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
@@ -872,7 +902,7 @@ __global__ void __launch_bounds__(AB) k_cw_adj_push(Dims d, WinConst c, const vo
       S.lam[5 * cap + i] = uz;
     }
   }
-  if (warp_run_sum<24>(key, sc)) {
+  if (warp_sorted_run_sum<24>(key, sc)) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const long long g = key + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
