@@ -17,6 +17,7 @@ set-ups shrunk so the FP64 CPU oracle finishes in seconds):
              (mcc96, mcc64, mcc32, mcc16: the same on smaller grids, for
              profiling captures and tests)
   poisson256 256^3 grid, two 16^3 electrodes at +-100 V, 64 Gaussian blobs
+             (poisson128, poisson64, poisson32: the same on smaller grids)
   penning    96x96x192 cells, e- 32 ppc, Bz = 0.1 T, end plates +200 V
              (electrode labels 2 and 3), side walls 0 V (label 1)
   mcc192     192^3 cells, e- + Ar+ 128 ppc (mixed precision only)
@@ -122,8 +123,8 @@ def workload(name: str) -> Workload:
         return Workload(name, n, 1e-4, [_box(n, 1e-4) + [1]], [0.0, 0.0], _ar_ion(),
                         Te=2.0, n0=1e15, ppc=128, dt=2e-11, steps=500,
                         B=(0.0, 0.0, 0.01), gas_pressure=1.0, gas_T=300.0, mixed_only=True)
-    if name in ("poisson256", "poisson64", "poisson32"):
-        m = {"poisson256": 256, "poisson64": 64, "poisson32": 32}[name]
+    if name in ("poisson256", "poisson128", "poisson64", "poisson32"):
+        m = {"poisson256": 256, "poisson128": 128, "poisson64": 64, "poisson32": 32}[name]
         n = (m, m, m)
         dxc = 1e-4 * 100.0
         e = 16 * m // 256 if m >= 128 else max(m // 16, 2)

@@ -470,7 +470,7 @@ class Simulation:
         todo = [self.sp[p] for p in (range(len(self.sp)) if species is None else species)]
         if self.mixed:
             for s in todo:
-                check(lib().lepic_dev_sort_mixed(C.byref(self.grid), C.byref(s.s), self._hint(s),
+                check(lib().lepic_dev_sort_mixed(C.byref(self.grid), C.byref(s.s), -1,
                                                  self._s()), "sort_mixed")
                 s.after_call()
             return
@@ -558,9 +558,9 @@ class Simulation:
         if self._acc is None:
             self._acc = torch.zeros((st.ntype, 2 + 2 * (st.geom.ngrid + 1)), dtype=torch.float64,
                                     device=self.dev)
-        # the FP64 push sizes its grid by the counts (a host read); the mixed
-        # push walks its tiles and a grid-stride tail and needs none
-        counts = None if self.mixed else torch.cat([s.count for s in self.sp]).cpu().numpy()
+        # no host read of the counts: the FP64 push launches over the capacity
+        # and its threads read the count on the device; the mixed push walks
+        # its tiles and a grid-stride tail
         self.np.zero_()
         for p, s in enumerate(self.sp):
             if st.charge[p] == 0.0:
@@ -575,7 +575,7 @@ class Simulation:
             check(lib().lepic_dev_push_deposit(C.byref(self.grid), _ptr(self.Ei), C.byref(s.s), p + 1,
                                                st.geom.ngrid, C.byref(self.P),
                                                C.c_void_p(self.np[p].data_ptr()),
-                                               C.c_void_p(self._acc[p].data_ptr()), int(counts[p]),
+                                               C.c_void_p(self._acc[p].data_ptr()), -1,
                                                self._s()), "push_deposit")
         if reduce:
             self._reduce_density()
@@ -746,9 +746,6 @@ class Simulation:
         snap_cnt.record_stream(self._copy_stream)
         self._io[slot] = (snap_phi, snap_cnt, done)
         return done
-
-    def _hint(self, s):
-        return int(s.count.item())
 
     def counts_host(self):
         return np.array([s.n() for s in self.sp])
