@@ -250,7 +250,7 @@ def _e2e(sim, st, steps, world, dist, torch):
     for lab in range(1, nl + 1):
         v_host[lab] = float(st.wl.V[lab]) if lab < len(st.wl.V) else 0.0
     phi_host = [torch.empty(tuple(st.geom.phi.shape), dtype=torch.float64).pin_memory() for _ in range(2)]
-    cnt_host = torch.zeros((steps, len(sim.sp)), dtype=torch.int32).pin_memory()
+    cnt_host = torch.zeros((max(steps, 2), len(sim.sp)), dtype=torch.int32).pin_memory()
     # warm-up: the first calls create the device snapshots and the copy stream
     for k in range(2):
         sim.step_host(v_host, phi_host[k], cnt_host[k])
@@ -267,7 +267,7 @@ def _e2e(sim, st, steps, world, dist, torch):
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     # particles pushed by each step: the count before it
-    nps = n0 + int(cnt_host[:-1].sum())
+    nps = n0 + int(cnt_host[:steps - 1].sum())
     if world > 1:
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -452,6 +452,7 @@ def run_adjoint(workload, K, every):
            "observable": "mean kinetic energy (eV) after K steps",
            "J": float(J), "dJ_dV_by_label": [float(x) for x in V.grad], "dJ_dBz": float(Bz.grad),
            "dJ_dv0_norm": float(v0.grad.norm()),
+           "setup_ms": setup_ms, "setup": "one sort of every species by cell, then the window's stores",
            "forward_ms": t["forward_ms"], "backward_ms": t["backward_ms"],
            "backward_over_forward": t["backward_ms"] / t["forward_ms"],
            "backward_kernel_ms": {k: round(v[0], 3) for k, v in sorted(timers.items())}}
@@ -498,7 +499,11 @@ def run_window_adjoint(sim, st, K, observable, production_ms_per_step):
     import torch
     from essaitemporaire_lepic_module_b200 import _lib
     from essaitemporaire_lepic_module_b200.adjoint import CollisionWindow
-    win = CollisionWindow(sim, K=K)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    win = CollisionWindow(sim, K=K, sort=True)     # the particles in cell order for the tiled scatters
+    torch.cuda.synchronize()
+    setup_ms = 1e3 * (time.perf_counter() - t0)
     V = [float(st.wl.V[lab]) if lab < len(st.wl.V) else 0.0 for lab in range(1, win.nlabel + 1)]
     Bz = float(st.Bconst[2])
     _lib.timing(enable=True)
@@ -684,6 +689,55 @@ def run_profile_step(args):
                       "particles": [s.n() for s in sim.sp]}), flush=True)
 
 
+def run_profile_poisson(args):
+    """One warm solve of the Poisson workload `--profile-poisson` (the source
+    scaled by 1.001 after a cold solve) in the form `--precision`, bracketed
+    by cudaProfilerStart/Stop for `ncu --profile-from-start off`."""
+    import torch
+    from essaitemporaire_lepic_module_b200 import config
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    st = config.build(args.profile_poisson)
+    form = "mixed" if args.precision == "both" else args.precision
+    sim = Simulation(st, cap=1024, precision=form)
+    sim.phi.copy_(torch.as_tensor(st.geom.phi, device="cuda"))
+    rhs0 = torch.as_tensor(st.rhs_blobs, device="cuda")
+    sim.rhs.copy_(rhs0)
+    cold = sim.pdesolver()
+    sim.rhs.copy_(rhs0 * 1.001)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    warm = sim.pdesolver()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profiled": "warm solve", "workload": args.profile_poisson, "form": form,
+                      "cold": list(cold), "warm": list(warm)}), flush=True)
+
+
+def run_profile_window(args):
+    """The collisional window of `--profile-window` steps (forward, then the
+    backward pass) on the mixed-precision workload `--workload` after
+    `--warmup` plain steps, bracketed by cudaProfilerStart/Stop."""
+    import torch
+    from essaitemporaire_lepic_module_b200 import config
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    from essaitemporaire_lepic_module_b200.adjoint import CollisionWindow
+    st = config.build(args.workload)
+    sim = Simulation(st, precision="mixed", sort_policy=args.sort_policy)
+    sim.load_uniform()
+    for _ in range(args.warmup):
+        sim.step()
+    w = CollisionWindow(sim, K=args.profile_window, sort=True)
+    V = [float(st.wl.V[lab]) if lab < len(st.wl.V) else 0.0 for lab in range(1, st.geom.ngrid + 1)]
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    J = w.forward(V, float(st.Bconst[2]), observable="probe")
+    g = w.backward()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profiled": "collisional window", "workload": args.workload, "K": args.profile_window,
+                      "J": J, "dJ_dBz": g[1], "timing_ms": w.timing}), flush=True)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -813,8 +867,17 @@ def main():
     ap.add_argument("--dropin-steps", type=int, default=10)
     ap.add_argument("--profile-step", type=int, default=0,
                     help="run only up to this step, the last one between cudaProfilerStart/Stop (for ncu)")
+    ap.add_argument("--profile-poisson", default=None,
+                    help="run only one warm solve of this Poisson workload between cudaProfilerStart/Stop")
+    ap.add_argument("--profile-window", type=int, default=0,
+                    help="run only a collisional window of this many steps (forward + backward) on --workload "
+                         "after --warmup steps, between cudaProfilerStart/Stop")
     args = ap.parse_args()
-    if args.profile_step > 0:
+    if args.profile_poisson:
+        run_profile_poisson(args)
+    elif args.profile_window > 0:
+        run_profile_window(args)
+    elif args.profile_step > 0:
         run_profile_step(args)
     elif args.impl == "reference":
         run_reference(args)

@@ -57,7 +57,8 @@ class LepicSpeciesMixed(C.Structure):
 class LepicWinSpecies(C.Structure):
     """lepic_win_species_t: one species of the differentiable collisional window."""
     _fields_ = [("cell", C.c_void_p), ("p", C.c_void_p), ("lam", C.c_void_p), ("bl", C.c_void_p),
-                ("count", C.c_void_p), ("cap", C.c_int), ("fp64", C.c_int)]
+                ("count", C.c_void_p), ("cap", C.c_int), ("fp64", C.c_int), ("tile_off", C.c_void_p),
+                ("tile_end", C.c_int), ("pad", C.c_int)]
 
 
 class LepicWinEvent(C.Structure):

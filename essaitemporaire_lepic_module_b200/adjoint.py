@@ -280,10 +280,15 @@ class CollisionWindow:
     the FP64 multigrid: the FP64 reference of the same events.  The backward
     pass needs no particle checkpoints: it undoes each push (the inverse
     Boris rotation), each collision (from its record), and keeps only the
-    potential of every step."""
+    potential of every step.
+
+    sort=True sorts the simulation's particles by cell first (every species),
+    which the FP32 kernels' tile-by-tile scatter is fast on; a second window
+    on the same initial state (the FP64 reference) must then be made with
+    sort=False, after the first, so that both see the same slots."""
 
     def __init__(self, sim, K, fp64=False, ns_coll=None, first_it=None, log_cap=None, keep_initial=False,
-                 seed=None):
+                 seed=None, sort=False):
         st = sim.st
         if not sim.mixed:
             raise ValueError("the collisional window runs on a mixed-precision Simulation")
@@ -291,6 +296,8 @@ class CollisionWindow:
             raise ValueError("the collisional window supports Dirichlet (metal) walls only")
         if st.bfield is not None:
             raise ValueError("the collisional window differentiates a uniform B, not a B-field map")
+        if sort:
+            sim.sort()
         self.sim, self.st, self.K, self.fp64 = sim, st, int(K), bool(fp64)
         self.dev = sim.dev
         self.ntype = st.ntype
@@ -313,6 +320,13 @@ class CollisionWindow:
             w = self.ws[p]
             w.cell, w.p, w.lam = d["cell"].data_ptr(), d["p"].data_ptr(), d["lam"].data_ptr()
             w.bl, w.count, w.cap, w.fp64 = d["bl"].data_ptr(), d["count"].data_ptr(), d["cap"], int(self.fp64)
+            if not self.fp64:
+                # the tiles of the simulation's last sort: the FP32 deposit and
+                # push adjoint scatter tile by tile (fast when the particles
+                # are still in that sort's order, correct in any order)
+                d["tile_off"] = sp.tile_off.clone()
+                w.tile_off = d["tile_off"].data_ptr()
+                w.tile_end = int(d["tile_off"][-1].item())
         self.count0 = [int(d["count"].item()) for d in self.stores]
         self.initial = None
         if keep_initial:

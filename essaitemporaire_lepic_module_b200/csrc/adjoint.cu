@@ -90,8 +90,8 @@ __device__ __forceinline__ unsigned lanemask_le() {
 // contribute zeros.  All 32 lanes must call this.  The window's particles are
 // sorted by cell, so a warp holds few runs and the atomics that follow are
 // one per run instead of one per particle.
-template <int NV>
-__device__ __forceinline__ bool warp_run_sum(long long key, double (&v)[NV]) {
+template <int NV, class T = double>
+__device__ __forceinline__ bool warp_run_sum(long long key, T (&v)[NV]) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const long long prev = __shfl_up_sync(full, key, 1);
@@ -106,41 +106,11 @@ __device__ __forceinline__ bool warp_run_sum(long long key, double (&v)[NV]) {
     const bool same = (lane + o < 32) && orid == rid;
 #pragma unroll
     for (int c = 0; c < NV; ++c) {
-      const double t = __shfl_down_sync(full, v[c], o);
+      const T t = __shfl_down_sync(full, v[c], o);
       if (same) v[c] += t;
     }
   }
   return head && key >= 0;
-}
-
-// The same after a bitonic sort of (key, lane) across the warp: the lanes of
-// one key form one run wherever they sat, so particles that left their
-// sorted order since the last sort still share one atomic per cell.  key and
-// v become the sorted lane's.
-template <int NV>
-__device__ __forceinline__ bool warp_sorted_run_sum(long long &key, double (&v)[NV]) {
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  long long sk = key < 0 ? (long long)0x7fffffffffffffffLL : key;
-  int sl = lane;
-#pragma unroll
-  for (int k = 2; k <= 32; k <<= 1) {
-#pragma unroll
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      const long long ok = __shfl_xor_sync(full, sk, j);
-      const int ol = __shfl_xor_sync(full, sl, j);
-      const bool up = (lane & k) == 0, lower = (lane & j) == 0;
-      const bool mine_first = sk < ok || (sk == ok && sl < ol);
-      if (((lower == up) ? mine_first : !mine_first) == false) {
-        sk = ok;
-        sl = ol;
-      }
-    }
-  }
-#pragma unroll
-  for (int c = 0; c < NV; ++c) v[c] = __shfl_sync(full, v[c], sl);
-  key = sk == (long long)0x7fffffffffffffffLL ? -1 : sk;
-  return warp_run_sum<NV>(key, v);
 }
 
 __device__ __forceinline__ void cross(double ax, double ay, double az, double bx, double by, double bz, double &rx,
@@ -681,29 +651,85 @@ __device__ __forceinline__ void block_add(double v, double *dst) {
   }
 }
 
-// deposit of the particles of step `step` (created before it, not lost
-// before its push) into np, kq applied
+// The window's particles of one tile of the sort that ordered them (slots
+// tile_off[t] .. tile_off[t+1]) are scattered by one block into a box of
+// nodes in shared memory: the tile's 8^3 cells and WH halo cells on each
+// side, FP32 sums flushed into the FP64 grid after every WFLUSH particles and
+// at the end.  A particle whose cell left the box (it drifted more than WH
+// cells from its tile during the window) adds into the FP64 grid directly,
+// and slots past the last tile (appended since that sort, collision
+// products) are scattered by the untiled kernels.  Any slot order gives the
+// same sums; the order only decides how many land in the box.
+constexpr int WTC = LEPIC_TILE_CELLS;
+constexpr int WH = 2;                       // halo cells
+constexpr int WB = WTC + 2 * WH + 1;        // box nodes per axis
+constexpr int WBN = WB * WB * WB;
+constexpr int WFLUSH = 8 * AB;              // particles between flushes
+
+struct WinTiles {
+  const int *off;     // tile_off[0..ntiles] of the sort
+  int ntx, nty;       // tiles per axis
+};
+
+WinTiles win_tiles(const lepic_grid_t &g, const lepic_win_species_t &w) {
+  WinTiles T;
+  T.off = w.tile_off;
+  T.ntx = (g.n[0] + WTC - 1) / WTC;
+  T.nty = (g.n[1] + WTC - 1) / WTC;
+  return T;
+}
+
+// box origin (grid node of box node 0) of tile t
+__device__ __forceinline__ void tile_box(const WinTiles &T, int t, int &bx, int &by, int &bz) {
+  const int tx = t % T.ntx, ty = (t / T.ntx) % T.nty, tz = t / (T.ntx * T.nty);
+  bx = tx * WTC + 1 - WH;
+  by = ty * WTC + 1 - WH;
+  bz = tz * WTC + 1 - WH;
+}
+
+// box-local base node of cell (ix, iy, iz), or -1 when the cell's 8 nodes
+// are not all in the box
+__device__ __forceinline__ int box_base(int ix, int iy, int iz, int bx, int by, int bz) {
+  const int lx = ix - bx, ly = iy - by, lz = iz - bz;
+  if ((unsigned)lx >= (unsigned)(WB - 1) || (unsigned)ly >= (unsigned)(WB - 1) || (unsigned)lz >= (unsigned)(WB - 1))
+    return -1;
+  return lx + WB * (ly + WB * lz);
+}
+
+__device__ __forceinline__ int box_off(int q) { return ox(q) + WB * (oy(q) + WB * oz(q)); }
+
+// the deposit weights of slot i at step `step` (created before it, not lost
+// before its push): true with the cell and the 8 weights
+template <class R>
+__device__ __forceinline__ bool cw_dep_one(const WinS<R> &S, long long i, int step, int &ix, int &iy, int &iz,
+                                           R (&w)[8]) {
+  const int b = S.bl[i];
+  if (!(born_of(b) < step && lost_of(b) >= step)) return false;
+  unpack_cell(S.cell[i], ix, iy, iz);
+  weights8<R>(S.p[i], S.p[S.cap + i], S.p[2 * S.cap + i], w);
+  return true;
+}
+
+// deposit of the slots first.. into np, kq applied
 template <class R>
 __global__ void __launch_bounds__(AB) k_cw_deposit(Dims d, WinConst c, WinS<R> S, const int *__restrict__ count,
-                                                   int step, const double *__restrict__ kq, double *__restrict__ np) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+                                                   long long first, int step, const double *__restrict__ kq,
+                                                   double *__restrict__ np) {
+  const long long i = first + blockIdx.x * (long long)blockDim.x + threadIdx.x;
   long long key = -1;
   double v[8];
 #pragma unroll
   for (int q = 0; q < 8; ++q) v[q] = 0.0;
   if (i < *count) {
-    const int b = S.bl[i];
-    if (born_of(b) < step && lost_of(b) >= step) {
-      int ix, iy, iz;
-      unpack_cell(S.cell[i], ix, iy, iz);
-      R w[8];
-      weights8<R>(S.p[i], S.p[S.cap + i], S.p[2 * S.cap + i], w);
+    int ix, iy, iz;
+    R w[8];
+    if (cw_dep_one<R>(S, i, step, ix, iy, iz, w)) {
       key = d.g(ix, iy, iz);
 #pragma unroll
       for (int q = 0; q < 8; ++q) v[q] = (double)w[q];
     }
   }
-  if (warp_sorted_run_sum<8>(key, v)) {
+  if (warp_run_sum<8>(key, v)) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const long long g = key + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
@@ -712,59 +738,210 @@ __global__ void __launch_bounds__(AB) k_cw_deposit(Dims d, WinConst c, WinS<R> S
   }
 }
 
+// the box's non-zero node sums (NC components per node) into the FP64 grid
+// dst (NC values per node, scaled by kdep kq[node] when kq is given), then
+// cleared
+template <int NC>
+__device__ void flush_box(const Dims &d, float *box, int bx, int by, int bz, const double *__restrict__ kq,
+                          double kdep, double *__restrict__ dst) {
+  for (int e = threadIdx.x; e < WBN; e += blockDim.x) {
+    float v[NC];
+    bool any = false;
+#pragma unroll
+    for (int a = 0; a < NC; ++a) {
+      v[a] = box[NC * e + a];
+      any = any || v[a] != 0.f;
+    }
+    if (!any) continue;
+    const int lx = e % WB, ly = (e / WB) % WB, lz = e / (WB * WB);
+    const int gx = bx + lx, gy = by + ly, gz = bz + lz;
+    // only nodes of cells 1..n receive weights: the box part outside the grid stays 0
+    if (gx >= 0 && gy >= 0 && gz >= 0 && gx <= d.n1 + 2 && gy <= d.n2 + 2 && gz <= d.n3 + 2) {
+      const long long g = d.g(gx, gy, gz);
+      const double k = kq ? kq[g] * kdep : 1.0;
+#pragma unroll
+      for (int a = 0; a < NC; ++a)
+        if (v[a] != 0.f) atomicAdd(&dst[NC * g + a], k * (double)v[a]);
+    }
+#pragma unroll
+    for (int a = 0; a < NC; ++a) box[NC * e + a] = 0.f;
+  }
+}
+
+// the FP32 window's deposit, one block per tile
+__global__ void __launch_bounds__(AB) k_cw_deposit_tiles(Dims d, WinConst c, WinS<float> S, const int *__restrict__ count,
+                                                         WinTiles T, int step, const double *__restrict__ kq,
+                                                         double *__restrict__ np) {
+  __shared__ float s_box[WBN];
+  int bx, by, bz;
+  tile_box(T, blockIdx.x, bx, by, bz);
+  for (int e = threadIdx.x; e < WBN; e += AB) s_box[e] = 0.f;
+  __syncthreads();
+  const long long N = *count;
+  const long long lo = T.off[blockIdx.x];
+  long long hi = T.off[blockIdx.x + 1];
+  if (hi > N) hi = N;
+  int chunks = 0;
+  for (long long base = lo; base < hi; base += AB) {
+    // every lane takes part in the run sums (base is uniform over the block)
+    const long long i = base + threadIdx.x;
+    int ix = 0, iy = 0, iz = 0;
+    float w[8];
+    long long key = -1;
+    if (i < hi && cw_dep_one<float>(S, i, step, ix, iy, iz, w))
+      key = d.g(ix, iy, iz);
+    else
+#pragma unroll
+      for (int q = 0; q < 8; ++q) w[q] = 0.f;
+    // lanes of one cell (consecutive in the sort's order) summed first: one
+    // lane adds for the run, so a cell's particles do not contend for the
+    // same shared words
+    if (warp_run_sum<8, float>(key, w)) {
+      const int b0 = box_base(ix, iy, iz, bx, by, bz);
+      if (b0 >= 0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) atomicAdd(&s_box[b0 + box_off(q)], w[q]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const long long g = key + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
+          atomicAdd(&np[g], kq[g] * (c.kdep * (double)w[q]));
+        }
+      }
+    }
+    if (++chunks == WFLUSH / AB && base + AB < hi) {
+      chunks = 0;
+      __syncthreads();
+      flush_box<1>(d, s_box, bx, by, bz, kq, c.kdep, np);
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  flush_box<1>(d, s_box, bx, by, bz, kq, c.kdep, np);
+}
+
+// E gathers of a cell's 8 nodes in the order of gather_E: from the FP32 /
+// FP64 node array, or (FP32 window, one block per tile) from the tile's node
+// box in shared memory when the cell lies in it
+struct EGlobal {
+  Dims d;
+  const void *E;
+  template <class R>
+  __device__ __forceinline__ void operator()(int ix, int iy, int iz, const R (&w)[8], R &Ex, R &Ey, R &Ez) const {
+    gather_E<R>(d, E, d.g(ix, iy, iz), w, Ex, Ey, Ez);
+  }
+};
+
+struct ETile {
+  Dims d;
+  const void *E;
+  const float4 *box;
+  int bx, by, bz;
+  __device__ __forceinline__ void operator()(int ix, int iy, int iz, const float (&w)[8], float &Ex, float &Ey,
+                                             float &Ez) const {
+    const int b0 = box_base(ix, iy, iz, bx, by, bz);
+    if (b0 < 0) {
+      gather_E<float>(d, E, d.g(ix, iy, iz), w, Ex, Ey, Ez);
+      return;
+    }
+    Ex = Ey = Ez = 0.f;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float4 e = box[b0 + box_off(q)];
+      Ex += w[q] * e.x;
+      Ey += w[q] * e.y;
+      Ez += w[q] * e.z;
+    }
+  }
+};
+
+// E (one float4 per node) of tile t's node box into shared memory
+__device__ void stage_E_box(const Dims &d, const float4 *__restrict__ E, int bx, int by, int bz, float4 *box) {
+  for (int e = threadIdx.x; e < WBN; e += blockDim.x) {
+    const int gx = bx + e % WB, gy = by + (e / WB) % WB, gz = bz + e / (WB * WB);
+    const bool in = gx >= 0 && gy >= 0 && gz >= 0 && gx <= d.n1 + 2 && gy <= d.n2 + 2 && gz <= d.n3 + 2;
+    box[e] = in ? E[d.g(gx, gy, gz)] : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
 // push of step `step`; a particle whose new cell is a wall cell (or outside
 // the grid) is lost at this step and keeps its state from before the push;
-// wall_acc += the kinetic energy (J) the lost macroparticles carry
+// wl += the kinetic energy (J) the lost macroparticle carries
+template <class R, class G>
+__device__ __forceinline__ void cw_push_one(const Dims &d, const WinConst &c, const unsigned char *__restrict__ cw,
+                                            const WinS<R> &S, long long i, int step, const G &gather, double &wl) {
+  const int b = S.bl[i];
+  if (!(born_of(b) <= step && lost_of(b) >= step)) return;
+  int ix, iy, iz;
+  unpack_cell(S.cell[i], ix, iy, iz);
+  const long long cap = S.cap;
+  R fx = S.p[i], fy = S.p[cap + i], fz = S.p[2 * cap + i];
+  R vx = S.p[3 * cap + i], vy = S.p[4 * cap + i], vz = S.p[5 * cap + i];
+  R w[8];
+  weights8<R>(fx, fy, fz, w);
+  R Ex, Ey, Ez;
+  gather(ix, iy, iz, w, Ex, Ey, Ez);
+  boris<R>(c, Ex, Ey, Ez, vx, vy, vz);
+  const int ax = ix + move_offset<R>(fx, vx * (R)(c.dt / c.h0));
+  const int ay = iy + move_offset<R>(fy, vy * (R)(c.dt / c.h1));
+  const int az = iz + move_offset<R>(fz, vz * (R)(c.dt / c.h2));
+  const int cx = ax < 0 ? 0 : (ax > d.n1 + 1 ? d.n1 + 1 : ax);
+  const int cy = ay < 0 ? 0 : (ay > d.n2 + 1 ? d.n2 + 1 : ay);
+  const int cz = az < 0 ? 0 : (az > d.n3 + 1 ? d.n3 + 1 : az);
+  const bool lost = ax < 1 || ay < 1 || az < 1 || ax > d.n1 || ay > d.n2 || az > d.n3 || cw[d.c(cx, cy, cz)];
+  if (lost) {
+    S.bl[i] = (b & 0xffff) | (step << 16);
+    wl += 0.5 * c.Nm * c.mass * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+  } else {
+    S.cell[i] = pack_cell(ax, ay, az);
+    S.p[i] = fx;
+    S.p[cap + i] = fy;
+    S.p[2 * cap + i] = fz;
+    S.p[3 * cap + i] = vx;
+    S.p[4 * cap + i] = vy;
+    S.p[5 * cap + i] = vz;
+  }
+}
+
+// slots first..; wall_acc += the kinetic energy carried to the walls
 template <class R>
 __global__ void __launch_bounds__(AB) k_cw_push(Dims d, WinConst c, const void *__restrict__ E,
                                                 const unsigned char *__restrict__ cw, WinS<R> S,
-                                                const int *__restrict__ count, int step, double *wall_acc) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+                                                const int *__restrict__ count, long long first, int step,
+                                                double *wall_acc) {
+  const long long i = first + blockIdx.x * (long long)blockDim.x + threadIdx.x;
   double wl = 0.0;
-  if (i < *count) {
-    const int b = S.bl[i];
-    if (born_of(b) <= step && lost_of(b) >= step) {
-      int ix, iy, iz;
-      unpack_cell(S.cell[i], ix, iy, iz);
-      const long long cap = S.cap;
-      R fx = S.p[i], fy = S.p[cap + i], fz = S.p[2 * cap + i];
-      R vx = S.p[3 * cap + i], vy = S.p[4 * cap + i], vz = S.p[5 * cap + i];
-      R w[8];
-      weights8<R>(fx, fy, fz, w);
-      R Ex, Ey, Ez;
-      gather_E<R>(d, E, d.g(ix, iy, iz), w, Ex, Ey, Ez);
-      boris<R>(c, Ex, Ey, Ez, vx, vy, vz);
-      const int ax = ix + move_offset<R>(fx, vx * (R)(c.dt / c.h0));
-      const int ay = iy + move_offset<R>(fy, vy * (R)(c.dt / c.h1));
-      const int az = iz + move_offset<R>(fz, vz * (R)(c.dt / c.h2));
-      const int cx = ax < 0 ? 0 : (ax > d.n1 + 1 ? d.n1 + 1 : ax);
-      const int cy = ay < 0 ? 0 : (ay > d.n2 + 1 ? d.n2 + 1 : ay);
-      const int cz = az < 0 ? 0 : (az > d.n3 + 1 ? d.n3 + 1 : az);
-      const bool lost = ax < 1 || ay < 1 || az < 1 || ax > d.n1 || ay > d.n2 || az > d.n3 || cw[d.c(cx, cy, cz)];
-      if (lost) {
-        S.bl[i] = (b & 0xffff) | (step << 16);
-        wl = 0.5 * c.Nm * c.mass * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
-      } else {
-        S.cell[i] = pack_cell(ax, ay, az);
-        S.p[i] = fx;
-        S.p[cap + i] = fy;
-        S.p[2 * cap + i] = fz;
-        S.p[3 * cap + i] = vx;
-        S.p[4 * cap + i] = vy;
-        S.p[5 * cap + i] = vz;
-      }
-    }
-  }
+  if (i < *count) cw_push_one<R>(d, c, cw, S, i, step, EGlobal{d, E}, wl);
+  block_add(wl, wall_acc);
+}
+
+// the FP32 window's push, one block per tile, E of the tile's box staged.
+// (A variant that also deposited the kept particles for the next step, in a
+// node box beside E, was 4 % slower than this push and k_cw_deposit_tiles.)
+__global__ void __launch_bounds__(AB) k_cw_push_tiles(Dims d, WinConst c, const float4 *__restrict__ E,
+                                                      const unsigned char *__restrict__ cw, WinS<float> S,
+                                                      const int *__restrict__ count, WinTiles T, int step,
+                                                      double *wall_acc) {
+  __shared__ float4 s_E[WBN];
+  int bx, by, bz;
+  tile_box(T, blockIdx.x, bx, by, bz);
+  stage_E_box(d, E, bx, by, bz, s_E);
+  __syncthreads();
+  const ETile G{d, E, s_E, bx, by, bz};
+  const long long N = *count;
+  const long long lo = T.off[blockIdx.x];
+  long long hi = T.off[blockIdx.x + 1];
+  if (hi > N) hi = N;
+  double wl = 0.0;
+  for (long long i = lo + threadIdx.x; i < hi; i += AB) cw_push_one<float>(d, c, cw, S, i, step, G, wl);
   block_add(wl, wall_acc);
 }
 
 // the push of step `step` undone for the particles it kept: x^n from
 // x^{n+1} and v^{n+1/2}, then v+ by the inverse rotation with E^n at x^n
-template <class R>
-__global__ void __launch_bounds__(AB) k_cw_reverse(Dims d, WinConst c, const void *__restrict__ E, WinS<R> S,
-                                                   const int *__restrict__ count, int step) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= *count) return;
+template <class R, class G>
+__device__ __forceinline__ void cw_reverse_one(const Dims &d, const WinConst &c, const WinS<R> &S, long long i,
+                                               int step, const G &gather) {
   const int b = S.bl[i];
   if (!(born_of(b) <= step && lost_of(b) > step)) return;
   int ix, iy, iz;
@@ -781,7 +958,7 @@ __global__ void __launch_bounds__(AB) k_cw_reverse(Dims d, WinConst c, const voi
   R w[8];
   weights8<R>(fx, fy, fz, w);
   R Ex, Ey, Ez;
-  gather_E<R>(d, E, d.g(ix, iy, iz), w, Ex, Ey, Ez);
+  gather(ix, iy, iz, w, Ex, Ey, Ez);
   boris_inverse<R>(c, Ex, Ey, Ez, vx, vy, vz);
   S.cell[i] = pack_cell(ix, iy, iz);
   S.p[i] = fx;
@@ -792,117 +969,194 @@ __global__ void __launch_bounds__(AB) k_cw_reverse(Dims d, WinConst c, const voi
   S.p[5 * cap + i] = vz;
 }
 
+template <class R>
+__global__ void __launch_bounds__(AB) k_cw_reverse(Dims d, WinConst c, const void *__restrict__ E, WinS<R> S,
+                                                   const int *__restrict__ count, long long first, int step) {
+  const long long i = first + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < *count) cw_reverse_one<R>(d, c, S, i, step, EGlobal{d, E});
+}
+
+__global__ void __launch_bounds__(AB) k_cw_reverse_tiles(Dims d, WinConst c, const float4 *__restrict__ E,
+                                                         WinS<float> S, const int *__restrict__ count, WinTiles T,
+                                                         int step) {
+  __shared__ float4 s_E[WBN];
+  int bx, by, bz;
+  tile_box(T, blockIdx.x, bx, by, bz);
+  stage_E_box(d, E, bx, by, bz, s_E);
+  __syncthreads();
+  const ETile G{d, E, s_E, bx, by, bz};
+  const long long N = *count;
+  const long long lo = T.off[blockIdx.x];
+  long long hi = T.off[blockIdx.x + 1];
+  if (hi > N) hi = N;
+  for (long long i = lo + threadIdx.x; i < hi; i += AB) cw_reverse_one<float>(d, c, S, i, step, G);
+}
+
 // adjoint of the push of step `step` at the state (x^n, v+) for the
 // particles it moved: lam (dJ/dx^{n+1}, dJ/dv^{n+1/2}) -> (the push's part of
 // dJ/dx^n, dJ/dv+), lE += gather^T, dBz.  A particle lost at this step has no
 // later use except the wall-flux observable: wflux Nm m v^{n+1/2}.
+// Per slot: true when slot i was pushed at `step`, with its cell, its 24
+// contributions to lE (node q, component a at 3 q + a) and gB += its dJ/dB_z.
+template <class R, class N>
+__device__ __forceinline__ bool cw_adj_push_one(const WinConst &c, const N &nodes, const WinS<R> &S, long long i,
+                                                int step, double wflux, int &ix, int &iy, int &iz, R (&sc)[24],
+                                                double &gB) {
+  const int b = S.bl[i];
+  if (!(born_of(b) <= step && lost_of(b) >= step)) return false;
+  const long long cap = S.cap;
+  unpack_cell(S.cell[i], ix, iy, iz);
+  const R fx = S.p[i], fy = S.p[cap + i], fz = S.p[2 * cap + i];
+  const R vx = S.p[3 * cap + i], vy = S.p[4 * cap + i], vz = S.p[5 * cap + i];
+  R w[8];
+  weights8<R>(fx, fy, fz, w);
+  // E at the cell's 8 nodes, read once for the gather and its weight gradient
+  R en[8][3];
+  nodes(ix, iy, iz, en);
+  R Ex = R(0), Ey = R(0), Ez = R(0);   // the order of gather_E
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    Ex += w[q] * en[q][0];
+    Ey += w[q] * en[q][1];
+    Ez += w[q] * en[q][2];
+  }
+  R lx, ly, lz, lvx, lvy, lvz;
+  if (lost_of(b) == step) {
+    lx = ly = lz = R(0);
+    lvx = lvy = lvz = R(0);
+    if (wflux != 0.0) {
+      R ux = vx, uy = vy, uz = vz;
+      boris<R>(c, Ex, Ey, Ez, ux, uy, uz);
+      const R k = (R)(wflux * c.Nm * c.mass);
+      lvx = k * ux;
+      lvy = k * uy;
+      lvz = k * uz;
+    }
+  } else {
+    lx = S.lam[i];
+    ly = S.lam[cap + i];
+    lz = S.lam[2 * cap + i];
+    lvx = S.lam[3 * cap + i];
+    lvy = S.lam[4 * cap + i];
+    lvz = S.lam[5 * cap + i];
+  }
+  // x^{n+1} = x^n + dt v^{n+1/2}
+  const R dt = (R)c.dt, k1 = (R)c.k1, kk = (R)c.kk;
+  lvx += dt * lx;
+  lvy += dt * ly;
+  lvz += dt * lz;
+  R lEx, lEy, lEz, ux, uy, uz;
+  if (c.boris) {
+    const R Bx = (R)c.Bx, By = (R)c.By, Bz = (R)c.Bz;
+    const R v1x = vx + k1 * Ex, v1y = vy + k1 * Ey, v1z = vz + k1 * Ez;
+    const R v3x = v1x + k1 * (v1y * Bz - v1z * By), v3y = v1y + k1 * (v1z * Bx - v1x * Bz),
+            v3z = v1z + k1 * (v1x * By - v1y * Bx);
+    // d v^{n+1/2} / d Bz: v2 = v1 + kk (v3 x B), v3 = v1 + k1 (v1 x B)
+    const R ax = v3y * Bz - v3z * By, ay = v3z * Bx - v3x * Bz, az = v3x * By - v3y * Bx;   // v3 x B
+    const R bx = v1y, by = -v1x;                                                            // v1 x e_z
+    const R cx = k1 * (by * Bz), cy = k1 * (-bx * Bz), cz = k1 * (bx * By - by * Bx);     // (k1 v1 x e_z) x B
+    const R ex = v3y, ey = -v3x;                                                            // v3 x e_z
+    const R dkk = (R)c.dkk;
+    gB += (double)(lvx * (dkk * ax + kk * (cx + ex)) + lvy * (dkk * ay + kk * (cy + ey)) + lvz * (dkk * az + kk * cz));
+    lEx = k1 * lvx;
+    lEy = k1 * lvy;
+    lEz = k1 * lvz;
+    // l3 = kk (B x lv), u = lv + l3 + k1 (B x l3)
+    const R l3x = kk * (By * lvz - Bz * lvy), l3y = kk * (Bz * lvx - Bx * lvz), l3z = kk * (Bx * lvy - By * lvx);
+    ux = lvx + l3x + k1 * (By * l3z - Bz * l3y);
+    uy = lvy + l3y + k1 * (Bz * l3x - Bx * l3z);
+    uz = lvz + l3z + k1 * (Bx * l3y - By * l3x);
+    lEx += k1 * ux;
+    lEy += k1 * uy;
+    lEz += k1 * uz;
+  } else {
+    ux = lvx;
+    uy = lvy;
+    uz = lvz;
+    lEx = R(2) * k1 * lvx;
+    lEy = R(2) * k1 * lvy;
+    lEz = R(2) * k1 * lvz;
+  }
+  // gather^T and the weight gradient of the gather into lx
+  const R px = R(1) - fx, py = R(1) - fy, pz = R(1) - fz;
+  const R hx = (R)(1.0 / c.h0), hy = (R)(1.0 / c.h1), hz = (R)(1.0 / c.h2);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    sc[3 * q + 0] = w[q] * lEx;
+    sc[3 * q + 1] = w[q] * lEy;
+    sc[3 * q + 2] = w[q] * lEz;
+    const R ax_ = ox(q) ? R(1) - px : px, ay_ = oy(q) ? R(1) - py : py, az_ = oz(q) ? R(1) - pz : pz;
+    const R sx = ox(q) ? hx : -hx, sy = oy(q) ? hy : -hy, sz = oz(q) ? hz : -hz;
+    const R s = en[q][0] * lEx + en[q][1] * lEy + en[q][2] * lEz;
+    lx += sx * ay_ * az_ * s;
+    ly += ax_ * sy * az_ * s;
+    lz += ax_ * ay_ * sz * s;
+  }
+  S.lam[i] = lx;
+  S.lam[cap + i] = ly;
+  S.lam[2 * cap + i] = lz;
+  S.lam[3 * cap + i] = ux;
+  S.lam[4 * cap + i] = uy;
+  S.lam[5 * cap + i] = uz;
+  return true;
+}
+
+// E at the 8 nodes of a cell: from the node array, or from the tile's node
+// box in shared memory when the cell lies in it
+struct ENodesGlobal {
+  Dims d;
+  const void *E;
+  template <class R>
+  __device__ __forceinline__ void operator()(int ix, int iy, int iz, R (&en)[8][3]) const {
+    const long long g0 = d.g(ix, iy, iz);
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      node_E<R>(E, g0 + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q)), en[q][0], en[q][1], en[q][2]);
+  }
+};
+
+struct ENodesTile {
+  Dims d;
+  const void *E;
+  const float4 *box;
+  int bx, by, bz;
+  __device__ __forceinline__ void operator()(int ix, int iy, int iz, float (&en)[8][3]) const {
+    const int b0 = box_base(ix, iy, iz, bx, by, bz);
+    if (b0 < 0) {
+      ENodesGlobal{d, E}(ix, iy, iz, en);
+      return;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float4 e = box[b0 + box_off(q)];
+      en[q][0] = e.x;
+      en[q][1] = e.y;
+      en[q][2] = e.z;
+    }
+  }
+};
+
+// slots first..: warp run sums and FP64 atomics into lE
 template <class R>
 __global__ void __launch_bounds__(AB) k_cw_adj_push(Dims d, WinConst c, const void *__restrict__ E, WinS<R> S,
-                                                    const int *__restrict__ count, int step, double wflux,
-                                                    double *__restrict__ lE, double *dBz) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+                                                    const int *__restrict__ count, long long first, int step,
+                                                    double wflux, double *__restrict__ lE, double *dBz) {
+  const long long i = first + blockIdx.x * (long long)blockDim.x + threadIdx.x;
   double gB = 0.0;
   long long key = -1;
   double sc[24];
 #pragma unroll
   for (int q = 0; q < 24; ++q) sc[q] = 0.0;
   if (i < *count) {
-    const int b = S.bl[i];
-    if (born_of(b) <= step && lost_of(b) >= step) {
-      const long long cap = S.cap;
-      int ix, iy, iz;
-      unpack_cell(S.cell[i], ix, iy, iz);
-      const R fx = S.p[i], fy = S.p[cap + i], fz = S.p[2 * cap + i];
-      const R vx = S.p[3 * cap + i], vy = S.p[4 * cap + i], vz = S.p[5 * cap + i];
-      R w[8];
-      weights8<R>(fx, fy, fz, w);
-      const long long g0 = d.g(ix, iy, iz);
-      R Ex, Ey, Ez;
-      gather_E<R>(d, E, g0, w, Ex, Ey, Ez);
-      R lx, ly, lz, lvx, lvy, lvz;
-      if (lost_of(b) == step) {
-        lx = ly = lz = R(0);
-        lvx = lvy = lvz = R(0);
-        if (wflux != 0.0) {
-          R ux = vx, uy = vy, uz = vz;
-          boris<R>(c, Ex, Ey, Ez, ux, uy, uz);
-          const R k = (R)(wflux * c.Nm * c.mass);
-          lvx = k * ux;
-          lvy = k * uy;
-          lvz = k * uz;
-        }
-      } else {
-        lx = S.lam[i];
-        ly = S.lam[cap + i];
-        lz = S.lam[2 * cap + i];
-        lvx = S.lam[3 * cap + i];
-        lvy = S.lam[4 * cap + i];
-        lvz = S.lam[5 * cap + i];
-      }
-      // x^{n+1} = x^n + dt v^{n+1/2}
-      const R dt = (R)c.dt, k1 = (R)c.k1, kk = (R)c.kk;
-      lvx += dt * lx;
-      lvy += dt * ly;
-      lvz += dt * lz;
-      R lEx, lEy, lEz, ux, uy, uz;
-      if (c.boris) {
-        const R Bx = (R)c.Bx, By = (R)c.By, Bz = (R)c.Bz;
-        const R v1x = vx + k1 * Ex, v1y = vy + k1 * Ey, v1z = vz + k1 * Ez;
-        const R v3x = v1x + k1 * (v1y * Bz - v1z * By), v3y = v1y + k1 * (v1z * Bx - v1x * Bz),
-                v3z = v1z + k1 * (v1x * By - v1y * Bx);
-        // d v^{n+1/2} / d Bz: v2 = v1 + kk (v3 x B), v3 = v1 + k1 (v1 x B)
-        const R ax = v3y * Bz - v3z * By, ay = v3z * Bx - v3x * Bz, az = v3x * By - v3y * Bx;   // v3 x B
-        const R bx = v1y, by = -v1x;                                                            // v1 x e_z
-        const R cx = k1 * (by * Bz), cy = k1 * (-bx * Bz), cz = k1 * (bx * By - by * Bx);     // (k1 v1 x e_z) x B
-        const R ex = v3y, ey = -v3x;                                                            // v3 x e_z
-        const R dkk = (R)c.dkk;
-        gB = (double)(lvx * (dkk * ax + kk * (cx + ex)) + lvy * (dkk * ay + kk * (cy + ey)) + lvz * (dkk * az + kk * cz));
-        lEx = k1 * lvx;
-        lEy = k1 * lvy;
-        lEz = k1 * lvz;
-        // l3 = kk (B x lv), u = lv + l3 + k1 (B x l3)
-        const R l3x = kk * (By * lvz - Bz * lvy), l3y = kk * (Bz * lvx - Bx * lvz), l3z = kk * (Bx * lvy - By * lvx);
-        ux = lvx + l3x + k1 * (By * l3z - Bz * l3y);
-        uy = lvy + l3y + k1 * (Bz * l3x - Bx * l3z);
-        uz = lvz + l3z + k1 * (Bx * l3y - By * l3x);
-        lEx += k1 * ux;
-        lEy += k1 * uy;
-        lEz += k1 * uz;
-      } else {
-        ux = lvx;
-        uy = lvy;
-        uz = lvz;
-        lEx = R(2) * k1 * lvx;
-        lEy = R(2) * k1 * lvy;
-        lEz = R(2) * k1 * lvz;
-      }
-      // gather^T (below) and the weight gradient of the gather into lx
-      const R px = R(1) - fx, py = R(1) - fy, pz = R(1) - fz;
-      const R hx = (R)(1.0 / c.h0), hy = (R)(1.0 / c.h1), hz = (R)(1.0 / c.h2);
+    int ix, iy, iz;
+    R r[24];
+    if (cw_adj_push_one<R>(c, ENodesGlobal{d, E}, S, i, step, wflux, ix, iy, iz, r, gB)) {
+      key = d.g(ix, iy, iz);
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        sc[3 * q + 0] = (double)(w[q] * lEx);
-        sc[3 * q + 1] = (double)(w[q] * lEy);
-        sc[3 * q + 2] = (double)(w[q] * lEz);
-        const R ax_ = ox(q) ? R(1) - px : px, ay_ = oy(q) ? R(1) - py : py, az_ = oz(q) ? R(1) - pz : pz;
-        const R sx = ox(q) ? hx : -hx, sy = oy(q) ? hy : -hy, sz = oz(q) ? hz : -hz;
-        R ex_, ey_, ez_;
-        node_E<R>(E, g0 + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q)), ex_, ey_, ez_);
-        const R s = ex_ * lEx + ey_ * lEy + ez_ * lEz;
-        lx += sx * ay_ * az_ * s;
-        ly += ax_ * sy * az_ * s;
-        lz += ax_ * ay_ * sz * s;
-      }
-      key = g0;
-      S.lam[i] = lx;
-      S.lam[cap + i] = ly;
-      S.lam[2 * cap + i] = lz;
-      S.lam[3 * cap + i] = ux;
-      S.lam[4 * cap + i] = uy;
-      S.lam[5 * cap + i] = uz;
+      for (int q = 0; q < 24; ++q) sc[q] = (double)r[q];
     }
   }
-  if (warp_sorted_run_sum<24>(key, sc)) {
+  if (warp_run_sum<24>(key, sc)) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const long long g = key + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
@@ -914,28 +1168,86 @@ __global__ void __launch_bounds__(AB) k_cw_adj_push(Dims d, WinConst c, const vo
   block_add(gB, dBz);
 }
 
+// the FP32 window's push adjoint, one block per tile: E of the tile's node
+// box staged, lE summed in the box (FP32, flushed into FP64 after every
+// WFLUSH particles); dynamic shared memory CW_ADJ_SMEM
+constexpr int CW_ADJ_SMEM = WBN * (16 + 12);
+__global__ void __launch_bounds__(AB, 3) k_cw_adj_push_tiles(Dims d, WinConst c, const float4 *__restrict__ E,
+                                                          WinS<float> S, const int *__restrict__ count, WinTiles T,
+                                                          int step, double wflux, double *__restrict__ lE,
+                                                          double *dBz) {
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  float4 *s_E = reinterpret_cast<float4 *>(s_dyn);
+  float *s_box = reinterpret_cast<float *>(s_dyn + 16 * WBN);
+  int bx, by, bz;
+  tile_box(T, blockIdx.x, bx, by, bz);
+  stage_E_box(d, E, bx, by, bz, s_E);
+  for (int e = threadIdx.x; e < 3 * WBN; e += AB) s_box[e] = 0.f;
+  __syncthreads();
+  const ENodesTile nodes{d, E, s_E, bx, by, bz};
+  const long long N = *count;
+  const long long lo = T.off[blockIdx.x];
+  long long hi = T.off[blockIdx.x + 1];
+  if (hi > N) hi = N;
+  double gB = 0.0;
+  int chunks = 0;
+  for (long long base = lo; base < hi; base += AB) {
+    // every lane takes part in the run sums (base is uniform over the block)
+    const long long i = base + threadIdx.x;
+    int ix = 0, iy = 0, iz = 0;
+    float r[24];
+    long long key = -1;
+    if (i < hi && cw_adj_push_one<float>(c, nodes, S, i, step, wflux, ix, iy, iz, r, gB))
+      key = d.g(ix, iy, iz);
+    else
+#pragma unroll
+      for (int q = 0; q < 24; ++q) r[q] = 0.f;
+    if (warp_run_sum<24, float>(key, r)) {
+      const int b0 = box_base(ix, iy, iz, bx, by, bz);
+      if (b0 >= 0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          float *t = &s_box[3 * (b0 + box_off(q))];
+          atomicAdd(t + 0, r[3 * q + 0]);
+          atomicAdd(t + 1, r[3 * q + 1]);
+          atomicAdd(t + 2, r[3 * q + 2]);
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const long long g = key + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
+          atomicAdd(&lE[3 * g + 0], (double)r[3 * q + 0]);
+          atomicAdd(&lE[3 * g + 1], (double)r[3 * q + 1]);
+          atomicAdd(&lE[3 * g + 2], (double)r[3 * q + 2]);
+        }
+      }
+    }
+    if (++chunks == WFLUSH / AB && base + AB < hi) {
+      chunks = 0;
+      __syncthreads();
+      flush_box<3>(d, s_box, bx, by, bz, nullptr, 1.0, lE);
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  flush_box<3>(d, s_box, bx, by, bz, nullptr, 1.0, lE);
+  block_add(gB, dBz);
+}
+
 // lx += deposit^T of the adjoint potential mu for the particles deposited at
 // `step`: the deposit adds kq kdep w to np, rhs = -q np, so
 // dJ/dx += -q kdep sum_c kq mu grad w_c
-template <class R>
-__global__ void __launch_bounds__(AB) k_cw_adj_deposit(Dims d, WinConst c, WinS<R> S, const int *__restrict__ count,
-                                                       int step, const double *__restrict__ kq,
-                                                       const double *__restrict__ mu) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= *count) return;
-  const int b = S.bl[i];
-  if (!(born_of(b) < step && lost_of(b) >= step)) return;
-  int ix, iy, iz;
-  unpack_cell(S.cell[i], ix, iy, iz);
+// the deposit adjoint of slot i at `step` given the weights m_q = -q kdep kq
+// mu at its cell's 8 nodes (M(q) returns them)
+template <class R, class M>
+__device__ __forceinline__ void cw_adj_dep_one(const WinConst &c, const WinS<R> &S, long long i, M m) {
   const long long cap = S.cap;
   const double fx = S.p[i], fy = S.p[cap + i], fz = S.p[2 * cap + i];
   const double px = 1.0 - fx, py = 1.0 - fy, pz = 1.0 - fz;
-  const long long g0 = d.g(ix, iy, iz);
   double lx = 0.0, ly = 0.0, lz = 0.0;
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
-    const long long g = g0 + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
-    const double s = -c.q * c.kdep * kq[g] * mu[g];
+    const double s = m(q);
     const double ax = ox(q) ? 1.0 - px : px, ay = oy(q) ? 1.0 - py : py, az = oz(q) ? 1.0 - pz : pz;
     const double sx = ox(q) ? 1.0 / c.h0 : -1.0 / c.h0, sy = oy(q) ? 1.0 / c.h1 : -1.0 / c.h1,
                  sz = oz(q) ? 1.0 / c.h2 : -1.0 / c.h2;
@@ -946,6 +1258,64 @@ __global__ void __launch_bounds__(AB) k_cw_adj_deposit(Dims d, WinConst c, WinS<
   S.lam[i] += (R)lx;
   S.lam[cap + i] += (R)ly;
   S.lam[2 * cap + i] += (R)lz;
+}
+
+template <class R>
+__global__ void __launch_bounds__(AB) k_cw_adj_deposit(Dims d, WinConst c, WinS<R> S, const int *__restrict__ count,
+                                                       long long first, int step, const double *__restrict__ kq,
+                                                       const double *__restrict__ mu) {
+  const long long i = first + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= *count) return;
+  const int b = S.bl[i];
+  if (!(born_of(b) < step && lost_of(b) >= step)) return;
+  int ix, iy, iz;
+  unpack_cell(S.cell[i], ix, iy, iz);
+  const long long g0 = d.g(ix, iy, iz);
+  cw_adj_dep_one<R>(c, S, i, [&](int q) {
+    const long long g = g0 + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
+    return -c.q * c.kdep * kq[g] * mu[g];
+  });
+}
+
+// the FP32 window's deposit adjoint, one block per tile: -q kdep kq mu of
+// the tile's node box read into shared memory once
+__global__ void __launch_bounds__(AB) k_cw_adj_deposit_tiles(Dims d, WinConst c, WinS<float> S,
+                                                             const int *__restrict__ count, WinTiles T, int step,
+                                                             const double *__restrict__ kq,
+                                                             const double *__restrict__ mu) {
+  __shared__ double s_m[WBN];
+  int bx, by, bz;
+  tile_box(T, blockIdx.x, bx, by, bz);
+  for (int e = threadIdx.x; e < WBN; e += AB) {
+    const int gx = bx + e % WB, gy = by + (e / WB) % WB, gz = bz + e / (WB * WB);
+    double m = 0.0;
+    if (gx >= 0 && gy >= 0 && gz >= 0 && gx <= d.n1 + 2 && gy <= d.n2 + 2 && gz <= d.n3 + 2) {
+      const long long g = d.g(gx, gy, gz);
+      m = -c.q * c.kdep * kq[g] * mu[g];
+    }
+    s_m[e] = m;
+  }
+  __syncthreads();
+  const long long N = *count;
+  const long long lo = T.off[blockIdx.x];
+  long long hi = T.off[blockIdx.x + 1];
+  if (hi > N) hi = N;
+  for (long long i = lo + threadIdx.x; i < hi; i += AB) {
+    const int b = S.bl[i];
+    if (!(born_of(b) < step && lost_of(b) >= step)) continue;
+    int ix, iy, iz;
+    unpack_cell(S.cell[i], ix, iy, iz);
+    const int b0 = box_base(ix, iy, iz, bx, by, bz);
+    if (b0 >= 0) {
+      cw_adj_dep_one<float>(c, S, i, [&](int q) { return s_m[b0 + box_off(q)]; });
+    } else {
+      const long long g0 = d.g(ix, iy, iz);
+      cw_adj_dep_one<float>(c, S, i, [&](int q) {
+        const long long g = g0 + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
+        return -c.q * c.kdep * kq[g] * mu[g];
+      });
+    }
+  }
 }
 
 // every species of the window, for the collision kernels
@@ -1174,12 +1544,20 @@ int lepic_dev_cw_deposit(const lepic_grid_t *g, const lepic_win_species_t *ws, i
   cudaStream_t s = (cudaStream_t)stream;
   const lepic::WinConst c = lepic::win_const(*g, *P, ptype);
   int tm = lepic::timer_start("cw_deposit", s);
-  if (ws->fp64)
+  if (ws->fp64) {
     lepic::k_cw_deposit<double><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
-        d, c, lepic::win_view<double>(*ws), ws->count, step, g->kq, np);
-  else
-    lepic::k_cw_deposit<float><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
-        d, c, lepic::win_view<float>(*ws), ws->count, step, g->kq, np);
+        d, c, lepic::win_view<double>(*ws), ws->count, 0, step, g->kq, np);
+  } else {
+    long long first = 0;
+    if (ws->tile_off) {
+      const lepic::WinTiles T = lepic::win_tiles(*g, *ws);
+      lepic::k_cw_deposit_tiles<<<LEPIC_TILES(g->n), lepic::AB, 0, s>>>(d, c, lepic::win_view<float>(*ws), ws->count,
+                                                                         T, step, g->kq, np);
+      first = ws->tile_end;
+    }
+    lepic::k_cw_deposit<float><<<lepic::grid_for(ws->cap - first, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, lepic::win_view<float>(*ws), ws->count, first, step, g->kq, np);
+  }
   lepic::timer_stop(tm, s);
   LEPIC_CUDA(cudaGetLastError());
   return LEPIC_OK;
@@ -1193,12 +1571,20 @@ int lepic_dev_cw_push(const lepic_grid_t *g, const void *E, lepic_win_species_t 
   cudaStream_t s = (cudaStream_t)stream;
   const lepic::WinConst c = lepic::win_const(*g, *P, ptype);
   int tm = lepic::timer_start("cw_push", s);
-  if (ws->fp64)
+  if (ws->fp64) {
     lepic::k_cw_push<double><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
-        d, c, E, g->cell_wall, lepic::win_view<double>(*ws), ws->count, step, wall_acc);
-  else
-    lepic::k_cw_push<float><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
-        d, c, E, g->cell_wall, lepic::win_view<float>(*ws), ws->count, step, wall_acc);
+        d, c, E, g->cell_wall, lepic::win_view<double>(*ws), ws->count, 0, step, wall_acc);
+  } else {
+    long long first = 0;
+    if (ws->tile_off) {
+      const lepic::WinTiles T = lepic::win_tiles(*g, *ws);
+      lepic::k_cw_push_tiles<<<LEPIC_TILES(g->n), lepic::AB, 0, s>>>(
+          d, c, (const float4 *)E, g->cell_wall, lepic::win_view<float>(*ws), ws->count, T, step, wall_acc);
+      first = ws->tile_end;
+    }
+    lepic::k_cw_push<float><<<lepic::grid_for(ws->cap - first, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, E, g->cell_wall, lepic::win_view<float>(*ws), ws->count, first, step, wall_acc);
+  }
   lepic::timer_stop(tm, s);
   LEPIC_CUDA(cudaGetLastError());
   return LEPIC_OK;
@@ -1211,12 +1597,21 @@ int lepic_dev_cw_reverse(const lepic_grid_t *g, const void *E, lepic_win_species
   cudaStream_t s = (cudaStream_t)stream;
   const lepic::WinConst c = lepic::win_const(*g, *P, ptype);
   int tm = lepic::timer_start("cw_reverse", s);
-  if (ws->fp64)
+  if (ws->fp64) {
     lepic::k_cw_reverse<double><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
-        d, c, E, lepic::win_view<double>(*ws), ws->count, step);
-  else
-    lepic::k_cw_reverse<float><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
-        d, c, E, lepic::win_view<float>(*ws), ws->count, step);
+        d, c, E, lepic::win_view<double>(*ws), ws->count, 0, step);
+  } else {
+    long long first = 0;
+    if (ws->tile_off) {
+      const lepic::WinTiles T = lepic::win_tiles(*g, *ws);
+      lepic::k_cw_reverse_tiles<<<LEPIC_TILES(g->n), lepic::AB, 0, s>>>(d, c, (const float4 *)E,
+                                                                         lepic::win_view<float>(*ws), ws->count, T,
+                                                                         step);
+      first = ws->tile_end;
+    }
+    lepic::k_cw_reverse<float><<<lepic::grid_for(ws->cap - first, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, E, lepic::win_view<float>(*ws), ws->count, first, step);
+  }
   lepic::timer_stop(tm, s);
   LEPIC_CUDA(cudaGetLastError());
   return LEPIC_OK;
@@ -1229,12 +1624,22 @@ int lepic_dev_cw_adj_push(const lepic_grid_t *g, const void *E, lepic_win_specie
   cudaStream_t s = (cudaStream_t)stream;
   const lepic::WinConst c = lepic::win_const(*g, *P, ptype);
   int tm = lepic::timer_start("cw_adj_push", s);
-  if (ws->fp64)
+  if (ws->fp64) {
     lepic::k_cw_adj_push<double><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
-        d, c, E, lepic::win_view<double>(*ws), ws->count, step, wflux, lE, dBz);
-  else
-    lepic::k_cw_adj_push<float><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
-        d, c, E, lepic::win_view<float>(*ws), ws->count, step, wflux, lE, dBz);
+        d, c, E, lepic::win_view<double>(*ws), ws->count, 0, step, wflux, lE, dBz);
+  } else {
+    long long first = 0;
+    if (ws->tile_off) {
+      const lepic::WinTiles T = lepic::win_tiles(*g, *ws);
+      cudaFuncSetAttribute(lepic::k_cw_adj_push_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           lepic::CW_ADJ_SMEM);
+      lepic::k_cw_adj_push_tiles<<<LEPIC_TILES(g->n), lepic::AB, lepic::CW_ADJ_SMEM, s>>>(
+          d, c, (const float4 *)E, lepic::win_view<float>(*ws), ws->count, T, step, wflux, lE, dBz);
+      first = ws->tile_end;
+    }
+    lepic::k_cw_adj_push<float><<<lepic::grid_for(ws->cap - first, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, E, lepic::win_view<float>(*ws), ws->count, first, step, wflux, lE, dBz);
+  }
   lepic::timer_stop(tm, s);
   LEPIC_CUDA(cudaGetLastError());
   return LEPIC_OK;
@@ -1247,12 +1652,20 @@ int lepic_dev_cw_adj_deposit(const lepic_grid_t *g, lepic_win_species_t *ws, int
   cudaStream_t s = (cudaStream_t)stream;
   const lepic::WinConst c = lepic::win_const(*g, *P, ptype);
   int tm = lepic::timer_start("cw_adj_deposit", s);
-  if (ws->fp64)
+  if (ws->fp64) {
     lepic::k_cw_adj_deposit<double><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
-        d, c, lepic::win_view<double>(*ws), ws->count, step, g->kq, mu);
-  else
-    lepic::k_cw_adj_deposit<float><<<lepic::grid_for(ws->cap, lepic::AB), lepic::AB, 0, s>>>(
-        d, c, lepic::win_view<float>(*ws), ws->count, step, g->kq, mu);
+        d, c, lepic::win_view<double>(*ws), ws->count, 0, step, g->kq, mu);
+  } else {
+    long long first = 0;
+    if (ws->tile_off) {
+      const lepic::WinTiles T = lepic::win_tiles(*g, *ws);
+      lepic::k_cw_adj_deposit_tiles<<<LEPIC_TILES(g->n), lepic::AB, 0, s>>>(d, c, lepic::win_view<float>(*ws),
+                                                                             ws->count, T, step, g->kq, mu);
+      first = ws->tile_end;
+    }
+    lepic::k_cw_adj_deposit<float><<<lepic::grid_for(ws->cap - first, lepic::AB), lepic::AB, 0, s>>>(
+        d, c, lepic::win_view<float>(*ws), ws->count, first, step, g->kq, mu);
+  }
   lepic::timer_stop(tm, s);
   LEPIC_CUDA(cudaGetLastError());
   return LEPIC_OK;

@@ -598,6 +598,16 @@ typedef struct {
   int *count;             /* device int                                       */
   int cap;
   int fp64;               /* 1: p and lam are double planes, 0: float         */
+  const int *tile_off;    /* FP32 window: the slot offsets of the 8^3-cell
+                             tiles of the sort the particles are in
+                             (LEPIC_TILES(n) + 1 device ints), or NULL; the
+                             deposit and the push adjoint then scatter tile
+                             by tile through shared memory (any slot order
+                             gives the same result, the sort's order makes
+                             it fast)                                         */
+  int tile_end;           /* tile_off[LEPIC_TILES(n)] (a host copy): slots
+                             from here on are scattered untiled               */
+  int pad;
 } lepic_win_species_t;
 
 /* One collision of the window's MCC (neutral targets), recorded by the
