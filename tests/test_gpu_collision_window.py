@@ -12,7 +12,7 @@ Bars:
   * the FP64 adjoint (the same events, FP64 particles and multigrid) against
     central finite differences of the FP64 window (events replayed):
     dJ/dV per wall label and dJ/dB_z within 1e-4, a directional derivative in
-    the initial velocities within 1e-3 (steps of 1e-3 V, 1e-9 T, 1e-2 m/s),
+    the initial velocities within 1e-3 (steps of 1e-5 V, 1e-9 T, 1e-2 m/s),
     for the mean electron energy and the probe potential at the box centre;
   * the mixed-precision adjoint (FP32 particles and pushes, FP32 V-cycles in
     FP64 refinement) within 1e-4 of the FP64 adjoint for all three
@@ -91,16 +91,18 @@ def test_fp64_adjoint_vs_central_differences(windows, observable):
     _, _, w64, V, Bz = windows
     w64.forward(V, Bz, observable=observable)
     gV, gB, gv = w64.backward()
+    # small steps: the replayed events are fixed, but an ionization just
+    # above its threshold gives its products a speed growing as the square
+    # root of the energy above it, which curves J within a larger step (the
+    # events a run records depend on the FP32 window's rounding)
+    hV = 1e-5
     fd = []
     for lab in range(len(V)):
         Vp, Vm = list(V), list(V)
-        Vp[lab] += 1e-3
-        Vm[lab] -= 1e-3
-        fd.append((w64.forward(Vp, Bz, observable=observable) - w64.forward(Vm, Bz, observable=observable)) / 2e-3)
+        Vp[lab] += hV
+        Vm[lab] -= hV
+        fd.append((w64.forward(Vp, Bz, observable=observable) - w64.forward(Vm, Bz, observable=observable)) / (2 * hV))
     assert _close(gV, np.array(fd), 1e-4), (gV, fd)
-    # small steps in B_z and v0: an ionization just above its threshold gives
-    # its products a speed growing as the square root of the energy above it,
-    # which curves J within a larger step
     hB = 1e-9
     fB = (w64.forward(V, Bz + hB, observable=observable) - w64.forward(V, Bz - hB, observable=observable)) / (2 * hB)
     assert _close(gB, fB, 1e-4), (gB, fB)
