@@ -452,7 +452,6 @@ def run_adjoint(workload, K, every):
            "observable": "mean kinetic energy (eV) after K steps",
            "J": float(J), "dJ_dV_by_label": [float(x) for x in V.grad], "dJ_dBz": float(Bz.grad),
            "dJ_dv0_norm": float(v0.grad.norm()),
-           "setup_ms": setup_ms, "setup": "one sort of every species by cell, then the window's stores",
            "forward_ms": t["forward_ms"], "backward_ms": t["backward_ms"],
            "backward_over_forward": t["backward_ms"] / t["forward_ms"],
            "backward_kernel_ms": {k: round(v[0], 3) for k, v in sorted(timers.items())}}
@@ -523,6 +522,7 @@ def run_window_adjoint(sim, st, K, observable, production_ms_per_step):
                           "energy": "mean electron kinetic energy after the window (eV)",
                           "flux": "kinetic energy carried to the walls in the window (J)"}[observable],
            "J": J, "dJ_dV_by_label": [float(x) for x in gV], "dJ_dBz": gB, "dJ_dv0_norm": float(gv.norm()),
+           "setup_ms": setup_ms, "setup": "one sort of every species by cell, then the window's stores",
            "forward_ms": t["forward_ms"], "backward_ms": t["backward_ms"],
            "backward_over_forward": t["backward_ms"] / t["forward_ms"],
            "production_forward_ms": production_ms_per_step * K,
