@@ -924,19 +924,39 @@ __device__ void stage_E_box(const Dims &d, const float4 *__restrict__ E, int bx,
   }
 }
 
+// the stored state of slot i (history word, cell, offsets, velocities),
+// read in one go so that a thread can have two slots' loads in flight
+template <class R>
+struct PSt {
+  int b, cell;
+  R f[3], v[3];
+};
+template <class R>
+__device__ __forceinline__ void pst_load(const WinS<R> &S, long long i, PSt<R> &s) {
+  const long long cap = S.cap;
+  s.b = S.bl[i];
+  s.cell = S.cell[i];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    s.f[a] = S.p[a * cap + i];
+    s.v[a] = S.p[(3 + a) * cap + i];
+  }
+}
+
 // push of step `step`; a particle whose new cell is a wall cell (or outside
 // the grid) is lost at this step and keeps its state from before the push;
 // wl += the kinetic energy (J) the lost macroparticle carries
 template <class R, class G>
 __device__ __forceinline__ void cw_push_one(const Dims &d, const WinConst &c, const unsigned char *__restrict__ cw,
-                                            const WinS<R> &S, long long i, int step, const G &gather, double &wl) {
-  const int b = S.bl[i];
+                                            const WinS<R> &S, long long i, const PSt<R> &st, int step,
+                                            const G &gather, double &wl) {
+  const int b = st.b;
   if (!(born_of(b) <= step && lost_of(b) >= step)) return;
   int ix, iy, iz;
-  unpack_cell(S.cell[i], ix, iy, iz);
+  unpack_cell(st.cell, ix, iy, iz);
   const long long cap = S.cap;
-  R fx = S.p[i], fy = S.p[cap + i], fz = S.p[2 * cap + i];
-  R vx = S.p[3 * cap + i], vy = S.p[4 * cap + i], vz = S.p[5 * cap + i];
+  R fx = st.f[0], fy = st.f[1], fz = st.f[2];
+  R vx = st.v[0], vy = st.v[1], vz = st.v[2];
   R w[8];
   weights8<R>(fx, fy, fz, w);
   R Ex, Ey, Ez;
@@ -971,14 +991,18 @@ __global__ void __launch_bounds__(AB) k_cw_push(Dims d, WinConst c, const void *
                                                 double *wall_acc) {
   const long long i = first + blockIdx.x * (long long)blockDim.x + threadIdx.x;
   double wl = 0.0;
-  if (i < *count) cw_push_one<R>(d, c, cw, S, i, step, EGlobal{d, E}, wl);
+  if (i < *count) {
+    PSt<R> st;
+    pst_load<R>(S, i, st);
+    cw_push_one<R>(d, c, cw, S, i, st, step, EGlobal{d, E}, wl);
+  }
   block_add(wl, wall_acc);
 }
 
 // the FP32 window's push, one block per tile, E of the tile's box staged.
 // (A variant that also deposited the kept particles for the next step, in a
 // node box beside E, was 4 % slower than this push and k_cw_deposit_tiles.)
-__global__ void __launch_bounds__(AB) k_cw_push_tiles(Dims d, WinConst c, const float4 *__restrict__ E,
+__global__ void __launch_bounds__(AB, 3) k_cw_push_tiles(Dims d, WinConst c, const float4 *__restrict__ E,
                                                       const unsigned char *__restrict__ cw, WinS<float> S,
                                                       const int *__restrict__ count, WinTiles T, int step,
                                                       double *wall_acc) {
@@ -993,7 +1017,15 @@ __global__ void __launch_bounds__(AB) k_cw_push_tiles(Dims d, WinConst c, const 
   long long hi = T.off[blockIdx.x + 1];
   if (hi > N) hi = N;
   double wl = 0.0;
-  for (long long i = lo + threadIdx.x; i < hi; i += AB) cw_push_one<float>(d, c, cw, S, i, step, G, wl);
+  // two slots per pass, both loaded before either is pushed
+  for (long long i = lo + threadIdx.x; i < hi; i += 2 * AB) {
+    const long long j = i + AB;
+    PSt<float> s0, s1;
+    pst_load<float>(S, i, s0);
+    if (j < hi) pst_load<float>(S, j, s1);
+    cw_push_one<float>(d, c, cw, S, i, s0, step, G, wl);
+    if (j < hi) cw_push_one<float>(d, c, cw, S, j, s1, step, G, wl);
+  }
   block_add(wl, wall_acc);
 }
 
@@ -1001,14 +1033,14 @@ __global__ void __launch_bounds__(AB) k_cw_push_tiles(Dims d, WinConst c, const 
 // x^{n+1} and v^{n+1/2}, then v+ by the inverse rotation with E^n at x^n
 template <class R, class G>
 __device__ __forceinline__ void cw_reverse_one(const Dims &d, const WinConst &c, const WinS<R> &S, long long i,
-                                               int step, const G &gather) {
-  const int b = S.bl[i];
+                                               const PSt<R> &st, int step, const G &gather) {
+  const int b = st.b;
   if (!(born_of(b) <= step && lost_of(b) > step)) return;
   int ix, iy, iz;
-  unpack_cell(S.cell[i], ix, iy, iz);
+  unpack_cell(st.cell, ix, iy, iz);
   const long long cap = S.cap;
-  R fx = S.p[i], fy = S.p[cap + i], fz = S.p[2 * cap + i];
-  R vx = S.p[3 * cap + i], vy = S.p[4 * cap + i], vz = S.p[5 * cap + i];
+  R fx = st.f[0], fy = st.f[1], fz = st.f[2];
+  R vx = st.v[0], vy = st.v[1], vz = st.v[2];
   ix += move_offset<R>(fx, -vx * (R)(c.dt / c.h0));
   iy += move_offset<R>(fy, -vy * (R)(c.dt / c.h1));
   iz += move_offset<R>(fz, -vz * (R)(c.dt / c.h2));
@@ -1033,10 +1065,14 @@ template <class R>
 __global__ void __launch_bounds__(AB) k_cw_reverse(Dims d, WinConst c, const void *__restrict__ E, WinS<R> S,
                                                    const int *__restrict__ count, long long first, int step) {
   const long long i = first + blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i < *count) cw_reverse_one<R>(d, c, S, i, step, EGlobal{d, E});
+  if (i < *count) {
+    PSt<R> st;
+    pst_load<R>(S, i, st);
+    cw_reverse_one<R>(d, c, S, i, st, step, EGlobal{d, E});
+  }
 }
 
-__global__ void __launch_bounds__(AB) k_cw_reverse_tiles(Dims d, WinConst c, const float4 *__restrict__ E,
+__global__ void __launch_bounds__(AB, 3) k_cw_reverse_tiles(Dims d, WinConst c, const float4 *__restrict__ E,
                                                          WinS<float> S, const int *__restrict__ count, WinTiles T,
                                                          int step) {
   __shared__ float4 s_E[WBN];
@@ -1049,7 +1085,14 @@ __global__ void __launch_bounds__(AB) k_cw_reverse_tiles(Dims d, WinConst c, con
   const long long lo = T.off[blockIdx.x];
   long long hi = T.off[blockIdx.x + 1];
   if (hi > N) hi = N;
-  for (long long i = lo + threadIdx.x; i < hi; i += AB) cw_reverse_one<float>(d, c, S, i, step, G);
+  for (long long i = lo + threadIdx.x; i < hi; i += 2 * AB) {
+    const long long j = i + AB;
+    PSt<float> s0, s1;
+    pst_load<float>(S, i, s0);
+    if (j < hi) pst_load<float>(S, j, s1);
+    cw_reverse_one<float>(d, c, S, i, s0, step, G);
+    if (j < hi) cw_reverse_one<float>(d, c, S, j, s1, step, G);
+  }
 }
 
 // adjoint of the push of step `step` at the state (x^n, v+) for the
@@ -1353,20 +1396,31 @@ __global__ void __launch_bounds__(AB) k_cw_adj_deposit_tiles(Dims d, WinConst c,
   const long long lo = T.off[blockIdx.x];
   long long hi = T.off[blockIdx.x + 1];
   if (hi > N) hi = N;
-  for (long long i = lo + threadIdx.x; i < hi; i += AB) {
-    const int b = S.bl[i];
-    if (!(born_of(b) < step && lost_of(b) >= step)) continue;
-    int ix, iy, iz;
-    unpack_cell(S.cell[i], ix, iy, iz);
-    const int b0 = box_base(ix, iy, iz, bx, by, bz);
-    if (b0 >= 0) {
-      cw_adj_dep_one<float>(c, S, i, [&](int q) { return s_m[b0 + box_off(q)]; });
-    } else {
-      const long long g0 = d.g(ix, iy, iz);
-      cw_adj_dep_one<float>(c, S, i, [&](int q) {
-        const long long g = g0 + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
-        return -c.q * c.kdep * kq[g] * mu[g];
-      });
+  // two slots per pass: both slots' history words and cells read first
+  for (long long i0 = lo + threadIdx.x; i0 < hi; i0 += 2 * AB) {
+    int bb[2], cc[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const long long i = i0 + u * AB;
+      bb[u] = i < hi ? S.bl[i] : -1;
+      cc[u] = i < hi ? S.cell[i] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const long long i = i0 + u * AB;
+      if (i >= hi || !(born_of(bb[u]) < step && lost_of(bb[u]) >= step)) continue;
+      int ix, iy, iz;
+      unpack_cell(cc[u], ix, iy, iz);
+      const int b0 = box_base(ix, iy, iz, bx, by, bz);
+      if (b0 >= 0) {
+        cw_adj_dep_one<float>(c, S, i, [&](int q) { return s_m[b0 + box_off(q)]; });
+      } else {
+        const long long g0 = d.g(ix, iy, iz);
+        cw_adj_dep_one<float>(c, S, i, [&](int q) {
+          const long long g = g0 + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
+          return -c.q * c.kdep * kq[g] * mu[g];
+        });
+      }
     }
   }
 }
