@@ -24,6 +24,8 @@
 //   the gather-weight gradient of the field term.
 #include <cstring>
 
+#include <type_traits>
+
 #include "lepic_internal.cuh"
 
 namespace lepic {
@@ -788,8 +790,16 @@ __global__ void __launch_bounds__(AB) k_cw_deposit(Dims d, WinConst c, WinS<R> S
     R w[8];
     if (cw_dep_one<R>(S, i, step, ix, iy, iz, w)) {
       key = d.g(ix, iy, iz);
+      if constexpr (std::is_same<R, float>::value) {
+        // the FP32 window deposits the integer weights of the mixed step
+        int qw[8];
+        qweights(S.p[i], S.p[S.cap + i], S.p[2 * S.cap + i], qw);
 #pragma unroll
-      for (int q = 0; q < 8; ++q) v[q] = (double)w[q];
+        for (int q = 0; q < 8; ++q) v[q] = (double)qw[q] * QI;
+      } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = (double)w[q];
+      }
     }
   }
   if (warp_run_sum<8>(key, v)) {
@@ -831,14 +841,34 @@ __device__ void flush_box(const Dims &d, float *box, int bx, int by, int bz, con
   }
 }
 
-// the FP32 window's deposit, one block per tile
+// the box's non-zero integer weight sums (units of 2^-QBITS, exact modulo
+// 2^32: a node's sum over WFLUSH particles lies in [-5 WFLUSH, 2^31]) into
+// the FP64 grid, kdep kq applied, then cleared
+__device__ void flush_qbox(const Dims &d, unsigned *box, int bx, int by, int bz, const double *__restrict__ kq,
+                           double kdep, double *__restrict__ np) {
+  for (int e = threadIdx.x; e < WBN; e += blockDim.x) {
+    const unsigned v = box[e];
+    if (!v) continue;
+    const int gx = bx + e % WB, gy = by + (e / WB) % WB, gz = bz + e / (WB * WB);
+    if (gx >= 0 && gy >= 0 && gz >= 0 && gx <= d.n1 + 2 && gy <= d.n2 + 2 && gz <= d.n3 + 2) {
+      const long long g = d.g(gx, gy, gz);
+      const double val = v <= 0x80000000u ? (double)v : (double)v - 4294967296.0;
+      atomicAdd(&np[g], kq[g] * (kdep * (val * QI)));
+    }
+    box[e] = 0u;
+  }
+}
+static_assert((long long)WFLUSH << QBITS <= (1LL << 31), "node sums of a flush window fit 2^31");
+
+// the FP32 window's deposit, one block per tile: the integer weights of the
+// mixed step (2^20 units per particle), summed exactly in a 32-bit node box
 __global__ void __launch_bounds__(AB) k_cw_deposit_tiles(Dims d, WinConst c, WinS<float> S, const int *__restrict__ count,
                                                          WinTiles T, int step, const double *__restrict__ kq,
                                                          double *__restrict__ np) {
-  __shared__ float s_box[WBN];
+  __shared__ unsigned s_box[WBN];
   int bx, by, bz;
   tile_box(T, blockIdx.x, bx, by, bz);
-  for (int e = threadIdx.x; e < WBN; e += AB) s_box[e] = 0.f;
+  for (int e = threadIdx.x; e < WBN; e += AB) s_box[e] = 0u;
   __syncthreads();
   const long long N = *count;
   const long long lo = T.off[blockIdx.x];
@@ -849,35 +879,37 @@ __global__ void __launch_bounds__(AB) k_cw_deposit_tiles(Dims d, WinConst c, Win
     // every lane takes part in the run sums (base is uniform over the block)
     const long long i = base + threadIdx.x;
     int ix = 0, iy = 0, iz = 0;
-    float w[8];
+    int w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long key = -1;
-    int b0 = -1;
-    if (i < hi && cw_dep_one<float>(S, i, step, ix, iy, iz, w)) {
+    float wf[8];
+    if (i < hi && cw_dep_one<float>(S, i, step, ix, iy, iz, wf)) {
       key = d.g(ix, iy, iz);
-      b0 = box_base(ix, iy, iz, bx, by, bz);
-    } else {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) w[q] = 0.f;
+      qweights(S.p[i], S.p[S.cap + i], S.p[2 * S.cap + i], w);
     }
     // the lanes of one cell (consecutive in the sort's order) are summed
     // first, so a cell's particles do not contend for the same shared words
-    warp_scatter_sum<8>(key, b0, w, [&](long long k, int b, int q, float val) {
-      if (b >= 0) {
-        atomicAdd(&s_box[b + box_off(q)], val);
+    if (warp_run_sum<8, int>(key, w)) {
+      const int b0 = box_base(ix, iy, iz, bx, by, bz);
+      if (b0 >= 0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) atomicAdd(&s_box[b0 + box_off(q)], (unsigned)w[q]);
       } else {
-        const long long g = k + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
-        atomicAdd(&np[g], kq[g] * (c.kdep * (double)val));
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const long long g = key + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
+          atomicAdd(&np[g], kq[g] * (c.kdep * ((double)w[q] * QI)));
+        }
       }
-    });
+    }
     if (++chunks == WFLUSH / AB && base + AB < hi) {
       chunks = 0;
       __syncthreads();
-      flush_box<1>(d, s_box, bx, by, bz, kq, c.kdep, np);
+      flush_qbox(d, s_box, bx, by, bz, kq, c.kdep, np);
       __syncthreads();
     }
   }
   __syncthreads();
-  flush_box<1>(d, s_box, bx, by, bz, kq, c.kdep, np);
+  flush_qbox(d, s_box, bx, by, bz, kq, c.kdep, np);
 }
 
 // E gathers of a cell's 8 nodes in the order of gather_E: from the FP32 /

@@ -41,8 +41,6 @@ constexpr int TC = LEPIC_TILE_CELLS;       // tile edge in cells
 constexpr int TN = TC + 3;                 // node tile edge (halo cell each side)
 constexpr int TT = TN * TN * TN;
 constexpr int CHUNK = 4 * MBK;             // particles per block iteration
-constexpr int QBITS = 20;                  // 2^20 weight units per particle
-constexpr double QI = 1.0 / 1048576.0;
 constexpr int FLUSH_PARTICLES = 2048;      // node sums <= 2048 * 2^20 = 2^31
 static_assert(FLUSH_PARTICLES % CHUNK == 0, "flush windows are whole chunks");
 constexpr int CB = LEPIC_CELL_BITS, CM = LEPIC_CELL_MAX - 1;
@@ -95,32 +93,6 @@ __device__ __noinline__ void dielectric_charge_cells(Dielectric die, long long N
     atomicAdd(&q[2 * (cy + 1 + NY * (cz + 1))], die.k3 * (1.0 - py) * (1.0 - pz));
     atomicAdd(&q[2 * (cy + NY * (cz + 1))], die.k3 * py * (1.0 - pz));
   }
-}
-
-// x rounded to the nearest integer for 0 <= x <= 2^22, by the FP32 addition
-// of 1.5 * 2^23 (whose unit in the last place is 1) and integer arithmetic
-// (weights are at most 2^QBITS <= 2^22)
-__device__ __forceinline__ int round_q(float x) { return __float_as_int(x + 12582912.f) - 0x4B400000; }
-
-// integer CIC weights of offsets (gx, gy, gz) in units of 2^-20 summing to
-// exactly 2^20 (node order of Src/part_expmover.f90:591-656: (0,0,0),
-// (1,0,0), (1,1,0), (0,1,0), then the same at z+1): seven rounded, the
-// eighth the remainder.  The remainder may be a few units below zero for a
-// particle next to the opposite corner (the seven rounding errors are at
-// most 0.7 units each); the 32-bit node sums are exact modulo 2^32 and
-// flush_tile reads them back from that range.
-__device__ __forceinline__ void qweights(float gx, float gy, float gz, int w[8]) {
-  const float S = (float)(1 << QBITS);
-  const float qx = 1.f - gx, qy = 1.f - gy, qz = 1.f - gz;
-  const float a = qy * qz * S, b = gy * qz * S, e = qy * gz * S, f = gy * gz * S;
-  w[0] = round_q(qx * a);
-  w[1] = round_q(gx * a);
-  w[2] = round_q(gx * b);
-  w[3] = round_q(qx * b);
-  w[4] = round_q(qx * e);
-  w[5] = round_q(gx * e);
-  w[6] = round_q(gx * f);
-  w[7] = (1 << QBITS) - (w[0] + w[1] + w[2] + w[3] + w[4] + w[5] + w[6]);
 }
 
 // FP32 copy of the B-field map (Src/part_expmover.f90:148-203): one float4
