@@ -597,66 +597,40 @@ __device__ __noinline__ void coarse_cycle(const XArgs &a, unsigned char *sm) {
 // FP64 residual b - A u of the finest level on its interior nodes, written
 // as the FP32 right-hand side of the V-cycle (+inf on walls), the correction
 // cleared; returns this thread's share of the L1 norm over the plasma nodes
-// (bcnd = -1).  Each thread takes U nodes at once and issues all their
-// loads before any arithmetic.
+// (bcnd = -1).  (A flat node index per thread, with two integer divisions per
+// node, made this phase 7 % of the 128^3 solve slower.)
 __device__ __noinline__ double g_residual_f64(const XArgs &a, const GLev &L1, float *e1) {
-  constexpr int U = 2;
-  const int tid = (int)(blockIdx.x * blockDim.x + threadIdx.x), nth = (int)(gridDim.x * blockDim.x);
-  const int ni = L1.n1 + 1, nj = L1.n2 + 1;
-  const int total = ni * nj * (L1.n3 + 1);
+  // one grid row (j, k) per warp at a time, the lanes along i: coalesced
+  // loads, no division per node, the arguments in registers
+  const int lane = threadIdx.x & 31;
+  const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+  const int ni = L1.n1 + 1, nj = L1.n2 + 1, nk = L1.n3 + 1;
   const long long sy = L1.n1 + 3, sz = (long long)(L1.n1 + 3) * (L1.n2 + 3);
   const long long ry = L1.n1 + 2, rz = (long long)(L1.n1 + 2) * (L1.n2 + 2);
-  const double *u = a.u;
+  const double *__restrict__ u = a.u;
+  const double *__restrict__ bb = a.b;
+  const int *__restrict__ bcnd = a.bcnd;
+  const double aw = a.aw, an = a.an, at = a.at, ac = a.ac;
+  float *__restrict__ r1 = L1.r;
+  float *__restrict__ e = e1;
   double acc = 0.0;
-  for (int base = tid; base < total; base += U * nth) {
-    long long q[U], rq[U];
-    int ii[U], jj[U], kk[U];
-    bool ok[U];
-#pragma unroll
-    for (int v = 0; v < U; ++v) {
-      const int t = base + v * nth;
-      ok[v] = t < total;
-      q[v] = rq[v] = 0;
-      ii[v] = jj[v] = kk[v] = 1;
-      if (ok[v]) {
-        const int row = t / ni, i = t - row * ni + 1;
-        const int k = row / nj + 1, j = row - (k - 1) * nj + 1;
-        ii[v] = i;
-        jj[v] = j;
-        kk[v] = k;
-        q[v] = i + sy * j + sz * k;
-        rq[v] = i + ry * j + rz * k;
-      }
-    }
-    int bc[U];
-    double bv[U], c0[U], uw[U], un[U], us[U], ue[U], ut[U], ub[U];
-#pragma unroll
-    for (int v = 0; v < U; ++v) {
-      if (!ok[v]) continue;
-      const long long w = q[v];
-      bc[v] = a.bcnd[w];
-      bv[v] = a.b[rq[v]];
-      c0[v] = u[w];
-      uw[v] = u[w - 1];
-      un[v] = u[w + sy];
-      us[v] = u[w - sy];
-      ue[v] = u[w + 1];
-      ut[v] = u[w + sz];
-      ub[v] = u[w - sz];
-    }
-#pragma unroll
-    for (int v = 0; v < U; ++v) {
-      if (!ok[v]) continue;
+  for (int row = gw; row < nj * nk; row += nw) {
+    const int k = row / nj + 1, j = row - (k - 1) * nj + 1;
+    const long long w0 = sy * j + sz * k, r0 = ry * j + rz * k, o0 = L1.g(0, j, k);
+#pragma unroll 2
+    for (int i = 1 + lane; i <= ni; i += 32) {
+      const long long w = w0 + i;
+      const int bc = bcnd[w];
+      const double bv = bb[r0 + i], c0 = u[w], uw = u[w - 1], un = u[w + sy], us = u[w - sy], ue = u[w + 1],
+                   ut = u[w + sz], ub = u[w - sz];
       float rf = INFINITY;
-      if (bc[v] <= 0) {
-        const double rv = bv[v] - (a.aw * uw[v] + a.an * un[v] + a.an * us[v] + a.aw * ue[v] + a.ac * c0[v] +
-                                   a.at * ut[v] + a.at * ub[v]);
-        if (bc[v] == -1) acc += fabs(rv);
+      if (bc <= 0) {
+        const double rv = bv - (aw * uw + an * un + an * us + aw * ue + ac * c0 + at * ut + at * ub);
+        if (bc == -1) acc += fabs(rv);
         rf = (float)rv;
       }
-      const long long o = L1.g(ii[v], jj[v], kk[v]);
-      L1.r[o] = rf;
-      e1[o] = 0.f;
+      r1[o0 + i] = rf;
+      e[o0 + i] = 0.f;
     }
   }
   return acc;
