@@ -457,9 +457,27 @@ __device__ __noinline__ void tile_pass(const XArgs &a, const XMaps &maps, int l,
 template <class F>
 __device__ __forceinline__ void block_box(int i0, int ni, int j0, int nj, int k0, int nk, F &&body) {
   const int tot = ni * nj * nk;
-  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-    const int row = t / ni, k = row / nj;
-    body(i0 + (t - row * ni), j0 + (row - k * nj), k0 + k);
+  int t = threadIdx.x;
+  if (t >= tot) return;
+  // (i, j, k) of the thread's first element, then stepped by the block size
+  // with carries instead of two integer divisions per element
+  const int row0 = t / ni;
+  int i = t - row0 * ni, k = row0 / nj, j = row0 - k * nj;
+  const int bd = blockDim.x, srow = bd / ni, si = bd - srow * ni;   // bd = srow ni + si
+  const int sk = srow / nj, sj = srow - sk * nj;                    // srow = sk nj + sj
+  for (; t < tot; t += bd) {
+    body(i0 + i, j0 + j, k0 + k);
+    i += si;
+    j += sj;
+    k += sk;
+    if (i >= ni) {
+      i -= ni;
+      ++j;
+    }
+    if (j >= nj) {
+      j -= nj;
+      ++k;
+    }
   }
 }
 
@@ -636,19 +654,22 @@ __device__ __noinline__ double g_residual_f64(const XArgs &a, const GLev &L1, fl
   return acc;
 }
 
-// r = +inf on the ghost nodes of level 1 (never updated, correction 0)
+// r = +inf on the ghost nodes of level 1 (never updated, correction 0):
+// one grid row (j, k) per warp, the whole row on the ghost planes j, k = 0,
+// n + 2, else its two end nodes
 __device__ __noinline__ void g_ghosts(const GLev &L) {
-  const int tid = (int)(blockIdx.x * blockDim.x + threadIdx.x), nth = (int)(gridDim.x * blockDim.x);
+  const int lane = threadIdx.x & 31;
+  const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
   const int N1 = L.n1 + 3, N2 = L.n2 + 3, N3 = L.n3 + 3;
-  const int total = N1 * N2 * N3;
-  // the ghost faces: planes k = 0, n3+2, rows j = 0, n2+2, columns i = 0, n1+2
-  for (int t = tid; t < total; t += nth) {
-    const int row = t / N1, i = t - row * N1;
+  for (int row = gw; row < N2 * N3; row += nw) {
     const int k = row / N2, j = row - k * N2;
-    if (i == 0 || j == 0 || k == 0 || i == N1 - 1 || j == N2 - 1 || k == N3 - 1) {
-      L.r[L.g(i, j, k)] = INFINITY;
-      L.e[0][L.g(i, j, k)] = 0.f;
-      L.e[1][L.g(i, j, k)] = 0.f;
+    const bool face = j == 0 || k == 0 || j == N2 - 1 || k == N3 - 1;
+    for (int t = lane; t < (face ? N1 : 2); t += 32) {
+      const int i = face ? t : (t == 0 ? 0 : N1 - 1);
+      const long long q = L.g(i, j, k);
+      L.r[q] = INFINITY;
+      L.e[0][q] = 0.f;
+      L.e[1][q] = 0.f;
     }
   }
 }
