@@ -467,13 +467,7 @@ void part_mover_(const int *n, const double *h, const double *Ei, const double *
                  const int *iproc, const int *ptype, int *flag_cex, int *cnt_cex, double *cnt_dead,
                  double *beam_div, double *sum_q_xz, double *sum_q_yz, const int *dtype,
                  int *iseed, const int *n_B, const double *h_B) {
-  (void)flag_cex;
-  (void)cnt_cex;
-  (void)cnt_dead;
-  (void)beam_div;
-  (void)iseed;
   if (*nproc != 1 || *iproc != 1) return record(LEPIC_ERR_UNSUPPORTED);
-  if (part_info_int_.tag_neg == *ptype || part_info_dp_1_.gam_sec > 0.0) return record(LEPIC_ERR_UNSUPPORTED);
   lepic_phys_t P = phys_from_common(*ntype);
   cudaStream_t s = 0;
   Dims d(n);
@@ -516,12 +510,87 @@ void part_mover_(const int *n, const double *h, const double *Ei, const double *
     if (!rc) rc = cuda_ok(cudaMemsetAsync(qyz_d, 0, sizeof(double) * nyz, s), "memset");
     if (rc) return record(rc);
   }
+  // negative ions (this species is tag_neg): flag_cex(1:nmax) follows the
+  // particles; cnt_cex(3), cnt_dead(1), beam_div(4) accumulate
+  // (Src/part_expmover.f90:76, 278-301, 416-470)
+  MoverExtras ex;
+  memset(&ex, 0, sizeof(ex));
+  ex.tag_neg = part_info_int_.tag_neg;
+  ex.tag_neu = part_info_int_.tag_neu;
+  ex.num_grd = part_info_int_.num_grd;
+  const bool neg = ex.tag_neg == *ptype;
+  double *xacc = nullptr;   // cnt_dead, beam_div(4), P_loss(4,1)
+  int *xcnt = nullptr;      // cnt_cex(3)
+  if (neg) {
+    if (!flag_cex || !cnt_cex || !cnt_dead || !beam_div) return record(LEPIC_ERR_ARG);
+    ex.cex = upload("dropin_cex", flag_cex, (size_t)*nmax, s);
+    ex.cex_out = (int *)scratch("dropin_cex_out", sizeof(int) * (size_t)*nmax);
+    if (!ex.cex || !ex.cex_out) return record(LEPIC_ERR_CUDA);
+  }
+  // secondary emission from positive ions on the emissive grid, appended to
+  // the electrons (species 1) (Src/part_expmover.f90:353-400)
+  const bool sec = part_info_dp_1_.gam_sec > 0.0 && P.charge[p] > 0.0;
+  if (neg || sec) {
+    xacc = (double *)scratch("dropin_xacc", sizeof(double) * 6);
+    xcnt = (int *)scratch("dropin_xcnt", sizeof(int) * 3);
+    if (!xacc || !xcnt) return record(LEPIC_ERR_CUDA);
+    rc = cuda_ok(cudaMemsetAsync(xacc, 0, sizeof(double) * 6, s), "memset");
+    if (!rc) rc = cuda_ok(cudaMemsetAsync(xcnt, 0, sizeof(int) * 3, s), "memset");
+    if (rc) return record(rc);
+    ex.cnt_dead = xacc;
+    ex.beam_div = xacc + 1;
+    ex.ploss4 = xacc + 5;
+    ex.cnt_cex = xcnt;
+  }
+  SpeciesView v1;
+  if (sec) {
+    if (!iseed) return record(LEPIC_ERR_ARG);
+    ex.gam_sec = part_info_dp_1_.gam_sec;
+    ex.THm = part_info_dp_1_.THm;
+    ex.zg_sec[0] = part_info_dp_1_.zg_sec[0];
+    ex.zg_sec[1] = part_info_dp_1_.zg_sec[1];
+    ex.igrid_sec = part_info_int_.igrid_sec;
+    // the draws are keyed by the caller's ran2 seed, which then advances one
+    // ran2 step so that the next call draws differently
+    ex.key0 = (uint32_t)*iseed;
+    ex.key1 = 0x4C455049u;
+    ex.call = (uint32_t)*ptype;
+    {
+      const int ia = 16807, im = 2147483647, iq = 127773, ir = 2836;
+      const int k = *iseed / iq;
+      *iseed = ia * (*iseed - k * iq) - ir * k;
+      if (*iseed < 0) *iseed += im;
+    }
+    if (p == 0) return record(LEPIC_ERR_ARG);
+    rc = acquire_species(v1, vxp, np_tot[0], *nmax, 1, nullptr, s);
+    if (rc) return record(rc);
+    ex.e1 = &v1.s;
+  }
   SpeciesView v;
   rc = acquire_species(v, vxp_p, np_tot[p], *nmax, 0, fd_p, s);
   if (rc) return record(rc);
-  rc = launch_part_mover(g, E_d, v.s, *ptype, *ntype, *ngrid, P, p_mac, P_loss, s, dt_d, qxz_d, qyz_d);
+  rc = launch_part_mover(g, E_d, v.s, *ptype, *ntype, *ngrid, P, p_mac, P_loss, s, dt_d, qxz_d, qyz_d,
+                         (neg || sec) ? &ex : nullptr);
   record(rc);
   record(release_species(v, &np_tot[p], fd_p, *nmax, true, s));
+  if (sec) record(release_species(v1, &np_tot[0], nullptr, *nmax, true, s));
+  if ((neg || sec) && !rc) {
+    double hx[6];
+    int hc[3];
+    rc = cuda_ok(cudaMemcpyAsync(hx, xacc, sizeof(hx), cudaMemcpyDeviceToHost, s), "copy");
+    if (!rc) rc = cuda_ok(cudaMemcpyAsync(hc, xcnt, sizeof(hc), cudaMemcpyDeviceToHost, s), "copy");
+    if (!rc && neg)
+      rc = cuda_ok(cudaMemcpyAsync(flag_cex, ex.cex_out, sizeof(int) * (size_t)np_tot[p], cudaMemcpyDeviceToHost, s),
+                   "copy");
+    if (!rc) rc = cuda_ok(cudaStreamSynchronize(s), "sync");
+    record(rc);
+    if (!rc && neg) {
+      *cnt_dead += hx[0];
+      for (int a = 0; a < 4; ++a) beam_div[a] += hx[1 + a];
+      for (int a = 0; a < 3; ++a) cnt_cex[a] += hc[a];
+    }
+    if (!rc && sec && P_loss) P_loss[3] += hx[5];
+  }
   if (die && !rc) {
     std::vector<double> hxz(nxz), hyz(nyz);
     rc = cuda_ok(cudaMemcpyAsync(hxz.data(), qxz_d, sizeof(double) * nxz, cudaMemcpyDeviceToHost, s), "copy");

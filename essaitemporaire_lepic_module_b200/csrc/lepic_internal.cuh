@@ -250,13 +250,31 @@ int launch_pdesolver(const Dims &d, const double h[3], double *u, const double *
                      int ncycl, double eps, double omega, int ng, double eps0, int *k, double *ktot,
                      double *res, cudaStream_t s, int pbc = 0, int nmn = 0);
 // particles.cu
+// The drop-in mover's negative-ion bookkeeping (species tag_neg: flag_cex in
+// slot order in cex, compacted into cex_out; device counters cnt_cex[3],
+// cnt_dead, beam_div[4] accumulated) and secondary emission (gam_sec > 0, a
+// positive species: electrons appended to species e1, *ploss4 accumulated,
+// Philox key key0/key1/call).  Src/part_expmover.f90:76, 278-301, 353-470.
+struct MoverExtras {
+  int tag_neg, tag_neu, num_grd;
+  const int *cex;
+  int *cex_out;
+  int *cnt_cex;
+  double *cnt_dead;
+  double *beam_div;
+  double gam_sec, THm, zg_sec[2];
+  int igrid_sec;
+  lepic_species_f64_t *e1;
+  double *ploss4;
+  uint32_t key0, key1, call;
+};
 // dtype_dev (device dtype(0:ngrid)) with qxz_dev / qyz_dev (device planes of
 // the species pushed): the charge of particles lost on dielectric walls
 // (without them, the walls of P, if any)
 int launch_part_mover(const lepic_grid_t &g, const double *Ei, lepic_species_f64_t &sp, int ptype,
                       int ntype, int ngrid, const lepic_phys_t &P, double *p_mac, double *P_loss,
                       cudaStream_t s, const int *dtype_dev = nullptr, double *qxz_dev = nullptr,
-                      double *qyz_dev = nullptr);
+                      double *qyz_dev = nullptr, const MoverExtras *ex = nullptr);
 int launch_deposit(const lepic_grid_t &g, const lepic_species_f64_t &sp, int ptype,
                    const lepic_phys_t &P, double *np, cudaStream_t s);
 int launch_sort(const lepic_grid_t &g, lepic_species_f64_t &sp, int *Plist, int pl_max,

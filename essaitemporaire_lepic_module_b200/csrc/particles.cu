@@ -94,10 +94,65 @@ __device__ __forceinline__ void push_one(const Dims &d, const PushConst &c, cons
   izn = izn < 0 ? 0 : (izn > d.n3 + 1 ? d.n3 + 1 : izn);
 }
 
+// The negative-ion bookkeeping and the secondary emission of the drop-in
+// mover (Src/part_expmover.f90:76, 278-301, 353-400, 416-470).
+struct MoverExtra {
+  int neg;                   // this species is tag_neg
+  int tag_neu, num_grd;
+  const int *cex;            // flag_cex of the species, slot order (neg)
+  int *cnt_cex;              // [3]
+  double *cnt_dead;          // [1]
+  double *beam_div;          // [4]
+  double k_dead;             // Nm q of the species
+  int sec;                   // secondary emission (a positive species, gam_sec > 0)
+  int igrid_sec;
+  double gam, vt, zg0, zg1;  // gam_sec, sqrt(2 qe |THm| / m_e), cathode planes
+  double Nm1, m1;            // species 1
+  double *p1;                // species 1 planes, capacity cap1, count count1
+  long long cap1;
+  int *count1;
+  double *ploss4;            // [1]: P_loss(4, species 1)
+  uint32_t k0, k1, call;     // Philox key and call counter
+  double pi;
+};
+
+// Secondary electrons of an ion lost on the emissive grid: INT(gam) of
+// them, one more with probability gam - INT(gam), appended behind species
+// 1's count at the ion's (x, y) on the cathode plane it moved towards, with
+// a flux-Maxwellian normal velocity and the Gaussian transverse velocity of
+// load_gauss (Src/load_part.f90:268-291).  The reference draws from its
+// serial ran2 stream; here Philox4x32-10 keyed by (ion slot, call).
+__device__ void emit_secondaries(const MoverExtra &x, long long i, double xp, double yp, double vz_ion, int *err) {
+  const U4 r0 = philox4x32_10({(uint32_t)i, (uint32_t)(i >> 32), x.call, 0x53454330u}, x.k0, x.k1);
+  int n_sec = (int)x.gam;
+  if (u01(r0.x) <= x.gam - n_sec) n_sec += 1;
+  for (int k = 0; k < n_sec; ++k) {
+    const U4 r = philox4x32_10({(uint32_t)i, (uint32_t)(i >> 32), x.call, 0x53454331u + (uint32_t)k}, x.k0, x.k1);
+    const double vz = (vz_ion >= 0.0 ? -1.0 : 1.0) * x.vt * sqrt(-log(1.0 - u01(r.x)));
+    const double vp = x.vt * sqrt(-log(1.0 - u01(r.y))), theta = 2.0 * x.pi * u01(r.z);
+    const double vxs = vp * cos(theta), vys = vp * sin(theta);
+    const int slot = atomicAdd(x.count1, 1);
+    if (slot >= x.cap1) {
+      atomicSub(x.count1, 1);
+      raise_err(err, LEPIC_ERR_CAPACITY, (int)i);
+      return;
+    }
+    double *q = x.p1 + slot;
+    q[0] = xp;
+    q[x.cap1] = yp;
+    q[2 * x.cap1] = vz_ion < 0.0 ? x.zg0 : x.zg1;
+    q[3 * x.cap1] = vxs;
+    q[4 * x.cap1] = vys;
+    q[5 * x.cap1] = vz;
+    // P_loss(4,1) as the reference sums it (vz twice, vy not at all)
+    atomicAdd(x.ploss4, 0.5 * x.Nm1 * x.m1 * (vxs * vxs + vz * vz + vz * vz));
+  }
+}
+
 // Loss accumulators: acc[0] P_loss(1), acc[1] P_loss(3), acc[2+2g] p_mac
 // count at label g, acc[3+2g] p_mac energy at label g.
 template <bool BMAP>
-__global__ void __launch_bounds__(PB) k_push_f64(Dims d, PushConst c, BMapF64 m, Dielectric die,
+__global__ void __launch_bounds__(PB) k_push_f64(Dims d, PushConst c, BMapF64 m, Dielectric die, MoverExtra x,
                                                  const double *__restrict__ Ei,
                                                  const int *__restrict__ bcnd,
                                                  const unsigned char *__restrict__ cw,
@@ -114,6 +169,7 @@ __global__ void __launch_bounds__(PB) k_push_f64(Dims d, PushConst c, BMapF64 m,
     flag_dead[i] = 0;
     double Eki = 0.5 * c.Nm * c.mass * (vx * vx + vy * vy + vz * vz);
     atomicAdd(&acc[1], -Eki);
+    if (x.neg) atomicAdd(x.cnt_dead, x.k_dead);
     keep[i] = 0;
     return;
   }
@@ -125,14 +181,30 @@ __global__ void __launch_bounds__(PB) k_push_f64(Dims d, PushConst c, BMapF64 m,
   }
   int ix, iy, iz;
   push_one<BMAP>(d, c, m, Ei, xp, yp, zp, vx, vy, vz, ix, iy, iz);
-  if (cw[d.c(ix, iy, iz)]) {
+  // negative ions leave through the Neumann plane (no specular reflection),
+  // counted at label 0 (Src/part_expmover.f90:278-280, 300)
+  const bool neu_loss = x.neg && xp < 0.0 && c.flag_nmn == 1;
+  if (neu_loss || cw[d.c(ix, iy, iz)]) {
     double Eki = 0.5 * c.Nm * c.mass * (vx * vx + vy * vy + vz * vz);
-    int igrid = bcnd[d.g(ix, iy, iz)];
+    int igrid = neu_loss ? 0 : bcnd[d.g(ix, iy, iz)];
     atomicAdd(&acc[0], Eki);
     if (igrid >= 0 && igrid <= c.ngrid) {
+      dielectric_charge(die, d, igrid, xp, yp, zp, ix, iy, iz, c.h0, c.h1, c.h2, c.flag_pbc, c.zmax);
+      if (x.sec && igrid == x.igrid_sec) emit_secondaries(x, i, xp, yp, vz, err);
       atomicAdd(&acc[2 + 2 * igrid], 1.0);
       atomicAdd(&acc[3 + 2 * igrid], Eki);
-      dielectric_charge(die, d, igrid, xp, yp, zp, ix, iy, iz, c.h0, c.h1, c.h2, c.flag_pbc, c.zmax);
+      if (x.neg && igrid == x.num_grd) {
+        const int f = x.cex[i];
+        atomicAdd(&x.cnt_cex[0], 1);
+        if (abs(f) == x.tag_neu) atomicAdd(&x.cnt_cex[1], 1);
+        if (f == -x.tag_neu) atomicAdd(&x.cnt_cex[2], 1);
+        double theta = atan(vy / vx);
+        atomicAdd(&x.beam_div[0], theta);
+        atomicAdd(&x.beam_div[1], theta * theta);
+        theta = atan(vz / vx);
+        atomicAdd(&x.beam_div[2], theta);
+        atomicAdd(&x.beam_div[3], theta * theta);
+      }
     }
     keep[i] = 0;
     return;
@@ -156,16 +228,18 @@ __global__ void __launch_bounds__(PB) k_push_f64(Dims d, PushConst c, BMapF64 m,
   keep[i] = 1;
 }
 
-// scatter kept particles to their compacted (in-order) slot
+// scatter kept particles to their compacted (in-order) slot, with their
+// flag_cex when given (the negative-ion species)
 __global__ void k_compact(const double *__restrict__ pin, double *__restrict__ pout, long long cap,
                           const int *__restrict__ count, const int *__restrict__ keep,
-                          const int *__restrict__ pos) {
+                          const int *__restrict__ pos, const int *__restrict__ cex_in, int *__restrict__ cex_out) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= *count) return;
   if (!keep[i]) return;
   long long j = pos[i];
 #pragma unroll
   for (int c = 0; c < 6; ++c) pout[c * cap + j] = pin[c * cap + i];
+  if (cex_in) cex_out[j] = cex_in[i];
 }
 
 __global__ void k_set_count(int *count, const int *keep, const int *pos) {
@@ -332,7 +406,8 @@ int exclusive_scan_i32(const int *in, int *out, long long n, cudaStream_t s) {
 
 int launch_part_mover(const lepic_grid_t &g, const double *Ei, lepic_species_f64_t &sp, int ptype,
                       int ntype, int ngrid, const lepic_phys_t &P, double *p_mac, double *P_loss,
-                      cudaStream_t s, const int *dtype_dev, double *qxz_dev, double *qyz_dev) {
+                      cudaStream_t s, const int *dtype_dev, double *qxz_dev, double *qyz_dev,
+                      const MoverExtras *ex) {
   Dims d(g.n);
   const int p = ptype - 1;
   PushConst c;
@@ -363,6 +438,40 @@ int launch_part_mover(const lepic_grid_t &g, const double *Ei, lepic_species_f64
     die.qyz = qyz_dev;
     die.k3 = P.Nm[p] * P.charge[p];
   }
+  MoverExtra x;
+  memset(&x, 0, sizeof(x));
+  x.pi = P.pi;
+  int *cex_out = nullptr;
+  if (ex && ex->tag_neg == ptype) {
+    if (!ex->cex || !ex->cex_out || !ex->cnt_cex || !ex->cnt_dead || !ex->beam_div) return LEPIC_ERR_ARG;
+    x.neg = 1;
+    x.tag_neu = ex->tag_neu;
+    x.num_grd = ex->num_grd;
+    x.cex = ex->cex;
+    x.cnt_cex = ex->cnt_cex;
+    x.cnt_dead = ex->cnt_dead;
+    x.beam_div = ex->beam_div;
+    x.k_dead = P.Nm[p] * P.charge[p];
+    cex_out = ex->cex_out;
+  }
+  if (ex && ex->gam_sec > 0.0 && P.charge[p] > 0.0) {
+    if (!ex->e1 || !ex->ploss4) return LEPIC_ERR_ARG;
+    x.sec = 1;
+    x.igrid_sec = ex->igrid_sec;
+    x.gam = ex->gam_sec;
+    x.vt = sqrt(2.0 * P.qe * fabs(ex->THm) / fabs(P.mass[0]));
+    x.zg0 = ex->zg_sec[0];
+    x.zg1 = ex->zg_sec[1];
+    x.Nm1 = P.Nm[0];
+    x.m1 = P.mass[0];
+    x.p1 = ex->e1->p;
+    x.cap1 = ex->e1->cap;
+    x.count1 = ex->e1->count;
+    x.ploss4 = ex->ploss4;
+    x.k0 = ex->key0;
+    x.k1 = ex->key1;
+    x.call = ex->call;
+  }
   const long long cap = sp.cap;
   int nacc = 2 + 2 * (ngrid + 1);
   double *acc = (double *)scratch("push_acc", sizeof(double) * nacc);
@@ -376,11 +485,11 @@ int launch_part_mover(const lepic_grid_t &g, const double *Ei, lepic_species_f64
   if (N > 0) {
     int t0 = timer_start("push_f64", s);
     if (m.B)
-      k_push_f64<true><<<grid_for(N, PB), PB, 0, s>>>(d, c, m, die, Ei, g.bcnd, g.cell_wall, sp.p, sp.p_alt, cap,
-                                                      sp.count, sp.flag_dead, keep, acc, ctx().d_err);
+      k_push_f64<true><<<grid_for(N, PB), PB, 0, s>>>(d, c, m, die, x, Ei, g.bcnd, g.cell_wall, sp.p, sp.p_alt,
+                                                      cap, sp.count, sp.flag_dead, keep, acc, ctx().d_err);
     else
-      k_push_f64<false><<<grid_for(N, PB), PB, 0, s>>>(d, c, m, die, Ei, g.bcnd, g.cell_wall, sp.p, sp.p_alt, cap,
-                                                       sp.count, sp.flag_dead, keep, acc, ctx().d_err);
+      k_push_f64<false><<<grid_for(N, PB), PB, 0, s>>>(d, c, m, die, x, Ei, g.bcnd, g.cell_wall, sp.p, sp.p_alt,
+                                                       cap, sp.count, sp.flag_dead, keep, acc, ctx().d_err);
     timer_stop(t0, s);
     LEPIC_CUDA(cudaGetLastError());
     int t1 = timer_start("compact_scan", s);
@@ -388,7 +497,8 @@ int launch_part_mover(const lepic_grid_t &g, const double *Ei, lepic_species_f64
     timer_stop(t1, s);
     if (rc) return rc;
     int t2 = timer_start("compact_f64", s);
-    k_compact<<<grid_for(N, PB), PB, 0, s>>>(sp.p_alt, sp.p, cap, sp.count, keep, pos);
+    k_compact<<<grid_for(N, PB), PB, 0, s>>>(sp.p_alt, sp.p, cap, sp.count, keep, pos, x.neg ? x.cex : nullptr,
+                                             cex_out);
     timer_stop(t2, s);
     k_set_count<<<1, 1, 0, s>>>(sp.count, keep, pos);
     LEPIC_CUDA(cudaGetLastError());

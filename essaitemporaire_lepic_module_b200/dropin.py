@@ -232,12 +232,41 @@ def _bi(st):
     return Bi, np.array([1, 1, 1], dtype=np.int32), np.ascontiguousarray(st.h, dtype=np.float64)
 
 
-def part_mover(st, Ei, vxp, np_tot, flag_dead, p_mac, P_loss, ptype, ngrid=None, sum_q=None):
+class MoverExtra:
+    """The negative-ion bookkeeping and secondary emission of part_mover_
+    (Src/part_expmover.f90:76, 278-301, 353-400, 416-470): the COMMON values
+    (tag_neg, tag_neu, num_grd; gam_sec, igrid_sec, THm, zg_sec) and the
+    caller's arrays flag_cex(1:nmax), cnt_cex(3), cnt_dead, beam_div(4) and the
+    ran2 seed iseed."""
+
+    def __init__(self, nmax, tag_neg=0, tag_neu=0, num_grd=0, gam_sec=0.0, igrid_sec=0, THm=0.0,
+                 zg_sec=(0.0, 0.0), iseed=-1):
+        self.flag_cex = np.zeros(nmax, dtype=np.int32)
+        self.cnt_cex = np.zeros(3, dtype=np.int32)
+        self.cnt_dead = np.zeros(1)
+        self.beam_div = np.zeros(4)
+        self.iseed = np.array([iseed], dtype=np.int32)
+        self.tag_neg, self.tag_neu, self.num_grd = int(tag_neg), int(tag_neu), int(num_grd)
+        self.gam_sec, self.igrid_sec, self.THm = float(gam_sec), int(igrid_sec), float(THm)
+        self.zg_sec = tuple(float(z) for z in zg_sec)
+
+    def set_commons(self):
+        cm = commons()
+        pi_, d1 = cm["part_info_int"], cm["part_info_dp_1"]
+        pi_.tag_neg, pi_.tag_neu, pi_.num_grd, pi_.igrid_sec = self.tag_neg, self.tag_neu, self.num_grd, \
+            self.igrid_sec
+        d1.gam_sec = self.gam_sec if self.gam_sec > 0.0 else -1.0
+        d1.THm = self.THm
+        d1.zg_sec[0], d1.zg_sec[1] = self.zg_sec
+
+
+def part_mover(st, Ei, vxp, np_tot, flag_dead, p_mac, P_loss, ptype, ngrid=None, sum_q=None, extra=None):
     """Src/part_expmover.f90:1 -- in place on vxp / np_tot / flag_dead /
     p_mac (ntype, 2, 0:ngrid) C-order (ngrid+1, 2, ntype) / P_loss (ntype, 4).
     sum_q: (sum_q_xz, sum_q_yz), the surface charges of the dielectric walls
     (flag_die = 1), C-order (ntype, n3+3, n1+3) and (ntype, n3+3, n2+3, 2),
-    accumulated for ptype."""
+    accumulated for ptype.  extra: a MoverExtra (negative ions, secondary
+    emission into species 1); its COMMON values are set for the call."""
     ngrid = st.geom.ngrid if ngrid is None else ngrid
     n = _lib.np_i(st.n)
     h = np.ascontiguousarray(st.h, dtype=np.float64)
@@ -258,11 +287,20 @@ def part_mover(st, Ei, vxp, np_tot, flag_dead, p_mac, P_loss, ptype, ngrid=None,
         assert qxz.shape == (st.ntype, n3 + 3, n1 + 3) and qyz.shape == (st.ntype, n3 + 3, n2 + 3, 2)
         assert qxz.flags["C_CONTIGUOUS"] and qyz.flags["C_CONTIGUOUS"] and qxz.dtype == np.float64
         dt = st.geom.dtype_array()
-    lib().part_mover_(_pi(n), _pd(h), _pd(E), _pd(Bi), _pd(p_mac), _pd(P_loss), _pd(vxp), _pi(bc),
-                      _i(nmax), _i(st.ntype), _i(ngrid), flag_dead.ctypes.data_as(_lib.P_i8), _i(1),
-                      _pi(np_tot), _i(1), _i(ptype), _pi(dummy_i), _pi(dummy_i), _pd(dummy_d),
-                      _pd(dummy_d), _pd(qxz), _pd(qyz), _pi(dt), _pi(dummy_i), _pi(nB),
-                      _pd(hB))
+    cex, ccex, cdead, bdiv, seed = dummy_i, dummy_i, dummy_d, dummy_d, dummy_i
+    if extra is not None:
+        extra.set_commons()
+        assert len(extra.flag_cex) >= nmax
+        cex, ccex, cdead, bdiv, seed = extra.flag_cex, extra.cnt_cex, extra.cnt_dead, extra.beam_div, extra.iseed
+    try:
+        lib().part_mover_(_pi(n), _pd(h), _pd(E), _pd(Bi), _pd(p_mac), _pd(P_loss), _pd(vxp), _pi(bc),
+                          _i(nmax), _i(st.ntype), _i(ngrid), flag_dead.ctypes.data_as(_lib.P_i8), _i(1),
+                          _pi(np_tot), _i(1), _i(ptype), _pi(cex), _pi(ccex), _pd(cdead),
+                          _pd(bdiv), _pd(qxz), _pd(qyz), _pi(dt), _pi(seed), _pi(nB),
+                          _pd(hB))
+    finally:
+        if extra is not None:
+            MoverExtra(1).set_commons()   # back to no negative ions, no emission
     check(lib().lepic_gpu_last_error(), "part_mover")
 
 

@@ -127,7 +127,16 @@ void calc_efield_(const int *n, const double *h, const double *phi, double *Ei, 
  * flag_die = 1 in COMMON /part_info_int/ the charge of the particles lost
  * on dielectric walls (dtype(igrid) = 2: Y = const plane, 3 / 4: X = const
  * planes) is added to sum_q_xz(0:n1+2,0:n3+2,ntype,nproc) and
- * sum_q_yz(2,0:n2+2,0:n3+2,ntype,nproc) (Src/part_expmover.f90:302-348). */
+ * sum_q_yz(2,0:n2+2,0:n3+2,ntype,nproc) (Src/part_expmover.f90:302-348).
+ * For ptype = tag_neg (COMMON /part_info_int/) the negative-ion bookkeeping
+ * (Src/part_expmover.f90:76, 278-301, 416-470): flag_cex(1:nmax) follows the
+ * compaction, a negative ion reaching x < 0 with flag_nmn = 1 is lost at
+ * label 0, cnt_dead += Nm q per killed particle, and a particle lost on
+ * num_grd counts in cnt_cex(1:3) and adds its divergence angles to
+ * beam_div(1:4).  With gam_sec > 0 a positive species lost on igrid_sec emits
+ * secondary electrons into species 1 (vxp(:,np_tot(1)+1:,1), P_loss(4,1);
+ * Src/part_expmover.f90:353-400); the draws come from Philox keyed by *iseed,
+ * which then advances one ran2 step, not from the reference's ran2 stream. */
 void part_mover_(const int *n, const double *h, const double *Ei, const double *Bi, double *p_mac,
                  double *P_loss, double *vxp, const int *bcnd, const int *nmax, const int *ntype,
                  const int *ngrid, signed char *flag_dead, const int *nproc, int *np_tot,

@@ -243,18 +243,57 @@ def calc_efield(st, phi, Ei=None):
     return E
 
 
-def part_mover(st, Ei, S, p_mac, P_loss, ptype, ngrid=None, sum_q=None):
+class OMoverExtra(C.Structure):
+    _fields_ = [("tag_neg", C.c_int), ("tag_neu", C.c_int), ("num_grd", C.c_int),
+                ("flag_cex", P_int), ("cnt_cex", P_int), ("cnt_dead", P_dbl), ("beam_div", P_dbl),
+                ("gam_sec", C.c_double), ("THm", C.c_double), ("zg_sec", C.c_double * 2),
+                ("igrid_sec", C.c_int), ("iseed", P_int)]
+
+
+class MoverExtra:
+    """The negative-ion bookkeeping and secondary emission of the mover
+    (Src/part_expmover.f90:76, 278-301, 353-400, 416-470): the COMMON values
+    and the caller's arrays (flag_cex of the tag_neg species, cnt_cex(3),
+    cnt_dead, beam_div(4), the ran2 seed)."""
+
+    def __init__(self, nmax, tag_neg=0, tag_neu=0, num_grd=0, gam_sec=0.0, igrid_sec=0, THm=0.0,
+                 zg_sec=(0.0, 0.0), iseed=-1):
+        self.flag_cex = np.zeros(nmax, dtype=np.int32)
+        self.cnt_cex = np.zeros(3, dtype=np.int32)
+        self.cnt_dead = np.zeros(1)
+        self.beam_div = np.zeros(4)
+        self.iseed = np.array([iseed], dtype=np.int32)
+        self.tag_neg, self.tag_neu, self.num_grd = tag_neg, tag_neu, num_grd
+        self.gam_sec, self.igrid_sec, self.THm, self.zg_sec = gam_sec, igrid_sec, THm, tuple(zg_sec)
+
+    def copy(self):
+        c = MoverExtra(len(self.flag_cex), self.tag_neg, self.tag_neu, self.num_grd, self.gam_sec,
+                       self.igrid_sec, self.THm, self.zg_sec, int(self.iseed[0]))
+        for a in ("flag_cex", "cnt_cex", "cnt_dead", "beam_div", "iseed"):
+            getattr(c, a)[...] = getattr(self, a)
+        return c
+
+    def struct(self):
+        return OMoverExtra(self.tag_neg, self.tag_neu, self.num_grd, _pi(self.flag_cex), _pi(self.cnt_cex),
+                           _pd(self.cnt_dead), _pd(self.beam_div), self.gam_sec, self.THm,
+                           (C.c_double * 2)(*self.zg_sec), self.igrid_sec, _pi(self.iseed))
+
+
+def part_mover(st, Ei, S, p_mac, P_loss, ptype, ngrid=None, sum_q=None, extra=None):
     """sum_q: (sum_q_xz (ntype, n3+3, n1+3), sum_q_yz (ntype, n3+3, n2+3, 2))
-    C-order, accumulated for the dielectric walls (flag_die = 1)."""
+    C-order, accumulated for the dielectric walls (flag_die = 1).  extra:
+    a MoverExtra (negative ions, secondary emission into species 1)."""
     ngrid = st.geom.ngrid if ngrid is None else ngrid
     n = np.array(st.n, dtype=np.int32)
     h = np.ascontiguousarray(st.h)
     bc = np.ascontiguousarray(st.geom.bcnd, dtype=np.int32)
     P = ophys(st)
+    X = extra.struct() if extra is not None else None
     rc = lib().oracle_part_mover(_pi(n), _pd(h), _pd(np.ascontiguousarray(Ei)), _pd(p_mac),
                                  _pd(P_loss), _pd(S.vxp), _pi(bc), C.c_int(S.vxp.shape[1]),
                                  C.c_int(st.ntype), C.c_int(ngrid), S.flag_dead.ctypes.data_as(P_i8),
-                                 _pi(S.np_tot), C.c_int(ptype), C.byref(P), *_die_args(st, sum_q))
+                                 _pi(S.np_tot), C.c_int(ptype), C.byref(P), *_die_args(st, sum_q),
+                                 C.byref(X) if X is not None else None)
     if rc:
         raise RuntimeError(f"oracle part_mover status {rc}")
 

@@ -1109,7 +1109,7 @@ void oracle_dielectric_phi(const int n[3], double *phi, const int *bcnd, const i
 int oracle_part_mover(const int n[3], const double h[3], const double *Ei, double *p_mac,
                       double *P_loss, double *vxp, const int *bcnd, int nmax, int ntype, int ngrid,
                       signed char *flag_dead, int *np_tot, int ptype, const OPhys *P,
-                      const int *dtype, double *sum_q_xz, double *sum_q_yz) {
+                      const int *dtype, double *sum_q_xz, double *sum_q_yz, const OMoverExtra *X) {
   // Two passes: the push of every particle (independent, OpenMP over
   // contiguous particle slices like the reference's thread slices), then the
   // in-order compaction i_shift = i - np_lost (Src/part_expmover.f90:454-470).
@@ -1127,8 +1127,13 @@ int oracle_part_mover(const int n[3], const double h[3], const double *Ei, doubl
   std::vector<double> lost_E(N, 0.0);
   // dielectric walls: the new position and cell of each lost particle
   const bool die = dtype && sum_q_xz && sum_q_yz;
-  std::vector<double> lost_x(die ? 3L * N : 0);
-  std::vector<int> lost_c(die ? 3L * N : 0);
+  // negative ions (this species is tag_neg) and secondary emission (a
+  // positive ion on the emissive grid): the lost particle's new state
+  const bool neg = X && X->tag_neg == ptype;
+  const bool sec = X && X->gam_sec > 0.0 && q > 0.0;
+  const bool keep_x = die || neg || sec;
+  std::vector<double> lost_x(keep_x ? 3L * N : 0), lost_v(keep_x ? 3L * N : 0);
+  std::vector<int> lost_c(keep_x ? 3L * N : 0);
   int bad = 0;
 #pragma omp parallel for schedule(static) reduction(| : bad)
   for (int i = 0; i < N; ++i) {
@@ -1252,15 +1257,21 @@ int oracle_part_mover(const int n[3], const double h[3], const double *Ei, doubl
                bcnd[d.g(ix + 1, iy + 1, iz)] >= 1 && bcnd[d.g(ix, iy + 1, iz)] >= 1 &&
                bcnd[d.g(ix, iy, iz + 1)] >= 1 && bcnd[d.g(ix + 1, iy, iz + 1)] >= 1 &&
                bcnd[d.g(ix + 1, iy + 1, iz + 1)] >= 1 && bcnd[d.g(ix, iy + 1, iz + 1)] >= 1;
+    // negative ions leave through the Neumann plane (no specular
+    // reflection), counted at label 0 (Src/part_expmover.f90:278-280, 300)
+    if (neg && xp < 0.0 && P->flag_nmn == 1) lost = 2;
     if (lost) {
       state[i] = 2;
       lost_E[i] = 0.5 * Nm * mass * (vx * vx + vy * vy + vz * vz);
-      lost_grid[i] = bcnd[d.g(ix, iy, iz)];
+      lost_grid[i] = lost == 2 ? 0 : bcnd[d.g(ix, iy, iz)];
       if (lost_grid[i] > ngrid) bad = 1;
-      if (die) {
+      if (keep_x) {
         lost_x[3L * i] = xp;
         lost_x[3L * i + 1] = yp;
         lost_x[3L * i + 2] = zp;
+        lost_v[3L * i] = vx;
+        lost_v[3L * i + 1] = vy;
+        lost_v[3L * i + 2] = vz;
         lost_c[3L * i] = ix;
         lost_c[3L * i + 1] = iy;
         lost_c[3L * i + 2] = iz;
@@ -1291,24 +1302,74 @@ int oracle_part_mover(const int n[3], const double h[3], const double *Ei, doubl
   };
   auto PL = [&](int which) -> double & { return P_loss[which + 4L * p]; };
   int np_lost = 0;
+  double *V1 = vxp;   // species 1: the secondary electrons
+  int rc = ORACLE_OK;
   for (int i = 0; i < N; ++i) {
     if (state[i] == 1) {
       np_lost++;
+      if (neg) *X->cnt_dead = *X->cnt_dead + Nm * q;
       PL(2) = PL(2) - lost_E[i];
     } else if (state[i] == 2) {
       np_lost++;
+      const int igrid = lost_grid[i];
       PL(0) = PL(0) + lost_E[i];
-      pm(0, lost_grid[i]) = pm(0, lost_grid[i]) + 1.0;
-      pm(1, lost_grid[i]) = pm(1, lost_grid[i]) + lost_E[i];
-      if (die && dtype[lost_grid[i]] > 1) die_charge(d, h, P, dtype[lost_grid[i]], Nm * q, &lost_x[3L * i],
-                                                     &lost_c[3L * i], sum_q_xz + (long)p * (d.n1 + 3) * (d.n3 + 3),
-                                                     sum_q_yz + (long)p * 2 * (d.n2 + 3) * (d.n3 + 3));
+      if (die && dtype[igrid] > 1) die_charge(d, h, P, dtype[igrid], Nm * q, &lost_x[3L * i],
+                                              &lost_c[3L * i], sum_q_xz + (long)p * (d.n1 + 3) * (d.n3 + 3),
+                                              sum_q_yz + (long)p * 2 * (d.n2 + 3) * (d.n3 + 3));
+      if (sec && igrid == X->igrid_sec) {
+        // Src/part_expmover.f90:353-400: INT(gam_sec) electrons, one more with
+        // probability gam_sec - INT(gam_sec), at the ion's (x, y) on the
+        // cathode plane it moved towards, flux-Maxwellian normal velocity and
+        // Gaussian transverse velocity of temperature THm
+        int n_sec = (int)X->gam_sec;
+        if (oracle_ran2(X->iseed) <= X->gam_sec - n_sec) n_sec = n_sec + 1;
+        const double vz_ion = lost_v[3L * i + 2];
+        for (int k = 0; k < n_sec; ++k) {
+          if (np_tot[0] >= nmax) {
+            rc = ORACLE_ERR_CAPACITY;
+            break;
+          }
+          const double vt = std::sqrt(2.0 * P->qe * std::fabs(X->THm) / std::fabs(P->mass[0]));
+          const double r1 = oracle_ran2(X->iseed);
+          const double vz_sec = -std::copysign(1.0, vz_ion) * vt * std::sqrt(-std::log(1.0 - r1));
+          const double ra = oracle_ran2(X->iseed), rb = oracle_ran2(X->iseed);
+          // load_gauss (Src/load_part.f90:268-291)
+          const double vp = vt * std::sqrt(-std::log(1.0 - ra)), theta = 2.0 * P->pi * rb;
+          const double vx_sec = vp * std::cos(theta), vy_sec = vp * std::sin(theta);
+          double *e = V1 + (long)np_tot[0] * 6;
+          e[0] = lost_x[3L * i];
+          e[1] = lost_x[3L * i + 1];
+          e[2] = vz_ion < 0.0 ? X->zg_sec[0] : X->zg_sec[1];
+          e[3] = vx_sec;
+          e[4] = vy_sec;
+          e[5] = vz_sec;
+          np_tot[0] = np_tot[0] + 1;
+          // P_loss(4,1) as the reference sums it (vz twice, vy not at all)
+          P_loss[3] = P_loss[3] + 0.5 * P->Nm[0] * P->mass[0] *
+                                      (vx_sec * vx_sec + vz_sec * vz_sec + vz_sec * vz_sec);
+        }
+      }
+      pm(0, igrid) = pm(0, igrid) + 1.0;
+      pm(1, igrid) = pm(1, igrid) + lost_E[i];
+      if (neg && igrid == X->num_grd) {
+        X->cnt_cex[0] = X->cnt_cex[0] + 1;
+        if (std::abs(X->flag_cex[i]) == X->tag_neu) X->cnt_cex[1] = X->cnt_cex[1] + 1;
+        if (X->flag_cex[i] == -X->tag_neu) X->cnt_cex[2] = X->cnt_cex[2] + 1;
+        const double vxl = lost_v[3L * i], vyl = lost_v[3L * i + 1], vzl = lost_v[3L * i + 2];
+        double theta = std::atan(vyl / vxl);
+        X->beam_div[0] = X->beam_div[0] + theta;
+        X->beam_div[1] = X->beam_div[1] + theta * theta;
+        theta = std::atan(vzl / vxl);
+        X->beam_div[2] = X->beam_div[2] + theta;
+        X->beam_div[3] = X->beam_div[3] + theta * theta;
+      }
     } else if (np_lost) {
       std::memcpy(V + (long)(i - np_lost) * 6, V + (long)i * 6, 6 * sizeof(double));
+      if (neg) X->flag_cex[i - np_lost] = X->flag_cex[i];
     }
   }
   np_tot[p] = N - np_lost;
-  return ORACLE_OK;
+  return rc;
 }
 
 // Src/part_expmover.f90:570-686 (charge_deposition): CIC with kq.  np of

@@ -119,12 +119,27 @@ void oracle_calc_efield(const int n[3], const double h[3], const double *phi,
 void oracle_dielectric_phi(const int n[3], double *phi, const int *bcnd,
                            const int *dtype, int ngrid, double *qxz,
                            double *qyz, int ntype, double Ca, int flag_pbc);
+/* The negative-ion bookkeeping and the secondary emission of the mover
+ * (Src/part_expmover.f90:76, 278-301, 353-400, 416-470): COMMON values and
+ * the caller's arrays.  tag_neg 0: no negative ions; gam_sec <= 0: no
+ * secondary emission. */
+typedef struct OMoverExtra {
+  int tag_neg, tag_neu, num_grd;
+  int *flag_cex;                   /* flag_cex(1:nmax) of species tag_neg    */
+  int *cnt_cex;                    /* cnt_cex(1:3)                           */
+  double *cnt_dead;                /* cnt_dead(1)                            */
+  double *beam_div;                /* beam_div(1:4)                          */
+  double gam_sec, THm, zg_sec[2];
+  int igrid_sec;
+  int *iseed;                      /* ran2 state of the secondary draws      */
+} OMoverExtra;
+
 int oracle_part_mover(const int n[3], const double h[3], const double *Ei,
                       double *p_mac, double *P_loss, double *vxp,
                       const int *bcnd, int nmax, int ntype, int ngrid,
                       signed char *flag_dead, int *np_tot, int ptype,
                       const OPhys *P, const int *dtype, double *sum_q_xz,
-                      double *sum_q_yz);
+                      double *sum_q_yz, const OMoverExtra *X);
 void oracle_charge_deposition(const int n[3], const double h[3],
                               const double *vxp, int nmax, int ntype,
                               const double *kq, double *np, const int *np_tot,
