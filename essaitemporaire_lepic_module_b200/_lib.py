@@ -220,6 +220,8 @@ def lib():
                                    vp], _I),
         "lepic_dev_cw_deposit": ([C.POINTER(LepicGrid), C.POINTER(LepicWinSpecies), _I, C.POINTER(LepicPhys),
                                   _I, vp, vp], _I),
+        "lepic_dev_cw_back": ([C.POINTER(LepicGrid), vp, C.POINTER(LepicWinSpecies), _I, C.POINTER(LepicPhys),
+                               _I, vp, C.c_double, vp, vp, vp], _I),
         "lepic_dev_cw_push": ([C.POINTER(LepicGrid), vp, C.POINTER(LepicWinSpecies), _I, C.POINTER(LepicPhys),
                                _I, vp, vp], _I),
         "lepic_dev_cw_reverse": ([C.POINTER(LepicGrid), vp, C.POINTER(LepicWinSpecies), _I,
@@ -311,7 +313,7 @@ def exported_symbols():
             "lepic_dev_pdesolver_mixed", "lepic_dev_collisions_mixed", "lepic_dev_load_uniform",
             "lepic_dev_win_push", "lepic_dev_win_deposit", "lepic_dev_adj_push", "lepic_dev_adj_efield",
             "lepic_dev_adj_rhs", "lepic_dev_adj_walls", "lepic_dev_adj_deposit", "lepic_dev_cell_wall",
-            "lepic_dev_cw_deposit", "lepic_dev_cw_push", "lepic_dev_cw_reverse", "lepic_dev_cw_adj_push",
+            "lepic_dev_cw_deposit", "lepic_dev_cw_back", "lepic_dev_cw_push", "lepic_dev_cw_reverse", "lepic_dev_cw_adj_push",
             "lepic_dev_cw_adj_deposit", "lepic_dev_win_collisions", "lepic_dev_cw_replay",
             "lepic_dev_cw_adj_collide",
             "lepic_dev_dielectric_phi",

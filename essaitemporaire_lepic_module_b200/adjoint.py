@@ -518,19 +518,16 @@ class CollisionWindow:
         ac = 2.0 * EPS0 * (1.0 / h[0] ** 2 + 1.0 / h[1] ** 2 + 1.0 / h[2] ** 2)
         alpha = (n1 + 1) * (n2 + 1) * (n3 + 1) * ac
 
-        def field_adjoint(step):
-            # lphi -> mu (A mu = lphi on plasma nodes), dJ/dV, and the deposit
-            # adjoint of the particles deposited at `step`
+        def field_adjoint():
+            # lphi -> mu (A mu = lphi on plasma nodes) and dJ/dV; the deposit
+            # adjoint of the step's particles follows with mu (fused into the
+            # previous step's backward kernels, or last for step 0)
             check(L.lepic_dev_adj_rhs(C.byref(sim.grid), _p(lphi), _p(b), self._s()), "adj_rhs")
             r0 = float(b.abs().sum()) / alpha
             if r0 > 0.0:
                 self._solve(mu, b, eps=wl.eps * r0)   # warm start: mu of the later step (walls 0)
             check(L.lepic_dev_adj_walls(C.byref(sim.grid), C.byref(sim.P), 1, _p(lphi), _p(mu), _p(lnp), _p(dV),
                                         self.nlabel, self._s()), "adj_walls")
-            for p in range(self.ntype):
-                if st.charge[p] != 0.0:
-                    check(L.lepic_dev_cw_adj_deposit(C.byref(sim.grid), C.byref(self.ws[p]), p + 1, C.byref(sim.P),
-                                                     step, _p(mu), self._s()), "cw_adj_deposit")
 
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record()
@@ -541,32 +538,37 @@ class CollisionWindow:
             d = self.stores[0]
             d["lam"][3:6, :n] = ((gJ * m / (QE * self.n_alive)) * d["p"][3:6, :n].to(torch.float64)
                                  * a.to(torch.float64)).to(d["lam"].dtype)
-        elif self.observable == "probe":
+        have_mu = False
+        if self.observable == "probe":
             lphi.zero_()
             k, j, i = self.centre
             lphi[k, j, i] = gJ
-            field_adjoint(self.K)
-        else:
+            field_adjoint()
+            have_mu = True
+        elif self.observable == "flux":
             wflux = gJ
         for n in reversed(range(self.K)):
             sim.phi.copy_(self.phis[n])
             self._efield()
-            for p in range(self.ntype):
-                if st.charge[p] != 0.0:
-                    check(L.lepic_dev_cw_reverse(C.byref(sim.grid), _p(self._E()), C.byref(self.ws[p]), p + 1,
-                                                 C.byref(sim.P), n, self._s()), "cw_reverse")
             lE.zero_()
+            # the deposit adjoint of step n + 1, the push of step n undone and
+            # its adjoint, per species in one pass over the particles
             for p in range(self.ntype):
                 if st.charge[p] != 0.0:
-                    check(L.lepic_dev_cw_adj_push(C.byref(sim.grid), _p(self._E()), C.byref(self.ws[p]), p + 1,
-                                                  C.byref(sim.P), n, C.c_double(wflux), _p(lE), _p(dBz),
-                                                  self._s()), "cw_adj_push")
+                    check(L.lepic_dev_cw_back(C.byref(sim.grid), _p(self._E()), C.byref(self.ws[p]), p + 1,
+                                              C.byref(sim.P), n, _p(mu) if have_mu else None, C.c_double(wflux),
+                                              _p(lE), _p(dBz), self._s()), "cw_back")
             if n in self.ev_range:
                 evp, ne = self._events(n)
                 check(L.lepic_dev_cw_adj_collide(C.byref(sim.grid), self.ws, self.ntype, C.byref(sim.P), evp, ne,
                                                  self._s()), "cw_adj_collide")
             check(L.lepic_dev_adj_efield(C.byref(sim.grid), _p(lE), _p(lphi), self._s()), "adj_efield")
-            field_adjoint(n)
+            field_adjoint()
+            have_mu = True
+        for p in range(self.ntype):
+            if st.charge[p] != 0.0:
+                check(L.lepic_dev_cw_adj_deposit(C.byref(sim.grid), C.byref(self.ws[p]), p + 1, C.byref(sim.P), 0,
+                                                 _p(mu), self._s()), "cw_adj_deposit")
         ev1.record()
         torch.cuda.synchronize()
         self.timing["backward_ms"] = ev0.elapsed_time(ev1)

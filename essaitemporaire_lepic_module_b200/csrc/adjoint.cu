@@ -148,9 +148,9 @@ __device__ __forceinline__ float warp_transpose_sum(const float (&v)[NV]) {
 // For more than 16 values a warp with one or two keys (particles sorted by
 // cell: ions, electrons soon after the sort) sums by warp_transpose_sum, the
 // totals landing on NV lanes that add at once (24 values: 5 % faster push
-// adjoint; 8 values: the run sums are cheaper); otherwise by warp_run_sum, one
-// lane per run adding.  All 32 lanes must call this; lanes with key -1
-// contribute nothing.
+// adjoint; 8 values: the run sums are cheaper), and a warp with more keys
+// sorts them first; otherwise warp_run_sum, one lane per run adding.  All 32
+// lanes must call this; lanes with key -1 contribute nothing.
 template <int NV, class F>
 __device__ __forceinline__ void warp_scatter_sum(long long key, int slot, float (&v)[NV], F add) {
   const unsigned full = 0xffffffffu;
@@ -169,6 +169,36 @@ __device__ __forceinline__ void warp_scatter_sum(long long key, int slot, float 
       for (int q = 0; q < NV; ++q) m[q] = key == kt ? v[q] : 0.f;
       const float tot = warp_transpose_sum<NV>(m);
       if (lane < NV) add(kt, t ? s1 : s0, lane, tot);
+    }
+    return;
+  }
+  if (NV > 16) {
+    // more cells: a bitonic sort of (key, lane) makes each cell one run
+    // before the run sums (7 % faster push adjoint than the unsorted runs,
+    // in which one cell can recur and its head lanes contend)
+    long long sk = key < 0 ? (long long)0x7fffffffffffffffLL : key;
+    int sl = lane;
+#pragma unroll
+    for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+      for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+        const long long ok = __shfl_xor_sync(full, sk, jj);
+        const int ol = __shfl_xor_sync(full, sl, jj);
+        const bool up = (lane & kk) == 0, lower = (lane & jj) == 0;
+        const bool mine_first = sk < ok || (sk == ok && sl < ol);
+        if ((lower == up) ? !mine_first : mine_first) {
+          sk = ok;
+          sl = ol;
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < NV; ++c) v[c] = __shfl_sync(full, v[c], sl);
+    const int sslot = __shfl_sync(full, slot, sl);
+    const long long skey = sk == (long long)0x7fffffffffffffffLL ? -1 : sk;
+    if (warp_run_sum<NV, float>(skey, v)) {
+#pragma unroll
+      for (int q = 0; q < NV; ++q) add(skey, sslot, q, v[q]);
     }
     return;
   }
@@ -1063,14 +1093,15 @@ __global__ void __launch_bounds__(AB, 3) k_cw_push_tiles(Dims d, WinConst c, con
 
 // the push of step `step` undone for the particles it kept: x^n from
 // x^{n+1} and v^{n+1/2}, then v+ by the inverse rotation with E^n at x^n
+// on a state in registers: true when the push of `step` was undone (st
+// updated in place)
 template <class R, class G>
-__device__ __forceinline__ void cw_reverse_one(const Dims &d, const WinConst &c, const WinS<R> &S, long long i,
-                                               const PSt<R> &st, int step, const G &gather) {
+__device__ __forceinline__ bool cw_reverse_core(const Dims &d, const WinConst &c, PSt<R> &st, int step,
+                                                const G &gather) {
   const int b = st.b;
-  if (!(born_of(b) <= step && lost_of(b) > step)) return;
+  if (!(born_of(b) <= step && lost_of(b) > step)) return false;
   int ix, iy, iz;
   unpack_cell(st.cell, ix, iy, iz);
-  const long long cap = S.cap;
   R fx = st.f[0], fy = st.f[1], fz = st.f[2];
   R vx = st.v[0], vy = st.v[1], vz = st.v[2];
   ix += move_offset<R>(fx, -vx * (R)(c.dt / c.h0));
@@ -1084,13 +1115,32 @@ __device__ __forceinline__ void cw_reverse_one(const Dims &d, const WinConst &c,
   R Ex, Ey, Ez;
   gather(ix, iy, iz, w, Ex, Ey, Ez);
   boris_inverse<R>(c, Ex, Ey, Ez, vx, vy, vz);
-  S.cell[i] = pack_cell(ix, iy, iz);
-  S.p[i] = fx;
-  S.p[cap + i] = fy;
-  S.p[2 * cap + i] = fz;
-  S.p[3 * cap + i] = vx;
-  S.p[4 * cap + i] = vy;
-  S.p[5 * cap + i] = vz;
+  st.cell = pack_cell(ix, iy, iz);
+  st.f[0] = fx;
+  st.f[1] = fy;
+  st.f[2] = fz;
+  st.v[0] = vx;
+  st.v[1] = vy;
+  st.v[2] = vz;
+  return true;
+}
+
+template <class R>
+__device__ __forceinline__ void pst_store(const WinS<R> &S, long long i, const PSt<R> &st) {
+  const long long cap = S.cap;
+  S.cell[i] = st.cell;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    S.p[a * cap + i] = st.f[a];
+    S.p[(3 + a) * cap + i] = st.v[a];
+  }
+}
+
+template <class R, class G>
+__device__ __forceinline__ void cw_reverse_one(const Dims &d, const WinConst &c, const WinS<R> &S, long long i,
+                                               const PSt<R> &st0, int step, const G &gather) {
+  PSt<R> st = st0;
+  if (cw_reverse_core<R>(d, c, st, step, gather)) pst_store<R>(S, i, st);
 }
 
 template <class R>
@@ -1133,16 +1183,18 @@ __global__ void __launch_bounds__(AB, 3) k_cw_reverse_tiles(Dims d, WinConst c, 
 // later use except the wall-flux observable: wflux Nm m v^{n+1/2}.
 // Per slot: true when slot i was pushed at `step`, with its cell, its 24
 // contributions to lE (node q, component a at 3 q + a) and gB += its dJ/dB_z.
+// On a state and adjoint held in registers: st the particle at (x^n, v+),
+// lam in: (dJ/dx^{n+1}, dJ/dv^{n+1/2}), out: the push's part of dJ/dx^n and
+// dJ/dv+ (a particle lost at this step starts from zero, or from wflux).
 template <class R, class N>
-__device__ __forceinline__ bool cw_adj_push_one(const WinConst &c, const N &nodes, const WinS<R> &S, long long i,
-                                                int step, double wflux, int &ix, int &iy, int &iz, R (&sc)[24],
-                                                double &gB) {
-  const int b = S.bl[i];
+__device__ __forceinline__ bool cw_adj_push_core(const WinConst &c, const N &nodes, const PSt<R> &st, int step,
+                                                 double wflux, R (&lam)[6], int &ix, int &iy, int &iz,
+                                                 R (&sc)[24], double &gB) {
+  const int b = st.b;
   if (!(born_of(b) <= step && lost_of(b) >= step)) return false;
-  const long long cap = S.cap;
-  unpack_cell(S.cell[i], ix, iy, iz);
-  const R fx = S.p[i], fy = S.p[cap + i], fz = S.p[2 * cap + i];
-  const R vx = S.p[3 * cap + i], vy = S.p[4 * cap + i], vz = S.p[5 * cap + i];
+  unpack_cell(st.cell, ix, iy, iz);
+  const R fx = st.f[0], fy = st.f[1], fz = st.f[2];
+  const R vx = st.v[0], vy = st.v[1], vz = st.v[2];
   R w[8];
   weights8<R>(fx, fy, fz, w);
   // E at the cell's 8 nodes, read once for the gather and its weight gradient
@@ -1168,12 +1220,12 @@ __device__ __forceinline__ bool cw_adj_push_one(const WinConst &c, const N &node
       lvz = k * uz;
     }
   } else {
-    lx = S.lam[i];
-    ly = S.lam[cap + i];
-    lz = S.lam[2 * cap + i];
-    lvx = S.lam[3 * cap + i];
-    lvy = S.lam[4 * cap + i];
-    lvz = S.lam[5 * cap + i];
+    lx = lam[0];
+    ly = lam[1];
+    lz = lam[2];
+    lvx = lam[3];
+    lvy = lam[4];
+    lvz = lam[5];
   }
   // x^{n+1} = x^n + dt v^{n+1/2}
   const R dt = (R)c.dt, k1 = (R)c.k1, kk = (R)c.kk;
@@ -1227,12 +1279,30 @@ __device__ __forceinline__ bool cw_adj_push_one(const WinConst &c, const N &node
     ly += ax_ * sy * az_ * s;
     lz += ax_ * ay_ * sz * s;
   }
-  S.lam[i] = lx;
-  S.lam[cap + i] = ly;
-  S.lam[2 * cap + i] = lz;
-  S.lam[3 * cap + i] = ux;
-  S.lam[4 * cap + i] = uy;
-  S.lam[5 * cap + i] = uz;
+  lam[0] = lx;
+  lam[1] = ly;
+  lam[2] = lz;
+  lam[3] = ux;
+  lam[4] = uy;
+  lam[5] = uz;
+  return true;
+}
+
+// the same on slot i of the window's stores
+template <class R, class N>
+__device__ __forceinline__ bool cw_adj_push_one(const WinConst &c, const N &nodes, const WinS<R> &S, long long i,
+                                                int step, double wflux, int &ix, int &iy, int &iz, R (&sc)[24],
+                                                double &gB) {
+  PSt<R> st;
+  pst_load<R>(S, i, st);
+  if (!(born_of(st.b) <= step && lost_of(st.b) >= step)) return false;
+  const long long cap = S.cap;
+  R lam[6];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) lam[a] = S.lam[a * cap + i];
+  cw_adj_push_core<R>(c, nodes, st, step, wflux, lam, ix, iy, iz, sc, gB);
+#pragma unroll
+  for (int a = 0; a < 6; ++a) S.lam[a * cap + i] = lam[a];
   return true;
 }
 
@@ -1365,6 +1435,25 @@ __global__ void __launch_bounds__(AB, 3) k_cw_adj_push_tiles(Dims d, WinConst c,
 // lx += deposit^T of the adjoint potential mu for the particles deposited at
 // `step`: the deposit adds kq kdep w to np, rhs = -q np, so
 // dJ/dx += -q kdep sum_c kq mu grad w_c
+// the deposit adjoint of a particle at offsets (fx, fy, fz) given the
+// weights m_q = -q kdep kq mu at its cell's 8 nodes (M(q) returns them):
+// (lx, ly, lz) += -q kdep sum kq mu grad w
+template <class M>
+__device__ __forceinline__ void cw_adj_dep_core(const WinConst &c, double fx, double fy, double fz, M m, double &lx,
+                                                double &ly, double &lz) {
+  const double px = 1.0 - fx, py = 1.0 - fy, pz = 1.0 - fz;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const double s = m(q);
+    const double ax = ox(q) ? 1.0 - px : px, ay = oy(q) ? 1.0 - py : py, az = oz(q) ? 1.0 - pz : pz;
+    const double sx = ox(q) ? 1.0 / c.h0 : -1.0 / c.h0, sy = oy(q) ? 1.0 / c.h1 : -1.0 / c.h1,
+                 sz = oz(q) ? 1.0 / c.h2 : -1.0 / c.h2;
+    lx += sx * ay * az * s;
+    ly += ax * sy * az * s;
+    lz += ax * ay * sz * s;
+  }
+}
+
 // the deposit adjoint of slot i at `step` given the weights m_q = -q kdep kq
 // mu at its cell's 8 nodes (M(q) returns them)
 template <class R, class M>
@@ -1455,6 +1544,114 @@ __global__ void __launch_bounds__(AB) k_cw_adj_deposit_tiles(Dims d, WinConst c,
       }
     }
   }
+}
+
+// One backward step of the FP32 window fused per particle, one block per
+// tile: the deposit adjoint of step + 1 at x^{step+1} (mu of that step's
+// adjoint solve, none when mu is null), the push of `step` undone, and the
+// adjoint of that push (lE scattered through the node box as
+// k_cw_adj_push_tiles does).  The particle's state and adjoint are read and
+// written once instead of by three kernels.  Dynamic shared memory
+// CW_BACK_SMEM: E (float4), -q kdep kq mu (double) and lE (3 floats) of the
+// tile's node box.
+constexpr int CW_BACK_SMEM = WBN * (16 + 8 + 12);
+__global__ void __launch_bounds__(AB, 2) k_cw_back_tiles(Dims d, WinConst c, const float4 *__restrict__ E,
+                                                         WinS<float> S, const int *__restrict__ count, WinTiles T,
+                                                         int step, const double *__restrict__ kq,
+                                                         const double *__restrict__ mu, double wflux,
+                                                         double *__restrict__ lE, double *dBz) {
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  float4 *s_E = reinterpret_cast<float4 *>(s_dyn);
+  double *s_m = reinterpret_cast<double *>(s_dyn + 16 * WBN);
+  float *s_box = reinterpret_cast<float *>(s_dyn + 24 * WBN);
+  int bx, by, bz;
+  tile_box(T, blockIdx.x, bx, by, bz);
+  stage_E_box(d, E, bx, by, bz, s_E);
+  for (int e = threadIdx.x; e < WBN; e += AB) {
+    const int gx = bx + e % WB, gy = by + (e / WB) % WB, gz = bz + e / (WB * WB);
+    double m = 0.0;
+    if (mu && gx >= 0 && gy >= 0 && gz >= 0 && gx <= d.n1 + 2 && gy <= d.n2 + 2 && gz <= d.n3 + 2) {
+      const long long g = d.g(gx, gy, gz);
+      m = -c.q * c.kdep * kq[g] * mu[g];
+    }
+    s_m[e] = m;
+  }
+  for (int e = threadIdx.x; e < 3 * WBN; e += AB) s_box[e] = 0.f;
+  __syncthreads();
+  const ETile G{d, E, s_E, bx, by, bz};
+  const ENodesTile nodes{d, E, s_E, bx, by, bz};
+  const long long N = *count;
+  const long long lo = T.off[blockIdx.x];
+  long long hi = T.off[blockIdx.x + 1];
+  if (hi > N) hi = N;
+  const long long cap = S.cap;
+  double gB = 0.0;
+  int chunks = 0;
+  for (long long base = lo; base < hi; base += AB) {
+    // every lane takes part in the scatter sums (base is uniform over the block)
+    const long long i = base + threadIdx.x;
+    int ix = 0, iy = 0, iz = 0;
+    float r[24];
+    long long key = -1;
+    int b0 = -1;
+#pragma unroll
+    for (int q = 0; q < 24; ++q) r[q] = 0.f;
+    if (i < hi) {
+      PSt<float> st;
+      pst_load<float>(S, i, st);
+      float lam[6];
+#pragma unroll
+      for (int a = 0; a < 6; ++a) lam[a] = S.lam[a * cap + i];
+      bool lam_changed = false;
+      // the deposit adjoint of step + 1, at the position before the undo
+      if (mu && born_of(st.b) < step + 1 && lost_of(st.b) >= step + 1) {
+        int jx, jy, jz;
+        unpack_cell(st.cell, jx, jy, jz);
+        double lx = 0.0, ly = 0.0, lz = 0.0;
+        const int bm = box_base(jx, jy, jz, bx, by, bz);
+        if (bm >= 0) {
+          cw_adj_dep_core(c, st.f[0], st.f[1], st.f[2], [&](int q) { return s_m[bm + box_off(q)]; }, lx, ly, lz);
+        } else {
+          const long long g0 = d.g(jx, jy, jz);
+          cw_adj_dep_core(c, st.f[0], st.f[1], st.f[2], [&](int q) {
+            const long long g = g0 + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
+            return -c.q * c.kdep * kq[g] * mu[g];
+          }, lx, ly, lz);
+        }
+        lam[0] += (float)lx;
+        lam[1] += (float)ly;
+        lam[2] += (float)lz;
+        lam_changed = true;
+      }
+      if (cw_reverse_core<float>(d, c, st, step, G)) pst_store<float>(S, i, st);
+      if (cw_adj_push_core<float>(c, nodes, st, step, wflux, lam, ix, iy, iz, r, gB)) {
+        key = d.g(ix, iy, iz);
+        b0 = box_base(ix, iy, iz, bx, by, bz);
+        lam_changed = true;
+      }
+      if (lam_changed)
+#pragma unroll
+        for (int a = 0; a < 6; ++a) S.lam[a * cap + i] = lam[a];
+    }
+    warp_scatter_sum<24>(key, b0, r, [&](long long k, int b, int v, float val) {
+      const int q = v / 3, a = v - 3 * q;
+      if (b >= 0) {
+        atomicAdd(&s_box[3 * (b + box_off(q)) + a], val);
+      } else {
+        const long long g = k + ox(q) + d.N1 * (oy(q) + d.N2 * (long long)oz(q));
+        atomicAdd(&lE[3 * g + a], (double)val);
+      }
+    });
+    if (++chunks == WFLUSH / AB && base + AB < hi) {
+      chunks = 0;
+      __syncthreads();
+      flush_box<3>(d, s_box, bx, by, bz, nullptr, 1.0, lE);
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  flush_box<3>(d, s_box, bx, by, bz, nullptr, 1.0, lE);
+  block_add(gB, dBz);
 }
 
 // every species of the window, for the collision kernels
@@ -1778,6 +1975,39 @@ int lepic_dev_cw_adj_push(const lepic_grid_t *g, const void *E, lepic_win_specie
     }
     lepic::k_cw_adj_push<float><<<lepic::grid_for(ws->cap - first, lepic::AB), lepic::AB, 0, s>>>(
         d, c, E, lepic::win_view<float>(*ws), ws->count, first, step, wflux, lE, dBz);
+  }
+  lepic::timer_stop(tm, s);
+  LEPIC_CUDA(cudaGetLastError());
+  return LEPIC_OK;
+}
+
+int lepic_dev_cw_back(const lepic_grid_t *g, const void *E, lepic_win_species_t *ws, int ptype, const lepic_phys_t *P,
+                      int step, const double *mu, double wflux, double *lE, double *dBz, void *stream) {
+  if (!g || !E || !ws || !P || !lE || !dBz || ptype < 1 || ptype > LEPIC_NPART) return LEPIC_ERR_ARG;
+  const Dims d(g->n);
+  cudaStream_t s = (cudaStream_t)stream;
+  const lepic::WinConst c = lepic::win_const(*g, *P, ptype);
+  int tm = lepic::timer_start("cw_back", s);
+  if (ws->fp64) {
+    const lepic::WinS<double> S = lepic::win_view<double>(*ws);
+    const int gb = lepic::grid_for(ws->cap, lepic::AB);
+    if (mu) lepic::k_cw_adj_deposit<double><<<gb, lepic::AB, 0, s>>>(d, c, S, ws->count, 0, step + 1, g->kq, mu);
+    lepic::k_cw_reverse<double><<<gb, lepic::AB, 0, s>>>(d, c, E, S, ws->count, 0, step);
+    lepic::k_cw_adj_push<double><<<gb, lepic::AB, 0, s>>>(d, c, E, S, ws->count, 0, step, wflux, lE, dBz);
+  } else {
+    const lepic::WinS<float> S = lepic::win_view<float>(*ws);
+    long long first = 0;
+    if (ws->tile_off) {
+      const lepic::WinTiles T = lepic::win_tiles(*g, *ws);
+      cudaFuncSetAttribute(lepic::k_cw_back_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, lepic::CW_BACK_SMEM);
+      lepic::k_cw_back_tiles<<<LEPIC_TILES(g->n), lepic::AB, lepic::CW_BACK_SMEM, s>>>(
+          d, c, (const float4 *)E, S, ws->count, T, step, g->kq, mu, wflux, lE, dBz);
+      first = ws->tile_end;
+    }
+    const int gb = lepic::grid_for(ws->cap - first, lepic::AB);
+    if (mu) lepic::k_cw_adj_deposit<float><<<gb, lepic::AB, 0, s>>>(d, c, S, ws->count, first, step + 1, g->kq, mu);
+    lepic::k_cw_reverse<float><<<gb, lepic::AB, 0, s>>>(d, c, E, S, ws->count, first, step);
+    lepic::k_cw_adj_push<float><<<gb, lepic::AB, 0, s>>>(d, c, E, S, ws->count, first, step, wflux, lE, dBz);
   }
   lepic::timer_stop(tm, s);
   LEPIC_CUDA(cudaGetLastError());

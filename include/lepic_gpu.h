@@ -726,6 +726,13 @@ int lepic_dev_cw_reverse(const lepic_grid_t *g, const void *E, lepic_win_species
                          const lepic_phys_t *P, int step, void *stream);
 int lepic_dev_cw_adj_push(const lepic_grid_t *g, const void *E, lepic_win_species_t *ws, int ptype,
                           const lepic_phys_t *P, int step, double wflux, double *lE, double *dBz, void *stream);
+/* One backward step, fused: cw_adj_deposit of step + 1 (mu of that step;
+ * NULL: none), cw_reverse of step, cw_adj_push of step -- what the three
+ * calls do in that order, with the particle state read once (FP32 window
+ * with tile offsets: one kernel per tile). */
+int lepic_dev_cw_back(const lepic_grid_t *g, const void *E, lepic_win_species_t *ws, int ptype,
+                      const lepic_phys_t *P, int step, const double *mu, double wflux, double *lE, double *dBz,
+                      void *stream);
 int lepic_dev_cw_adj_deposit(const lepic_grid_t *g, lepic_win_species_t *ws, int ptype, const lepic_phys_t *P,
                              int step, const double *mu, void *stream);
 int lepic_dev_win_collisions(const lepic_grid_t *g, lepic_win_species_t *ws, int ntype, const lepic_tables_t *T,
