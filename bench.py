@@ -284,7 +284,7 @@ def _e2e(sim, st, steps, world, dist, torch):
 # on the 96^3 workload (5.7e7 particles per species); the traffic grows in
 # proportion to the particles, so a launch's traffic is this times its
 # particles
-MEASURED_TRAFFIC_PER_PARTICLE = {"push_deposit_mixed": 57.4, "push_deposit_f64": 96.6}
+MEASURED_TRAFFIC_PER_PARTICLE = {"push_mixed": 57.4, "deposit_mixed_tiles": 17.0, "push_deposit_f64": 96.6}
 
 
 def _roofline(timers, kname, bytes_per_particle, nps):
@@ -478,7 +478,8 @@ def run_large(args):
            "particles_at_end": int(R["sim"].counts_host().sum()),
            "phi_err_vs_f64": perr["mixed"], "phi_err_detail": perr,
            "poisson_iters_per_solve": float(np.mean(R["iters"])) if R["iters"] else None,
-           "roofline": _roofline(timers, "push_deposit_mixed", 57.0, R["nps"]),
+           "roofline": _roofline(timers, "push_mixed", 57.0, R["nps"]),
+           "roofline_deposit": _roofline(timers, "deposit_mixed_tiles", 17.0, R["nps"]),
            "kernel_ms": {k: round(v[0], 3) for k, v in sorted(timers.items())},
            "kernel_launches": {k: v[1] for k, v in sorted(timers.items())},
            "clocks": R["clocks"]}
@@ -765,7 +766,7 @@ def run_ours(args):
         if world > 1:
             dist.destroy_process_group()
         return
-    kname = "push_deposit_mixed" if head == "mixed" else (
+    kname = "push_mixed" if head == "mixed" else (
         "push_deposit_f64" if "push_deposit_f64" in R["timers"] else "push_f64")
     bpp = 57.0 if head == "mixed" else 96.0
     timers = R["timers"]

@@ -383,6 +383,40 @@ __device__ __forceinline__ void qweights(float gx, float gy, float gz, int w[8])
   w[7] = (1 << QBITS) - (w[0] + w[1] + w[2] + w[3] + w[4] + w[5] + w[6]);
 }
 
+__device__ __forceinline__ unsigned run_lanemask_le() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_le;" : "=r"(m));
+  return m;
+}
+
+// Sum of v over each run of consecutive lanes with the same key: afterwards
+// the first lane of a run (head) holds the run's totals.  Lanes with key -1
+// contribute zeros.  All 32 lanes must call this.  Particles sorted by cell
+// give a warp few runs, so the atomics that follow are one per run instead
+// of one per particle (lanes adding to one shared word are serialised).
+template <int NV, class T = double>
+__device__ __forceinline__ bool warp_run_sum(long long key, T (&v)[NV]) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const long long prev = __shfl_up_sync(full, key, 1);
+  const bool head = (lane == 0) || prev != key;
+  const unsigned heads = __ballot_sync(full, head);
+  const int rid = __popc(heads & run_lanemask_le());
+  const unsigned above = heads & ~(0xffffffffu >> (31 - lane));
+  const int len = head ? ((above ? __ffs(above) - 1 : 32) - lane) : 0;
+  const int maxlen = (int)__reduce_max_sync(full, (unsigned)len);
+  for (int o = 1; o < maxlen; o <<= 1) {
+    const int orid = __shfl_down_sync(full, rid, o);
+    const bool same = (lane + o < 32) && orid == rid;
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+      const T t = __shfl_down_sync(full, v[c], o);
+      if (same) v[c] += t;
+    }
+  }
+  return head && key >= 0;
+}
+
 }  // namespace lepic
 
 #define LEPIC_CUDA(call)                                                 \

@@ -115,12 +115,13 @@ struct Tile {
   const float4 *B;            // B map at the box nodes (map on the node grid)
 };
 
-// box-local coordinates of cell (ix,iy,iz) when the cell's 8 nodes are in the box
+// box-local coordinates of cell (ix,iy,iz) when the cell's 8 nodes are in the
+// box (a block with no box, the untiled tail, has neither acc nor E)
 __device__ __forceinline__ bool in_box(const Tile &T, int ix, int iy, int iz, int &lx, int &ly, int &lz) {
   lx = ix - T.bx;
   ly = iy - T.by;
   lz = iz - T.bz;
-  return T.acc && (unsigned)lx < (unsigned)(TN - 1) && (unsigned)ly < (unsigned)(TN - 1) &&
+  return (T.acc || T.E) && (unsigned)lx < (unsigned)(TN - 1) && (unsigned)ly < (unsigned)(TN - 1) &&
          (unsigned)lz < (unsigned)(TN - 1);
 }
 
@@ -241,10 +242,77 @@ __device__ __forceinline__ bool bmap_gather_mixed(const MixedBMap &m, const Tile
   return true;
 }
 
+// Deposit of a lane's up to four particles (jx < 0: none) at cells (jx, jy,
+// jz) and offsets (gx, gy, gz): the particles that end in the lane's first
+// particle's cell are merged before touching shared memory
+__device__ __forceinline__ void deposit_quad(const Dims &d, const Tile &T, const int (&jx)[4], const int (&jy)[4],
+                                             const int (&jz)[4], const float (&gx)[4], const float (&gy)[4],
+                                             const float (&gz)[4], double kdep, const double *__restrict__ kq,
+                                             double *__restrict__ np) {
+  // the first particle's cell by selects (an index into jx would put the
+  // arrays in local memory)
+  int ax = -1, ay = 0, az = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (ax < 0 && jx[k] >= 0) {
+      ax = jx[k];
+      ay = jy[k];
+      az = jz[k];
+    }
+  if (ax < 0) return;
+  int wa[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (jx[k] < 0) continue;
+    int w[8];
+    qweights(gx[k], gy[k], gz[k], w);
+    if (jx[k] == ax && jy[k] == ay && jz[k] == az) {
+#pragma unroll
+      for (int cc = 0; cc < 8; ++cc) wa[cc] += w[cc];
+    } else {
+      deposit8(d, T, jx[k], jy[k], jz[k], d.g(jx[k], jy[k], jz[k]), w, kdep, kq, np);
+    }
+  }
+  deposit8(d, T, ax, ay, az, d.g(ax, ay, az), wa, kdep, kq, np);
+}
+
+// deposit_quad with the first-cell sums of the warp's lanes merged per run
+// of lanes starting in one cell (sorted particles: one to three runs per
+// warp), so that a cell's 8 shared words take one add per run instead of one
+// per lane.  All 32 lanes must call this.
+__device__ __forceinline__ void deposit_quad_warp(const Dims &d, const Tile &T, const int (&jx)[4],
+                                                  const int (&jy)[4], const int (&jz)[4], const float (&gx)[4],
+                                                  const float (&gy)[4], const float (&gz)[4], double kdep,
+                                                  const double *__restrict__ kq, double *__restrict__ np) {
+  int ax = -1, ay = 0, az = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (ax < 0 && jx[k] >= 0) {
+      ax = jx[k];
+      ay = jy[k];
+      az = jz[k];
+    }
+  int wa[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (jx[k] < 0) continue;
+    int w[8];
+    qweights(gx[k], gy[k], gz[k], w);
+    if (jx[k] == ax && jy[k] == ay && jz[k] == az) {
+#pragma unroll
+      for (int cc = 0; cc < 8; ++cc) wa[cc] += w[cc];
+    } else {
+      deposit8(d, T, jx[k], jy[k], jz[k], d.g(jx[k], jy[k], jz[k]), w, kdep, kq, np);
+    }
+  }
+  const long long key = ax >= 0 ? d.g(ax, ay, az) : -1LL;
+  if (warp_run_sum<8, int>(key, wa)) deposit8(d, T, ax, ay, az, key, wa, kdep, kq, np);
+}
+
 // Push + loss test + deposit of the particle quad Q starting at i0;
 // particles outside the range are not touched.  Every lane of the warp must
 // call this (warp-wide hole appends).  BMAP: B from the map m.
-template <bool BMAP, bool DIE>
+template <bool BMAP, bool DIE, bool DEP = true>
 __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, const MixedBMap &m, const Tile &T,
                                           long long i0, Quad &Q, const float4 *__restrict__ E4,
                                           const int *__restrict__ bcnd, const unsigned char *__restrict__ cw,
@@ -459,48 +527,29 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
       }
     }
   }
-  // deposit: merge this lane's particles that end in its first particle's cell
-  int a0 = -1;
-#pragma unroll
-  for (int k = 0; k < 4; ++k)
-    if (a0 < 0 && jx[k] >= 0) a0 = k;
-  if (a0 < 0) return;
-  int wa[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  const int ax = jx[a0], ay = jy[a0], az = jz[a0];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (jx[k] < 0) continue;
-    int w[8];
-    qweights(gxs[k], gys[k], gzs[k], w);
-    if (jx[k] == ax && jy[k] == ay && jz[k] == az) {
-#pragma unroll
-      for (int cc = 0; cc < 8; ++cc) wa[cc] += w[cc];
-    } else {
-      deposit8(d, T, jx[k], jy[k], jz[k], d.g(jx[k], jy[k], jz[k]), w, c.kdep, kq, np);
-    }
-  }
-  deposit8(d, T, ax, ay, az, d.g(ax, ay, az), wa, c.kdep, kq, np);
+  if (DEP) deposit_quad(d, T, jx, jy, jz, gxs, gys, gzs, c.kdep, kq, np);
 }
 
 // one block per tile: the particles [tile_off[t], tile_off[t+1]) of the last
 // sort, clipped to the current count; E and the wall flags of the tile's box
-// are read into shared memory once
+// are read into shared memory once.  The push only: k_deposit_tiles deposits
+// the pushed particles of the tile afterwards (one kernel doing both was 6 %
+// slower: its shared-memory adds and flush barriers sat between the push's
+// memory accesses)
 template <bool BMAP, bool DIE>
-__global__ void __launch_bounds__(MBK, 3) k_push_deposit_tiles(
+__global__ void __launch_bounds__(MBK, 3) k_push_tiles(
     Dims d, MixedConst c, MixedBMap m, const float4 *__restrict__ E4, const int *__restrict__ bcnd,
     const unsigned char *__restrict__ cw, int *__restrict__ cell, float *__restrict__ p, long long cap,
     const int *__restrict__ count, signed char *__restrict__ flag, const int *__restrict__ tile_off,
     const double *__restrict__ kq, double *__restrict__ np, int *__restrict__ holes, int *__restrict__ nholes,
     double *__restrict__ acc, int *__restrict__ err) {
-  __shared__ unsigned s_acc[TT];
   __shared__ float4 s_E[TT];
   __shared__ unsigned char s_cw[(TN - 1) * (TN - 1) * (TN - 1)];
   __shared__ float4 s_B[BMAP ? TT : 1];
   const int t = blockIdx.x;
   const int tx = t % c.ntx, ty = (t / c.ntx) % c.nty, tz = t / (c.ntx * c.nty);
-  const Tile T{s_acc, s_E, s_cw, tx * TC, ty * TC, tz * TC, s_B};
+  const Tile T{nullptr, s_E, s_cw, tx * TC, ty * TC, tz * TC, s_B};
   for (int e = threadIdx.x; e < TT; e += MBK) {
-    s_acc[e] = 0u;
     const int lx = e % TN, ly = (e / TN) % TN, lz = e / (TN * TN);
     const int gx = T.bx + lx, gy = T.by + ly, gz = T.bz + lz;
     const bool ing = gx <= d.n1 + 2 && gy <= d.n2 + 2 && gz <= d.n3 + 2;
@@ -519,21 +568,74 @@ __global__ void __launch_bounds__(MBK, 3) k_push_deposit_tiles(
   const long long lo = tile_off[t];
   long long hi = tile_off[t + 1];
   if (hi > N) hi = N;
-  int chunks = 0;
   for (long long base = lo & ~3LL; base < hi; base += CHUNK) {
     Quad Q;
     const long long i0 = base + 4 * threadIdx.x;
     load_quad(Q, i0, lo, hi, cell, p, cap, flag);
-    push_quad<BMAP, DIE>(d, c, m, T, i0, Q, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes, acc, err);
+    push_quad<BMAP, DIE, false>(d, c, m, T, i0, Q, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes, acc,
+                                err);
+  }
+}
+
+// The deposit of a tile's pushed particles (those the push kept: holes, flag
+// 2, skipped) into a 32-bit node tile in shared memory, flushed into the FP64
+// grid after every FLUSH_PARTICLES particles
+__global__ void __launch_bounds__(MBK, 4) k_deposit_tiles(Dims d, int ntx, int nty, double kdep,
+                                                        const int *__restrict__ cell, const float *__restrict__ p,
+                                                        long long cap, const int *__restrict__ count,
+                                                        const signed char *__restrict__ flag,
+                                                        const int *__restrict__ tile_off,
+                                                        const double *__restrict__ kq, double *__restrict__ np) {
+  __shared__ unsigned s_acc[TT];
+  const int t = blockIdx.x;
+  const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
+  const Tile T{s_acc, nullptr, nullptr, tx * TC, ty * TC, tz * TC, nullptr};
+  for (int e = threadIdx.x; e < TT; e += MBK) s_acc[e] = 0u;
+  __syncthreads();
+  const long long N = *count;
+  const long long lo = tile_off[t];
+  long long hi = tile_off[t + 1];
+  if (hi > N) hi = N;
+  int chunks = 0;
+  for (long long base = lo & ~3LL; base < hi; base += CHUNK) {
+    const long long i0 = base + 4 * threadIdx.x;
+    int jx[4], jy[4], jz[4];
+    float gx[4], gy[4], gz[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      jx[k] = -1;
+      jy[k] = jz[k] = 0;
+      gx[k] = gy[k] = gz[k] = 0.f;
+    }
+    if (i0 < hi) {
+      const int4 c4 = *reinterpret_cast<const int4 *>(cell + i0);
+      const char4 f4 = *reinterpret_cast<const char4 *>(flag + i0);
+      const float4 P0 = *reinterpret_cast<const float4 *>(p + i0);
+      const float4 P1 = *reinterpret_cast<const float4 *>(p + cap + i0);
+      const float4 P2 = *reinterpret_cast<const float4 *>(p + 2 * cap + i0);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int cc = (&c4.x)[k];
+        if (i0 + k >= lo && i0 + k < hi && (&f4.x)[k] != 2) {
+          jx[k] = (cc & CM) + 1;
+          jy[k] = ((cc >> CB) & CM) + 1;
+          jz[k] = (cc >> (2 * CB)) + 1;
+          gx[k] = (&P0.x)[k];
+          gy[k] = (&P1.x)[k];
+          gz[k] = (&P2.x)[k];
+        }
+      }
+    }
+    deposit_quad_warp(d, T, jx, jy, jz, gx, gy, gz, kdep, kq, np);
     if (++chunks == FLUSH_PARTICLES / CHUNK && base + CHUNK < hi) {
       chunks = 0;
       __syncthreads();
-      flush_tile(d, T, c.kdep, kq, np);
+      flush_tile(d, T, kdep, kq, np);
       __syncthreads();
     }
   }
   __syncthreads();
-  flush_tile(d, T, c.kdep, kq, np);
+  flush_tile(d, T, kdep, kq, np);
 }
 
 // particles past the last tile (appended since the sort), or all of them
@@ -966,7 +1068,7 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
     }
   }
   const float4 *E = reinterpret_cast<const float4 *>(E4);
-  int t0 = timer_start("push_deposit_mixed", s);
+  int t0 = timer_start("push_mixed", s);
   // the tail: at most what was appended since the sort unless never sorted
   long long tail = sp.tile_off ? (long long)ctx().sms * 2 : grid_for(n_hint > 0 ? n_hint : sp.cap, CHUNK);
   if (tail > (long long)ctx().sms * 8) tail = (long long)ctx().sms * 8;
@@ -975,12 +1077,9 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
   auto run = [&](auto bmap, auto die) {
     constexpr bool B = decltype(bmap)::value, D = decltype(die)::value;
     if (sp.tile_off)
-      k_push_deposit_tiles<B, D><<<c.ntiles, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap,
-                                                          sp.count, sp.flag_dead, sp.tile_off, g.kq, np, holes,
-                                                          side, acc, ctx().d_err);
-    k_push_deposit_tail<B, D><<<(int)tail, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap,
-                                                        sp.count, sp.flag_dead, sp.tile_off, g.kq, np, holes,
-                                                        side, acc, ctx().d_err);
+      k_push_tiles<B, D><<<c.ntiles, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap, sp.count,
+                                                  sp.flag_dead, sp.tile_off, g.kq, np, holes, side, acc,
+                                                  ctx().d_err);
   };
   const bool die = c.die.dtype != nullptr;
   if (m.B && die)
@@ -992,6 +1091,28 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
   else
     run(std::false_type{}, std::false_type{});
   timer_stop(t0, s);
+  int td = timer_start("deposit_mixed_tiles", s);
+  if (sp.tile_off)
+    k_deposit_tiles<<<c.ntiles, MBK, 0, s>>>(d, c.ntx, c.nty, c.kdep, sp.cell, sp.p, sp.cap, sp.count, sp.flag_dead,
+                                             sp.tile_off, g.kq, np);
+  timer_stop(td, s);
+  // the tail (appended since the sort): push and deposit in one pass
+  int t2 = timer_start("push_deposit_mixed_tail", s);
+  auto run_tail = [&](auto bmap, auto die) {
+    constexpr bool B = decltype(bmap)::value, D = decltype(die)::value;
+    k_push_deposit_tail<B, D><<<(int)tail, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap,
+                                                        sp.count, sp.flag_dead, sp.tile_off, g.kq, np, holes,
+                                                        side, acc, ctx().d_err);
+  };
+  if (m.B && die)
+    run_tail(std::true_type{}, std::true_type{});
+  else if (m.B)
+    run_tail(std::true_type{}, std::false_type{});
+  else if (die)
+    run_tail(std::false_type{}, std::true_type{});
+  else
+    run_tail(std::false_type{}, std::false_type{});
+  timer_stop(t2, s);
   LEPIC_CUDA(cudaGetLastError());
   int t1 = timer_start("fill_holes_mixed", s);
   const int fb = ctx().sms * 2;
