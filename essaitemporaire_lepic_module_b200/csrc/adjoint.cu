@@ -841,8 +841,8 @@ __device__ void flush_box(const Dims &d, float *box, int bx, int by, int bz, con
 }
 
 // the box's non-zero integer weight sums (units of 2^-QBITS, exact modulo
-// 2^32: a node's sum over WFLUSH particles lies in [-5 WFLUSH, 2^31]) into
-// the FP64 grid, kdep kq applied, then cleared
+// 2^32: a node's sum over WFLUSH particles lies in [-5, 2^20 + 5] x WFLUSH)
+// into the FP64 grid, kdep kq applied, then cleared
 __device__ void flush_qbox(const Dims &d, unsigned *box, int bx, int by, int bz, const double *__restrict__ kq,
                            double kdep, double *__restrict__ np) {
   for (int e = threadIdx.x; e < WBN; e += blockDim.x) {
@@ -851,13 +851,12 @@ __device__ void flush_qbox(const Dims &d, unsigned *box, int bx, int by, int bz,
     const int gx = bx + e % WB, gy = by + (e / WB) % WB, gz = bz + e / (WB * WB);
     if (gx >= 0 && gy >= 0 && gz >= 0 && gx <= d.n1 + 2 && gy <= d.n2 + 2 && gz <= d.n3 + 2) {
       const long long g = d.g(gx, gy, gz);
-      const double val = v <= 0x80000000u ? (double)v : (double)v - 4294967296.0;
-      atomicAdd(&np[g], kq[g] * (kdep * (val * QI)));
+      atomicAdd(&np[g], kq[g] * (kdep * (qsum_value(v, WFLUSH) * QI)));
     }
     box[e] = 0u;
   }
 }
-static_assert((long long)WFLUSH << QBITS <= (1LL << 31), "node sums of a flush window fit 2^31");
+static_assert(qsum_window_ok(WFLUSH), "node sums of a flush window are read back modulo 2^32");
 
 // the FP32 window's deposit, one block per tile: the integer weights of the
 // mixed step (2^20 units per particle), summed exactly in a 32-bit node box

@@ -367,8 +367,8 @@ __device__ __forceinline__ int round_q(float x) { return __float_as_int(x + 1258
 // (1,0,0), (1,1,0), (0,1,0), then the same at z+1): seven rounded, the
 // eighth the remainder.  The remainder may be a few units below zero for a
 // particle next to the opposite corner (the seven rounding errors are at
-// most 0.7 units each); 32-bit node sums are exact modulo 2^32 and are read
-// back from that range when they are flushed into the FP64 grid.
+// most 0.5 units each), and no weight is above 2^20.
+constexpr int QNEG = 5;                    // a weight is above -QNEG units
 __device__ __forceinline__ void qweights(float gx, float gy, float gz, int w[8]) {
   const float S = (float)(1 << QBITS);
   const float qx = 1.f - gx, qy = 1.f - gy, qz = 1.f - gz;
@@ -381,6 +381,14 @@ __device__ __forceinline__ void qweights(float gx, float gy, float gz, int w[8])
   w[5] = round_q(gx * e);
   w[6] = round_q(gx * f);
   w[7] = (1 << QBITS) - (w[0] + w[1] + w[2] + w[3] + w[4] + w[5] + w[6]);
+}
+
+// A node's 32-bit sum over a window of at most n particles lies in
+// [-QNEG n, 2^20 n]; read back modulo 2^32 (the two ends must stay apart:
+// qsum_window_ok)
+constexpr bool qsum_window_ok(long long n) { return n * ((1LL << QBITS) + 2 * QNEG) < (1LL << 32); }
+__device__ __forceinline__ double qsum_value(unsigned v, long long n) {
+  return v <= (unsigned)(n * ((1LL << QBITS) + QNEG)) ? (double)v : (double)v - 4294967296.0;
 }
 
 __device__ __forceinline__ unsigned run_lanemask_le() {
@@ -417,7 +425,36 @@ __device__ __forceinline__ bool warp_run_sum(long long key, T (&v)[NV]) {
   return head && key >= 0;
 }
 
+// ------------------------------------------------------------- mbarriers
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long gtime() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// wait for phase `parity` of the mbarrier, at most one second
+__device__ inline bool mbar_wait(uint32_t bar, uint32_t parity) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = gtime();
+  while (!mbar_try(bar, parity))
+    if (gtime() - t0 > 1000000000ull) return false;
+  return true;
+}
+
 }  // namespace lepic
+
 
 #define LEPIC_CUDA(call)                                                 \
   do {                                                                   \

@@ -171,33 +171,6 @@ __device__ double grid_sum(const XArgs &a, double v, int parity, cg::grid_group 
 }
 
 // ------------------------------------------------------------ tile copies
-__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ unsigned long long gtime() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// wait for phase `parity` of the mbarrier, at most one second
-__device__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  if (mbar_try(bar, parity)) return true;
-  const unsigned long long t0 = gtime();
-  while (!mbar_try(bar, parity))
-    if (gtime() - t0 > 1000000000ull) return false;
-  return true;
-}
-
 __device__ __forceinline__ void tma_box(uint32_t dst, const CUtensorMap *m, int x, int y, int z, uint32_t bar) {
   asm volatile(
       "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "

@@ -19,8 +19,8 @@
 // shared-memory adds into a node tile covering the tile's cells plus one halo
 // cell on each side.  The node tile is added to the FP64 grid (one atomic per
 // non-zero node) and cleared after every FLUSH_PARTICLES particles, so a
-// node's sum stays within [-5 FLUSH_PARTICLES, FLUSH_PARTICLES * 2^20 = 2^31]
-// however the particles are placed.  Particles outside the box (drifted since the sort, moved by
+// node's sum stays within [-5, 2^20] x FLUSH_PARTICLES however the particles
+// are placed and is read back unambiguously modulo 2^32.  Particles outside the box (drifted since the sort, moved by
 // hole filling, appended by collisions) add their integer weights to the grid
 // directly.  kdep and kq are applied in FP64 to the integer sums.
 //
@@ -41,8 +41,9 @@ constexpr int TC = LEPIC_TILE_CELLS;       // tile edge in cells
 constexpr int TN = TC + 3;                 // node tile edge (halo cell each side)
 constexpr int TT = TN * TN * TN;
 constexpr int CHUNK = 4 * MBK;             // particles per block iteration
-constexpr int FLUSH_PARTICLES = 2048;      // node sums <= 2048 * 2^20 = 2^31
+constexpr int FLUSH_PARTICLES = 3072;      // node sums <= 3072 * 2^20 = 0xC0000000
 static_assert(FLUSH_PARTICLES % CHUNK == 0, "flush windows are whole chunks");
+static_assert(qsum_window_ok(FLUSH_PARTICLES), "window sums are read back modulo 2^32");
 constexpr int CB = LEPIC_CELL_BITS, CM = LEPIC_CELL_MAX - 1;
 
 __device__ __forceinline__ unsigned lmask_lt() {
@@ -115,6 +116,27 @@ struct Tile {
   const float4 *B;            // B map at the box nodes (map on the node grid)
 };
 
+// sum of k_i e_i, i = 0..7, rounded as a chain of multiply-adds in order
+__device__ __forceinline__ float gather8(float k0, float k1, float k2, float k3, float k4, float k5, float k6,
+                                         float k7, float e0, float e1, float e2, float e3, float e4, float e5,
+                                         float e6, float e7) {
+  float s = __fmul_rn(k0, e0);
+  s = __fmaf_rn(k1, e1, s);
+  s = __fmaf_rn(k2, e2, s);
+  s = __fmaf_rn(k3, e3, s);
+  s = __fmaf_rn(k4, e4, s);
+  s = __fmaf_rn(k5, e5, s);
+  s = __fmaf_rn(k6, e6, s);
+  return __fmaf_rn(k7, e7, s);
+}
+
+// a float4 from shared memory at 32-bit shared address a
+__device__ __forceinline__ float4 lds4(uint32_t a) {
+  float4 v;
+  asm("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+  return v;
+}
+
 // box-local coordinates of cell (ix,iy,iz) when the cell's 8 nodes are in the
 // box (a block with no box, the untiled tail, has neither acc nor E)
 __device__ __forceinline__ bool in_box(const Tile &T, int ix, int iy, int iz, int &lx, int &ly, int &lz) {
@@ -134,10 +156,12 @@ __device__ __forceinline__ void deposit8(const Dims &d, const Tile &T, int jx, i
   const long long o[8] = {0, 1, 1 + sy, sy, sz, 1 + sz, 1 + sy + sz, sy + sz};
   int lx, ly, lz;
   if (in_box(T, jx, jy, jz, lx, ly, lz)) {
-    const int t = lx + TN * (ly + TN * lz);
-    const int to[8] = {0, 1, 1 + TN, TN, TN * TN, 1 + TN * TN, 1 + TN + TN * TN, TN + TN * TN};
+    // shared-memory reductions on 32-bit addresses
+    const uint32_t a0 = smem_addr(T.acc) + 4u * (uint32_t)(lx + TN * (ly + TN * lz));
+    const uint32_t to[8] = {0, 1, 1 + TN, TN, TN * TN, 1 + TN * TN, 1 + TN + TN * TN, TN + TN * TN};
 #pragma unroll
-    for (int c = 0; c < 8; ++c) atomicAdd(&T.acc[t + to[c]], (unsigned)w[c]);
+    for (int c = 0; c < 8; ++c)
+      asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(a0 + 4u * to[c]), "r"((unsigned)w[c]) : "memory");
   } else {
 #pragma unroll
     for (int c = 0; c < 8; ++c) atomicAdd(&np[q + o[c]], __ldg(&kq[q + o[c]]) * (kdep * ((double)w[c] * QI)));
@@ -154,9 +178,7 @@ __device__ void flush_tile(const Dims &d, const Tile &T, double kdep, const doub
       const int gx = T.bx + lx, gy = T.by + ly, gz = T.bz + lz;
       if (gx <= d.n1 + 2 && gy <= d.n2 + 2 && gz <= d.n3 + 2) {
         const long long node = d.g(gx, gy, gz);
-        // a node's sum over a window lies in [-5 FLUSH_PARTICLES, 2^31]
-        // (a remainder weight is at least -5 units): read it modulo 2^32
-        const double val = v <= 0x80000000u ? (double)v : (double)v - 4294967296.0;
+        const double val = qsum_value(v, FLUSH_PARTICLES);
         atomicAdd(&np[node], __ldg(&kq[node]) * (kdep * (val * QI)));
       }
       T.acc[e] = 0u;
@@ -357,25 +379,44 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
     const float k0 = px * py * pz, ka = (1.f - px) * py * pz, kb = (1.f - px) * (1.f - py) * pz,
                 kc = px * (1.f - py) * pz, kd = px * py * (1.f - pz), ke = (1.f - px) * py * (1.f - pz),
                 kf = (1.f - px) * (1.f - py) * (1.f - pz), kg = px * (1.f - py) * (1.f - pz);
-    // from the box in shared memory when the cell is in it, else from HBM
-    const float4 *Eb = E4;
-    long long g0 = d.g(ix, iy, iz), sy = d.N1, sz = d.N1 * d.N2;
-    bool boxed = false;
-    {
-      int lx, ly, lz;
-      if (in_box(T, ix, iy, iz, lx, ly, lz)) {
-        Eb = T.E;
-        g0 = lx + TN * (ly + TN * lz);
-        sy = TN;
-        sz = TN * TN;
-        boxed = true;
-      }
+    // from the box in shared memory when the cell is in it (shared-memory
+    // loads on 32-bit addresses), else from HBM
+    long long g0, sy, sz;
+    float4 e0, e1, e2, e3, e4, e5, e6, e7;
+    int lx, ly, lz;
+    const bool boxed = in_box(T, ix, iy, iz, lx, ly, lz);
+    if (boxed) {
+      g0 = lx + TN * (ly + TN * lz);
+      sy = TN;
+      sz = TN * TN;
+      const uint32_t a0 = smem_addr(T.E) + 16u * (uint32_t)g0;
+      e0 = lds4(a0);
+      e1 = lds4(a0 + 16u);
+      e2 = lds4(a0 + 16u * (1 + TN));
+      e3 = lds4(a0 + 16u * TN);
+      e4 = lds4(a0 + 16u * TN * TN);
+      e5 = lds4(a0 + 16u * (1 + TN * TN));
+      e6 = lds4(a0 + 16u * (1 + TN + TN * TN));
+      e7 = lds4(a0 + 16u * (TN + TN * TN));
+    } else {
+      g0 = d.g(ix, iy, iz);
+      sy = d.N1;
+      sz = d.N1 * d.N2;
+      const float4 *q = E4 + g0;
+      e0 = __ldg(q);
+      e1 = __ldg(q + 1);
+      e2 = __ldg(q + 1 + sy);
+      e3 = __ldg(q + sy);
+      e4 = __ldg(q + sz);
+      e5 = __ldg(q + 1 + sz);
+      e6 = __ldg(q + 1 + sy + sz);
+      e7 = __ldg(q + sy + sz);
     }
-    const float4 e0 = Eb[g0], e1 = Eb[g0 + 1], e2 = Eb[g0 + 1 + sy], e3 = Eb[g0 + sy], e4 = Eb[g0 + sz],
-                 e5 = Eb[g0 + 1 + sz], e6 = Eb[g0 + 1 + sy + sz], e7 = Eb[g0 + sy + sz];
-    const float Ex = k0 * e0.x + ka * e1.x + kb * e2.x + kc * e3.x + kd * e4.x + ke * e5.x + kf * e6.x + kg * e7.x;
-    const float Ey = k0 * e0.y + ka * e1.y + kb * e2.y + kc * e3.y + kd * e4.y + ke * e5.y + kf * e6.y + kg * e7.y;
-    const float Ez = k0 * e0.z + ka * e1.z + kb * e2.z + kc * e3.z + kd * e4.z + ke * e5.z + kf * e6.z + kg * e7.z;
+    // the weighted sums as explicit multiply-adds in node order: the same
+    // rounding whichever path loaded the nodes and whichever kernel pushes
+    const float Ex = gather8(k0, ka, kb, kc, kd, ke, kf, kg, e0.x, e1.x, e2.x, e3.x, e4.x, e5.x, e6.x, e7.x);
+    const float Ey = gather8(k0, ka, kb, kc, kd, ke, kf, kg, e0.y, e1.y, e2.y, e3.y, e4.y, e5.y, e6.y, e7.y);
+    const float Ez = gather8(k0, ka, kb, kc, kd, ke, kf, kg, e0.z, e1.z, e2.z, e3.z, e4.z, e5.z, e6.z, e7.z);
     const float k1 = c.k1;
     float Bx = c.Bx, By = c.By, Bz = c.Bz, kk = c.kk;
     bool boris = c.boris;
@@ -530,12 +571,29 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
   if (DEP) deposit_quad(d, T, jx, jy, jz, gxs, gys, gzs, c.kdep, kq, np);
 }
 
+// A thread's next quad (cell, six FP32 planes, flags) copied into shared
+// memory by cp.async while it pushes the current one: plane a of thread j at
+// s_stage[a][j] (16 bytes per thread and plane, conflict-free), the flags
+// after the seven planes.  Each thread reads back only what it copied, so no
+// barrier orders the copies.
+constexpr int STAGE_BYTES = MBK * (7 * 16 + 4);
+extern __shared__ __align__(16) unsigned char mx_stage[];
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+
 // one block per tile: the particles [tile_off[t], tile_off[t+1]) of the last
 // sort, clipped to the current count; E and the wall flags of the tile's box
-// are read into shared memory once.  The push only: k_deposit_tiles deposits
-// the pushed particles of the tile afterwards (one kernel doing both was 6 %
-// slower: its shared-memory adds and flush barriers sat between the push's
-// memory accesses)
+// are read into shared memory once, and each thread's next quad is in flight
+// (cp.async) while it pushes the current one, so the particle loads do not
+// stall the warps.  The push only: k_deposit_tiles deposits the pushed
+// particles of the tile afterwards (one kernel doing both was 6 % slower: its
+// shared-memory adds and flush barriers sat between the push's memory
+// accesses)
 template <bool BMAP, bool DIE>
 __global__ void __launch_bounds__(MBK, 3) k_push_tiles(
     Dims d, MixedConst c, MixedBMap m, const float4 *__restrict__ E4, const int *__restrict__ bcnd,
@@ -546,9 +604,28 @@ __global__ void __launch_bounds__(MBK, 3) k_push_tiles(
   __shared__ float4 s_E[TT];
   __shared__ unsigned char s_cw[(TN - 1) * (TN - 1) * (TN - 1)];
   __shared__ float4 s_B[BMAP ? TT : 1];
+  float4 *s_st = reinterpret_cast<float4 *>(mx_stage);   // [7][MBK]
+  char4 *s_fl = reinterpret_cast<char4 *>(mx_stage + 7 * 16 * MBK);
   const int t = blockIdx.x;
   const int tx = t % c.ntx, ty = (t / c.ntx) % c.nty, tz = t / (c.ntx * c.nty);
   const Tile T{nullptr, s_E, s_cw, tx * TC, ty * TC, tz * TC, s_B};
+  const long long N = *count;
+  const long long lo = tile_off[t];
+  long long hi = tile_off[t + 1];
+  if (hi > N) hi = N;
+  const long long first = lo & ~3LL;
+  // the copies of this thread's quad at i0 (i0 < hi: i0 + 3 < cap, 16-byte
+  // aligned as i0 is a multiple of 4)
+  auto fetch = [&](long long i0) {
+    if (i0 < hi) {
+      cp_async16(&s_st[threadIdx.x], cell + i0);
+#pragma unroll
+      for (int a = 0; a < 6; ++a) cp_async16(&s_st[(a + 1) * MBK + threadIdx.x], p + a * cap + i0);
+      cp_async4(&s_fl[threadIdx.x], flag + i0);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  fetch(first + 4 * threadIdx.x);
   for (int e = threadIdx.x; e < TT; e += MBK) {
     const int lx = e % TN, ly = (e / TN) % TN, lz = e / (TN * TN);
     const int gx = T.bx + lx, gy = T.by + ly, gz = T.bz + lz;
@@ -564,33 +641,45 @@ __global__ void __launch_bounds__(MBK, 3) k_push_tiles(
     s_cw[e] = (gx <= d.n1 + 1 && gy <= d.n2 + 1 && gz <= d.n3 + 1) ? cw[d.c(gx, gy, gz)] : (unsigned char)1;
   }
   __syncthreads();
-  const long long N = *count;
-  const long long lo = tile_off[t];
-  long long hi = tile_off[t + 1];
-  if (hi > N) hi = N;
-  for (long long base = lo & ~3LL; base < hi; base += CHUNK) {
+  for (long long base = first; base < hi; base += CHUNK) {
     Quad Q;
     const long long i0 = base + 4 * threadIdx.x;
-    load_quad(Q, i0, lo, hi, cell, p, cap, flag);
+    quad_range(Q, i0, lo, hi);
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    if (i0 < hi) {
+      Q.c4 = *reinterpret_cast<const int4 *>(&s_st[threadIdx.x]);
+#pragma unroll
+      for (int a = 0; a < 6; ++a) Q.P[a] = s_st[(a + 1) * MBK + threadIdx.x];
+      Q.f4 = s_fl[threadIdx.x];
+    } else {
+      Q.c4 = make_int4(-1, -1, -1, -1);
+      Q.f4 = make_char4(0, 0, 0, 0);
+#pragma unroll
+      for (int a = 0; a < 6; ++a) Q.P[a] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    fetch(i0 + CHUNK);
     push_quad<BMAP, DIE, false>(d, c, m, T, i0, Q, E4, bcnd, cw, cell, p, cap, flag, kq, np, holes, nholes, acc,
                                 err);
   }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
 // The deposit of a tile's pushed particles (those the push kept: holes, flag
 // 2, skipped) into a 32-bit node tile in shared memory, flushed into the FP64
-// grid after every FLUSH_PARTICLES particles
+// grid after every FLUSH_PARTICLES particles.  Two node tiles take turns: the
+// one a window filled is flushed while the next window adds into the other,
+// so a window ends with one block barrier.
 __global__ void __launch_bounds__(MBK, 4) k_deposit_tiles(Dims d, int ntx, int nty, double kdep,
                                                         const int *__restrict__ cell, const float *__restrict__ p,
                                                         long long cap, const int *__restrict__ count,
                                                         const signed char *__restrict__ flag,
                                                         const int *__restrict__ tile_off,
                                                         const double *__restrict__ kq, double *__restrict__ np) {
-  __shared__ unsigned s_acc[TT];
+  __shared__ unsigned s_acc[2 * TT];
   const int t = blockIdx.x;
   const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
-  const Tile T{s_acc, nullptr, nullptr, tx * TC, ty * TC, tz * TC, nullptr};
-  for (int e = threadIdx.x; e < TT; e += MBK) s_acc[e] = 0u;
+  Tile T{s_acc, nullptr, nullptr, tx * TC, ty * TC, tz * TC, nullptr};
+  for (int e = threadIdx.x; e < 2 * TT; e += MBK) s_acc[e] = 0u;
   __syncthreads();
   const long long N = *count;
   const long long lo = tile_off[t];
@@ -629,9 +718,12 @@ __global__ void __launch_bounds__(MBK, 4) k_deposit_tiles(Dims d, int ntx, int n
     deposit_quad_warp(d, T, jx, jy, jz, gx, gy, gz, kdep, kq, np);
     if (++chunks == FLUSH_PARTICLES / CHUNK && base + CHUNK < hi) {
       chunks = 0;
+      // every add of this window is in T.acc, and every thread has flushed
+      // (and cleared) the other tile after the previous barrier
       __syncthreads();
-      flush_tile(d, T, kdep, kq, np);
-      __syncthreads();
+      const Tile F = T;
+      T.acc = (T.acc == s_acc) ? s_acc + TT : s_acc;
+      flush_tile(d, F, kdep, kq, np);
     }
   }
   __syncthreads();
@@ -1076,21 +1168,26 @@ int launch_push_deposit_mixed(const lepic_grid_t &g, const float *E4, lepic_spec
   // uniform kernels without walls keep their registers)
   auto run = [&](auto bmap, auto die) {
     constexpr bool B = decltype(bmap)::value, D = decltype(die)::value;
-    if (sp.tile_off)
-      k_push_tiles<B, D><<<c.ntiles, MBK, 0, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap, sp.count,
-                                                  sp.flag_dead, sp.tile_off, g.kq, np, holes, side, acc,
-                                                  ctx().d_err);
+    if (sp.tile_off) {
+      LEPIC_CUDA(cudaFuncSetAttribute(k_push_tiles<B, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_BYTES));
+      k_push_tiles<B, D><<<c.ntiles, MBK, STAGE_BYTES, s>>>(d, c, m, E, g.bcnd, g.cell_wall, sp.cell, sp.p, sp.cap,
+                                                            sp.count, sp.flag_dead, sp.tile_off, g.kq, np, holes,
+                                                            side, acc, ctx().d_err);
+    }
+    return LEPIC_OK;
   };
   const bool die = c.die.dtype != nullptr;
+  int rc;
   if (m.B && die)
-    run(std::true_type{}, std::true_type{});
+    rc = run(std::true_type{}, std::true_type{});
   else if (m.B)
-    run(std::true_type{}, std::false_type{});
+    rc = run(std::true_type{}, std::false_type{});
   else if (die)
-    run(std::false_type{}, std::true_type{});
+    rc = run(std::false_type{}, std::true_type{});
   else
-    run(std::false_type{}, std::false_type{});
+    rc = run(std::false_type{}, std::false_type{});
   timer_stop(t0, s);
+  if (rc) return rc;
   int td = timer_start("deposit_mixed_tiles", s);
   if (sp.tile_off)
     k_deposit_tiles<<<c.ntiles, MBK, 0, s>>>(d, c.ntx, c.nty, c.kdep, sp.cell, sp.p, sp.cap, sp.count, sp.flag_dead,
