@@ -284,7 +284,7 @@ def _e2e(sim, st, steps, world, dist, torch):
 # on the 96^3 workload (5.7e7 particles per species); the traffic grows in
 # proportion to the particles, so a launch's traffic is this times its
 # particles
-MEASURED_TRAFFIC_PER_PARTICLE = {"push_mixed": 57.4, "deposit_mixed_tiles": 17.0, "push_deposit_f64": 96.6}
+MEASURED_TRAFFIC_PER_PARTICLE = {"push_mixed": 56.7, "deposit_mixed_tiles": 17.5, "push_deposit_f64": 96.6}
 
 
 def _roofline(timers, kname, bytes_per_particle, nps):
@@ -788,6 +788,7 @@ def run_ours(args):
         "kernel_ms": {k: round(v[0], 3) for k, v in sorted(timers.items())},
         "kernel_launches": {k: v[1] for k, v in sorted(timers.items())},
         "roofline": _roofline(timers, kname, bpp, R["nps"]),
+        "roofline_deposit": _roofline(timers, "deposit_mixed_tiles", 17.0, R["nps"]) if head == "mixed" else None,
         "e2e": R["e2e"],
         "clocks": R["clocks"],
     }
