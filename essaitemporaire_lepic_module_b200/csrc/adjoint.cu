@@ -1519,10 +1519,13 @@ __global__ void __launch_bounds__(AB) k_cw_adj_deposit_tiles(Dims d, WinConst c,
 // adjoint solve, none when mu is null), the push of `step` undone, and the
 // adjoint of that push (lE scattered through the node box as
 // k_cw_adj_push_tiles does).  The particle's state and adjoint are read and
-// written once instead of by three kernels.  Dynamic shared memory
+// written once instead of by three kernels; a thread's next slot (history
+// word, cell, 6 planes, 6 adjoint planes) is copied into shared memory by
+// cp.async while it works on the current one.  Dynamic shared memory
 // CW_BACK_SMEM: E (float4), -q kdep kq mu (double) and lE (3 floats) of the
-// tile's node box.
-constexpr int CW_BACK_SMEM = WBN * (16 + 8 + 12);
+// tile's node box, then the staging slots (14 words per thread).
+constexpr int CW_BACK_PF = 14;
+constexpr int CW_BACK_SMEM = WBN * (16 + 8 + 12) + CW_BACK_PF * 4 * AB;
 __global__ void __launch_bounds__(AB, 2) k_cw_back_tiles(Dims d, WinConst c, const float4 *__restrict__ E,
                                                          WinS<float> S, const int *__restrict__ count, WinTiles T,
                                                          int step, const double *__restrict__ kq,
@@ -1532,6 +1535,27 @@ __global__ void __launch_bounds__(AB, 2) k_cw_back_tiles(Dims d, WinConst c, con
   float4 *s_E = reinterpret_cast<float4 *>(s_dyn);
   double *s_m = reinterpret_cast<double *>(s_dyn + 16 * WBN);
   float *s_box = reinterpret_cast<float *>(s_dyn + 24 * WBN);
+  unsigned *s_pf = reinterpret_cast<unsigned *>(s_dyn + 36 * WBN);   // [CW_BACK_PF][AB]
+  const long long N = *count;
+  const long long lo = T.off[blockIdx.x];
+  long long hi = T.off[blockIdx.x + 1];
+  if (hi > N) hi = N;
+  const long long cap = S.cap;
+  // the copies of slot i into this thread's staging words
+  auto fetch = [&](long long i) {
+    if (i < hi) {
+      unsigned *w = s_pf + threadIdx.x;
+      cp_async4(w, S.bl + i);
+      cp_async4(w + AB, S.cell + i);
+#pragma unroll
+      for (int a = 0; a < 6; ++a) {
+        cp_async4(w + (2 + a) * AB, S.p + a * cap + i);
+        cp_async4(w + (8 + a) * AB, S.lam + a * cap + i);
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  fetch(lo + threadIdx.x);
   int bx, by, bz;
   tile_box(T, blockIdx.x, bx, by, bz);
   stage_E_box(d, E, bx, by, bz, s_E);
@@ -1548,11 +1572,6 @@ __global__ void __launch_bounds__(AB, 2) k_cw_back_tiles(Dims d, WinConst c, con
   __syncthreads();
   const ETile G{d, E, s_E, bx, by, bz};
   const ENodesTile nodes{d, E, s_E, bx, by, bz};
-  const long long N = *count;
-  const long long lo = T.off[blockIdx.x];
-  long long hi = T.off[blockIdx.x + 1];
-  if (hi > N) hi = N;
-  const long long cap = S.cap;
   double gB = 0.0;
   int chunks = 0;
   for (long long base = lo; base < hi; base += AB) {
@@ -1564,12 +1583,23 @@ __global__ void __launch_bounds__(AB, 2) k_cw_back_tiles(Dims d, WinConst c, con
     int b0 = -1;
 #pragma unroll
     for (int q = 0; q < 24; ++q) r[q] = 0.f;
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    PSt<float> st;
+    float lam[6];
     if (i < hi) {
-      PSt<float> st;
-      pst_load<float>(S, i, st);
-      float lam[6];
+      const unsigned *w = s_pf + threadIdx.x;
+      st.b = (int)w[0];
+      st.cell = (int)w[AB];
 #pragma unroll
-      for (int a = 0; a < 6; ++a) lam[a] = S.lam[a * cap + i];
+      for (int a = 0; a < 3; ++a) {
+        st.f[a] = __uint_as_float(w[(2 + a) * AB]);
+        st.v[a] = __uint_as_float(w[(5 + a) * AB]);
+      }
+#pragma unroll
+      for (int a = 0; a < 6; ++a) lam[a] = __uint_as_float(w[(8 + a) * AB]);
+    }
+    fetch(i + AB);
+    if (i < hi) {
       bool lam_changed = false;
       // the deposit adjoint of step + 1, at the position before the undo
       if (mu && born_of(st.b) < step + 1 && lost_of(st.b) >= step + 1) {
@@ -1617,6 +1647,7 @@ __global__ void __launch_bounds__(AB, 2) k_cw_back_tiles(Dims d, WinConst c, con
       __syncthreads();
     }
   }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   __syncthreads();
   flush_box<3>(d, s_box, bx, by, bz, nullptr, 1.0, lE);
   block_add(gB, dBz);

@@ -425,7 +425,7 @@ __device__ __forceinline__ bool warp_run_sum(long long key, T (&v)[NV]) {
   return head && key >= 0;
 }
 
-// ------------------------------------------------------------- mbarriers
+// ------------------------------------------------ async copies and mbarriers
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ unsigned long long gtime() {
@@ -442,6 +442,15 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
       : "r"(bar), "r"(parity)
       : "memory");
   return ok != 0;
+}
+
+// per-thread asynchronous copies global -> shared (16 bytes: both 16-byte
+// aligned; 4 bytes: both 4-byte aligned), completed by cp.async.wait_group
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
 
 // wait for phase `parity` of the mbarrier, at most one second

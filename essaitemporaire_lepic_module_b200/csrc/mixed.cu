@@ -579,13 +579,6 @@ __device__ __forceinline__ void push_quad(const Dims &d, const MixedConst &c, co
 constexpr int STAGE_BYTES = MBK * (7 * 16 + 4);
 extern __shared__ __align__(16) unsigned char mx_stage[];
 
-__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
-}
-
 // one block per tile: the particles [tile_off[t], tile_off[t+1]) of the last
 // sort, clipped to the current count; E and the wall flags of the tile's box
 // are read into shared memory once, and each thread's next quad is in flight
