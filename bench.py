@@ -308,7 +308,8 @@ def _run_form(args, st, precision, rank, world, dist, torch, e2e=True):
     from essaitemporaire_lepic_module_b200.sim import Simulation
     cap = int(st.n_particles() * args.cap_factor) + 1024 if args.cap_factor else None
     sim = Simulation(st, cap=cap, seed=20240601 + 7919 * rank, nsort=args.nsort, fused=not args.unfused,
-                     precision=precision, comm=True if world > 1 else None, sort_policy=args.sort_policy)
+                     precision=precision, comm=True if world > 1 else None, sort_policy=args.sort_policy,
+                     ns_coll=args.ns_coll)
     sim.load_uniform()
     torch.cuda.synchronize()
     n_start = int(sim.counts_host().sum())
@@ -777,7 +778,7 @@ def run_ours(args):
         "dtype": "f32 particles + f64 grids" if head == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": args.workload, "form": head, "grid": list(st.n), "species": st.ntype,
                    "particles_per_species": st.n_particles(), "Bz_T": st.Bconst[2],
-                   "mcc": "Ar 1 Pa 300 K, every 10 steps", "sort_every": R["sim"].sort_every,
+                   "mcc": f"Ar 1 Pa 300 K, every {R['sim'].ns_coll} steps", "sort_every": R["sim"].sort_every,
                    "sort_policy": R["sim"].sort_policy,
                    "l2": "inputs larger than L2 (>= 7.5 GB particle state)",
                    "particles_at_start": R["n_start"]},
@@ -837,6 +838,8 @@ def main():
     ap.add_argument("--cpu-ppc", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--nsort", type=int, default=None, help="sort cadence (default: the reference's 10)")
+    ap.add_argument("--ns-coll", type=int, default=None,
+                    help="MCC every N steps (default: the workload's cadence, 10 as in the reference)")
     ap.add_argument("--sort-policy", default="adaptive", choices=["adaptive", "reference"],
                     help="adaptive: species slower than half a cell per nsort steps are sorted 10x less "
                          "often (both forms); reference: every species every nsort steps")
