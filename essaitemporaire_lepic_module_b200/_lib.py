@@ -168,6 +168,7 @@ def lib():
         "lepic_gpu_mirror_stats": ([C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), P_int], _I),
         "lepic_dev_info": ([P_int, C.c_char_p, _I], _I),
         "lepic_dev_check": ([vp, P_int], _I),
+        "lepic_dev_wait_selftest": ([C.c_longlong, vp], _I),
         "lepic_dev_calc_rho": ([C.POINTER(LepicGrid), vp, vp, _I, C.POINTER(LepicPhys), vp], _I),
         "lepic_dev_calc_efield": ([C.POINTER(LepicGrid), vp, vp, vp], _I),
         "lepic_dev_pdesolver": ([C.POINTER(LepicGrid), vp, vp, _I, _D, _D, _I, C.POINTER(LepicPhys),
@@ -301,6 +302,7 @@ def commons():
 def exported_symbols():
     """Names declared in include/lepic_gpu.h that the library must export."""
     return ["lepic_gpu_last_error", "lepic_gpu_strerror", "lepic_build_info", "lepic_dev_info", "lepic_dev_check",
+            "lepic_dev_wait_selftest",
             "lepic_gpu_set_residency", "lepic_gpu_residency", "lepic_gpu_sync_to_host",
             "lepic_gpu_update_host", "lepic_gpu_update_device", "lepic_gpu_release",
             "lepic_gpu_release_all", "lepic_gpu_mirror_zero", "lepic_gpu_mirror_copy",

@@ -270,9 +270,33 @@ const char *lepic_gpu_strerror(int code) {
 
 const char *lepic_build_info(void) {
   static char buf[128];
-  snprintf(buf, sizeof buf, "lepic_gpu sm_100a nvcc %d.%d fmad=off", __CUDACC_VER_MAJOR__,
+  snprintf(buf, sizeof buf, "lepic_gpu sm_100a nvcc %d.%d (FP64 kernels without fmad)", __CUDACC_VER_MAJOR__,
            __CUDACC_VER_MINOR__);
   return buf;
+}
+
+namespace lepic {
+namespace {
+// one block: thread 0 waits on an mbarrier phase that nothing completes, at
+// most limit_ns, then records LEPIC_ERR_TIMEOUT as a tile-copy wait does
+__global__ void k_wait_selftest(unsigned long long limit_ns, int *err) {
+  __shared__ __align__(8) unsigned long long bar;
+  const uint32_t b = smem_addr(&bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait_ns(b, 0u, limit_ns)) raise_err(err, LEPIC_ERR_TIMEOUT, 0);
+}
+}  // namespace
+}  // namespace lepic
+
+int lepic_dev_wait_selftest(long long limit_ns, void *stream) {
+  if (limit_ns <= 0 || limit_ns > 2000000000LL) return LEPIC_ERR_ARG;
+  lepic::k_wait_selftest<<<1, 32, 0, S(stream)>>>((unsigned long long)limit_ns, ctx().d_err);
+  LEPIC_CUDA(cudaGetLastError());
+  return LEPIC_OK;
 }
 
 int lepic_dev_check(void *stream, int *detail) {

@@ -453,14 +453,17 @@ __device__ __forceinline__ void cp_async4(void *dst, const void *src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
 
-// wait for phase `parity` of the mbarrier, at most one second
-__device__ inline bool mbar_wait(uint32_t bar, uint32_t parity) {
+// wait for phase `parity` of the mbarrier, at most limit_ns of %globaltimer
+__device__ inline bool mbar_wait_ns(uint32_t bar, uint32_t parity, unsigned long long limit_ns) {
   if (mbar_try(bar, parity)) return true;
   const unsigned long long t0 = gtime();
   while (!mbar_try(bar, parity))
-    if (gtime() - t0 > 1000000000ull) return false;
+    if (gtime() - t0 > limit_ns) return false;
   return true;
 }
+
+// the library's waits on copies: at most one second
+__device__ inline bool mbar_wait(uint32_t bar, uint32_t parity) { return mbar_wait_ns(bar, parity, 1000000000ull); }
 
 }  // namespace lepic
 

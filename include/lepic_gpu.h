@@ -765,6 +765,14 @@ int lepic_dev_info(int *sm_count, char *name, int name_len);
  * does).  No counterpart in the reference (it stops the run in place,
  * Src/utils.f90:529-546). */
 int lepic_dev_check(void *stream, int *detail);
+/* The failure path of the bounded device waits, for tests: one block whose
+ * first thread waits on an mbarrier phase that nothing completes, at most
+ * limit_ns (0 < limit_ns <= 2e9) nanoseconds of %globaltimer, then records
+ * LEPIC_ERR_TIMEOUT in the device error word as the library's tile-copy
+ * waits do when a copy never lands; the context stays usable.  Returns the
+ * launch status; the recorded one is read with lepic_dev_check.  No
+ * counterpart in the reference. */
+int lepic_dev_wait_selftest(long long limit_ns, void *stream);
 /* Library build identification (nvcc version, arch). */
 const char *lepic_build_info(void);
 

@@ -8,6 +8,9 @@ context stays usable afterwards.
   * a refinement cap too small for the tolerance  -> LEPIC_ERR_NOT_CONVERGED (23)
   * a NaN in the right-hand side                  -> a non-zero status, then a
                                                      clean solve succeeds
+  * a bounded device wait that nothing completes  -> LEPIC_ERR_TIMEOUT (25)
+                                                     after its limit, then the
+                                                     context runs a step
 """
 import numpy as np
 import pytest
@@ -84,3 +87,31 @@ def test_nan_in_rhs_is_reported_and_the_next_solve_works():
     sim.phi.copy_(torch.as_tensor(st.geom.phi, device="cuda"))
     it, _, res = sim.pdesolver_mixed()
     assert res < st.wl.eps and bool(torch.isfinite(sim.phi).all())
+
+
+def test_bounded_wait_times_out_and_context_stays_usable():
+    """An mbarrier phase that no copy completes: the wait gives up after its
+    limit (50 ms here; the library's copy waits allow one second) and the
+    kernel records LEPIC_ERR_TIMEOUT instead of hanging; the status is read
+    once and cleared, and a step runs afterwards."""
+    import ctypes as C
+    import time
+    import torch
+    from essaitemporaire_lepic_module_b200._lib import lib
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    torch.cuda.synchronize()
+    L = lib()
+    t0 = time.perf_counter()
+    assert L.lepic_dev_wait_selftest(50_000_000, None) == 0
+    detail = C.c_int(-1)
+    assert L.lepic_dev_check(None, C.byref(detail)) == 25
+    elapsed = time.perf_counter() - t0
+    assert 0.045 <= elapsed < 5.0, elapsed
+    assert L.lepic_dev_check(None, C.byref(detail)) == 0          # read once, then cleared
+    assert L.lepic_dev_wait_selftest(0, None) == 21                # limit out of range: LEPIC_ERR_ARG
+    st = config.build("box16")
+    sim = Simulation(st, precision="mixed")
+    sim.load_uniform()
+    sim.step()
+    torch.cuda.synchronize()
+    assert L.lepic_dev_check(None, C.byref(detail)) == 0
