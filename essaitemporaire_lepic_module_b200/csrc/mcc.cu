@@ -418,8 +418,224 @@ struct Round {
   int first;
 };
 
+// The scattering of a colliding candidate i of reaction sel
+// (Src/collisions.f90:743-1020), from the state its selection recorded:
+// the incident's velocity before, the partner, the tags of a charged target
+// and the two draws of r0 that set the scattering angles.
 template <class Acc, bool DSMC>
-__global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D, const int *__restrict__ cand,
+__device__ __forceinline__ void mcc_apply(const MCCConst &c, const Acc &S, const Targets &D, long long i, int sel, bool tgt,
+                          double vx0, double vy0, double vz0, const TState &ts, uint32_t r0z, uint32_t r0w,
+                          signed char *flag_dead, int *add, double *cnt_col, int *err) {
+  const int P = c.ptype - 1;
+  U4 ctr = {(uint32_t)i, 0u, c.c2, c.c3};
+  const U4 r0 = {0u, 0u, r0z, r0w};
+    const int rt = c.R[sel].rt;
+    const int T = c.R[sel].tt - 1;
+    const double mu_t = ts.mu, vr_t = ts.vr, vxc = ts.vxc, vyc = ts.vyc, vzc = ts.vzc;
+    // the window's record of this collision
+    lepic_win_event_t *ev = nullptr;
+    if (c.log) {
+      const int k = atomicAdd(c.nlog, 1);
+      if (k < c.log_cap) {
+        ev = c.log + k;
+        ev->step = c.step;
+        ev->P = P;
+        ev->i = (int)i;
+        ev->r = sel;
+        ev->rt = rt;
+        ev->nby = c.R[sel].n_by;
+        ev->ind = c.R[sel].ind;
+        ev->tv[0] = ts.tvx;
+        ev->tv[1] = ts.tvy;
+        ev->tv[2] = ts.tvz;
+        ev->vold[0] = vx0;
+        ev->vold[1] = vy0;
+        ev->vold[2] = vz0;
+        ev->m_t = fabs(c.mass[T]);
+        ev->Eth = c.R[sel].Eth;
+        for (int a = 0; a < MAXBY; ++a) {
+          ev->by[a] = -1;
+          ev->slot[a] = -1;
+        }
+      } else {
+        raise_err(err, LEPIC_ERR_CAPACITY, -1);
+      }
+    }
+    // P_loss(3, B) += the kinetic energy change of a particle of species
+    // B set to (nx, ny, nz) from a speed squared of o2 (0: created)
+    auto energy = [&](int B, double nx, double ny, double nz, double o2) {
+      if (c.ploss3)
+        atomicAdd(&c.ploss3[B], 0.5 * c.Nm[B] * c.mass[B] * (nx * nx + ny * ny + nz * nz - o2));
+    };
+    auto speed2 = [&](int B, long long k) {
+      double ox, oy, oz;
+      S.load_v(B, k, ox, oy, oz);
+      return ox * ox + oy * oy + oz * oz;
+    };
+    if (rt == 4) {
+      // charge exchange (Src/collisions.f90:948-998): the incident takes
+      // the target's velocity, a charged target the incident's
+      for (int a = 0; a < c.R[sel].n_by; ++a) {
+        const int bt = c.R[sel].by[a];
+        if (c.mass[bt - 1] <= 0) continue;
+        if (ev && bt == c.ptype) ev->by[a] = bt - 1;
+        if (bt == c.ptype) {
+          if (c.ploss3) energy(P, ts.tvx, ts.tvy, ts.tvz, speed2(P, i));
+          S.store_v(P, i, ts.tvx, ts.tvy, ts.tvz);
+        } else if (tgt && bt - 1 == T) {
+          if (c.ploss3) energy(T, vx0, vy0, vz0, speed2(T, ts.idx));
+          S.store_v(T, ts.idx, vx0, vy0, vz0);
+        }
+      }
+    } else {
+      double Ee = 0.5 * mu_t * (vr_t * vr_t) - c.R[sel].Eth * c.qe;
+      if (Ee < 0.0) {
+        raise_err(err, LEPIC_ERR_NEG_ENERGY, (int)i);
+        Ee = 0.0;
+      }
+      const int nby = c.R[sel].n_by;
+      double sum_mass = 0.0;
+      for (int a = 0; a < nby; ++a) sum_mass = sum_mass + 1.0 / fabs(c.mass[c.R[sel].by[a] - 1]);
+      if (ev) ev->sum_mass = sum_mass;
+      const double th_add = 2.0 * c.pi / (double)nby;
+      const double cos_th = 1.0 - 2.0 * u01(r0.z);
+      double th = acos(cos_th);
+      const double phi = 2.0 * c.pi * u01(r0.w);
+      double sin_ph, cos_ph;
+      sincos(phi, &sin_ph, &cos_ph);
+      ctr.y = 2u;
+      const U4 r2 = philox4x32_10(ctr, c.k0, c.k1);
+      const double cos_th_s = 1.0 - 2.0 * u01(r2.x);
+      const double phi_s = 2.0 * c.pi * u01(r2.y);
+      bool incident_reused = false;
+      for (int a = 0; a < nby; ++a) {
+        double sth, cth;
+        sincos(th, &sth, &cth);
+        th = th + th_add;
+        const double ex = cth, ey = sth * sin_ph, ez = sth * cos_ph;
+        double ex1 = 0, ey1 = 0, ez1 = 0;
+        scatter(ex1, ey1, ez1, ex, ey, ez, cos_th_s, phi_s);
+        const int bt = c.R[sel].by[a];
+        if (c.mass[bt - 1] <= 0) continue;
+        if (ev) {
+          ev->by[a] = bt - 1;
+          ev->e1[a][0] = (float)ex1;
+          ev->e1[a][1] = (float)ey1;
+          ev->e1[a][2] = (float)ez1;
+        }
+        const double mb = fabs(c.mass[bt - 1]);
+        const double vp = sqrt(2.0 * (Ee / sum_mass) / (mb * mb));
+        const double nvx = vxc + vp * ex1, nvy = vyc + vp * ey1, nvz = vzc + vp * ez1;
+        const bool reuse = (a == 0 && bt == c.ptype) || ((rt == 1 || rt == 3) && bt == c.ptype);
+        if (reuse) {
+          if (c.ploss3) energy(P, nvx, nvy, nvz, speed2(P, i));
+          S.store_v(P, i, nvx, nvy, nvz);
+          incident_reused = true;
+        } else if ((rt == 1 || rt == 3) && tgt && bt - 1 == T) {
+          // elastic / excitation keep a charged target (Src/collisions.f90:843-851)
+          if (c.ploss3) energy(T, nvx, nvy, nvz, speed2(T, ts.idx));
+          S.store_v(T, ts.idx, nvx, nvy, nvz);
+        } else {
+          const int B = bt - 1;
+          const int slot = atomicAdd(&add[B], 1);
+          const long long j = (long long)*S.count[B] + slot;
+          if (j >= S.cap[B]) {
+            raise_err(err, LEPIC_ERR_CAPACITY, B);
+          } else {
+            S.append(P, i, B, j, nvx, nvy, nvz);
+            if (ev) ev->slot[a] = (int)j;
+            energy(B, nvx, nvy, nvz, 0.0);
+            if (c.sxy) {
+              // the new particle's source count on the two plot planes
+              int sx, sy, sz;
+              S.cell_of(c, P, i, sx, sy, sz);
+              if (sz == c.iz_pl) atomicAdd(&c.sxy[sx + (c.n1 + 3) * (sy + (long long)(c.n2 + 3) * B)], 1);
+              if (sy == c.iy_pl) atomicAdd(&c.sxz[sx + (c.n1 + 3) * (sz + (long long)(c.n3 + 3) * B)], 1);
+            }
+          }
+        }
+      }
+      if (!incident_reused && flag_dead) flag_dead[i] = 1;
+      // other reactions remove a charged target (Src/collisions.f90:913-938)
+      if (tgt && rt != 1 && rt != 3 && D.fd[T]) D.fd[T][ts.idx] = 1;
+    }
+    if (cnt_col) {
+      int ix, iy, iz;
+      S.cell_of(c, P, i, ix, iy, iz);
+      for (int gq = 0; gq < c.n_rg; ++gq) {
+        if (ix >= c.ixl[gq] && ix <= c.ixr[gq] && iy >= c.iyl && iy <= c.iyr && iz >= c.izl &&
+            iz <= c.izr) {
+          atomicAdd(&cnt_col[(c.R[sel].ind - 1) + (long long)c.ncol_mx * gq], c.w_rg[gq]);
+          break;
+        }
+      }
+    }
+}
+
+// The colliding candidates of a warp wait in a queue in shared memory until
+// 32 of them can be scattered at once, one per lane (the selection leaves
+// most lanes of a warp without a collision).  Per warp QCAP entries, fields
+// in separate arrays: 11 doubles, 2 indices, 4 words.
+constexpr int QCAP = 64;
+constexpr int Q_WARP_BYTES = QCAP * (11 * 8 + 2 * 8 + 4 * 4);
+constexpr int Q_SMEM = (MB / 32) * Q_WARP_BYTES;
+
+struct QEntry {
+  long long i;
+  int sel, tgt;
+  double v0[3];
+  TState ts;
+  uint32_t r0z, r0w;
+};
+
+struct WarpQueue {
+  double *d;      // [11][QCAP]
+  long long *l;   // [2][QCAP]
+  int *w;         // [4][QCAP]
+  __device__ __forceinline__ void put(int k, const QEntry &e) const {
+    d[k] = e.v0[0];
+    d[QCAP + k] = e.v0[1];
+    d[2 * QCAP + k] = e.v0[2];
+    d[3 * QCAP + k] = e.ts.tvx;
+    d[4 * QCAP + k] = e.ts.tvy;
+    d[5 * QCAP + k] = e.ts.tvz;
+    d[6 * QCAP + k] = e.ts.mu;
+    d[7 * QCAP + k] = e.ts.vr;
+    d[8 * QCAP + k] = e.ts.vxc;
+    d[9 * QCAP + k] = e.ts.vyc;
+    d[10 * QCAP + k] = e.ts.vzc;
+    l[k] = e.i;
+    l[QCAP + k] = e.ts.idx;
+    w[k] = e.sel;
+    w[QCAP + k] = e.tgt;
+    w[2 * QCAP + k] = (int)e.r0z;
+    w[3 * QCAP + k] = (int)e.r0w;
+  }
+  __device__ __forceinline__ void get(int k, QEntry &e) const {
+    e.v0[0] = d[k];
+    e.v0[1] = d[QCAP + k];
+    e.v0[2] = d[2 * QCAP + k];
+    e.ts.tvx = d[3 * QCAP + k];
+    e.ts.tvy = d[4 * QCAP + k];
+    e.ts.tvz = d[5 * QCAP + k];
+    e.ts.mu = d[6 * QCAP + k];
+    e.ts.vr = d[7 * QCAP + k];
+    e.ts.vxc = d[8 * QCAP + k];
+    e.ts.vyc = d[9 * QCAP + k];
+    e.ts.vzc = d[10 * QCAP + k];
+    e.ts.Ekr = 0.0;
+    e.ts.ok = true;
+    e.i = l[k];
+    e.ts.idx = l[QCAP + k];
+    e.sel = w[k];
+    e.tgt = w[QCAP + k];
+    e.r0z = (uint32_t)w[2 * QCAP + k];
+    e.r0w = (uint32_t)w[3 * QCAP + k];
+  }
+};
+
+template <class Acc, bool DSMC>
+__global__ void __launch_bounds__(MB, 2) k_mcc_collide(MCCConst c, Acc S, Targets D, const int *__restrict__ cand,
                                                     const int *__restrict__ ncand_p,
                                                     const double *__restrict__ Er,
                                                     const double *__restrict__ sig, signed char *flag_dead,
@@ -431,9 +647,15 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
   const int lane = threadIdx.x & 31;
   const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  extern __shared__ __align__(16) unsigned char q_smem[];
+  unsigned char *qb = q_smem + (threadIdx.x >> 5) * Q_WARP_BYTES;
+  const WarpQueue Q{reinterpret_cast<double *>(qb), reinterpret_cast<long long *>(qb + 11 * 8 * QCAP),
+                    reinterpret_cast<int *>(qb + 13 * 8 * QCAP)};
+  int qn = 0;   // entries in the warp's queue (the same in every lane)
   for (long long wb = warp0 * 32; wb < ncand; wb += nwarps * 32) {
     const long long t = wb + lane;
     int sel = -1;
+    QEntry qe;
     if (t < ncand) {
       const long long i = cand[t];
       U4 ctr = {(uint32_t)i, 0u, c.c2, c.c3};
@@ -558,147 +780,43 @@ __global__ void __launch_bounds__(MB) k_mcc_collide(MCCConst c, Acc S, Targets D
         }
       }
       if (sel >= 0) {
-        const int rt = c.R[sel].rt;
-        const int T = c.R[sel].tt - 1;
-        const double mu_t = ts.mu, vr_t = ts.vr, vxc = ts.vxc, vyc = ts.vyc, vzc = ts.vzc;
-        // the window's record of this collision
-        lepic_win_event_t *ev = nullptr;
-        if (c.log) {
-          const int k = atomicAdd(c.nlog, 1);
-          if (k < c.log_cap) {
-            ev = c.log + k;
-            ev->step = c.step;
-            ev->P = P;
-            ev->i = (int)i;
-            ev->r = sel;
-            ev->rt = rt;
-            ev->nby = c.R[sel].n_by;
-            ev->ind = c.R[sel].ind;
-            ev->tv[0] = ts.tvx;
-            ev->tv[1] = ts.tvy;
-            ev->tv[2] = ts.tvz;
-            ev->vold[0] = vx0;
-            ev->vold[1] = vy0;
-            ev->vold[2] = vz0;
-            ev->m_t = fabs(c.mass[T]);
-            ev->Eth = c.R[sel].Eth;
-            for (int a = 0; a < MAXBY; ++a) {
-              ev->by[a] = -1;
-              ev->slot[a] = -1;
-            }
-          } else {
-            raise_err(err, LEPIC_ERR_CAPACITY, -1);
-          }
+        qe.i = i;
+        qe.sel = sel;
+        qe.tgt = tgt ? 1 : 0;
+        qe.v0[0] = vx0;
+        qe.v0[1] = vy0;
+        qe.v0[2] = vz0;
+        qe.ts = ts;
+        qe.r0z = r0.z;
+        qe.r0w = r0.w;
+      }
+    }
+    {
+      // the warp's colliding candidates into its queue; 32 of them
+      // scattered at once when the queue holds that many, and the rest
+      // after the warp's last candidates (one call site, uniform over the
+      // warp)
+      const unsigned m = __ballot_sync(full, sel >= 0);
+      if (sel >= 0) Q.put(qn + __popc(m & lanemask_lt_m()), qe);
+      qn += __popc(m);
+      __syncwarp();
+      const bool last = wb + nwarps * 32 >= ncand;
+      while (qn >= 32 || (last && qn > 0)) {
+        const int k = qn < 32 ? qn : 32;
+        if (lane < k) {
+          QEntry f;
+          Q.get(lane, f);
+          mcc_apply<Acc, DSMC>(c, S, D, f.i, f.sel, f.tgt != 0, f.v0[0], f.v0[1], f.v0[2], f.ts, f.r0z, f.r0w,
+                               flag_dead, add, cnt_col, err);
         }
-        // P_loss(3, B) += the kinetic energy change of a particle of species
-        // B set to (nx, ny, nz) from a speed squared of o2 (0: created)
-        auto energy = [&](int B, double nx, double ny, double nz, double o2) {
-          if (c.ploss3)
-            atomicAdd(&c.ploss3[B], 0.5 * c.Nm[B] * c.mass[B] * (nx * nx + ny * ny + nz * nz - o2));
-        };
-        auto speed2 = [&](int B, long long k) {
-          double ox, oy, oz;
-          S.load_v(B, k, ox, oy, oz);
-          return ox * ox + oy * oy + oz * oz;
-        };
-        if (rt == 4) {
-          // charge exchange (Src/collisions.f90:948-998): the incident takes
-          // the target's velocity, a charged target the incident's
-          for (int a = 0; a < c.R[sel].n_by; ++a) {
-            const int bt = c.R[sel].by[a];
-            if (c.mass[bt - 1] <= 0) continue;
-            if (ev && bt == c.ptype) ev->by[a] = bt - 1;
-            if (bt == c.ptype) {
-              if (c.ploss3) energy(P, ts.tvx, ts.tvy, ts.tvz, speed2(P, i));
-              S.store_v(P, i, ts.tvx, ts.tvy, ts.tvz);
-            } else if (tgt && bt - 1 == T) {
-              if (c.ploss3) energy(T, vx0, vy0, vz0, speed2(T, ts.idx));
-              S.store_v(T, ts.idx, vx0, vy0, vz0);
-            }
-          }
-        } else {
-          double Ee = 0.5 * mu_t * (vr_t * vr_t) - c.R[sel].Eth * c.qe;
-          if (Ee < 0.0) {
-            raise_err(err, LEPIC_ERR_NEG_ENERGY, (int)i);
-            Ee = 0.0;
-          }
-          const int nby = c.R[sel].n_by;
-          double sum_mass = 0.0;
-          for (int a = 0; a < nby; ++a) sum_mass = sum_mass + 1.0 / fabs(c.mass[c.R[sel].by[a] - 1]);
-          if (ev) ev->sum_mass = sum_mass;
-          const double th_add = 2.0 * c.pi / (double)nby;
-          const double cos_th = 1.0 - 2.0 * u01(r0.z);
-          double th = acos(cos_th);
-          const double phi = 2.0 * c.pi * u01(r0.w);
-          double sin_ph, cos_ph;
-          sincos(phi, &sin_ph, &cos_ph);
-          ctr.y = 2u;
-          const U4 r2 = philox4x32_10(ctr, c.k0, c.k1);
-          const double cos_th_s = 1.0 - 2.0 * u01(r2.x);
-          const double phi_s = 2.0 * c.pi * u01(r2.y);
-          bool incident_reused = false;
-          for (int a = 0; a < nby; ++a) {
-            double sth, cth;
-            sincos(th, &sth, &cth);
-            th = th + th_add;
-            const double ex = cth, ey = sth * sin_ph, ez = sth * cos_ph;
-            double ex1 = 0, ey1 = 0, ez1 = 0;
-            scatter(ex1, ey1, ez1, ex, ey, ez, cos_th_s, phi_s);
-            const int bt = c.R[sel].by[a];
-            if (c.mass[bt - 1] <= 0) continue;
-            if (ev) {
-              ev->by[a] = bt - 1;
-              ev->e1[a][0] = (float)ex1;
-              ev->e1[a][1] = (float)ey1;
-              ev->e1[a][2] = (float)ez1;
-            }
-            const double mb = fabs(c.mass[bt - 1]);
-            const double vp = sqrt(2.0 * (Ee / sum_mass) / (mb * mb));
-            const double nvx = vxc + vp * ex1, nvy = vyc + vp * ey1, nvz = vzc + vp * ez1;
-            const bool reuse = (a == 0 && bt == c.ptype) || ((rt == 1 || rt == 3) && bt == c.ptype);
-            if (reuse) {
-              if (c.ploss3) energy(P, nvx, nvy, nvz, speed2(P, i));
-              S.store_v(P, i, nvx, nvy, nvz);
-              incident_reused = true;
-            } else if ((rt == 1 || rt == 3) && tgt && bt - 1 == T) {
-              // elastic / excitation keep a charged target (Src/collisions.f90:843-851)
-              if (c.ploss3) energy(T, nvx, nvy, nvz, speed2(T, ts.idx));
-              S.store_v(T, ts.idx, nvx, nvy, nvz);
-            } else {
-              const int B = bt - 1;
-              const int slot = atomicAdd(&add[B], 1);
-              const long long j = (long long)*S.count[B] + slot;
-              if (j >= S.cap[B]) {
-                raise_err(err, LEPIC_ERR_CAPACITY, B);
-              } else {
-                S.append(P, i, B, j, nvx, nvy, nvz);
-                if (ev) ev->slot[a] = (int)j;
-                energy(B, nvx, nvy, nvz, 0.0);
-                if (c.sxy) {
-                  // the new particle's source count on the two plot planes
-                  int sx, sy, sz;
-                  S.cell_of(c, P, i, sx, sy, sz);
-                  if (sz == c.iz_pl) atomicAdd(&c.sxy[sx + (c.n1 + 3) * (sy + (long long)(c.n2 + 3) * B)], 1);
-                  if (sy == c.iy_pl) atomicAdd(&c.sxz[sx + (c.n1 + 3) * (sz + (long long)(c.n3 + 3) * B)], 1);
-                }
-              }
-            }
-          }
-          if (!incident_reused && flag_dead) flag_dead[i] = 1;
-          // other reactions remove a charged target (Src/collisions.f90:913-938)
-          if (tgt && rt != 1 && rt != 3 && D.fd[T]) D.fd[T][ts.idx] = 1;
+        __syncwarp();
+        if (lane < qn - k) {
+          QEntry g;
+          Q.get(k + lane, g);
+          Q.put(lane, g);
         }
-        if (cnt_col) {
-          int ix, iy, iz;
-          S.cell_of(c, P, i, ix, iy, iz);
-          for (int gq = 0; gq < c.n_rg; ++gq) {
-            if (ix >= c.ixl[gq] && ix <= c.ixr[gq] && iy >= c.iyl && iy <= c.iyr && iz >= c.izl &&
-                iz <= c.izr) {
-              atomicAdd(&cnt_col[(c.R[sel].ind - 1) + (long long)c.ncol_mx * gq], c.w_rg[gq]);
-              break;
-            }
-          }
-        }
+        qn -= k;
+        __syncwarp();
       }
     }
     // warp-aggregated collision counters
@@ -934,6 +1052,8 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
     }
     timer_stop(tm, s);
     tm = timer_start(tname, s);
+    LEPIC_CUDA(cudaFuncSetAttribute(k_mcc_collide<Acc, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, Q_SMEM));
+    LEPIC_CUDA(cudaFuncSetAttribute(k_mcc_collide<Acc, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, Q_SMEM));
     if (c.any_dsmc) {
       // rounds until no collision is deferred: the list of round r is read
       // from one buffer while the deferrals of the round go to the other
@@ -957,7 +1077,7 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
           rd.first = r == 0;
           const int *in = (r & 1) ? defer : cand;
           const int *nin = r == 0 ? ncand + (p - 1) : rc + r;
-          k_mcc_collide<Acc, true><<<ctx().sms * 8, MB, 0, s>>>(c, S, D, in, nin, T.sig_Er, T.sig,
+          k_mcc_collide<Acc, true><<<ctx().sms * 8, MB, Q_SMEM, s>>>(c, S, D, in, nin, T.sig_Er, T.sig,
                                                                 flag_dead[p - 1], add, cnt, cc, ctx().d_err, rd);
           LEPIC_CUDA(cudaGetLastError());
         }
@@ -972,7 +1092,7 @@ int run_collisions(const lepic_grid_t &g, Acc S, int *const *counts_dev, signed 
       }
     } else {
       Round rd{nullptr, nullptr, 0, 1};
-      k_mcc_collide<Acc, false><<<ctx().sms * 8, MB, 0, s>>>(c, S, D, cand, ncand + (p - 1), T.sig_Er, T.sig,
+      k_mcc_collide<Acc, false><<<ctx().sms * 8, MB, Q_SMEM, s>>>(c, S, D, cand, ncand + (p - 1), T.sig_Er, T.sig,
                                                              flag_dead[p - 1], add, cnt, cc, ctx().d_err, rd);
     }
     timer_stop(tm, s);
