@@ -346,6 +346,7 @@ __global__ void __launch_bounds__(MB) k_mcc_select(MCCConst c, const int *__rest
 // collision pass never use.  The segment is sized for about four candidates
 // per thread (a short serial chain, few threads when Pmax is tiny).
 constexpr double SKIP_PMAX = 0.25;  // above it: one draw per particle
+constexpr int SEL_BUF = 256;        // picks per warp between two reservations
 
 int skip_segment(double Pmax) {
   int seg = 256;
@@ -367,6 +368,20 @@ __global__ void __launch_bounds__(MB) k_mcc_select_skip(MCCConst c, const int *_
   uint32_t draw = 0;
   U4 r = {0u, 0u, 0u, 0u};
   int left = 0;
+  // the warp's picks gather in shared memory and reserve their range of the
+  // list with one atomic per SEL_BUF picks instead of one per round
+  __shared__ int sbuf[MB / 32][SEL_BUF];
+  int *wbuf = sbuf[threadIdx.x >> 5];
+  int nb = 0;   // picks in the warp's buffer (the same in every lane)
+  auto flush = [&]() {
+    __syncwarp();
+    int base = 0;
+    if (lane == 0) base = atomicAdd(ncand, nb);
+    base = __shfl_sync(full, base, 0);
+    for (int k = lane; k < nb; k += 32) cand[base + k] = wbuf[k];
+    __syncwarp();
+    nb = 0;
+  };
   while (__any_sync(full, live)) {
     long long pick = -1;
     if (live) {
@@ -387,13 +402,12 @@ __global__ void __launch_bounds__(MB) k_mcc_select_skip(MCCConst c, const int *_
     }
     const unsigned m = __ballot_sync(full, pick >= 0);
     if (m) {
-      const int leader = __ffs(m) - 1;
-      int base = 0;
-      if (lane == leader) base = atomicAdd(ncand, __popc(m));
-      base = __shfl_sync(full, base, leader);
-      if (pick >= 0) cand[base + __popc(m & lanemask_lt_m())] = (int)pick;
+      if (nb + 32 > SEL_BUF) flush();
+      if (pick >= 0) wbuf[nb + __popc(m & lanemask_lt_m())] = (int)pick;
+      nb += __popc(m);
     }
   }
+  if (nb) flush();
 }
 
 // pass 2: the collision physics on the candidates (grid-stride over warps so
