@@ -453,10 +453,19 @@ class CollisionWindow:
                     a = int(self.nlog.item())
                     nu = (C.c_double * 10)()
                     cnt = (C.c_longlong * 64)()
-                    check(L.lepic_dev_win_collisions(C.byref(sim.grid), self.ws, self.ntype, C.byref(sim._tables),
-                                                     C.byref(sim.P), C.c_ulonglong(self.seed), C.c_ulonglong(it), n,
-                                                     _p(self.log), self.log_cap, _p(self.nlog), nu, cnt, self._s()),
-                          "win_collisions")
+                    # Pmax = nu_max ns_coll dt with the window's own cadence
+                    # (Src/collisions.f90:122)
+                    ns0 = sim.P.ns_coll
+                    sim.P.ns_coll = self.ns_coll
+                    try:
+                        check(L.lepic_dev_win_collisions(C.byref(sim.grid), self.ws, self.ntype,
+                                                         C.byref(sim._tables), C.byref(sim.P),
+                                                         C.c_ulonglong(self.seed), C.c_ulonglong(it), n,
+                                                         _p(self.log), self.log_cap, _p(self.nlog), nu, cnt,
+                                                         self._s()),
+                              "win_collisions")
+                    finally:
+                        sim.P.ns_coll = ns0
                     self.counts[:64] += np.array(cnt[:], dtype=np.int64)
                     self.ev_range[n] = (a, int(self.nlog.item()))
                 else:

@@ -514,6 +514,9 @@ class MainLoop:
         if self.collide:
             set_commons(self.st, ncol=self.ncol, npt=self.npt, p_ncol=self.p_ncol)
             pi_ = commons()["part_info_int"]
+            # the loop's MCC cadence, which sets Pmax = nu_max ns_coll dt
+            # (Src/collisions.f90:122)
+            pi_.ns_coll = self.ns_coll
             pi_.n_rg = len(self.regions)
             for g, (lo, hi) in enumerate(self.regions):
                 pi_.ixl_rg[g], pi_.ixr_rg[g] = int(lo), int(hi)

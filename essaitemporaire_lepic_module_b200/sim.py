@@ -201,6 +201,9 @@ class Simulation:
             self.Bmap = torch.as_tensor(np.ascontiguousarray(st.bfield.Bi), dtype=torch.float64,
                                         device=self.dev)
         self.P = phys_struct(st, bmap_ptr=None if self.Bmap is None else self.Bmap.data_ptr())
+        # the collision probability of a call covers the steps since the last
+        # one (Pmax = nu_max ns_coll dt, Src/collisions.f90:122)
+        self.P.ns_coll = self.ns_coll
         self.comm = comm
         if comm is not None:
             import torch.distributed as dist

@@ -346,7 +346,7 @@ def pl_max_of(st):
     return st.n[0] + st.n[0] * (st.n[1] + st.n[1] * st.n[2]) + 1
 
 
-def collisions(st, S, err=None):
+def collisions(st, S, err=None, ns_coll=None):
     """Src/collisions.f90 with one thread, after dens_red (Src/main.f90:1194:
     np_mx of the charged species is the maximum of their density over the
     plasma nodes); charged targets (DSMC) are picked with the per-cell
@@ -357,6 +357,8 @@ def collisions(st, S, err=None):
     n = np.array(st.n, dtype=np.int32)
     h = np.ascontiguousarray(st.h)
     P = ophys(st)
+    if ns_coll is not None:
+        P.ns_coll = ns_coll          # Pmax = nu_max ns_coll dt (Src/collisions.f90:122)
     _, mx = dens_red(st, S.np)
     for p in range(st.ntype):
         P.np_mx[p] = mx[p]
@@ -442,7 +444,7 @@ def step(st, S, phi, Ei, it, p_mac=None, P_loss=None, nsort=10, ns_coll=10, mg=N
                 S.Plist[p - 1] = pl
     mcc = None
     if st.tables is not None and it > 1 and it % ns_coll == 1 % ns_coll:
-        mcc = collisions(st, S)
+        mcc = collisions(st, S, ns_coll=ns_coll)
     ng1 = st.geom.ngrid + 1
     if p_mac is None:
         p_mac = np.zeros((ng1, 2, st.ntype))
