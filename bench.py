@@ -218,15 +218,22 @@ def _timed_steps(sim, steps, world, dist, torch):
     acc = torch.zeros(1, dtype=torch.int64, device="cuda")
     counts = [s.count for s in sim.sp]
     vcycles = []
+    c0 = sim._mg_count
     e0.record()
     for _ in range(steps):
         for c in counts:
             acc += c
         sim.step()
-        vcycles.append(sim.mg_last[0])
+        if not sim.nonblocking:
+            vcycles.append(sim.mg_last[0])
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    if sim.nonblocking:
+        # the solves' refinements, copied out in stream order during the
+        # steps; statuses recorded by the last steps' kernels are read here
+        vcycles = sim.solve_history(steps) if sim._mg_count - c0 == steps else [sim.mg_last[0]]
+        sim.flush_checks()
     nps = int(acc.item())
     if world > 1:
         t = torch.tensor([ms], device="cuda")
@@ -309,7 +316,7 @@ def _run_form(args, st, precision, rank, world, dist, torch, e2e=True):
     cap = int(st.n_particles() * args.cap_factor) + 1024 if args.cap_factor else None
     sim = Simulation(st, cap=cap, seed=20240601 + 7919 * rank, nsort=args.nsort, fused=not args.unfused,
                      precision=precision, comm=True if world > 1 else None, sort_policy=args.sort_policy,
-                     ns_coll=args.ns_coll)
+                     ns_coll=args.ns_coll, nonblocking=True)
     sim.load_uniform()
     torch.cuda.synchronize()
     n_start = int(sim.counts_host().sum())

@@ -169,6 +169,7 @@ def lib():
         "lepic_dev_info": ([P_int, C.c_char_p, _I], _I),
         "lepic_dev_check": ([vp, P_int], _I),
         "lepic_dev_wait_selftest": ([C.c_longlong, vp], _I),
+        "lepic_dev_check_async": ([vp, vp], _I),
         "lepic_dev_calc_rho": ([C.POINTER(LepicGrid), vp, vp, _I, C.POINTER(LepicPhys), vp], _I),
         "lepic_dev_calc_efield": ([C.POINTER(LepicGrid), vp, vp, vp], _I),
         "lepic_dev_pdesolver": ([C.POINTER(LepicGrid), vp, vp, _I, _D, _D, _I, C.POINTER(LepicPhys),
@@ -199,6 +200,7 @@ def lib():
                                     C.c_longlong, C.c_longlong, vp], _I),
         "lepic_dev_pdesolver_mixed": ([C.POINTER(LepicGrid), vp, vp, _D, _D, _I, C.POINTER(LepicPhys),
                                        _I, _I, _I, _I, _I, _I, P_int, P_dbl, vp], _I),
+        "lepic_dev_pdesolver_mixed_stats": ([vp, vp, vp], _I),
         "lepic_dev_collisions_mixed": ([C.POINTER(LepicGrid), C.POINTER(LepicSpeciesMixed), _I,
                                         C.POINTER(LepicTables), C.POINTER(LepicPhys), C.c_ulonglong,
                                         C.c_ulonglong, P_dbl, C.POINTER(C.c_longlong), vp], _I),
@@ -302,7 +304,7 @@ def commons():
 def exported_symbols():
     """Names declared in include/lepic_gpu.h that the library must export."""
     return ["lepic_gpu_last_error", "lepic_gpu_strerror", "lepic_build_info", "lepic_dev_info", "lepic_dev_check",
-            "lepic_dev_wait_selftest",
+            "lepic_dev_wait_selftest", "lepic_dev_check_async", "lepic_dev_pdesolver_mixed_stats",
             "lepic_gpu_set_residency", "lepic_gpu_residency", "lepic_gpu_sync_to_host",
             "lepic_gpu_update_host", "lepic_gpu_update_device", "lepic_gpu_release",
             "lepic_gpu_release_all", "lepic_gpu_mirror_zero", "lepic_gpu_mirror_copy",

@@ -299,6 +299,14 @@ int lepic_dev_wait_selftest(long long limit_ns, void *stream) {
   return LEPIC_OK;
 }
 
+int lepic_dev_check_async(void *stream, int *host) {
+  if (!host) return LEPIC_ERR_ARG;
+  Ctx &c = ctx();
+  LEPIC_CUDA(cudaMemcpyAsync(host, c.d_err, 2 * sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
+  LEPIC_CUDA(cudaMemsetAsync(c.d_err, 0, 2 * sizeof(int), S(stream)));
+  return LEPIC_OK;
+}
+
 int lepic_dev_check(void *stream, int *detail) {
   Ctx &c = ctx();
   const int rc = check_err(S(stream));

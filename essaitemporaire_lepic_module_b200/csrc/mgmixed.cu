@@ -800,6 +800,12 @@ int box_map(CUtensorMap *m, float *base, const GLev &L, unsigned bx, unsigned by
 
 }  // namespace
 
+// the status of the last solve (not converged, diverged) into the device
+// error word, for a caller that does not wait for the solve
+__global__ void k_solve_status(const int *out_i, int *err) {
+  if (out_i[1] != 0) raise_err(err, out_i[1], out_i[0]);
+}
+
 int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const double *b, const int *bcnd,
                            double eps, double omega, int ng, double eps0, int max_refine, int nu_fine_pre,
                            int nu_fine_post, int nu_pre, int nu_post, int coarse_sweeps, int *iters,
@@ -935,6 +941,12 @@ int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const do
   int tm = timer_start("pdesolver_mixed", s);
   LEPIC_CUDA(cudaLaunchCooperativeKernel((void *)k_refine_mixed, dim3(blocks), dim3(XM_BLOCK), args, smem, s));
   timer_stop(tm, s);
+  if (!iters && !res_out) {
+    // no wait: the solve's status goes to the device error word
+    k_solve_status<<<1, 1, 0, s>>>(A.out_i, ctx().d_err);
+    LEPIC_CUDA(cudaGetLastError());
+    return LEPIC_OK;
+  }
   int hi[4];
   double hd[2];
   LEPIC_CUDA(cudaMemcpyAsync(hi, A.out_i, sizeof(hi), cudaMemcpyDeviceToHost, s));
@@ -946,7 +958,21 @@ int launch_pdesolver_mixed(const Dims &d, const double h[3], double *u, const do
   return hi[1];
 }
 
+int pdesolver_mixed_stats(int *iters, double *res, cudaStream_t s) {
+  if (!iters || !res) return LEPIC_ERR_ARG;
+  const int *oi = (const int *)scratch("xm_out_i", sizeof(int) * 4);
+  const double *od = (const double *)scratch("xm_out_d", sizeof(double) * 2);
+  if (!oi || !od) return LEPIC_ERR_CUDA;
+  LEPIC_CUDA(cudaMemcpyAsync(iters, oi, sizeof(int), cudaMemcpyDeviceToHost, s));
+  LEPIC_CUDA(cudaMemcpyAsync(res, od, sizeof(double), cudaMemcpyDeviceToHost, s));
+  return LEPIC_OK;
+}
+
 }  // namespace lepic
+
+extern "C" int lepic_dev_pdesolver_mixed_stats(int *iters, double *res, void *stream) {
+  return lepic::pdesolver_mixed_stats(iters, res, (cudaStream_t)stream);
+}
 
 extern "C" int lepic_dev_pdesolver_mixed(const lepic_grid_t *g, double *u, const double *b, double eps,
                                          double omega, int ng, const lepic_phys_t *P, int max_refine,

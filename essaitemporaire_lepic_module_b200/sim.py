@@ -163,7 +163,7 @@ class Simulation:
 
     def __init__(self, st, cap=None, device="cuda", seed=123456, nsort=None, ns_coll=None,
                  fused=True, precision="f64", mg_mixed=None, comm=None, sort_policy="reference",
-                 check_every=1, heating=None, injection=None):
+                 check_every=1, heating=None, injection=None, nonblocking=False):
         if precision not in ("f64", "mixed"):
             raise ValueError(f"precision must be 'f64' or 'mixed', not {precision!r}")
         if st.geom.flag_die and not st.Ca > 0.0:
@@ -194,6 +194,21 @@ class Simulation:
         # that met a bad cell, a full particle array or a collision-table
         # overflow raises LepicError at the next read
         self.check_every = int(check_every)
+        # nonblocking: the step loop never waits for the device.  The mixed
+        # solve is launched without waiting (its refinements and residual
+        # are copied into pinned host memory in stream order, read when
+        # mg_last or solve_history() is asked for), and the device error
+        # word is snapshotted into pinned memory and read at a later step,
+        # so a failure surfaces one or two steps after the step that met it
+        # (flush_checks() waits for the last snapshot).
+        self.nonblocking = bool(nonblocking)
+        self._mg_ring = 8192
+        self._mg_count = 0
+        self._mg_last_sync = None
+        self._mg_it = self._mg_res = None
+        self._err_host = None
+        self._err_ev = None
+        self._err_pending = False
         self.seed = int(seed)
         self.Bmap = None
         if getattr(st, "bfield", None) is not None:
@@ -441,10 +456,14 @@ class Simulation:
         return self.mg_last
 
     def pdesolver_mixed(self, eps=None, ng=None, **kw):
-        """FP32 V-cycles inside FP64 refinement; returns (refinements, 0, res)."""
+        """FP32 V-cycles inside FP64 refinement; returns (refinements, 0, res)
+        (None in nonblocking mode: see mg_last)."""
         wl = self.st.wl
         m = dict(self.mg_mixed)
         m.update(kw)
+        if self.nonblocking:
+            self._pdesolver_mixed_nowait(eps, ng, m)
+            return None
         it = C.c_int(0)
         res = C.c_double(0)
         check(lib().lepic_dev_pdesolver_mixed(C.byref(self.grid), _ptr(self.phi), _ptr(self.rhs),
@@ -456,6 +475,48 @@ class Simulation:
                                               self._s()), "pdesolver_mixed")
         self.mg_last = (it.value, 0.0, res.value)
         return self.mg_last
+
+    def _pdesolver_mixed_nowait(self, eps, ng, m):
+        """The mixed solve without a wait; its refinements and residual go to
+        slot (count mod ring) of the pinned history."""
+        wl = self.st.wl
+        if self._mg_it is None:
+            self._mg_it = torch.zeros(self._mg_ring, dtype=torch.int32).pin_memory()
+            self._mg_res = torch.zeros(self._mg_ring, dtype=torch.float64).pin_memory()
+        check(lib().lepic_dev_pdesolver_mixed(C.byref(self.grid), _ptr(self.phi), _ptr(self.rhs),
+                                              wl.eps if eps is None else eps, m["omega"],
+                                              self.st.ng if ng is None else ng, C.byref(self.P),
+                                              m["max_refine"], m["nu_fine_pre"], m["nu_fine_post"],
+                                              m["nu_pre"], m["nu_post"], m["coarse_sweeps"],
+                                              None, None, self._s()), "pdesolver_mixed")
+        k = self._mg_count % self._mg_ring
+        check(lib().lepic_dev_pdesolver_mixed_stats(C.c_void_p(self._mg_it[k:].data_ptr()),
+                                                    C.c_void_p(self._mg_res[k:].data_ptr()), self._s()),
+              "pdesolver_mixed_stats")
+        self._mg_count += 1
+        self._mg_last_sync = None
+
+    @property
+    def mg_last(self):
+        """(refinements or V-cycles, ktot, residual) of the last solve; in
+        nonblocking mode reading it waits for the stream."""
+        if self._mg_last_sync is None and self._mg_count:
+            self.stream.synchronize()
+            k = (self._mg_count - 1) % self._mg_ring
+            self._mg_last_sync = (int(self._mg_it[k]), 0.0, float(self._mg_res[k]))
+        return self._mg_last_sync
+
+    @mg_last.setter
+    def mg_last(self, v):
+        self._mg_last_sync = v
+
+    def solve_history(self, n):
+        """Refinements of the last n nonblocking mixed solves (waits for the
+        stream)."""
+        self.stream.synchronize()
+        n = min(n, self._mg_count, self._mg_ring)
+        idx = [(self._mg_count - n + j) % self._mg_ring for j in range(n)]
+        return [int(self._mg_it[k]) for k in idx]
 
     def efield(self):
         check(lib().lepic_dev_calc_efield(C.byref(self.grid), _ptr(self.phi), _ptr(self.Ei),
@@ -696,7 +757,39 @@ class Simulation:
 
     def check_device(self):
         """Read and clear the device error word; raise LepicError when a
-        kernel recorded a status since the last read."""
+        kernel recorded a status since the last read.  In nonblocking mode
+        the word is snapshotted into pinned memory without a wait and the
+        previous snapshot is read if the stream has passed it."""
+        if self.nonblocking:
+            if self._err_host is None:
+                self._err_host = torch.zeros(2, dtype=torch.int32).pin_memory()
+                self._err_ev = torch.cuda.Event()
+            if self._err_pending:
+                if not self._err_ev.query():
+                    return
+                self._err_pending = False
+                rc, det = int(self._err_host[0]), int(self._err_host[1])
+                if rc:
+                    check(rc, f"device status at or before step {self.it} (detail {det})")
+            check(lib().lepic_dev_check_async(self._s(), C.c_void_p(self._err_host.data_ptr())),
+                  "check_async")
+            self._err_ev.record(self.stream)
+            self._err_pending = True
+            return
+        detail = C.c_int(0)
+        rc = lib().lepic_dev_check(self._s(), C.byref(detail))
+        if rc:
+            check(rc, f"device status after step {self.it} (detail {detail.value})")
+
+    def flush_checks(self):
+        """Nonblocking mode: wait for the last snapshot of the error word and
+        read it, then read the word itself."""
+        if self._err_pending:
+            self._err_ev.synchronize()
+            self._err_pending = False
+            rc, det = int(self._err_host[0]), int(self._err_host[1])
+            if rc:
+                check(rc, f"device status at or before step {self.it} (detail {det})")
         detail = C.c_int(0)
         rc = lib().lepic_dev_check(self._s(), C.byref(detail))
         if rc:

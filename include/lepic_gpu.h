@@ -470,11 +470,20 @@ int lepic_dev_mixed_to_f64(const lepic_grid_t *g, const lepic_species_mixed_t *i
  * in FP64, until sum|r| / alpha < eps, with the sum over plasma nodes and the
  * alpha of the reference's exit test (or max_refine refinements).  One
  * cooperative launch.  iters: refinements done; res: the final
- * sum|r| / alpha. */
+ * sum|r| / alpha; the call waits for the solve and returns its status.  With
+ * iters and res both NULL it does not wait: a solve that does not converge
+ * or diverges records its status in the device error word
+ * (lepic_dev_check / lepic_dev_check_async), and
+ * lepic_dev_pdesolver_mixed_stats copies its refinements and residual out
+ * later in stream order. */
 int lepic_dev_pdesolver_mixed(const lepic_grid_t *g, double *u, const double *b, double eps,
                               double omega, int ng, const lepic_phys_t *P, int max_refine,
                               int nu_fine_pre, int nu_fine_post, int nu_pre, int nu_post,
                               int coarse_sweeps, int *iters, double *res, void *stream);
+/* Enqueues on `stream` copies of the last mixed solve's refinements and
+ * residual on this device into *iters and *res (pinned host memory); no
+ * wait: they hold the values once the stream has passed this point. */
+int lepic_dev_pdesolver_mixed_stats(int *iters, double *res, void *stream);
 /* lepic_dev_collisions for species in the mixed layout (same physics; the
  * post-collision velocities are stored in FP32). */
 int lepic_dev_collisions_mixed(const lepic_grid_t *g, lepic_species_mixed_t *sp, int ntype,
@@ -765,6 +774,13 @@ int lepic_dev_info(int *sm_count, char *name, int name_len);
  * does).  No counterpart in the reference (it stops the run in place,
  * Src/utils.f90:529-546). */
 int lepic_dev_check(void *stream, int *detail);
+/* lepic_dev_check without the wait: enqueues on `stream` a copy of the device
+ * error word (status, detail) into host[0], host[1] (pinned host memory) and
+ * clears it.  The host reads host[] once the stream has passed this point (an
+ * event recorded after the call), so a step loop sees a step's status a step
+ * or two later without stalling its launches.  Statuses recorded by kernels
+ * on other streams between the copy and the clear are lost. */
+int lepic_dev_check_async(void *stream, int *host);
 /* The failure path of the bounded device waits, for tests: one block whose
  * first thread waits on an mbarrier phase that nothing completes, at most
  * limit_ns (0 < limit_ns <= 2e9) nanoseconds of %globaltimer, then records

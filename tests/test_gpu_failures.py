@@ -115,3 +115,26 @@ def test_bounded_wait_times_out_and_context_stays_usable():
     sim.step()
     torch.cuda.synchronize()
     assert L.lepic_dev_check(None, C.byref(detail)) == 0
+
+
+def test_nonblocking_loop_reports_failures_later():
+    """Nonblocking mode (no wait in the step loop): a particle moved outside
+    the grid is reported by a later step's check or at flush_checks, with
+    the same status code, and the loop goes on afterwards."""
+    from essaitemporaire_lepic_module_b200._lib import LepicError
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    st = config.build("box16")
+    sim = Simulation(st, precision="mixed", nonblocking=True)
+    sim.load_uniform()
+    sim.step()
+    sim.flush_checks()
+    n1 = st.n[0]
+    sim.sp[0].cell[7] = (n1 + 4) | (2 << 10) | (2 << 20)
+    with pytest.raises(LepicError) as e:
+        for _ in range(4):
+            sim.step()
+        sim.flush_checks()
+    assert e.value.code == 22
+    sim.flush_checks()
+    sim.step()
+    sim.flush_checks()

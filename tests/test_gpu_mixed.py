@@ -326,3 +326,34 @@ def test_mixed_steps_with_mcc():
         em = float((mx.particles_f64(p)[3:6] ** 2).sum(dim=0).mean())
         assert abs(em / ef - 1) <= 1e-2, (p, em, ef)
     assert rel(mx.phi.cpu().numpy(), f64.phi.cpu().numpy()) <= 5e-2
+
+
+def test_nonblocking_steps_match_blocking():
+    """The step loop without waits (mixed solve launched without reading its
+    refinements, the device error word snapshotted asynchronously) moves the
+    same particles to the same phi as the blocking loop, and its solve
+    history holds the same refinements."""
+    import torch
+    from essaitemporaire_lepic_module_b200.sim import Simulation
+    st = config.build("box32")
+    runs = []
+    for nb in (False, True):
+        sim = Simulation(st, precision="mixed", seed=5, nonblocking=nb)
+        sim.load_uniform()
+        its = []
+        for _ in range(12):
+            sim.step()
+            if not nb:
+                its.append(sim.mg_last[0])
+        if nb:
+            its = sim.solve_history(12)
+            sim.flush_checks()
+        torch.cuda.synchronize()
+        runs.append((sim.phi.cpu().numpy(), list(sim.counts_host()), its, sim.mg_last[0]))
+    # the FP64 density sums are atomic (their rounding follows the thread
+    # order), so two runs agree to rounding, not bit for bit
+    (pa, ca, ia, la), (pb, cb, ib, lb) = runs
+    assert all(abs(x - y) <= 1e-4 * x + 2 for x, y in zip(ca, cb)), (ca, cb)
+    assert len(ib) == 12 and lb == ib[-1] and la == ia[-1]
+    assert all(abs(x - y) <= 1 for x, y in zip(ia, ib)), (ia, ib)
+    assert np.abs(pa - pb).max() <= 1e-6 * np.abs(pa).max()
