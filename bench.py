@@ -433,7 +433,7 @@ def run_adjoint(workload, K, every):
     Bz = torch.tensor(float(st.Bconst[2]), dtype=torch.float64, requires_grad=True)
     v0 = win.x0[3:6].clone().requires_grad_(True)
     from essaitemporaire_lepic_module_b200 import _lib
-    win.forward(V0, float(Bz))  # warm-up (allocations)
+    win.forward(V0, float(Bz.detach()))  # warm-up (allocations)
     J = window_objective(win, V, Bz, v0)
     _lib.timing(enable=True)
     _lib.timing(reset=True)
@@ -443,7 +443,7 @@ def run_adjoint(workload, K, every):
     t = dict(win.timing)
     # the FP64 reference gradient: the same window with FP64 multigrid adjoint solves
     win.adjoint_solver = "f64"
-    win.forward(V0, float(Bz))
+    win.forward(V0, float(Bz.detach()))
     rV, rB, rv = win.backward()
     tf = dict(win.timing)
     win.adjoint_solver = "mixed"
