@@ -147,13 +147,10 @@ __device__ __forceinline__ bool in_box(const Tile &T, int ix, int iy, int iz, in
          (unsigned)lz < (unsigned)(TN - 1);
 }
 
-// 8 weights of base node q (grid coordinates jx,jy,jz) into the tile when the
+// 8 weights of the cell with base node (jx,jy,jz) into the tile when the
 // cell lies in the box, else into the FP64 grid
-__device__ __forceinline__ void deposit8(const Dims &d, const Tile &T, int jx, int jy, int jz, long long q,
-                                         const int w[8], double kdep, const double *__restrict__ kq,
-                                         double *__restrict__ np) {
-  const long long sy = d.N1, sz = d.N1 * d.N2;
-  const long long o[8] = {0, 1, 1 + sy, sy, sz, 1 + sz, 1 + sy + sz, sy + sz};
+__device__ __forceinline__ void deposit8(const Dims &d, const Tile &T, int jx, int jy, int jz, const int w[8],
+                                         double kdep, const double *__restrict__ kq, double *__restrict__ np) {
   int lx, ly, lz;
   if (in_box(T, jx, jy, jz, lx, ly, lz)) {
     // shared-memory reductions on 32-bit addresses
@@ -163,6 +160,8 @@ __device__ __forceinline__ void deposit8(const Dims &d, const Tile &T, int jx, i
     for (int c = 0; c < 8; ++c)
       asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(a0 + 4u * to[c]), "r"((unsigned)w[c]) : "memory");
   } else {
+    const long long q = d.g(jx, jy, jz), sy = d.N1, sz = d.N1 * d.N2;
+    const long long o[8] = {0, 1, 1 + sy, sy, sz, 1 + sz, 1 + sy + sz, sy + sz};
 #pragma unroll
     for (int c = 0; c < 8; ++c) atomicAdd(&np[q + o[c]], __ldg(&kq[q + o[c]]) * (kdep * ((double)w[c] * QI)));
   }
@@ -292,43 +291,41 @@ __device__ __forceinline__ void deposit_quad(const Dims &d, const Tile &T, const
 #pragma unroll
       for (int cc = 0; cc < 8; ++cc) wa[cc] += w[cc];
     } else {
-      deposit8(d, T, jx[k], jy[k], jz[k], d.g(jx[k], jy[k], jz[k]), w, kdep, kq, np);
+      deposit8(d, T, jx[k], jy[k], jz[k], w, kdep, kq, np);
     }
   }
-  deposit8(d, T, ax, ay, az, d.g(ax, ay, az), wa, kdep, kq, np);
+  deposit8(d, T, ax, ay, az, wa, kdep, kq, np);
 }
 
-// deposit_quad with the first-cell sums of the warp's lanes merged per run
-// of lanes starting in one cell (sorted particles: one to three runs per
-// warp), so that a cell's 8 shared words take one add per run instead of one
-// per lane.  All 32 lanes must call this.
-__device__ __forceinline__ void deposit_quad_warp(const Dims &d, const Tile &T, const int (&jx)[4],
-                                                  const int (&jy)[4], const int (&jz)[4], const float (&gx)[4],
-                                                  const float (&gy)[4], const float (&gz)[4], double kdep,
-                                                  const double *__restrict__ kq, double *__restrict__ np) {
-  int ax = -1, ay = 0, az = 0;
+// The deposit of a lane's up to four particles given by their packed cells
+// (cc < 0: none) and offsets: those in the first particle's cell are summed,
+// then the first-cell sums of the warp's lanes are merged per run of lanes
+// starting in one cell (sorted particles: one to three runs per warp), so
+// that a cell's 8 shared words take one add per run instead of one per lane;
+// the others are added one by one.  All 32 lanes must call this.
+__device__ __forceinline__ void deposit_quad_warp(const Dims &d, const Tile &T, const int (&cc)[4],
+                                                  const float (&gx)[4], const float (&gy)[4], const float (&gz)[4],
+                                                  double kdep, const double *__restrict__ kq,
+                                                  double *__restrict__ np) {
+  int a = -1;
 #pragma unroll
-  for (int k = 0; k < 4; ++k)
-    if (ax < 0 && jx[k] >= 0) {
-      ax = jx[k];
-      ay = jy[k];
-      az = jz[k];
-    }
+  for (int k = 0; k < 4; ++k) a = (a < 0) ? cc[k] : a;
   int wa[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    if (jx[k] < 0) continue;
+    if (cc[k] < 0) continue;
     int w[8];
     qweights(gx[k], gy[k], gz[k], w);
-    if (jx[k] == ax && jy[k] == ay && jz[k] == az) {
+    if (cc[k] == a) {
 #pragma unroll
-      for (int cc = 0; cc < 8; ++cc) wa[cc] += w[cc];
+      for (int c = 0; c < 8; ++c) wa[c] += w[c];
     } else {
-      deposit8(d, T, jx[k], jy[k], jz[k], d.g(jx[k], jy[k], jz[k]), w, kdep, kq, np);
+      deposit8(d, T, (cc[k] & CM) + 1, ((cc[k] >> CB) & CM) + 1, (cc[k] >> (2 * CB)) + 1, w, kdep, kq, np);
     }
   }
-  const long long key = ax >= 0 ? d.g(ax, ay, az) : -1LL;
-  if (warp_run_sum<8, int>(key, wa)) deposit8(d, T, ax, ay, az, key, wa, kdep, kq, np);
+  // the packed cell is the run key (one value per cell, -1: none)
+  if (warp_run_sum<8, int>((long long)a, wa))
+    deposit8(d, T, (a & CM) + 1, ((a >> CB) & CM) + 1, (a >> (2 * CB)) + 1, wa, kdep, kq, np);
 }
 
 // Push + loss test + deposit of the particle quad Q starting at i0;
@@ -703,14 +700,8 @@ __global__ void __launch_bounds__(MBK, 4) k_deposit_tiles(Dims d, int ntx, int n
   int chunks = 0;
   for (long long base = lo & ~3LL; base < hi; base += CHUNK) {
     const long long i0 = base + 4 * threadIdx.x;
-    int jx[4], jy[4], jz[4];
-    float gx[4], gy[4], gz[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      jx[k] = -1;
-      jy[k] = jz[k] = 0;
-      gx[k] = gy[k] = gz[k] = 0.f;
-    }
+    int cc[4] = {-1, -1, -1, -1};
+    float gx[4] = {0.f, 0.f, 0.f, 0.f}, gy[4] = {0.f, 0.f, 0.f, 0.f}, gz[4] = {0.f, 0.f, 0.f, 0.f};
     if (i0 < hi) {
       const int4 c4 = *reinterpret_cast<const int4 *>(cell + i0);
       const char4 f4 = *reinterpret_cast<const char4 *>(flag + i0);
@@ -719,18 +710,15 @@ __global__ void __launch_bounds__(MBK, 4) k_deposit_tiles(Dims d, int ntx, int n
       const float4 P2 = *reinterpret_cast<const float4 *>(p + 2 * cap + i0);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        const int cc = (&c4.x)[k];
         if (i0 + k >= lo && i0 + k < hi && (&f4.x)[k] != 2) {
-          jx[k] = (cc & CM) + 1;
-          jy[k] = ((cc >> CB) & CM) + 1;
-          jz[k] = (cc >> (2 * CB)) + 1;
+          cc[k] = (&c4.x)[k];
           gx[k] = (&P0.x)[k];
           gy[k] = (&P1.x)[k];
           gz[k] = (&P2.x)[k];
         }
       }
     }
-    deposit_quad_warp(d, T, jx, jy, jz, gx, gy, gz, kdep, kq, np);
+    deposit_quad_warp(d, T, cc, gx, gy, gz, kdep, kq, np);
     if (++chunks == FLUSH_PARTICLES / CHUNK && base + CHUNK < hi) {
       chunks = 0;
       // every add of this window is in T.acc, and every thread has flushed
@@ -1080,7 +1068,7 @@ __global__ void k_deposit_mixed(Dims d, double kdep, const int *__restrict__ cel
   int w[8];
   qweights(p[i], p[cap + i], p[2 * cap + i], w);
   const Tile T{nullptr, nullptr, nullptr, 0, 0, 0, nullptr};
-  deposit8(d, T, ix, iy, iz, d.g(ix, iy, iz), w, kdep, kq, np);
+  deposit8(d, T, ix, iy, iz, w, kdep, kq, np);
 }
 
 bool aligned16(const void *q) { return ((uintptr_t)q & 15u) == 0; }
