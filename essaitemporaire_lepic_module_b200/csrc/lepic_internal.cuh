@@ -444,6 +444,14 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
+// a float4 from shared memory at 32-bit shared address a (a box staged
+// before a barrier and not written afterwards)
+__device__ __forceinline__ float4 lds4(uint32_t a) {
+  float4 v;
+  asm("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+  return v;
+}
+
 // per-thread asynchronous copies global -> shared (16 bytes: both 16-byte
 // aligned; 4 bytes: both 4-byte aligned), completed by cp.async.wait_group
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {

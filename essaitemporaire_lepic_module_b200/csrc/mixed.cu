@@ -130,13 +130,6 @@ __device__ __forceinline__ float gather8(float k0, float k1, float k2, float k3,
   return __fmaf_rn(k7, e7, s);
 }
 
-// a float4 from shared memory at 32-bit shared address a
-__device__ __forceinline__ float4 lds4(uint32_t a) {
-  float4 v;
-  asm("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
-  return v;
-}
-
 // box-local coordinates of cell (ix,iy,iz) when the cell's 8 nodes are in the
 // box (a block with no box, the untiled tail, has neither acc nor E)
 __device__ __forceinline__ bool in_box(const Tile &T, int ix, int iy, int iz, int &lx, int &ly, int &lz) {
